@@ -1,0 +1,944 @@
+/*
+ * lhl_oracle.c -- CPU restatement of LHLFactorization.jl's hot path.
+ *
+ * TEST INFRASTRUCTURE ONLY.  This file is the parity checker for the CUDA library and
+ * the timed CPU baseline ("port") of bench.py.  Nothing in the product path links it.
+ *
+ * Parity status: the reference is Julia and no Julia runtime exists where this build
+ * runs, so the oracle cannot be compared with the reference's own outputs.  It is pinned
+ * instead by the reference's relation tests (test/core_tests.jl), ported to pytest:
+ * reconstruction Z H Z^-1 = J, |l| <= 1, blocked ipiv == unblocked ipiv, solves against a
+ * dense LU, the bit-exact shift-LU reference of test/core_tests.jl:119-171, refinement
+ * backward errors; and by an exact-rational restatement on small integer matrices.
+ *
+ * Every function cites the reference lines it restates ("F:" = src/LHLFactorization.jl).
+ * Index conventions follow the reference: loops are 1-based, matrices column-major, and
+ * ipiv / perm / iperm hold 1-based row indices.  Floating-point operation order follows
+ * the path the reference runs for Float64 on x86-64 (vector width W = 4): explicit fused
+ * multiply-adds (fma()) exactly where the reference calls llvm.fmuladd, plain IEEE
+ * operations everywhere else.  Build with -ffp-contract=off so the compiler adds no
+ * contractions of its own.
+ *
+ * OpenMP is used only over independent rows, columns or shifts, so results do not depend
+ * on the thread count (the reference makes the same guarantee, F:708-725).
+ */
+#include <math.h>
+#include <stdint.h>
+#include <stdlib.h>
+#include <string.h>
+#ifdef _OPENMP
+#include <omp.h>
+#endif
+
+#define M1(A, ld, i, j) ((A)[(size_t)((j) - 1) * (size_t)(ld) + (size_t)((i) - 1)])
+
+static inline void dswap(double* a, double* b) { double t = *a; *a = *b; *b = t; }
+
+/* ------------------------------------------------------------------------------------ */
+/* Balancing: Parlett-Reinsch power-of-two scaling, Gauss-Seidel over i, <= 20 sweeps.    */
+/* F:299-340.                                                                              */
+/* ------------------------------------------------------------------------------------ */
+void lhlo_balance(int n, double* A, int ld, double* d, double* isc)
+{
+    for (int i = 1; i <= n; ++i) { d[i - 1] = 1.0; isc[i - 1] = 1.0; }
+    for (int sweep = 0; sweep < 20; ++sweep) {
+        int converged = 1;
+        for (int i = 1; i <= n; ++i) {
+            double c = 0.0, r = 0.0;
+            for (int j = 1; j <= n; ++j) {
+                if (j == i) continue;
+                c += fabs(M1(A, ld, j, i));
+                r += fabs(M1(A, ld, i, j));
+            }
+            if (c == 0.0 || r == 0.0) continue;
+            double f = 1.0;
+            double s = c + r;
+            while (c < r / 2.0) { c *= 2.0; r /= 2.0; f *= 2.0; }
+            while (c >= 2.0 * r) { c /= 2.0; r *= 2.0; f /= 2.0; }
+            if (c + r < 0.95 * s) {
+                converged = 0;
+                d[i - 1] *= f;
+                isc[i - 1] /= f;
+                for (int j = 1; j <= n; ++j) {
+                    M1(A, ld, i, j) /= f;
+                    M1(A, ld, j, i) *= f;
+                }
+            }
+        }
+        if (converged) break;
+    }
+}
+
+/* ------------------------------------------------------------------------------------ */
+/* Unblocked ELMHES, F:466-501.  The trailing update is the reference's row-block kernel  */
+/* for n >= 8 (F:547-678: per row, left update a = fma(l_i, -p_j, a), accumulator         */
+/* s = fma(v_j, a, s) over j = k+2..n in order, then A[i,k+1] += s) and the generic       */
+/* paired sweep below that (F:508-538).                                                    */
+/* ------------------------------------------------------------------------------------ */
+static void trailing_generic(int n, double* A, int ld, int k)
+{
+    int j = k + 2;
+    while (j + 1 <= n) {
+        double pj = M1(A, ld, k + 1, j), pj1 = M1(A, ld, k + 1, j + 1);
+        for (int i = k + 2; i <= n; ++i) {
+            double l = M1(A, ld, i, k);
+            M1(A, ld, i, j) -= l * pj;
+            M1(A, ld, i, j + 1) -= l * pj1;
+        }
+        double vj = M1(A, ld, j, k), vj1 = M1(A, ld, j + 1, k);
+        for (int i = 1; i <= n; ++i)
+            M1(A, ld, i, k + 1) += vj * M1(A, ld, i, j) + vj1 * M1(A, ld, i, j + 1);
+        j += 2;
+    }
+    if (j <= n) {
+        double pj = M1(A, ld, k + 1, j);
+        for (int i = k + 2; i <= n; ++i) M1(A, ld, i, j) -= M1(A, ld, i, k) * pj;
+        double vj = M1(A, ld, j, k);
+        for (int i = 1; i <= n; ++i) M1(A, ld, i, k + 1) += vj * M1(A, ld, i, j);
+    }
+}
+
+static void trailing_rowblock(int n, double* A, int ld, int k)
+{
+#pragma omp parallel for schedule(static) if (n >= 256)
+    for (int i = 1; i <= n; ++i) {
+        double s = 0.0;
+        if (i >= k + 2) {
+            double li = M1(A, ld, i, k);
+            for (int j = k + 2; j <= n; ++j) {
+                double a = fma(li, -M1(A, ld, k + 1, j), M1(A, ld, i, j));
+                M1(A, ld, i, j) = a;
+                s = fma(M1(A, ld, j, k), a, s);
+            }
+        } else {
+            for (int j = k + 2; j <= n; ++j) s = fma(M1(A, ld, j, k), M1(A, ld, i, j), s);
+        }
+        M1(A, ld, i, k + 1) = M1(A, ld, i, k + 1) + s;
+    }
+}
+
+void lhlo_reduce_unblocked(int n, double* A, int ld, int64_t* ipiv)
+{
+    for (int k = 1; k <= n - 2; ++k) {
+        int p = k + 1;
+        double amax = fabs(M1(A, ld, k + 1, k));
+        for (int i = k + 2; i <= n; ++i) {
+            double a = fabs(M1(A, ld, i, k));
+            if (a > amax) { amax = a; p = i; }
+        }
+        ipiv[k - 1] = p;
+        if (p != k + 1) {
+            for (int j = 1; j <= n; ++j) dswap(&M1(A, ld, k + 1, j), &M1(A, ld, p, j));
+            for (int i = 1; i <= n; ++i) dswap(&M1(A, ld, i, k + 1), &M1(A, ld, i, p));
+        }
+        double piv = M1(A, ld, k + 1, k);
+        if (piv == 0.0) continue;
+        for (int i = k + 2; i <= n; ++i) M1(A, ld, i, k) /= piv;
+        double pk = M1(A, ld, k + 1, k + 1);
+        if (pk != 0.0)
+            for (int i = k + 2; i <= n; ++i) M1(A, ld, i, k + 1) -= M1(A, ld, i, k) * pk;
+        if (n < 8) trailing_generic(n, A, ld, k);
+        else trailing_rowblock(n, A, ld, k);
+    }
+}
+
+/* ------------------------------------------------------------------------------------ */
+/* Blocked (delayed-update) reduction: the reference's generic path.                      */
+/* Driver F:765-783; panel steps F:787-850; interchanges F:857-890; row swap sweep        */
+/* F:1336-1342; deferred swaps F:1383-1393; GEMV F:1418-1440; top GEMM F:1588-1607;       */
+/* GEMM F:1676-1689; TRSM F:1917-1927.                                                     */
+/* ------------------------------------------------------------------------------------ */
+
+/* w[r0:r1] = sum_{j=c0}^{c1} A[j,k] * A[r0:r1, j], four columns per pass (F:1418-1440).  */
+static void gemv_cols(double* w, const double* A, int ld, int k, int r0, int r1, int c0, int c1)
+{
+#pragma omp parallel for schedule(static) if (r1 - r0 >= 512)
+    for (int i = r0; i <= r1; ++i) {
+        double acc = 0.0;
+        int j = c0;
+        while (j + 3 <= c1) {
+            double l1 = M1(A, ld, j, k), l2 = M1(A, ld, j + 1, k), l3 = M1(A, ld, j + 2, k),
+                   l4 = M1(A, ld, j + 3, k);
+            acc += (l1 * M1(A, ld, i, j) + l2 * M1(A, ld, i, j + 1)) +
+                   (l3 * M1(A, ld, i, j + 2) + l4 * M1(A, ld, i, j + 3));
+            j += 4;
+        }
+        while (j <= c1) {
+            double lj = M1(A, ld, j, k);
+            if (lj != 0.0) acc += lj * M1(A, ld, i, j);
+            j += 1;
+        }
+        w[i - 1] = acc;
+    }
+}
+
+/* A[i0:i1, c0:c1] += sgn * A[i0:i1, j0:j1] * A[r0:r0+K-1, cB:cB+(c1-c0)]  (F:1676-1689). */
+static void gemm_generic(double* A, int ld, int i0, int i1, int j0, int j1, int r0, int cB,
+                         int c0, int c1, double sgn)
+{
+    if (i1 < i0 || j1 < j0 || c1 < c0) return;
+#pragma omp parallel for schedule(static) if ((long)(c1 - c0 + 1) * (i1 - i0 + 1) >= 65536)
+    for (int c = c0; c <= c1; ++c) {
+        for (int j = j0; j <= j1; ++j) {
+            int jj = j - j0 + 1;
+            double b = sgn * M1(A, ld, r0 + jj - 1, cB + c - c0);
+            if (b == 0.0) continue;
+            for (int i = i0; i <= i1; ++i) M1(A, ld, i, c) += M1(A, ld, i, j) * b;
+        }
+    }
+}
+
+/* F:857-890 */
+static void step_swaps(int n, double* A, int ld, double* B0, int ldb, const int64_t* ipiv,
+                       int k0, int kb, int k, int p)
+{
+    for (int j = k0; j <= kb + 1; ++j) {
+        if (j == k) continue;
+        dswap(&M1(A, ld, k + 1, j), &M1(A, ld, p, j));
+    }
+    if (p <= kb + 1) {
+        for (int i = 1; i <= n; ++i) {
+            dswap(&M1(A, ld, i, k + 1), &M1(A, ld, i, p));
+            dswap(&M1(B0, ldb, i, k + 1 - k0), &M1(B0, ldb, i, p - k0));
+        }
+    } else {
+        for (int i = 1; i <= n; ++i) {
+            double t = M1(A, ld, i, p);
+            M1(A, ld, i, p) = M1(B0, ldb, i, k + 1 - k0);
+            M1(B0, ldb, i, k + 1 - k0) = t;
+            M1(A, ld, i, k + 1) = t;
+        }
+        for (int kk = k0; kk <= k; ++kk) {
+            int q = (int)ipiv[kk - 1];
+            if (q != kk + 1) dswap(&M1(A, ld, kk + 1, k + 1), &M1(A, ld, q, k + 1));
+        }
+        for (int kk = k0; kk <= k - 1; ++kk) {
+            double x = M1(A, ld, kk + 1, k + 1);
+            if (x == 0.0) continue;
+            for (int i = kk + 2; i <= n; ++i) M1(A, ld, i, k + 1) -= M1(A, ld, i, kk) * x;
+        }
+    }
+}
+
+/* F:787-850 (generic panel steps) */
+static void panel_steps(int n, double* A, int ld, int64_t* ipiv, double* B0, int ldb, double* w,
+                        int k0, int kb)
+{
+    for (int j = k0 + 1; j <= kb + 1; ++j)
+        for (int i = 1; i <= n; ++i) M1(B0, ldb, i, j - k0) = M1(A, ld, i, j);
+    for (int k = k0; k <= kb; ++k) {
+        int p = k + 1;
+        double amax = fabs(M1(A, ld, k + 1, k));
+        for (int i = k + 2; i <= n; ++i) {
+            double a = fabs(M1(A, ld, i, k));
+            if (a > amax) { amax = a; p = i; }
+        }
+        ipiv[k - 1] = p;
+        if (p != k + 1) {
+            dswap(&M1(A, ld, k + 1, k), &M1(A, ld, p, k));
+            step_swaps(n, A, ld, B0, ldb, ipiv, k0, kb, k, p);
+        }
+        double piv = M1(A, ld, k + 1, k);
+        if (piv == 0.0) continue;
+        for (int i = k + 2; i <= n; ++i) M1(A, ld, i, k) /= piv;
+        for (int j = k + 1; j <= kb + 1; ++j) {
+            double pj = M1(A, ld, k + 1, j);
+            if (pj == 0.0) continue;
+            for (int i = k + 2; i <= n; ++i) M1(A, ld, i, j) -= M1(A, ld, i, k) * pj;
+        }
+        for (int j = k + 2; j <= kb + 1; ++j) {
+            double vj = M1(A, ld, j, k);
+            if (vj == 0.0) continue;
+            for (int i = k0 + 1; i <= n; ++i) M1(A, ld, i, k + 1) += vj * M1(A, ld, i, j);
+        }
+        if (!(kb + 2 <= n)) continue;
+        gemv_cols(w, A, ld, k, k0 + 1, n, kb + 2, n);
+        for (int kk = k0; kk <= k; ++kk) {
+            int q = (int)ipiv[kk - 1];
+            if (q != kk + 1) dswap(&w[kk], &w[q - 1]);
+        }
+        for (int kk = k0; kk <= k; ++kk) {
+            double x = w[kk];
+            if (x == 0.0) continue;
+            for (int i = kk + 2; i <= n; ++i) w[i - 1] -= M1(A, ld, i, kk) * x;
+        }
+        for (int i = k0 + 1; i <= n; ++i) M1(A, ld, i, k + 1) += w[i - 1];
+    }
+}
+
+void lhlo_reduce_blocked(int n, double* A, int ld, int64_t* ipiv, int nb)
+{
+    if (n < 3) return;
+    int ldb = n;
+    double* B0 = (double*)malloc(sizeof(double) * (size_t)n * (size_t)(nb + 1));
+    double* w = (double*)malloc(sizeof(double) * (size_t)n);
+    for (int k0 = 1; k0 <= n - 2; k0 += nb) {
+        int kb = k0 + nb - 1 < n - 2 ? k0 + nb - 1 : n - 2;
+        panel_steps(n, A, ld, ipiv, B0, ldb, w, k0, kb);
+        if (kb + 2 <= n) {
+            /* interchange sweep on the trailing block, F:1336-1342 */
+#pragma omp parallel for schedule(static) if (n >= 512)
+            for (int c = kb + 2; c <= n; ++c)
+                for (int k = k0; k <= kb; ++k) {
+                    int p = (int)ipiv[k - 1];
+                    if (p != k + 1) dswap(&M1(A, ld, k + 1, c), &M1(A, ld, p, c));
+                }
+            /* small unit-lower TRSM on rows k0+1:kb+1, F:1917-1927 */
+#pragma omp parallel for schedule(static) if (n >= 512)
+            for (int c = kb + 2; c <= n; ++c)
+                for (int k = k0; k <= kb; ++k) {
+                    double x = M1(A, ld, k + 1, c);
+                    if (x == 0.0) continue;
+                    for (int i = k + 2; i <= kb + 1; ++i) M1(A, ld, i, c) -= M1(A, ld, i, k) * x;
+                }
+            /* rank-nb trailing GEMM, sign -1, F:777 */
+            gemm_generic(A, ld, kb + 2, n, k0, kb, k0 + 1, kb + 2, kb + 2, n, -1.0);
+        }
+        /* deferred right updates of rows 1:k0 of the panel columns, F:1588-1607 */
+        for (int k = k0; k <= kb; ++k)
+            for (int j = k + 2; j <= kb + 1; ++j) {
+                double vj = M1(A, ld, j, k);
+                if (vj == 0.0) continue;
+                for (int i = 1; i <= k0; ++i) M1(A, ld, i, k + 1) += vj * M1(A, ld, i, j);
+            }
+        for (int kk = kb + 2; kk <= n; kk += nb) {
+            int ke = kk + nb - 1 < n ? kk + nb - 1 : n;
+            gemm_generic(A, ld, 1, k0, kk, ke, kk, k0, k0 + 1, kb + 1, 1.0);
+        }
+    }
+    /* interchanges deferred on the multipliers, F:1383-1393 */
+    for (int k0 = 1; k0 <= n - 2; k0 += nb) {
+        int kb = k0 + nb - 1 < n - 2 ? k0 + nb - 1 : n - 2;
+        for (int c = k0; c <= kb; ++c)
+            for (int k = kb + 1; k <= n - 2; ++k) {
+                int p = (int)ipiv[k - 1];
+                if (p != k + 1) dswap(&M1(A, ld, k + 1, c), &M1(A, ld, p, c));
+            }
+    }
+    free(B0);
+    free(w);
+}
+
+/* ------------------------------------------------------------------------------------ */
+/* Blocked reduction, the pointer path the reference runs for Float64 (F:907-1006 and its */
+/* helpers), restated per element:                                                        */
+/*  - GEMV in 64-column groups (F:1451-1553): per row, the first four-column pass assigns */
+/*    (l1 a1 + l2 a2) + (l3 a3 + l4 a4), later passes add it, single tail columns add    */
+/*    l a (skipped when l == 0); group sums added in group order (F:1558-1583);           */
+/*  - the row kernel F:1166-1296 (interchange, pulled column, panel left / right updates, */
+/*    correction by the panel's interchanges and left transforms, pivot search);          */
+/*  - the pulled-column tables F:1088-1132;                                                */
+/*  - panel end: interchange sweep F:1344-1379, TRSM as an explicit (M^-1 - I) product    */
+/*    F:1933-2001, trailing GEMM F:1860-1911 and top GEMM F:1613-1672, where every output */
+/*    element is one fused multiply-add chain over K in order (F:1729-1857);              */
+/*  - deferred swaps F:1395-1415.                                                           */
+/* ------------------------------------------------------------------------------------ */
+#define LHL_GEMV_GROUP 64
+
+/* F:1088-1132: the pulled column p's values at rows k0+1..k+1 and at the swap partners of */
+/* steps k0..k, after those interchanges and the left transforms k0..k-1 (rows <= k+1).   */
+static int pulled_tables(const double* A, int ld, const double* RP, double* OV, int* OR, double* CX,
+                         const int64_t* ipiv, int k0, int k, int p)
+{
+    int m = k - k0 + 1;
+    for (int kk = k0; kk <= k; ++kk) {
+        OV[kk - k0] = M1(A, ld, kk + 1, p);
+        OR[kk - k0] = kk + 1;
+    }
+    int nov = m;
+    for (int kk = k0; kk <= k; ++kk) {
+        int q = (int)ipiv[kk - 1];
+        if (q == kk + 1) continue;
+        int s = -1;
+        for (int r = 0; r < nov; ++r)
+            if (OR[r] == q) { s = r; break; }
+        if (s < 0) {
+            s = nov++;
+            OV[s] = M1(A, ld, q, p);
+            OR[s] = q;
+        }
+        double a = OV[kk - k0];
+        OV[kk - k0] = OV[s];
+        OV[s] = a;
+    }
+    for (int kk = k0; kk <= k - 1; ++kk) {
+        double x = OV[kk - k0];
+        CX[kk - k0] = x;
+        if (x == 0.0) continue;
+        for (int i = kk + 2; i <= k + 1; ++i) {
+            double aik = (i == k + 1) ? RP[kk - k0] : M1(A, ld, i, kk);
+            OV[i - k0 - 1] = OV[i - k0 - 1] - aik * x;
+        }
+    }
+    return nov;
+}
+
+/* One 64-column group's partial for rows r0..r1 (F:1496-1553).  The multipliers A[c0:c1,k] */
+/* are already divided by the pivot; column psub is read from `sub`.                       */
+static void gemv_group(double* out, const double* A, int ld, int k, int r0, int r1, int c0, int c1,
+                       int psub, const double* sub)
+{
+#define COLP(j) ((j) == psub ? sub : A + (size_t)((j) - 1) * ld)
+    /* per row: the same operation order as the reference's vector loop; rows run innermost */
+    int j = c0;
+    if (j + 3 <= c1) {
+        const double *p1 = COLP(j), *p2 = COLP(j + 1), *p3 = COLP(j + 2), *p4 = COLP(j + 3);
+        double l1 = M1(A, ld, j, k), l2 = M1(A, ld, j + 1, k), l3 = M1(A, ld, j + 2, k), l4 = M1(A, ld, j + 3, k);
+        for (int i = r0; i <= r1; ++i)
+            out[i - 1] = (l1 * p1[i - 1] + l2 * p2[i - 1]) + (l3 * p3[i - 1] + l4 * p4[i - 1]);
+        j += 4;
+    } else {
+        const double* p1 = COLP(j);
+        double lj = M1(A, ld, j, k);
+        for (int i = r0; i <= r1; ++i) out[i - 1] = lj * p1[i - 1];
+        j += 1;
+    }
+    while (j + 3 <= c1) {
+        const double *p1 = COLP(j), *p2 = COLP(j + 1), *p3 = COLP(j + 2), *p4 = COLP(j + 3);
+        double l1 = M1(A, ld, j, k), l2 = M1(A, ld, j + 1, k), l3 = M1(A, ld, j + 2, k), l4 = M1(A, ld, j + 3, k);
+        for (int i = r0; i <= r1; ++i)
+            out[i - 1] = out[i - 1] + ((l1 * p1[i - 1] + l2 * p2[i - 1]) + (l3 * p3[i - 1] + l4 * p4[i - 1]));
+        j += 4;
+    }
+    while (j <= c1) {
+        double lj = M1(A, ld, j, k);
+        if (lj != 0.0) {
+            const double* p1 = COLP(j);
+            for (int i = r0; i <= r1; ++i) out[i - 1] = out[i - 1] + lj * p1[i - 1];
+        }
+        j += 1;
+    }
+#undef COLP
+}
+
+static void panel_steps_ptr(int n, double* A, int ld, int64_t* ipiv, double* B0, int ldb, double* w,
+                            double* part, int k0, int kb, int nb)
+{
+    double R1[64], RP[64], PJ[64], OV[160], CX[64], LW[64], LQ[64], XS[64];
+    int OR[160], LR[64];
+    for (int j = k0 + 1; j <= kb + 1; ++j)
+        for (int i = 1; i <= n; ++i) M1(B0, ldb, i, j - k0) = M1(A, ld, i, j);
+    for (int k = k0; k <= kb; ++k) {
+        int p = k + 1;
+        double amax = fabs(M1(A, ld, k + 1, k));
+        for (int i = k + 2; i <= n; ++i) {
+            double a = fabs(M1(A, ld, i, k));
+            if (a > amax) { amax = a; p = i; }
+        }
+        ipiv[k - 1] = p;
+        for (int j = k0; j <= kb + 1; ++j) {
+            R1[j - k0] = M1(A, ld, k + 1, j);
+            RP[j - k0] = M1(A, ld, p, j);
+        }
+        if (p != k + 1) dswap(&M1(A, ld, k + 1, k), &M1(A, ld, p, k));
+        double piv = M1(A, ld, k + 1, k);
+        int pulled = p > kb + 1;
+        if (piv == 0.0) {
+            if (p != k + 1) step_swaps(n, A, ld, B0, ldb, ipiv, k0, kb, k, p);
+            continue;
+        }
+        for (int i = k + 2; i <= kb + 1; ++i) M1(A, ld, i, k) /= piv;
+        int nov = pulled ? pulled_tables(A, ld, RP, OV, OR, CX, ipiv, k0, k, p) : 0;
+        for (int j = k + 1; j <= kb + 1; ++j) PJ[j - k - 1] = RP[j - k0];
+        if (pulled) PJ[0] = OV[k - k0];
+        else if (p != k + 1) {
+            PJ[0] = RP[p - k0];
+            PJ[p - k - 1] = RP[k + 1 - k0];
+        }
+        int trailing = kb + 2 <= n;
+        if (trailing) {
+            /* groups: scale their rows of the multiplier column, then their partials */
+            int c0 = kb + 2, P = (n - c0 + 1 + LHL_GEMV_GROUP - 1) / LHL_GEMV_GROUP;
+            const double* sub = pulled ? B0 + (size_t)(k - k0) * ldb : NULL;
+            int psub = pulled ? p : 0;
+#pragma omp parallel for schedule(static) if (n - k0 >= 256)
+            for (int g = 1; g <= P; ++g) {
+                int ga = c0 + (g - 1) * LHL_GEMV_GROUP;
+                int gb = ga + LHL_GEMV_GROUP - 1 < n ? ga + LHL_GEMV_GROUP - 1 : n;
+                for (int j = ga; j <= gb; ++j) M1(A, ld, j, k) = M1(A, ld, j, k) / piv;
+            }
+#pragma omp parallel for schedule(static) if (n - k0 >= 256)
+            for (int g = 1; g <= P; ++g) {
+                int ga = c0 + (g - 1) * LHL_GEMV_GROUP;
+                int gb = ga + LHL_GEMV_GROUP - 1 < n ? ga + LHL_GEMV_GROUP - 1 : n;
+                gemv_group(part + (size_t)(g - 1) * n, A, ld, k, k0 + 1, n, ga, gb, psub, sub);
+            }
+#pragma omp parallel for schedule(static) if (n - k0 >= 256)
+            for (int i = k0 + 1; i <= n; ++i) {
+                double s = part[i - 1];
+                for (int g = 2; g <= P; ++g) s += part[(size_t)(g - 1) * n + i - 1];
+                w[i - 1] = s;
+            }
+        }
+        /* the row kernel (F:1166-1296) over rows k0+1..n */
+        if (p != k + 1) {
+            for (int j = k0; j <= kb + 1; ++j) {
+                if (j == k) continue;
+                M1(A, ld, k + 1, j) = RP[j - k0];
+                M1(A, ld, p, j) = R1[j - k0];
+            }
+            for (int i = 1; i <= n; ++i) { /* column part of the interchange, all rows (F:1135-1161) */
+                if (p <= kb + 1) {
+                    dswap(&M1(A, ld, i, k + 1), &M1(A, ld, i, p));
+                    dswap(&M1(B0, ldb, i, k + 1 - k0), &M1(B0, ldb, i, p - k0));
+                } else {
+                    double t = M1(A, ld, i, p);
+                    M1(A, ld, i, p) = M1(B0, ldb, i, k + 1 - k0);
+                    M1(B0, ldb, i, k + 1 - k0) = t;
+                    M1(A, ld, i, k + 1) = t;
+                }
+            }
+        }
+        if (pulled) {
+            for (int r = 0; r < nov; ++r) M1(A, ld, OR[r], k + 1) = OV[r];
+            for (int kk = k0; kk <= k - 1; ++kk) {
+                double x = CX[kk - k0];
+                if (x == 0.0) continue;
+                for (int i = k + 2; i <= n; ++i)
+                    M1(A, ld, i, k + 1) = M1(A, ld, i, k + 1) - M1(A, ld, i, kk) * x;
+            }
+        }
+        for (int j = k + 1; j <= kb + 1; ++j) {
+            double pj = PJ[j - k - 1];
+            if (pj == 0.0) continue;
+            for (int i = k + 2; i <= n; ++i) M1(A, ld, i, j) = M1(A, ld, i, j) - M1(A, ld, i, k) * pj;
+        }
+        for (int j = k + 2; j <= kb + 1; ++j) {
+            double vj = M1(A, ld, j, k);
+            if (vj == 0.0) continue;
+            for (int i = k0 + 1; i <= n; ++i) M1(A, ld, i, k + 1) = M1(A, ld, i, k + 1) + vj * M1(A, ld, i, j);
+        }
+        if (trailing) {
+            int m = k - k0 + 1;
+            for (int i = k0 + 1; i <= k + 1; ++i) LW[i - k0 - 1] = w[i - 1];
+            int nq = 0;
+            for (int kk = k0; kk <= k; ++kk) {
+                int q = (int)ipiv[kk - 1];
+                if (q == kk + 1) continue;
+                if (q <= k + 1) {
+                    double a = LW[kk - k0];
+                    LW[kk - k0] = LW[q - k0 - 1];
+                    LW[q - k0 - 1] = a;
+                } else {
+                    int s = -1;
+                    for (int r = 0; r < nq; ++r)
+                        if (LR[r] == q) { s = r; break; }
+                    if (s < 0) { s = nq++; LQ[s] = w[q - 1]; LR[s] = q; }
+                    double a = LW[kk - k0];
+                    LW[kk - k0] = LQ[s];
+                    LQ[s] = a;
+                }
+            }
+            (void)m;
+            for (int kk = k0; kk <= k; ++kk) {
+                double x = LW[kk - k0];
+                XS[kk - k0] = x;
+                if (x == 0.0) continue;
+                for (int i = kk + 2; i <= k; ++i) LW[i - k0 - 1] = LW[i - k0 - 1] - M1(A, ld, i, kk) * x;
+                if (kk + 2 <= k + 1) LW[k - k0] = LW[k - k0] - RP[kk - k0] * x;
+            }
+            for (int i = k0 + 1; i <= k + 1; ++i) {
+                double v = LW[i - k0 - 1];
+                w[i - 1] = v;
+                M1(A, ld, i, k + 1) = M1(A, ld, i, k + 1) + v;
+            }
+            for (int r = 0; r < nq; ++r) w[LR[r] - 1] = LQ[r];
+            for (int kk = k0; kk <= k; ++kk) {
+                double x = XS[kk - k0];
+                if (x == 0.0) continue;
+                for (int i = k + 2; i <= n; ++i) w[i - 1] = w[i - 1] - M1(A, ld, i, kk) * x;
+            }
+            for (int i = k + 2; i <= n; ++i) M1(A, ld, i, k + 1) = M1(A, ld, i, k + 1) + w[i - 1];
+        }
+    }
+    (void)nb;
+}
+
+void lhlo_reduce_blocked_ptr(int n, double* A, int ld, int64_t* ipiv, int nb)
+{
+    if (n < 3) return;
+    int ldb = n;
+    double* B0 = (double*)malloc(sizeof(double) * (size_t)n * (size_t)(nb + 1));
+    double* w = (double*)malloc(sizeof(double) * (size_t)n);
+    int Pmax = (n + LHL_GEMV_GROUP - 1) / LHL_GEMV_GROUP;
+    double* part = (double*)malloc(sizeof(double) * (size_t)n * (size_t)Pmax);
+    double* Pm = (double*)malloc(sizeof(double) * (size_t)nb * (size_t)nb);
+    double* Tsnap = (double*)malloc(sizeof(double) * (size_t)n * (size_t)(nb + 1));
+    for (int k0 = 1; k0 <= n - 2; k0 += nb) {
+        int kb = k0 + nb - 1 < n - 2 ? k0 + nb - 1 : n - 2;
+        panel_steps_ptr(n, A, ld, ipiv, B0, ldb, w, part, k0, kb, nb);
+        if (kb + 2 <= n) {
+            int nbp = kb - k0 + 1;
+            /* P = M^-1 - I, M[r,s] = A[k0+r, k0+s-1] for r > s (F:1944-1955) */
+            for (int q = 1; q <= nbp; ++q) {
+                for (int r = 1; r <= q; ++r) Pm[(r - 1) + (size_t)(q - 1) * nbp] = 0.0;
+                for (int r = q + 1; r <= nbp; ++r) {
+                    double acc = -M1(A, ld, k0 + r, k0 + q - 1);
+                    for (int s = q + 1; s <= r - 1; ++s)
+                        acc = acc - M1(A, ld, k0 + r, k0 + s - 1) * Pm[(s - 1) + (size_t)(q - 1) * nbp];
+                    Pm[(r - 1) + (size_t)(q - 1) * nbp] = acc;
+                }
+            }
+#pragma omp parallel for schedule(static) if (n >= 512)
+            for (int c = kb + 2; c <= n; ++c) {
+                double Bs[64];
+                for (int k = k0; k <= kb; ++k) {
+                    int p = (int)ipiv[k - 1];
+                    if (p != k + 1) dswap(&M1(A, ld, k + 1, c), &M1(A, ld, p, c));
+                }
+                if (nbp >= 2) {
+                    for (int s = 1; s <= nbp; ++s) Bs[s - 1] = M1(A, ld, k0 + s, c);
+                    for (int r = 1; r <= nbp; ++r) {
+                        double v = M1(A, ld, k0 + r, c);
+                        for (int s = 1; s <= nbp; ++s) v = fma(Pm[(r - 1) + (size_t)(s - 1) * nbp], Bs[s - 1], v);
+                        M1(A, ld, k0 + r, c) = v;
+                    }
+                }
+                for (int i = kb + 2; i <= n; ++i) {
+                    double v = M1(A, ld, i, c);
+                    for (int kk = 1; kk <= nbp; ++kk)
+                        v = fma(-M1(A, ld, i, k0 + kk - 1), M1(A, ld, k0 + kk, c), v);
+                    M1(A, ld, i, c) = v;
+                }
+            }
+        }
+        /* top rows 1..k0 of the panel columns: panel part (plain), then one fma chain over
+         * j = kb+2..n per element (F:1635-1672); rows run innermost, same per-element order */
+        {
+            int ncp = kb - k0 + 1;
+            double* pre = Tsnap; /* k0 x ncp snapshot of the panel columns' top rows */
+            for (int c = k0 + 1; c <= kb + 1; ++c)
+                for (int i = 1; i <= k0; ++i) pre[(size_t)(c - k0 - 1) * k0 + i - 1] = M1(A, ld, i, c);
+#pragma omp parallel for schedule(dynamic, 1) if (k0 >= 128)
+            for (int c = k0 + 1; c <= kb + 1; ++c) {
+                double* v = A + (size_t)(c - 1) * ld;
+                for (int j = c + 1; j <= kb + 1; ++j) {
+                    double vj = M1(A, ld, j, c - 1);
+                    if (vj == 0.0) continue;
+                    const double* pj = pre + (size_t)(j - k0 - 1) * k0;
+                    for (int i = 1; i <= k0; ++i) v[i - 1] = v[i - 1] + vj * pj[i - 1];
+                }
+                for (int j = kb + 2; j <= n; ++j) {
+                    double b = M1(A, ld, j, c - 1);
+                    const double* aj = A + (size_t)(j - 1) * ld;
+                    for (int i = 1; i <= k0; ++i) v[i - 1] = fma(aj[i - 1], b, v[i - 1]);
+                }
+            }
+            (void)ncp;
+        }
+    }
+    for (int k0 = 1; k0 <= n - 2; k0 += nb) {
+        int kb = k0 + nb - 1 < n - 2 ? k0 + nb - 1 : n - 2;
+        for (int c = k0; c <= kb; ++c)
+            for (int k = kb + 1; k <= n - 2; ++k) {
+                int p = (int)ipiv[k - 1];
+                if (p != k + 1) dswap(&M1(A, ld, k + 1, c), &M1(A, ld, p, c));
+            }
+    }
+    free(B0); free(w); free(part); free(Pm); free(Tsnap);
+}
+
+/* ------------------------------------------------------------------------------------ */
+/* lhl_reduce! driver, F:355-405 (balance, path choice at n >= 500 for Float64, Ht fill   */
+/* F:2024-2039, perm / iperm F:376-387).  path: 0 = the reference's choice, 1 = unblocked,  */
+/* 2 = blocked.  F receives the n x n factors (leading dimension ldf), Ht n x n with      */
+/* Ht[j,i] = H[i,j] for i <= j+1 and zero elsewhere.                                       */
+/* ------------------------------------------------------------------------------------ */
+int lhlo_reduce(int n, const double* J, int ldj, int balance, int path, int nb, double* F, int ldf,
+                int64_t* ipiv, double* scale, double* iscale, int64_t* perm, int64_t* iperm, double* Ht)
+{
+    if (n < 0 || ldj < n || ldf < n) return -1;
+    for (int j = 1; j <= n; ++j)
+        for (int i = 1; i <= n; ++i) M1(F, ldf, i, j) = M1(J, ldj, i, j);
+    if (balance) lhlo_balance(n, F, ldf, scale, iscale);
+    else for (int i = 0; i < n; ++i) { scale[i] = 1.0; iscale[i] = 1.0; }
+    /* path: 0 = the reference's choice (pointer blocked path at n >= 500, F:398-402),
+     * 1 = unblocked, 2 = generic blocked, 3 = pointer blocked */
+    if (nb <= 0 || nb > 48) nb = 16;
+    if (path == 0) path = n >= 500 ? 3 : 1;
+    if (path == 3) lhlo_reduce_blocked_ptr(n, F, ldf, ipiv, nb);
+    else if (path == 2) lhlo_reduce_blocked(n, F, ldf, ipiv, nb);
+    else lhlo_reduce_unblocked(n, F, ldf, ipiv);
+    if (Ht) {
+        memset(Ht, 0, sizeof(double) * (size_t)n * (size_t)n);
+        for (int i = 1; i <= n; ++i)
+            for (int j = (i - 1 > 1 ? i - 1 : 1); j <= n; ++j) M1(Ht, n, j, i) = M1(F, ldf, i, j);
+    }
+    for (int i = 1; i <= n; ++i) perm[i - 1] = i;
+    for (int k = 1; k <= n - 2; ++k) {
+        int64_t p = ipiv[k - 1];
+        int64_t t = perm[k]; perm[k] = perm[p - 1]; perm[p - 1] = t;
+    }
+    for (int i = 1; i <= n; ++i) iperm[perm[i - 1] - 1] = i;
+    return 0;
+}
+
+/* ------------------------------------------------------------------------------------ */
+/* Shift LU of G = sigma I + tau H (real), F:2529-2594 == test/core_tests.jl:119-171.     */
+/* Gt is (ldg x n), column k holds row k of U (Gt[j,k] = U[k,j], j >= k); Gt[k,k+1] holds */
+/* the multiplier l_k.  Returns info (first zero pivot, 0 if none).                        */
+/* ------------------------------------------------------------------------------------ */
+int lhlo_shift(int n, const double* Ht, int ldh, double sigma, double tau, double* Gt, int ldg,
+               uint8_t* swp, double* rdiag, double* r /* work, n */)
+{
+    if (n == 0) return 0;
+    for (int j = 1; j <= n; ++j) r[j - 1] = tau * M1(Ht, ldh, j, 1);
+    r[0] = r[0] + sigma;
+    int info = 0;
+    for (int k = 1; k <= n - 1; ++k) {
+        double a = r[k - 1];
+        double b = tau * M1(Ht, ldh, k, k + 1);
+        if (fabs(b) > fabs(a)) {
+            swp[k - 1] = 1;
+            M1(Gt, ldg, k, k) = b;
+            double l = a / b;
+            M1(Gt, ldg, k, k + 1) = l;
+            for (int j = k + 1; j <= n; ++j) {
+                double g = tau * M1(Ht, ldh, j, k + 1);
+                M1(Gt, ldg, j, k) = g;
+                r[j - 1] = r[j - 1] - l * g;
+            }
+            M1(Gt, ldg, k + 1, k) = M1(Gt, ldg, k + 1, k) + sigma;
+            r[k] = r[k] - l * sigma;
+        } else {
+            swp[k - 1] = 0;
+            M1(Gt, ldg, k, k) = a;
+            double l;
+            if (a == 0.0) { if (info == 0) info = k; l = 0.0; }
+            else l = b / a;
+            M1(Gt, ldg, k, k + 1) = l;
+            for (int j = k + 1; j <= n; ++j) {
+                double rj = r[j - 1];
+                M1(Gt, ldg, j, k) = rj;
+                r[j - 1] = tau * M1(Ht, ldh, j, k + 1) - l * rj;
+            }
+            r[k] = r[k] + sigma;
+        }
+    }
+    double rn = r[n - 1];
+    M1(Gt, ldg, n, n) = rn;
+    swp[n - 1] = 0;
+    if (rn == 0.0 && info == 0) info = n;
+    for (int j = 1; j <= n; ++j) rdiag[j - 1] = 1.0 / M1(Gt, ldg, j, j);
+    return info;
+}
+
+/* ------------------------------------------------------------------------------------ */
+/* Solves.  L (the multipliers) is read from the factors F: L[i,k] = F[i,k], i >= k+2.    */
+/* Sweeps follow the Float64 padded-buffer kernels (F:2265-2434: fused multiply-adds in a */
+/* group of four steps, head triangle first); the Hessenberg solve follows F:2967-3039.  */
+/* ------------------------------------------------------------------------------------ */
+static void zinvsweep(int n, const double* F, int ldf, double* y)
+{
+    int G = (n - 2 > 0 ? n - 2 : 0) >> 2;
+    for (int g = 1; g <= G; ++g) {
+        int k = 4 * g - 3;
+        double x1 = y[k];
+        double x2 = fma(-M1(F, ldf, k + 2, k), x1, y[k + 1]);
+        y[k + 1] = x2;
+        double x3 = fma(-M1(F, ldf, k + 3, k + 1), x2, fma(-M1(F, ldf, k + 3, k), x1, y[k + 2]));
+        y[k + 2] = x3;
+        double x4 = fma(-M1(F, ldf, k + 4, k + 2), x3,
+                        fma(-M1(F, ldf, k + 4, k + 1), x2, fma(-M1(F, ldf, k + 4, k), x1, y[k + 3])));
+        y[k + 3] = x4;
+        for (int i = k + 5; i <= n; ++i) {
+            double v = y[i - 1];
+            v = fma(M1(F, ldf, i, k), -x1, v);
+            v = fma(M1(F, ldf, i, k + 1), -x2, v);
+            v = fma(M1(F, ldf, i, k + 2), -x3, v);
+            v = fma(M1(F, ldf, i, k + 3), -x4, v);
+            y[i - 1] = v;
+        }
+    }
+    for (int k = 4 * G + 1; k <= n - 2; ++k) {
+        double b = -y[k];
+        for (int i = k + 2; i <= n; ++i) y[i - 1] = fma(M1(F, ldf, i, k), b, y[i - 1]);
+    }
+}
+
+static void zsweep(int n, const double* F, int ldf, double* y)
+{
+    int G = (n - 2 > 0 ? n - 2 : 0) >> 2;
+    for (int k = n - 2; k >= 4 * G + 1; --k) {
+        double b = y[k];
+        for (int i = k + 2; i <= n; ++i) y[i - 1] = fma(M1(F, ldf, i, k), b, y[i - 1]);
+    }
+    for (int g = G; g >= 1; --g) {
+        int k = 4 * g - 3;
+        double x1 = y[k], x2 = y[k + 1], x3 = y[k + 2], x4 = y[k + 3];
+        y[k + 1] = fma(M1(F, ldf, k + 2, k), x1, x2);
+        y[k + 2] = fma(M1(F, ldf, k + 3, k + 1), x2, fma(M1(F, ldf, k + 3, k), x1, x3));
+        y[k + 3] = fma(M1(F, ldf, k + 4, k + 2), x3,
+                       fma(M1(F, ldf, k + 4, k + 1), x2, fma(M1(F, ldf, k + 4, k), x1, x4)));
+        for (int i = k + 5; i <= n; ++i) {
+            double v = y[i - 1];
+            v = fma(M1(F, ldf, i, k), x1, v);
+            v = fma(M1(F, ldf, i, k + 1), x2, v);
+            v = fma(M1(F, ldf, i, k + 2), x3, v);
+            v = fma(M1(F, ldf, i, k + 3), x4, v);
+            y[i - 1] = v;
+        }
+    }
+}
+
+/* Forward 2x2 select-swap steps F:2806-2816, then the four-row pipelined back substitution
+ * F:2967-3039 with four-lane vector accumulators (lane = (i - j - 1) mod 4) summed in
+ * lane order. */
+static void hess_solve(int n, const double* Gt, int ldg, const uint8_t* swp, const double* rd, double* y)
+{
+    for (int k = 1; k <= n - 1; ++k) {
+        int s = swp[k - 1];
+        double a = y[k - 1], b = y[k];
+        double xk = s ? b : a;
+        y[k - 1] = xk;
+        y[k] = (s ? a : b) - M1(Gt, ldg, k, k + 1) * xk;
+    }
+#define G1(i, j) M1(Gt, ldg, i, j)
+    int j = n;
+    double s1 = 0.0, s2 = 0.0, s3 = 0.0, s4 = 0.0;
+    while (j - 3 >= 1) {
+        double xj = (y[j - 1] - s1) * rd[j - 1];
+        y[j - 1] = xj;
+        s2 = fma(G1(j, j - 1), xj, s2);
+        s3 = fma(G1(j, j - 2), xj, s3);
+        s4 = fma(G1(j, j - 3), xj, s4);
+        double xj1 = (y[j - 2] - s2) * rd[j - 2];
+        y[j - 2] = xj1;
+        s3 = fma(G1(j - 1, j - 2), xj1, s3);
+        s4 = fma(G1(j - 1, j - 3), xj1, s4);
+        double xj2 = (y[j - 3] - s3) * rd[j - 3];
+        y[j - 3] = xj2;
+        s4 = fma(G1(j - 2, j - 3), xj2, s4);
+        double xj3 = (y[j - 4] - s4) * rd[j - 4];
+        y[j - 4] = xj3;
+        int jn = j - 4;
+        if (jn - 3 >= 1) {
+            double a[4][4] = {{0}};
+            for (int i = j + 1; i <= n; ++i) {
+                int lane = (i - j - 1) & 3;
+                double v = y[i - 1];
+                a[0][lane] = fma(G1(i, jn), v, a[0][lane]);
+                a[1][lane] = fma(G1(i, jn - 1), v, a[1][lane]);
+                a[2][lane] = fma(G1(i, jn - 2), v, a[2][lane]);
+                a[3][lane] = fma(G1(i, jn - 3), v, a[3][lane]);
+            }
+            double t[4];
+            for (int c = 0; c < 4; ++c) t[c] = ((a[c][0] + a[c][1]) + a[c][2]) + a[c][3];
+            s1 = t[0] + ((G1(j, jn) * xj + G1(j - 1, jn) * xj1) + (G1(j - 2, jn) * xj2 + G1(j - 3, jn) * xj3));
+            s2 = t[1] + ((G1(j, jn - 1) * xj + G1(j - 1, jn - 1) * xj1) +
+                         (G1(j - 2, jn - 1) * xj2 + G1(j - 3, jn - 1) * xj3));
+            s3 = t[2] + ((G1(j, jn - 2) * xj + G1(j - 1, jn - 2) * xj1) +
+                         (G1(j - 2, jn - 2) * xj2 + G1(j - 3, jn - 2) * xj3));
+            s4 = t[3] + ((G1(j, jn - 3) * xj + G1(j - 1, jn - 3) * xj1) +
+                         (G1(j - 2, jn - 3) * xj2 + G1(j - 3, jn - 3) * xj3));
+        }
+        j = jn;
+    }
+    while (j >= 1) {
+        double s = 0.0;
+        for (int i = j + 1; i <= n; ++i) s += G1(i, j) * y[i - 1];
+        y[j - 1] = (y[j - 1] - s) * rd[j - 1];
+        j -= 1;
+    }
+#undef G1
+}
+
+/* lhl_ldiv! for a real shift, F:3052-3068: gather, L^-1 sweep, Hessenberg solve, L sweep,
+ * scatter.  y is a work vector of length n. */
+void lhlo_ldiv(int n, const double* F, int ldf, const int64_t* perm, const int64_t* iperm,
+               const double* scale, const double* iscale, const double* Gt, int ldg,
+               const uint8_t* swp, const double* rdiag, double* x, double* y)
+{
+    for (int i = 1; i <= n; ++i) {
+        int64_t p = perm[i - 1];
+        y[i - 1] = x[p - 1] * iscale[p - 1];
+    }
+    zinvsweep(n, F, ldf, y);
+    hess_solve(n, Gt, ldg, swp, rdiag, y);
+    zsweep(n, F, ldf, y);
+    for (int i = 1; i <= n; ++i) x[i - 1] = y[iperm[i - 1] - 1] * scale[i - 1];
+}
+
+/* x <- Z x and x <- Z^-1 x (F:2069-2126), real vectors. */
+void lhlo_applyZ(int n, const double* F, int ldf, const int64_t* iperm, const double* scale,
+                 double* x, double* y)
+{
+    for (int i = 0; i < n; ++i) y[i] = x[i];
+    zsweep(n, F, ldf, y);
+    for (int i = 1; i <= n; ++i) x[i - 1] = y[iperm[i - 1] - 1] * scale[i - 1];
+}
+
+void lhlo_applyZinv(int n, const double* F, int ldf, const int64_t* perm, const double* iscale,
+                    double* x, double* y)
+{
+    for (int i = 1; i <= n; ++i) {
+        int64_t p = perm[i - 1];
+        y[i - 1] = x[p - 1] * iscale[p - 1];
+    }
+    zinvsweep(n, F, ldf, y);
+    for (int i = 0; i < n; ++i) x[i] = y[i];
+}
+
+/* lhl_refine!, F:3144-3157, with A = sigma I + tau J applied as r = sigma x + tau (J x):
+ * r = b - A x; ldiv(r); x += r; `steps` times. */
+void lhlo_refine(int n, const double* J, int ldj, double sigma, double tau, const double* b,
+                 const double* F, int ldf, const int64_t* perm, const int64_t* iperm,
+                 const double* scale, const double* iscale, const double* Gt, int ldg,
+                 const uint8_t* swp, const double* rdiag, double* x, int steps, double* r, double* y)
+{
+    for (int s = 0; s < steps; ++s) {
+        for (int i = 0; i < n; ++i) r[i] = 0.0;
+        for (int j = 1; j <= n; ++j) {
+            double xj = x[j - 1];
+            for (int i = 1; i <= n; ++i) r[i - 1] += M1(J, ldj, i, j) * xj;
+        }
+        for (int i = 0; i < n; ++i) r[i] = b[i] - (sigma * x[i] + tau * r[i]);
+        lhlo_ldiv(n, F, ldf, perm, iperm, scale, iscale, Gt, ldg, swp, rdiag, r, y);
+        for (int i = 0; i < n; ++i) x[i] += r[i];
+    }
+}
+
+/* ------------------------------------------------------------------------------------ */
+/* Batched driver used as the timed CPU baseline: S shifts, one RHS each, shift LU +      */
+/* ldiv + `steps` refinement steps per shift; shifts run in parallel (independent).       */
+/* ------------------------------------------------------------------------------------ */
+int lhlo_shift_solve_batch(int n, const double* J, int ldj, const double* Ht, const double* F, int ldf,
+                           const int64_t* perm, const int64_t* iperm, const double* scale,
+                           const double* iscale, int S, const double* sigma, const double* tau,
+                           const double* B, double* X, int steps, int* info_out)
+{
+    int ldg = n + 4;
+    int bad = 0;
+#pragma omp parallel reduction(| : bad)
+    {
+        double* Gt = (double*)calloc((size_t)ldg * (size_t)n, sizeof(double));
+        double* rd = (double*)malloc(sizeof(double) * (size_t)n);
+        uint8_t* sw = (uint8_t*)malloc((size_t)n);
+        double* w = (double*)malloc(sizeof(double) * (size_t)n * 3);
+        if (!Gt || !rd || !sw || !w) bad = 1;
+        else {
+#pragma omp for schedule(dynamic, 1)
+            for (int s = 0; s < S; ++s) {
+                int info = lhlo_shift(n, Ht, n, sigma[s], tau[s], Gt, ldg, sw, rd, w);
+                info_out[s] = info;
+                double* x = X + (size_t)s * n;
+                for (int i = 0; i < n; ++i) x[i] = B[(size_t)s * n + i];
+                lhlo_ldiv(n, F, ldf, perm, iperm, scale, iscale, Gt, ldg, sw, rd, x, w);
+                if (steps > 0)
+                    lhlo_refine(n, J, ldj, sigma[s], tau[s], B + (size_t)s * n, F, ldf, perm, iperm, scale,
+                                iscale, Gt, ldg, sw, rd, x, steps, w + n, w + 2 * (size_t)n);
+            }
+        }
+        free(Gt); free(rd); free(sw); free(w);
+    }
+    return bad ? -1 : 0;
+}
+
+int lhlo_num_threads(void)
+{
+#ifdef _OPENMP
+    return omp_get_max_threads();
+#else
+    return 1;
+#endif
+}

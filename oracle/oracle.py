@@ -1,0 +1,255 @@
+"""CPU oracle for the LHL hot path: ctypes bindings to ``liblhl_oracle.so``.
+
+TEST INFRASTRUCTURE ONLY: imported by ``tests/``, ``__graft_entry__.smoke()`` and the
+``cpu_baseline`` / ``--impl reference`` legs of ``bench.py``, always as the checker or the
+timed CPU baseline, never by the product path.
+
+The C source (``lhl_oracle.c``) restates src/LHLFactorization.jl function by function; see
+its header for what pins it.  Arrays are numpy, column-major (``order='F'``) float64;
+``ipiv``/``perm``/``iperm`` are int64 with 1-based values, like the reference's.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import subprocess
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+_LIB_PATH = os.path.join(_HERE, "liblhl_oracle.so")
+_lib = None
+
+_dp = np.ctypeslib.ndpointer(dtype=np.float64, flags="F_CONTIGUOUS")
+_dv = np.ctypeslib.ndpointer(dtype=np.float64, flags="C_CONTIGUOUS")
+_iv = np.ctypeslib.ndpointer(dtype=np.int64, flags="C_CONTIGUOUS")
+_u8 = np.ctypeslib.ndpointer(dtype=np.uint8, flags="C_CONTIGUOUS")
+_i32 = np.ctypeslib.ndpointer(dtype=np.int32, flags="C_CONTIGUOUS")
+
+
+def build() -> str:
+    """Compile the oracle with its Makefile (gcc, OpenMP)."""
+    subprocess.run(["make", "-s", "-C", _HERE], check=True)
+    return _LIB_PATH
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not os.path.exists(_LIB_PATH):
+            build()
+        L = C.CDLL(_LIB_PATH)
+        i, d = C.c_int, C.c_double
+        L.lhlo_balance.argtypes = [i, _dp, i, _dv, _dv]
+        L.lhlo_reduce_unblocked.argtypes = [i, _dp, i, _iv]
+        L.lhlo_reduce_blocked.argtypes = [i, _dp, i, _iv, i]
+        L.lhlo_reduce_blocked_ptr.argtypes = [i, _dp, i, _iv, i]
+        L.lhlo_reduce.argtypes = [i, _dp, i, i, i, i, _dp, i, _iv, _dv, _dv, _iv, _iv, _dp]
+        L.lhlo_reduce.restype = i
+        L.lhlo_shift.argtypes = [i, _dp, i, d, d, _dp, i, _u8, _dv, _dv]
+        L.lhlo_shift.restype = i
+        L.lhlo_ldiv.argtypes = [i, _dp, i, _iv, _iv, _dv, _dv, _dp, i, _u8, _dv, _dv, _dv]
+        L.lhlo_applyZ.argtypes = [i, _dp, i, _iv, _dv, _dv, _dv]
+        L.lhlo_applyZinv.argtypes = [i, _dp, i, _iv, _dv, _dv, _dv]
+        L.lhlo_refine.argtypes = [i, _dp, i, d, d, _dv, _dp, i, _iv, _iv, _dv, _dv, _dp, i, _u8, _dv,
+                                  _dv, i, _dv, _dv]
+        L.lhlo_shift_solve_batch.argtypes = [i, _dp, i, _dp, _dp, i, _iv, _iv, _dv, _dv, i, _dv, _dv,
+                                             _dp, _dp, i, _i32]
+        L.lhlo_shift_solve_batch.restype = i
+        L.lhlo_num_threads.restype = i
+        _lib = L
+    return _lib
+
+
+def num_threads() -> int:
+    return int(lib().lhlo_num_threads())
+
+
+class Reduction:
+    """The outputs of ``lhl_reduce!`` (F:355-390) for a real Float64 J."""
+
+    def __init__(self, n):
+        self.n = n
+        self.factors = np.zeros((n, n), order="F")
+        self.ipiv = np.zeros(max(n - 2, 0), dtype=np.int64)
+        self.scale = np.ones(n)
+        self.iscale = np.ones(n)
+        self.perm = np.arange(1, n + 1, dtype=np.int64)
+        self.iperm = np.arange(1, n + 1, dtype=np.int64)
+        self.Ht = np.zeros((n, n), order="F")
+
+    @property
+    def H(self):
+        return np.triu(self.factors, -1)
+
+    @property
+    def L(self):
+        """Unit lower triangular L with L[i, k+1] = factors[i, k] for i >= k+2 (0-based: i >= k+2)."""
+        n = self.n
+        Lm = np.eye(n)
+        for k in range(n - 2):
+            Lm[k + 2:, k + 1] = self.factors[k + 2:, k]
+        return Lm
+
+    def Z(self):
+        """Z = D P L as a dense matrix (columns: applyZ of unit vectors)."""
+        n = self.n
+        Zm = np.eye(n, order="F")
+        for j in range(n):
+            Zm[:, j] = apply_z(self, Zm[:, j].copy())
+        return Zm
+
+    def Zinv(self):
+        n = self.n
+        Zm = np.eye(n, order="F")
+        for j in range(n):
+            Zm[:, j] = apply_zinv(self, Zm[:, j].copy())
+        return Zm
+
+
+def _ipiv_buf(n):
+    return np.zeros(max(n - 2, 1), dtype=np.int64)
+
+
+def reduce(J, balance=True, path=0, nb=16) -> Reduction:
+    """``lhl(J; balance)``: path 0 = the reference's choice (pointer blocked at n >= 500), 1 = unblocked, 2 = generic blocked, 3 = pointer blocked."""
+    J = np.asfortranarray(J, dtype=np.float64)
+    n = J.shape[0]
+    R = Reduction(n)
+    ip = _ipiv_buf(n)
+    F = np.zeros((max(n, 1), max(n, 1)), order="F")
+    Ht = np.zeros((max(n, 1), max(n, 1)), order="F")
+    sc = np.ones(max(n, 1))
+    isc = np.ones(max(n, 1))
+    pm = np.zeros(max(n, 1), dtype=np.int64)
+    ipm = np.zeros(max(n, 1), dtype=np.int64)
+    Jp = J if n > 0 else np.zeros((1, 1), order="F")
+    rc = lib().lhlo_reduce(n, Jp, max(n, 1), int(balance), path, nb, F, max(n, 1), ip, sc, isc, pm, ipm, Ht)
+    assert rc == 0
+    R.factors = F[:n, :n].copy(order="F")
+    R.ipiv = ip[: max(n - 2, 0)].copy()
+    R.scale, R.iscale = sc[:n].copy(), isc[:n].copy()
+    R.perm, R.iperm = pm[:n].copy(), ipm[:n].copy()
+    R.Ht = Ht[:n, :n].copy(order="F")
+    return R
+
+
+def reduce_unblocked_raw(A):
+    """``_lhl_reduce_unblocked!`` on a copy of A (no balancing): returns (factors, ipiv)."""
+    A = np.array(A, dtype=np.float64, order="F", copy=True)
+    n = A.shape[0]
+    ip = _ipiv_buf(n)
+    lib().lhlo_reduce_unblocked(n, A, max(n, 1), ip)
+    return A, ip[: max(n - 2, 0)].copy()
+
+
+def reduce_blocked_raw(A, nb=16):
+    A = np.array(A, dtype=np.float64, order="F", copy=True)
+    n = A.shape[0]
+    ip = _ipiv_buf(n)
+    lib().lhlo_reduce_blocked(n, A, max(n, 1), ip, nb)
+    return A, ip[: max(n - 2, 0)].copy()
+
+
+def balance_raw(A):
+    A = np.array(A, dtype=np.float64, order="F", copy=True)
+    n = A.shape[0]
+    d = np.ones(n)
+    isc = np.ones(n)
+    lib().lhlo_balance(n, A, n, d, isc)
+    return A, d, isc
+
+
+class Shift:
+    """The outputs of ``lhl_shift!`` for a real shift (F:2456-2594)."""
+
+    def __init__(self, n):
+        self.n = n
+        self.ldg = n + 4
+        self.Gt = np.zeros((self.ldg, max(n, 1)), order="F")
+        self.swap = np.zeros(max(n, 1), dtype=np.uint8)
+        self.rdiag = np.zeros(max(n, 1))
+        self.info = 0
+        self.sigma = 0.0
+        self.tau = 0.0
+
+    def state(self):
+        """(U, l, swap, rdiag, info) exactly as test/core_tests.jl:173-190 extracts it."""
+        n = self.n
+        G = self.Gt
+        U = np.array([G[j, k] for k in range(n) for j in range(k, n)])
+        l = np.array([G[k, k + 1] for k in range(n - 1)])
+        return U, l, self.swap[:n].copy(), self.rdiag[:n].copy(), self.info
+
+
+def shift(R: Reduction, sigma, tau) -> Shift:
+    n = R.n
+    S = Shift(n)
+    w = np.zeros(max(n, 1))
+    Ht = R.Ht if n > 0 else np.zeros((1, 1), order="F")
+    S.info = int(lib().lhlo_shift(n, Ht, max(n, 1), float(sigma), float(tau), S.Gt, S.ldg, S.swap, S.rdiag, w))
+    S.sigma, S.tau = float(sigma), float(tau)
+    return S
+
+
+def ldiv(R: Reduction, S: Shift, b):
+    x = np.array(b, dtype=np.float64, copy=True)
+    y = np.zeros(max(R.n, 1))
+    lib().lhlo_ldiv(R.n, R.factors, max(R.n, 1), R.perm, R.iperm, R.scale, R.iscale, S.Gt, S.ldg, S.swap,
+                    S.rdiag, x, y)
+    return x
+
+
+def apply_z(R: Reduction, x):
+    x = np.array(x, dtype=np.float64, copy=True)
+    y = np.zeros(max(R.n, 1))
+    lib().lhlo_applyZ(R.n, R.factors, max(R.n, 1), R.iperm, R.scale, x, y)
+    return x
+
+
+def apply_zinv(R: Reduction, x):
+    x = np.array(x, dtype=np.float64, copy=True)
+    y = np.zeros(max(R.n, 1))
+    lib().lhlo_applyZinv(R.n, R.factors, max(R.n, 1), R.perm, R.iscale, x, y)
+    return x
+
+
+def refine(R: Reduction, S: Shift, J, b, x, steps=1):
+    J = np.asfortranarray(J, dtype=np.float64)
+    x = np.array(x, dtype=np.float64, copy=True)
+    b = np.ascontiguousarray(b, dtype=np.float64)
+    r = np.zeros(max(R.n, 1))
+    y = np.zeros(max(R.n, 1))
+    lib().lhlo_refine(R.n, J, max(R.n, 1), S.sigma, S.tau, b, R.factors, max(R.n, 1), R.perm, R.iperm, R.scale,
+                      R.iscale, S.Gt, S.ldg, S.swap, S.rdiag, x, steps, r, y)
+    return x
+
+
+def shift_solve_batch(R: Reduction, J, sigmas, taus, B, steps=1):
+    """S shifts, one RHS each (columns of B, n x S): shift LU + ldiv + `steps` refinements."""
+    n = R.n
+    sig = np.ascontiguousarray(sigmas, dtype=np.float64)
+    tau = np.ascontiguousarray(taus, dtype=np.float64)
+    S = sig.shape[0]
+    B = np.asfortranarray(B, dtype=np.float64)
+    X = np.zeros((n, S), order="F")
+    info = np.zeros(S, dtype=np.int32)
+    rc = lib().lhlo_shift_solve_batch(n, np.asfortranarray(J, dtype=np.float64), n, R.Ht, R.factors, n, R.perm,
+                                      R.iperm, R.scale, R.iscale, S, sig, tau, B, X, steps, info)
+    assert rc == 0
+    return X, info
+
+
+def bwd(W, x, b):
+    """The reference tests' backward error (test/core_tests.jl:3)."""
+    return np.linalg.norm(b - W @ x, np.inf) / (np.linalg.norm(W, np.inf) * np.linalg.norm(x, np.inf)
+                                                 + np.linalg.norm(b, np.inf))
+
+
+def reduce_blocked_ptr_raw(A, nb=16):
+    """The pointer blocked path (what the reference runs for Float64, n >= 500), no balancing."""
+    A = np.array(A, dtype=np.float64, order="F", copy=True)
+    n = A.shape[0]
+    ip = _ipiv_buf(n)
+    lib().lhlo_reduce_blocked_ptr(n, A, max(n, 1), ip, nb)
+    return A, ip[: max(n - 2, 0)].copy()
