@@ -1,0 +1,125 @@
+/*
+ * lhl_gpu.h -- C ABI of liblhl_gpu.so, the sm_100a (B200) implementation of
+ * LHLFactorization.jl's hot path: the ELMHES reduction J = Z H Z^-1 (Z = D P L) and the
+ * per-shift chain lhl_shift! -> Hessenberg LU -> lhl_ldiv! -> lhl_refine!.
+ *
+ * Every entry point takes plain pointers and sizes.  Matrix / vector arguments named d*
+ * are DEVICE pointers owned by the caller (a Julia CuArray, a torch tensor, cudaMalloc);
+ * the workspace and shift objects own their device scratch.  All work is enqueued on the
+ * given stream (a cudaStream_t passed as void*; NULL = the legacy default stream).
+ * Arguments are validated on the host before anything is launched.  Return value: 0 or
+ * one of the LHL_ERR_* codes.  Matrices are column-major FP64 with a leading dimension;
+ * pivot and permutation vectors are int64 with 1-based values, exactly as the reference
+ * stores them.  One workspace / shift object must not serve concurrent calls (the
+ * reference's rule, docs/src/release_notes.md:53-54, src/LHLFactorization.jl:81-82).
+ *
+ * "F:" below is src/LHLFactorization.jl of the reference.
+ */
+#ifndef LHL_GPU_H
+#define LHL_GPU_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+enum {
+    LHL_OK = 0,
+    LHL_ERR_ARG = 1,      /* ArgumentError in the reference (F:167-169, F:2463-2473, F:3084-3085) */
+    LHL_ERR_DIM = 2,      /* DimensionMismatch (F:2071, F:3056-3057) */
+    LHL_ERR_CUDA = 3,     /* a CUDA runtime call failed */
+    LHL_ERR_TIMEOUT = 4,  /* a bounded grid-barrier wait expired inside a persistent kernel */
+    LHL_ERR_ALLOC = 5     /* device allocation failed */
+};
+
+enum {
+    LHL_PREC_FP64 = 0,    /* plain form: FP64 throughout, the reference's operation order */
+    LHL_PREC_MIXED = 1    /* mixed form: FP32 reduction on tensor cores, FP64 refinement */
+};
+
+typedef struct lhl_ws_s* lhl_ws_t;       /* LHLWorkspace{Float64} (F:144-178) */
+typedef struct lhl_shift_s* lhl_shift_t; /* a batch of LHLShift{Float64} (F:84-116) */
+
+/* Device views of a workspace's reduction (all device pointers, owned by the workspace). */
+typedef struct {
+    int64_t n;
+    double* factors;  /* n x n, ld n: H in triu(factors,-1), multipliers below (F:127-129) */
+    double* Ht;       /* n x n, ld n: Ht[j,i] = H[i,j] for i <= j+1, zero elsewhere (F:2005) */
+    int64_t* ipiv;    /* n-2 pivots, 1-based (F:478) */
+    int64_t* perm;    /* P as a vector, 1-based (F:376-384) */
+    int64_t* iperm;   /* its inverse (F:385-387) */
+    double* scale;    /* balancing D (powers of two) (F:299-340) */
+    double* iscale;   /* 1 ./ scale */
+} lhl_ws_view;
+
+/* Device views of a shift batch: shift s occupies Gt + s*ldg*n, swap + s*n, ... */
+typedef struct {
+    int64_t n, nshifts, ldg;
+    double* Gt;       /* LU of sigma I + tau H transposed (F:70-73), ldg = n + 4 rows, pad zero */
+    uint8_t* swap;    /* interchanges (F:2540) */
+    double* rdiag;    /* 1 / pivots (F:2590) */
+    int32_t* info;    /* first zero pivot, 0 if none (F:2450) */
+    double* sigma;
+    double* tau;
+} lhl_shift_view;
+
+/* ---- workspace ------------------------------------------------------------------ */
+/* LHLWorkspace{Float64}(n) (F:164-178).  precision: LHL_PREC_*. */
+int lhl_ws_create(int64_t n, int precision, lhl_ws_t* ws);
+int lhl_ws_destroy(lhl_ws_t ws);
+int lhl_ws_get_view(lhl_ws_t ws, lhl_ws_view* view);
+/* Waits for the stream and reports a device-side error recorded by the last reduction
+ * (LHL_ERR_TIMEOUT from a bounded barrier wait), then clears it. */
+int lhl_ws_check(lhl_ws_t ws, void* stream);
+/* Test hook: the wall-time limit of every grid-barrier wait of this workspace's kernels. */
+int lhl_ws_set_barrier_limit_ns(lhl_ws_t ws, uint64_t limit_ns);
+
+/* lhl_reduce!(ws, J, balance) (F:355-390): balance, reduce (unblocked below n = 500,
+ * blocked with nb = 16 panels otherwise, F:398-402), fill Ht, build perm / iperm.
+ * dJ (n x n, leading dimension ldj) is not modified. */
+int lhl_reduce(lhl_ws_t ws, const double* dJ, int64_t ldj, int balance, void* stream);
+
+/* ---- shifts --------------------------------------------------------------------- */
+/* A batch of nshifts LHLShift{Float64}(n) objects (F:107-116). */
+int lhl_shift_create(int64_t n, int64_t nshifts, lhl_shift_t* sh);
+int lhl_shift_destroy(lhl_shift_t sh);
+int lhl_shift_get_view(lhl_shift_t sh, lhl_shift_view* view);
+
+/* lhl_shift!(sh, ws, sigma, tau) for shifts s0..s0+count-1 of the batch, with the
+ * shifts given as device arrays (F:2456-2594).  One launch; info per shift in the view. */
+int lhl_shift_batched(lhl_shift_t sh, lhl_ws_t ws, int64_t s0, int64_t count, const double* dsigma,
+                      const double* dtau, void* stream);
+/* lhl_shift!(ws, sigma, tau) for one shift slot with host scalars. */
+int lhl_shift(lhl_shift_t sh, lhl_ws_t ws, int64_t slot, double sigma, double tau, void* stream);
+
+/* ---- solves --------------------------------------------------------------------- */
+/* lhl_ldiv!(x, sh, ws) (F:3052-3068) for nrhs columns of dX (n x nrhs, leading dimension
+ * ldx), in place.  Column j is solved with shift slot j / rhs_per_shift. */
+int lhl_ldiv(lhl_shift_t sh, lhl_ws_t ws, double* dX, int64_t ldx, int64_t nrhs, int64_t rhs_per_shift,
+             void* stream);
+
+/* lhl_refine!(x, A, b, sh, ws, steps) (F:3144-3157) with A = sigma_s I + tau_s J applied
+ * from J (dJ, n x n, ld ldj): r = b - A x, ldiv(r), x += r, `steps` times per column.
+ * dR (n x nrhs, ld ldx) is caller scratch for the residual. */
+int lhl_refine(lhl_shift_t sh, lhl_ws_t ws, const double* dJ, int64_t ldj, const double* dB, int64_t ldb,
+               double* dX, int64_t ldx, double* dR, int64_t nrhs, int64_t rhs_per_shift, int steps,
+               void* stream);
+
+/* Relative residuals ||b - (sigma I + tau J) x||_2 / ||b||_2 per column into dres (nrhs). */
+int lhl_residual_norms(lhl_shift_t sh, const double* dJ, int64_t ldj, const double* dB, int64_t ldb,
+                       const double* dX, int64_t ldx, double* dR, double* dres, int64_t nrhs,
+                       int64_t rhs_per_shift, void* stream);
+
+/* applyZ!(x, ws) / applyZinv!(x, ws) (F:2069-2126) on nrhs columns. */
+int lhl_applyZ(lhl_ws_t ws, double* dX, int64_t ldx, int64_t nrhs, void* stream);
+int lhl_applyZinv(lhl_ws_t ws, double* dX, int64_t ldx, int64_t nrhs, void* stream);
+
+/* Library build identification (for loaders that check they bound the right .so). */
+const char* lhl_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* LHL_GPU_H */

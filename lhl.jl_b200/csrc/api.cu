@@ -1,0 +1,375 @@
+// api.cu -- the C ABI of liblhl_gpu.so (declared in include/lhl_gpu.h): argument checks
+// on the host, device buffers of the workspace and shift objects, stream-ordered launches.
+#include <stdlib.h>
+#include <string.h>
+
+#include <new>
+
+#include "internal.cuh"
+
+struct lhl_ws_s {
+    int64_t n;
+    int precision;
+    int grid;
+    double *F, *Ht, *scale, *iscale, *B0, *part, *tab, *cand_v, *buf2, *tsnap, *bsum, *bfac;
+    int64_t *ipiv, *perm, *iperm;
+    int *cand_i, *bflag, *err;
+    unsigned int* bar;
+    unsigned long long limit_ns;
+};
+
+struct lhl_shift_s {
+    int64_t n, nshifts, ldg;
+    double *Gt, *rdiag, *sigma, *tau;
+    uint8_t* swap;
+    int32_t* info;
+};
+
+static int cuda_status(cudaError_t e) { return e == cudaSuccess ? LHL_OK : LHL_ERR_CUDA; }
+
+template <class T>
+static cudaError_t dalloc(T** p, size_t count)
+{
+    *p = nullptr;
+    if (count == 0) count = 1;
+    return cudaMalloc((void**)p, count * sizeof(T));
+}
+
+static void ws_free(lhl_ws_t w)
+{
+    if (!w) return;
+    void* ptrs[] = {w->F, w->Ht, w->scale, w->iscale, w->B0, w->part, w->tab, w->cand_v, w->buf2, w->tsnap,
+                    w->bsum, w->bfac, w->ipiv, w->perm, w->iperm, w->cand_i, w->bflag, w->err, w->bar};
+    for (void* p : ptrs)
+        if (p) cudaFree(p);
+    delete w;
+}
+
+extern "C" {
+
+const char* lhl_version(void) { return "lhl_gpu 0.1 sm_100a"; }
+
+int lhl_ws_create(int64_t n, int precision, lhl_ws_t* out)
+{
+    if (!out) return LHL_ERR_ARG;
+    *out = nullptr;
+    if (n < 0 || n > 16384) return LHL_ERR_DIM;
+    if (precision != LHL_PREC_FP64 && precision != LHL_PREC_MIXED) return LHL_ERR_ARG;
+    lhl_ws_t w = new (std::nothrow) lhl_ws_s();
+    if (!w) return LHL_ERR_ALLOC;
+    memset(w, 0, sizeof(*w));
+    w->n = n;
+    w->precision = precision;
+    w->grid = lhl::reduce_grid_size();
+    w->limit_ns = 2000000000ull;  // 2 s per barrier wait
+    const size_t nn = (size_t)n * (size_t)n;
+    const size_t Pmax = (size_t)((n + 63) / 64);
+    cudaError_t e = cudaSuccess;
+#define A_(p, cnt) if (e == cudaSuccess) e = dalloc(&w->p, (cnt))
+    A_(F, nn);
+    A_(Ht, nn);
+    A_(scale, n);
+    A_(iscale, n);
+    A_(B0, (size_t)n * 17);
+    A_(part, Pmax * n);
+    A_(tab, (lhl::stepTabBytes() + 7) / 8);
+    A_(cand_v, w->grid > 0 ? w->grid : 1);
+    A_(cand_i, w->grid > 0 ? w->grid : 1);
+    A_(buf2, n < 500 ? nn : 1);
+    A_(tsnap, (size_t)n * 17);
+    A_(bsum, 2 * (size_t)n);
+    A_(bfac, n);
+    A_(ipiv, n > 2 ? n - 2 : 1);
+    A_(perm, n);
+    A_(iperm, n);
+    A_(bflag, 4);
+    A_(err, 4);
+    A_(bar, 4);
+#undef A_
+    if (e == cudaSuccess) e = cudaMemset(w->err, 0, 4 * sizeof(int));
+    if (e == cudaSuccess) e = cudaMemset(w->Ht, 0, (nn ? nn : 1) * sizeof(double));
+    if (e != cudaSuccess) {
+        ws_free(w);
+        return e == cudaErrorMemoryAllocation ? LHL_ERR_ALLOC : LHL_ERR_CUDA;
+    }
+    *out = w;
+    return LHL_OK;
+}
+
+int lhl_ws_destroy(lhl_ws_t ws)
+{
+    if (!ws) return LHL_ERR_ARG;
+    ws_free(ws);
+    return LHL_OK;
+}
+
+int lhl_ws_get_view(lhl_ws_t ws, lhl_ws_view* v)
+{
+    if (!ws || !v) return LHL_ERR_ARG;
+    v->n = ws->n;
+    v->factors = ws->F;
+    v->Ht = ws->Ht;
+    v->ipiv = ws->ipiv;
+    v->perm = ws->perm;
+    v->iperm = ws->iperm;
+    v->scale = ws->scale;
+    v->iscale = ws->iscale;
+    return LHL_OK;
+}
+
+int lhl_ws_set_barrier_limit_ns(lhl_ws_t ws, uint64_t limit_ns)
+{
+    if (!ws || limit_ns == 0) return LHL_ERR_ARG;
+    ws->limit_ns = limit_ns;
+    return LHL_OK;
+}
+
+int lhl_ws_check(lhl_ws_t ws, void* stream)
+{
+    if (!ws) return LHL_ERR_ARG;
+    cudaStream_t st = (cudaStream_t)stream;
+    cudaError_t e = cudaStreamSynchronize(st);
+    if (e != cudaSuccess) return LHL_ERR_CUDA;
+    int err = 0;
+    e = cudaMemcpy(&err, ws->err, sizeof(int), cudaMemcpyDeviceToHost);
+    if (e != cudaSuccess) return LHL_ERR_CUDA;
+    if (err) cudaMemset(ws->err, 0, sizeof(int));
+    return err ? err : LHL_OK;
+}
+
+int lhl_reduce(lhl_ws_t ws, const double* dJ, int64_t ldj, int balance, void* stream)
+{
+    if (!ws || (!dJ && ws->n > 0)) return LHL_ERR_ARG;
+    const int64_t n = ws->n;
+    if (ldj < n || ldj < 1) return LHL_ERR_DIM;
+    if (n == 0) return LHL_OK;
+    cudaStream_t st = (cudaStream_t)stream;
+    cudaError_t e = cudaMemcpy2DAsync(ws->F, n * sizeof(double), dJ, ldj * sizeof(double), n * sizeof(double), n,
+                                      cudaMemcpyDeviceToDevice, st);
+    if (e == cudaSuccess) e = cudaMemsetAsync(ws->bar, 0, sizeof(unsigned int), st);
+    if (e == cudaSuccess) e = cudaMemsetAsync(ws->err, 0, sizeof(int), st);
+    if (e != cudaSuccess) return LHL_ERR_CUDA;
+    lhl::RedArgs a;
+    memset(&a, 0, sizeof(a));
+    a.n = (int)n;
+    a.nb = 16;
+    a.A = ws->F;
+    a.ipiv = ws->ipiv;
+    a.B0 = ws->B0;
+    a.part = ws->part;
+    a.tab = ws->tab;
+    a.cand_v = ws->cand_v;
+    a.cand_i = ws->cand_i;
+    a.buf2 = ws->buf2;
+    a.tsnap = ws->tsnap;
+    a.scale = ws->scale;
+    a.iscale = ws->iscale;
+    a.bsum = ws->bsum;
+    a.bfac = ws->bfac;
+    a.bflag = ws->bflag;
+    a.bar = ws->bar;
+    a.err = ws->err;
+    a.limit_ns = ws->limit_ns;
+    const int mode = n <= 2 ? 0 : (n < 500 ? 1 : 2);
+    if (!balance) {
+        // scale = iscale = 1
+        e = lhl::launch_fill_ones(ws->scale, ws->iscale, (int)n, st);
+        if (e != cudaSuccess) return LHL_ERR_CUDA;
+    }
+    e = lhl::launch_reduce(a, balance ? 1 : 0, mode, st);
+    if (e != cudaSuccess) return LHL_ERR_CUDA;
+    if (mode == 1) {
+        e = lhl::launch_unblocked_assemble((int)n, ws->F, ws->buf2, ws->ipiv, st);
+        if (e != cudaSuccess) return LHL_ERR_CUDA;
+    }
+    e = lhl::launch_ht_perm((int)n, ws->F, ws->Ht, ws->ipiv, ws->perm, ws->iperm, st);
+    return cuda_status(e);
+}
+
+int lhl_shift_create(int64_t n, int64_t nshifts, lhl_shift_t* out)
+{
+    if (!out) return LHL_ERR_ARG;
+    *out = nullptr;
+    if (n < 0 || n > 16384 || nshifts < 1) return LHL_ERR_DIM;
+    lhl_shift_t s = new (std::nothrow) lhl_shift_s();
+    if (!s) return LHL_ERR_ALLOC;
+    memset(s, 0, sizeof(*s));
+    s->n = n;
+    s->nshifts = nshifts;
+    s->ldg = n + 4;
+    const size_t gsz = (size_t)s->ldg * (size_t)n * (size_t)nshifts;
+    cudaError_t e = dalloc(&s->Gt, gsz);
+    if (e == cudaSuccess) e = dalloc(&s->rdiag, (size_t)n * nshifts);
+    if (e == cudaSuccess) e = dalloc(&s->sigma, nshifts);
+    if (e == cudaSuccess) e = dalloc(&s->tau, nshifts);
+    if (e == cudaSuccess) e = dalloc(&s->swap, (size_t)n * nshifts);
+    if (e == cudaSuccess) e = dalloc(&s->info, nshifts);
+    if (e == cudaSuccess) e = cudaMemset(s->Gt, 0, (gsz ? gsz : 1) * sizeof(double));
+    if (e == cudaSuccess) e = cudaMemset(s->info, 0, nshifts * sizeof(int32_t));
+    if (e == cudaSuccess) e = cudaMemset(s->sigma, 0, nshifts * sizeof(double));
+    if (e == cudaSuccess) e = cudaMemset(s->tau, 0, nshifts * sizeof(double));
+    if (e != cudaSuccess) {
+        lhl_shift_destroy(s);
+        return e == cudaErrorMemoryAllocation ? LHL_ERR_ALLOC : LHL_ERR_CUDA;
+    }
+    *out = s;
+    return LHL_OK;
+}
+
+int lhl_shift_destroy(lhl_shift_t s)
+{
+    if (!s) return LHL_ERR_ARG;
+    void* ptrs[] = {s->Gt, s->rdiag, s->sigma, s->tau, s->swap, s->info};
+    for (void* p : ptrs)
+        if (p) cudaFree(p);
+    delete s;
+    return LHL_OK;
+}
+
+int lhl_shift_get_view(lhl_shift_t s, lhl_shift_view* v)
+{
+    if (!s || !v) return LHL_ERR_ARG;
+    v->n = s->n;
+    v->nshifts = s->nshifts;
+    v->ldg = s->ldg;
+    v->Gt = s->Gt;
+    v->swap = s->swap;
+    v->rdiag = s->rdiag;
+    v->info = s->info;
+    v->sigma = s->sigma;
+    v->tau = s->tau;
+    return LHL_OK;
+}
+
+int lhl_shift_batched(lhl_shift_t sh, lhl_ws_t ws, int64_t s0, int64_t count, const double* dsigma,
+                      const double* dtau, void* stream)
+{
+    if (!sh || !ws) return LHL_ERR_ARG;
+    if (sh->n != ws->n) return LHL_ERR_DIM;
+    if (s0 < 0 || count < 0 || s0 + count > sh->nshifts) return LHL_ERR_DIM;
+    if (count == 0 || ws->n == 0) return LHL_OK;
+    if (!dsigma || !dtau) return LHL_ERR_ARG;
+    cudaStream_t st = (cudaStream_t)stream;
+    cudaError_t e = cudaSuccess;
+    if (dsigma != sh->sigma + s0)
+        e = cudaMemcpyAsync(sh->sigma + s0, dsigma, count * sizeof(double), cudaMemcpyDeviceToDevice, st);
+    if (e == cudaSuccess && dtau != sh->tau + s0)
+        e = cudaMemcpyAsync(sh->tau + s0, dtau, count * sizeof(double), cudaMemcpyDeviceToDevice, st);
+    if (e != cudaSuccess) return LHL_ERR_CUDA;
+    e = lhl::launch_shift_lu((int)ws->n, ws->Ht, (int)ws->n, sh->sigma + s0, sh->tau + s0, (int)s0, (int)count,
+                             sh->Gt, (int)sh->ldg, sh->swap, sh->rdiag, sh->info, st);
+    return cuda_status(e);
+}
+
+int lhl_shift(lhl_shift_t sh, lhl_ws_t ws, int64_t slot, double sigma, double tau, void* stream)
+{
+    if (!sh || !ws) return LHL_ERR_ARG;
+    if (sh->n != ws->n) return LHL_ERR_DIM;
+    if (slot < 0 || slot >= sh->nshifts) return LHL_ERR_DIM;
+    if (ws->n == 0) return LHL_OK;
+    cudaStream_t st = (cudaStream_t)stream;
+    cudaError_t e = lhl::launch_set_pair(sh->sigma + slot, sh->tau + slot, sigma, tau, st);
+    if (e != cudaSuccess) return LHL_ERR_CUDA;
+    e = lhl::launch_shift_lu((int)ws->n, ws->Ht, (int)ws->n, sh->sigma + slot, sh->tau + slot, (int)slot, 1,
+                             sh->Gt, (int)sh->ldg, sh->swap, sh->rdiag, sh->info, st);
+    return cuda_status(e);
+}
+
+static int ldiv_common(lhl_shift_t sh, lhl_ws_t ws, double* dX, int64_t ldx, int64_t nrhs, int64_t rps, int mode,
+                       cudaStream_t st)
+{
+    const int64_t n = ws->n;
+    if (nrhs < 0) return LHL_ERR_DIM;
+    if (nrhs == 0 || n == 0) return LHL_OK;
+    if (!dX) return LHL_ERR_ARG;
+    if (ldx < n) return LHL_ERR_DIM;
+    if (n > 8192) return LHL_ERR_DIM;
+    lhl::LdivArgs a;
+    memset(&a, 0, sizeof(a));
+    a.n = (int)n;
+    a.F = ws->F;
+    a.ldf = (int)n;
+    a.perm = ws->perm;
+    a.iperm = ws->iperm;
+    a.scale = ws->scale;
+    a.iscale = ws->iscale;
+    a.X = dX;
+    a.ldx = (int)ldx;
+    a.mode = mode;
+    a.rhs_per_shift = 1;
+    if (sh) {
+        a.Gt = sh->Gt;
+        a.ldg = (int)sh->ldg;
+        a.swp = sh->swap;
+        a.rdiag = sh->rdiag;
+        a.rhs_per_shift = (int)rps;
+    }
+    return cuda_status(lhl::launch_ldiv(a, (int)nrhs, st));
+}
+
+int lhl_ldiv(lhl_shift_t sh, lhl_ws_t ws, double* dX, int64_t ldx, int64_t nrhs, int64_t rhs_per_shift, void* stream)
+{
+    if (!sh || !ws) return LHL_ERR_ARG;
+    if (sh->n != ws->n) return LHL_ERR_DIM;
+    if (rhs_per_shift < 1) return LHL_ERR_ARG;
+    if (nrhs > 0 && (nrhs + rhs_per_shift - 1) / rhs_per_shift > sh->nshifts) return LHL_ERR_DIM;
+    return ldiv_common(sh, ws, dX, ldx, nrhs, rhs_per_shift, 0, (cudaStream_t)stream);
+}
+
+int lhl_applyZ(lhl_ws_t ws, double* dX, int64_t ldx, int64_t nrhs, void* stream)
+{
+    if (!ws) return LHL_ERR_ARG;
+    return ldiv_common(nullptr, ws, dX, ldx, nrhs, 1, 2, (cudaStream_t)stream);
+}
+
+int lhl_applyZinv(lhl_ws_t ws, double* dX, int64_t ldx, int64_t nrhs, void* stream)
+{
+    if (!ws) return LHL_ERR_ARG;
+    return ldiv_common(nullptr, ws, dX, ldx, nrhs, 1, 1, (cudaStream_t)stream);
+}
+
+int lhl_refine(lhl_shift_t sh, lhl_ws_t ws, const double* dJ, int64_t ldj, const double* dB, int64_t ldb, double* dX,
+               int64_t ldx, double* dR, int64_t nrhs, int64_t rhs_per_shift, int steps, void* stream)
+{
+    if (!sh || !ws) return LHL_ERR_ARG;
+    const int64_t n = ws->n;
+    if (sh->n != n) return LHL_ERR_DIM;
+    if (rhs_per_shift < 1 || steps < 0) return LHL_ERR_ARG;
+    if (nrhs < 0) return LHL_ERR_DIM;
+    if (nrhs == 0 || n == 0 || steps == 0) return LHL_OK;
+    if (!dJ || !dB || !dX || !dR) return LHL_ERR_ARG;
+    if (ldj < n || ldb < n || ldx < n) return LHL_ERR_DIM;
+    if ((nrhs + rhs_per_shift - 1) / rhs_per_shift > sh->nshifts) return LHL_ERR_DIM;
+    cudaStream_t st = (cudaStream_t)stream;
+    for (int s = 0; s < steps; ++s) {
+        cudaError_t e = lhl::launch_residual((int)n, dJ, (int)ldj, dB, (int)ldb, dX, (int)ldx, dR, (int)ldx, (int)nrhs,
+                                             (int)rhs_per_shift, sh->sigma, sh->tau, st);
+        if (e != cudaSuccess) return LHL_ERR_CUDA;
+        int rc = ldiv_common(sh, ws, dR, ldx, nrhs, rhs_per_shift, 0, st);
+        if (rc != LHL_OK) return rc;
+        e = lhl::launch_axpy_cols((int)n, dX, (int)ldx, dR, (int)ldx, (int)nrhs, st);
+        if (e != cudaSuccess) return LHL_ERR_CUDA;
+    }
+    return LHL_OK;
+}
+
+int lhl_residual_norms(lhl_shift_t sh, const double* dJ, int64_t ldj, const double* dB, int64_t ldb,
+                       const double* dX, int64_t ldx, double* dR, double* dres, int64_t nrhs, int64_t rhs_per_shift,
+                       void* stream)
+{
+    if (!sh) return LHL_ERR_ARG;
+    const int64_t n = sh->n;
+    if (rhs_per_shift < 1) return LHL_ERR_ARG;
+    if (nrhs < 0) return LHL_ERR_DIM;
+    if (nrhs == 0 || n == 0) return LHL_OK;
+    if (!dJ || !dB || !dX || !dR || !dres) return LHL_ERR_ARG;
+    if (ldj < n || ldb < n || ldx < n) return LHL_ERR_DIM;
+    if ((nrhs + rhs_per_shift - 1) / rhs_per_shift > sh->nshifts) return LHL_ERR_DIM;
+    cudaStream_t st = (cudaStream_t)stream;
+    cudaError_t e = lhl::launch_residual((int)n, dJ, (int)ldj, dB, (int)ldb, dX, (int)ldx, dR, (int)ldx, (int)nrhs,
+                                         (int)rhs_per_shift, sh->sigma, sh->tau, st);
+    if (e != cudaSuccess) return LHL_ERR_CUDA;
+    return cuda_status(lhl::launch_relres((int)n, dR, (int)ldx, dB, (int)ldb, dres, (int)nrhs, st));
+}
+
+}  // extern "C"

@@ -1,0 +1,110 @@
+// common.cuh -- shared device helpers for the LHL sm_100a kernels.
+//
+// Conventions (mirroring src/LHLFactorization.jl): matrices are column-major FP64,
+// indices in the algorithm text are 1-based, pivot / permutation vectors hold 1-based
+// int64 row indices.  Device code indexes with the 1-based macro M1 below so the
+// kernels read like the reference they restate.
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "../../include/lhl_gpu.h"
+
+#define M1(A, ld, i, j) ((A)[(size_t)((j) - 1) * (size_t)(ld) + (size_t)((i) - 1)])
+
+namespace lhl {
+
+// IEEE operations that the compiler must not fuse: the plain FP64 form reproduces the
+// reference's operation order exactly (fused multiply-adds only where it calls fmuladd).
+__device__ __forceinline__ double dmul(double a, double b) { return __dmul_rn(a, b); }
+__device__ __forceinline__ double dadd(double a, double b) { return __dadd_rn(a, b); }
+__device__ __forceinline__ double dsub(double a, double b) { return __dsub_rn(a, b); }
+__device__ __forceinline__ double dfma(double a, double b, double c) { return __fma_rn(a, b, c); }
+
+__device__ __forceinline__ uint64_t globaltimer_ns()
+{
+    uint64_t t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+
+__device__ __forceinline__ unsigned int ld_acquire_u32(const unsigned int* p)
+{
+    unsigned int v;
+    asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+    return v;
+}
+
+__device__ __forceinline__ int ld_acquire_i32(const int* p)
+{
+    int v;
+    asm volatile("ld.acquire.gpu.global.s32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+    return v;
+}
+
+// Grid-wide barrier for a cooperative (co-resident) grid.  `counter` only grows: the
+// b-th barrier of a launch waits until it reaches b * gridDim.x.  The wait is bounded
+// by `limit_ns` of wall time; on expiry the CTA records LHL_ERR_TIMEOUT in *err and
+// returns false, and every CTA that sees *err set also returns false, so a lost CTA
+// ends the kernel with an error status instead of a hang.
+struct GridBarrier {
+    unsigned int* counter;
+    int* err;
+    unsigned long long limit_ns;
+    unsigned int seq;
+
+    __device__ __forceinline__ bool sync()
+    {
+        __shared__ int s_ok;
+        ++seq;
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            int ok = 1;
+            __threadfence();
+            atomicAdd(counter, 1u);
+            const unsigned int target = seq * gridDim.x;
+            const uint64_t t0 = globaltimer_ns();
+            unsigned int spins = 0;
+            while (ld_acquire_u32(counter) < target) {
+                if (ld_acquire_i32(err) != 0) { ok = 0; break; }
+                if ((++spins & 63u) == 0 && globaltimer_ns() - t0 > limit_ns) {
+                    atomicCAS(err, 0, (int)LHL_ERR_TIMEOUT);
+                    ok = 0;
+                    break;
+                }
+            }
+            if (ok && ld_acquire_i32(err) != 0) ok = 0;
+            __threadfence();
+            s_ok = ok;
+        }
+        __syncthreads();
+        return s_ok != 0;
+    }
+};
+
+__device__ __forceinline__ double warp_sum(double v)
+{
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    return v;
+}
+
+// First-maximum combine: larger |value| wins, ties go to the lower row (the reference's
+// strict `>` scan in increasing row order, F:799-806).  Row 0 means "no candidate".
+__device__ __forceinline__ void argmax_combine(double& a, int& ia, double b, int ib)
+{
+    if (ib == 0) return;
+    if (ia == 0 || b > a || (b == a && ib < ia)) { a = b; ia = ib; }
+}
+
+__device__ __forceinline__ void warp_argmax(double& a, int& ia)
+{
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        double b = __shfl_xor_sync(0xffffffffu, a, o);
+        int ib = __shfl_xor_sync(0xffffffffu, ia, o);
+        argmax_combine(a, ia, b, ib);
+    }
+}
+
+}  // namespace lhl

@@ -1,0 +1,69 @@
+// internal.cuh -- argument blocks and launchers shared by the .cu files of liblhl_gpu.
+#pragma once
+#include "common.cuh"
+
+namespace lhl {
+
+// Device buffers of one reduction (see reduce.cu).
+struct RedArgs {
+    int n;
+    int nb;
+    double* A;        // n x n, ld n (factors in place)
+    int64_t* ipiv;    // n-2
+    double* B0;       // n x (nb+1): pre-panel copies of the panel columns
+    double* part;     // GEMV partials, Pmax x n
+    double* tab;      // per-step table
+    double* cand_v;   // per-CTA pivot candidates
+    int* cand_i;
+    double* buf2;     // unblocked path: second matrix buffer (n x n)
+    double* tsnap;    // blocked path: rows 1..k0 of the panel columns before the top GEMM
+    double* scale;    // balancing D
+    double* iscale;
+    double* bsum;     // balancing: 2n sums
+    double* bfac;     // balancing: per-sweep factors (n)
+    int* bflag;       // balancing: [0] scaled-in-sweep flag
+    unsigned int* bar;
+    int* err;
+    unsigned long long limit_ns;
+};
+
+// One solve launch (see solve.cu).
+struct LdivArgs {
+    int n;
+    const double* F;      // factors, ld ldf
+    int ldf;
+    const int64_t* perm;
+    const int64_t* iperm;
+    const double* scale;
+    const double* iscale;
+    const double* Gt;     // shift batch base
+    int ldg;
+    const uint8_t* swp;
+    const double* rdiag;
+    double* X;
+    int ldx;
+    int rhs_per_shift;
+    int mode;             // 0 ldiv, 1 applyZinv, 2 applyZ
+};
+
+cudaError_t launch_reduce(RedArgs a, int balance, int mode, cudaStream_t st);
+cudaError_t launch_unblocked_assemble(int n, double* A, const double* B2, const int64_t* ipiv, cudaStream_t st);
+cudaError_t launch_ht_perm(int n, const double* A, double* Ht, const int64_t* ipiv, int64_t* perm, int64_t* iperm,
+                           cudaStream_t st);
+cudaError_t launch_fill_ones(double* a, double* b, int n, cudaStream_t st);
+cudaError_t launch_set_pair(double* a, double* b, double va, double vb, cudaStream_t st);
+size_t stepTabBytes();
+int reduce_grid_size();
+
+cudaError_t launch_shift_lu(int n, const double* Ht, int ldh, const double* sig, const double* tau, int s0, int count,
+                            double* Gt, int ldg, uint8_t* swp, double* rd, int32_t* info, cudaStream_t st);
+
+cudaError_t launch_ldiv(const LdivArgs& a, int nrhs, cudaStream_t st);
+cudaError_t launch_residual(int n, const double* J, int ldj, const double* B, int ldb, const double* X, int ldx,
+                            double* R, int ldr, int nrhs, int rhs_per_shift, const double* sig, const double* tau,
+                            cudaStream_t st);
+cudaError_t launch_axpy_cols(int n, double* X, int ldx, const double* R, int ldr, int nrhs, cudaStream_t st);
+cudaError_t launch_relres(int n, const double* R, int ldr, const double* B, int ldb, double* out, int nrhs,
+                          cudaStream_t st);
+
+}  // namespace lhl

@@ -1,0 +1,1011 @@
+// reduce.cu -- lhl_reduce! on sm_100a: balancing (F:299-340), the unblocked ELMHES
+// reduction (n < 500, F:466-678) and the blocked delayed-update reduction (n >= 500,
+// F:765-1006 with its helpers), Ht fill (F:2005-2061) and perm / iperm (F:376-387).
+//
+// Plain FP64 form: every element of H and L is produced by the same sequence of IEEE
+// operations as the reference's Float64 path on x86-64 (fused multiply-add exactly where
+// the reference calls llvm.fmuladd), so pivots, H and L are bit-identical to a faithful
+// CPU restatement.  Summation orders are the reference's own: 64-column GEMV groups with
+// four-column passes, group sums added in order, per-element fma chains in the panel-end
+// products.  Parallelism comes from rows, columns and column groups, never from
+// reassociating a sum.
+//
+// Both reductions are single cooperative launches: one CTA per SM, phases separated by
+// a grid barrier whose wait is bounded (common.cuh).  The matrix stays in HBM/L2,
+// column-major with leading dimension n.
+#include "internal.cuh"
+
+namespace lhl {
+
+constexpr int RT = 256;        // threads per CTA of the reduction kernels
+constexpr int RW = RT / 32;    // warps per CTA
+constexpr int NBMAX = 16;      // panel width nb (F:706)
+constexpr int GEMV_GROUP = 64; // _LHL_GEMV_GROUP (F:1451)
+
+
+// ---------------------------------------------------------------------------------
+// Per-step table written by one warp in phase A and read by every CTA in phase B.
+// ---------------------------------------------------------------------------------
+struct StepTab {
+    int p, pulled, nov, skip;
+    double piv;
+    double R1[NBMAX + 2], RP[NBMAX + 2], PJ[NBMAX + 2], VJ[NBMAX + 2], CX[NBMAX + 2];
+    double OV[2 * NBMAX + 4];
+    int OR[2 * NBMAX + 4];
+};
+
+__device__ __forceinline__ void combine_candidates(const RedArgs& a, int* s_p, double* s_red, int* s_redi)
+{
+    // every CTA reads all CTA candidates and reduces them (first max, F:1038-1051)
+    const int t = threadIdx.x;
+    double v = 0.0;
+    int vi = 0;
+    for (int c = t; c < (int)gridDim.x; c += RT) {
+        const int ci = ((volatile int*)a.cand_i)[c];
+        const double cv = ((volatile double*)a.cand_v)[c];
+        argmax_combine(v, vi, cv, ci);
+    }
+    warp_argmax(v, vi);
+    if ((t & 31) == 0) {
+        s_red[t >> 5] = v;
+        s_redi[t >> 5] = vi;
+    }
+    __syncthreads();
+    if (t == 0) {
+        double bv = 0.0;
+        int bi = 0;
+        for (int w = 0; w < RW; ++w) argmax_combine(bv, bi, s_red[w], s_redi[w]);
+        *s_p = bi;
+    }
+    __syncthreads();
+}
+
+// CTA-local first-max over this thread's candidate, published to cand[blockIdx.x].
+__device__ __forceinline__ void publish_candidate(const RedArgs& a, double v, int vi, double* s_red, int* s_redi)
+{
+    warp_argmax(v, vi);
+    const int t = threadIdx.x;
+    if ((t & 31) == 0) {
+        s_red[t >> 5] = v;
+        s_redi[t >> 5] = vi;
+    }
+    __syncthreads();
+    if (t == 0) {
+        double bv = 0.0;
+        int bi = 0;
+        for (int w = 0; w < RW; ++w) argmax_combine(bv, bi, s_red[w], s_redi[w]);
+        a.cand_v[blockIdx.x] = bv;
+        a.cand_i[blockIdx.x] = bi;
+    }
+    __syncthreads();
+}
+
+// ---------------------------------------------------------------------------------
+// Balancing (F:299-340).  Per sweep: (1) every index's column and row 1-norm (without
+// the diagonal), each one summed sequentially in the reference's order by one thread;
+// (2) one thread walks i = 1..n in order taking the reference's decision; after a
+// scaling it patches the sums of the indices still to come (the only sums it changes);
+// (3) all CTAs apply the sweep's power-of-two factors to A (exact).
+// ---------------------------------------------------------------------------------
+__device__ bool balance_phase(const RedArgs& a, GridBarrier& gb)
+{
+    const int n = a.n;
+    double* A = a.A;
+    const int gt = blockIdx.x * RT + threadIdx.x;
+    const int gsz = gridDim.x * RT;
+    for (int i = gt; i < n; i += gsz) {
+        a.scale[i] = 1.0;
+        a.iscale[i] = 1.0;
+    }
+    for (int sweep = 0; sweep < 20; ++sweep) {
+        // (1) sums
+        for (int i = 1 + gt; i <= n; i += gsz) {
+            double c = 0.0, r = 0.0;
+            for (int j = 1; j <= n; ++j) {
+                if (j == i) continue;
+                c += fabs(M1(A, n, j, i));
+                r += fabs(M1(A, n, i, j));
+            }
+            a.bsum[i - 1] = c;
+            a.bsum[n + i - 1] = r;
+            a.bfac[i - 1] = 1.0;
+        }
+        if (gt == 0) a.bflag[0] = 0;
+        if (!gb.sync()) return false;
+        // (2) the sequential decision walk, CTA 0
+        if (blockIdx.x == 0) {
+            __shared__ double s_f;
+            __shared__ int s_i;
+            int i = 1;
+            while (i <= n) {
+                if (threadIdx.x == 0) {
+                    s_i = 0;
+                    for (; i <= n; ++i) {
+                        double c = a.bsum[i - 1], r = a.bsum[n + i - 1];
+                        if (c == 0.0 || r == 0.0) continue;
+                        double f = 1.0;
+                        const double s = c + r;
+                        int guard = 0;
+                        while (c < r / 2.0 && guard < 4200) { c *= 2.0; r /= 2.0; f *= 2.0; ++guard; }
+                        while (c >= 2.0 * r && guard < 8400) { c /= 2.0; r *= 2.0; f /= 2.0; ++guard; }
+                        if (c + r < 0.95 * s) {
+                            s_i = i;
+                            s_f = f;
+                            a.bflag[0] = 1;
+                            break;
+                        }
+                    }
+                }
+                __syncthreads();
+                const int si = s_i;
+                if (si == 0) break;
+                const double f = s_f;
+                // current A[si, m] = A0[si, m] * fac[m] / fac[si]; patch sums of m > si
+                const double fi = a.bfac[si - 1];
+                for (int m = si + 1 + threadIdx.x; m <= n; m += RT) {
+                    const double fm = a.bfac[m - 1];
+                    const double vr = fabs(M1(A, n, si, m)) * fm / fi;  // row si entry in column m
+                    const double vc = fabs(M1(A, n, m, si)) * fi / fm;  // column si entry in row m
+                    a.bsum[m - 1] = (a.bsum[m - 1] - vr) + vr / f;
+                    a.bsum[n + m - 1] = (a.bsum[n + m - 1] - vc) + vc * f;
+                }
+                __syncthreads();
+                if (threadIdx.x == 0) {
+                    a.bfac[si - 1] = fi * f;
+                    a.scale[si - 1] *= f;
+                    a.iscale[si - 1] /= f;
+                }
+                __syncthreads();
+                i = si + 1;
+            }
+        }
+        if (!gb.sync()) return false;
+        const int scaled = ((volatile int*)a.bflag)[0];
+        if (!scaled) break;
+        // (3) apply: A[i,j] <- A[i,j] / fac[i] * fac[j] (powers of two, exact)
+        for (size_t e = gt; e < (size_t)n * n; e += gsz) {
+            const int i = (int)(e % n), j = (int)(e / n);
+            const double fi = a.bfac[i], fj = a.bfac[j];
+            if (fi != 1.0 || fj != 1.0) A[e] = (A[e] / fi) * fj;
+        }
+        if (!gb.sync()) return false;
+    }
+    return true;
+}
+
+// ---------------------------------------------------------------------------------
+// Unblocked reduction (F:466-501), per-row semantics of the row-block kernel (F:547-678)
+// for n >= 8 and of the paired sweep (F:508-538) below.  Step k reads the matrix of step
+// k-1 (buffer (k-1)&1, rows and columns k+1 <-> p swapped on the fly) and writes buffer
+// k&1, one thread per row, so a step needs one grid barrier (the pivot search).  Column
+// j's final values land in buffer j&1 at step j; later interchanges reach them in the
+// final assembly.
+// ---------------------------------------------------------------------------------
+__device__ bool unblocked_phase(const RedArgs& a, GridBarrier& gb)
+{
+    const int n = a.n;
+    double* buf[2] = {a.A, a.buf2};
+    __shared__ double s_l[512];
+    __shared__ double s_red[RW];
+    __shared__ int s_redi[RW];
+    __shared__ int s_p;
+    const int gt = blockIdx.x * RT + threadIdx.x;
+    const int i = gt + 1;  // this thread's row
+    const bool generic = n < 8;
+
+    // candidates for column 1
+    {
+        double v = 0.0;
+        int vi = 0;
+        if (i >= 2 && i <= n) { v = fabs(M1(a.A, n, i, 1)); vi = i; }
+        publish_candidate(a, v, vi, s_red, s_redi);
+    }
+    if (!gb.sync()) return false;
+    for (int k = 1; k <= n - 2; ++k) {
+        const double* R = buf[(k - 1) & 1];
+        double* W = buf[k & 1];
+        combine_candidates(a, &s_p, s_red, s_redi);
+        const int p = (s_p >= k + 1 && s_p <= n) ? s_p : k + 1;
+        if (gt == 0) a.ipiv[k - 1] = p;
+        auto sw = [&](int r) { return r == k + 1 ? p : (r == p ? k + 1 : r); };
+        const double piv = M1(R, n, p, k);
+        // multipliers l_j = A'[j,k] / piv, j = k+2..n, into shared memory
+        for (int j = k + 2 + threadIdx.x; j <= n; j += RT)
+            s_l[j - 1] = (piv != 0.0) ? M1(R, n, sw(j), k) / piv : M1(R, n, sw(j), k);
+        __syncthreads();
+        double cand = 0.0;
+        int candi = 0;
+        if (i <= n) {
+            const int si = sw(i);
+            // column k
+            double ck = M1(R, n, si, k);
+            if (piv != 0.0 && i >= k + 2) ck = s_l[i - 1];
+            M1(W, n, i, k) = ck;
+            // column k+1 (swapped with p), left update by pk = A'[k+1,k+1]
+            double ck1 = M1(R, n, si, p);
+            if (piv == 0.0) {
+                // step skipped (F:488): rows/columns still carry the interchange
+                for (int j = k + 2; j <= n; ++j) M1(W, n, i, j) = M1(R, n, si, sw(j));
+                M1(W, n, i, k + 1) = ck1;
+            } else {
+                const double pk = M1(R, n, p, p);
+                const double li = (i >= k + 2) ? s_l[i - 1] : 0.0;
+                if (pk != 0.0 && i >= k + 2) ck1 = dsub(ck1, dmul(li, pk));
+                if (!generic) {
+                    double s = 0.0;
+                    for (int j = k + 2; j <= n; ++j) {
+                        const int sj = sw(j);
+                        double v = M1(R, n, si, sj);
+                        if (i >= k + 2) v = dfma(li, -M1(R, n, p, sj), v);
+                        M1(W, n, i, j) = v;
+                        s = dfma(s_l[j - 1], v, s);
+                    }
+                    ck1 = dadd(ck1, s);
+                } else {
+                    int j = k + 2;
+                    while (j + 1 <= n) {
+                        double v0 = M1(R, n, si, sw(j)), v1 = M1(R, n, si, sw(j + 1));
+                        if (i >= k + 2) {
+                            v0 = dsub(v0, dmul(li, M1(R, n, p, sw(j))));
+                            v1 = dsub(v1, dmul(li, M1(R, n, p, sw(j + 1))));
+                        }
+                        M1(W, n, i, j) = v0;
+                        M1(W, n, i, j + 1) = v1;
+                        ck1 = dadd(ck1, dadd(dmul(s_l[j - 1], v0), dmul(s_l[j], v1)));
+                        j += 2;
+                    }
+                    if (j <= n) {
+                        double v0 = M1(R, n, si, sw(j));
+                        if (i >= k + 2) v0 = dsub(v0, dmul(li, M1(R, n, p, sw(j))));
+                        M1(W, n, i, j) = v0;
+                        ck1 = dadd(ck1, dmul(s_l[j - 1], v0));
+                    }
+                }
+                M1(W, n, i, k + 1) = ck1;
+            }
+            if (i >= k + 2) { cand = fabs(ck1); candi = i; }
+        }
+        publish_candidate(a, cand, candi, s_red, s_redi);
+        if (!gb.sync()) return false;
+    }
+    return true;
+}
+
+// Final assembly of the unblocked result into a.A: column j from buffer j&1 (columns
+// n-1, n from the last step's buffer), with the interchanges of steps j+1..n-2 applied
+// (the reference applies them as they happen, F:480-485).  One CTA per column.
+__global__ void __launch_bounds__(RT) unblocked_assemble_kernel(int n, double* A, const double* B2,
+                                                                const int64_t* ipiv)
+{
+    const int j = blockIdx.x + 1;
+    if (j > n) return;
+    const double* src;
+    int from;
+    if (j <= n - 2) {
+        src = (j & 1) ? B2 : A;
+        from = j + 1;
+    } else {
+        const int kl = n - 2;  // last step
+        src = (kl >= 1 && (kl & 1)) ? B2 : A;
+        from = n - 1;
+    }
+    __shared__ double col[512];
+    for (int i = threadIdx.x; i < n; i += RT) col[i] = src[(size_t)(j - 1) * n + i];
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        for (int k = from; k <= n - 2; ++k) {
+            const int p = (int)ipiv[k - 1];
+            if (p > k + 1 && p <= n) {
+                const double t = col[k];
+                col[k] = col[p - 1];
+                col[p - 1] = t;
+            }
+        }
+    }
+    __syncthreads();
+    for (int i = threadIdx.x; i < n; i += RT) A[(size_t)(j - 1) * n + i] = col[i];
+}
+
+// ---------------------------------------------------------------------------------
+// Blocked reduction (the reference's Float64 pointer path), nb = 16.
+// ---------------------------------------------------------------------------------
+struct PanelSh {
+    StepTab tab;
+    double LW[NBMAX + 2], LQ[NBMAX + 2], XS[NBMAX + 2];
+    int LR[NBMAX + 2];
+    int nq;
+    double Pm[NBMAX][NBMAX];
+    int srow[2 * NBMAX + 2];  // rows touched by the panel's interchanges
+    int ssrc[2 * NBMAX + 2];  // source slot of each after all interchanges
+    int nsr;
+    double red[RW];
+    int redi[RW];
+    int p;
+};
+
+// Phase A table (one warp; lane 0 does the sequential parts): F:952-980, F:1088-1132.
+__device__ void build_step_table(const RedArgs& a, StepTab* T, int k0, int kb, int k, int p, double piv)
+{
+    const int n = a.n;
+    const double* A = a.A;
+    const int lane = threadIdx.x & 31;
+    for (int j = k0 + lane; j <= kb + 1; j += 32) {
+        T->R1[j - k0] = M1(A, n, k + 1, j);
+        T->RP[j - k0] = M1(A, n, p, j);
+    }
+    for (int j = k + 2 + lane; j <= kb + 1; j += 32) {
+        const double v = (j == p) ? M1(A, n, k + 1, k) : M1(A, n, j, k);
+        T->VJ[j - k0] = v / piv;
+    }
+    __syncwarp();
+    if (lane == 0) {
+        T->p = p;
+        T->piv = piv;
+        const int pulled = p > kb + 1;
+        T->pulled = pulled;
+        int nov = 0;
+        if (pulled) {
+            for (int kk = k0; kk <= k; ++kk) {
+                T->OV[kk - k0] = M1(A, n, kk + 1, p);
+                T->OR[kk - k0] = kk + 1;
+            }
+            nov = k - k0 + 1;
+            for (int kk = k0; kk <= k; ++kk) {
+                const int q = (kk == k) ? p : (int)a.ipiv[kk - 1];
+                if (q == kk + 1) continue;
+                int s = -1;
+                for (int r = 0; r < nov; ++r)
+                    if (T->OR[r] == q) { s = r; break; }
+                if (s < 0) {
+                    s = nov++;
+                    T->OV[s] = M1(A, n, q, p);
+                    T->OR[s] = q;
+                }
+                const double t = T->OV[kk - k0];
+                T->OV[kk - k0] = T->OV[s];
+                T->OV[s] = t;
+            }
+            for (int kk = k0; kk <= k - 1; ++kk) {
+                const double x = T->OV[kk - k0];
+                T->CX[kk - k0] = x;
+                if (x == 0.0) continue;
+                for (int i = kk + 2; i <= k + 1; ++i) {
+                    const double aik = (i == k + 1) ? T->RP[kk - k0] : M1(A, n, i, kk);
+                    T->OV[i - k0 - 1] = dsub(T->OV[i - k0 - 1], dmul(aik, x));
+                }
+            }
+        }
+        T->nov = nov;
+        for (int j = k + 1; j <= kb + 1; ++j) T->PJ[j - k - 1] = T->RP[j - k0];
+        if (pulled) T->PJ[0] = T->OV[k - k0];
+        else if (p != k + 1) {
+            T->PJ[0] = T->RP[p - k0];
+            T->PJ[p - k - 1] = T->RP[k + 1 - k0];
+        }
+    }
+}
+
+// sum of the GEMV partials of row i in group order (F:1558-1583)
+__device__ __forceinline__ double partial_sum(const RedArgs& a, int P, int i)
+{
+    const double* pp = a.part + (i - 1);
+    double s = pp[0];
+    for (int g = 1; g < P; ++g) s = dadd(s, pp[(size_t)g * a.n]);
+    return s;
+}
+
+// GEMV partials of phase A (F:1496-1553): task = (group g, 32-row tile), lane = row.
+__device__ void gemv_tasks(const RedArgs& a, int k0, int kb, int k, int p, double piv, int skip_warp)
+{
+    const int n = a.n;
+    const double* A = a.A;
+    const int c0 = kb + 2;
+    const int P = (n - c0 + 1 + GEMV_GROUP - 1) / GEMV_GROUP;
+    const int ntiles = (n - k0 + 31) / 32;
+    const int lane = threadIdx.x & 31;
+    const int gw = blockIdx.x * RW + (threadIdx.x >> 5);
+    const int nw = gridDim.x * RW;
+    const bool pulled = p > kb + 1;
+    const double* sub = a.B0 + (size_t)(k - k0) * n;  // pre-panel copy of column k+1
+    const int ntask = P * ntiles;
+    if (gw < skip_warp) return;
+    for (int task = gw - skip_warp; task < ntask; task += nw - skip_warp) {
+        const int g = task / ntiles, tile = task % ntiles;
+        const int ga = c0 + g * GEMV_GROUP;
+        const int gb = min(ga + GEMV_GROUP - 1, n);
+        // multipliers of the group's columns: lane m holds columns ga+m and ga+32+m
+        double l0 = 0.0, l1 = 0.0;
+        {
+            const int j0 = ga + lane, j1 = ga + 32 + lane;
+            if (j0 <= gb) l0 = ((j0 == p) ? M1(A, n, k + 1, k) : M1(A, n, j0, k)) / piv;
+            if (j1 <= gb) l1 = ((j1 == p) ? M1(A, n, k + 1, k) : M1(A, n, j1, k)) / piv;
+        }
+        const int i = k0 + 1 + tile * 32 + lane;
+        const bool act = i <= n;
+        const int ii = act ? i : n;
+        auto L = [&](int j) -> double {
+            const int m = j - ga;
+            const double v0 = __shfl_sync(0xffffffffu, l0, m & 31);
+            const double v1 = __shfl_sync(0xffffffffu, l1, m & 31);
+            return m < 32 ? v0 : v1;
+        };
+        auto COL = [&](int j) -> const double* { return (pulled && j == p) ? sub : A + (size_t)(j - 1) * n; };
+        double acc;
+        int j = ga;
+        if (j + 3 <= gb) {
+            const double q1 = L(j), q2 = L(j + 1), q3 = L(j + 2), q4 = L(j + 3);
+            acc = dadd(dadd(dmul(q1, COL(j)[ii - 1]), dmul(q2, COL(j + 1)[ii - 1])),
+                       dadd(dmul(q3, COL(j + 2)[ii - 1]), dmul(q4, COL(j + 3)[ii - 1])));
+            j += 4;
+        } else {
+            acc = dmul(L(j), COL(j)[ii - 1]);
+            j += 1;
+        }
+        while (j + 3 <= gb) {
+            const double q1 = L(j), q2 = L(j + 1), q3 = L(j + 2), q4 = L(j + 3);
+            acc = dadd(acc, dadd(dadd(dmul(q1, COL(j)[ii - 1]), dmul(q2, COL(j + 1)[ii - 1])),
+                                 dadd(dmul(q3, COL(j + 2)[ii - 1]), dmul(q4, COL(j + 3)[ii - 1]))));
+            j += 4;
+        }
+        while (j <= gb) {
+            const double lj = L(j);
+            if (lj != 0.0) acc = dadd(acc, dmul(lj, COL(j)[ii - 1]));
+            j += 1;
+        }
+        if (act) a.part[(size_t)g * n + (i - 1)] = acc;
+    }
+}
+
+// The correction triangle of phase B, computed redundantly by every CTA's warp 0
+// (F:1232-1269): LW (rows k0+1..k+1), LQ (swap partners beyond k+1), XS (the x's).
+__device__ void correction_triangle(const RedArgs& a, PanelSh& S, int k0, int k, int P)
+{
+    const int n = a.n;
+    const double* A = a.A;
+    const int lane = threadIdx.x & 31;
+    const int m = k - k0 + 1;
+    if (lane < m) S.LW[lane] = partial_sum(a, P, k0 + 1 + lane);
+    __syncwarp();
+    if (lane == 0) {
+        int nq = 0;
+        for (int kk = k0; kk <= k; ++kk) {
+            const int q = (int)a.ipiv[kk - 1];
+            if (q == kk + 1) continue;
+            if (q <= k + 1) {
+                const double t = S.LW[kk - k0];
+                S.LW[kk - k0] = S.LW[q - k0 - 1];
+                S.LW[q - k0 - 1] = t;
+            } else {
+                int s = -1;
+                for (int r = 0; r < nq; ++r)
+                    if (S.LR[r] == q) { s = r; break; }
+                if (s < 0) {
+                    s = nq++;
+                    S.LQ[s] = partial_sum(a, P, q);
+                    S.LR[s] = q;
+                }
+                const double t = S.LW[kk - k0];
+                S.LW[kk - k0] = S.LQ[s];
+                S.LQ[s] = t;
+            }
+        }
+        S.nq = nq;
+    }
+    __syncwarp();
+    // x triangle: lanes hold rows k0+1+lane, sequential over kk
+    double lw = (lane < m) ? S.LW[lane] : 0.0;
+    const int row = k0 + 1 + lane;
+    for (int kk = k0; kk <= k; ++kk) {
+        const double x = __shfl_sync(0xffffffffu, lw, kk - k0);
+        if (lane == 0) S.XS[kk - k0] = x;
+        if (x != 0.0 && lane < m) {
+            if (row >= kk + 2 && row <= k) lw = dsub(lw, dmul(M1(A, n, row, kk), x));
+            else if (row == k + 1 && kk + 2 <= k + 1) lw = dsub(lw, dmul(S.tab.RP[kk - k0], x));
+        }
+    }
+    if (lane < m) S.LW[lane] = lw;
+    __syncwarp();
+}
+
+// Phase B row work for row i in k0+1..n (F:1166-1296); returns |A[i,k+1]| candidate.
+template <int NB>
+__device__ void panel_row(const RedArgs& a, const PanelSh& S, int k0, int kb, int k, int P, int i, double& cand,
+                          int& candi)
+{
+    const int n = a.n;
+    double* A = a.A;
+    const StepTab& T = S.tab;
+    const int p = T.p;
+    const int w = kb + 1 - k0 + 1;  // columns k0..kb+1
+    double v[NB + 2];
+#pragma unroll
+    for (int c = 0; c < NB + 2; ++c) v[c] = (c < w) ? M1(A, n, i, k0 + c) : 0.0;
+    const int ck = k - k0, ck1 = k + 1 - k0;
+    if (T.skip) {
+        if (i >= k + 2) { cand = fabs(v[ck1]); candi = i; }
+        return;
+    }
+    const double piv = T.piv;
+    // (1) interchange: rows k+1 <-> p on the panel columns, then columns k+1 <-> p
+    if (p != k + 1) {
+        if (i == k + 1) {
+#pragma unroll
+            for (int c = 0; c < NB + 2; ++c) if (c < w) v[c] = T.RP[c];
+        } else if (i == p) {
+#pragma unroll
+            for (int c = 0; c < NB + 2; ++c) if (c < w) v[c] = T.R1[c];
+        }
+        if (p <= kb + 1) {
+            const int cp = p - k0;
+#pragma unroll
+            for (int c = 0; c < NB + 2; ++c)
+                if (c == cp) { const double t = v[ck1]; v[ck1] = v[c]; v[c] = t; }
+            double* b1 = a.B0 + (size_t)(k - k0) * n + (i - 1);
+            double* bp = a.B0 + (size_t)(p - k0 - 1) * n + (i - 1);
+            const double t = *b1;
+            *b1 = *bp;
+            *bp = t;
+        } else {
+            double* ap = A + (size_t)(p - 1) * n + (i - 1);
+            double* b1 = a.B0 + (size_t)(k - k0) * n + (i - 1);
+            const double t = *ap;
+            *ap = *b1;
+            *b1 = t;
+            v[ck1] = t;
+        }
+    }
+    // (2) the pulled column's tables and catch-up (F:1193-1205)
+    if (T.pulled) {
+        for (int r = 0; r < T.nov; ++r)
+            if (T.OR[r] == i) v[ck1] = T.OV[r];
+        if (i >= k + 2) {
+#pragma unroll
+            for (int c = 0; c < NB; ++c) {
+                if (c < ck) {
+                    const double x = T.CX[c];
+                    if (x != 0.0) v[ck1] = dsub(v[ck1], dmul(v[c], x));
+                }
+            }
+        }
+    }
+    // scale the multiplier (F:968-970, F:1503-1505)
+    if (i >= k + 2) v[ck] = v[ck] / piv;
+    // (3) left update of the panel columns (F:1206-1213)
+    if (i >= k + 2) {
+#pragma unroll
+        for (int c = 1; c < NB + 2; ++c) {
+            if (c >= ck1 && c < w) {
+                const double pj = T.PJ[c - ck1];
+                if (pj != 0.0) v[c] = dsub(v[c], dmul(v[ck], pj));
+            }
+        }
+    }
+    // (4) right update from the panel columns (F:1214-1221)
+#pragma unroll
+    for (int c = 2; c < NB + 2; ++c) {
+        if (c >= ck1 + 1 && c < w) {
+            const double vj = T.VJ[c];
+            if (vj != 0.0) v[ck1] = dadd(v[ck1], dmul(vj, v[c]));
+        }
+    }
+    // (5) the GEMV part with its correction (F:1222-1293)
+    if (i <= k + 1) {
+        v[ck1] = dadd(v[ck1], S.LW[i - k0 - 1]);
+    } else {
+        double wv;
+        int r = -1;
+        for (int q = 0; q < S.nq; ++q)
+            if (S.LR[q] == i) r = q;
+        wv = (r >= 0) ? S.LQ[r] : partial_sum(a, P, i);
+#pragma unroll
+        for (int c = 0; c < NB; ++c) {
+            if (c <= ck) {
+                const double x = S.XS[c];
+                if (x != 0.0) wv = dsub(wv, dmul(v[c], x));
+            }
+        }
+        v[ck1] = dadd(v[ck1], wv);
+        cand = fabs(v[ck1]);
+        candi = i;
+    }
+#pragma unroll
+    for (int c = 0; c < NB + 2; ++c)
+        if (c < w && c >= ck) M1(A, n, i, k0 + c) = v[c];
+    if (p != k + 1 && (i == k + 1 || i == p)) {
+#pragma unroll
+        for (int c = 0; c < NB + 2; ++c)
+            if (c < w && c < ck) M1(A, n, i, k0 + c) = v[c];
+    }
+}
+
+// Panel-end interchange map: rows touched by steps k0..kb and, for each, the row whose
+// pre-sweep value it receives after the whole sequence (F:1344-1379, F:1395-1415).
+__device__ void build_swap_map(const RedArgs& a, PanelSh& S, int k0, int kb)
+{
+    if (threadIdx.x == 0) {
+        int nsr = 0;
+        int val[2 * NBMAX + 2];
+        auto find = [&](int r) {
+            for (int q = 0; q < nsr; ++q)
+                if (S.srow[q] == r) return q;
+            S.srow[nsr] = r;
+            val[nsr] = r;
+            return nsr++;
+        };
+        for (int k = k0; k <= kb; ++k) {
+            const int p = (int)a.ipiv[k - 1];
+            if (p <= k + 1 || p > a.n) continue;
+            const int s1 = find(k + 1), s2 = find(p);
+            const int t = val[s1];
+            val[s1] = val[s2];
+            val[s2] = t;
+        }
+        for (int q = 0; q < nsr; ++q) S.ssrc[q] = val[q];
+        S.nsr = nsr;
+    }
+    __syncthreads();
+}
+
+// P = M^-1 - I of the panel's multipliers (F:1944-1955), into shared memory.
+__device__ void build_trsm_inverse(const RedArgs& a, PanelSh& S, int k0, int kb)
+{
+    const int n = a.n;
+    const int nbp = kb - k0 + 1;
+    const int q = threadIdx.x + 1;  // column q of P
+    if (threadIdx.x < nbp) {
+        for (int r = 1; r <= nbp; ++r) {
+            if (r <= q) { S.Pm[r - 1][q - 1] = 0.0; continue; }
+            double acc = -M1(a.A, n, k0 + r, k0 + q - 1);
+            for (int s = q + 1; s <= r - 1; ++s) acc = dsub(acc, dmul(M1(a.A, n, k0 + r, k0 + s - 1), S.Pm[s - 1][q - 1]));
+            S.Pm[r - 1][q - 1] = acc;
+        }
+    }
+    __syncthreads();
+}
+
+// Apply the panel's interchanges to column c (rows in the swap map); for a trailing
+// column also the TRSM on rows k0+1..kb+1 (F:1933-2001).
+__device__ void column_end(const RedArgs& a, const PanelSh& S, int k0, int kb, int c, bool trsm)
+{
+    const int n = a.n;
+    double* col = a.A + (size_t)(c - 1) * n;
+    double old[2 * NBMAX + 2];
+    for (int q = 0; q < S.nsr; ++q) old[q] = col[S.ssrc[q] - 1];
+    for (int q = 0; q < S.nsr; ++q) col[S.srow[q] - 1] = old[q];
+    if (!trsm) return;
+    const int nbp = kb - k0 + 1;
+    if (nbp < 2) return;
+    double B[NBMAX];
+    for (int s = 0; s < nbp; ++s) B[s] = col[k0 + s];
+    for (int r = 0; r < nbp; ++r) {
+        double v = B[r];
+        for (int s = 0; s < nbp; ++s) v = dfma(S.Pm[r][s], B[s], v);
+        col[k0 + r] = v;
+    }
+}
+
+template <int NB>
+__device__ bool blocked_phase(const RedArgs& a, GridBarrier& gb, PanelSh& S)
+{
+    const int n = a.n;
+    const int nb = NB;
+    double* A = a.A;
+    const int gt = blockIdx.x * RT + threadIdx.x;
+    const int gsz = gridDim.x * RT;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    StepTab* gtab = (StepTab*)a.tab;
+
+    // setup: candidates of column 1, B0 of the first panel
+    {
+        double v = 0.0;
+        int vi = 0;
+        for (int i = 2 + gt; i <= n; i += gsz) argmax_combine(v, vi, fabs(M1(A, n, i, 1)), i);
+        publish_candidate(a, v, vi, S.red, S.redi);
+        const int kb = min(nb, n - 2);
+        for (size_t e = gt; e < (size_t)n * (kb + 1 - 1); e += gsz) {
+            const int i = (int)(e % n), c = (int)(e / n);
+            a.B0[(size_t)c * n + i] = A[(size_t)(c + 1) * n + i];
+        }
+    }
+    if (!gb.sync()) return false;
+
+    for (int k0 = 1; k0 <= n - 2; k0 += nb) {
+        const int kb = min(k0 + nb - 1, n - 2);
+        const int P = (n - kb - 1 + GEMV_GROUP - 1) / GEMV_GROUP;
+        for (int k = k0; k <= kb; ++k) {
+            // ---- phase A: pivot, table, GEMV partials ----
+            combine_candidates(a, &S.p, S.red, S.redi);
+            const int p = (S.p >= k + 1 && S.p <= n) ? S.p : k + 1;
+            const double piv = (p == k + 1) ? M1(A, n, k + 1, k) : M1(A, n, p, k);
+            if (blockIdx.x == 0 && warp == 0) {
+                if (lane == 0) a.ipiv[k - 1] = p;
+                if (piv != 0.0) build_step_table(a, gtab, k0, kb, k, p, piv);
+                if (lane == 0) {
+                    gtab->skip = (piv == 0.0);
+                    gtab->p = p;
+                    gtab->piv = piv;
+                }
+            }
+            if (piv != 0.0) gemv_tasks(a, k0, kb, k, p, piv, 1);
+            if (!gb.sync()) return false;
+            // ---- phase B: rows ----
+            for (int e = threadIdx.x; e < (int)(sizeof(StepTab) / sizeof(int)); e += RT)
+                ((int*)&S.tab)[e] = ((volatile int*)gtab)[e];
+            __syncthreads();
+            const bool skip = S.tab.skip != 0;
+            if (!skip && warp == 0) correction_triangle(a, S, k0, k, P);
+            __syncthreads();
+            double cand = 0.0;
+            int candi = 0;
+            for (int i = 1 + gt; i <= n; i += gsz) {
+                if (i >= k0 + 1) {
+                    panel_row<NB>(a, S, k0, kb, k, P, i, cand, candi);
+                } else if (!skip && p != k + 1) {
+                    // top rows: the column part of the interchange (F:1135-1161)
+                    if (p <= kb + 1) {
+                        double* x1 = A + (size_t)k * n + (i - 1);
+                        double* xp = A + (size_t)(p - 1) * n + (i - 1);
+                        double t = *x1; *x1 = *xp; *xp = t;
+                        double* b1 = a.B0 + (size_t)(k - k0) * n + (i - 1);
+                        double* bp = a.B0 + (size_t)(p - k0 - 1) * n + (i - 1);
+                        t = *b1; *b1 = *bp; *bp = t;
+                    } else {
+                        double* ap = A + (size_t)(p - 1) * n + (i - 1);
+                        double* b1 = a.B0 + (size_t)(k - k0) * n + (i - 1);
+                        const double t = *ap;
+                        *ap = *b1;
+                        *b1 = t;
+                        A[(size_t)k * n + (i - 1)] = t;
+                    }
+                }
+            }
+            publish_candidate(a, cand, candi, S.red, S.redi);
+            if (!gb.sync()) return false;
+        }
+        // ---- panel end E1: interchange map, TRSM inverse, column sweeps ----
+        build_swap_map(a, S, k0, kb);
+        build_trsm_inverse(a, S, k0, kb);
+        for (int c = 1 + gt; c <= n; c += gsz) {
+            if (c >= kb + 2) column_end(a, S, k0, kb, c, true);
+            else if (c < k0) column_end(a, S, k0, kb, c, false);
+        }
+        {
+            const int nbp = kb - k0 + 1;
+            for (size_t e = gt; e < (size_t)k0 * nbp; e += gsz) {
+                const int i = (int)(e % k0), c = (int)(e / k0);
+                a.tsnap[(size_t)c * n + i] = A[(size_t)(k0 + c) * n + i];
+            }
+        }
+        if (!gb.sync()) return false;
+        // ---- panel end E2: trailing GEMM, top GEMM, next panel's B0 ----
+        {
+            const int nbp = kb - k0 + 1;
+            const int k0n = kb + 1;
+            const int kbn = min(k0n + nb - 1, n - 2);
+            const bool more = k0n <= n - 2;
+            const int m = n - kb - 1;                    // trailing size
+            const int tiles = (m + 31) / 32;
+            const int ntr = tiles * tiles;               // 32x32 trailing tiles
+            const int ntop = ((k0 + 31) / 32) * ((nbp + 3) / 4);
+            const int gw = blockIdx.x * RW + warp, nw = gridDim.x * RW;
+            for (int task = gw; task < ntr + ntop; task += nw) {
+                if (task < ntr) {
+                    const int ti = task % tiles, tj = task / tiles;
+                    const int i = kb + 2 + ti * 32 + lane;
+                    const bool act = i <= n;
+                    double Lr[NBMAX];
+#pragma unroll
+                    for (int s = 0; s < NBMAX; ++s) Lr[s] = (act && s < nbp) ? -M1(A, n, i, k0 + s) : 0.0;
+                    const int cend = min(kb + 2 + tj * 32 + 31, n);
+                    for (int c = kb + 2 + tj * 32; c <= cend; ++c) {
+                        const double* U = A + (size_t)(c - 1) * n + k0;  // rows k0+1..kb+1
+                        double uv = (lane < nbp) ? U[lane] : 0.0;
+                        if (act) {
+                            double v = M1(A, n, i, c);
+#pragma unroll
+                            for (int s = 0; s < NBMAX; ++s)
+                                if (s < nbp) v = dfma(Lr[s], __shfl_sync(0xffffffffu, uv, s), v);
+                                else (void)0;
+                            M1(A, n, i, c) = v;
+                            if (more && c >= k0n + 1 && c <= kbn + 1) a.B0[(size_t)(c - k0n - 1) * n + (i - 1)] = v;
+                        } else {
+#pragma unroll
+                            for (int s = 0; s < NBMAX; ++s) if (s < nbp) (void)__shfl_sync(0xffffffffu, uv, s);
+                        }
+                    }
+                } else {
+                    // top rows 1..k0 of panel columns c0..c0+3 (F:1635-1672)
+                    const int tt = task - ntr;
+                    const int rt = tt / ((nbp + 3) / 4), cg = tt % ((nbp + 3) / 4);
+                    const int i = 1 + rt * 32 + lane;
+                    const bool act = i <= k0;
+                    const int ii = act ? i : 1;
+                    double pre[NBMAX + 1];
+#pragma unroll
+                    for (int c = 0; c < NBMAX + 1; ++c) pre[c] = (c < nbp) ? a.tsnap[(size_t)c * n + (ii - 1)] : 0.0;
+                    double acc[4];
+#pragma unroll
+                    for (int q = 0; q < 4; ++q) {
+                        const int cc = cg * 4 + q;  // column k0+1+cc
+                        double v = (cc < nbp) ? pre[cc] : 0.0;
+#pragma unroll
+                        for (int j = 0; j < NBMAX + 1; ++j) {
+                            if (cc < nbp && j > cc && j < nbp) {
+                                const double vj = M1(A, n, k0 + 1 + j, k0 + cc);
+                                if (vj != 0.0) v = dadd(v, dmul(vj, pre[j]));
+                            }
+                        }
+                        acc[q] = v;
+                    }
+                    for (int j = kb + 2; j <= n; ++j) {
+                        const double aij = M1(A, n, ii, j);
+#pragma unroll
+                        for (int q = 0; q < 4; ++q) {
+                            const int cc = cg * 4 + q;
+                            if (cc < nbp) acc[q] = dfma(aij, M1(A, n, j, k0 + cc), acc[q]);
+                        }
+                    }
+                    if (act) {
+#pragma unroll
+                        for (int q = 0; q < 4; ++q) {
+                            const int cc = cg * 4 + q;
+                            if (cc < nbp) M1(A, n, i, k0 + 1 + cc) = acc[q];
+                        }
+                    }
+                }
+            }
+            // next panel's B0, rows 1..kb+1 (rows below come from the GEMM writers)
+            if (more) {
+                const int wn = kbn + 1 - k0n;  // columns k0n+1..kbn+1
+                for (size_t e = gt; e < (size_t)(kb + 1) * wn; e += gsz) {
+                    const int i = (int)(e % (kb + 1)), c = (int)(e / (kb + 1));
+                    a.B0[(size_t)c * n + i] = A[(size_t)(k0n + c) * n + i];
+                }
+            }
+        }
+        if (!gb.sync()) return false;
+    }
+    return true;
+}
+
+// ---------------------------------------------------------------------------------
+// The reduction kernel: mode 0 = balance only, 1 = unblocked, 2 = blocked.  Balancing,
+// when requested, runs first in the same launch.
+// ---------------------------------------------------------------------------------
+__global__ void __launch_bounds__(RT, 1) reduce_kernel(RedArgs a, int balance, int mode)
+{
+    __shared__ PanelSh S;
+    GridBarrier gb{a.bar, a.err, a.limit_ns, 0};
+    if (balance) {
+        if (!balance_phase(a, gb)) return;
+    }
+    if (mode == 1) {
+        unblocked_phase(a, gb);
+    } else if (mode == 2) {
+        blocked_phase<NBMAX>(a, gb, S);
+    }
+}
+
+// Ht[j,i] = A[i,j] for i <= j+1, zero elsewhere (F:2005-2061); 32x32 tiles.
+__global__ void ht_fill_kernel(int n, const double* __restrict__ A, double* __restrict__ Ht)
+{
+    __shared__ double tile[32][33];
+    const int bi = blockIdx.y * 32, bj = blockIdx.x * 32;  // tile of A rows bi.., cols bj..
+    for (int r = threadIdx.y; r < 32; r += blockDim.y) {
+        const int i = bi + threadIdx.x, j = bj + r;
+        tile[r][threadIdx.x] = (i < n && j < n) ? A[(size_t)j * n + i] : 0.0;
+    }
+    __syncthreads();
+    for (int r = threadIdx.y; r < 32; r += blockDim.y) {
+        const int i = bi + r, j = bj + threadIdx.x;  // Ht[j, i] = A[i, j]
+        if (i < n && j < n) Ht[(size_t)i * n + j] = (i <= j + 1) ? tile[threadIdx.x][r] : 0.0;
+    }
+}
+
+// perm from ipiv (F:376-384) and its inverse (F:385-387): one CTA, shared memory.
+__global__ void perm_kernel(int n, const int64_t* __restrict__ ipiv, int64_t* __restrict__ perm,
+                            int64_t* __restrict__ iperm)
+{
+    extern __shared__ int sp[];
+    for (int i = threadIdx.x; i < n; i += blockDim.x) sp[i] = i + 1;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        for (int k = 1; k <= n - 2; ++k) {
+            const int p = (int)ipiv[k - 1];
+            if (p < k + 1 || p > n) continue;  // never produced by a completed reduction
+            const int t = sp[k];
+            sp[k] = sp[p - 1];
+            sp[p - 1] = t;
+        }
+    }
+    __syncthreads();
+    for (int i = threadIdx.x; i < n; i += blockDim.x) {
+        perm[i] = sp[i];
+        iperm[sp[i] - 1] = i + 1;
+    }
+}
+
+// Reset of the per-reduction state: ipiv[k] = k+1 (no interchange) and empty candidates,
+// so that a reduction that ends early on a barrier timeout leaves only valid indices.
+__global__ void reduce_init_kernel(int n, int64_t* ipiv, double* cand_v, int* cand_i, int ncand)
+{
+    for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < n - 2; k += gridDim.x * blockDim.x) ipiv[k] = k + 2;
+    for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < ncand; c += gridDim.x * blockDim.x) {
+        cand_v[c] = 0.0;
+        cand_i[c] = 0;
+    }
+}
+
+int reduce_grid_size()
+{
+    static int g = 0;
+    if (g == 0) {
+        int dev = 0, sms = 0, per = 0;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, reduce_kernel, RT, 0);
+        g = sms * (per > 0 ? 1 : 0);
+    }
+    return g;
+}
+
+cudaError_t launch_reduce(RedArgs a, int balance, int mode, cudaStream_t st)
+{
+    const int grid = reduce_grid_size();
+    if (grid <= 0) return cudaErrorCooperativeLaunchTooLarge;
+    reduce_init_kernel<<<64, 256, 0, st>>>(a.n, a.ipiv, a.cand_v, a.cand_i, grid);
+    cudaError_t e0 = cudaGetLastError();
+    if (e0 != cudaSuccess) return e0;
+    int bal = balance;
+    void* args[] = {&a, &bal, &mode};
+    return cudaLaunchCooperativeKernel((void*)reduce_kernel, dim3(grid), dim3(RT), args, 0, st);
+}
+
+cudaError_t launch_unblocked_assemble(int n, double* A, const double* B2, const int64_t* ipiv, cudaStream_t st)
+{
+    if (n <= 0 || n > 512) return cudaErrorInvalidValue;
+    unblocked_assemble_kernel<<<n, RT, 0, st>>>(n, A, B2, ipiv);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_ht_perm(int n, const double* A, double* Ht, const int64_t* ipiv, int64_t* perm, int64_t* iperm,
+                           cudaStream_t st)
+{
+    dim3 grid((n + 31) / 32, (n + 31) / 32);
+    ht_fill_kernel<<<grid, dim3(32, 8), 0, st>>>(n, A, Ht);
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+    perm_kernel<<<1, 256, sizeof(int) * (size_t)n, st>>>(n, ipiv, perm, iperm);
+    return cudaGetLastError();
+}
+
+size_t stepTabBytes() { return sizeof(StepTab); }
+
+__global__ void fill_ones_kernel(double* a, double* b, int n)
+{
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        a[i] = 1.0;
+        b[i] = 1.0;
+    }
+}
+
+cudaError_t launch_fill_ones(double* a, double* b, int n, cudaStream_t st)
+{
+    if (n <= 0) return cudaSuccess;
+    fill_ones_kernel<<<(n + 255) / 256, 256, 0, st>>>(a, b, n);
+    return cudaGetLastError();
+}
+
+__global__ void set_pair_kernel(double* a, double* b, double va, double vb)
+{
+    *a = va;
+    *b = vb;
+}
+
+cudaError_t launch_set_pair(double* a, double* b, double va, double vb, cudaStream_t st)
+{
+    set_pair_kernel<<<1, 1, 0, st>>>(a, b, va, vb);
+    return cudaGetLastError();
+}
+
+}  // namespace lhl

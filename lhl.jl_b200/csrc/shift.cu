@@ -1,0 +1,138 @@
+// shift.cu -- lhl_shift!: LU with partial pivoting of G = sigma I + tau H, H upper
+// Hessenberg, stored transposed (Gt[j,k] = U[k,j]) -- src/LHLFactorization.jl F:2529-2594,
+// identical to the bit-exact reference of test/core_tests.jl:119-171.
+//
+// One CTA per shift.  Element j of the pending row r (the not-yet-chosen candidate row,
+// F:2522-2527) lives in a register of thread (j-1) mod T for the whole elimination, so a
+// step costs one CTA barrier: the owner of element k+1 publishes it, every thread takes
+// the pivot decision of the next step from it.  Ht[j, k+1] (row k+1 of H) is prefetched
+// one step ahead.  Every operation is the reference's, in its order, with no fused
+// multiply-add, so Gt, swap, rdiag and info are bit-identical to the reference.
+#include "common.cuh"
+
+namespace lhl {
+
+template <int T, int E>
+__global__ void __launch_bounds__(T) shift_lu_kernel(int n, const double* __restrict__ Ht, int ldh,
+                                                     const double* __restrict__ sig, const double* __restrict__ tau_,
+                                                     int s0, double* __restrict__ Gt_all, int ldg,
+                                                     uint8_t* __restrict__ swap_all, double* __restrict__ rdiag_all,
+                                                     int32_t* __restrict__ info_all)
+{
+    const int s = s0 + blockIdx.x;
+    const double sigma = sig[blockIdx.x];
+    const double tau = tau_[blockIdx.x];
+    double* Gt = Gt_all + (size_t)s * ldg * n;
+    uint8_t* swp = swap_all + (size_t)s * n;
+    double* rdiag = rdiag_all + (size_t)s * n;
+    const int t = threadIdx.x;
+
+    __shared__ double s_next[2];  // r[k+1] after step k, double-buffered by step parity
+    __shared__ int s_info;
+
+    double r[E];
+    double h[E];
+    // row 1 of G: r[j] = tau * Ht[j, 1], r[1] += sigma (F:2536-2539)
+#pragma unroll
+    for (int e = 0; e < E; ++e) {
+        const int j = 1 + t + e * T;
+        r[e] = (j <= n) ? dmul(tau, M1(Ht, ldh, j, 1)) : 0.0;
+        if (j == 1) r[e] = dadd(r[e], sigma);
+        h[e] = (j <= n && n >= 2) ? M1(Ht, ldh, j, 2) : 0.0;
+    }
+    double hb = (n >= 2) ? M1(Ht, ldh, 1, 2) : 0.0;  // Ht[k, k+1] of the coming step
+    if (t == 0) {
+        s_next[1] = r[0];
+        s_info = 0;
+    }
+    __syncthreads();
+
+    for (int k = 1; k <= n - 1; ++k) {
+        const double a = s_next[k & 1];
+        const double b = dmul(tau, hb);
+        hb = (k + 2 <= n) ? M1(Ht, ldh, k + 1, k + 2) : 0.0;
+        const bool sw = fabs(b) > fabs(a);
+        double l;
+        if (sw) {
+            l = a / b;
+        } else if (a == 0.0) {
+            l = 0.0;
+        } else {
+            l = b / a;
+        }
+        if (t == 0) {
+            swp[k - 1] = sw ? 1 : 0;
+            M1(Gt, ldg, k, k) = sw ? b : a;
+            M1(Gt, ldg, k, k + 1) = l;
+            if (!sw && a == 0.0 && s_info == 0) s_info = k;
+        }
+        // prefetch Ht[j, k+2] for the next step
+        double hn[E];
+#pragma unroll
+        for (int e = 0; e < E; ++e) {
+            const int j = 1 + t + e * T;
+            hn[e] = (j >= k + 1 && j <= n && k + 2 <= n) ? M1(Ht, ldh, j, k + 2) : 0.0;
+        }
+#pragma unroll
+        for (int e = 0; e < E; ++e) {
+            const int j = 1 + t + e * T;
+            if (j >= k + 1 && j <= n) {
+                if (sw) {
+                    const double g = dmul(tau, h[e]);
+                    double gk = g;
+                    double rj = dsub(r[e], dmul(l, g));
+                    if (j == k + 1) {
+                        gk = dadd(g, sigma);              // Gt[k+1,k] += sigma
+                        rj = dsub(rj, dmul(l, sigma));    // r[k+1] -= l*sigma
+                    }
+                    M1(Gt, ldg, j, k) = gk;
+                    r[e] = rj;
+                } else {
+                    const double rj = r[e];
+                    M1(Gt, ldg, j, k) = rj;
+                    double rn = dsub(dmul(tau, h[e]), dmul(l, rj));
+                    if (j == k + 1) rn = dadd(rn, sigma); // r[k+1] += sigma
+                    r[e] = rn;
+                }
+                if (j == k + 1) s_next[(k + 1) & 1] = r[e];  // owner of element k+1
+            }
+            h[e] = hn[e];
+        }
+        __syncthreads();
+    }
+    // finish (F:2579-2594)
+    if (t == 0) {
+        const double rn = s_next[n & 1];
+        M1(Gt, ldg, n, n) = rn;
+        swp[n - 1] = 0;
+        int info = s_info;
+        if (rn == 0.0 && info == 0) info = n;
+        info_all[s] = info;
+    }
+    __syncthreads();
+    for (int j = 1 + t; j <= n; j += T) rdiag[j - 1] = 1.0 / M1(Gt, ldg, j, j);
+}
+
+template <int T, int E>
+static cudaError_t launch_shift_T(int n, const double* Ht, int ldh, const double* sig, const double* tau, int s0,
+                                  int count, double* Gt, int ldg, uint8_t* swp, double* rd, int32_t* info,
+                                  cudaStream_t st)
+{
+    shift_lu_kernel<T, E><<<count, T, 0, st>>>(n, Ht, ldh, sig, tau, s0, Gt, ldg, swp, rd, info);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_shift_lu(int n, const double* Ht, int ldh, const double* sig, const double* tau, int s0, int count,
+                            double* Gt, int ldg, uint8_t* swp, double* rd, int32_t* info, cudaStream_t st)
+{
+    if (count <= 0 || n <= 0) return cudaSuccess;
+    if (n <= 256) return launch_shift_T<256, 1>(n, Ht, ldh, sig, tau, s0, count, Gt, ldg, swp, rd, info, st);
+    if (n <= 1024) return launch_shift_T<512, 2>(n, Ht, ldh, sig, tau, s0, count, Gt, ldg, swp, rd, info, st);
+    if (n <= 2048) return launch_shift_T<512, 4>(n, Ht, ldh, sig, tau, s0, count, Gt, ldg, swp, rd, info, st);
+    if (n <= 4096) return launch_shift_T<512, 8>(n, Ht, ldh, sig, tau, s0, count, Gt, ldg, swp, rd, info, st);
+    if (n <= 8192) return launch_shift_T<1024, 8>(n, Ht, ldh, sig, tau, s0, count, Gt, ldg, swp, rd, info, st);
+    if (n <= 16384) return launch_shift_T<1024, 16>(n, Ht, ldh, sig, tau, s0, count, Gt, ldg, swp, rd, info, st);
+    return cudaErrorInvalidValue;
+}
+
+}  // namespace lhl

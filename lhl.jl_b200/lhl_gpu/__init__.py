@@ -1,0 +1,463 @@
+"""Python host mirror of LHLFactorization.jl's API over liblhl_gpu.so (sm_100a).
+
+The Julia names map one to one (a trailing underscore marks the mutating `!` forms):
+
+    lhl(J; balance)                 -> lhl(J, balance=True)            (src/LHLFactorization.jl:3179)
+    lhl!(ws, J; balance)            -> lhl_(ws, J, balance=True)       (:3192)
+    lhl_reduce!(ws, J, balance)     -> lhl_reduce_(ws, J, balance)     (:355)
+    lhl_shift!(ws, sigma, tau)      -> lhl_shift_(ws, sigma, tau)      (:2456)
+    lhl_shift!(sh, ws, sigma, tau)  -> lhl_shift_(sh, ws, sigma, tau)  (:2461)
+    lhl_ldiv!(x, ws) / (x, sh, ws)  -> lhl_ldiv_(x, ws) / (x, sh, ws)  (:3052-3054)
+    lhl_refine!(x, A, b, ws, steps) -> lhl_refine_(x, J, b, ws, steps) (:3144; A = sigma I + tau J)
+    applyZ!(x, ws) / applyZinv!     -> applyZ_(x, ws) / applyZinv_      (:2069, :2104)
+
+Arrays are torch CUDA float64 tensors.  Matrices may have any strides; vectors and the
+columns of an (n, k) right-hand-side block are solved in place.  Mutating calls return
+their first mutated argument, as in the reference.  Errors mirror the reference:
+ArgumentError and DimensionMismatch (both ValueError subclasses).
+
+There is no CPU fallback: importing this module without liblhl_gpu.so, or calling it
+without a CUDA device, raises.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+import torch
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+_LIB_PATH = os.path.join(os.path.dirname(_HERE), "liblhl_gpu.so")
+
+LHL_OK, LHL_ERR_ARG, LHL_ERR_DIM, LHL_ERR_CUDA, LHL_ERR_TIMEOUT, LHL_ERR_ALLOC = range(6)
+LHL_PREC_FP64, LHL_PREC_MIXED = 0, 1
+
+
+class ArgumentError(ValueError):
+    pass
+
+
+class DimensionMismatch(ValueError):
+    pass
+
+
+class LHLDeviceError(RuntimeError):
+    pass
+
+
+class _WsView(C.Structure):
+    _fields_ = [("n", C.c_int64), ("factors", C.c_void_p), ("Ht", C.c_void_p), ("ipiv", C.c_void_p),
+                ("perm", C.c_void_p), ("iperm", C.c_void_p), ("scale", C.c_void_p), ("iscale", C.c_void_p)]
+
+
+class _ShView(C.Structure):
+    _fields_ = [("n", C.c_int64), ("nshifts", C.c_int64), ("ldg", C.c_int64), ("Gt", C.c_void_p),
+                ("swap", C.c_void_p), ("rdiag", C.c_void_p), ("info", C.c_void_p), ("sigma", C.c_void_p),
+                ("tau", C.c_void_p)]
+
+
+def _load():
+    if not os.path.exists(_LIB_PATH):
+        raise ImportError(f"liblhl_gpu.so not built ({_LIB_PATH}); run lhl.jl_b200/build.py")
+    L = C.CDLL(_LIB_PATH)
+    vp, i64, i32, d = C.c_void_p, C.c_int64, C.c_int, C.c_double
+    sig = {
+        "lhl_ws_create": [i64, i32, C.POINTER(vp)],
+        "lhl_ws_destroy": [vp],
+        "lhl_ws_get_view": [vp, C.POINTER(_WsView)],
+        "lhl_ws_check": [vp, vp],
+        "lhl_ws_set_barrier_limit_ns": [vp, C.c_uint64],
+        "lhl_reduce": [vp, vp, i64, i32, vp],
+        "lhl_shift_create": [i64, i64, C.POINTER(vp)],
+        "lhl_shift_destroy": [vp],
+        "lhl_shift_get_view": [vp, C.POINTER(_ShView)],
+        "lhl_shift_batched": [vp, vp, i64, i64, vp, vp, vp],
+        "lhl_shift": [vp, vp, i64, d, d, vp],
+        "lhl_ldiv": [vp, vp, vp, i64, i64, i64, vp],
+        "lhl_refine": [vp, vp, vp, i64, vp, i64, vp, i64, vp, i64, i64, i32, vp],
+        "lhl_residual_norms": [vp, vp, i64, vp, i64, vp, i64, vp, vp, i64, i64, vp],
+        "lhl_applyZ": [vp, vp, i64, i64, vp],
+        "lhl_applyZinv": [vp, vp, i64, i64, vp],
+    }
+    for name, args in sig.items():
+        f = getattr(L, name)
+        f.argtypes = args
+        f.restype = C.c_int
+    L.lhl_version.restype = C.c_char_p
+    return L
+
+
+_lib = _load()
+
+
+def lib():
+    return _lib
+
+
+def _check(rc, what=""):
+    if rc == LHL_OK:
+        return
+    if rc == LHL_ERR_ARG:
+        raise ArgumentError(what)
+    if rc == LHL_ERR_DIM:
+        raise DimensionMismatch(what)
+    if rc == LHL_ERR_TIMEOUT:
+        raise LHLDeviceError(f"{what}: a bounded grid-barrier wait expired")
+    if rc == LHL_ERR_ALLOC:
+        raise MemoryError(what)
+    raise LHLDeviceError(f"{what}: CUDA error (status {rc})")
+
+
+def _stream(stream=None):
+    s = stream if stream is not None else torch.cuda.current_stream()
+    return C.c_void_p(s.cuda_stream)
+
+
+class _DevArray:
+    """A zero-copy torch view of device memory owned by the library."""
+
+    def __init__(self, ptr, shape, dtype, strides=None):
+        self.__cuda_array_interface__ = {
+            "shape": tuple(shape), "typestr": dtype, "data": (int(ptr or 0), False), "version": 3,
+            "strides": strides,
+        }
+
+
+def _view(ptr, shape, typestr="<f8", strides=None):
+    if any(s == 0 for s in shape):
+        return torch.empty(shape, dtype={"<f8": torch.float64, "<i8": torch.int64, "|u1": torch.uint8,
+                                         "<i4": torch.int32}[typestr], device="cuda")
+    return torch.as_tensor(_DevArray(ptr, shape, typestr, strides), device="cuda")
+
+
+def _colmajor(M: torch.Tensor) -> torch.Tensor:
+    """A tensor whose memory is M in column-major order with leading dimension rows."""
+    if M.dim() != 2:
+        raise DimensionMismatch("matrix expected")
+    if M.stride(0) == 1 and M.stride(1) >= max(M.shape[0], 1):
+        return M
+    return M.t().contiguous().t()
+
+
+def _require_cuda_f64(x: torch.Tensor, name: str):
+    if not isinstance(x, torch.Tensor) or not x.is_cuda:
+        raise ArgumentError(f"{name} must be a CUDA tensor")
+    if x.dtype != torch.float64:
+        raise ArgumentError(f"{name} must be float64 (complex shifts need an LHLShift built for them)")
+
+
+class LHLShift:
+    """``LHLShift{Float64}(n)``: a batch of ``nshifts`` shift slots (src/LHLFactorization.jl:84-116)."""
+
+    def __init__(self, n, nshifts: int = 1):
+        if isinstance(n, LHLWorkspace):
+            n = n.n
+        self._h = C.c_void_p()
+        _check(_lib.lhl_shift_create(int(n), int(nshifts), C.byref(self._h)), "LHLShift")
+        self.n = int(n)
+        self.nshifts = int(nshifts)
+        v = _ShView()
+        _check(_lib.lhl_shift_get_view(self._h, C.byref(v)))
+        self._v = v
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        if h is not None and h.value:
+            _lib.lhl_shift_destroy(h)
+            self._h = None
+
+    @property
+    def ldg(self):
+        return int(self._v.ldg)
+
+    def Gt(self, slot: int = 0) -> torch.Tensor:
+        n, ldg = self.n, self.ldg
+        base = self._v.Gt + 8 * slot * ldg * n
+        return _view(base, (ldg, n), strides=(8, 8 * ldg))
+
+    def swap(self, slot: int = 0) -> torch.Tensor:
+        return _view(self._v.swap + slot * self.n, (self.n,), "|u1")
+
+    def rdiag(self, slot: int = 0) -> torch.Tensor:
+        return _view(self._v.rdiag + 8 * slot * self.n, (self.n,))
+
+    @property
+    def info_all(self) -> torch.Tensor:
+        return _view(self._v.info, (self.nshifts,), "<i4")
+
+    @property
+    def sigma_all(self) -> torch.Tensor:
+        return _view(self._v.sigma, (self.nshifts,))
+
+    @property
+    def tau_all(self) -> torch.Tensor:
+        return _view(self._v.tau, (self.nshifts,))
+
+    @property
+    def info(self) -> int:
+        torch.cuda.current_stream().synchronize()
+        return int(self.info_all[0].item())
+
+    @property
+    def σ(self):
+        return float(self.sigma_all[0].item())
+
+    @property
+    def τ(self):
+        return float(self.tau_all[0].item())
+
+
+class LHLWorkspace:
+    """``LHLWorkspace{Float64}(n)`` on the device (src/LHLFactorization.jl:144-178).
+
+    Holds the reduction and, in ``.shift``, one shift slot (the reference's ``ws.shift``);
+    the shift fields are forwarded as in the reference (F:182-191)."""
+
+    _SHIFT_FIELDS = ("Gt", "rdiag", "swap", "info", "σ", "τ")
+
+    def __init__(self, n: int, precision: int = LHL_PREC_FP64):
+        self._h = C.c_void_p()
+        _check(_lib.lhl_ws_create(int(n), int(precision), C.byref(self._h)), "LHLWorkspace")
+        self.n = int(n)
+        self.precision = precision
+        v = _WsView()
+        _check(_lib.lhl_ws_get_view(self._h, C.byref(v)))
+        self._v = v
+        self.shift = LHLShift(self.n, 1)
+        self.reduced = False
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        if h is not None and h.value:
+            _lib.lhl_ws_destroy(h)
+            self._h = None
+
+    def __getattr__(self, name):
+        if name in LHLWorkspace._SHIFT_FIELDS:
+            sh = self.__dict__["shift"]
+            a = getattr(sh, name)
+            return a() if callable(a) else a
+        raise AttributeError(name)
+
+    # device views (column-major n x n tensors are returned as (n, n) with strides (1, n))
+    @property
+    def factors(self) -> torch.Tensor:
+        n = self.n
+        return _view(self._v.factors, (n, n), strides=(8, 8 * n))
+
+    @property
+    def Ht(self) -> torch.Tensor:
+        n = self.n
+        return _view(self._v.Ht, (n, n), strides=(8, 8 * n))
+
+    @property
+    def ipiv(self) -> torch.Tensor:
+        return _view(self._v.ipiv, (max(self.n - 2, 0),), "<i8")
+
+    @property
+    def perm(self) -> torch.Tensor:
+        return _view(self._v.perm, (self.n,), "<i8")
+
+    @property
+    def iperm(self) -> torch.Tensor:
+        return _view(self._v.iperm, (self.n,), "<i8")
+
+    @property
+    def scale(self) -> torch.Tensor:
+        return _view(self._v.scale, (self.n,))
+
+    @property
+    def iscale(self) -> torch.Tensor:
+        return _view(self._v.iscale, (self.n,))
+
+    def check(self, stream=None):
+        """Wait for the stream and raise a device-side error recorded by the last reduction."""
+        _check(_lib.lhl_ws_check(self._h, _stream(stream)), "lhl_reduce")
+
+    def set_barrier_limit_ns(self, ns: int):
+        _check(_lib.lhl_ws_set_barrier_limit_ns(self._h, int(ns)))
+
+
+# ---------------------------------------------------------------------------------------
+def lhl_reduce_(ws: LHLWorkspace, J: torch.Tensor, balance: bool, thread=True, stream=None) -> LHLWorkspace:
+    """``lhl_reduce!(ws, J, balance)`` (F:355).  J is not modified.  The workspace must have
+    been built for J's order (the device workspace does not resize in place)."""
+    _require_cuda_f64(J, "J")
+    if J.dim() != 2 or J.shape[0] != J.shape[1]:
+        raise DimensionMismatch(f"matrix is not square: dimensions are {tuple(J.shape)}")
+    if J.shape[0] != ws.n:
+        raise DimensionMismatch(f"J is {J.shape[0]}x{J.shape[0]}, the workspace is {ws.n}x{ws.n}")
+    Jc = _colmajor(J)
+    ld = max(Jc.stride(1), 1)
+    _check(_lib.lhl_reduce(ws._h, C.c_void_p(Jc.data_ptr()), ld, int(bool(balance)), _stream(stream)), "lhl_reduce")
+    ws.reduced = True
+    ws._J_keepalive = Jc
+    return ws
+
+
+def lhl(J: torch.Tensor, balance: bool = True, thread=True, precision: int = LHL_PREC_FP64,
+        stream=None) -> LHLWorkspace:
+    """``lhl(J; balance=true)`` (F:3179): allocate a workspace and reduce J into it."""
+    _require_cuda_f64(J, "J")
+    if J.dim() != 2 or J.shape[0] != J.shape[1]:
+        raise DimensionMismatch(f"matrix is not square: dimensions are {tuple(J.shape)}")
+    ws = LHLWorkspace(J.shape[0], precision)
+    return lhl_reduce_(ws, J, balance, thread, stream)
+
+
+def lhl_(ws: LHLWorkspace, J: torch.Tensor, balance: bool = True, thread=True, stream=None) -> LHLWorkspace:
+    """``lhl!(ws, J; balance)`` (F:3192).  A workspace of another order is rebuilt in place."""
+    if J.shape[0] != ws.n:
+        new = LHLWorkspace(J.shape[0], ws.precision)
+        ws.__dict__.update({k: v for k, v in new.__dict__.items()})
+        new._h = None
+    return lhl_reduce_(ws, J, balance, thread, stream)
+
+
+def _shift_args(a):
+    if len(a) == 3:
+        ws, sigma, tau = a
+        return ws.shift, ws, sigma, tau, ws
+    if len(a) == 4:
+        sh, ws, sigma, tau = a
+        return sh, ws, sigma, tau, sh
+    raise TypeError("lhl_shift_(ws, sigma, tau) or lhl_shift_(sh, ws, sigma, tau)")
+
+
+def lhl_shift_(*args, slot: int = 0, stream=None):
+    """``lhl_shift!(ws, sigma, tau)`` / ``lhl_shift!(sh, ws, sigma, tau)`` (F:2456-2489)."""
+    sh, ws, sigma, tau, ret = _shift_args(args)
+    for v in (sigma, tau):
+        if isinstance(v, complex) and v.imag != 0:
+            raise ArgumentError(f"complex shift ({sigma}, {tau}) on a real LHLShift")
+    sigma = float(sigma.real if isinstance(sigma, complex) else sigma)
+    tau = float(tau.real if isinstance(tau, complex) else tau)
+    if sh.n != ws.n:
+        raise DimensionMismatch(f"the LHLShift is {sh.n}x{sh.n}, the workspace {ws.n}x{ws.n}")
+    _check(_lib.lhl_shift(sh._h, ws._h, int(slot), sigma, tau, _stream(stream)), "lhl_shift")
+    return ret
+
+
+def lhl_shift_batched_(sh: LHLShift, ws: LHLWorkspace, sigmas: torch.Tensor, taus: torch.Tensor, s0: int = 0,
+                       stream=None) -> LHLShift:
+    """Load len(sigmas) shifts into slots s0.. of ``sh`` in one launch (device arrays)."""
+    _require_cuda_f64(sigmas, "sigmas")
+    _require_cuda_f64(taus, "taus")
+    sigmas = sigmas.contiguous()
+    taus = taus.contiguous()
+    if sigmas.numel() != taus.numel():
+        raise DimensionMismatch("sigmas and taus differ in length")
+    _check(_lib.lhl_shift_batched(sh._h, ws._h, int(s0), sigmas.numel(), C.c_void_p(sigmas.data_ptr()),
+                                  C.c_void_p(taus.data_ptr()), _stream(stream)), "lhl_shift_batched")
+    return sh
+
+
+def _as_cols(x: torch.Tensor, n: int):
+    if x.dim() == 1:
+        if x.shape[0] != n:
+            raise DimensionMismatch(f"x has length {x.shape[0]}, the workspace is {n}x{n}")
+        if x.stride(0) != 1:
+            raise ArgumentError("x must be contiguous")
+        return x, 1, n
+    if x.dim() == 2:
+        if x.shape[0] != n:
+            raise DimensionMismatch(f"x has {x.shape[0]} rows, the workspace is {n}x{n}")
+        if x.stride(0) != 1 and x.shape[1] > 1:
+            raise ArgumentError("x must be column-major (stride (1, ld))")
+        return x, x.shape[1], max(x.stride(1), n) if x.shape[1] > 1 else n
+    raise DimensionMismatch("x must be a vector or an (n, k) block")
+
+
+def lhl_ldiv_(x: torch.Tensor, *args, rhs_per_shift: int = 1, stream=None) -> torch.Tensor:
+    """``lhl_ldiv!(x, ws)`` / ``lhl_ldiv!(x, sh, ws)`` (F:3052-3068).  Column j of an (n, k)
+    block uses shift slot j // rhs_per_shift."""
+    if len(args) == 1:
+        ws = args[0]
+        sh = ws.shift
+    else:
+        sh, ws = args
+    if x.is_complex():
+        raise ArgumentError("a complex right-hand side needs an LHLShift built for complex shifts")
+    _require_cuda_f64(x, "x")
+    if sh.n != ws.n:
+        raise DimensionMismatch(f"the LHLShift is {sh.n}x{sh.n}, the workspace {ws.n}x{ws.n}")
+    xx, k, ld = _as_cols(x, ws.n)
+    _check(_lib.lhl_ldiv(sh._h, ws._h, C.c_void_p(xx.data_ptr()), ld, k, int(rhs_per_shift), _stream(stream)),
+           "lhl_ldiv")
+    return x
+
+
+def lhl_refine_(x: torch.Tensor, J: torch.Tensor, b: torch.Tensor, *args, steps: int = 1, rhs_per_shift: int = 1,
+                stream=None) -> torch.Tensor:
+    """``lhl_refine!(x, A, b, ws, steps)`` with A = sigma I + tau J given by J and the shift
+    slot's (sigma, tau) (F:3144-3157).  Forms: (x, J, b, ws, steps) or (x, J, b, sh, ws, steps)."""
+    if len(args) == 2:
+        ws, steps = args
+        sh = ws.shift
+    elif len(args) == 3:
+        sh, ws, steps = args
+    elif len(args) == 1:
+        ws = args[0]
+        sh = ws.shift
+    else:
+        raise TypeError("lhl_refine_(x, J, b, ws, steps) or (x, J, b, sh, ws, steps)")
+    if steps <= 0:
+        return x
+    for t, nm in ((x, "x"), (J, "J"), (b, "b")):
+        _require_cuda_f64(t, nm)
+    n = ws.n
+    xx, k, ldx = _as_cols(x, n)
+    bb, kb, ldb = _as_cols(b, n)
+    if kb != k:
+        raise DimensionMismatch("x and b differ in column count")
+    Jc = _colmajor(J)
+    R = torch.empty((n, k), dtype=torch.float64, device=x.device).t().contiguous().t() if k > 1 else \
+        torch.empty(n, dtype=torch.float64, device=x.device)
+    ldr = n
+    if ldx != ldr:
+        raise ArgumentError("x must have leading dimension n")
+    _check(_lib.lhl_refine(sh._h, ws._h, C.c_void_p(Jc.data_ptr()), max(Jc.stride(1), n), C.c_void_p(bb.data_ptr()),
+                           ldb, C.c_void_p(xx.data_ptr()), ldx, C.c_void_p(R.data_ptr()), k, int(rhs_per_shift),
+                           int(steps), _stream(stream)), "lhl_refine")
+    return x
+
+
+def residual_norms(sh: LHLShift, J: torch.Tensor, b: torch.Tensor, x: torch.Tensor, rhs_per_shift: int = 1,
+                   stream=None) -> torch.Tensor:
+    """||b - (sigma I + tau J) x||_2 / ||b||_2 per column, on the device."""
+    n = sh.n
+    xx, k, ldx = _as_cols(x, n)
+    bb, _, ldb = _as_cols(b, n)
+    Jc = _colmajor(J)
+    R = torch.empty((k, n), dtype=torch.float64, device=x.device)
+    out = torch.empty(k, dtype=torch.float64, device=x.device)
+    _check(_lib.lhl_residual_norms(sh._h, C.c_void_p(Jc.data_ptr()), max(Jc.stride(1), n), C.c_void_p(bb.data_ptr()),
+                                   ldb, C.c_void_p(xx.data_ptr()), ldx, C.c_void_p(R.data_ptr()),
+                                   C.c_void_p(out.data_ptr()), k, int(rhs_per_shift), _stream(stream)),
+           "residual_norms")
+    return out
+
+
+def applyZ_(x: torch.Tensor, ws: LHLWorkspace, stream=None) -> torch.Tensor:
+    """``applyZ!(x, ws)``: x <- Z x (F:2069)."""
+    _require_cuda_f64(x, "x")
+    xx, k, ld = _as_cols(x, ws.n)
+    _check(_lib.lhl_applyZ(ws._h, C.c_void_p(xx.data_ptr()), ld, k, _stream(stream)), "applyZ")
+    return x
+
+
+def applyZinv_(x: torch.Tensor, ws: LHLWorkspace, stream=None) -> torch.Tensor:
+    """``applyZinv!(x, ws)``: x <- Z^-1 x (F:2104)."""
+    _require_cuda_f64(x, "x")
+    xx, k, ld = _as_cols(x, ws.n)
+    _check(_lib.lhl_applyZinv(ws._h, C.c_void_p(xx.data_ptr()), ld, k, _stream(stream)), "applyZinv")
+    return x
+
+
+def version() -> str:
+    return _lib.lhl_version().decode()
+
+
+__all__ = ["LHLWorkspace", "LHLShift", "lhl", "lhl_", "lhl_reduce_", "lhl_shift_", "lhl_shift_batched_",
+           "lhl_ldiv_", "lhl_refine_", "applyZ_", "applyZinv_", "residual_norms", "ArgumentError",
+           "DimensionMismatch", "LHLDeviceError", "LHL_PREC_FP64", "LHL_PREC_MIXED", "version", "lib"]

@@ -1,0 +1,65 @@
+"""CPU-side checks of the drop-in boundary: the library builds, loads without a GPU and
+exports every entry point include/lhl_gpu.h declares; the host mirror rejects bad
+arguments before touching the device."""
+import ctypes
+import os
+import re
+
+import pytest
+
+REPO = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+HEADER = os.path.join(REPO, "include", "lhl_gpu.h")
+LIB = os.path.join(REPO, "lhl.jl_b200", "liblhl_gpu.so")
+
+
+def declared_functions():
+    src = open(HEADER).read()
+    src = re.sub(r"/\*.*?\*/", "", src, flags=re.S)
+    names = re.findall(r"^\s*(?:int|const char\*)\s+(lhl_\w+)\s*\(", src, flags=re.M)
+    return sorted(set(names))
+
+
+def test_header_declares_the_api():
+    names = declared_functions()
+    for must in ("lhl_ws_create", "lhl_reduce", "lhl_shift", "lhl_shift_batched", "lhl_ldiv", "lhl_refine",
+                 "lhl_applyZ", "lhl_applyZinv"):
+        assert must in names
+
+
+def test_library_exports_every_declared_symbol():
+    if not os.path.exists(LIB):
+        import importlib.util
+        spec = importlib.util.spec_from_file_location("lhl_build", os.path.join(REPO, "lhl.jl_b200", "build.py"))
+        m = importlib.util.module_from_spec(spec)
+        spec.loader.exec_module(m)
+        m.build()
+    L = ctypes.CDLL(LIB)
+    missing = [n for n in declared_functions() if not hasattr(L, n)]
+    assert not missing, missing
+    L.lhl_version.restype = ctypes.c_char_p
+    assert b"sm_100a" in L.lhl_version()
+
+
+def test_null_handles_rejected_on_host():
+    L = ctypes.CDLL(LIB)
+    vp = ctypes.c_void_p
+    assert L.lhl_ws_destroy(vp(0)) == 1
+    assert L.lhl_shift_destroy(vp(0)) == 1
+    L.lhl_ws_create.argtypes = [ctypes.c_int64, ctypes.c_int, ctypes.POINTER(vp)]
+    h = vp()
+    assert L.lhl_ws_create(-1, 0, ctypes.byref(h)) == 2        # DimensionMismatch
+    assert L.lhl_ws_create(4, 7, ctypes.byref(h)) == 1         # ArgumentError: precision
+    L.lhl_ldiv.argtypes = [vp, vp, vp, ctypes.c_int64, ctypes.c_int64, ctypes.c_int64, vp]
+    assert L.lhl_ldiv(vp(0), vp(0), vp(0), 1, 1, 1, vp(0)) == 1
+
+
+def test_configs_are_seeded_and_shaped():
+    import sys
+    sys.path.insert(0, os.path.join(REPO, "lhl.jl_b200"))
+    from lhl_gpu import configs
+    c1 = configs.config1()
+    assert c1["J"].shape == (400, 400) and c1["J"].flags.f_contiguous
+    assert list(-c1["tau"]) == [0.01, 0.013, 0.021]
+    c2a, c2b = configs.config2(8), configs.config2(8)
+    assert (c2a["J"] == c2b["J"]).all() and (c2a["tau"] == c2b["tau"]).all()
+    assert (-c2a["tau"] >= 1e-4).all() and (-c2a["tau"] <= 1e-1).all()

@@ -1,0 +1,243 @@
+"""Parity of the CUDA path with the CPU oracle, through the library's C ABI (via the
+lhl_gpu host mirror).  Plain FP64 form: reduction (pivots, factors, Ht, D) and shift LU
+(Gt, swap, rdiag, info) bit for bit; solves within the reference tests' tolerances and
+the 1e-12 relative residual after one refinement step."""
+import numpy as np
+import pytest
+
+from oracle import oracle as O
+
+pytestmark = pytest.mark.gpu
+
+
+def _mods():
+    import torch
+    import lhl_gpu as G
+    return torch, G
+
+
+def dev(a):
+    torch, _ = _mods()
+    t = torch.as_tensor(np.asfortranarray(a)).cuda()
+    return t
+
+
+def host(t):
+    return t.detach().cpu().numpy()
+
+
+def bits_equal(a, b):
+    a = np.ascontiguousarray(a, dtype=np.float64)
+    b = np.ascontiguousarray(b, dtype=np.float64)
+    return a.shape == b.shape and np.array_equal(a.view(np.int64), b.view(np.int64))
+
+
+def rng(seed):
+    return np.random.default_rng(seed)
+
+
+REDUCE_SIZES = [1, 2, 3, 4, 5, 7, 8, 9, 17, 31, 64, 80, 128, 200, 301, 400, 499, 500, 501, 520, 600, 777, 1030]
+
+
+@pytest.mark.parametrize("n", REDUCE_SIZES)
+@pytest.mark.parametrize("balance", [True, False])
+def test_reduce_bitexact(n, balance):
+    torch, G = _mods()
+    J = rng(n).standard_normal((n, n))
+    R = O.reduce(J, balance=balance)
+    ws = G.lhl(dev(J), balance=balance)
+    ws.check()
+    assert np.array_equal(host(ws.ipiv), R.ipiv)
+    assert bits_equal(host(ws.scale), R.scale)
+    assert bits_equal(host(ws.factors), R.factors)
+    assert bits_equal(host(ws.Ht), R.Ht)
+    assert np.array_equal(host(ws.perm), R.perm) and np.array_equal(host(ws.iperm), R.iperm)
+
+
+@pytest.mark.parametrize("n", [150, 520])
+def test_reduce_ties_and_zeros_bitexact(n):
+    """rand(-1:1) matrices: exact zeros, ties in the pivot search, pulled columns."""
+    torch, G = _mods()
+    J = rng(9).integers(-1, 2, (n, n)).astype(float)
+    R = O.reduce(J)
+    ws = G.lhl(dev(J))
+    ws.check()
+    assert np.array_equal(host(ws.ipiv), R.ipiv)
+    assert bits_equal(host(ws.factors), R.factors)
+
+
+def test_reduce_graded_balancing_bitexact():
+    """A graded matrix that balancing rescales: D, then the blocked reduction."""
+    torch, G = _mods()
+    n = 600
+    J = np.diag(10.0 ** np.linspace(-6, 6, n)) @ rng(3).standard_normal((n, n)) @ np.diag(10.0 ** np.linspace(6, -6, n))
+    R = O.reduce(J)
+    assert (R.scale != 1.0).any()
+    ws = G.lhl(dev(J))
+    ws.check()
+    assert bits_equal(host(ws.scale), R.scale)
+    assert np.array_equal(host(ws.ipiv), R.ipiv)
+    assert bits_equal(host(ws.factors), R.factors)
+
+
+SHIFTS = [(1.0, -0.1), (0.0, 1.0), (1.0, -3.0), (2.0, 0.0), (0.0, 0.0)]
+
+
+@pytest.mark.parametrize("n", list(range(1, 34)) + [63, 64, 65, 255, 256, 257, 511, 512, 513, 1024, 2048])
+@pytest.mark.parametrize("tie", [False, True])
+def test_shift_bitexact(n, tie):
+    """test/core_tests.jl:192-212 on the device: the shift LU state against the oracle's
+    restatement of `_lhl_shift_ref!`, bit for bit, including zero pivots."""
+    torch, G = _mods()
+    g = rng(31 + n + 1000 * tie)
+    J = g.integers(-2, 3, (n, n)).astype(float) if tie else g.standard_normal((n, n))
+    R = O.reduce(J)
+    ws = G.LHLWorkspace(n)
+    ws.Ht.copy_(dev(R.Ht))
+    for s, t in SHIFTS:
+        with np.errstate(divide="ignore", invalid="ignore"):
+            S = O.shift(R, s, t)
+        G.lhl_shift_(ws, s, t)
+        torch.cuda.synchronize()
+        Gt = host(ws.shift.Gt())
+        U = np.array([Gt[j, k] for k in range(n) for j in range(k, n)])
+        l = np.array([Gt[k, k + 1] for k in range(n - 1)])
+        U0, l0, sw0, rd0, info0 = S.state()
+        assert bits_equal(U, U0), (n, s, t)
+        assert bits_equal(l, l0)
+        assert np.array_equal(host(ws.shift.swap()), sw0)
+        assert bits_equal(host(ws.shift.rdiag()), rd0)
+        assert ws.shift.info == info0
+
+
+@pytest.mark.parametrize("n", [1, 2, 3, 5, 40, 129, 260, 400, 600])
+def test_shifted_solves(n):
+    """test/core_tests.jl:23-36 on the device: solves against a dense LU, rtol 1e-9, and the
+    backward error bound of :38-59; agreement with the oracle's solve."""
+    torch, G = _mods()
+    J = rng(n).standard_normal((n, n))
+    b = rng(n + 7).standard_normal(n)
+    R = O.reduce(J)
+    ws = G.lhl(dev(J))
+    for s, t in ((1.0, 0.0), (1.0, -1e-8), (1.0, -0.05), (1.0, 1.7), (0.0, 1.0), (-3.0, 2.0)):
+        W = s * np.eye(n) + t * J
+        if np.linalg.matrix_rank(W) < n:
+            continue
+        G.lhl_shift_(ws, s, t)
+        x = host(G.lhl_ldiv_(dev(b), ws))
+        xr = np.linalg.solve(W, b)
+        assert np.linalg.norm(x - xr) <= 1e-9 * np.linalg.norm(xr)
+        if n <= 500:
+            assert O.bwd(W, x, b) < 50 * np.finfo(float).eps
+        xo = O.ldiv(R, O.shift(R, s, t), b)
+        assert np.linalg.norm(x - xo) <= 1e-9 * np.linalg.norm(xo)
+
+
+def test_config1_refined_residual():
+    """Config 1: J 400x400, three shifts (1, -g), one ldiv + one refinement step each;
+    relative residual <= 1e-12, and the solution agrees with the oracle's."""
+    torch, G = _mods()
+    from lhl_gpu import configs
+    c = configs.config1()
+    n = c["n"]
+    R = O.reduce(c["J"])
+    Jd = dev(c["J"])
+    ws = G.lhl(Jd)
+    ws.check()
+    assert np.array_equal(host(ws.ipiv), R.ipiv)
+    assert bits_equal(host(ws.factors), R.factors)
+    sh = G.LHLShift(n, 3)
+    G.lhl_shift_batched_(sh, ws, dev(c["sigma"]), dev(c["tau"]))
+    B = dev(c["B"])
+    X = B.clone()
+    G.lhl_ldiv_(X, sh, ws)
+    G.lhl_refine_(X, Jd, B, sh, ws, 1)
+    res = host(G.residual_norms(sh, Jd, B, X))
+    assert (res <= 1e-12).all(), res
+    for s in range(3):
+        So = O.shift(R, c["sigma"][s], c["tau"][s])
+        xo = O.refine(R, So, c["J"], c["B"][:, s], O.ldiv(R, So, c["B"][:, s]), 1)
+        x = host(X[:, s])
+        assert np.linalg.norm(x - xo) <= 1e-11 * np.linalg.norm(xo)
+
+
+@pytest.mark.parametrize("n", [50, 700])
+def test_batched_shifts_match_single(n):
+    torch, G = _mods()
+    J = rng(7 + n).standard_normal((n, n))
+    ws = G.lhl(dev(J))
+    sig = np.ones(6)
+    tau = -np.array([1e-4, 1e-3, 0.01, 0.05, 0.1, 0.3])
+    sh = G.LHLShift(n, 6)
+    G.lhl_shift_batched_(sh, ws, dev(sig), dev(tau))
+    B = rng(8).standard_normal((n, 12))
+    X = dev(B)
+    G.lhl_ldiv_(X, sh, ws, rhs_per_shift=2)
+    Xh = host(X)
+    for s in range(6):
+        G.lhl_shift_(ws, sig[s], tau[s])
+        assert bits_equal(host(ws.shift.Gt()), host(sh.Gt(s)))
+        for r in range(2):
+            x1 = host(G.lhl_ldiv_(dev(B[:, 2 * s + r]), ws))
+            assert bits_equal(x1, Xh[:, 2 * s + r])
+
+
+@pytest.mark.parametrize("n", [3, 37, 600])
+def test_applyZ_roundtrip(n):
+    """test/core_tests.jl:5-21 and test/Interface/public_interface.jl:15-19."""
+    torch, G = _mods()
+    J = rng(n).standard_normal((n, n))
+    ws = G.lhl(dev(J))
+    x0 = rng(1).standard_normal(n)
+    x = dev(x0)
+    assert G.applyZ_(x, ws) is x
+    assert G.applyZinv_(x, ws) is x
+    assert np.allclose(host(x), x0, rtol=1e-10, atol=1e-12)
+    R = O.reduce(J)
+    assert np.allclose(host(G.applyZ_(dev(x0), ws)), O.apply_z(R, x0), rtol=1e-12, atol=1e-13)
+
+
+def test_singular_shift_reported():
+    torch, G = _mods()
+    ws = G.lhl(dev(np.array([[1.0, 0.0], [0.0, 2.0]])))
+    G.lhl_shift_(ws, 1.0, -1.0)
+    assert ws.shift.info != 0
+
+
+def test_errors_mirror_the_reference():
+    torch, G = _mods()
+    ws = G.lhl(dev(rng(1).standard_normal((6, 6))))
+    with pytest.raises(G.DimensionMismatch):
+        G.lhl_ldiv_(dev(np.zeros(7)), ws)
+    with pytest.raises(G.DimensionMismatch):
+        G.applyZ_(dev(np.zeros(5)), ws)
+    with pytest.raises(G.ArgumentError):
+        G.lhl_shift_(ws, 1.0, -0.3j)
+    sh = G.LHLShift(5)
+    with pytest.raises(G.DimensionMismatch):
+        G.lhl_ldiv_(dev(np.zeros(6)), sh, ws)
+    with pytest.raises(G.DimensionMismatch):
+        G.lhl(dev(np.zeros((3, 4))))
+    # mutating calls return their first argument (test/Interface/public_interface.jl:7-18)
+    assert G.lhl_shift_(ws, 1.0, -0.1) is ws
+    x = dev(np.ones(6))
+    assert G.lhl_ldiv_(x, ws) is x
+
+
+def test_barrier_timeout_reports_and_recovers():
+    """A grid-barrier wait limit of 1 ns expires: the reduction returns LHL_ERR_TIMEOUT
+    instead of hanging, and the same workspace then reduces correctly."""
+    torch, G = _mods()
+    n = 600
+    J = rng(5).standard_normal((n, n))
+    ws = G.LHLWorkspace(n)
+    ws.set_barrier_limit_ns(1)
+    G.lhl_reduce_(ws, dev(J), True)
+    with pytest.raises(G.LHLDeviceError):
+        ws.check()
+    ws.set_barrier_limit_ns(2_000_000_000)
+    G.lhl_reduce_(ws, dev(J), True)
+    ws.check()
+    R = O.reduce(J)
+    assert np.array_equal(host(ws.ipiv), R.ipiv)
+    assert bits_equal(host(ws.factors), R.factors)
