@@ -231,6 +231,7 @@ def main():
         phase[name] = float(np.mean(tt))
     red = float(np.mean(red_ms))
     phase["reduce"] = red
+    phase["reduce_inside_ms"] = {k: v / 1e6 for k, v in ws.phase_ns().items()}
     alg_bytes = 8.0 * (n ** 3) / 3.0 + 16.0 * n * n   # GEMV stream (8 n^3/3) + J in, Ht/L out
     peak, peak_kind = peaks()
     achieved = alg_bytes / (red * 1e-3) / 1e9

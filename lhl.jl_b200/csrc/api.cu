@@ -16,6 +16,7 @@ struct lhl_ws_s {
     int *cand_i, *bflag, *err;
     unsigned int* bar;
     unsigned long long limit_ns;
+    unsigned long long* ptimes;
 };
 
 struct lhl_shift_s {
@@ -39,7 +40,8 @@ static void ws_free(lhl_ws_t w)
 {
     if (!w) return;
     void* ptrs[] = {w->F, w->Ht, w->scale, w->iscale, w->B0, w->part, w->tab, w->cand_v, w->buf2, w->tsnap,
-                    w->bsum, w->bfac, w->ipiv, w->perm, w->iperm, w->cand_i, w->bflag, w->err, w->bar};
+                    w->bsum, w->bfac, w->ipiv, w->perm, w->iperm, w->cand_i, w->bflag, w->err, w->bar,
+                    w->ptimes};
     for (void* p : ptrs)
         if (p) cudaFree(p);
     delete w;
@@ -85,8 +87,10 @@ int lhl_ws_create(int64_t n, int precision, lhl_ws_t* out)
     A_(bflag, 4);
     A_(err, 4);
     A_(bar, 4);
+    A_(ptimes, 8);
 #undef A_
     if (e == cudaSuccess) e = cudaMemset(w->err, 0, 4 * sizeof(int));
+    if (e == cudaSuccess) e = cudaMemset(w->ptimes, 0, 8 * sizeof(unsigned long long));
     if (e == cudaSuccess) e = cudaMemset(w->Ht, 0, (nn ? nn : 1) * sizeof(double));
     if (e != cudaSuccess) {
         ws_free(w);
@@ -137,6 +141,14 @@ int lhl_ws_check(lhl_ws_t ws, void* stream)
     return err ? err : LHL_OK;
 }
 
+int lhl_ws_phase_ns(lhl_ws_t ws, uint64_t* out8, void* stream)
+{
+    if (!ws || !out8) return LHL_ERR_ARG;
+    cudaError_t e = cudaStreamSynchronize((cudaStream_t)stream);
+    if (e == cudaSuccess) e = cudaMemcpy(out8, ws->ptimes, 8 * sizeof(uint64_t), cudaMemcpyDeviceToHost);
+    return cuda_status(e);
+}
+
 int lhl_reduce(lhl_ws_t ws, const double* dJ, int64_t ldj, int balance, void* stream)
 {
     if (!ws || (!dJ && ws->n > 0)) return LHL_ERR_ARG;
@@ -148,6 +160,7 @@ int lhl_reduce(lhl_ws_t ws, const double* dJ, int64_t ldj, int balance, void* st
                                       cudaMemcpyDeviceToDevice, st);
     if (e == cudaSuccess) e = cudaMemsetAsync(ws->bar, 0, sizeof(unsigned int), st);
     if (e == cudaSuccess) e = cudaMemsetAsync(ws->err, 0, sizeof(int), st);
+    if (e == cudaSuccess) e = cudaMemsetAsync(ws->ptimes, 0, 8 * sizeof(unsigned long long), st);
     if (e != cudaSuccess) return LHL_ERR_CUDA;
     lhl::RedArgs a;
     memset(&a, 0, sizeof(a));
@@ -170,6 +183,7 @@ int lhl_reduce(lhl_ws_t ws, const double* dJ, int64_t ldj, int balance, void* st
     a.bar = ws->bar;
     a.err = ws->err;
     a.limit_ns = ws->limit_ns;
+    a.ptimes = ws->ptimes;
     const int mode = n <= 2 ? 0 : (n < 500 ? 1 : 2);
     if (!balance) {
         // scale = iscale = 1

@@ -25,6 +25,7 @@ struct RedArgs {
     unsigned int* bar;
     int* err;
     unsigned long long limit_ns;
+    unsigned long long* ptimes;  // per-phase wall time (ns) accumulated by CTA 0, 8 slots
 };
 
 // One solve launch (see solve.cu).

@@ -34,6 +34,16 @@ struct StepTab {
     int OR[2 * NBMAX + 4];
 };
 
+// Phase timers: CTA 0, thread 0 adds the wall time since the last mark to slot `slot`.
+__device__ __forceinline__ void tmark(const RedArgs& a, int slot, uint64_t& last)
+{
+    if (blockIdx.x == 0 && threadIdx.x == 0 && a.ptimes) {
+        const uint64_t t = globaltimer_ns();
+        a.ptimes[slot] += t - last;
+        last = t;
+    }
+}
+
 __device__ __forceinline__ void combine_candidates(const RedArgs& a, int* s_p, double* s_red, int* s_redi)
 {
     // every CTA reads all CTA candidates and reduces them (first max, F:1038-1051)
@@ -83,10 +93,24 @@ __device__ __forceinline__ void publish_candidate(const RedArgs& a, double v, in
 // ---------------------------------------------------------------------------------
 // Balancing (F:299-340).  Per sweep: (1) every index's column and row 1-norm (without
 // the diagonal), each one summed sequentially in the reference's order by one thread;
-// (2) one thread walks i = 1..n in order taking the reference's decision; after a
-// scaling it patches the sums of the indices still to come (the only sums it changes);
-// (3) all CTAs apply the sweep's power-of-two factors to A (exact).
+// (2) CTA 0 walks i = 1..n in order taking the reference's decision, RT indices at a
+// time: the first index of the chunk that scales is applied, the sums of the indices
+// still to come are patched for it (its row and column entries change by the factor),
+// and the walk resumes after it; (3) all CTAs apply the sweep's power-of-two factors to A
+// (exact).  The decision of an index after an in-sweep scaling therefore reads a patched
+// sum, which differs from a fresh sequential sum by rounding only.
 // ---------------------------------------------------------------------------------
+__device__ __forceinline__ bool balance_decide(double c, double r, double& f)
+{
+    if (c == 0.0 || r == 0.0) return false;
+    f = 1.0;
+    const double s = c + r;
+    int guard = 0;
+    while (c < r / 2.0 && guard < 4200) { c *= 2.0; r /= 2.0; f *= 2.0; ++guard; }
+    while (c >= 2.0 * r && guard < 8400) { c /= 2.0; r *= 2.0; f /= 2.0; ++guard; }
+    return c + r < 0.95 * s;
+}
+
 __device__ bool balance_phase(const RedArgs& a, GridBarrier& gb)
 {
     const int n = a.n;
@@ -97,11 +121,28 @@ __device__ bool balance_phase(const RedArgs& a, GridBarrier& gb)
         a.scale[i] = 1.0;
         a.iscale[i] = 1.0;
     }
+    __shared__ int s_first;
+    __shared__ double s_f;
     for (int sweep = 0; sweep < 20; ++sweep) {
-        // (1) sums
+        // (1) sums, sequential per index in the reference's order, loads in batches
         for (int i = 1 + gt; i <= n; i += gsz) {
             double c = 0.0, r = 0.0;
-            for (int j = 1; j <= n; ++j) {
+            int j = 1;
+            for (; j + 7 <= n; j += 8) {
+                double vc[8], vr[8];
+#pragma unroll
+                for (int u = 0; u < 8; ++u) {
+                    vc[u] = M1(A, n, j + u, i);
+                    vr[u] = M1(A, n, i, j + u);
+                }
+#pragma unroll
+                for (int u = 0; u < 8; ++u) {
+                    if (j + u == i) continue;
+                    c += fabs(vc[u]);
+                    r += fabs(vr[u]);
+                }
+            }
+            for (; j <= n; ++j) {
                 if (j == i) continue;
                 c += fabs(M1(A, n, j, i));
                 r += fabs(M1(A, n, i, j));
@@ -112,51 +153,42 @@ __device__ bool balance_phase(const RedArgs& a, GridBarrier& gb)
         }
         if (gt == 0) a.bflag[0] = 0;
         if (!gb.sync()) return false;
-        // (2) the sequential decision walk, CTA 0
+        // (2) the ordered decision walk, CTA 0
         if (blockIdx.x == 0) {
-            __shared__ double s_f;
-            __shared__ int s_i;
-            int i = 1;
-            while (i <= n) {
-                if (threadIdx.x == 0) {
-                    s_i = 0;
-                    for (; i <= n; ++i) {
-                        double c = a.bsum[i - 1], r = a.bsum[n + i - 1];
-                        if (c == 0.0 || r == 0.0) continue;
-                        double f = 1.0;
-                        const double s = c + r;
-                        int guard = 0;
-                        while (c < r / 2.0 && guard < 4200) { c *= 2.0; r /= 2.0; f *= 2.0; ++guard; }
-                        while (c >= 2.0 * r && guard < 8400) { c /= 2.0; r *= 2.0; f /= 2.0; ++guard; }
-                        if (c + r < 0.95 * s) {
-                            s_i = i;
-                            s_f = f;
-                            a.bflag[0] = 1;
-                            break;
-                        }
-                    }
+            int base = 1;
+            while (base <= n) {
+                if (threadIdx.x == 0) s_first = 0x7fffffff;
+                __syncthreads();
+                const int i = base + threadIdx.x;
+                double f = 1.0;
+                if (i <= n && balance_decide(a.bsum[i - 1], a.bsum[n + i - 1], f)) atomicMin(&s_first, i);
+                __syncthreads();
+                const int si = s_first;
+                if (si == 0x7fffffff) {
+                    base += RT;
+                    continue;
+                }
+                if (i == si) {
+                    s_f = f;
+                    a.bflag[0] = 1;
                 }
                 __syncthreads();
-                const int si = s_i;
-                if (si == 0) break;
-                const double f = s_f;
-                // current A[si, m] = A0[si, m] * fac[m] / fac[si]; patch sums of m > si
-                const double fi = a.bfac[si - 1];
+                const double fs = s_f;
+                // patch the sums of m > si: row si's entry in column m is divided by fs,
+                // column si's entry in row m multiplied (indices > si are unscaled so far)
                 for (int m = si + 1 + threadIdx.x; m <= n; m += RT) {
-                    const double fm = a.bfac[m - 1];
-                    const double vr = fabs(M1(A, n, si, m)) * fm / fi;  // row si entry in column m
-                    const double vc = fabs(M1(A, n, m, si)) * fi / fm;  // column si entry in row m
-                    a.bsum[m - 1] = (a.bsum[m - 1] - vr) + vr / f;
-                    a.bsum[n + m - 1] = (a.bsum[n + m - 1] - vc) + vc * f;
+                    const double vr = fabs(M1(A, n, si, m));
+                    const double vc = fabs(M1(A, n, m, si));
+                    a.bsum[m - 1] = (a.bsum[m - 1] - vr) + vr / fs;
+                    a.bsum[n + m - 1] = (a.bsum[n + m - 1] - vc) + vc * fs;
                 }
-                __syncthreads();
                 if (threadIdx.x == 0) {
-                    a.bfac[si - 1] = fi * f;
-                    a.scale[si - 1] *= f;
-                    a.iscale[si - 1] /= f;
+                    a.bfac[si - 1] = fs;
+                    a.scale[si - 1] *= fs;
+                    a.iscale[si - 1] /= fs;
                 }
                 __syncthreads();
-                i = si + 1;
+                base = si + 1;
             }
         }
         if (!gb.sync()) return false;
@@ -321,77 +353,145 @@ struct PanelSh {
     double red[RW];
     int redi[RW];
     int p;
+    double tri[NBMAX + 1][NBMAX + 1];  // A[k0+1+r, k0+c]: the panel's multipliers at rows <= k+1
+    double sval[2 * NBMAX + 2];        // values at the special rows
+    int slist[2 * NBMAX + 2];          // swap partners beyond row k+1, first-occurrence order
+    int nsl;
 };
 
-// Phase A table (one warp; lane 0 does the sequential parts): F:952-980, F:1088-1132.
-__device__ void build_step_table(const RedArgs& a, StepTab* T, int k0, int kb, int k, int p, double piv)
+// Rows k0+1..k+1 of the panel's multiplier columns k0..k into S.tri (one warp, parallel
+// loads), so the sequential triangles below run on shared memory only.
+__device__ __forceinline__ void load_tri(const RedArgs& a, PanelSh& S, int k0, int k)
+{
+    const int m = k - k0 + 1;
+    const int lane = threadIdx.x & 31;
+    for (int e = lane; e < m * m; e += 32) {
+        const int r = e % m, c = e / m;
+        S.tri[r][c] = M1(a.A, a.n, k0 + 1 + r, k0 + c);
+    }
+}
+
+// Swap partners beyond row k+1 of steps k0..k (q = p for step k), first-occurrence order.
+__device__ __forceinline__ void partner_list(const RedArgs& a, PanelSh& S, int k0, int k, int p)
+{
+    if ((threadIdx.x & 31) == 0) {
+        int np = 0;
+        for (int kk = k0; kk <= k; ++kk) {
+            const int q = (kk == k) ? p : (int)a.ipiv[kk - 1];
+            if (q <= k + 1) continue;
+            bool found = false;
+            for (int r = 0; r < np; ++r)
+                if (S.slist[r] == q) found = true;
+            if (!found) S.slist[np++] = q;
+        }
+        S.nsl = np;
+    }
+    __syncwarp();
+}
+
+// sum of the GEMV partials of row i in group order (F:1558-1583); loads issued in batches
+__device__ __forceinline__ double partial_sum(const RedArgs& a, int P, int i)
+{
+    const double* pp = a.part + (i - 1);
+    const size_t st = (size_t)a.n;
+    double s = pp[0];
+    int g = 1;
+    for (; g + 7 < P; g += 8) {
+        double v[8];
+#pragma unroll
+        for (int u = 0; u < 8; ++u) v[u] = pp[(size_t)(g + u) * st];
+#pragma unroll
+        for (int u = 0; u < 8; ++u) s = dadd(s, v[u]);
+    }
+    for (; g < P; ++g) s = dadd(s, pp[(size_t)g * st]);
+    return s;
+}
+
+// Phase A table, one warp of CTA 0 (F:952-980 and the pulled-column tables F:1088-1132).
+// Loads are issued in parallel into shared memory; the sequential parts (interchanges,
+// catch-up triangle) then run on shared memory.  The table is published to G.
+__device__ void build_step_table(const RedArgs& a, PanelSh& S, StepTab* G, int k0, int kb, int k, int p, double piv)
 {
     const int n = a.n;
     const double* A = a.A;
     const int lane = threadIdx.x & 31;
+    StepTab& T = S.tab;
     for (int j = k0 + lane; j <= kb + 1; j += 32) {
-        T->R1[j - k0] = M1(A, n, k + 1, j);
-        T->RP[j - k0] = M1(A, n, p, j);
+        T.R1[j - k0] = M1(A, n, k + 1, j);
+        T.RP[j - k0] = M1(A, n, p, j);
     }
     for (int j = k + 2 + lane; j <= kb + 1; j += 32) {
         const double v = (j == p) ? M1(A, n, k + 1, k) : M1(A, n, j, k);
-        T->VJ[j - k0] = v / piv;
+        T.VJ[j - k0] = v / piv;
     }
-    __syncwarp();
-    if (lane == 0) {
-        T->p = p;
-        T->piv = piv;
-        const int pulled = p > kb + 1;
-        T->pulled = pulled;
-        int nov = 0;
-        if (pulled) {
-            for (int kk = k0; kk <= k; ++kk) {
-                T->OV[kk - k0] = M1(A, n, kk + 1, p);
-                T->OR[kk - k0] = kk + 1;
-            }
-            nov = k - k0 + 1;
+    const int pulled = p > kb + 1;
+    const int m = k - k0 + 1;
+    int nov = 0;
+    if (pulled) {
+        if (lane < m) {
+            T.OV[lane] = M1(A, n, k0 + 1 + lane, p);
+            T.OR[lane] = k0 + 1 + lane;
+        }
+        load_tri(a, S, k0, k);
+        partner_list(a, S, k0, k, p);
+        if (lane < S.nsl) S.sval[lane] = M1(A, n, S.slist[lane], p);
+        __syncwarp();
+        if (lane == 0) {
+            nov = m;
             for (int kk = k0; kk <= k; ++kk) {
                 const int q = (kk == k) ? p : (int)a.ipiv[kk - 1];
                 if (q == kk + 1) continue;
                 int s = -1;
-                for (int r = 0; r < nov; ++r)
-                    if (T->OR[r] == q) { s = r; break; }
-                if (s < 0) {
-                    s = nov++;
-                    T->OV[s] = M1(A, n, q, p);
-                    T->OR[s] = q;
+                if (q <= k + 1) {
+                    s = q - k0 - 1;
+                } else {
+                    for (int r = m; r < nov; ++r)
+                        if (T.OR[r] == q) { s = r; break; }
+                    if (s < 0) {
+                        s = nov++;
+                        int idx = 0;
+                        for (int r = 0; r < S.nsl; ++r)
+                            if (S.slist[r] == q) idx = r;
+                        T.OV[s] = S.sval[idx];
+                        T.OR[s] = q;
+                    }
                 }
-                const double t = T->OV[kk - k0];
-                T->OV[kk - k0] = T->OV[s];
-                T->OV[s] = t;
+                const double t = T.OV[kk - k0];
+                T.OV[kk - k0] = T.OV[s];
+                T.OV[s] = t;
             }
-            for (int kk = k0; kk <= k - 1; ++kk) {
-                const double x = T->OV[kk - k0];
-                T->CX[kk - k0] = x;
-                if (x == 0.0) continue;
-                for (int i = kk + 2; i <= k + 1; ++i) {
-                    const double aik = (i == k + 1) ? T->RP[kk - k0] : M1(A, n, i, kk);
-                    T->OV[i - k0 - 1] = dsub(T->OV[i - k0 - 1], dmul(aik, x));
-                }
+            T.nov = nov;
+        }
+        __syncwarp();
+        // catch-up of rows k0+1..k+1 by the left transforms k0..k-1, lanes = rows
+        double ov = (lane < m) ? T.OV[lane] : 0.0;
+        const int row = k0 + 1 + lane;
+        for (int kk = k0; kk <= k - 1; ++kk) {
+            const double x = __shfl_sync(0xffffffffu, ov, kk - k0);
+            if (lane == 0) T.CX[kk - k0] = x;
+            if (x != 0.0 && lane < m && row >= kk + 2) {
+                const double aik = (row == k + 1) ? T.RP[kk - k0] : S.tri[lane][kk - k0];
+                ov = dsub(ov, dmul(aik, x));
             }
         }
-        T->nov = nov;
-        for (int j = k + 1; j <= kb + 1; ++j) T->PJ[j - k - 1] = T->RP[j - k0];
-        if (pulled) T->PJ[0] = T->OV[k - k0];
+        if (lane < m) T.OV[lane] = ov;
+        __syncwarp();
+    }
+    if (lane == 0) {
+        T.p = p;
+        T.piv = piv;
+        T.pulled = pulled;
+        T.skip = 0;
+        if (!pulled) T.nov = 0;
+        for (int j = k + 1; j <= kb + 1; ++j) T.PJ[j - k - 1] = T.RP[j - k0];
+        if (pulled) T.PJ[0] = T.OV[k - k0];
         else if (p != k + 1) {
-            T->PJ[0] = T->RP[p - k0];
-            T->PJ[p - k - 1] = T->RP[k + 1 - k0];
+            T.PJ[0] = T.RP[p - k0];
+            T.PJ[p - k - 1] = T.RP[k + 1 - k0];
         }
     }
-}
-
-// sum of the GEMV partials of row i in group order (F:1558-1583)
-__device__ __forceinline__ double partial_sum(const RedArgs& a, int P, int i)
-{
-    const double* pp = a.part + (i - 1);
-    double s = pp[0];
-    for (int g = 1; g < P; ++g) s = dadd(s, pp[(size_t)g * a.n]);
-    return s;
+    __syncwarp();
+    for (int e = lane; e < (int)(sizeof(StepTab) / sizeof(int)); e += 32) ((int*)G)[e] = ((const int*)&T)[e];
 }
 
 // GEMV partials of phase A (F:1496-1553): task = (group g, 32-row tile), lane = row.
@@ -458,18 +558,25 @@ __device__ void gemv_tasks(const RedArgs& a, int k0, int kb, int k, int p, doubl
 
 // The correction triangle of phase B, computed redundantly by every CTA's warp 0
 // (F:1232-1269): LW (rows k0+1..k+1), LQ (swap partners beyond k+1), XS (the x's).
-__device__ void correction_triangle(const RedArgs& a, PanelSh& S, int k0, int k, int P)
+// All special-row sums are formed in parallel first; the interchange pass and the
+// triangle then run on shared memory.
+__device__ void correction_triangle(const RedArgs& a, PanelSh& S, int k0, int k, int p, int P)
 {
-    const int n = a.n;
-    const double* A = a.A;
     const int lane = threadIdx.x & 31;
     const int m = k - k0 + 1;
-    if (lane < m) S.LW[lane] = partial_sum(a, P, k0 + 1 + lane);
+    load_tri(a, S, k0, k);
+    partner_list(a, S, k0, k, p);
+    for (int idx = lane; idx < m + S.nsl; idx += 32) {
+        const int row = (idx < m) ? k0 + 1 + idx : S.slist[idx - m];
+        const double v = partial_sum(a, P, row);
+        if (idx < m) S.LW[idx] = v;
+        else S.sval[idx - m] = v;
+    }
     __syncwarp();
     if (lane == 0) {
         int nq = 0;
         for (int kk = k0; kk <= k; ++kk) {
-            const int q = (int)a.ipiv[kk - 1];
+            const int q = (kk == k) ? p : (int)a.ipiv[kk - 1];
             if (q == kk + 1) continue;
             if (q <= k + 1) {
                 const double t = S.LW[kk - k0];
@@ -481,7 +588,10 @@ __device__ void correction_triangle(const RedArgs& a, PanelSh& S, int k0, int k,
                     if (S.LR[r] == q) { s = r; break; }
                 if (s < 0) {
                     s = nq++;
-                    S.LQ[s] = partial_sum(a, P, q);
+                    int idx = 0;
+                    for (int r = 0; r < S.nsl; ++r)
+                        if (S.slist[r] == q) idx = r;
+                    S.LQ[s] = S.sval[idx];
                     S.LR[s] = q;
                 }
                 const double t = S.LW[kk - k0];
@@ -499,7 +609,7 @@ __device__ void correction_triangle(const RedArgs& a, PanelSh& S, int k0, int k,
         const double x = __shfl_sync(0xffffffffu, lw, kk - k0);
         if (lane == 0) S.XS[kk - k0] = x;
         if (x != 0.0 && lane < m) {
-            if (row >= kk + 2 && row <= k) lw = dsub(lw, dmul(M1(A, n, row, kk), x));
+            if (row >= kk + 2 && row <= k) lw = dsub(lw, dmul(S.tri[lane][kk - k0], x));
             else if (row == k + 1 && kk + 2 <= k + 1) lw = dsub(lw, dmul(S.tab.RP[kk - k0], x));
         }
     }
@@ -685,7 +795,7 @@ __device__ void column_end(const RedArgs& a, const PanelSh& S, int k0, int kb, i
 }
 
 template <int NB>
-__device__ bool blocked_phase(const RedArgs& a, GridBarrier& gb, PanelSh& S)
+__device__ bool blocked_phase(const RedArgs& a, GridBarrier& gb, PanelSh& S, uint64_t& last)
 {
     const int n = a.n;
     const int nb = NB;
@@ -719,21 +829,25 @@ __device__ bool blocked_phase(const RedArgs& a, GridBarrier& gb, PanelSh& S)
             const double piv = (p == k + 1) ? M1(A, n, k + 1, k) : M1(A, n, p, k);
             if (blockIdx.x == 0 && warp == 0) {
                 if (lane == 0) a.ipiv[k - 1] = p;
-                if (piv != 0.0) build_step_table(a, gtab, k0, kb, k, p, piv);
-                if (lane == 0) {
-                    gtab->skip = (piv == 0.0);
+                if (piv != 0.0) {
+                    build_step_table(a, S, gtab, k0, kb, k, p, piv);
+                } else if (lane == 0) {
+                    gtab->skip = 1;
                     gtab->p = p;
                     gtab->piv = piv;
+                    gtab->pulled = 0;
+                    gtab->nov = 0;
                 }
             }
             if (piv != 0.0) gemv_tasks(a, k0, kb, k, p, piv, 1);
             if (!gb.sync()) return false;
+            tmark(a, 1, last);
             // ---- phase B: rows ----
             for (int e = threadIdx.x; e < (int)(sizeof(StepTab) / sizeof(int)); e += RT)
                 ((int*)&S.tab)[e] = ((volatile int*)gtab)[e];
             __syncthreads();
             const bool skip = S.tab.skip != 0;
-            if (!skip && warp == 0) correction_triangle(a, S, k0, k, P);
+            if (!skip && warp == 0) correction_triangle(a, S, k0, k, p, P);
             __syncthreads();
             double cand = 0.0;
             int candi = 0;
@@ -761,6 +875,7 @@ __device__ bool blocked_phase(const RedArgs& a, GridBarrier& gb, PanelSh& S)
             }
             publish_candidate(a, cand, candi, S.red, S.redi);
             if (!gb.sync()) return false;
+            tmark(a, 2, last);
         }
         // ---- panel end E1: interchange map, TRSM inverse, column sweeps ----
         build_swap_map(a, S, k0, kb);
@@ -777,6 +892,7 @@ __device__ bool blocked_phase(const RedArgs& a, GridBarrier& gb, PanelSh& S)
             }
         }
         if (!gb.sync()) return false;
+        tmark(a, 3, last);
         // ---- panel end E2: trailing GEMM, top GEMM, next panel's B0 ----
         {
             const int nbp = kb - k0 + 1;
@@ -797,6 +913,7 @@ __device__ bool blocked_phase(const RedArgs& a, GridBarrier& gb, PanelSh& S)
 #pragma unroll
                     for (int s = 0; s < NBMAX; ++s) Lr[s] = (act && s < nbp) ? -M1(A, n, i, k0 + s) : 0.0;
                     const int cend = min(kb + 2 + tj * 32 + 31, n);
+#pragma unroll 4
                     for (int c = kb + 2 + tj * 32; c <= cend; ++c) {
                         const double* U = A + (size_t)(c - 1) * n + k0;  // rows k0+1..kb+1
                         double uv = (lane < nbp) ? U[lane] : 0.0;
@@ -837,13 +954,28 @@ __device__ bool blocked_phase(const RedArgs& a, GridBarrier& gb, PanelSh& S)
                         }
                         acc[q] = v;
                     }
-                    for (int j = kb + 2; j <= n; ++j) {
+                    // one fma chain per element over j = kb+2..n, in order; loads in batches of 8
+                    const int c0q = cg * 4;
+                    const int nq = min(4, nbp - c0q);
+                    int j = kb + 2;
+                    for (; j + 7 <= n; j += 8) {
+                        double av[8], lv[8][4];
+#pragma unroll
+                        for (int u = 0; u < 8; ++u) {
+                            av[u] = M1(A, n, ii, j + u);
+#pragma unroll
+                            for (int q = 0; q < 4; ++q) lv[u][q] = (q < nq) ? M1(A, n, j + u, k0 + c0q + q) : 0.0;
+                        }
+#pragma unroll
+                        for (int u = 0; u < 8; ++u)
+#pragma unroll
+                            for (int q = 0; q < 4; ++q) acc[q] = dfma(av[u], lv[u][q], acc[q]);
+                    }
+                    for (; j <= n; ++j) {
                         const double aij = M1(A, n, ii, j);
 #pragma unroll
-                        for (int q = 0; q < 4; ++q) {
-                            const int cc = cg * 4 + q;
-                            if (cc < nbp) acc[q] = dfma(aij, M1(A, n, j, k0 + cc), acc[q]);
-                        }
+                        for (int q = 0; q < 4; ++q)
+                            if (q < nq) acc[q] = dfma(aij, M1(A, n, j, k0 + c0q + q), acc[q]);
                     }
                     if (act) {
 #pragma unroll
@@ -864,6 +996,7 @@ __device__ bool blocked_phase(const RedArgs& a, GridBarrier& gb, PanelSh& S)
             }
         }
         if (!gb.sync()) return false;
+        tmark(a, 4, last);
     }
     return true;
 }
@@ -876,14 +1009,18 @@ __global__ void __launch_bounds__(RT, 1) reduce_kernel(RedArgs a, int balance, i
 {
     __shared__ PanelSh S;
     GridBarrier gb{a.bar, a.err, a.limit_ns, 0};
+    uint64_t t0 = globaltimer_ns(), last = t0;
     if (balance) {
         if (!balance_phase(a, gb)) return;
     }
+    tmark(a, 0, last);
     if (mode == 1) {
         unblocked_phase(a, gb);
+        tmark(a, 1, last);
     } else if (mode == 2) {
-        blocked_phase<NBMAX>(a, gb, S);
+        blocked_phase<NBMAX>(a, gb, S, last);
     }
+    if (blockIdx.x == 0 && threadIdx.x == 0 && a.ptimes) a.ptimes[7] += globaltimer_ns() - t0;
 }
 
 // Ht[j,i] = A[i,j] for i <= j+1, zero elsewhere (F:2005-2061); 32x32 tiles.
