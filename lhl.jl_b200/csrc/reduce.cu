@@ -916,18 +916,17 @@ __device__ bool blocked_phase(const RedArgs& a, GridBarrier& gb, PanelSh& S, uin
 #pragma unroll 4
                     for (int c = kb + 2 + tj * 32; c <= cend; ++c) {
                         const double* U = A + (size_t)(c - 1) * n + k0;  // rows k0+1..kb+1
-                        double uv = (lane < nbp) ? U[lane] : 0.0;
+                        const double uv = (lane < nbp) ? U[lane] : 0.0;
+                        double us[NBMAX];
+#pragma unroll
+                        for (int s = 0; s < NBMAX; ++s) us[s] = __shfl_sync(0xffffffffu, uv, s);  // all lanes
                         if (act) {
                             double v = M1(A, n, i, c);
 #pragma unroll
                             for (int s = 0; s < NBMAX; ++s)
-                                if (s < nbp) v = dfma(Lr[s], __shfl_sync(0xffffffffu, uv, s), v);
-                                else (void)0;
+                                if (s < nbp) v = dfma(Lr[s], us[s], v);
                             M1(A, n, i, c) = v;
                             if (more && c >= k0n + 1 && c <= kbn + 1) a.B0[(size_t)(c - k0n - 1) * n + (i - 1)] = v;
-                        } else {
-#pragma unroll
-                            for (int s = 0; s < NBMAX; ++s) if (s < nbp) (void)__shfl_sync(0xffffffffu, uv, s);
                         }
                     }
                 } else {
