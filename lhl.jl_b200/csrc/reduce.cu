@@ -424,6 +424,7 @@ __device__ void build_step_table(const RedArgs& a, PanelSh& S, StepTab* G, int k
         const double v = (j == p) ? M1(A, n, k + 1, k) : M1(A, n, j, k);
         T.VJ[j - k0] = v / piv;
     }
+    __syncwarp();  // R1 / RP / VJ are read by other lanes below
     const int pulled = p > kb + 1;
     const int m = k - k0 + 1;
     int nov = 0;
