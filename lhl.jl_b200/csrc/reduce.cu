@@ -357,6 +357,7 @@ struct PanelSh {
     double sval[2 * NBMAX + 2];        // values at the special rows
     int slist[2 * NBMAX + 2];          // swap partners beyond row k+1, first-occurrence order
     int nsl;
+    int ipv[NBMAX];                    // ipiv[k0..k] of the panel so far
 };
 
 // Rows k0+1..k+1 of the panel's multiplier columns k0..k into S.tri (one warp, parallel
@@ -371,13 +372,17 @@ __device__ __forceinline__ void load_tri(const RedArgs& a, PanelSh& S, int k0, i
     }
 }
 
-// Swap partners beyond row k+1 of steps k0..k (q = p for step k), first-occurrence order.
+// The panel's pivots ipiv[k0..k] (p for step k) into S.ipv, then the swap partners beyond
+// row k+1 in first-occurrence order.  One warp.
 __device__ __forceinline__ void partner_list(const RedArgs& a, PanelSh& S, int k0, int k, int p)
 {
-    if ((threadIdx.x & 31) == 0) {
+    const int lane = threadIdx.x & 31;
+    if (lane <= k - k0) S.ipv[lane] = (k0 + lane == k) ? p : (int)a.ipiv[k0 + lane - 1];
+    __syncwarp();
+    if (lane == 0) {
         int np = 0;
         for (int kk = k0; kk <= k; ++kk) {
-            const int q = (kk == k) ? p : (int)a.ipiv[kk - 1];
+            const int q = S.ipv[kk - k0];
             if (q <= k + 1) continue;
             bool found = false;
             for (int r = 0; r < np; ++r)
@@ -440,7 +445,7 @@ __device__ void build_step_table(const RedArgs& a, PanelSh& S, StepTab* G, int k
         if (lane == 0) {
             nov = m;
             for (int kk = k0; kk <= k; ++kk) {
-                const int q = (kk == k) ? p : (int)a.ipiv[kk - 1];
+                const int q = S.ipv[kk - k0];
                 if (q == kk + 1) continue;
                 int s = -1;
                 if (q <= k + 1) {
@@ -524,34 +529,46 @@ __device__ void gemv_tasks(const RedArgs& a, int k0, int kb, int k, int p, doubl
         const int i = k0 + 1 + tile * 32 + lane;
         const bool act = i <= n;
         const int ii = act ? i : n;
-        auto L = [&](int j) -> double {
-            const int m = j - ga;
-            const double v0 = __shfl_sync(0xffffffffu, l0, m & 31);
-            const double v1 = __shfl_sync(0xffffffffu, l1, m & 31);
-            return m < 32 ? v0 : v1;
-        };
         auto COL = [&](int j) -> const double* { return (pulled && j == p) ? sub : A + (size_t)(j - 1) * n; };
-        double acc;
-        int j = ga;
-        if (j + 3 <= gb) {
-            const double q1 = L(j), q2 = L(j + 1), q3 = L(j + 2), q4 = L(j + 3);
-            acc = dadd(dadd(dmul(q1, COL(j)[ii - 1]), dmul(q2, COL(j + 1)[ii - 1])),
-                       dadd(dmul(q3, COL(j + 2)[ii - 1]), dmul(q4, COL(j + 3)[ii - 1])));
-            j += 4;
-        } else {
-            acc = dmul(L(j), COL(j)[ii - 1]);
-            j += 1;
-        }
-        while (j + 3 <= gb) {
-            const double q1 = L(j), q2 = L(j + 1), q3 = L(j + 2), q4 = L(j + 3);
-            acc = dadd(acc, dadd(dadd(dmul(q1, COL(j)[ii - 1]), dmul(q2, COL(j + 1)[ii - 1])),
-                                 dadd(dmul(q3, COL(j + 2)[ii - 1]), dmul(q4, COL(j + 3)[ii - 1]))));
-            j += 4;
-        }
-        while (j <= gb) {
-            const double lj = L(j);
-            if (lj != 0.0) acc = dadd(acc, dmul(lj, COL(j)[ii - 1]));
-            j += 1;
+        // the reference's group order: the first four-column pass assigns, later passes add,
+        // single tail columns add l*a (skipped when l == 0; a group of <= 3 columns assigns
+        // its first); operands are fetched 16 columns at a time
+        const int w = gb - ga + 1;
+        const int nquad = w >> 2;
+        double acc = 0.0;
+        bool have = false;
+        for (int b0 = 0; b0 < w; b0 += 16) {
+            double av[16], lv[16];
+#pragma unroll
+            for (int u = 0; u < 16; ++u) av[u] = (b0 + u < w) ? COL(ga + b0 + u)[ii - 1] : 0.0;
+#pragma unroll
+            for (int u = 0; u < 16; ++u) {
+                const int m = b0 + u;
+                const double v0 = __shfl_sync(0xffffffffu, l0, m & 31);
+                const double v1 = __shfl_sync(0xffffffffu, l1, m & 31);
+                lv[u] = m < 32 ? v0 : v1;
+            }
+#pragma unroll
+            for (int q = 0; q < 4; ++q) {
+                if (((b0 >> 2) + q) < nquad) {
+                    const double quad = dadd(dadd(dmul(lv[4 * q], av[4 * q]), dmul(lv[4 * q + 1], av[4 * q + 1])),
+                                             dadd(dmul(lv[4 * q + 2], av[4 * q + 2]), dmul(lv[4 * q + 3], av[4 * q + 3])));
+                    acc = have ? dadd(acc, quad) : quad;
+                    have = true;
+                }
+            }
+#pragma unroll
+            for (int u = 0; u < 16; ++u) {
+                const int off = b0 + u;
+                if (off >= 4 * nquad && off < w) {
+                    if (!have) {
+                        acc = dmul(lv[u], av[u]);
+                        have = true;
+                    } else if (lv[u] != 0.0) {
+                        acc = dadd(acc, dmul(lv[u], av[u]));
+                    }
+                }
+            }
         }
         if (act) a.part[(size_t)g * n + (i - 1)] = acc;
     }
@@ -577,7 +594,7 @@ __device__ void correction_triangle(const RedArgs& a, PanelSh& S, int k0, int k,
     if (lane == 0) {
         int nq = 0;
         for (int kk = k0; kk <= k; ++kk) {
-            const int q = (kk == k) ? p : (int)a.ipiv[kk - 1];
+            const int q = S.ipv[kk - k0];
             if (q == kk + 1) continue;
             if (q <= k + 1) {
                 const double t = S.LW[kk - k0];
@@ -733,6 +750,8 @@ __device__ void panel_row(const RedArgs& a, const PanelSh& S, int k0, int kb, in
 // pre-sweep value it receives after the whole sequence (F:1344-1379, F:1395-1415).
 __device__ void build_swap_map(const RedArgs& a, PanelSh& S, int k0, int kb)
 {
+    if ((int)threadIdx.x <= kb - k0) S.ipv[threadIdx.x] = (int)a.ipiv[k0 + threadIdx.x - 1];
+    __syncthreads();
     if (threadIdx.x == 0) {
         int nsr = 0;
         int val[2 * NBMAX + 2];
@@ -744,7 +763,7 @@ __device__ void build_swap_map(const RedArgs& a, PanelSh& S, int k0, int kb)
             return nsr++;
         };
         for (int k = k0; k <= kb; ++k) {
-            const int p = (int)a.ipiv[k - 1];
+            const int p = S.ipv[k - k0];
             if (p <= k + 1 || p > a.n) continue;
             const int s1 = find(k + 1), s2 = find(p);
             const int t = val[s1];
@@ -760,14 +779,15 @@ __device__ void build_swap_map(const RedArgs& a, PanelSh& S, int k0, int kb)
 // P = M^-1 - I of the panel's multipliers (F:1944-1955), into shared memory.
 __device__ void build_trsm_inverse(const RedArgs& a, PanelSh& S, int k0, int kb)
 {
-    const int n = a.n;
     const int nbp = kb - k0 + 1;
+    if (threadIdx.x < 32) load_tri(a, S, k0, kb);  // tri[r-1][s-1] = M[r,s] = A[k0+r, k0+s-1]
+    __syncthreads();
     const int q = threadIdx.x + 1;  // column q of P
     if (threadIdx.x < nbp) {
         for (int r = 1; r <= nbp; ++r) {
             if (r <= q) { S.Pm[r - 1][q - 1] = 0.0; continue; }
-            double acc = -M1(a.A, n, k0 + r, k0 + q - 1);
-            for (int s = q + 1; s <= r - 1; ++s) acc = dsub(acc, dmul(M1(a.A, n, k0 + r, k0 + s - 1), S.Pm[s - 1][q - 1]));
+            double acc = -S.tri[r - 1][q - 1];
+            for (int s = q + 1; s <= r - 1; ++s) acc = dsub(acc, dmul(S.tri[r - 1][s - 1], S.Pm[s - 1][q - 1]));
             S.Pm[r - 1][q - 1] = acc;
         }
     }
@@ -958,16 +978,16 @@ __device__ bool blocked_phase(const RedArgs& a, GridBarrier& gb, PanelSh& S, uin
                     const int c0q = cg * 4;
                     const int nq = min(4, nbp - c0q);
                     int j = kb + 2;
-                    for (; j + 7 <= n; j += 8) {
-                        double av[8], lv[8][4];
+                    for (; j + 15 <= n; j += 16) {
+                        double av[16], lv[16][4];
 #pragma unroll
-                        for (int u = 0; u < 8; ++u) {
+                        for (int u = 0; u < 16; ++u) {
                             av[u] = M1(A, n, ii, j + u);
 #pragma unroll
                             for (int q = 0; q < 4; ++q) lv[u][q] = (q < nq) ? M1(A, n, j + u, k0 + c0q + q) : 0.0;
                         }
 #pragma unroll
-                        for (int u = 0; u < 8; ++u)
+                        for (int u = 0; u < 16; ++u)
 #pragma unroll
                             for (int q = 0; q < 4; ++q) acc[q] = dfma(av[u], lv[u][q], acc[q]);
                     }
