@@ -74,8 +74,11 @@ int lhl_ws_get_view(lhl_ws_t ws, lhl_ws_view* view);
 int lhl_ws_check(lhl_ws_t ws, void* stream);
 /* Wall time (ns) of the last reduction by phase, measured on the device: [0] balancing,
  * [1] pivot + GEMV phases, [2] row phases, [3] panel-end interchanges / TRSM, [4] panel-end
- * GEMMs, [7] the whole persistent kernel.  Waits for the stream. */
+ * GEMMs, [5] CTA 0's total grid-barrier wait, [6] CTA 0's per-step table builds, [7] the
+ * whole persistent kernel.  Waits for the stream. */
 int lhl_ws_phase_ns(lhl_ws_t ws, uint64_t* out8, void* stream);
+/* Finer device timers of the last reduction, per sub-phase of one CTA (16 slots). */
+int lhl_ws_probe_ns(lhl_ws_t ws, uint64_t* out16, void* stream);
 /* Test hook: the wall-time limit of every grid-barrier wait of this workspace's kernels. */
 int lhl_ws_set_barrier_limit_ns(lhl_ws_t ws, uint64_t limit_ns);
 

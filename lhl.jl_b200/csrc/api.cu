@@ -87,10 +87,10 @@ int lhl_ws_create(int64_t n, int precision, lhl_ws_t* out)
     A_(bflag, 4);
     A_(err, 4);
     A_(bar, 4);
-    A_(ptimes, 8);
+    A_(ptimes, 24);
 #undef A_
     if (e == cudaSuccess) e = cudaMemset(w->err, 0, 4 * sizeof(int));
-    if (e == cudaSuccess) e = cudaMemset(w->ptimes, 0, 8 * sizeof(unsigned long long));
+    if (e == cudaSuccess) e = cudaMemset(w->ptimes, 0, 24 * sizeof(unsigned long long));
     if (e == cudaSuccess) e = cudaMemset(w->Ht, 0, (nn ? nn : 1) * sizeof(double));
     if (e != cudaSuccess) {
         ws_free(w);
@@ -149,6 +149,14 @@ int lhl_ws_phase_ns(lhl_ws_t ws, uint64_t* out8, void* stream)
     return cuda_status(e);
 }
 
+int lhl_ws_probe_ns(lhl_ws_t ws, uint64_t* out16, void* stream)
+{
+    if (!ws || !out16) return LHL_ERR_ARG;
+    cudaError_t e = cudaStreamSynchronize((cudaStream_t)stream);
+    if (e == cudaSuccess) e = cudaMemcpy(out16, ws->ptimes + 8, 16 * sizeof(uint64_t), cudaMemcpyDeviceToHost);
+    return cuda_status(e);
+}
+
 int lhl_reduce(lhl_ws_t ws, const double* dJ, int64_t ldj, int balance, void* stream)
 {
     if (!ws || (!dJ && ws->n > 0)) return LHL_ERR_ARG;
@@ -160,7 +168,7 @@ int lhl_reduce(lhl_ws_t ws, const double* dJ, int64_t ldj, int balance, void* st
                                       cudaMemcpyDeviceToDevice, st);
     if (e == cudaSuccess) e = cudaMemsetAsync(ws->bar, 0, sizeof(unsigned int), st);
     if (e == cudaSuccess) e = cudaMemsetAsync(ws->err, 0, sizeof(int), st);
-    if (e == cudaSuccess) e = cudaMemsetAsync(ws->ptimes, 0, 8 * sizeof(unsigned long long), st);
+    if (e == cudaSuccess) e = cudaMemsetAsync(ws->ptimes, 0, 24 * sizeof(unsigned long long), st);
     if (e != cudaSuccess) return LHL_ERR_CUDA;
     lhl::RedArgs a;
     memset(&a, 0, sizeof(a));

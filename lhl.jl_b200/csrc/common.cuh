@@ -52,6 +52,7 @@ struct GridBarrier {
     int* err;
     unsigned long long limit_ns;
     unsigned int seq;
+    unsigned long long* wait_ns;  // optional: CTA 0 accumulates its wait (arrival -> release)
 
     __device__ __forceinline__ bool sync()
     {
@@ -75,6 +76,7 @@ struct GridBarrier {
             }
             if (ok && ld_acquire_i32(err) != 0) ok = 0;
             __threadfence();
+            if (wait_ns && blockIdx.x == 0) *wait_ns += globaltimer_ns() - t0;
             s_ok = ok;
         }
         __syncthreads();

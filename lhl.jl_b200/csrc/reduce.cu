@@ -44,6 +44,16 @@ __device__ __forceinline__ void tmark(const RedArgs& a, int slot, uint64_t& last
     }
 }
 
+// Finer probe: thread 0 of CTA `cta` adds the time since `last` into slot 8 + slot.
+__device__ __forceinline__ void tprobe(const RedArgs& a, int cta, int slot, uint64_t& last)
+{
+    if (blockIdx.x == cta && threadIdx.x == 0 && a.ptimes) {
+        const uint64_t t = globaltimer_ns();
+        a.ptimes[8 + slot] += t - last;
+        last = t;
+    }
+}
+
 __device__ __forceinline__ void combine_candidates(const RedArgs& a, int* s_p, double* s_red, int* s_redi)
 {
     // every CTA reads all CTA candidates and reduces them (first max, F:1038-1051)
@@ -845,13 +855,17 @@ __device__ bool blocked_phase(const RedArgs& a, GridBarrier& gb, PanelSh& S, uin
         const int P = (n - kb - 1 + GEMV_GROUP - 1) / GEMV_GROUP;
         for (int k = k0; k <= kb; ++k) {
             // ---- phase A: pivot, table, GEMV partials ----
+            uint64_t pa = globaltimer_ns();
             combine_candidates(a, &S.p, S.red, S.redi);
+            tprobe(a, 0, 5, pa);
             const int p = (S.p >= k + 1 && S.p <= n) ? S.p : k + 1;
             const double piv = (p == k + 1) ? M1(A, n, k + 1, k) : M1(A, n, p, k);
             if (blockIdx.x == 0 && warp == 0) {
-                if (lane == 0) a.ipiv[k - 1] = p;
+                uint64_t tb = 0;
+                if (lane == 0) { a.ipiv[k - 1] = p; tb = globaltimer_ns(); }
                 if (piv != 0.0) {
                     build_step_table(a, S, gtab, k0, kb, k, p, piv);
+                    if (lane == 0 && a.ptimes) a.ptimes[6] += globaltimer_ns() - tb;
                 } else if (lane == 0) {
                     gtab->skip = 1;
                     gtab->p = p;
@@ -860,16 +874,25 @@ __device__ bool blocked_phase(const RedArgs& a, GridBarrier& gb, PanelSh& S, uin
                     gtab->nov = 0;
                 }
             }
-            if (piv != 0.0) gemv_tasks(a, k0, kb, k, p, piv, 1);
+            tprobe(a, 0, 6, pa);
+            {
+                uint64_t pg = globaltimer_ns();
+                if (piv != 0.0) gemv_tasks(a, k0, kb, k, p, piv, 1);
+                tprobe(a, 1, 7, pg);
+            }
             if (!gb.sync()) return false;
+            tprobe(a, 0, 8, pa);
             tmark(a, 1, last);
             // ---- phase B: rows ----
+            uint64_t pb = globaltimer_ns();
             for (int e = threadIdx.x; e < (int)(sizeof(StepTab) / sizeof(int)); e += RT)
                 ((int*)&S.tab)[e] = ((volatile int*)gtab)[e];
             __syncthreads();
             const bool skip = S.tab.skip != 0;
+            tprobe(a, 1, 0, pb);
             if (!skip && warp == 0) correction_triangle(a, S, k0, k, p, P);
             __syncthreads();
+            tprobe(a, 1, 1, pb);
             double cand = 0.0;
             int candi = 0;
             for (int i = 1 + gt; i <= n; i += gsz) {
@@ -894,8 +917,11 @@ __device__ bool blocked_phase(const RedArgs& a, GridBarrier& gb, PanelSh& S, uin
                     }
                 }
             }
+            tprobe(a, 1, 2, pb);
             publish_candidate(a, cand, candi, S.red, S.redi);
+            tprobe(a, 1, 3, pb);
             if (!gb.sync()) return false;
+            tprobe(a, 1, 4, pb);
             tmark(a, 2, last);
         }
         // ---- panel end E1: interchange map, TRSM inverse, column sweeps ----
@@ -1028,7 +1054,7 @@ __device__ bool blocked_phase(const RedArgs& a, GridBarrier& gb, PanelSh& S, uin
 __global__ void __launch_bounds__(RT, 1) reduce_kernel(RedArgs a, int balance, int mode)
 {
     __shared__ PanelSh S;
-    GridBarrier gb{a.bar, a.err, a.limit_ns, 0};
+    GridBarrier gb{a.bar, a.err, a.limit_ns, 0, a.ptimes ? a.ptimes + 5 : nullptr};
     uint64_t t0 = globaltimer_ns(), last = t0;
     if (balance) {
         if (!balance_phase(a, gb)) return;

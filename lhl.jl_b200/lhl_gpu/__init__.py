@@ -69,6 +69,7 @@ def _load():
         "lhl_ws_set_barrier_limit_ns": [vp, C.c_uint64],
         "lhl_reduce": [vp, vp, i64, i32, vp],
         "lhl_ws_phase_ns": [vp, C.POINTER(C.c_uint64), vp],
+        "lhl_ws_probe_ns": [vp, C.POINTER(C.c_uint64), vp],
         "lhl_shift_create": [i64, i64, C.POINTER(vp)],
         "lhl_shift_destroy": [vp],
         "lhl_shift_get_view": [vp, C.POINTER(_ShView)],
@@ -279,8 +280,14 @@ class LHLWorkspace:
         """Device wall time of the last reduction by phase (see lhl_ws_phase_ns)."""
         buf = (C.c_uint64 * 8)()
         _check(_lib.lhl_ws_phase_ns(self._h, buf, _stream(stream)), "phase_ns")
-        names = ["balance", "pivot_gemv", "rows", "panel_swaps_trsm", "panel_gemm", "", "", "total"]
+        names = ["balance", "pivot_gemv", "rows", "panel_swaps_trsm", "panel_gemm", "barrier_wait_cta0",
+                 "step_table_cta0", "total"]
         return {nm: buf[i] for i, nm in enumerate(names) if nm}
+
+    def probe_ns(self, stream=None):
+        buf = (C.c_uint64 * 16)()
+        _check(_lib.lhl_ws_probe_ns(self._h, buf, _stream(stream)), "probe_ns")
+        return list(buf)
 
     def set_barrier_limit_ns(self, ns: int):
         _check(_lib.lhl_ws_set_barrier_limit_ns(self._h, int(ns)))
