@@ -122,6 +122,22 @@ int lhl_residual_norms(lhl_shift_t sh, const double* dJ, int64_t ldj, const doub
 int lhl_applyZ(lhl_ws_t ws, double* dX, int64_t ldx, int64_t nrhs, void* stream);
 int lhl_applyZinv(lhl_ws_t ws, double* dX, int64_t ldx, int64_t nrhs, void* stream);
 
+/* ---- reduction without device allocation ------------------------------------------ */
+/* No counterpart in the reference (which allocates its workspace in Julia).  For callers
+ * that cannot call cudaMalloc -- a host that owns a fixed device-memory budget, a Julia
+ * session whose CUDA.jl pool must stay the only allocator, code that must not trigger an
+ * allocation's device synchronization: the same reduction as lhl_reduce, with every input
+ * and output passed in (dJ n x n ld ldj; dfactors and dHt n x n with leading dimension n;
+ * dipiv n-2; dperm, diperm, dscale, discale n) and the scratch held in a fixed static device
+ * array of the library (about 2.5 MB, present on every GPU that loads it until exit).
+ * n <= LHL_NOALLOC_NMAX, else LHL_ERR_DIM.  The first call on a device resolves the array's
+ * device address (make it before any stream capture).  All calls share the array: calls
+ * whose work overlaps on the GPU race.  Allocates nothing. */
+#define LHL_NOALLOC_NMAX 1024
+int lhl_reduce_noalloc(int64_t n, const double* dJ, int64_t ldj, int balance, double* dfactors, double* dHt,
+                       int64_t* dipiv, int64_t* dperm, int64_t* diperm, double* dscale, double* discale,
+                       void* stream);
+
 /* Library build identification (for loaders that check they bound the right .so). */
 const char* lhl_version(void);
 
