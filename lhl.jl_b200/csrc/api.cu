@@ -11,7 +11,7 @@ struct lhl_ws_s {
     int64_t n;
     int precision;
     int grid;
-    double *F, *Ht, *scale, *iscale, *B0, *part, *tab, *cand_v, *buf2, *tsnap, *bsum, *bfac;
+    double *F, *Ht, *scale, *iscale, *B0, *part, *tab, *cand_v, *cand_s, *buf2, *tsnap, *bsum, *bfac;
     int64_t *ipiv, *perm, *iperm;
     int *cand_i, *bflag, *err;
     unsigned int* bar;
@@ -39,7 +39,7 @@ static cudaError_t dalloc(T** p, size_t count)
 static void ws_free(lhl_ws_t w)
 {
     if (!w) return;
-    void* ptrs[] = {w->F, w->Ht, w->scale, w->iscale, w->B0, w->part, w->tab, w->cand_v, w->buf2, w->tsnap,
+    void* ptrs[] = {w->F, w->Ht, w->scale, w->iscale, w->B0, w->part, w->tab, w->cand_v, w->cand_s, w->buf2, w->tsnap,
                     w->bsum, w->bfac, w->ipiv, w->perm, w->iperm, w->cand_i, w->bflag, w->err, w->bar,
                     w->ptimes};
     for (void* p : ptrs)
@@ -76,6 +76,7 @@ int lhl_ws_create(int64_t n, int precision, lhl_ws_t* out)
     A_(part, Pmax * n);
     A_(tab, (lhl::stepTabBytes() + 7) / 8);
     A_(cand_v, w->grid > 0 ? w->grid : 1);
+    A_(cand_s, w->grid > 0 ? w->grid : 1);
     A_(cand_i, w->grid > 0 ? w->grid : 1);
     A_(buf2, n < 500 ? nn : 1);
     A_(tsnap, (size_t)n * 17);
@@ -180,6 +181,7 @@ int lhl_reduce(lhl_ws_t ws, const double* dJ, int64_t ldj, int balance, void* st
     a.part = ws->part;
     a.tab = ws->tab;
     a.cand_v = ws->cand_v;
+    a.cand_s = ws->cand_s;
     a.cand_i = ws->cand_i;
     a.buf2 = ws->buf2;
     a.tsnap = ws->tsnap;

@@ -13,8 +13,9 @@ struct RedArgs {
     double* B0;       // n x (nb+1): pre-panel copies of the panel columns
     double* part;     // GEMV partials, Pmax x n
     double* tab;      // per-step table
-    double* cand_v;   // per-CTA pivot candidates
+    double* cand_v;   // per-CTA pivot candidates: |value|, row, signed value
     int* cand_i;
+    double* cand_s;
     double* buf2;     // unblocked path: second matrix buffer (n x n)
     double* tsnap;    // blocked path: rows 1..k0 of the panel columns before the top GEMM
     double* scale;    // balancing D

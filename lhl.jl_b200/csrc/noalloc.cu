@@ -36,7 +36,8 @@ constexpr size_t OFF_BUF2 = OFF_PART + (size_t)(NMAX / 64) * NMAX; // 499 x 499 
 constexpr size_t OFF_BSUM = OFF_BUF2 + (size_t)499 * 499;          // 2 NMAX
 constexpr size_t OFF_BFAC = OFF_BSUM + 2 * (size_t)NMAX;           // NMAX
 constexpr size_t OFF_CANDV = OFF_BFAC + (size_t)NMAX;              // NCAND
-constexpr size_t OFF_TAB = OFF_CANDV + NCAND;                      // step table (<= 512 doubles)
+constexpr size_t OFF_CANDS = OFF_CANDV + NCAND;                    // NCAND
+constexpr size_t OFF_TAB = OFF_CANDS + NCAND;                      // step table (<= 512 doubles)
 constexpr size_t OFF_INTS = OFF_TAB + 512;                         // ints: cand_i, flags, barrier
 constexpr size_t NDOUBLE = OFF_INTS + (NCAND + 64) / 2 + 1;
 
@@ -87,6 +88,7 @@ extern "C" int lhl_reduce_noalloc(int64_t n, const double* dJ, int64_t ldj, int 
     a.bsum = base + OFF_BSUM;
     a.bfac = base + OFF_BFAC;
     a.cand_v = base + OFF_CANDV;
+    a.cand_s = base + OFF_CANDS;
     a.tab = base + OFF_TAB;
     a.cand_i = ints;
     a.bflag = ints + NCAND;

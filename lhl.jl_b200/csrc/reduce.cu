@@ -352,57 +352,21 @@ __global__ void __launch_bounds__(RT) unblocked_assemble_kernel(int n, double* A
 // Blocked reduction (the reference's Float64 pointer path), nb = 16.
 // ---------------------------------------------------------------------------------
 struct PanelSh {
-    StepTab tab;
-    double LW[NBMAX + 2], LQ[NBMAX + 2], XS[NBMAX + 2];
-    int LR[NBMAX + 2];
-    int nq;
+    StepTab tab;                       // this step's table (built by warp 0 of every CTA)
+    double LW[NBMAX + 2], XS[NBMAX + 2];
+    double VAL[2 * NBMAX + 2];         // values at the special slots (see slot_map)
     double Pm[NBMAX][NBMAX];
     int srow[2 * NBMAX + 2];  // rows touched by the panel's interchanges
     int ssrc[2 * NBMAX + 2];  // source slot of each after all interchanges
     int nsr;
     double red[RW];
     int redi[RW];
-    int p;
-    double tri[NBMAX + 1][NBMAX + 1];  // A[k0+1+r, k0+c]: the panel's multipliers at rows <= k+1
-    double sval[2 * NBMAX + 2];        // values at the special rows
+    double tri[NBMAX + 1][NBMAX + 1];  // A[k0+1+r, k0+c] (r > c): the panel's multipliers, final rows
     int slist[2 * NBMAX + 2];          // swap partners beyond row k+1, first-occurrence order
+    int slot[NBMAX + 1];               // step kk's swap partner slot (-1: no interchange)
     int nsl;
-    int ipv[NBMAX];                    // ipiv[k0..k] of the panel so far
+    int ipv[NBMAX + 1];                // pivots of the panel's steps so far
 };
-
-// Rows k0+1..k+1 of the panel's multiplier columns k0..k into S.tri (one warp, parallel
-// loads), so the sequential triangles below run on shared memory only.
-__device__ __forceinline__ void load_tri(const RedArgs& a, PanelSh& S, int k0, int k)
-{
-    const int m = k - k0 + 1;
-    const int lane = threadIdx.x & 31;
-    for (int e = lane; e < m * m; e += 32) {
-        const int r = e % m, c = e / m;
-        S.tri[r][c] = M1(a.A, a.n, k0 + 1 + r, k0 + c);
-    }
-}
-
-// The panel's pivots ipiv[k0..k] (p for step k) into S.ipv, then the swap partners beyond
-// row k+1 in first-occurrence order.  One warp.
-__device__ __forceinline__ void partner_list(const RedArgs& a, PanelSh& S, int k0, int k, int p)
-{
-    const int lane = threadIdx.x & 31;
-    if (lane <= k - k0) S.ipv[lane] = (k0 + lane == k) ? p : (int)a.ipiv[k0 + lane - 1];
-    __syncwarp();
-    if (lane == 0) {
-        int np = 0;
-        for (int kk = k0; kk <= k; ++kk) {
-            const int q = S.ipv[kk - k0];
-            if (q <= k + 1) continue;
-            bool found = false;
-            for (int r = 0; r < np; ++r)
-                if (S.slist[r] == q) found = true;
-            if (!found) S.slist[np++] = q;
-        }
-        S.nsl = np;
-    }
-    __syncwarp();
-}
 
 // sum of the GEMV partials of row i in group order (F:1558-1583); loads issued in batches
 __device__ __forceinline__ double partial_sum(const RedArgs& a, int P, int i)
@@ -411,94 +375,175 @@ __device__ __forceinline__ double partial_sum(const RedArgs& a, int P, int i)
     const size_t st = (size_t)a.n;
     double s = pp[0];
     int g = 1;
-    for (; g + 7 < P; g += 8) {
-        double v[8];
+    for (; g + 15 < P; g += 16) {
+        double v[16];
 #pragma unroll
-        for (int u = 0; u < 8; ++u) v[u] = pp[(size_t)(g + u) * st];
+        for (int u = 0; u < 16; ++u) v[u] = pp[(size_t)(g + u) * st];
 #pragma unroll
-        for (int u = 0; u < 8; ++u) s = dadd(s, v[u]);
+        for (int u = 0; u < 16; ++u) s = dadd(s, v[u]);
+    }
+    for (; g + 3 < P; g += 4) {
+        double v[4];
+#pragma unroll
+        for (int u = 0; u < 4; ++u) v[u] = pp[(size_t)(g + u) * st];
+#pragma unroll
+        for (int u = 0; u < 4; ++u) s = dadd(s, v[u]);
     }
     for (; g < P; ++g) s = dadd(s, pp[(size_t)g * st]);
     return s;
 }
 
-// Phase A table, one warp of CTA 0 (F:952-980 and the pulled-column tables F:1088-1132).
-// Loads are issued in parallel into shared memory; the sequential parts (interchanges,
-// catch-up triangle) then run on shared memory.  The table is published to G.
-__device__ void build_step_table(const RedArgs& a, PanelSh& S, StepTab* G, int k0, int kb, int k, int p, double piv)
+// Every warp reads all CTA candidates and reduces them (first max, F:1038-1051); returns p
+// and the signed pivot value A[p, k] published with it.
+__device__ __forceinline__ int warp_combine(const RedArgs& a, double& pivs)
+{
+    const int lane = threadIdx.x & 31;
+    double v = 0.0, sv = 0.0;
+    int vi = 0;
+    for (int c = lane; c < (int)gridDim.x; c += 32) {
+        const int ci = ((volatile int*)a.cand_i)[c];
+        const double cv = ((volatile double*)a.cand_v)[c];
+        const double cs = ((volatile double*)a.cand_s)[c];
+        if (ci != 0 && (vi == 0 || cv > v || (cv == v && ci < vi))) { v = cv; vi = ci; sv = cs; }
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        const double b = __shfl_xor_sync(0xffffffffu, v, o);
+        const int ib = __shfl_xor_sync(0xffffffffu, vi, o);
+        const double sb = __shfl_xor_sync(0xffffffffu, sv, o);
+        if (ib != 0 && (vi == 0 || b > v || (b == v && ib < vi))) { v = b; vi = ib; sv = sb; }
+    }
+    pivs = sv;
+    return vi;
+}
+
+// CTA-local first-max candidate (|value|, row, signed value) published to slot blockIdx.x.
+__device__ __forceinline__ void publish_cand(const RedArgs& a, double v, int vi, double sv, PanelSh& S)
+{
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        const double b = __shfl_xor_sync(0xffffffffu, v, o);
+        const int ib = __shfl_xor_sync(0xffffffffu, vi, o);
+        const double sb = __shfl_xor_sync(0xffffffffu, sv, o);
+        if (ib != 0 && (vi == 0 || b > v || (b == v && ib < vi))) { v = b; vi = ib; sv = sb; }
+    }
+    const int t = threadIdx.x;
+    if ((t & 31) == 0) {
+        S.red[t >> 5] = v;
+        S.redi[t >> 5] = vi;
+        S.VAL[t >> 5] = sv;  // VAL is free at this point of the step
+    }
+    __syncthreads();
+    if (t == 0) {
+        double bv = 0.0, bs = 0.0;
+        int bi = 0;
+        for (int w = 0; w < RW; ++w) {
+            const int ib = S.redi[w];
+            if (ib != 0 && (bi == 0 || S.red[w] > bv || (S.red[w] == bv && ib < bi))) {
+                bv = S.red[w];
+                bi = ib;
+                bs = S.VAL[w];
+            }
+        }
+        a.cand_v[blockIdx.x] = bv;
+        a.cand_i[blockIdx.x] = bi;
+        a.cand_s[blockIdx.x] = bs;
+    }
+    __syncthreads();
+}
+
+// Slot map of step k (one warp).  Slots 0..m-1 are rows k0+1..k+1; slots m.. are the swap
+// partners beyond row k+1 of steps k0..k in first-occurrence order.  slot[kk-k0] is the
+// slot step kk's row kk+1 exchanges with (-1: no interchange).  Both the pulled column's
+// table (F:1104-1124) and the correction's special sums (F:1236-1259) move on these slots.
+__device__ __forceinline__ void slot_map(PanelSh& S, int k0, int k, int p)
+{
+    const int lane = threadIdx.x & 31;
+    const int m = k - k0 + 1;
+    const bool act = lane < m;
+    const int q = act ? ((lane == m - 1) ? p : S.ipv[lane]) : 0;
+    const bool partner = act && q > k + 1;
+    const unsigned am = __ballot_sync(0xffffffffu, act);
+    const unsigned same = __match_any_sync(0xffffffffu, partner ? q : -1 - lane);
+    const int first = __ffs(same & am) - 1;                     // first lane with this q
+    const bool isfirst = partner && first == lane;
+    const unsigned fm = __ballot_sync(0xffffffffu, isfirst);
+    const int idx_first = __popc(fm & ((1u << lane) - 1u));   // partner index if first
+    const int idx = __shfl_sync(0xffffffffu, idx_first, partner ? first : lane);
+    if (isfirst) S.slist[idx_first] = q;
+    if (act) S.slot[lane] = (q == k0 + lane + 1) ? -1 : (q <= k + 1 ? q - k0 - 1 : m + idx);
+    if (lane == 0) S.nsl = __popc(fm);
+    __syncwarp();
+}
+
+// Apply the interchanges of steps k0..k to a slot vector (one lane; shared memory only).
+__device__ __forceinline__ void slot_swaps(PanelSh& S, double* V, int k0, int k)
+{
+    for (int kk = 0; kk <= k - k0; ++kk) {
+        const int s = S.slot[kk];
+        if (s < 0) continue;
+        const double t = V[kk];
+        V[kk] = V[s];
+        V[s] = t;
+    }
+}
+
+// Phase A step table, warp 0 of every CTA (F:952-980; pulled tables F:1088-1132).
+// r1 / vsrc were prefetched before the pivot was known.
+__device__ void step_table(const RedArgs& a, PanelSh& S, int k0, int kb, int k, int p, double piv, double r1,
+                           double vsrc)
 {
     const int n = a.n;
     const double* A = a.A;
     const int lane = threadIdx.x & 31;
     StepTab& T = S.tab;
-    for (int j = k0 + lane; j <= kb + 1; j += 32) {
-        T.R1[j - k0] = M1(A, n, k + 1, j);
-        T.RP[j - k0] = M1(A, n, p, j);
-    }
-    for (int j = k + 2 + lane; j <= kb + 1; j += 32) {
-        const double v = (j == p) ? M1(A, n, k + 1, k) : M1(A, n, j, k);
-        T.VJ[j - k0] = v / piv;
-    }
-    __syncwarp();  // R1 / RP / VJ are read by other lanes below
-    const int pulled = p > kb + 1;
+    const int w = kb + 2 - k0;  // panel columns k0..kb+1
     const int m = k - k0 + 1;
-    int nov = 0;
+    const int pulled = p > kb + 1;
+    slot_map(S, k0, k, p);
+    // one batch of loads: row p of the panel, and the pulled column at the slot rows
+    const double rp = (lane < w) ? M1(A, n, p, k0 + lane) : 0.0;
+    double ov = 0.0;
     if (pulled) {
-        if (lane < m) {
-            T.OV[lane] = M1(A, n, k0 + 1 + lane, p);
-            T.OR[lane] = k0 + 1 + lane;
-        }
-        load_tri(a, S, k0, k);
-        partner_list(a, S, k0, k, p);
-        if (lane < S.nsl) S.sval[lane] = M1(A, n, S.slist[lane], p);
+        if (lane < m) ov = M1(A, n, k0 + 1 + lane, p);
+        else if (lane < m + S.nsl) ov = M1(A, n, S.slist[lane - m], p);
+    }
+    if (lane < w) {
+        T.R1[lane] = r1;
+        T.RP[lane] = rp;
+    }
+    {
+        const int j = k + 2 + lane;
+        const double r1k = __shfl_sync(0xffffffffu, r1, k - k0);  // A[k+1, k], the pre-swap row k+1
+        if (j <= kb + 1) T.VJ[j - k0] = ((j == p) ? r1k : vsrc) / piv;
+    }
+    if (pulled) {
+        S.VAL[lane] = ov;
         __syncwarp();
-        if (lane == 0) {
-            nov = m;
-            for (int kk = k0; kk <= k; ++kk) {
-                const int q = S.ipv[kk - k0];
-                if (q == kk + 1) continue;
-                int s = -1;
-                if (q <= k + 1) {
-                    s = q - k0 - 1;
-                } else {
-                    for (int r = m; r < nov; ++r)
-                        if (T.OR[r] == q) { s = r; break; }
-                    if (s < 0) {
-                        s = nov++;
-                        int idx = 0;
-                        for (int r = 0; r < S.nsl; ++r)
-                            if (S.slist[r] == q) idx = r;
-                        T.OV[s] = S.sval[idx];
-                        T.OR[s] = q;
-                    }
-                }
-                const double t = T.OV[kk - k0];
-                T.OV[kk - k0] = T.OV[s];
-                T.OV[s] = t;
-            }
-            T.nov = nov;
-        }
+        if (lane == 0) slot_swaps(S, S.VAL, k0, k);
         __syncwarp();
         // catch-up of rows k0+1..k+1 by the left transforms k0..k-1, lanes = rows
-        double ov = (lane < m) ? T.OV[lane] : 0.0;
+        double o = (lane < m) ? S.VAL[lane] : 0.0;
         const int row = k0 + 1 + lane;
         for (int kk = k0; kk <= k - 1; ++kk) {
-            const double x = __shfl_sync(0xffffffffu, ov, kk - k0);
+            const double x = __shfl_sync(0xffffffffu, o, kk - k0);
             if (lane == 0) T.CX[kk - k0] = x;
             if (x != 0.0 && lane < m && row >= kk + 2) {
                 const double aik = (row == k + 1) ? T.RP[kk - k0] : S.tri[lane][kk - k0];
-                ov = dsub(ov, dmul(aik, x));
+                o = dsub(o, dmul(aik, x));
             }
         }
-        if (lane < m) T.OV[lane] = ov;
+        if (lane < m) S.VAL[lane] = o;
         __syncwarp();
+        if (lane < m + S.nsl) T.OV[lane] = S.VAL[lane];
     }
+    __syncwarp();
     if (lane == 0) {
         T.p = p;
         T.piv = piv;
         T.pulled = pulled;
         T.skip = 0;
-        if (!pulled) T.nov = 0;
+        T.nov = pulled ? m + S.nsl : 0;
         for (int j = k + 1; j <= kb + 1; ++j) T.PJ[j - k - 1] = T.RP[j - k0];
         if (pulled) T.PJ[0] = T.OV[k - k0];
         else if (p != k + 1) {
@@ -506,12 +551,14 @@ __device__ void build_step_table(const RedArgs& a, PanelSh& S, StepTab* G, int k
             T.PJ[p - k - 1] = T.RP[k + 1 - k0];
         }
     }
+    // row k+1 is final after this step: its multipliers (pre-swap row p) join the triangle
+    if (lane < m - 1) S.tri[m - 1][lane] = T.RP[lane];
+    if (lane == 0) S.ipv[m - 1] = p;
     __syncwarp();
-    for (int e = lane; e < (int)(sizeof(StepTab) / sizeof(int)); e += 32) ((int*)G)[e] = ((const int*)&T)[e];
 }
 
 // GEMV partials of phase A (F:1496-1553): task = (group g, 32-row tile), lane = row.
-__device__ void gemv_tasks(const RedArgs& a, int k0, int kb, int k, int p, double piv, int skip_warp)
+__device__ void gemv_tasks(const RedArgs& a, int k0, int kb, int k, int p, double piv)
 {
     const int n = a.n;
     const double* A = a.A;
@@ -519,13 +566,12 @@ __device__ void gemv_tasks(const RedArgs& a, int k0, int kb, int k, int p, doubl
     const int P = (n - c0 + 1 + GEMV_GROUP - 1) / GEMV_GROUP;
     const int ntiles = (n - k0 + 31) / 32;
     const int lane = threadIdx.x & 31;
-    const int gw = blockIdx.x * RW + (threadIdx.x >> 5);
-    const int nw = gridDim.x * RW;
+    const int gw = blockIdx.x * (RW - 1) + (threadIdx.x >> 5) - 1;  // warps 1..RW-1 of every CTA
+    const int nw = gridDim.x * (RW - 1);
     const bool pulled = p > kb + 1;
     const double* sub = a.B0 + (size_t)(k - k0) * n;  // pre-panel copy of column k+1
     const int ntask = P * ntiles;
-    if (gw < skip_warp) return;
-    for (int task = gw - skip_warp; task < ntask; task += nw - skip_warp) {
+    for (int task = gw; task < ntask; task += nw) {
         const int g = task / ntiles, tile = task % ntiles;
         const int ga = c0 + g * GEMV_GROUP;
         const int gb = min(ga + GEMV_GROUP - 1, n);
@@ -584,54 +630,23 @@ __device__ void gemv_tasks(const RedArgs& a, int k0, int kb, int k, int p, doubl
     }
 }
 
-// The correction triangle of phase B, computed redundantly by every CTA's warp 0
-// (F:1232-1269): LW (rows k0+1..k+1), LQ (swap partners beyond k+1), XS (the x's).
-// All special-row sums are formed in parallel first; the interchange pass and the
-// triangle then run on shared memory.
-__device__ void correction_triangle(const RedArgs& a, PanelSh& S, int k0, int k, int p, int P)
+// The correction triangle of phase B, warp 0 of every CTA with rows to finish (F:1232-1269):
+// the GEMV sums at the special slots, the interchanges of steps k0..k on them, then the
+// x's: LW (rows k0+1..k+1), VAL[m..] (the partners' values), XS.
+__device__ void correction_triangle(const RedArgs& a, PanelSh& S, int k0, int k, int P)
 {
     const int lane = threadIdx.x & 31;
     const int m = k - k0 + 1;
-    load_tri(a, S, k0, k);
-    partner_list(a, S, k0, k, p);
-    for (int idx = lane; idx < m + S.nsl; idx += 32) {
+    const int ns = m + S.nsl;
+    for (int idx = lane; idx < ns; idx += 32) {
         const int row = (idx < m) ? k0 + 1 + idx : S.slist[idx - m];
-        const double v = partial_sum(a, P, row);
-        if (idx < m) S.LW[idx] = v;
-        else S.sval[idx - m] = v;
+        S.VAL[idx] = partial_sum(a, P, row);
     }
     __syncwarp();
-    if (lane == 0) {
-        int nq = 0;
-        for (int kk = k0; kk <= k; ++kk) {
-            const int q = S.ipv[kk - k0];
-            if (q == kk + 1) continue;
-            if (q <= k + 1) {
-                const double t = S.LW[kk - k0];
-                S.LW[kk - k0] = S.LW[q - k0 - 1];
-                S.LW[q - k0 - 1] = t;
-            } else {
-                int s = -1;
-                for (int r = 0; r < nq; ++r)
-                    if (S.LR[r] == q) { s = r; break; }
-                if (s < 0) {
-                    s = nq++;
-                    int idx = 0;
-                    for (int r = 0; r < S.nsl; ++r)
-                        if (S.slist[r] == q) idx = r;
-                    S.LQ[s] = S.sval[idx];
-                    S.LR[s] = q;
-                }
-                const double t = S.LW[kk - k0];
-                S.LW[kk - k0] = S.LQ[s];
-                S.LQ[s] = t;
-            }
-        }
-        S.nq = nq;
-    }
+    if (lane == 0) slot_swaps(S, S.VAL, k0, k);
     __syncwarp();
     // x triangle: lanes hold rows k0+1+lane, sequential over kk
-    double lw = (lane < m) ? S.LW[lane] : 0.0;
+    double lw = (lane < m) ? S.VAL[lane] : 0.0;
     const int row = k0 + 1 + lane;
     for (int kk = k0; kk <= k; ++kk) {
         const double x = __shfl_sync(0xffffffffu, lw, kk - k0);
@@ -647,8 +662,8 @@ __device__ void correction_triangle(const RedArgs& a, PanelSh& S, int k0, int k,
 
 // Phase B row work for row i in k0+1..n (F:1166-1296); returns |A[i,k+1]| candidate.
 template <int NB>
-__device__ void panel_row(const RedArgs& a, const PanelSh& S, int k0, int kb, int k, int P, int i, double& cand,
-                          int& candi)
+__device__ void panel_row(const RedArgs& a, const PanelSh& S, int k0, int kb, int k, int P, int i, double wsum,
+                          double& cand, int& candi, double& cands)
 {
     const int n = a.n;
     double* A = a.A;
@@ -660,7 +675,7 @@ __device__ void panel_row(const RedArgs& a, const PanelSh& S, int k0, int kb, in
     for (int c = 0; c < NB + 2; ++c) v[c] = (c < w) ? M1(A, n, i, k0 + c) : 0.0;
     const int ck = k - k0, ck1 = k + 1 - k0;
     if (T.skip) {
-        if (i >= k + 2) { cand = fabs(v[ck1]); candi = i; }
+        if (i >= k + 2) { cand = fabs(v[ck1]); candi = i; cands = v[ck1]; }
         return;
     }
     const double piv = T.piv;
@@ -694,8 +709,12 @@ __device__ void panel_row(const RedArgs& a, const PanelSh& S, int k0, int kb, in
     }
     // (2) the pulled column's tables and catch-up (F:1193-1205)
     if (T.pulled) {
-        for (int r = 0; r < T.nov; ++r)
-            if (T.OR[r] == i) v[ck1] = T.OV[r];
+        int sl = -1;
+        if (i >= k0 + 1 && i <= k + 1) sl = i - k0 - 1;
+        else
+            for (int r = 0; r < S.nsl; ++r)
+                if (S.slist[r] == i) sl = k - k0 + 1 + r;
+        if (sl >= 0) v[ck1] = T.OV[sl];
         if (i >= k + 2) {
 #pragma unroll
             for (int c = 0; c < NB; ++c) {
@@ -730,11 +749,10 @@ __device__ void panel_row(const RedArgs& a, const PanelSh& S, int k0, int kb, in
     if (i <= k + 1) {
         v[ck1] = dadd(v[ck1], S.LW[i - k0 - 1]);
     } else {
-        double wv;
         int r = -1;
-        for (int q = 0; q < S.nq; ++q)
-            if (S.LR[q] == i) r = q;
-        wv = (r >= 0) ? S.LQ[r] : partial_sum(a, P, i);
+        for (int q = 0; q < S.nsl; ++q)
+            if (S.slist[q] == i) r = q;
+        double wv = (r >= 0) ? S.VAL[k - k0 + 1 + r] : wsum;
 #pragma unroll
         for (int c = 0; c < NB; ++c) {
             if (c <= ck) {
@@ -745,6 +763,7 @@ __device__ void panel_row(const RedArgs& a, const PanelSh& S, int k0, int kb, in
         v[ck1] = dadd(v[ck1], wv);
         cand = fabs(v[ck1]);
         candi = i;
+        cands = v[ck1];
     }
 #pragma unroll
     for (int c = 0; c < NB + 2; ++c)
@@ -760,8 +779,6 @@ __device__ void panel_row(const RedArgs& a, const PanelSh& S, int k0, int kb, in
 // pre-sweep value it receives after the whole sequence (F:1344-1379, F:1395-1415).
 __device__ void build_swap_map(const RedArgs& a, PanelSh& S, int k0, int kb)
 {
-    if ((int)threadIdx.x <= kb - k0) S.ipv[threadIdx.x] = (int)a.ipiv[k0 + threadIdx.x - 1];
-    __syncthreads();
     if (threadIdx.x == 0) {
         int nsr = 0;
         int val[2 * NBMAX + 2];
@@ -789,9 +806,7 @@ __device__ void build_swap_map(const RedArgs& a, PanelSh& S, int k0, int kb)
 // P = M^-1 - I of the panel's multipliers (F:1944-1955), into shared memory.
 __device__ void build_trsm_inverse(const RedArgs& a, PanelSh& S, int k0, int kb)
 {
-    const int nbp = kb - k0 + 1;
-    if (threadIdx.x < 32) load_tri(a, S, k0, kb);  // tri[r-1][s-1] = M[r,s] = A[k0+r, k0+s-1]
-    __syncthreads();
+    const int nbp = kb - k0 + 1;   // S.tri[r-1][s-1] = M[r,s] = A[k0+r, k0+s-1], r > s
     const int q = threadIdx.x + 1;  // column q of P
     if (threadIdx.x < nbp) {
         for (int r = 1; r <= nbp; ++r) {
@@ -834,14 +849,16 @@ __device__ bool blocked_phase(const RedArgs& a, GridBarrier& gb, PanelSh& S, uin
     const int gt = blockIdx.x * RT + threadIdx.x;
     const int gsz = gridDim.x * RT;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    StepTab* gtab = (StepTab*)a.tab;
 
     // setup: candidates of column 1, B0 of the first panel
     {
-        double v = 0.0;
+        double v = 0.0, sv = 0.0;
         int vi = 0;
-        for (int i = 2 + gt; i <= n; i += gsz) argmax_combine(v, vi, fabs(M1(A, n, i, 1)), i);
-        publish_candidate(a, v, vi, S.red, S.redi);
+        for (int i = 2 + gt; i <= n; i += gsz) {
+            const double x = M1(A, n, i, 1);
+            if (vi == 0 || fabs(x) > v) { v = fabs(x); vi = i; sv = x; }
+        }
+        publish_cand(a, v, vi, sv, S);
         const int kb = min(nb, n - 2);
         for (size_t e = gt; e < (size_t)n * (kb + 1 - 1); e += gsz) {
             const int i = (int)(e % n), c = (int)(e / n);
@@ -854,30 +871,40 @@ __device__ bool blocked_phase(const RedArgs& a, GridBarrier& gb, PanelSh& S, uin
         const int kb = min(k0 + nb - 1, n - 2);
         const int P = (n - kb - 1 + GEMV_GROUP - 1) / GEMV_GROUP;
         for (int k = k0; k <= kb; ++k) {
-            // ---- phase A: pivot, table, GEMV partials ----
+            // ---- phase A: pivot (every warp), step table (warp 0 of every CTA), GEMV ----
             uint64_t pa = globaltimer_ns();
-            combine_candidates(a, &S.p, S.red, S.redi);
-            tprobe(a, 0, 5, pa);
-            const int p = (S.p >= k + 1 && S.p <= n) ? S.p : k + 1;
-            const double piv = (p == k + 1) ? M1(A, n, k + 1, k) : M1(A, n, p, k);
-            if (blockIdx.x == 0 && warp == 0) {
-                uint64_t tb = 0;
-                if (lane == 0) { a.ipiv[k - 1] = p; tb = globaltimer_ns(); }
-                if (piv != 0.0) {
-                    build_step_table(a, S, gtab, k0, kb, k, p, piv);
-                    if (lane == 0 && a.ptimes) a.ptimes[6] += globaltimer_ns() - tb;
-                } else if (lane == 0) {
-                    gtab->skip = 1;
-                    gtab->p = p;
-                    gtab->piv = piv;
-                    gtab->pulled = 0;
-                    gtab->nov = 0;
-                }
+            double r1 = 0.0, vsrc = 0.0;
+            if (warp == 0) {  // prefetch what the table needs before the pivot is known
+                if (lane < kb + 2 - k0) r1 = M1(A, n, k + 1, k0 + lane);
+                if (k + 2 + lane <= kb + 1) vsrc = M1(A, n, k + 2 + lane, k);
             }
-            tprobe(a, 0, 6, pa);
-            {
+            double piv = 0.0;
+            int p = warp_combine(a, piv);
+            if (p < k + 1 || p > n) {  // no candidate (a zero column): no interchange
+                p = k + 1;
+                piv = M1(A, n, k + 1, k);
+            }
+            tprobe(a, 0, 5, pa);
+            if (warp == 0) {
+                if (blockIdx.x == 0 && lane == 0) a.ipiv[k - 1] = p;
+                if (piv != 0.0) {
+                    step_table(a, S, k0, kb, k, p, piv, r1, vsrc);
+                } else {
+                    if (lane == 0) {
+                        S.tab.skip = 1;
+                        S.tab.p = p;
+                        S.tab.piv = piv;
+                        S.tab.pulled = 0;
+                        S.tab.nov = 0;
+                        S.ipv[k - k0] = p;
+                    }
+                    if (lane < k - k0) S.tri[k - k0][lane] = r1;  // p == k+1: row k+1 is final as is
+                    __syncwarp();
+                }
+                tprobe(a, 0, 6, pa);
+            } else {
                 uint64_t pg = globaltimer_ns();
-                if (piv != 0.0) gemv_tasks(a, k0, kb, k, p, piv, 1);
+                if (piv != 0.0) gemv_tasks(a, k0, kb, k, p, piv);
                 tprobe(a, 1, 7, pg);
             }
             if (!gb.sync()) return false;
@@ -885,40 +912,39 @@ __device__ bool blocked_phase(const RedArgs& a, GridBarrier& gb, PanelSh& S, uin
             tmark(a, 1, last);
             // ---- phase B: rows ----
             uint64_t pb = globaltimer_ns();
-            for (int e = threadIdx.x; e < (int)(sizeof(StepTab) / sizeof(int)); e += RT)
-                ((int*)&S.tab)[e] = ((volatile int*)gtab)[e];
-            __syncthreads();
             const bool skip = S.tab.skip != 0;
+            const int i = 1 + gt;  // this thread's row
+            const bool cta_rows = (blockIdx.x + 1) * RT >= k0 + 1 && blockIdx.x * RT + 1 <= n;
             tprobe(a, 1, 0, pb);
-            if (!skip && warp == 0) correction_triangle(a, S, k0, k, p, P);
+            double wsum = 0.0;
+            if (warp == 0 && !skip && cta_rows) correction_triangle(a, S, k0, k, P);
+            if (!skip && i >= k + 2 && i <= n) wsum = partial_sum(a, P, i);
             __syncthreads();
             tprobe(a, 1, 1, pb);
-            double cand = 0.0;
+            double cand = 0.0, cands = 0.0;
             int candi = 0;
-            for (int i = 1 + gt; i <= n; i += gsz) {
-                if (i >= k0 + 1) {
-                    panel_row<NB>(a, S, k0, kb, k, P, i, cand, candi);
-                } else if (!skip && p != k + 1) {
-                    // top rows: the column part of the interchange (F:1135-1161)
-                    if (p <= kb + 1) {
-                        double* x1 = A + (size_t)k * n + (i - 1);
-                        double* xp = A + (size_t)(p - 1) * n + (i - 1);
-                        double t = *x1; *x1 = *xp; *xp = t;
-                        double* b1 = a.B0 + (size_t)(k - k0) * n + (i - 1);
-                        double* bp = a.B0 + (size_t)(p - k0 - 1) * n + (i - 1);
-                        t = *b1; *b1 = *bp; *bp = t;
-                    } else {
-                        double* ap = A + (size_t)(p - 1) * n + (i - 1);
-                        double* b1 = a.B0 + (size_t)(k - k0) * n + (i - 1);
-                        const double t = *ap;
-                        *ap = *b1;
-                        *b1 = t;
-                        A[(size_t)k * n + (i - 1)] = t;
-                    }
+            if (i >= k0 + 1 && i <= n) {
+                panel_row<NB>(a, S, k0, kb, k, P, i, wsum, cand, candi, cands);
+            } else if (i <= k0 && !skip && p != k + 1) {
+                // top rows: the column part of the interchange (F:1135-1161)
+                if (p <= kb + 1) {
+                    double* x1 = A + (size_t)k * n + (i - 1);
+                    double* xp = A + (size_t)(p - 1) * n + (i - 1);
+                    double t = *x1; *x1 = *xp; *xp = t;
+                    double* b1 = a.B0 + (size_t)(k - k0) * n + (i - 1);
+                    double* bp = a.B0 + (size_t)(p - k0 - 1) * n + (i - 1);
+                    t = *b1; *b1 = *bp; *bp = t;
+                } else {
+                    double* ap = A + (size_t)(p - 1) * n + (i - 1);
+                    double* b1 = a.B0 + (size_t)(k - k0) * n + (i - 1);
+                    const double t = *ap;
+                    *ap = *b1;
+                    *b1 = t;
+                    A[(size_t)k * n + (i - 1)] = t;
                 }
             }
             tprobe(a, 1, 2, pb);
-            publish_candidate(a, cand, candi, S.red, S.redi);
+            publish_cand(a, cand, candi, cands, S);
             tprobe(a, 1, 3, pb);
             if (!gb.sync()) return false;
             tprobe(a, 1, 4, pb);
