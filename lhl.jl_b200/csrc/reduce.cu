@@ -361,6 +361,7 @@ struct PanelSh {
     int nsr;
     double red[RW];
     int redi[RW];
+    double reds[RW];                   // signed values of the warps' candidates
     double tri[NBMAX + 1][NBMAX + 1];  // A[k0+1+r, k0+c] (r > c): the panel's multipliers, final rows
     int slist[2 * NBMAX + 2];          // swap partners beyond row k+1, first-occurrence order
     int slot[NBMAX + 1];               // step kk's swap partner slot (-1: no interchange)
@@ -431,7 +432,7 @@ __device__ __forceinline__ void publish_cand(const RedArgs& a, double v, int vi,
     if ((t & 31) == 0) {
         S.red[t >> 5] = v;
         S.redi[t >> 5] = vi;
-        S.VAL[t >> 5] = sv;  // VAL is free at this point of the step
+        S.reds[t >> 5] = sv;
     }
     __syncthreads();
     if (t == 0) {
@@ -442,7 +443,7 @@ __device__ __forceinline__ void publish_cand(const RedArgs& a, double v, int vi,
             if (ib != 0 && (bi == 0 || S.red[w] > bv || (S.red[w] == bv && ib < bi))) {
                 bv = S.red[w];
                 bi = ib;
-                bs = S.VAL[w];
+                bs = S.reds[w];
             }
         }
         a.cand_v[blockIdx.x] = bv;
