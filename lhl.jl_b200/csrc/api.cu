@@ -194,6 +194,7 @@ int lhl_reduce(lhl_ws_t ws, const double* dJ, int64_t ldj, int balance, void* st
     a.err = ws->err;
     a.limit_ns = ws->limit_ns;
     a.ptimes = ws->ptimes;
+    a.use_tma = (n % 2 == 0) ? 1 : 0;
     const int mode = n <= 2 ? 0 : (n < 500 ? 1 : 2);
     if (!balance) {
         // scale = iscale = 1

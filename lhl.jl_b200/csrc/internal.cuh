@@ -1,5 +1,8 @@
 // internal.cuh -- argument blocks and launchers shared by the .cu files of liblhl_gpu.
 #pragma once
+#include <cuda.h>
+#include <string.h>
+
 #include "common.cuh"
 
 namespace lhl {
@@ -27,6 +30,7 @@ struct RedArgs {
     int* err;
     unsigned long long limit_ns;
     unsigned long long* ptimes;  // per-phase wall time (ns) accumulated by CTA 0, 8 slots
+    int use_tma;                 // GEMV through TMA tiles (needs an even n >= 64)
 };
 
 // One solve launch (see solve.cu).

@@ -99,6 +99,7 @@ extern "C" int lhl_reduce_noalloc(int64_t n, const double* dJ, int64_t ldj, int 
     a.limit_ns = 2000000000ull;
     a.ptimes = nullptr;
     if (lhl::reduce_grid_size() > NCAND || lhl::stepTabBytes() > 512 * sizeof(double)) return LHL_ERR_CUDA;
+    a.use_tma = (n % 2 == 0) ? 1 : 0;
     const int mode = n <= 2 ? 0 : (n < 500 ? 1 : 2);
     if (!balance) {
         e = lhl::launch_fill_ones(dscale, discale, (int)n, st);

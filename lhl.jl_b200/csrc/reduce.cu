@@ -15,12 +15,16 @@
 // column-major with leading dimension n.
 #include "internal.cuh"
 
+#include <cudaTypedefs.h>
+
 namespace lhl {
 
 constexpr int RT = 256;        // threads per CTA of the reduction kernels
 constexpr int RW = RT / 32;    // warps per CTA
 constexpr int NBMAX = 16;      // panel width nb (F:706)
 constexpr int GEMV_GROUP = 64; // _LHL_GEMV_GROUP (F:1451)
+constexpr int TMA_SLOTS = 6;   // 64x64 FP64 tiles in flight per CTA in the GEMV phase
+constexpr int TILE_BYTES = 64 * 64 * 8;
 
 
 // ---------------------------------------------------------------------------------
@@ -631,6 +635,94 @@ __device__ void gemv_tasks(const RedArgs& a, int k0, int kb, int k, int p, doubl
     }
 }
 
+// GEMV partials of phase A through TMA: the trailing block is streamed in 64x64 FP64
+// tiles (64 rows x one 64-column group), TMA_SLOTS tiles in flight per CTA, completion on
+// one mbarrier per slot.  Two warps consume a tile (32 rows each); the arithmetic per row
+// is the reference's group order (F:1496-1553), read from shared memory.  The pulled
+// column (p > kb+1) is taken from its pre-panel copy in B0, as the reference reads it
+// from pSub (F:1492).  Warp 0 only joins the per-round CTA barriers.
+__device__ void gemv_tma(const RedArgs& a, const void* tmA, uint64_t* bars, double* tiles, int k0, int kb, int k,
+                         int p, double piv, uint32_t& ph)
+{
+    const int n = a.n;
+    const double* A = a.A;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int P = (n - kb - 1 + GEMV_GROUP - 1) / GEMV_GROUP;
+    const int r0t = k0 / 64;  // first 64-row tile holding 0-based row k0 (= row k0+1)
+    const int RTn = (n + 63) / 64 - r0t;
+    const int ntask = RTn * P;
+    const int G = gridDim.x, bid = blockIdx.x;
+    const int cnt = (ntask > bid) ? (ntask - bid - 1) / G + 1 : 0;
+    const bool pulled = p > kb + 1;
+    const double* sub = a.B0 + (size_t)(k - k0) * n;
+    for (int base = 0; base < cnt; base += TMA_SLOTS) {
+        const int nr = min(TMA_SLOTS, cnt - base);
+        if (threadIdx.x == 32) {
+            fence_proxy_async_global();
+            fence_proxy_async_shared();
+            for (int s = 0; s < nr; ++s) {
+                const int t = bid + (base + s) * G;
+                const int g = t / RTn, rt = r0t + t % RTn;
+                mbar_expect_tx(&bars[s], TILE_BYTES);
+                tma_load_2d(tiles + (size_t)s * 4096, tmA, rt * 64, kb + 1 + 64 * g, &bars[s]);
+            }
+        }
+        if (warp >= 1) {
+            for (int u = warp - 1; u < 2 * nr; u += RW - 1) {
+                const int s = u >> 1, half = u & 1;
+                const int t = bid + (base + s) * G;
+                const int g = t / RTn, rt = r0t + t % RTn;
+                const int ga = kb + 2 + 64 * g;
+                const int gb = min(ga + 63, n);
+                const int w = gb - ga + 1;
+                double l0 = 0.0, l1 = 0.0;
+                {
+                    const int j0 = ga + lane, j1 = ga + 32 + lane;
+                    if (j0 <= gb) l0 = ((j0 == p) ? M1(A, n, k + 1, k) : M1(A, n, j0, k)) / piv;
+                    if (j1 <= gb) l1 = ((j1 == p) ? M1(A, n, k + 1, k) : M1(A, n, j1, k)) / piv;
+                }
+                const int r = half * 32 + lane;       // row within the tile
+                const int i = rt * 64 + r + 1;         // 1-based row
+                const bool act = i >= k0 + 1 && i <= n;
+                const bool psub = pulled && p >= ga && p <= gb;
+                const double bval = (psub && act) ? sub[i - 1] : 0.0;
+                if (!mbar_wait(&bars[s], (ph >> s) & 1u, 1u << 22)) atomicCAS(a.err, 0, (int)LHL_ERR_TIMEOUT);
+                const double* tl = tiles + (size_t)s * 4096 + r;
+                auto TV = [&](int j) -> double { return (psub && j == p) ? bval : tl[(j - ga) * 64]; };
+                auto LV = [&](int j) -> double {
+                    const int m = j - ga;
+                    const double v0 = __shfl_sync(0xffffffffu, l0, m & 31);
+                    const double v1 = __shfl_sync(0xffffffffu, l1, m & 31);
+                    return m < 32 ? v0 : v1;
+                };
+                const int nquad = w >> 2;
+                double acc = 0.0;
+                bool have = false;
+                for (int q = 0; q < nquad; ++q) {
+                    const int j = ga + 4 * q;
+                    const double q1 = LV(j), q2 = LV(j + 1), q3 = LV(j + 2), q4 = LV(j + 3);
+                    const double quad = dadd(dadd(dmul(q1, TV(j)), dmul(q2, TV(j + 1))),
+                                             dadd(dmul(q3, TV(j + 2)), dmul(q4, TV(j + 3))));
+                    acc = have ? dadd(acc, quad) : quad;
+                    have = true;
+                }
+                for (int j = ga + 4 * nquad; j <= gb; ++j) {
+                    const double lj = LV(j);
+                    if (!have) {
+                        acc = dmul(lj, TV(j));
+                        have = true;
+                    } else if (lj != 0.0) {
+                        acc = dadd(acc, dmul(lj, TV(j)));
+                    }
+                }
+                if (act) a.part[(size_t)g * n + (i - 1)] = acc;
+            }
+        }
+        __syncthreads();
+        ph ^= (1u << nr) - 1u;
+    }
+}
+
 // The correction triangle of phase B, warp 0 of every CTA with rows to finish (F:1232-1269):
 // the GEMV sums at the special slots, the interchanges of steps k0..k on them, then the
 // x's: LW (rows k0+1..k+1), VAL[m..] (the partners' values), XS.
@@ -842,8 +934,10 @@ __device__ void column_end(const RedArgs& a, const PanelSh& S, int k0, int kb, i
 }
 
 template <int NB>
-__device__ bool blocked_phase(const RedArgs& a, GridBarrier& gb, PanelSh& S, uint64_t& last)
+__device__ bool blocked_phase(const RedArgs& a, GridBarrier& gb, PanelSh& S, uint64_t& last, const void* tmA,
+                              uint64_t* bars, double* tiles)
 {
+    uint32_t ph = 0;  // per-slot mbarrier phase parity (identical in every thread)
     const int n = a.n;
     const int nb = NB;
     double* A = a.A;
@@ -903,9 +997,14 @@ __device__ bool blocked_phase(const RedArgs& a, GridBarrier& gb, PanelSh& S, uin
                     __syncwarp();
                 }
                 tprobe(a, 0, 6, pa);
-            } else {
+            } else if (!a.use_tma) {
                 uint64_t pg = globaltimer_ns();
                 if (piv != 0.0) gemv_tasks(a, k0, kb, k, p, piv);
+                tprobe(a, 1, 7, pg);
+            }
+            if (a.use_tma && piv != 0.0) {
+                uint64_t pg = globaltimer_ns();
+                gemv_tma(a, tmA, bars, tiles, k0, kb, k, p, piv, ph);
                 tprobe(a, 1, 7, pg);
             }
             if (!gb.sync()) return false;
@@ -1078,9 +1177,17 @@ __device__ bool blocked_phase(const RedArgs& a, GridBarrier& gb, PanelSh& S, uin
 // The reduction kernel: mode 0 = balance only, 1 = unblocked, 2 = blocked.  Balancing,
 // when requested, runs first in the same launch.
 // ---------------------------------------------------------------------------------
-__global__ void __launch_bounds__(RT, 1) reduce_kernel(RedArgs a, int balance, int mode)
+__global__ void __launch_bounds__(RT, 1) reduce_kernel(RedArgs a, int balance, int mode,
+                                                        const __grid_constant__ CUtensorMap tmA)
 {
     __shared__ PanelSh S;
+    __shared__ __align__(8) uint64_t bars[TMA_SLOTS];
+    extern __shared__ __align__(1024) double tiles[];
+    if (threadIdx.x == 0) {
+        for (int s = 0; s < TMA_SLOTS; ++s) mbar_init(&bars[s], 1);
+        mbar_fence_init();
+    }
+    __syncthreads();
     GridBarrier gb{a.bar, a.err, a.limit_ns, 0, a.ptimes ? a.ptimes + 5 : nullptr};
     uint64_t t0 = globaltimer_ns(), last = t0;
     if (balance) {
@@ -1091,7 +1198,7 @@ __global__ void __launch_bounds__(RT, 1) reduce_kernel(RedArgs a, int balance, i
         unblocked_phase(a, gb);
         tmark(a, 1, last);
     } else if (mode == 2) {
-        blocked_phase<NBMAX>(a, gb, S, last);
+        blocked_phase<NBMAX>(a, gb, S, last, &tmA, bars, tiles);
     }
     if (blockIdx.x == 0 && threadIdx.x == 0 && a.ptimes) a.ptimes[7] += globaltimer_ns() - t0;
 }
@@ -1146,6 +1253,8 @@ __global__ void reduce_init_kernel(int n, int64_t* ipiv, double* cand_v, int* ca
     }
 }
 
+constexpr size_t REDUCE_DSMEM = (size_t)TMA_SLOTS * TILE_BYTES;
+
 int reduce_grid_size()
 {
     static int g = 0;
@@ -1153,10 +1262,36 @@ int reduce_grid_size()
         int dev = 0, sms = 0, per = 0;
         cudaGetDevice(&dev);
         cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, reduce_kernel, RT, 0);
+        if (cudaFuncSetAttribute(reduce_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)REDUCE_DSMEM) !=
+            cudaSuccess)
+            return 0;
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, reduce_kernel, RT, REDUCE_DSMEM);
         g = sms * (per > 0 ? 1 : 0);
     }
     return g;
+}
+
+// Tensor map of an n x n column-major FP64 matrix (leading dimension n) in 64x64 boxes for
+// the GEMV's TMA loads.  TMA needs a 16-byte row pitch: n must be even.
+bool make_tmap_f64(void* tmap, const double* A, int n)
+{
+    if (n < 64 || (n & 1)) return false;
+    static PFN_cuTensorMapEncodeTiled_v12000 enc = nullptr;
+    if (!enc) {
+        void* fn = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &fn, cudaEnableDefault, &q) != cudaSuccess || !fn)
+            return false;
+        enc = (PFN_cuTensorMapEncodeTiled_v12000)fn;
+    }
+    const cuuint64_t dims[2] = {(cuuint64_t)n, (cuuint64_t)n};
+    const cuuint64_t strides[1] = {(cuuint64_t)n * sizeof(double)};
+    const cuuint32_t box[2] = {64, 64};
+    const cuuint32_t es[2] = {1, 1};
+    const CUresult r = enc((CUtensorMap*)tmap, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 2, (void*)A, dims, strides, box, es,
+                           CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                           CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    return r == CUDA_SUCCESS;
 }
 
 cudaError_t launch_reduce(RedArgs a, int balance, int mode, cudaStream_t st)
@@ -1167,8 +1302,11 @@ cudaError_t launch_reduce(RedArgs a, int balance, int mode, cudaStream_t st)
     cudaError_t e0 = cudaGetLastError();
     if (e0 != cudaSuccess) return e0;
     int bal = balance;
-    void* args[] = {&a, &bal, &mode};
-    return cudaLaunchCooperativeKernel((void*)reduce_kernel, dim3(grid), dim3(RT), args, 0, st);
+    CUtensorMap tm;
+    memset(&tm, 0, sizeof(tm));
+    if (a.use_tma && !make_tmap_f64(&tm, a.A, a.n)) a.use_tma = 0;
+    void* args[] = {&a, &bal, &mode, &tm};
+    return cudaLaunchCooperativeKernel((void*)reduce_kernel, dim3(grid), dim3(RT), args, REDUCE_DSMEM, st);
 }
 
 cudaError_t launch_unblocked_assemble(int n, double* A, const double* B2, const int64_t* ipiv, cudaStream_t st)
