@@ -758,6 +758,8 @@ template <int NB>
 __device__ void panel_row(const RedArgs& a, const PanelSh& S, int k0, int kb, int k, int P, int i, double wsum,
                           double& cand, int& candi, double& cands)
 {
+    // The row's panel values stay in registers: every access to v[] below has a compile-time
+    // index; the columns at run-time positions (k, k+1, p) are selected by predicates.
     const int n = a.n;
     double* A = a.A;
     const StepTab& T = S.tab;
@@ -767,8 +769,16 @@ __device__ void panel_row(const RedArgs& a, const PanelSh& S, int k0, int kb, in
 #pragma unroll
     for (int c = 0; c < NB + 2; ++c) v[c] = (c < w) ? M1(A, n, i, k0 + c) : 0.0;
     const int ck = k - k0, ck1 = k + 1 - k0;
+    auto GET = [&](int idx) -> double {
+        double r = 0.0;
+#pragma unroll
+        for (int c = 0; c < NB + 2; ++c)
+            if (c == idx) r = v[c];
+        return r;
+    };
+    double x1 = GET(ck1);  // column k+1
     if (T.skip) {
-        if (i >= k + 2) { cand = fabs(v[ck1]); candi = i; cands = v[ck1]; }
+        if (i >= k + 2) { cand = fabs(x1); candi = i; cands = x1; }
         return;
     }
     const double piv = T.piv;
@@ -781,23 +791,26 @@ __device__ void panel_row(const RedArgs& a, const PanelSh& S, int k0, int kb, in
 #pragma unroll
             for (int c = 0; c < NB + 2; ++c) if (c < w) v[c] = T.R1[c];
         }
+        x1 = GET(ck1);
         if (p <= kb + 1) {
             const int cp = p - k0;
+            const double t = x1;
+            x1 = GET(cp);
 #pragma unroll
             for (int c = 0; c < NB + 2; ++c)
-                if (c == cp) { const double t = v[ck1]; v[ck1] = v[c]; v[c] = t; }
+                if (c == cp) v[c] = t;
             double* b1 = a.B0 + (size_t)(k - k0) * n + (i - 1);
             double* bp = a.B0 + (size_t)(p - k0 - 1) * n + (i - 1);
-            const double t = *b1;
+            const double tb = *b1;
             *b1 = *bp;
-            *bp = t;
+            *bp = tb;
         } else {
             double* ap = A + (size_t)(p - 1) * n + (i - 1);
             double* b1 = a.B0 + (size_t)(k - k0) * n + (i - 1);
             const double t = *ap;
             *ap = *b1;
             *b1 = t;
-            v[ck1] = t;
+            x1 = t;
         }
     }
     // (2) the pulled column's tables and catch-up (F:1193-1205)
@@ -807,26 +820,30 @@ __device__ void panel_row(const RedArgs& a, const PanelSh& S, int k0, int kb, in
         else
             for (int r = 0; r < S.nsl; ++r)
                 if (S.slist[r] == i) sl = k - k0 + 1 + r;
-        if (sl >= 0) v[ck1] = T.OV[sl];
+        if (sl >= 0) x1 = T.OV[sl];
         if (i >= k + 2) {
 #pragma unroll
             for (int c = 0; c < NB; ++c) {
                 if (c < ck) {
                     const double x = T.CX[c];
-                    if (x != 0.0) v[ck1] = dsub(v[ck1], dmul(v[c], x));
+                    if (x != 0.0) x1 = dsub(x1, dmul(v[c], x));
                 }
             }
         }
     }
     // scale the multiplier (F:968-970, F:1503-1505)
-    if (i >= k + 2) v[ck] = v[ck] / piv;
+    double xk = GET(ck);
+    if (i >= k + 2) xk = xk / piv;
     // (3) left update of the panel columns (F:1206-1213)
     if (i >= k + 2) {
 #pragma unroll
         for (int c = 1; c < NB + 2; ++c) {
             if (c >= ck1 && c < w) {
                 const double pj = T.PJ[c - ck1];
-                if (pj != 0.0) v[c] = dsub(v[c], dmul(v[ck], pj));
+                if (pj != 0.0) {
+                    if (c == ck1) x1 = dsub(x1, dmul(xk, pj));
+                    else v[c] = dsub(v[c], dmul(xk, pj));
+                }
             }
         }
     }
@@ -835,12 +852,12 @@ __device__ void panel_row(const RedArgs& a, const PanelSh& S, int k0, int kb, in
     for (int c = 2; c < NB + 2; ++c) {
         if (c >= ck1 + 1 && c < w) {
             const double vj = T.VJ[c];
-            if (vj != 0.0) v[ck1] = dadd(v[ck1], dmul(vj, v[c]));
+            if (vj != 0.0) x1 = dadd(x1, dmul(vj, v[c]));
         }
     }
     // (5) the GEMV part with its correction (F:1222-1293)
     if (i <= k + 1) {
-        v[ck1] = dadd(v[ck1], S.LW[i - k0 - 1]);
+        x1 = dadd(x1, S.LW[i - k0 - 1]);
     } else {
         int r = -1;
         for (int q = 0; q < S.nsl; ++q)
@@ -850,21 +867,21 @@ __device__ void panel_row(const RedArgs& a, const PanelSh& S, int k0, int kb, in
         for (int c = 0; c < NB; ++c) {
             if (c <= ck) {
                 const double x = S.XS[c];
-                if (x != 0.0) wv = dsub(wv, dmul(v[c], x));
+                if (x != 0.0) wv = dsub(wv, dmul(c == ck ? xk : v[c], x));
             }
         }
-        v[ck1] = dadd(v[ck1], wv);
-        cand = fabs(v[ck1]);
+        x1 = dadd(x1, wv);
+        cand = fabs(x1);
         candi = i;
-        cands = v[ck1];
+        cands = x1;
     }
+    const bool swapped_row = p != k + 1 && (i == k + 1 || i == p);
 #pragma unroll
-    for (int c = 0; c < NB + 2; ++c)
-        if (c < w && c >= ck) M1(A, n, i, k0 + c) = v[c];
-    if (p != k + 1 && (i == k + 1 || i == p)) {
-#pragma unroll
-        for (int c = 0; c < NB + 2; ++c)
-            if (c < w && c < ck) M1(A, n, i, k0 + c) = v[c];
+    for (int c = 0; c < NB + 2; ++c) {
+        if (c < w && (c >= ck || swapped_row)) {
+            const double val = (c == ck) ? xk : ((c == ck1) ? x1 : v[c]);
+            M1(A, n, i, k0 + c) = val;
+        }
     }
 }
 
@@ -918,18 +935,29 @@ __device__ void column_end(const RedArgs& a, const PanelSh& S, int k0, int kb, i
 {
     const int n = a.n;
     double* col = a.A + (size_t)(c - 1) * n;
+    const int nsr = S.nsr;
     double old[2 * NBMAX + 2];
-    for (int q = 0; q < S.nsr; ++q) old[q] = col[S.ssrc[q] - 1];
-    for (int q = 0; q < S.nsr; ++q) col[S.srow[q] - 1] = old[q];
+#pragma unroll
+    for (int q = 0; q < 2 * NBMAX + 2; ++q)
+        if (q < nsr) old[q] = col[S.ssrc[q] - 1];
+#pragma unroll
+    for (int q = 0; q < 2 * NBMAX + 2; ++q)
+        if (q < nsr) col[S.srow[q] - 1] = old[q];
     if (!trsm) return;
     const int nbp = kb - k0 + 1;
     if (nbp < 2) return;
     double B[NBMAX];
-    for (int s = 0; s < nbp; ++s) B[s] = col[k0 + s];
-    for (int r = 0; r < nbp; ++r) {
-        double v = B[r];
-        for (int s = 0; s < nbp; ++s) v = dfma(S.Pm[r][s], B[s], v);
-        col[k0 + r] = v;
+#pragma unroll
+    for (int s = 0; s < NBMAX; ++s) B[s] = (s < nbp) ? col[k0 + s] : 0.0;
+#pragma unroll
+    for (int r = 0; r < NBMAX; ++r) {
+        if (r < nbp) {
+            double v = B[r];
+#pragma unroll
+            for (int s = 0; s < NBMAX; ++s)
+                if (s < nbp) v = dfma(S.Pm[r][s], B[s], v);
+            col[k0 + r] = v;
+        }
     }
 }
 
@@ -1130,16 +1158,16 @@ __device__ bool blocked_phase(const RedArgs& a, GridBarrier& gb, PanelSh& S, uin
                     const int c0q = cg * 4;
                     const int nq = min(4, nbp - c0q);
                     int j = kb + 2;
-                    for (; j + 15 <= n; j += 16) {
-                        double av[16], lv[16][4];
+                    for (; j + 7 <= n; j += 8) {
+                        double av[8], lv[8][4];
 #pragma unroll
-                        for (int u = 0; u < 16; ++u) {
+                        for (int u = 0; u < 8; ++u) {
                             av[u] = M1(A, n, ii, j + u);
 #pragma unroll
                             for (int q = 0; q < 4; ++q) lv[u][q] = (q < nq) ? M1(A, n, j + u, k0 + c0q + q) : 0.0;
                         }
 #pragma unroll
-                        for (int u = 0; u < 16; ++u)
+                        for (int u = 0; u < 8; ++u)
 #pragma unroll
                             for (int q = 0; q < 4; ++q) acc[q] = dfma(av[u], lv[u][q], acc[q]);
                     }
