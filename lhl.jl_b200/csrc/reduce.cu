@@ -23,8 +23,8 @@ constexpr int RT = 256;        // threads per CTA of the reduction kernels
 constexpr int RW = RT / 32;    // warps per CTA
 constexpr int NBMAX = 16;      // panel width nb (F:706)
 constexpr int GEMV_GROUP = 64; // _LHL_GEMV_GROUP (F:1451)
-constexpr int TMA_SLOTS = 20;  // 16x64 FP64 boxes in flight per CTA in the GEMV phase
-constexpr int RTILE = 16;      // rows per GEMV row tile
+constexpr int TMA_SLOTS = 32;  // 8x64 FP64 boxes in flight per CTA in the GEMV phase
+constexpr int RTILE = 8;       // rows per GEMV row tile
 constexpr int TILE_BYTES = RTILE * 64 * 8;
 constexpr int PMAX = 256;      // column groups (n <= 16384)
 
@@ -675,10 +675,11 @@ __device__ void gemv_tma(const RedArgs& a, const void* tmA, uint64_t* bars, doub
             }
             __syncthreads();
             if (warp >= 1) {
-                const int r = lane & 15;
+                const int r = lane & (RTILE - 1);
                 const int i = rt * RTILE + r + 1;  // 1-based row
                 const bool act = i >= k0 + 1 && i <= n;
-                for (int s = 2 * (warp - 1) + (lane >> 4); s < nr; s += 2 * (RW - 1)) {
+                constexpr int BPW = 32 / RTILE;    // boxes per warp and pass
+                for (int s = BPW * (warp - 1) + lane / RTILE; s < nr; s += BPW * (RW - 1)) {
                     const int g = g0 + s;
                     const int ga = kb + 2 + 64 * g;
                     const int gb = min(ga + 63, n);
@@ -712,7 +713,7 @@ __device__ void gemv_tma(const RedArgs& a, const void* tmA, uint64_t* bars, doub
                 }
             }
             __syncthreads();
-            ph ^= (1u << nr) - 1u;
+            ph ^= (nr >= 32) ? 0xffffffffu : ((1u << nr) - 1u);
         }
         // the rows' sums over the groups, in group order
         if (threadIdx.x < RTILE) {
