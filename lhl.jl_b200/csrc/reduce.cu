@@ -23,10 +23,12 @@ constexpr int RT = 256;        // threads per CTA of the reduction kernels
 constexpr int RW = RT / 32;    // warps per CTA
 constexpr int NBMAX = 16;      // panel width nb (F:706)
 constexpr int GEMV_GROUP = 64; // _LHL_GEMV_GROUP (F:1451)
-constexpr int TMA_SLOTS = 32;  // 8x64 FP64 boxes in flight per CTA in the GEMV phase
-constexpr int RTILE = 8;       // rows per GEMV row tile
-constexpr int TILE_BYTES = RTILE * 64 * 8;
 constexpr int PMAX = 256;      // column groups (n <= 16384)
+constexpr int T64_SLOTS = 5;   // 64x64 FP64 tiles in flight per CTA in the GEMV phase
+constexpr int TILE64_BYTES = 64 * 64 * 8;
+constexpr int PBOX_G = 32;     // groups per TMA box of GEMV partials (phase B)
+constexpr int PBOX_BYTES = RT * PBOX_G * 8;
+constexpr int PBOX_SLOTS = 2;
 
 
 // ---------------------------------------------------------------------------------
@@ -637,94 +639,91 @@ __device__ void gemv_tasks(const RedArgs& a, int k0, int kb, int k, int p, doubl
     }
 }
 
-// GEMV of phase A through TMA, one CTA per 16-row tile of the trailing block: the tile's
-// 64-column groups stream in as 16x64 FP64 boxes (TMA_SLOTS in flight, one mbarrier per
-// slot); each group's partial per row follows the reference's group order (F:1496-1553),
-// and the CTA then adds its rows' partials in group order (F:1558-1583), so the row sums
-// w[i] are final here and phase B reads one value per row.  The pulled column (p > kb+1)
-// comes from its pre-panel copy in B0, as the reference reads it from pSub (F:1492).
-// Warp 0 (busy with the step table) only joins the CTA barriers.
-__device__ void gemv_tma(const RedArgs& a, const void* tmA, uint64_t* bars, double* tiles, double* lsh, double* psh,
-                         int k0, int kb, int k, int p, double piv, uint32_t& ph)
+// GEMV partials of phase A through TMA: the trailing block is streamed in 64x64 FP64
+// tiles (64 rows x one 64-column group), T64_SLOTS tiles in flight per CTA, completion on
+// one mbarrier per slot.  Two warps consume a tile (32 rows each); the arithmetic per row
+// is the reference's group order (F:1496-1553), read from shared memory.  The pulled
+// column (p > kb+1) is taken from its pre-panel copy in B0, as the reference reads it
+// from pSub (F:1492).  Warp 0 only joins the per-round CTA barriers.
+__device__ void gemv_tma64(const RedArgs& a, const void* tmA, uint64_t* bars, double* tiles, int k0, int kb, int k,
+                         int p, double piv, uint32_t& ph)
 {
     const int n = a.n;
     const double* A = a.A;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const int P = (n - kb - 1 + GEMV_GROUP - 1) / GEMV_GROUP;
-    const int t0 = k0 / RTILE;                      // tile holding 0-based row k0 (= row k0+1)
-    const int nt = (n + RTILE - 1) / RTILE - t0;
+    const int r0t = k0 / 64;  // first 64-row tile holding 0-based row k0 (= row k0+1)
+    const int RTn = (n + 63) / 64 - r0t;
+    const int ntask = RTn * P;
+    const int G = gridDim.x, bid = blockIdx.x;
+    const int cnt = (ntask > bid) ? (ntask - bid - 1) / G + 1 : 0;
     const bool pulled = p > kb + 1;
     const double* sub = a.B0 + (size_t)(k - k0) * n;
-    const double ak1 = M1(A, n, k + 1, k);          // A[k+1,k] pre-swap: row p's multiplier source
-    for (int tt = blockIdx.x; tt < nt; tt += gridDim.x) {
-        const int rt = t0 + tt;
-        for (int g0 = 0; g0 < P; g0 += TMA_SLOTS) {
-            const int nr = min(TMA_SLOTS, P - g0);
-            if (threadIdx.x == 32) {
-                fence_proxy_async_global();
-                fence_proxy_async_shared();
-                for (int s = 0; s < nr; ++s) {
-                    mbar_expect_tx(&bars[s], TILE_BYTES);
-                    tma_load_2d(tiles + (size_t)s * (RTILE * 64), tmA, rt * RTILE, kb + 1 + 64 * (g0 + s), &bars[s]);
-                }
+    for (int base = 0; base < cnt; base += T64_SLOTS) {
+        const int nr = min(T64_SLOTS, cnt - base);
+        if (threadIdx.x == 32) {
+            fence_proxy_async_global();
+            fence_proxy_async_shared();
+            for (int s = 0; s < nr; ++s) {
+                const int t = bid + (base + s) * G;
+                const int g = t / RTn, rt = r0t + t % RTn;
+                mbar_expect_tx(&bars[s], TILE64_BYTES);
+                tma_load_2d(tiles + (size_t)s * 4096, tmA, rt * 64, kb + 1 + 64 * g, &bars[s]);
             }
-            // the round's multipliers l_j = A'[j,k] / piv (all threads, while the boxes fly)
-            for (int e = threadIdx.x; e < nr * 64; e += RT) {
-                const int j = kb + 2 + 64 * g0 + e;
-                lsh[e] = (j <= n) ? ((j == p) ? ak1 : M1(A, n, j, k)) / piv : 0.0;
-            }
-            __syncthreads();
-            if (warp >= 1) {
-                const int r = lane & (RTILE - 1);
-                const int i = rt * RTILE + r + 1;  // 1-based row
-                const bool act = i >= k0 + 1 && i <= n;
-                constexpr int BPW = 32 / RTILE;    // boxes per warp and pass
-                for (int s = BPW * (warp - 1) + lane / RTILE; s < nr; s += BPW * (RW - 1)) {
-                    const int g = g0 + s;
-                    const int ga = kb + 2 + 64 * g;
-                    const int gb = min(ga + 63, n);
-                    const int w = gb - ga + 1;
-                    const bool psub = pulled && p >= ga && p <= gb;
-                    const double bval = (psub && act) ? sub[i - 1] : 0.0;
-                    if (!mbar_wait(&bars[s], (ph >> s) & 1u, 1u << 22)) atomicCAS(a.err, 0, (int)LHL_ERR_TIMEOUT);
-                    const double* tl = tiles + (size_t)s * (RTILE * 64) + r;
-                    const double* ll = lsh + s * 64 - ga;
-                    auto TV = [&](int j) -> double { return (psub && j == p) ? bval : tl[(j - ga) * RTILE]; };
-                    const int nquad = w >> 2;
-                    double acc = 0.0;
-                    bool have = false;
-                    for (int q = 0; q < nquad; ++q) {
-                        const int j = ga + 4 * q;
-                        const double quad = dadd(dadd(dmul(ll[j], TV(j)), dmul(ll[j + 1], TV(j + 1))),
-                                                 dadd(dmul(ll[j + 2], TV(j + 2)), dmul(ll[j + 3], TV(j + 3))));
-                        acc = have ? dadd(acc, quad) : quad;
-                        have = true;
-                    }
-                    for (int j = ga + 4 * nquad; j <= gb; ++j) {
-                        const double lj = ll[j];
-                        if (!have) {
-                            acc = dmul(lj, TV(j));
-                            have = true;
-                        } else if (lj != 0.0) {
-                            acc = dadd(acc, dmul(lj, TV(j)));
-                        }
-                    }
-                    psh[g * RTILE + r] = acc;
-                }
-            }
-            __syncthreads();
-            ph ^= (nr >= 32) ? 0xffffffffu : ((1u << nr) - 1u);
         }
-        // the rows' sums over the groups, in group order
-        if (threadIdx.x < RTILE) {
-            const int i = rt * RTILE + threadIdx.x + 1;
-            if (i >= k0 + 1 && i <= n) {
-                double sacc = psh[threadIdx.x];
-                for (int g = 1; g < P; ++g) sacc = dadd(sacc, psh[g * RTILE + threadIdx.x]);
-                a.part[i - 1] = sacc;
+        if (warp >= 1) {
+            for (int u = warp - 1; u < 2 * nr; u += RW - 1) {
+                const int s = u >> 1, half = u & 1;
+                const int t = bid + (base + s) * G;
+                const int g = t / RTn, rt = r0t + t % RTn;
+                const int ga = kb + 2 + 64 * g;
+                const int gb = min(ga + 63, n);
+                const int w = gb - ga + 1;
+                double l0 = 0.0, l1 = 0.0;
+                {
+                    const int j0 = ga + lane, j1 = ga + 32 + lane;
+                    if (j0 <= gb) l0 = ((j0 == p) ? M1(A, n, k + 1, k) : M1(A, n, j0, k)) / piv;
+                    if (j1 <= gb) l1 = ((j1 == p) ? M1(A, n, k + 1, k) : M1(A, n, j1, k)) / piv;
+                }
+                const int r = half * 32 + lane;       // row within the tile
+                const int i = rt * 64 + r + 1;         // 1-based row
+                const bool act = i >= k0 + 1 && i <= n;
+                const bool psub = pulled && p >= ga && p <= gb;
+                const double bval = (psub && act) ? sub[i - 1] : 0.0;
+                if (!mbar_wait(&bars[s], (ph >> s) & 1u, 1u << 22)) atomicCAS(a.err, 0, (int)LHL_ERR_TIMEOUT);
+                const double* tl = tiles + (size_t)s * 4096 + r;
+                auto TV = [&](int j) -> double { return (psub && j == p) ? bval : tl[(j - ga) * 64]; };
+                auto LV = [&](int j) -> double {
+                    const int m = j - ga;
+                    const double v0 = __shfl_sync(0xffffffffu, l0, m & 31);
+                    const double v1 = __shfl_sync(0xffffffffu, l1, m & 31);
+                    return m < 32 ? v0 : v1;
+                };
+                const int nquad = w >> 2;
+                double acc = 0.0;
+                bool have = false;
+                for (int q = 0; q < nquad; ++q) {
+                    const int j = ga + 4 * q;
+                    const double q1 = LV(j), q2 = LV(j + 1), q3 = LV(j + 2), q4 = LV(j + 3);
+                    const double quad = dadd(dadd(dmul(q1, TV(j)), dmul(q2, TV(j + 1))),
+                                             dadd(dmul(q3, TV(j + 2)), dmul(q4, TV(j + 3))));
+                    acc = have ? dadd(acc, quad) : quad;
+                    have = true;
+                }
+                for (int j = ga + 4 * nquad; j <= gb; ++j) {
+                    const double lj = LV(j);
+                    if (!have) {
+                        acc = dmul(lj, TV(j));
+                        have = true;
+                    } else if (lj != 0.0) {
+                        acc = dadd(acc, dmul(lj, TV(j)));
+                    }
+                }
+                if (act) a.part[(size_t)g * n + (i - 1)] = acc;
             }
         }
         __syncthreads();
+        ph ^= (1u << nr) - 1u;
     }
 }
 
@@ -968,7 +967,7 @@ __device__ void column_end(const RedArgs& a, const PanelSh& S, int k0, int kb, i
 
 template <int NB>
 __device__ bool blocked_phase(const RedArgs& a, GridBarrier& gb, PanelSh& S, uint64_t& last, const void* tmA,
-                              uint64_t* bars, double* tiles)
+                              const void* tmP, uint64_t* bars, double* tiles)
 {
     uint32_t ph = 0;  // per-slot mbarrier phase parity (identical in every thread)
     const int n = a.n;
@@ -1037,8 +1036,7 @@ __device__ bool blocked_phase(const RedArgs& a, GridBarrier& gb, PanelSh& S, uin
             }
             if (a.use_tma && piv != 0.0) {
                 uint64_t pg = globaltimer_ns();
-                gemv_tma(a, tmA, bars, tiles, tiles + TMA_SLOTS * RTILE * 64, tiles + TMA_SLOTS * RTILE * 64 + TMA_SLOTS * 64,
-                         k0, kb, k, p, piv, ph);
+                gemv_tma64(a, tmA, bars, tiles, k0, kb, k, p, piv, ph);
                 tprobe(a, 1, 7, pg);
             }
             if (!gb.sync()) return false;
@@ -1051,10 +1049,42 @@ __device__ bool blocked_phase(const RedArgs& a, GridBarrier& gb, PanelSh& S, uin
             const bool cta_rows = (blockIdx.x + 1) * RT >= k0 + 1 && blockIdx.x * RT + 1 <= n;
             tprobe(a, (n - 1) / RT, 0, pb);
             double wsum = 0.0;
-            const int Pw = a.use_tma ? 1 : P;  // the TMA path leaves final row sums in part[0..n)
-            if (warp == 0 && !skip && cta_rows) correction_triangle(a, S, k0, k, Pw);
-            if (!skip && i >= k + 2 && i <= n) wsum = partial_sum(a, Pw, i);
+            if (a.use_tma && !skip && cta_rows && threadIdx.x == 32) {
+                // this CTA's rows of the GEMV partials, PBOX_G groups per box
+                fence_proxy_async_global();
+                fence_proxy_async_shared();
+                for (int s = 0; s < PBOX_SLOTS && s * PBOX_G < P; ++s) {
+                    mbar_expect_tx(&bars[s], PBOX_BYTES);
+                    tma_load_2d(tiles + (size_t)s * RT * PBOX_G, tmP, blockIdx.x * RT, s * PBOX_G, &bars[s]);
+                }
+            }
+            if (warp == 0 && !skip && cta_rows) correction_triangle(a, S, k0, k, P);
+            if (!skip && i >= k + 2 && i <= n) {
+                if (a.use_tma) {
+                    // sum from the staged partials, in group order; boxes beyond PBOX_SLOTS
+                    // (n > 4096) are read from global memory
+                    double sacc = 0.0;
+                    const int r = threadIdx.x;
+                    for (int s = 0; s < PBOX_SLOTS && s * PBOX_G < P; ++s) {
+                        if (!mbar_wait(&bars[s], (ph >> s) & 1u, 1u << 22)) atomicCAS(a.err, 0, (int)LHL_ERR_TIMEOUT);
+                        const double* pb = tiles + (size_t)s * RT * PBOX_G;
+                        const int gend = min(P - s * PBOX_G, PBOX_G);
+                        for (int gg = 0; gg < gend; ++gg) {
+                            const double x = pb[gg * RT + r];
+                            sacc = (s == 0 && gg == 0) ? x : dadd(sacc, x);
+                        }
+                    }
+                    for (int g = PBOX_SLOTS * PBOX_G; g < P; ++g) sacc = dadd(sacc, a.part[(size_t)g * n + (i - 1)]);
+                    wsum = sacc;
+                } else {
+                    wsum = partial_sum(a, P, i);
+                }
+            }
             __syncthreads();
+            if (a.use_tma && !skip && cta_rows) {
+                const int ns = min(PBOX_SLOTS, (P + PBOX_G - 1) / PBOX_G);
+                ph ^= (1u << ns) - 1u;
+            }
             tprobe(a, (n - 1) / RT, 1, pb);
             double cand = 0.0, cands = 0.0;
             int candi = 0;
@@ -1088,7 +1118,8 @@ __device__ bool blocked_phase(const RedArgs& a, GridBarrier& gb, PanelSh& S, uin
         // ---- panel end E1: interchange map, TRSM inverse, column sweeps ----
         build_swap_map(a, S, k0, kb);
         build_trsm_inverse(a, S, k0, kb);
-        for (int c = 1 + gt; c <= n; c += gsz) {
+        // columns spread over every CTA (column c on CTA c mod grid) for memory parallelism
+        for (int c = 1 + (int)blockIdx.x + (int)gridDim.x * (int)threadIdx.x; c <= n; c += gsz) {
             if (c >= kb + 2) column_end(a, S, k0, kb, c, true);
             else if (c < k0) column_end(a, S, k0, kb, c, false);
         }
@@ -1213,13 +1244,14 @@ __device__ bool blocked_phase(const RedArgs& a, GridBarrier& gb, PanelSh& S, uin
 // when requested, runs first in the same launch.
 // ---------------------------------------------------------------------------------
 __global__ void __launch_bounds__(RT, 1) reduce_kernel(RedArgs a, int balance, int mode,
-                                                        const __grid_constant__ CUtensorMap tmA)
+                                                        const __grid_constant__ CUtensorMap tmA,
+                                                        const __grid_constant__ CUtensorMap tmP)
 {
     __shared__ PanelSh S;
-    __shared__ __align__(8) uint64_t bars[TMA_SLOTS];
+    __shared__ __align__(8) uint64_t bars[T64_SLOTS];
     extern __shared__ __align__(1024) double tiles[];
     if (threadIdx.x == 0) {
-        for (int s = 0; s < TMA_SLOTS; ++s) mbar_init(&bars[s], 1);
+        for (int s = 0; s < T64_SLOTS; ++s) mbar_init(&bars[s], 1);
         mbar_fence_init();
     }
     __syncthreads();
@@ -1233,7 +1265,7 @@ __global__ void __launch_bounds__(RT, 1) reduce_kernel(RedArgs a, int balance, i
         unblocked_phase(a, gb);
         tmark(a, 1, last);
     } else if (mode == 2) {
-        blocked_phase<NBMAX>(a, gb, S, last, &tmA, bars, tiles);
+        blocked_phase<NBMAX>(a, gb, S, last, &tmA, &tmP, bars, tiles);
     }
     if (blockIdx.x == 0 && threadIdx.x == 0 && a.ptimes) a.ptimes[7] += globaltimer_ns() - t0;
 }
@@ -1288,7 +1320,9 @@ __global__ void reduce_init_kernel(int n, int64_t* ipiv, double* cand_v, int* ca
     }
 }
 
-constexpr size_t REDUCE_DSMEM = (size_t)TMA_SLOTS * TILE_BYTES + TMA_SLOTS * 64 * 8 + (size_t)PMAX * RTILE * 8;
+constexpr size_t REDUCE_DSMEM = (size_t)T64_SLOTS * TILE64_BYTES > (size_t)PBOX_SLOTS * PBOX_BYTES
+                                    ? (size_t)T64_SLOTS * TILE64_BYTES
+                                    : (size_t)PBOX_SLOTS * PBOX_BYTES;
 
 int reduce_grid_size()
 {
@@ -1306,11 +1340,11 @@ int reduce_grid_size()
     return g;
 }
 
-// Tensor map of an n x n column-major FP64 matrix (leading dimension n) in 64x64 boxes for
-// the GEMV's TMA loads.  TMA needs a 16-byte row pitch: n must be even.
-bool make_tmap_f64(void* tmap, const double* A, int n)
+// 2-D tensor map of a column-major FP64 array (rows x cols, leading dimension ld) in
+// boxes of box_r x box_c, for TMA loads.  TMA needs a 16-byte row pitch (even ld).
+static bool make_tmap_2d(void* tmap, const double* base, int rows, int cols, int ld, int box_r, int box_c)
 {
-    if (n < 64 || (n & 1) || n > PMAX * GEMV_GROUP) return false;
+    if ((ld & 1) || rows < 1 || cols < 1) return false;
     static PFN_cuTensorMapEncodeTiled_v12000 enc = nullptr;
     if (!enc) {
         void* fn = nullptr;
@@ -1319,11 +1353,11 @@ bool make_tmap_f64(void* tmap, const double* A, int n)
             return false;
         enc = (PFN_cuTensorMapEncodeTiled_v12000)fn;
     }
-    const cuuint64_t dims[2] = {(cuuint64_t)n, (cuuint64_t)n};
-    const cuuint64_t strides[1] = {(cuuint64_t)n * sizeof(double)};
-    const cuuint32_t box[2] = {RTILE, 64};
+    const cuuint64_t dims[2] = {(cuuint64_t)rows, (cuuint64_t)cols};
+    const cuuint64_t strides[1] = {(cuuint64_t)ld * sizeof(double)};
+    const cuuint32_t box[2] = {(cuuint32_t)box_r, (cuuint32_t)box_c};
     const cuuint32_t es[2] = {1, 1};
-    const CUresult r = enc((CUtensorMap*)tmap, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 2, (void*)A, dims, strides, box, es,
+    const CUresult r = enc((CUtensorMap*)tmap, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 2, (void*)base, dims, strides, box, es,
                            CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
                            CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
     return r == CUDA_SUCCESS;
@@ -1337,10 +1371,16 @@ cudaError_t launch_reduce(RedArgs a, int balance, int mode, cudaStream_t st)
     cudaError_t e0 = cudaGetLastError();
     if (e0 != cudaSuccess) return e0;
     int bal = balance;
-    CUtensorMap tm;
+    CUtensorMap tm, tp;
     memset(&tm, 0, sizeof(tm));
-    if (a.use_tma && !make_tmap_f64(&tm, a.A, a.n)) a.use_tma = 0;
-    void* args[] = {&a, &bal, &mode, &tm};
+    memset(&tp, 0, sizeof(tp));
+    if (a.use_tma) {
+        const int P = (a.n + GEMV_GROUP - 1) / GEMV_GROUP;
+        const bool ok = a.n >= 64 && a.n <= PMAX * GEMV_GROUP && make_tmap_2d(&tm, a.A, a.n, a.n, a.n, 64, 64) &&
+                        make_tmap_2d(&tp, a.part, a.n, P, a.n, RT, PBOX_G);
+        if (!ok) a.use_tma = 0;
+    }
+    void* args[] = {&a, &bal, &mode, &tm, &tp};
     return cudaLaunchCooperativeKernel((void*)reduce_kernel, dim3(grid), dim3(RT), args, REDUCE_DSMEM, st);
 }
 
