@@ -1,0 +1,69 @@
+"""Run one piece of the hot path on seeded inputs, for timing or for a profiler.
+
+    python lhl.jl_b200/profile_case.py --n 2048 --what reduce --reps 3
+    python lhl.jl_b200/profile_case.py --n 2048 --what chain --shifts 64 --reps 3
+
+--what reduce: lhl_reduce (balance + reduction + Ht/perm) of an N(0,1) matrix.
+--what chain:  one reduction, then per repetition the batched shift LUs, the solves and one
+               refinement step for `--shifts` shifts (1, -g) with one right-hand side each.
+Prints the CUDA-event time of each repetition."""
+from __future__ import annotations
+
+import argparse
+import os
+import sys
+
+import numpy as np
+import torch
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+if HERE not in sys.path:
+    sys.path.insert(0, HERE)
+
+import lhl_gpu as G  # noqa: E402
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--n", type=int, default=2048)
+    ap.add_argument("--what", default="reduce", choices=["reduce", "chain"])
+    ap.add_argument("--shifts", type=int, default=64)
+    ap.add_argument("--reps", type=int, default=3)
+    ap.add_argument("--seed", type=int, default=2)
+    args = ap.parse_args()
+    n = args.n
+    rng = np.random.default_rng(args.seed)
+    J = torch.as_tensor(np.asfortranarray(rng.standard_normal((n, n)))).cuda()
+    ws = G.LHLWorkspace(n)
+    ev = lambda: torch.cuda.Event(enable_timing=True)  # noqa: E731
+    if args.what == "reduce":
+        for r in range(args.reps):
+            a, b = ev(), ev()
+            a.record()
+            G.lhl_reduce_(ws, J, True)
+            b.record()
+            torch.cuda.synchronize()
+            ws.check()
+            print(f"reduce n={n} rep={r} ms={a.elapsed_time(b):.3f}", flush=True)
+        return
+    S = args.shifts
+    G.lhl_reduce_(ws, J, True)
+    sh = G.LHLShift(n, S)
+    sig = torch.ones(S, dtype=torch.float64, device="cuda")
+    tau = torch.as_tensor(-(10.0 ** rng.uniform(-4, -1, S))).cuda()
+    B = torch.as_tensor(np.asfortranarray(rng.standard_normal((n, S)))).cuda()
+    X = torch.empty_like(B)
+    for r in range(args.reps):
+        a, b = ev(), ev()
+        a.record()
+        G.lhl_shift_batched_(sh, ws, sig, tau)
+        X.copy_(B)
+        G.lhl_ldiv_(X, sh, ws)
+        G.lhl_refine_(X, J, B, sh, ws, 1)
+        b.record()
+        torch.cuda.synchronize()
+        print(f"chain n={n} shifts={S} rep={r} ms={a.elapsed_time(b):.3f}", flush=True)
+
+
+if __name__ == "__main__":
+    main()
