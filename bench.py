@@ -236,12 +236,11 @@ def main():
     peak, peak_kind = peaks()
     achieved = alg_bytes / (red * 1e-3) / 1e9
     traffic = None
-    tp = os.path.join(REPO, "profiles", "reduce_c2_traffic.json")
+    tp = os.path.join(REPO, "profiles", "reduce_kernel_c2_n2048.md")
     if os.path.exists(tp):
-        try:
-            traffic = json.load(open(tp)).get("dram_bytes_per_launch")
-        except Exception:
-            traffic = None
+        for line in open(tp):
+            if line.startswith("dram_bytes_per_launch:"):
+                traffic = float(line.split(":")[1])
 
     # ---- end to end through the public API: host buffers, copies inside the timed region ----
     def pinned_colmajor(a):
