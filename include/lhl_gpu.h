@@ -35,7 +35,8 @@ enum {
 
 enum {
     LHL_PREC_FP64 = 0,    /* plain form: FP64 throughout, the reference's operation order */
-    LHL_PREC_MIXED = 1    /* mixed form: FP32 reduction on tensor cores, FP64 refinement */
+    LHL_PREC_MIXED = 1    /* mixed form: FP32 reduction (FP64-accumulated column updates), FP64
+                             balancing, shifts, solves, residuals and refinement */
 };
 
 typedef struct lhl_ws_s* lhl_ws_t;       /* LHLWorkspace{Float64} (F:144-178) */
@@ -65,7 +66,9 @@ typedef struct {
 } lhl_shift_view;
 
 /* ---- workspace ------------------------------------------------------------------ */
-/* LHLWorkspace{Float64}(n) (F:164-178).  precision: LHL_PREC_*. */
+/* LHLWorkspace{Float64}(n) (F:164-178).  precision: LHL_PREC_*.  With LHL_PREC_MIXED,
+ * lhl_reduce computes the factors in FP32 (stored widened to FP64 in the same layout), for
+ * use with lhl_refine_tol; every other entry point is unchanged. */
 int lhl_ws_create(int64_t n, int precision, lhl_ws_t* ws);
 int lhl_ws_destroy(lhl_ws_t ws);
 int lhl_ws_get_view(lhl_ws_t ws, lhl_ws_view* view);
@@ -112,6 +115,17 @@ int lhl_ldiv(lhl_shift_t sh, lhl_ws_t ws, double* dX, int64_t ldx, int64_t nrhs,
 int lhl_refine(lhl_shift_t sh, lhl_ws_t ws, const double* dJ, int64_t ldj, const double* dB, int64_t ldb,
                double* dX, int64_t ldx, double* dR, int64_t nrhs, int64_t rhs_per_shift, int steps,
                void* stream);
+
+/* lhl_refine! driven by a tolerance instead of a step count: up to max_steps refinement
+ * steps; a column whose relative residual ||b - A x||_2 / ||b||_2 is already <= tol is left
+ * alone (its solve and update are skipped on the device, no host round trip).  On return
+ * dres (nrhs) holds every column's final relative residual.  This is how the mixed form
+ * (LHL_PREC_MIXED workspace) reaches FP64 accuracy from its FP32 factors.  The reference's
+ * lhl_refine! (F:3144-3157) takes a fixed step count; with max_steps = steps and tol = 0 this
+ * performs the same updates. */
+int lhl_refine_tol(lhl_shift_t sh, lhl_ws_t ws, const double* dJ, int64_t ldj, const double* dB, int64_t ldb,
+                   double* dX, int64_t ldx, double* dR, double* dres, int64_t nrhs, int64_t rhs_per_shift, double tol,
+                   int max_steps, void* stream);
 
 /* Relative residuals ||b - (sigma I + tau J) x||_2 / ||b||_2 per column into dres (nrhs). */
 int lhl_residual_norms(lhl_shift_t sh, const double* dJ, int64_t ldj, const double* dB, int64_t ldb,

@@ -17,6 +17,10 @@ struct lhl_ws_s {
     unsigned int* bar;
     unsigned long long limit_ns;
     unsigned long long* ptimes;
+    // mixed form (LHL_PREC_MIXED) only
+    lhl::MixPlan mplan;
+    unsigned long long* mhdr;
+    float *mcval, *mcrow, *mgrows;
 };
 
 struct lhl_shift_s {
@@ -41,7 +45,7 @@ static void ws_free(lhl_ws_t w)
     if (!w) return;
     void* ptrs[] = {w->F, w->Ht, w->scale, w->iscale, w->B0, w->part, w->tab, w->cand_v, w->cand_s, w->buf2, w->tsnap,
                     w->bsum, w->bfac, w->ipiv, w->perm, w->iperm, w->cand_i, w->bflag, w->err, w->bar,
-                    w->ptimes};
+                    w->ptimes, w->mhdr, w->mcval, w->mcrow, w->mgrows};
     for (void* p : ptrs)
         if (p) cudaFree(p);
     delete w;
@@ -89,6 +93,23 @@ int lhl_ws_create(int64_t n, int precision, lhl_ws_t* out)
     A_(err, 4);
     A_(bar, 4);
     A_(ptimes, 24);
+    if (precision == LHL_PREC_MIXED && n >= 3) {
+        int dev = 0, sms = 0;
+        if (e == cudaSuccess) e = cudaGetDevice(&dev);
+        if (e == cudaSuccess) e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+        if (e == cudaSuccess) {
+            lhl::mixed_plan((int)n, sms, &w->mplan);
+            if (!w->mplan.ok) {
+                ws_free(w);
+                return LHL_ERR_DIM;
+            }
+        }
+        const size_t ldr = (size_t)w->mplan.ldr, g = (size_t)w->mplan.grid;
+        A_(mhdr, 2 * g);
+        A_(mcval, 2 * (size_t)n);
+        A_(mcrow, 2 * g * ldr);
+        A_(mgrows, w->mplan.smem_rows ? 1 : (size_t)n * ldr);
+    }
 #undef A_
     if (e == cudaSuccess) e = cudaMemset(w->err, 0, 4 * sizeof(int));
     if (e == cudaSuccess) e = cudaMemset(w->ptimes, 0, 24 * sizeof(unsigned long long));
@@ -195,6 +216,29 @@ int lhl_reduce(lhl_ws_t ws, const double* dJ, int64_t ldj, int balance, void* st
     a.limit_ns = ws->limit_ns;
     a.ptimes = ws->ptimes;
     a.use_tma = (n % 2 == 0) ? 1 : 0;
+    if (ws->precision == LHL_PREC_MIXED && n >= 3) {
+        // balancing (FP64, the plain kernel's balance-only mode), then the FP32 reduction
+        if (!balance) e = lhl::launch_fill_ones(ws->scale, ws->iscale, (int)n, st);
+        if (e == cudaSuccess)
+            e = cudaMemsetAsync(ws->mhdr, 0, 2 * (size_t)ws->mplan.grid * sizeof(unsigned long long), st);
+        if (e == cudaSuccess) e = lhl::launch_reduce(a, balance ? 1 : 0, 0, st);
+        if (e != cudaSuccess) return LHL_ERR_CUDA;
+        lhl::MixArgs m;
+        memset(&m, 0, sizeof(m));
+        m.n = (int)n;
+        m.A = ws->F;
+        m.ipiv = ws->ipiv;
+        m.hdr = ws->mhdr;
+        m.cval = ws->mcval;
+        m.crow = ws->mcrow;
+        m.grows = ws->mgrows;
+        m.err = ws->err;
+        m.limit_ns = ws->limit_ns;
+        m.ptimes = ws->ptimes;
+        e = lhl::launch_reduce_mixed(m, ws->mplan, st);
+        if (e != cudaSuccess) return LHL_ERR_CUDA;
+        return cuda_status(lhl::launch_ht_perm((int)n, ws->F, ws->Ht, ws->ipiv, ws->perm, ws->iperm, st));
+    }
     const int mode = n <= 2 ? 0 : (n < 500 ? 1 : 2);
     if (!balance) {
         // scale = iscale = 1
@@ -373,6 +417,53 @@ int lhl_refine(lhl_shift_t sh, lhl_ws_t ws, const double* dJ, int64_t ldj, const
         int rc = ldiv_common(sh, ws, dR, ldx, nrhs, rhs_per_shift, 0, st);
         if (rc != LHL_OK) return rc;
         e = lhl::launch_axpy_cols((int)n, dX, (int)ldx, dR, (int)ldx, (int)nrhs, st);
+        if (e != cudaSuccess) return LHL_ERR_CUDA;
+    }
+    return LHL_OK;
+}
+
+int lhl_refine_tol(lhl_shift_t sh, lhl_ws_t ws, const double* dJ, int64_t ldj, const double* dB, int64_t ldb,
+                   double* dX, int64_t ldx, double* dR, double* dres, int64_t nrhs, int64_t rhs_per_shift, double tol,
+                   int max_steps, void* stream)
+{
+    if (!sh || !ws) return LHL_ERR_ARG;
+    const int64_t n = ws->n;
+    if (sh->n != n) return LHL_ERR_DIM;
+    if (rhs_per_shift < 1 || max_steps < 0 || !(tol >= 0.0)) return LHL_ERR_ARG;
+    if (nrhs < 0) return LHL_ERR_DIM;
+    if (nrhs == 0 || n == 0) return LHL_OK;
+    if (!dJ || !dB || !dX || !dR || !dres) return LHL_ERR_ARG;
+    if (ldj < n || ldb < n || ldx < n) return LHL_ERR_DIM;
+    if ((nrhs + rhs_per_shift - 1) / rhs_per_shift > sh->nshifts) return LHL_ERR_DIM;
+    if (n > 8192) return LHL_ERR_DIM;
+    cudaStream_t st = (cudaStream_t)stream;
+    for (int s = 0; s <= max_steps; ++s) {
+        cudaError_t e = lhl::launch_residual((int)n, dJ, (int)ldj, dB, (int)ldb, dX, (int)ldx, dR, (int)ldx, (int)nrhs,
+                                             (int)rhs_per_shift, sh->sigma, sh->tau, st);
+        if (e == cudaSuccess) e = lhl::launch_relres((int)n, dR, (int)ldx, dB, (int)ldb, dres, (int)nrhs, st);
+        if (e != cudaSuccess) return LHL_ERR_CUDA;
+        if (s == max_steps) break;
+        lhl::LdivArgs a;
+        memset(&a, 0, sizeof(a));
+        a.n = (int)n;
+        a.F = ws->F;
+        a.ldf = (int)n;
+        a.perm = ws->perm;
+        a.iperm = ws->iperm;
+        a.scale = ws->scale;
+        a.iscale = ws->iscale;
+        a.X = dR;
+        a.ldx = (int)ldx;
+        a.mode = 0;
+        a.Gt = sh->Gt;
+        a.ldg = (int)sh->ldg;
+        a.swp = sh->swap;
+        a.rdiag = sh->rdiag;
+        a.rhs_per_shift = (int)rhs_per_shift;
+        a.done = dres;
+        a.tol = tol;
+        e = lhl::launch_ldiv(a, (int)nrhs, st);
+        if (e == cudaSuccess) e = lhl::launch_axpy_cols((int)n, dX, (int)ldx, dR, (int)ldx, (int)nrhs, st, dres, tol);
         if (e != cudaSuccess) return LHL_ERR_CUDA;
     }
     return LHL_OK;

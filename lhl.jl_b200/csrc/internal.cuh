@@ -50,7 +50,32 @@ struct LdivArgs {
     int ldx;
     int rhs_per_shift;
     int mode;             // 0 ldiv, 1 applyZinv, 2 applyZ
+    const double* done;   // optional: column c is skipped when done[c] <= tol
+    double tol;
 };
+
+// Mixed-precision reduction (see reduce_mixed.cu).
+struct MixArgs {
+    int n, rpc, ldr;        // order, rows per CTA, row pitch (floats)
+    double* A;              // balanced J in, factors out (n x n, ld n)
+    int64_t* ipiv;
+    unsigned long long* hdr;  // 2 x grid: per CTA and step parity, value << 32 | step << 16 | row
+    float* cval;            // 2 x n column values by physical row
+    float* crow;            // 2 x grid x ldr candidate rows
+    float* grows;           // n x ldr rows when they do not fit in shared memory
+    int* err;
+    unsigned long long limit_ns;
+    unsigned long long* ptimes;
+};
+
+struct MixPlan {
+    int rpc, grid, ldr, smem_rows, ok;
+    size_t smem;
+};
+
+constexpr size_t MIX_SMEM_MAX = 227 * 1024 - 2048;  // dynamic part; the kernel's static shared arrays use < 1 KB
+void mixed_plan(int n, int sms, MixPlan* pl);
+cudaError_t launch_reduce_mixed(MixArgs a, const MixPlan& pl, cudaStream_t st);
 
 cudaError_t launch_reduce(RedArgs a, int balance, int mode, cudaStream_t st);
 cudaError_t launch_unblocked_assemble(int n, double* A, const double* B2, const int64_t* ipiv, cudaStream_t st);
@@ -68,7 +93,8 @@ cudaError_t launch_ldiv(const LdivArgs& a, int nrhs, cudaStream_t st);
 cudaError_t launch_residual(int n, const double* J, int ldj, const double* B, int ldb, const double* X, int ldx,
                             double* R, int ldr, int nrhs, int rhs_per_shift, const double* sig, const double* tau,
                             cudaStream_t st);
-cudaError_t launch_axpy_cols(int n, double* X, int ldx, const double* R, int ldr, int nrhs, cudaStream_t st);
+cudaError_t launch_axpy_cols(int n, double* X, int ldx, const double* R, int ldr, int nrhs, cudaStream_t st,
+                             const double* done = nullptr, double tol = 0.0);
 cudaError_t launch_relres(int n, const double* R, int ldr, const double* B, int ldb, double* out, int nrhs,
                           cudaStream_t st);
 

@@ -1,0 +1,424 @@
+// reduce_mixed.cu -- the mixed-precision reduction (LHL_PREC_MIXED): ELMHES (F:466-501,
+// the unblocked algorithm) with the matrix held in FP32 and every column-update dot product
+// accumulated in FP64, for use as the preconditioner of FP64 refinement (lhl_refine!,
+// F:3144-3157).  Balancing (F:299-340) runs before it in FP64, in the plain reduction
+// kernel's balance-only mode.
+//
+// Layout: one CTA per SM, each owning a contiguous block of `rpc` physical rows of the
+// (balanced) matrix, FP32, in shared memory (rows in global memory when they do not fit).
+// Rows never move: a row interchange only swaps logical labels (ph: logical -> physical,
+// lg: physical -> logical), which every CTA tracks identically.  Column interchanges are
+// applied in place by each owner.
+//
+// Step k (1-based, k = 1..n-2), per CTA:
+//   wait   -- warp 0 polls until every CTA has published step k: a 64-bit header per CTA
+//             (step number, best candidate's logical row and signed column value) stored with
+//             release semantics after the CTA's rows' column-k values (cval) and the
+//             candidate's row (crow).  The poll uses acquire loads and is bounded in wall time.
+//             Warp 0 then picks the pivot p (largest |value|, ties to the lowest logical row:
+//             the reference's first maximum, F:799-806) and swaps labels k+1 <-> p.
+//   load   -- swap columns k+1 <-> p in own rows; load the pivot row R from the winner's crow
+//             and every multiplier l_j = c_j / piv from cval (one L2 round trip).
+//   update -- new column k+1 of own row i (the column update A[:,k+1] += A[:,k+2:n] l after
+//             the row update A[i,:] -= l_i R):
+//                 c'_i = (A[i,k+1] - l_i R[k+1]) + A[i,k+2:n].l - l_i (R[k+2:n].l)
+//             with both dot products in FP64 (FP32 partial sums of at most 16 terms, added in
+//             FP64).  Warp 0 then publishes step k+1 while warps 1-7 apply the rank-1 row
+//             update to the other own rows; warp 0 updates the candidate row last and returns
+//             to polling.
+// At the end every CTA writes its rows, in FP64, to their logical positions of `factors`:
+// the same layout as the plain form (H in the upper Hessenberg part, multipliers below).
+#include "internal.cuh"
+
+namespace lhl {
+
+constexpr int MT = 256;
+constexpr int MW = MT / 32;
+constexpr int MIX_FLUSH = 16;  // float4 iterations per lane before the FP32 partials go to FP64
+constexpr int MIX_RPC_MAX = 64;
+
+__device__ __forceinline__ void st_release_u64(unsigned long long* p, unsigned long long v)
+{
+    asm volatile("st.release.gpu.global.u64 [%0], %1;" ::"l"(p), "l"(v) : "memory");
+}
+
+__device__ __forceinline__ unsigned long long ld_acquire_u64(const unsigned long long* p)
+{
+    unsigned long long v;
+    asm volatile("ld.acquire.gpu.global.u64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
+    return v;
+}
+
+// header word: value bits << 32 | (step & 0xffff) << 16 | logical row (0 = none)
+__device__ __forceinline__ unsigned long long mix_pack(unsigned int step, int idx, float val)
+{
+    return ((unsigned long long)__float_as_uint(val) << 32) | ((unsigned long long)(step & 0xffffu) << 16) |
+           (unsigned long long)(idx & 0xffff);
+}
+
+// Better candidate: larger |v|; ties go to the lower logical row; row 0 = none.
+__device__ __forceinline__ bool mix_better(float v, int i, float bv, int bi)
+{
+    if (i == 0) return false;
+    if (bi == 0) return true;
+    const float a = fabsf(v), b = fabsf(bv);
+    return a > b || (a == b && i < bi);
+}
+
+__device__ __forceinline__ void warp_best(float& bv, int& bi, int& bl)
+{
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        const float ov = __shfl_xor_sync(0xffffffffu, bv, o);
+        const int oi = __shfl_xor_sync(0xffffffffu, bi, o), ol = __shfl_xor_sync(0xffffffffu, bl, o);
+        if (mix_better(ov, oi, bv, bi)) { bv = ov; bi = oi; bl = ol; }
+    }
+}
+
+// x[c0..ldr) . l[c0..ldr) with FP64 accumulation of FP32 partials (warp-collective; pads of
+// x and l beyond n are zero).  The unaligned head c0..c4-1 is summed by the first lanes.
+__device__ __forceinline__ double mix_dot(const float* __restrict__ x, const float* __restrict__ l, int c0, int ldr,
+                                          int lane)
+{
+    const int c4 = (c0 + 3) & ~3;
+    double acc = 0.0;
+    if (c0 + lane < c4 && c0 + lane < ldr) acc = (double)(x[c0 + lane] * l[c0 + lane]);
+    const float4* x4 = reinterpret_cast<const float4*>(x);
+    const float4* l4 = reinterpret_cast<const float4*>(l);
+    float p0 = 0.f, p1 = 0.f, p2 = 0.f, p3 = 0.f;
+    int it = 0;
+    for (int g = (c4 >> 2) + lane; g < (ldr >> 2); g += 32) {
+        const float4 a = x4[g], b = l4[g];
+        p0 = fmaf(a.x, b.x, p0);
+        p1 = fmaf(a.y, b.y, p1);
+        p2 = fmaf(a.z, b.z, p2);
+        p3 = fmaf(a.w, b.w, p3);
+        if (++it == MIX_FLUSH) {
+            acc += ((double)p0 + (double)p1) + ((double)p2 + (double)p3);
+            p0 = p1 = p2 = p3 = 0.f;
+            it = 0;
+        }
+    }
+    acc += ((double)p0 + (double)p1) + ((double)p2 + (double)p3);
+    return warp_sum(acc);
+}
+
+// r[c] -= li * R[c] for c in [c0, ldr) (0-based), warp-collective; pads stay zero.
+__device__ __forceinline__ void mix_axpy(float* __restrict__ r, const float* __restrict__ R, float li, int c0, int ldr,
+                                         int lane)
+{
+    const int c4 = (c0 + 3) & ~3;
+    if (c0 + lane < c4 && c0 + lane < ldr) r[c0 + lane] = fmaf(-li, R[c0 + lane], r[c0 + lane]);
+    float4* r4 = reinterpret_cast<float4*>(r);
+    const float4* R4 = reinterpret_cast<const float4*>(R);
+    for (int g = (c4 >> 2) + lane; g < (ldr >> 2); g += 32) {
+        float4 a = r4[g];
+        const float4 b = R4[g];
+        a.x = fmaf(-li, b.x, a.x);
+        a.y = fmaf(-li, b.y, a.y);
+        a.z = fmaf(-li, b.z, a.z);
+        a.w = fmaf(-li, b.w, a.w);
+        r4[g] = a;
+    }
+}
+
+template <bool SROWS>
+__global__ void __launch_bounds__(MT, 1) reduce_mixed_kernel(MixArgs a)
+{
+    extern __shared__ __align__(16) float smx[];
+    __shared__ double s_dot[MIX_RPC_MAX + 1];
+    __shared__ float s_li[MIX_RPC_MAX];
+    __shared__ int s_win, s_p, s_ok, s_cand;
+    __shared__ float s_piv;
+
+    const int n = a.n, rpc = a.rpc, ldr = a.ldr, G = gridDim.x, b = blockIdx.x;
+    const int t = threadIdx.x, lane = t & 31, warp = t >> 5;
+    const int r0 = b * rpc;
+    const int nr = min(rpc, n - r0);
+    float* R = smx;                      // pivot row, logical column c at R[c-1]; pads zero
+    float* lv = R + ldr;                 // multipliers by logical row; pads zero
+    int* lg = (int*)(lv + ldr);          // physical -> logical (1-based)
+    int* ph = lg + ldr;                  // logical (1-based) -> physical, ph[0] unused
+    float* rows = SROWS ? (float*)(ph + ldr + 4) : a.grows + (size_t)r0 * ldr;  // nr x ldr
+    unsigned long long* hdr = a.hdr;
+
+    // ---- load own rows (FP64 -> FP32, zero pads), labels ----
+    for (int e = t; e < nr * ldr; e += MT) {
+        const int i = e % nr, c = e / nr;
+        rows[(size_t)i * ldr + c] = c < n ? (float)a.A[(size_t)c * n + r0 + i] : 0.f;
+    }
+    for (int q = t; q < ldr; q += MT) {
+        R[q] = 0.f;
+        lv[q] = 0.f;
+        if (q < n) {
+            lg[q] = q + 1;
+            ph[q + 1] = q;
+        }
+    }
+    for (int i = t; i < nr; i += MT) s_li[i] = 0.f;
+    __syncthreads();
+
+    // ---- publish step 1: column 1 values, candidate among logical rows >= 2 ----
+    if (warp == 0) {
+        float bv = 0.f;
+        int bi = 0, bl = -1;
+        for (int i = lane; i < nr; i += 32) {
+            const int L = r0 + i + 1;
+            const float v = rows[(size_t)i * ldr];
+            __stcg(&a.cval[(1 & 1) * n + r0 + i], v);
+            if (L >= 2 && mix_better(v, L, bv, bi)) { bv = v; bi = L; bl = i; }
+        }
+        warp_best(bv, bi, bl);
+        if (bl >= 0) {
+            const float4* src = reinterpret_cast<const float4*>(rows + (size_t)bl * ldr);
+            float4* dst = reinterpret_cast<float4*>(a.crow + ((size_t)(1 & 1) * G + b) * ldr);
+            for (int g = lane; g < (ldr >> 2); g += 32) __stcg(&dst[g], src[g]);
+        }
+        __syncwarp();
+        if (lane == 0) st_release_u64(&hdr[(1 & 1) * G + b], mix_pack(1u, bi, bv));
+    }
+
+    const uint64_t t_start = globaltimer_ns();
+    // CTA 0's time per sub-phase, summed over steps (probe slots 0-4: wait and pivot choice,
+    // interchange and loads, dot products and new column, publication, row update)
+    unsigned long long* probe = (b == 0 && t == 0 && a.ptimes) ? a.ptimes + 8 : nullptr;
+    uint64_t tp = t_start;
+    auto mark = [&](int slot) {
+        if (probe) {
+            const uint64_t now = globaltimer_ns();
+            probe[slot] += now - tp;
+            tp = now;
+        }
+    };
+    for (int k = 1; k <= n - 2; ++k) {
+        const int par = k & 1;
+        // ---- wait for step k from every CTA; pick the pivot; relabel ----
+        if (warp == 0) {
+            const unsigned long long* H = hdr + par * G;
+            const unsigned want = (unsigned)k & 0xffffu;
+            unsigned long long hv[5];  // G <= 160
+            unsigned pending = 0;
+            {
+                int q = 0;
+                for (int s = lane; s < G; s += 32, ++q) pending |= 1u << q;
+            }
+            const uint64_t t0 = globaltimer_ns();
+            unsigned spins = 0;
+            int ok = 1;
+            for (;;) {
+#pragma unroll
+                for (int qq = 0; qq < 5; ++qq) {
+                    const int s = lane + 32 * qq;
+                    if (s < G && ((pending >> qq) & 1u)) {
+                        const unsigned long long v = ld_acquire_u64(&H[s]);
+                        hv[qq] = v;
+                        if (((unsigned)(v >> 16) & 0xffffu) == want) pending &= ~(1u << qq);
+                    }
+                }
+                if (__all_sync(0xffffffffu, pending == 0)) break;
+                if ((++spins & 15u) == 0) {
+                    int bad = 0;
+                    if (lane == 0) {
+                        if (ld_acquire_i32(a.err) != 0) bad = 1;
+                        else if (globaltimer_ns() - t0 > a.limit_ns) {
+                            atomicCAS(a.err, 0, (int)LHL_ERR_TIMEOUT);
+                            bad = 1;
+                        }
+                    }
+                    if (__shfl_sync(0xffffffffu, bad, 0)) { ok = 0; break; }
+                }
+            }
+            float bv = 0.f;
+            int bi = 0, bs = -1;
+            if (ok) {
+#pragma unroll
+                for (int qq = 0; qq < 5; ++qq) {
+                    const int s = lane + 32 * qq;
+                    if (s < G) {
+                        const int i = (int)(hv[qq] & 0xffffu);
+                        const float v = __uint_as_float((unsigned)(hv[qq] >> 32));
+                        if (mix_better(v, i, bv, bi)) { bv = v; bi = i; bs = s; }
+                    }
+                }
+                warp_best(bv, bi, bs);
+            }
+            if (lane == 0) {
+                s_ok = ok;
+                const int p = (ok && bs >= 0 && bi >= k + 1 && bi <= n) ? bi : k + 1;
+                s_p = p;
+                s_win = (ok && bs >= 0 && bi >= k + 1 && bi <= n) ? bs : -1;
+                s_piv = s_win >= 0 ? bv : 0.f;
+                if (ok) {
+                    if (b == 0) a.ipiv[k - 1] = p;
+                    if (p != k + 1) {
+                        const int x = ph[k + 1], w = ph[p];
+                        ph[k + 1] = w;
+                        ph[p] = x;
+                        lg[w] = k + 1;
+                        lg[x] = p;
+                    }
+                }
+            }
+        }
+        __syncthreads();
+        if (!s_ok) return;
+        mark(0);
+        const int p = s_p;
+        const int win = s_win;
+        const float piv = s_piv;
+
+        // ---- interchange own columns; pivot row and multipliers (one L2 round trip) ----
+        if (p != k + 1)
+            for (int i = t; i < nr; i += MT) {
+                float* ri = rows + (size_t)i * ldr;
+                const float u = ri[k];
+                ri[k] = ri[p - 1];
+                ri[p - 1] = u;
+            }
+        {
+            const float* src = win >= 0 ? a.crow + ((size_t)par * G + win) * ldr : nullptr;
+            const float* cv = a.cval + (size_t)par * n;
+            for (int base = 0; base < n; base += 4 * MT) {
+                float rv[4], cvv[4];
+#pragma unroll
+                for (int u = 0; u < 4; ++u) {
+                    const int c = k + 1 + base + t + u * MT;  // logical column of R
+                    const int sc = c == k + 1 ? p : (c == p ? k + 1 : c);
+                    rv[u] = (src && c <= n) ? __ldcg(&src[sc - 1]) : 0.f;
+                    const int q = base + t + u * MT;
+                    cvv[u] = q < n ? __ldcg(&cv[q]) : 0.f;
+                }
+#pragma unroll
+                for (int u = 0; u < 4; ++u) {
+                    const int c = k + 1 + base + t + u * MT;
+                    if (c <= n) R[c - 1] = rv[u];
+                    const int q = base + t + u * MT;
+                    if (q < n) {
+                        const int j = lg[q];
+                        if (j >= k + 2) lv[j - 1] = piv != 0.f ? cvv[u] / piv : 0.f;
+                    }
+                }
+            }
+        }
+        __syncthreads();
+        mark(1);
+
+        // ---- dot products: own rows and the pivot row against l (FP64 accumulation) ----
+        for (int v = warp; v <= nr; v += MW) {
+            const float* x = v < nr ? rows + (size_t)v * ldr : R;
+            const double d = mix_dot(x, lv, k + 1, ldr, lane);
+            if (lane == 0) s_dot[v] = d;
+        }
+        __syncthreads();
+        // warp 0: new column k+1 of own rows, multipliers into column k, the next candidate
+        if (warp == 0) {
+            float bv = 0.f;
+            int bi = 0, bl = -1;
+            const int np = (k + 1) & 1;
+            for (int i = lane; i < nr; i += 32) {
+                float* ri = rows + (size_t)i * ldr;
+                const int L = lg[r0 + i];
+                double cn;
+                float li = 0.f;
+                if (L >= k + 2) {
+                    li = lv[L - 1];
+                    const float a1 = fmaf(-li, R[k], ri[k]);
+                    cn = ((double)a1 + s_dot[i]) - (double)li * s_dot[nr];
+                    ri[k - 1] = li;
+                } else {
+                    cn = (double)ri[k] + s_dot[i];
+                }
+                const float c32 = (float)cn;
+                ri[k] = c32;
+                s_li[i] = li;
+                if (k + 1 <= n - 2) __stcg(&a.cval[(size_t)np * n + r0 + i], c32);
+                if (L >= k + 2 && mix_better(c32, L, bv, bi)) { bv = c32; bi = L; bl = i; }
+            }
+            warp_best(bv, bi, bl);
+            if (lane == 0) {
+                s_cand = bl;
+                s_piv = bv;
+                s_p = bi;
+            }
+        }
+        __syncthreads();
+        mark(2);
+        const int cl = s_cand;
+        if (warp == 0) {
+            // ---- publish step k+1, then the candidate row's own row update ----
+            if (k + 1 <= n - 2) {
+                const int np = (k + 1) & 1;
+                if (cl >= 0) {
+                    const float4* rc = reinterpret_cast<const float4*>(rows + (size_t)cl * ldr);
+                    const float4* R4 = reinterpret_cast<const float4*>(R);
+                    float4* dst = reinterpret_cast<float4*>(a.crow + ((size_t)np * G + b) * ldr);
+                    const float li = s_li[cl];
+                    for (int g = ((k + 1) >> 2) + lane; g < (ldr >> 2); g += 32) {
+                        float4 x = rc[g];
+                        const float4 y = R4[g];
+                        x.x = fmaf(-li, y.x, x.x);
+                        x.y = fmaf(-li, y.y, x.y);
+                        x.z = fmaf(-li, y.z, x.z);
+                        x.w = fmaf(-li, y.w, x.w);
+                        __stcg(&dst[g], x);
+                    }
+                }
+                __syncwarp();
+                if (lane == 0) st_release_u64(&hdr[np * G + b], mix_pack((unsigned)(k + 1), s_p, s_piv));
+            }
+            mark(3);
+            if (cl >= 0 && s_li[cl] != 0.f) mix_axpy(rows + (size_t)cl * ldr, R, s_li[cl], k + 1, ldr, lane);
+        } else {
+            // ---- rank-1 row update of the other own active rows ----
+            for (int v = warp - 1; v < nr; v += MW - 1) {
+                const float li = s_li[v];
+                if (v == cl || li == 0.f) continue;
+                mix_axpy(rows + (size_t)v * ldr, R, li, k + 1, ldr, lane);
+            }
+        }
+    }
+    __syncthreads();
+    if (b == 0 && t == 0 && a.ptimes) a.ptimes[6] += globaltimer_ns() - t_start;
+
+    // ---- write own rows to their logical positions (FP64) ----
+    for (int e = t; e < nr * n; e += MT) {
+        const int i = e % nr, c = e / nr;
+        a.A[(size_t)c * n + (lg[r0 + i] - 1)] = (double)rows[(size_t)i * ldr + c];
+    }
+}
+
+static size_t mixed_fixed_smem(int ldr) { return (size_t)ldr * 4 * sizeof(float) + 16 * sizeof(float); }
+
+void mixed_plan(int n, int sms, MixPlan* pl)
+{
+    memset(pl, 0, sizeof(*pl));
+    if (n < 3 || sms <= 0) return;
+    if (sms > 160) sms = 160;
+    const int rpc = (n + sms - 1) / sms;
+    pl->rpc = rpc;
+    pl->grid = (n + rpc - 1) / rpc;
+    pl->ldr = (n + 3) & ~3;
+    const size_t fixed = mixed_fixed_smem(pl->ldr);
+    const size_t srows = (size_t)rpc * pl->ldr * sizeof(float);
+    pl->smem_rows = fixed + srows <= MIX_SMEM_MAX;
+    pl->smem = pl->smem_rows ? fixed + srows : fixed;
+    pl->ok = rpc <= MIX_RPC_MAX && fixed <= MIX_SMEM_MAX && n <= 16384;
+}
+
+cudaError_t launch_reduce_mixed(MixArgs a, const MixPlan& pl, cudaStream_t st)
+{
+    if (!pl.ok) return cudaErrorInvalidValue;
+    a.rpc = pl.rpc;
+    a.ldr = pl.ldr;
+    static size_t attr[2] = {0, 0};
+    const void* fn = pl.smem_rows ? (const void*)reduce_mixed_kernel<true> : (const void*)reduce_mixed_kernel<false>;
+    if (pl.smem > 48 * 1024 && pl.smem > attr[pl.smem_rows]) {
+        cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)pl.smem);
+        if (e != cudaSuccess) return e;
+        attr[pl.smem_rows] = pl.smem;
+    }
+    void* args[] = {&a};
+    return cudaLaunchCooperativeKernel(fn, dim3(pl.grid), dim3(MT), args, pl.smem, st);
+}
+
+}  // namespace lhl

@@ -87,12 +87,30 @@ __device__ void hess_solve(const LdivArgs& a, const double* Gt, const uint8_t* s
         y[n - 1] = c;
     }
     __syncthreads();
-    // back substitution in blocks of 32 rows from the bottom
+    // back substitution in blocks of 32 rows from the bottom, left-looking: the block's
+    // sums over the rows already solved are dot products with columns of Gt (column j of Gt
+    // is row j of U, contiguous), one warp per column, coalesced.  The same warp stages the
+    // block's part of that column (U[j, r0..r1]) in shared memory, and warp 0 then solves
+    // the 32 x 32 triangle from there.
+    __shared__ double tri[BS][BS + 1];
+    double* sj = sm;  // block partial sums (the multiplier copy in sm is no longer needed)
+    const int nwarps = SOLVE_T / 32;
     for (int r1 = n; r1 >= 1; r1 -= BS) {
         const int r0 = max(r1 - BS + 1, 1);
+        const int bs = r1 - r0 + 1;
+        for (int jj = warp; jj < bs; jj += nwarps) {
+            const int j = r0 + jj;
+            const double* g = Gt + (size_t)(j - 1) * a.ldg;  // Gt column j = row j of U
+            if (r0 + lane <= r1) tri[jj][lane] = g[r0 + lane - 1];  // U[j, r0 + lane]
+            double acc = 0.0;
+            for (int i = r1 + 1 + lane; i <= n; i += 32) acc = dfma(g[i - 1], y[i - 1], acc);
+            acc = warp_sum(acc);
+            if (lane == 0) sj[jj] = acc;
+        }
+        __syncthreads();
         if (warp == 0) {
             const int i = r0 + lane;
-            double yi = (i <= r1) ? y[i - 1] : 0.0;
+            double yi = (i <= r1) ? y[i - 1] - sj[lane] : 0.0;
             for (int j = r1; j >= r0; --j) {
                 double xj = 0.0;
                 if (i == j) {
@@ -100,16 +118,9 @@ __device__ void hess_solve(const LdivArgs& a, const double* Gt, const uint8_t* s
                     xj = yi;
                 }
                 xj = __shfl_sync(0xffffffffu, xj, j - r0);
-                if (i < j && i >= r0) yi = dfma(-M1(Gt, a.ldg, j, i), xj, yi);
+                if (i < j && i >= r0) yi = dfma(-tri[lane][j - r0], xj, yi);  // U[i, j]
             }
             if (i <= r1) y[i - 1] = yi;
-        }
-        __syncthreads();
-        for (int i = 1 + t; i < r0; i += SOLVE_T) {
-            double v = y[i - 1];
-            const double* g = Gt + (size_t)(i - 1) * a.ldg;  // Gt column i = row i of U
-            for (int j = r0; j <= r1; ++j) v = dfma(-g[j - 1], y[j - 1], v);
-            y[i - 1] = v;
         }
         __syncthreads();
     }
@@ -123,6 +134,7 @@ __global__ void __launch_bounds__(SOLVE_T) ldiv_kernel(LdivArgs a)
     double* y2 = smem + n;
     uint8_t* ssw = (uint8_t*)(smem + 2 * n);
     const int col = blockIdx.x;
+    if (a.done && a.done[col] <= a.tol) return;  // converged column (refinement to a tolerance)
     double* x = a.X + (size_t)col * a.ldx;
     const int t = threadIdx.x;
 
@@ -153,13 +165,14 @@ cudaError_t launch_ldiv(const LdivArgs& a, int nrhs, cudaStream_t st)
 {
     if (nrhs <= 0 || a.n <= 0) return cudaSuccess;
     const size_t smem = (size_t)a.n * 2 * sizeof(double) + (size_t)a.n + 16;
-    static bool attr = false;
-    if (!attr) {
-        cudaError_t e = cudaFuncSetAttribute(ldiv_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 220 * 1024);
+    // dynamic + static shared memory must stay within the 227 KB a CTA may use
+    if (smem > 200 * 1024) return cudaErrorInvalidValue;
+    static size_t attr = 0;
+    if (smem > 48 * 1024 && smem > attr) {
+        cudaError_t e = cudaFuncSetAttribute(ldiv_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
         if (e != cudaSuccess) return e;
-        attr = true;
+        attr = smem;
     }
-    if (smem > 220 * 1024) return cudaErrorInvalidValue;
     ldiv_kernel<<<nrhs, SOLVE_T, smem, st>>>(a);
     return cudaGetLastError();
 }
@@ -223,18 +236,21 @@ cudaError_t launch_residual(int n, const double* J, int ldj, const double* B, in
     return cudaGetLastError();
 }
 
-__global__ void axpy_cols_kernel(int n, double* __restrict__ X, int ldx, const double* __restrict__ R, int ldr)
+__global__ void axpy_cols_kernel(int n, double* __restrict__ X, int ldx, const double* __restrict__ R, int ldr,
+                                 const double* __restrict__ done, double tol)
 {
     const int c = blockIdx.y;
+    if (done && done[c] <= tol) return;
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
         X[(size_t)c * ldx + i] += R[(size_t)c * ldr + i];
 }
 
-cudaError_t launch_axpy_cols(int n, double* X, int ldx, const double* R, int ldr, int nrhs, cudaStream_t st)
+cudaError_t launch_axpy_cols(int n, double* X, int ldx, const double* R, int ldr, int nrhs, cudaStream_t st,
+                             const double* done, double tol)
 {
     if (nrhs <= 0 || n <= 0) return cudaSuccess;
     dim3 grid((n + 255) / 256 < 64 ? (n + 255) / 256 : 64, nrhs);
-    axpy_cols_kernel<<<grid, 256, 0, st>>>(n, X, ldx, R, ldr);
+    axpy_cols_kernel<<<grid, 256, 0, st>>>(n, X, ldx, R, ldr, done, tol);
     return cudaGetLastError();
 }
 

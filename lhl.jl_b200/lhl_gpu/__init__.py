@@ -77,6 +77,7 @@ def _load():
         "lhl_shift": [vp, vp, i64, d, d, vp],
         "lhl_ldiv": [vp, vp, vp, i64, i64, i64, vp],
         "lhl_refine": [vp, vp, vp, i64, vp, i64, vp, i64, vp, i64, i64, i32, vp],
+        "lhl_refine_tol": [vp, vp, vp, i64, vp, i64, vp, i64, vp, vp, i64, i64, d, i32, vp],
         "lhl_residual_norms": [vp, vp, i64, vp, i64, vp, i64, vp, vp, i64, i64, vp],
         "lhl_applyZ": [vp, vp, i64, i64, vp],
         "lhl_applyZinv": [vp, vp, i64, i64, vp],
@@ -437,6 +438,36 @@ def lhl_refine_(x: torch.Tensor, J: torch.Tensor, b: torch.Tensor, *args, steps:
     return x
 
 
+def lhl_refine_tol_(x: torch.Tensor, J: torch.Tensor, b: torch.Tensor, sh: LHLShift, ws: LHLWorkspace,
+                    tol: float = 1e-10, max_steps: int = 8, rhs_per_shift: int = 1, R: torch.Tensor = None,
+                    res: torch.Tensor = None, stream=None) -> torch.Tensor:
+    """Refinement to a tolerance (lhl_refine_tol of the C ABI): up to `max_steps` steps of
+    ``lhl_refine!`` (F:3144-3157); columns already at relative residual <= tol are skipped on
+    the device.  Returns the per-column final relative residuals (device tensor); x is updated
+    in place.  `R` (n x k scratch) and `res` (k) may be passed to avoid allocation."""
+    for t, nm in ((x, "x"), (J, "J"), (b, "b")):
+        _require_cuda_f64(t, nm)
+    n = ws.n
+    xx, k, ldx = _as_cols(x, n)
+    bb, kb, ldb = _as_cols(b, n)
+    if kb != k:
+        raise DimensionMismatch("x and b differ in column count")
+    if ldx != n:
+        raise ArgumentError("x must have leading dimension n")
+    Jc = _colmajor(J)
+    if R is None:
+        R = torch.empty((k, n), dtype=torch.float64, device=x.device)
+    if res is None:
+        res = torch.empty(k, dtype=torch.float64, device=x.device)
+    if R.numel() < n * k or res.numel() < k:
+        raise DimensionMismatch("scratch too small")
+    _check(_lib.lhl_refine_tol(sh._h, ws._h, C.c_void_p(Jc.data_ptr()), max(Jc.stride(1), n),
+                               C.c_void_p(bb.data_ptr()), ldb, C.c_void_p(xx.data_ptr()), ldx,
+                               C.c_void_p(R.data_ptr()), C.c_void_p(res.data_ptr()), k, int(rhs_per_shift),
+                               float(tol), int(max_steps), _stream(stream)), "lhl_refine_tol")
+    return res
+
+
 def residual_norms(sh: LHLShift, J: torch.Tensor, b: torch.Tensor, x: torch.Tensor, rhs_per_shift: int = 1,
                    stream=None) -> torch.Tensor:
     """||b - (sigma I + tau J) x||_2 / ||b||_2 per column, on the device."""
@@ -474,5 +505,6 @@ def version() -> str:
 
 
 __all__ = ["LHLWorkspace", "LHLShift", "lhl", "lhl_", "lhl_reduce_", "lhl_shift_", "lhl_shift_batched_",
+           "lhl_refine_tol_",
            "lhl_ldiv_", "lhl_refine_", "applyZ_", "applyZinv_", "residual_norms", "ArgumentError",
            "DimensionMismatch", "LHLDeviceError", "LHL_PREC_FP64", "LHL_PREC_MIXED", "version", "lib"]

@@ -4,6 +4,7 @@
     python lhl.jl_b200/profile_case.py --n 2048 --what chain --shifts 64 --reps 3
 
 --what reduce: lhl_reduce (balance + reduction + Ht/perm) of an N(0,1) matrix.
+--precision mixed: the mixed form's FP32 reduction (workspace LHL_PREC_MIXED).
 --what chain:  one reduction, then per repetition the batched shift LUs, the solves and one
                refinement step for `--shifts` shifts (1, -g) with one right-hand side each.
 Prints the CUDA-event time of each repetition."""
@@ -30,11 +31,12 @@ def main():
     ap.add_argument("--shifts", type=int, default=64)
     ap.add_argument("--reps", type=int, default=3)
     ap.add_argument("--seed", type=int, default=2)
+    ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed"])
     args = ap.parse_args()
     n = args.n
     rng = np.random.default_rng(args.seed)
     J = torch.as_tensor(np.asfortranarray(rng.standard_normal((n, n)))).cuda()
-    ws = G.LHLWorkspace(n)
+    ws = G.LHLWorkspace(n, G.LHL_PREC_MIXED if args.precision == "mixed" else G.LHL_PREC_FP64)
     ev = lambda: torch.cuda.Event(enable_timing=True)  # noqa: E731
     if args.what == "reduce":
         for r in range(args.reps):
@@ -44,7 +46,7 @@ def main():
             b.record()
             torch.cuda.synchronize()
             ws.check()
-            print(f"reduce n={n} rep={r} ms={a.elapsed_time(b):.3f}", flush=True)
+            print(f"reduce n={n} {args.precision} rep={r} ms={a.elapsed_time(b):.3f}", flush=True)
         return
     S = args.shifts
     G.lhl_reduce_(ws, J, True)
