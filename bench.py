@@ -2,9 +2,11 @@
 
 Workload (config 2): J 2048x2048 FP64 N(0,1); 64 shifts (1, -g), g log-uniform in
 [1e-4, 1e-1]; one N(0,1) right-hand side per shift.  One step = the whole path on one
-batch: reduction J = Z H Z^-1 (balance + blocked ELMHES), 64 shift LUs, 64 solves and one
-refinement step each (every solve ends at <= 1e-10 relative residual; checked after the
-timed region).  value = 64 solves / step time.
+batch: reduction J = Z H Z^-1, 64 shift LUs, 64 solves, then FP64 refinement until every
+solve is at <= 1e-10 relative residual (lhl_refine_tol; the final residuals are checked
+after the timed region).  value = 64 solves / step time of the mixed form (FP32 reduction);
+the plain FP64 form (bit-identical to the reference's operation order) is timed the same
+way and reported beside it, with the ratio.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
 
@@ -111,6 +113,58 @@ def cpu_reference_run(cfg, steps, warmup, threads_note):
     return times, X
 
 
+def time_events(stream, fn, reps, flush):
+    out = []
+    for k in range(reps):
+        flush.fill_(float(k))
+        import torch
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        fn()
+        b.record(stream)
+        torch.cuda.synchronize()
+        out.append(a.elapsed_time(b))
+    return float(np.mean(out))
+
+
+class Form:
+    """One form of the path on the device: the workspace, the shift batch and one step."""
+
+    def __init__(self, G, torch, precision, n, S, dev, max_steps):
+        self.G, self.torch = G, torch
+        self.precision = precision
+        self.ws = G.LHLWorkspace(n, precision)
+        self.sh = G.LHLShift(n, S)
+        self.X = torch.empty((S, n), dtype=torch.float64, device=dev).t()
+        self.Rs = torch.empty((S, n), dtype=torch.float64, device=dev)
+        self.res = torch.empty(S, dtype=torch.float64, device=dev)
+        self.max_steps = max_steps
+
+    def reduce(self, Jd):
+        self.G.lhl_reduce_(self.ws, Jd, True)
+
+    def chain(self, Jd, Bd, sig, tau):
+        G = self.G
+        G.lhl_shift_batched_(self.sh, self.ws, sig, tau)
+        self.X.copy_(Bd)
+        G.lhl_ldiv_(self.X, self.sh, self.ws)
+        G.lhl_refine_tol_(self.X, Jd, Bd, self.sh, self.ws, tol=TOL, max_steps=self.max_steps, R=self.Rs,
+                          res=self.res)
+
+    def step(self, Jd, Bd, sig, tau):
+        self.reduce(Jd)
+        self.chain(Jd, Bd, sig, tau)
+
+    def launches(self):
+        red = 5 if self.precision == self.G.LHL_PREC_MIXED else 4   # init, [balance,] coop, Ht, perm
+        return red + 1 + 1 + 4 * self.max_steps + 2                 # shift LU, ldiv, refinement steps, final check
+
+
+TOL = 1e-10
+MIXED_MAX_STEPS = 16
+PLAIN_MAX_STEPS = 2
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -125,9 +179,12 @@ def main():
     from lhl_gpu import configs
     cfg = configs.config2()
     n, S = cfg["n"], len(cfg["sigma"])
-    config = {"workload": "c2: J 2048x2048 FP64 N(0,1), 64 shifts (1,-g) g log-uniform [1e-4,1e-1], 1 RHS/shift, "
-                          "reduction + shift LU + ldiv + 1 refinement per step",
-              "n": n, "shifts": S, "rhs_per_shift": 1, "refine_steps": cfg["steps"], "form": "plain FP64",
+    config = {"workload": "c2: J 2048x2048 FP64 N(0,1), 64 shifts (1,-g) g log-uniform [1e-4,1e-1], 1 RHS/shift; "
+                          "one step = reduction + 64 shift LUs + 64 solves + refinement until every solve is at "
+                          "<= 1e-10 relative residual",
+              "n": n, "shifts": S, "rhs_per_shift": 1, "tolerance": TOL,
+              "form": "mixed: FP32 reduction (FP64-accumulated column updates), FP64 balancing, shift LU, solves, "
+                      "residuals and refinement",
               "l2": "flushed between timed steps (256 MiB write)", "replicas": world}
 
     if args.impl == "reference":
@@ -143,7 +200,8 @@ def main():
                 "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (numpy PCG64 seeds 2,3,4)",
                 "config": config,
                 "cpu_baseline": {"value": val, "unit": UNIT, "cores": threads, "kind": "port",
-                                 "sample": f"{len(times)} full step(s) of the workload: oracle C restatement, OpenMP"},
+                                 "sample": f"{len(times)} full step(s) of the workload (FP64 reduction + 64 shift "
+                                           f"LUs + solves + 1 refinement): oracle C restatement, OpenMP"},
                 "e2e": {"value": val, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
         print(json.dumps(line), flush=True)
         return
@@ -165,78 +223,67 @@ def main():
     Bd = torch.as_tensor(cfg["B"]).to(dev)
     sig = torch.as_tensor(cfg["sigma"]).to(dev)
     tau = torch.as_tensor(cfg["tau"]).to(dev)
-    X = torch.empty_like(Bd)
-    ws = G.LHLWorkspace(n)
-    sh = G.LHLShift(n, S)
     flush = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.float32, device=dev)
+    mixed = Form(G, torch, G.LHL_PREC_MIXED, n, S, dev, MIXED_MAX_STEPS)
+    plain = Form(G, torch, G.LHL_PREC_FP64, n, S, dev, PLAIN_MAX_STEPS)
 
-    def step():
-        G.lhl_reduce_(ws, Jd, True)
-        G.lhl_shift_batched_(sh, ws, sig, tau)
-        X.copy_(Bd)
-        G.lhl_ldiv_(X, sh, ws)
-        G.lhl_refine_(X, Jd, Bd, sh, ws, cfg["steps"])
-
-    launches_per_step = 4 + 1 + 1 + 3 * cfg["steps"]  # reduce(init, coop, ht, perm), shift, ldiv, refine
-    for _ in range(max(args.warmup, 3)):
-        step()
-    torch.cuda.synchronize()
-    ws.check()
-
-    # ---- timed region: K steps, per-step events, L2 flushed between steps ----
-    evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
-    if pg:
-        pg.barrier()
-    torch.cuda.synchronize()
-    with ClockSampler(local) as clk:
-        for k in range(args.steps):
-            flush.fill_(float(k))
-            evs[k][0].record(stream)
-            step()
-            evs[k][1].record(stream)
+    def timed(form):
+        for _ in range(max(args.warmup, 3)):
+            form.step(Jd, Bd, sig, tau)
         torch.cuda.synchronize()
-    if pg:
-        pg.barrier()
-    ms = [a.elapsed_time(b) for a, b in evs]
-    ms_step = float(np.mean(ms))
-    ws.check()
-
-    # ---- accuracy of the timed work (outside the timed region) ----
-    res = G.residual_norms(sh, Jd, Bd, X).cpu().numpy()
-    assert (res <= 1e-10).all(), f"residual above 1e-10: {res.max()}"
-
-    # ---- dominant kernel: the reduction, timed alone (events on the launching stream) ----
-    red_ms = []
-    for k in range(max(3, min(args.steps, 10))):
-        flush.fill_(float(k))
-        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        a.record(stream)
-        G.lhl_reduce_(ws, Jd, True)
-        b.record(stream)
+        form.ws.check()
+        evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+        if pg:
+            pg.barrier()
         torch.cuda.synchronize()
-        red_ms.append(a.elapsed_time(b))
-    phase = {}
-    for name, fn in (("shift", lambda: G.lhl_shift_batched_(sh, ws, sig, tau)),
-                     ("ldiv", lambda: G.lhl_ldiv_(X, sh, ws)),
-                     ("refine", lambda: G.lhl_refine_(X, Jd, Bd, sh, ws, cfg["steps"]))):
-        tt = []
-        for k in range(3):
-            flush.fill_(float(k))
-            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-            a.record(stream)
-            fn()
-            b.record(stream)
+        with ClockSampler(local) as clk:
+            for k in range(args.steps):
+                flush.fill_(float(k))
+                evs[k][0].record(stream)
+                form.step(Jd, Bd, sig, tau)
+                evs[k][1].record(stream)
             torch.cuda.synchronize()
-            tt.append(a.elapsed_time(b))
-        phase[name] = float(np.mean(tt))
-    red = float(np.mean(red_ms))
-    phase["reduce"] = red
-    phase["reduce_inside_ms"] = {k: v / 1e6 for k, v in ws.phase_ns().items()}
-    alg_bytes = 8.0 * (n ** 3) / 3.0 + 16.0 * n * n   # GEMV stream (8 n^3/3) + J in, Ht/L out
+        if pg:
+            pg.barrier()
+        form.ws.check()
+        ms = float(np.mean([a.elapsed_time(b) for a, b in evs]))
+        # every solve of the timed work is at <= 1e-10 (final residuals from the refinement)
+        res = form.res.cpu().numpy()
+        assert (res <= TOL).all(), f"residual above {TOL}: {res.max()}"
+        return ms, clk.summary(), float(res.max())
+
+    ms_mixed, clk_mixed, res_mixed = timed(mixed)
+    ms_plain, clk_plain, res_plain = timed(plain)
+
+    # ---- phases, each timed alone with events on the launching stream ----
+    def phases(form):
+        ph = {"reduce": time_events(stream, lambda: form.reduce(Jd), 5, flush),
+              "chain": time_events(stream, lambda: form.chain(Jd, Bd, sig, tau), 3, flush)}
+        ph["shift"] = time_events(stream, lambda: G.lhl_shift_batched_(form.sh, form.ws, sig, tau), 3, flush)
+        ph["ldiv"] = time_events(stream, lambda: G.lhl_ldiv_(form.X, form.sh, form.ws), 3, flush)
+        return ph
+
+    ph_mixed = phases(mixed)
+    ph_plain = phases(plain)
+    # refinement steps the mixed form needed (per column), from a fixed-step replay on the host side
+    G.lhl_shift_batched_(mixed.sh, mixed.ws, sig, tau)
+    X0 = Bd.clone()
+    G.lhl_ldiv_(X0, mixed.sh, mixed.ws)
+    need = np.full(S, -1)
+    for st in range(MIXED_MAX_STEPS + 1):
+        Xs = X0.clone()
+        r = G.lhl_refine_tol_(Xs, Jd, Bd, mixed.sh, mixed.ws, tol=0.0, max_steps=st).cpu().numpy()
+        need[(need < 0) & (r <= TOL)] = st
+        if (need >= 0).all():
+            break
+
+    # ---- roofline of the dominant kernel: the mixed reduction ----
+    alg_bytes = 4.0 * (n ** 3) / 3.0 + 16.0 * n * n   # FP32 GEMV stream (4 n^3/3) + J in, factors out (FP64)
     peak, peak_kind = peaks()
+    red = ph_mixed["reduce"]
     achieved = alg_bytes / (red * 1e-3) / 1e9
     traffic = None
-    tp = os.path.join(REPO, "profiles", "reduce_kernel_c2_n2048.md")
+    tp = os.path.join(REPO, "profiles", "reduce_mixed_kernel_c2_n2048.md")
     if os.path.exists(tp):
         for line in open(tp):
             if line.startswith("dram_bytes_per_launch:"):
@@ -260,36 +307,23 @@ def main():
         Jd2.copy_(Jh, non_blocking=True)
         Bd2.copy_(Bh, non_blocking=True)
         st2.copy_(sh_h, non_blocking=True)
-        G.lhl_reduce_(ws, Jd2, True)
-        G.lhl_shift_batched_(sh, ws, st2[0], st2[1])
-        X.copy_(Bd2)
-        G.lhl_ldiv_(X, sh, ws)
-        G.lhl_refine_(X, Jd2, Bd2, sh, ws, cfg["steps"])
-        Xh.copy_(X, non_blocking=True)
+        mixed.step(Jd2, Bd2, st2[0], st2[1])
+        Xh.copy_(mixed.X, non_blocking=True)
 
     for _ in range(2):
         e2e_step()
     torch.cuda.synchronize()
-    e_ms = []
-    for k in range(args.steps):
-        flush.fill_(float(k))
-        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        a.record(stream)
-        e2e_step()
-        b.record(stream)
-        torch.cuda.synchronize()
-        e_ms.append(a.elapsed_time(b))
-    e2e_ms = float(np.mean(e_ms))
+    e2e_ms = time_events(stream, e2e_step, args.steps, flush)
     h2d = Jh.numel() * 8 + Bh.numel() * 8 + sh_h.numel() * 8
     d2h = Xh.numel() * 8
 
     # ---- max over ranks ----
-    vals = torch.tensor([ms_step, e2e_ms], dtype=torch.float64, device=dev)
+    vals = torch.tensor([ms_mixed, ms_plain, e2e_ms], dtype=torch.float64, device=dev)
     if pg:
         pg.all_reduce(vals, op=pg.ReduceOp.MAX)
-    ms_step, e2e_ms = float(vals[0]), float(vals[1])
-    value = world * S / (ms_step * 1e-3)
-    e2e_value = world * S / (e2e_ms * 1e-3)
+    ms_mixed, ms_plain, e2e_ms = (float(v) for v in vals)
+    value = world * S / (ms_mixed * 1e-3)
+    plain_value = world * S / (ms_plain * 1e-3)
 
     if rank == 0:
         cpu = None
@@ -298,22 +332,31 @@ def main():
             times, Xc = cpu_reference_run(cfg, args.cpu_baseline_steps, 0, None)
             sec = float(np.mean(times))
             cpu = {"value": S / sec, "unit": UNIT, "cores": O.num_threads(), "kind": "port",
-                   "sample": f"{len(times)} full step(s) (reduction + 64 shift LUs + solves + 1 refinement), "
+                   "sample": f"{len(times)} full step(s) (FP64 reduction + 64 shift LUs + solves + 1 refinement), "
                              f"oracle C restatement with OpenMP, {sec:.2f} s/step"}
         line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
-                "warmup": max(args.warmup, 3), "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak",
-                "vs_baseline": None, "dtype": "f64", "data": "synthetic (numpy PCG64 seeds 2,3,4)",
-                "config": config,
-                "phases_ms": phase, "max_rel_residual": float(res.max()),
+                "warmup": max(args.warmup, 3), "ms_per_step": ms_mixed, "higher_is_better": True, "scaling": "weak",
+                "vs_baseline": None, "dtype": "f64 (mixed form: f32 reduction)",
+                "data": "synthetic (numpy PCG64 seeds 2,3,4)", "config": config,
+                "plain_fp64": {"value": plain_value, "unit": UNIT, "ms_per_step": ms_plain,
+                               "max_rel_residual": res_plain, "phases_ms": ph_plain,
+                               "form": "plain: FP64 throughout, bit-identical reduction and shift LUs",
+                               "clocks": clk_plain},
+                "mixed_vs_plain": value / plain_value,
+                "excluding_reduction": {"mixed": S / (ph_mixed["chain"] * 1e-3), "plain": S / (ph_plain["chain"] * 1e-3),
+                                        "unit": UNIT, "note": "S*R / T(shift + solve + refine), reduction excluded"},
+                "phases_ms": ph_mixed, "max_rel_residual": res_mixed,
+                "refine_steps_needed": {"max": int(need.max()), "mean": float(need.mean()),
+                                        "histogram": {int(k): int((need == k).sum()) for k in np.unique(need)}},
                 "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                              "frac": achieved / peak, "traffic": traffic, "peak_kind": peak_kind,
-                             "kernel": "reduce_kernel (balance + blocked ELMHES, one cooperative launch)",
+                             "kernel": "lhl_reduce, mixed form (balance + FP32 ELMHES, cooperative launches)",
                              "algorithmic_bytes": alg_bytes},
                 "cpu_baseline": cpu,
-                "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
-                        "ms_per_step": e2e_ms},
-                "gpu_launches": launches_per_step * args.steps,
-                "clocks": clk.summary()}
+                "e2e": {"value": world * S / (e2e_ms * 1e-3), "unit": UNIT, "h2d_bytes_per_step": h2d,
+                        "d2h_bytes_per_step": d2h, "ms_per_step": e2e_ms},
+                "gpu_launches": mixed.launches() * args.steps,
+                "clocks": clk_mixed}
         print(json.dumps(line), flush=True)
     if pg:
         pg.destroy_process_group()

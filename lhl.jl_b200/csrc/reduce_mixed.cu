@@ -42,12 +42,16 @@ __device__ __forceinline__ void st_release_u64(unsigned long long* p, unsigned l
     asm volatile("st.release.gpu.global.u64 [%0], %1;" ::"l"(p), "l"(v) : "memory");
 }
 
-__device__ __forceinline__ unsigned long long ld_acquire_u64(const unsigned long long* p)
+// Polling load: relaxed, so that a lane's loads of several headers are in flight together;
+// the poll ends with one acquire fence.
+__device__ __forceinline__ unsigned long long ld_relaxed_u64(const unsigned long long* p)
 {
     unsigned long long v;
-    asm volatile("ld.acquire.gpu.global.u64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
+    asm volatile("ld.relaxed.gpu.global.u64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
     return v;
 }
+
+__device__ __forceinline__ void fence_acq_rel_gpu() { asm volatile("fence.acq_rel.gpu;" ::: "memory"); }
 
 // header word: value bits << 32 | (step & 0xffff) << 16 | logical row (0 = none)
 __device__ __forceinline__ unsigned long long mix_pack(unsigned int step, int idx, float val)
@@ -192,6 +196,7 @@ __global__ void __launch_bounds__(MT, 1) reduce_mixed_kernel(MixArgs a)
     };
     for (int k = 1; k <= n - 2; ++k) {
         const int par = k & 1;
+        mark(4);
         // ---- wait for step k from every CTA; pick the pivot; relabel ----
         if (warp == 0) {
             const unsigned long long* H = hdr + par * G;
@@ -210,7 +215,7 @@ __global__ void __launch_bounds__(MT, 1) reduce_mixed_kernel(MixArgs a)
                 for (int qq = 0; qq < 5; ++qq) {
                     const int s = lane + 32 * qq;
                     if (s < G && ((pending >> qq) & 1u)) {
-                        const unsigned long long v = ld_acquire_u64(&H[s]);
+                        const unsigned long long v = ld_relaxed_u64(&H[s]);
                         hv[qq] = v;
                         if (((unsigned)(v >> 16) & 0xffffu) == want) pending &= ~(1u << qq);
                     }
@@ -228,6 +233,7 @@ __global__ void __launch_bounds__(MT, 1) reduce_mixed_kernel(MixArgs a)
                     if (__shfl_sync(0xffffffffu, bad, 0)) { ok = 0; break; }
                 }
             }
+            fence_acq_rel_gpu();  // the CTAs' column values and rows are read after this
             float bv = 0.f;
             int bi = 0, bs = -1;
             if (ok) {

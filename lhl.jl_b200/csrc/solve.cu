@@ -168,7 +168,7 @@ cudaError_t launch_ldiv(const LdivArgs& a, int nrhs, cudaStream_t st)
     // dynamic + static shared memory must stay within the 227 KB a CTA may use
     if (smem > 200 * 1024) return cudaErrorInvalidValue;
     static size_t attr = 0;
-    if (smem > 48 * 1024 && smem > attr) {
+    if (smem > 32 * 1024 && smem > attr) {  // the kernel's static shared arrays add about 8.5 KB
         cudaError_t e = cudaFuncSetAttribute(ldiv_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
         if (e != cudaSuccess) return e;
         attr = smem;
