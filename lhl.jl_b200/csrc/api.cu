@@ -17,6 +17,8 @@ struct lhl_ws_s {
     unsigned int* bar;
     unsigned long long limit_ns;
     unsigned long long* ptimes;
+    double* ybuf;  // ldiv scratch: n x ycap right-hand sides
+    int ycap;
     // mixed form (LHL_PREC_MIXED) only
     lhl::MixPlan mplan;
     unsigned long long* mhdr;
@@ -45,7 +47,7 @@ static void ws_free(lhl_ws_t w)
     if (!w) return;
     void* ptrs[] = {w->F, w->Ht, w->scale, w->iscale, w->B0, w->part, w->tab, w->cand_v, w->cand_s, w->buf2, w->tsnap,
                     w->bsum, w->bfac, w->ipiv, w->perm, w->iperm, w->cand_i, w->bflag, w->err, w->bar,
-                    w->ptimes, w->mhdr, w->mcval, w->mcrow, w->mgrows};
+                    w->ptimes, w->mhdr, w->mcval, w->mcrow, w->mgrows, w->ybuf};
     for (void* p : ptrs)
         if (p) cudaFree(p);
     delete w;
@@ -93,6 +95,8 @@ int lhl_ws_create(int64_t n, int precision, lhl_ws_t* out)
     A_(err, 4);
     A_(bar, 4);
     A_(ptimes, 24);
+    w->ycap = 256;
+    A_(ybuf, (size_t)n * w->ycap);
     if (precision == LHL_PREC_MIXED && n >= 3) {
         int dev = 0, sms = 0;
         if (e == cudaSuccess) e = cudaGetDevice(&dev);
@@ -366,6 +370,8 @@ static int ldiv_common(lhl_shift_t sh, lhl_ws_t ws, double* dX, int64_t ldx, int
     a.ldx = (int)ldx;
     a.mode = mode;
     a.rhs_per_shift = 1;
+    a.Y = ws->ybuf;
+    a.ycap = ws->ycap;
     if (sh) {
         a.Gt = sh->Gt;
         a.ldg = (int)sh->ldg;
@@ -462,6 +468,8 @@ int lhl_refine_tol(lhl_shift_t sh, lhl_ws_t ws, const double* dJ, int64_t ldj, c
         a.rhs_per_shift = (int)rhs_per_shift;
         a.done = dres;
         a.tol = tol;
+        a.Y = ws->ybuf;
+        a.ycap = ws->ycap;
         e = lhl::launch_ldiv(a, (int)nrhs, st);
         if (e == cudaSuccess) e = lhl::launch_axpy_cols((int)n, dX, (int)ldx, dR, (int)ldx, (int)nrhs, st, dres, tol);
         if (e != cudaSuccess) return LHL_ERR_CUDA;

@@ -52,6 +52,24 @@ struct LdivArgs {
     int mode;             // 0 ldiv, 1 applyZinv, 2 applyZ
     const double* done;   // optional: column c is skipped when done[c] <= tol
     double tol;
+    double* Y;            // ldiv scratch: n x ycap (the workspace's)
+    int ycap;
+};
+
+// One L sweep over a tile of right-hand sides (see solve.cu).
+struct ZArgs {
+    int n;
+    const double* F;
+    int ldf;
+    const int64_t* perm;
+    const double* scale;
+    const double* iscale;
+    const double* src;
+    int lds;
+    double* dst;
+    int ldd;
+    int m;       // right-hand sides
+    int gather;  // zinv: read x[perm[i]] * iscale[perm[i]]
 };
 
 // Mixed-precision reduction (see reduce_mixed.cu).
