@@ -19,6 +19,8 @@ struct lhl_ws_s {
     unsigned long long* ptimes;
     double* ybuf;  // ldiv scratch: n x ycap right-hand sides
     int ycap;
+    int* zflags;   // ldiv scratch: ready flags, ceil(n/64) x ceil(ycap/4)
+    int nzflags;
     // mixed form (LHL_PREC_MIXED) only
     lhl::MixPlan mplan;
     unsigned long long* mhdr;
@@ -47,7 +49,7 @@ static void ws_free(lhl_ws_t w)
     if (!w) return;
     void* ptrs[] = {w->F, w->Ht, w->scale, w->iscale, w->B0, w->part, w->tab, w->cand_v, w->cand_s, w->buf2, w->tsnap,
                     w->bsum, w->bfac, w->ipiv, w->perm, w->iperm, w->cand_i, w->bflag, w->err, w->bar,
-                    w->ptimes, w->mhdr, w->mcval, w->mcrow, w->mgrows, w->ybuf};
+                    w->ptimes, w->mhdr, w->mcval, w->mcrow, w->mgrows, w->ybuf, w->zflags};
     for (void* p : ptrs)
         if (p) cudaFree(p);
     delete w;
@@ -97,6 +99,8 @@ int lhl_ws_create(int64_t n, int precision, lhl_ws_t* out)
     A_(ptimes, 24);
     w->ycap = 256;
     A_(ybuf, (size_t)n * w->ycap);
+    w->nzflags = (int)(((n + 63) / 64) * ((w->ycap + 3) / 4));
+    A_(zflags, (size_t)w->nzflags);
     if (precision == LHL_PREC_MIXED && n >= 3) {
         int dev = 0, sms = 0;
         if (e == cudaSuccess) e = cudaGetDevice(&dev);
@@ -372,12 +376,17 @@ static int ldiv_common(lhl_shift_t sh, lhl_ws_t ws, double* dX, int64_t ldx, int
     a.rhs_per_shift = 1;
     a.Y = ws->ybuf;
     a.ycap = ws->ycap;
+    a.zflags = ws->zflags;
+    a.nzflags = ws->nzflags;
+    a.err = ws->err;
+    a.limit_ns = ws->limit_ns;
     if (sh) {
         a.Gt = sh->Gt;
         a.ldg = (int)sh->ldg;
         a.swp = sh->swap;
         a.rdiag = sh->rdiag;
         a.rhs_per_shift = (int)rps;
+        a.nshifts = (int)sh->nshifts;
     }
     return cuda_status(lhl::launch_ldiv(a, (int)nrhs, st));
 }
@@ -444,8 +453,9 @@ int lhl_refine_tol(lhl_shift_t sh, lhl_ws_t ws, const double* dJ, int64_t ldj, c
     if (n > 8192) return LHL_ERR_DIM;
     cudaStream_t st = (cudaStream_t)stream;
     for (int s = 0; s <= max_steps; ++s) {
+        // step 0 computes every residual; later steps only those of unconverged columns
         cudaError_t e = lhl::launch_residual((int)n, dJ, (int)ldj, dB, (int)ldb, dX, (int)ldx, dR, (int)ldx, (int)nrhs,
-                                             (int)rhs_per_shift, sh->sigma, sh->tau, st);
+                                             (int)rhs_per_shift, sh->sigma, sh->tau, st, s > 0 ? dres : nullptr, tol);
         if (e == cudaSuccess) e = lhl::launch_relres((int)n, dR, (int)ldx, dB, (int)ldb, dres, (int)nrhs, st);
         if (e != cudaSuccess) return LHL_ERR_CUDA;
         if (s == max_steps) break;
@@ -466,10 +476,15 @@ int lhl_refine_tol(lhl_shift_t sh, lhl_ws_t ws, const double* dJ, int64_t ldj, c
         a.swp = sh->swap;
         a.rdiag = sh->rdiag;
         a.rhs_per_shift = (int)rhs_per_shift;
+        a.nshifts = (int)sh->nshifts;
         a.done = dres;
         a.tol = tol;
         a.Y = ws->ybuf;
         a.ycap = ws->ycap;
+        a.zflags = ws->zflags;
+        a.nzflags = ws->nzflags;
+        a.err = ws->err;
+        a.limit_ns = ws->limit_ns;
         e = lhl::launch_ldiv(a, (int)nrhs, st);
         if (e == cudaSuccess) e = lhl::launch_axpy_cols((int)n, dX, (int)ldx, dR, (int)ldx, (int)nrhs, st, dres, tol);
         if (e != cudaSuccess) return LHL_ERR_CUDA;

@@ -150,6 +150,16 @@ __device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, uint32
     return false;
 }
 
+// Bounded wait on an mbarrier phase by wall time; returns false after limit_ns.
+__device__ __forceinline__ bool mbar_wait_ns(uint64_t* bar, uint32_t parity, unsigned long long limit_ns)
+{
+    const uint64_t t0 = globaltimer_ns();
+    for (uint32_t it = 0;; ++it) {
+        if (mbar_wait(bar, parity, 64)) return true;
+        if (globaltimer_ns() - t0 > limit_ns) return false;
+    }
+}
+
 // Order this thread's view of global memory (generic proxy) before its later TMA reads.
 __device__ __forceinline__ void fence_proxy_async_global()
 {

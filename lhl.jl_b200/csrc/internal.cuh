@@ -54,6 +54,11 @@ struct LdivArgs {
     double tol;
     double* Y;            // ldiv scratch: n x ycap (the workspace's)
     int ycap;
+    int nshifts;          // shift slots in the batch at Gt (for the tensor map over all of them)
+    int* zflags;          // ldiv scratch: ready flags of the blocked forward substitution
+    int nzflags;
+    int* err;             // bounded-wait status (the workspace's error word)
+    unsigned long long limit_ns;
 };
 
 // One L sweep over a tile of right-hand sides (see solve.cu).
@@ -70,6 +75,12 @@ struct ZArgs {
     int ldd;
     int m;       // right-hand sides
     int gather;  // zinv: read x[perm[i]] * iscale[perm[i]]
+    int* flags;  // zinv: per (row block, tile) ready flags, cleared before each launch
+    int nflags;
+    const double* done;  // optional: a tile whose columns all have done[c] <= tol is skipped
+    double tol;
+    int* err;
+    unsigned long long limit_ns;
 };
 
 // Mixed-precision reduction (see reduce_mixed.cu).
@@ -102,6 +113,9 @@ cudaError_t launch_ht_perm(int n, const double* A, double* Ht, const int64_t* ip
 cudaError_t launch_fill_ones(double* a, double* b, int n, cudaStream_t st);
 cudaError_t launch_set_pair(double* a, double* b, double va, double vb, cudaStream_t st);
 size_t stepTabBytes();
+// 2-D tensor map of a column-major FP64 array (rows x cols, leading dimension ld, even) in
+// boxes of box_r x box_c, for TMA loads (reduce.cu).
+bool make_tmap_2d(void* tmap, const double* base, int rows, int cols, int ld, int box_r, int box_c);
 int reduce_grid_size();
 
 cudaError_t launch_shift_lu(int n, const double* Ht, int ldh, const double* sig, const double* tau, int s0, int count,
@@ -110,7 +124,7 @@ cudaError_t launch_shift_lu(int n, const double* Ht, int ldh, const double* sig,
 cudaError_t launch_ldiv(const LdivArgs& a, int nrhs, cudaStream_t st);
 cudaError_t launch_residual(int n, const double* J, int ldj, const double* B, int ldb, const double* X, int ldx,
                             double* R, int ldr, int nrhs, int rhs_per_shift, const double* sig, const double* tau,
-                            cudaStream_t st);
+                            cudaStream_t st, const double* done = nullptr, double tol = 0.0);
 cudaError_t launch_axpy_cols(int n, double* X, int ldx, const double* R, int ldr, int nrhs, cudaStream_t st,
                              const double* done = nullptr, double tol = 0.0);
 cudaError_t launch_relres(int n, const double* R, int ldr, const double* B, int ldb, double* out, int nrhs,

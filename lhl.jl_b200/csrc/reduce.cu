@@ -1342,7 +1342,7 @@ int reduce_grid_size()
 
 // 2-D tensor map of a column-major FP64 array (rows x cols, leading dimension ld) in
 // boxes of box_r x box_c, for TMA loads.  TMA needs a 16-byte row pitch (even ld).
-static bool make_tmap_2d(void* tmap, const double* base, int rows, int cols, int ld, int box_r, int box_c)
+bool make_tmap_2d(void* tmap, const double* base, int rows, int cols, int ld, int box_r, int box_c)
 {
     if ((ld & 1) || rows < 1 || cols < 1) return false;
     static PFN_cuTensorMapEncodeTiled_v12000 enc = nullptr;

@@ -6,16 +6,13 @@
 //   ->  y <- L y  ->  scatter x = D P y.
 // Three launches, so that L (shared by every shift) is read once per tile of right-hand
 // sides and not once per right-hand side:
-//   zinv_kernel  -- gather and y <- L^-1 y for RT right-hand sides per CTA, the vectors in
-//                   shared memory.  Column blocks of 32: the block's 32 x 32 triangle is staged
-//                   in shared memory and solved by one warp per right-hand side (shuffles),
-//                   then every thread applies the block to its rows with 32 independent loads
-//                   of L in flight.
+//   zl_kernel<false> -- gather and y <- L^-1 y: a blocked forward substitution over a
+//                   cooperative grid, tasks (64-row block, 4 right-hand sides) with ready flags.
 //   hess_kernel  -- the Hessenberg solve with each right-hand side's shift LU, one CTA per
 //                   right-hand side (the forward select-swap recurrence, F:2806-2816, then a
 //                   left-looking back substitution over Gt's contiguous columns).
-//   zmul_kernel  -- y <- L y (no recurrence: original y on the right), rows split over CTAs,
-//                   and the scatter x[perm[i]] = (L y)[i] * scale[perm[i]].
+//   zl_kernel<true>  -- y <- L y (no recurrence: original y on the right), the same tasks
+//                   without flags, and the scatter x[perm[i]] = (L y)[i] * scale[perm[i]].
 // Summation order differs from the reference's (results agree to rounding; the solve's
 // contract is its residual, not its bits).
 #include "internal.cuh"
@@ -28,112 +25,143 @@ constexpr int BS = 32;
 
 constexpr int ZT = 512;
 
+// true when every column c0..c0+cnt-1 (< m) is marked converged
+__device__ __forceinline__ bool tile_done(const double* done, double tol, int c0, int cnt, int m)
+{
+    if (!done) return false;
+    for (int c = c0; c < c0 + cnt && c < m; ++c)
+        if (!(done[c] <= tol)) return false;
+    return true;
+}
+
 // L[i, c] (1-based) = F[i, c-1] for 2 <= c <= n-1, i >= c+1 (unit lower; column 1 is e1).
 __device__ __forceinline__ const double* lcol(const ZArgs& z, int c) { return z.F + (size_t)(c - 2) * z.ldf; }
 
-// y <- L^-1 P^-1 D^-1 x (gather = 1) or y <- L^-1 x, for RT right-hand sides per CTA.
-template <int RT>
-__global__ void __launch_bounds__(ZT) zinv_kernel(ZArgs z)
+// MUL = false: y <- L^-1 P^-1 D^-1 x (gather = 1) or y <- L^-1 x, a blocked forward
+// substitution spread over a cooperative grid.  MUL = true: x <- D P L y with the same tiles
+// and no dependencies between tasks.  Task (i, c) owns rows 64i..64i+63 of right-hand sides 4c..4c+3;
+// tasks are numbered block-major and handed out in order, so every task it waits for runs
+// earlier (on a co-resident CTA).  A task folds in L_ij y_j for each earlier block j as soon
+// as that block's ready flag is set (the L tile is loaded before the wait), then solves its
+// unit lower 64 x 64 diagonal block (one warp per right-hand side, shuffles), stores y_i and
+// sets its own flag with release semantics.  Every wait is bounded in wall time.
+constexpr int ZR = 64;   // rows per block
+constexpr int ZC = 4;    // right-hand sides per task
+constexpr int ZIT = 256;
+
+template <bool MUL>
+__global__ void __launch_bounds__(ZIT) zl_kernel(ZArgs z)
 {
-    extern __shared__ double ys[];  // RT x n, right-hand side j at ys + j n
-    __shared__ double tri[BS][BS + 1];
-    const int n = z.n;
+    __shared__ double Lt[ZR][ZR + 1];
+    __shared__ double Ys[ZR][ZC];
+    __shared__ int s_ok;
+    const int n = z.n, m = z.m;
     const int t = threadIdx.x, lane = t & 31, warp = t >> 5;
-    const int c0 = blockIdx.x * RT;
-    for (int j = 0; j < RT; ++j) {
-        const double* x = z.src + (size_t)(c0 + j) * z.lds;
-        for (int i = t; i < n; i += ZT) {
-            double v = 0.0;
-            if (c0 + j < z.m) {
-                if (z.gather) {
-                    const int64_t p = z.perm[i];
-                    v = x[p - 1] * z.iscale[p - 1];
-                } else {
-                    v = x[i];
+    const int nblk = (n + ZR - 1) / ZR, ntile = (m + ZC - 1) / ZC;
+    const int r = t & (ZR - 1), jr = t >> 6;  // this thread's row in the block and right-hand side
+    for (int task = blockIdx.x; task < nblk * ntile; task += gridDim.x) {
+        const int ib = task / ntile, c = task - ib * ntile;
+        const int i = MUL ? nblk - 1 - ib : ib;  // L y: the longest rows first
+        if (tile_done(z.done, z.tol, c * ZC, ZC, m)) continue;  // all of its tasks skip alike
+        const int row = i * ZR + r, col = c * ZC + jr;
+        const bool live = row < n && col < m;
+        double acc = 0.0;
+        if (live) {
+            const double* x = z.src + (size_t)col * z.lds;
+            if (!MUL && z.gather) {
+                const int64_t p = z.perm[row];
+                acc = x[p - 1] * z.iscale[p - 1];
+            } else {
+                acc = x[row];
+            }
+        }
+        // L tiles are software-pipelined: tile j+1 is in registers while tile j is used
+        constexpr int PER = ZR * ZR / ZIT;  // 16 entries per thread
+        double lreg[PER];
+        auto load_tile = [&](int j) {
+#pragma unroll
+            for (int u = 0; u < PER; ++u) {
+                const int e = t + u * ZIT;
+                const int rr = e & (ZR - 1), qq = e >> 6;
+                const int gr = i * ZR + rr, q = j * ZR + qq;
+                // L[row][q] = F[(q-1) ldf + row] for 1 <= q <= n-2 and row >= q+1, else 0
+                lreg[u] = (gr < n && q >= 1 && q <= n - 2 && gr >= q + 1) ? z.F[(size_t)(q - 1) * z.ldf + gr] : 0.0;
+            }
+        };
+        load_tile(0);
+        for (int j = 0; j <= i; ++j) {
+#pragma unroll
+            for (int u = 0; u < PER; ++u) {
+                const int e = t + u * ZIT;
+                Lt[e & (ZR - 1)][e >> 6] = lreg[u];
+            }
+            if (j < i) load_tile(j + 1);
+            if (MUL || j < i) {
+                if (!MUL) {
+                    if (t == 0) {
+                        int ok = 1;
+                        const int* f = z.flags + (size_t)j * ntile + c;
+                        const uint64_t t0 = globaltimer_ns();
+                        unsigned spins = 0;
+                        while (ld_acquire_i32(f) != 1) {
+                            if ((++spins & 63u) == 0) {
+                                if (ld_acquire_i32(z.err) != 0) { ok = 0; break; }
+                                if (globaltimer_ns() - t0 > z.limit_ns) {
+                                    atomicCAS(z.err, 0, (int)LHL_ERR_TIMEOUT);
+                                    ok = 0;
+                                    break;
+                                }
+                            }
+                        }
+                        s_ok = ok;
+                    }
+                    __syncthreads();
+                    if (!s_ok) return;
+                }
+                {
+                    const int qq = t & (ZR - 1), cc = t >> 6;
+                    const int q = j * ZR + qq;
+                    const double* yb = MUL ? z.src : z.dst;  // L y reads the input; L^-1 y the solved blocks
+                    const int ldy = MUL ? z.lds : z.ldd;
+                    Ys[qq][cc] = (q < n && c * ZC + cc < m) ? __ldcg(&yb[(size_t)(c * ZC + cc) * ldy + q]) : 0.0;
+                }
+                __syncthreads();
+                double s0 = 0.0, s1 = 0.0;
+#pragma unroll 8
+                for (int qq = 0; qq < ZR; qq += 2) {
+                    s0 = dfma(Lt[r][qq], Ys[qq][jr], s0);
+                    s1 = dfma(Lt[r][qq + 1], Ys[qq + 1][jr], s1);
+                }
+                if (MUL) acc += s0 + s1;
+                else acc -= s0 + s1;
+                __syncthreads();
+            } else {
+                // diagonal block: unit lower solve, one warp per right-hand side
+                Ys[r][jr] = acc;
+                __syncthreads();
+                if (warp < ZC && c * ZC + warp < m) {
+                    double y0 = Ys[lane][warp], y1 = Ys[lane + 32][warp];
+                    for (int q = 0; q < ZR - 1; ++q) {
+                        const double xq = __shfl_sync(0xffffffffu, q < 32 ? y0 : y1, q & 31);
+                        if (lane > q) y0 = dfma(-Lt[lane][q], xq, y0);
+                        if (lane + 32 > q) y1 = dfma(-Lt[lane + 32][q], xq, y1);
+                    }
+                    double* d = z.dst + (size_t)(c * ZC + warp) * z.ldd;
+                    if (i * ZR + lane < n) d[i * ZR + lane] = y0;
+                    if (i * ZR + lane + 32 < n) d[i * ZR + lane + 32] = y1;
+                }
+                __syncthreads();
+                if (t == 0) {
+                    __threadfence();
+                    asm volatile("st.release.gpu.global.s32 [%0], %1;" ::"l"(z.flags + (size_t)i * ntile + c), "r"(1)
+                                 : "memory");
                 }
             }
-            ys[j * n + i] = v;
         }
-    }
-    __syncthreads();
-    for (int cb0 = 2; cb0 <= n - 1; cb0 += BS) {
-        const int cb1 = min(cb0 + BS - 1, n - 1);
-        const int bw = cb1 - cb0 + 1;
-        for (int e = t; e < BS * BS; e += ZT) {
-            const int r = e & (BS - 1), q = e >> 5;
-            if (q < bw && r < bw && r > q) tri[r][q] = lcol(z, cb0 + q)[cb0 + r - 1];
+        if (MUL && live) {  // x[perm[row]] = (L y)[row] * scale[perm[row]]
+            const int64_t p = z.perm[row];
+            z.dst[(size_t)col * z.ldd + (p - 1)] = acc * z.scale[p - 1];
         }
-        __syncthreads();
-        if (warp < RT) {
-            double* y = ys + warp * n;
-            double yi = lane < bw ? y[cb0 + lane - 1] : 0.0;
-            for (int q = 0; q < bw - 1; ++q) {
-                const double xq = __shfl_sync(0xffffffffu, yi, q);
-                if (lane > q && lane < bw) yi = dfma(-tri[lane][q], xq, yi);
-            }
-            if (lane < bw) y[cb0 + lane - 1] = yi;
-        }
-        __syncthreads();
-        for (int i = cb1 + 1 + t; i <= n; i += ZT) {
-            double l[BS];
-#pragma unroll
-            for (int q = 0; q < BS; ++q) l[q] = q < bw ? lcol(z, cb0 + q)[i - 1] : 0.0;
-#pragma unroll
-            for (int j = 0; j < RT; ++j) {
-                const double* y = ys + j * n;
-                double v = y[i - 1];
-#pragma unroll
-                for (int q = 0; q < BS; ++q)
-                    if (q < bw) v = dfma(-l[q], y[cb0 + q - 1], v);
-                ys[j * n + i - 1] = v;
-            }
-        }
-        __syncthreads();
-    }
-    for (int j = 0; j < RT; ++j) {
-        if (c0 + j >= z.m) break;
-        double* d = z.dst + (size_t)(c0 + j) * z.ldd;
-        for (int i = t; i < n; i += ZT) d[i] = ys[j * n + i];
-    }
-}
-
-// x <- D P L y for RT right-hand sides per CTA; blockIdx.y splits the rows (row i costs i).
-template <int RT>
-__global__ void __launch_bounds__(ZT) zmul_kernel(ZArgs z)
-{
-    extern __shared__ double ys[];  // RT x n
-    const int n = z.n;
-    const int t = threadIdx.x;
-    const int c0 = blockIdx.x * RT;
-    for (int j = 0; j < RT; ++j) {
-        const double* y = z.src + (size_t)(c0 + j) * z.lds;
-        for (int i = t; i < n; i += ZT) ys[j * n + i] = (c0 + j < z.m) ? y[i] : 0.0;
-    }
-    __syncthreads();
-    // rows [i0, i1) of this CTA: equal shares of the n^2/2 work
-    const int S = gridDim.y, s = blockIdx.y;
-    const int i0 = (int)((double)n * sqrt((double)s / S)), i1 = s + 1 == S ? n : (int)((double)n * sqrt((double)(s + 1) / S));
-    for (int i = i0 + 1 + t; i <= i1; i += ZT) {
-        double acc[RT];
-#pragma unroll
-        for (int j = 0; j < RT; ++j) acc[j] = ys[j * n + i - 1];
-        for (int cb0 = 2; cb0 <= i - 1; cb0 += BS) {
-            const int bw = min(BS, i - cb0);
-            double l[BS];
-#pragma unroll
-            for (int q = 0; q < BS; ++q) l[q] = q < bw ? lcol(z, cb0 + q)[i - 1] : 0.0;
-#pragma unroll
-            for (int j = 0; j < RT; ++j) {
-                const double* y = ys + j * n;
-#pragma unroll
-                for (int q = 0; q < BS; ++q)
-                    if (q < bw) acc[j] = dfma(l[q], y[cb0 + q - 1], acc[j]);
-            }
-        }
-        const int64_t p = z.perm[i - 1];
-#pragma unroll
-        for (int j = 0; j < RT; ++j)
-            if (c0 + j < z.m) z.dst[(size_t)(c0 + j) * z.ldd + (p - 1)] = acc[j] * z.scale[p - 1];
     }
 }
 
@@ -227,32 +255,265 @@ __global__ void __launch_bounds__(SOLVE_T) hess_kernel(LdivArgs a, double* Y, in
     for (int i = t; i < n; i += SOLVE_T) yg[i] = y[i];
 }
 
-template <int RT>
-static cudaError_t launch_z(bool inv, const ZArgs& z, int zsplit, cudaStream_t st)
+// The same Hessenberg solve with Gt streamed by TMA (even n): the back substitution's 32-row
+// blocks read their 32 columns of Gt (rows r0..n) as 128 x 32 boxes through a ring of `ns`
+// shared-memory slots.  Warp 16 is the producer: it requests boxes in consumption order as
+// slots free up (per-slot "full" and "empty" mbarriers), starting before the forward
+// recurrence runs.  Warps 0-15 consume, two Gt columns each, and synchronise among
+// themselves (named barrier 1) only at block boundaries.  Every wait is bounded in time.
+constexpr int HB_ROWS = 128, HB_COLS = 32, HB_MAXSLOTS = 8;
+constexpr uint32_t HB_BYTES = HB_ROWS * HB_COLS * sizeof(double);
+constexpr int HCONS = 16;                 // consumer warps
+constexpr int HT = (HCONS + 1) * 32;      // + one producer warp
+
+__device__ __forceinline__ void cons_sync() { asm volatile("bar.sync 1, %0;" ::"r"(HCONS * 32) : "memory"); }
+
+__device__ __forceinline__ void mbar_arrive(uint64_t* bar)
 {
-    const size_t smem = (size_t)RT * z.n * sizeof(double);
-    static size_t attr[2] = {0, 0};
-    const void* fn = inv ? (const void*)zinv_kernel<RT> : (const void*)zmul_kernel<RT>;
-    if (smem > 32 * 1024 && smem > attr[inv]) {
-        cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-        if (e != cudaSuccess) return e;
-        attr[inv] = smem;
-    }
-    const dim3 grid((z.m + RT - 1) / RT, inv ? 1 : zsplit);
-    if (inv) zinv_kernel<RT><<<grid, ZT, smem, st>>>(z);
-    else zmul_kernel<RT><<<grid, ZT, smem, st>>>(z);
-    return cudaGetLastError();
+    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
 }
 
-static cudaError_t run_z(bool inv, const ZArgs& z, cudaStream_t st)
+// Forward select-swap recurrence of the Hessenberg solve (F:2806-2816) as a parallel scan.
+// Step k (1..n-1) maps c -> alpha_k c + beta_k: with an interchange x_k = y_k and
+// c <- c - l_k y_k (alpha = 1, beta = -l_k y_k); without, x_k = c and c <- y_k - l_k c
+// (alpha = -l_k, beta = y_k).  |l_k| <= 1 (the LU's pivoting), so composing the maps is
+// stable.  Each of the NT threads composes one contiguous chunk of steps, the chunk maps are
+// scanned across the threads (shuffles, then warp totals), and every thread replays its
+// chunk from the prefix value.  In place on y (x_k -> y[k-1], the last c -> y[n-1]).
+// Called by all NT threads (warps 0..NT/32-1); `sync` synchronises exactly those threads.
+template <int NT, class Sync>
+__device__ __forceinline__ void forward_scan(int n, double* y, const double* sm, const uint8_t* ssw, double* wA,
+                                             double* wB, Sync sync)
 {
-    // right-hand sides per CTA: as many as fit in shared memory, at most 4
-    const size_t per = (size_t)z.n * sizeof(double);
-    const int tiles4 = (z.m + 3) / 4;
-    const int zsplit = inv ? 1 : (tiles4 >= 64 ? 2 : (tiles4 >= 16 ? 8 : 16));
-    if (4 * per <= 190 * 1024) return launch_z<4>(inv, z, zsplit, st);
-    if (2 * per <= 190 * 1024) return launch_z<2>(inv, z, zsplit * 2, st);
-    return launch_z<1>(inv, z, zsplit * 4, st);
+    const int t = threadIdx.x, lane = t & 31, warp = t >> 5;
+    constexpr int NW = NT / 32;
+    const int C = (n - 1 + NT - 1) / NT;
+    const int k0 = 1 + t * C, k1 = min(k0 + C, n);  // steps [k0, k1)
+    double A = 1.0, B = 0.0;                          // chunk map: c_out = A c_in + B
+    for (int k = k0; k < k1; ++k) {
+        const double l = sm[k - 1], b = y[k];
+        if (ssw[k - 1]) {
+            B = B - l * b;
+        } else {
+            A = -l * A;
+            B = b - l * B;
+        }
+    }
+    const double blast = k0 < k1 ? y[k1 - 1] : 0.0;  // the next thread overwrites y[k1-1] below
+    // inclusive scan of the maps in thread order: earlier (pA, pB) then own (A, B)
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const double pA = __shfl_up_sync(0xffffffffu, A, o), pB = __shfl_up_sync(0xffffffffu, B, o);
+        if (lane >= o) {
+            B = A * pB + B;
+            A = A * pA;
+        }
+    }
+    if (lane == 31) {
+        wA[warp] = A;
+        wB[warp] = B;
+    }
+    sync();
+    if (warp == 0) {
+        double a = lane < NW ? wA[lane] : 1.0, bb = lane < NW ? wB[lane] : 0.0;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const double pA = __shfl_up_sync(0xffffffffu, a, o), pB = __shfl_up_sync(0xffffffffu, bb, o);
+            if (lane >= o) {
+                bb = a * pB + bb;
+                a = a * pA;
+            }
+        }
+        if (lane < NW) {
+            wA[lane] = a;
+            wB[lane] = bb;
+        }
+    }
+    sync();
+    double eA = __shfl_up_sync(0xffffffffu, A, 1), eB = __shfl_up_sync(0xffffffffu, B, 1);
+    if (lane == 0) {
+        eA = 1.0;
+        eB = 0.0;
+    }
+    const double pA = warp > 0 ? wA[warp - 1] : 1.0, pB = warp > 0 ? wB[warp - 1] : 0.0;
+    double c = eA * (pA * y[0] + pB) + eB;  // c before step k0
+    sync();                                 // y[0] and every chunk's last input read
+    for (int k = k0; k < k1; ++k) {
+        const double l = sm[k - 1], b = k == k1 - 1 ? blast : y[k];
+        double x;
+        if (ssw[k - 1]) {
+            x = b;
+            c = c - l * b;
+        } else {
+            x = c;
+            c = b - l * c;
+        }
+        y[k - 1] = x;
+    }
+    if (k1 == n && k0 < k1) y[n - 1] = c;
+    sync();
+}
+
+__global__ void __launch_bounds__(HT) hess_tma_kernel(LdivArgs a, double* Y, int ldy, int col0, int ns,
+                                                      const __grid_constant__ CUtensorMap tmG)
+{
+    extern __shared__ __align__(1024) double hsm[];
+    __shared__ __align__(8) uint64_t full[HB_MAXSLOTS], empty[HB_MAXSLOTS];
+    __shared__ double tri[BS][BS + 1];
+    __shared__ double sj[BS];
+    __shared__ int s_bad;
+    const int n = a.n;
+    double* box = hsm;  // ns boxes, column jj of a box at box + jj * HB_ROWS
+    double* y = hsm + (size_t)ns * HB_ROWS * HB_COLS;
+    double* sm = y + n;
+    uint8_t* ssw = (uint8_t*)(sm + n);
+    const int col = col0 + blockIdx.x;
+    if (a.done && a.done[col] <= a.tol) return;  // converged column: nothing requested yet
+    const int t = threadIdx.x, lane = t & 31, warp = t >> 5;
+    const int s = col / a.rhs_per_shift;
+    const uint8_t* swp = a.swp + (size_t)s * n;
+    const double* rd = a.rdiag + (size_t)s * n;
+    const double* Gt = a.Gt + (size_t)s * a.ldg * n;
+    // blocks b = 0.. from the bottom: r1 = n - 32 b, r0 = max(r1 - 31, 1) (odd for even n);
+    // block b needs ceil((n - r0 + 1) / 128) boxes
+    const int nblocks = (n + BS - 1) / BS;
+    if (t == 0) {
+        for (int u = 0; u < ns; ++u) {
+            mbar_init(&full[u], 1);
+            mbar_init(&empty[u], HCONS);
+        }
+        mbar_fence_init();
+        s_bad = 0;
+    }
+    __syncthreads();
+    if (warp == HCONS) {
+        // ---- producer ----
+        if (lane == 0) {
+            int u = 0;
+            for (int b = 0; b < nblocks && !s_bad; ++b) {
+                const int r1 = n - BS * b, r0 = max(r1 - (BS - 1), 1);
+                const int nk = (n - r0 + HB_ROWS) / HB_ROWS;
+                for (int k = 0; k < nk; ++k, ++u) {
+                    const int slot = u % ns;
+                    if (u >= ns && !mbar_wait_ns(&empty[slot], (uint32_t)((u / ns - 1) & 1), a.limit_ns)) {
+                        atomicCAS(a.err, 0, (int)LHL_ERR_TIMEOUT);
+                        s_bad = 1;
+                        break;
+                    }
+                    mbar_expect_tx(&full[slot], HB_BYTES);
+                    tma_load_2d(box + (size_t)slot * HB_ROWS * HB_COLS, &tmG, r0 - 1 + HB_ROWS * k, s * n + r0 - 1,
+                                &full[slot]);
+                }
+            }
+            // drain: wait (bounded) for the last copies of every slot, so that none lands after
+            // the block exits (on the normal path they completed long ago)
+            for (int v = max(u - ns, 0); v < u; ++v) mbar_wait_ns(&full[v % ns], (uint32_t)((v / ns) & 1), a.limit_ns);
+        }
+        return;
+    }
+    // ---- consumers (warps 0-15) ----
+    for (int i = t; i < n; i += HCONS * 32) y[i] = Y[(size_t)blockIdx.x * ldy + i];
+    for (int k = 1 + t; k <= n - 1; k += HCONS * 32) {
+        sm[k - 1] = M1(Gt, a.ldg, k, k + 1);
+        ssw[k - 1] = swp[k - 1];
+    }
+    cons_sync();
+    if (n >= 2) forward_scan<HCONS * 32>(n, y, sm, ssw, sj, sj + 16, []() { cons_sync(); });
+    cons_sync();
+    int u = 0;
+    bool bad = false;
+    for (int b = 0; b < nblocks; ++b) {
+        const int r1 = n - BS * b, r0 = max(r1 - (BS - 1), 1);
+        const int bw = r1 - r0 + 1;
+        const int nk = (n - r0 + HB_ROWS) / HB_ROWS;
+        double acc0 = 0.0, acc1 = 0.0;  // columns jj = warp and warp + 16
+        for (int k = 0; k < nk; ++k, ++u) {
+            const int slot = u % ns;
+            if (!bad && !mbar_wait_ns(&full[slot], (uint32_t)((u / ns) & 1), a.limit_ns)) {
+                atomicCAS(a.err, 0, (int)LHL_ERR_TIMEOUT);
+                bad = true;
+            }
+            const double* bx = box + (size_t)slot * HB_ROWS * HB_COLS;
+            const int rb = r0 + HB_ROWS * k;  // 1-based row of box row 0
+            if (k == 0)
+                for (int e = t; e < BS * BS; e += HCONS * 32) {
+                    const int jj = e >> 5, rr = e & 31;
+                    tri[jj][rr] = bx[jj * HB_ROWS + rr];  // Gt[r0 + rr, r0 + jj] = U[r0 + jj, r0 + rr]
+                }
+#pragma unroll
+            for (int h = 0; h < 2; ++h) {
+                const int jj = warp + HCONS * h;
+                if (jj < bw) {
+                    double p = 0.0;
+#pragma unroll
+                    for (int rr = lane; rr < HB_ROWS; rr += 32) {
+                        const int i = rb + rr;
+                        if (i > r1 && i <= n) p = dfma(bx[jj * HB_ROWS + rr], y[i - 1], p);
+                    }
+                    if (h == 0) acc0 += p;
+                    else acc1 += p;
+                }
+            }
+            __syncwarp();
+            if (lane == 0) mbar_arrive(&empty[slot]);  // this warp is done with the slot
+        }
+        acc0 = warp_sum(acc0);
+        acc1 = warp_sum(acc1);
+        if (lane == 0) {
+            if (warp < bw) sj[warp] = acc0;
+            if (warp + HCONS < bw) sj[warp + HCONS] = acc1;
+        }
+        cons_sync();
+        if (warp == 0) {
+            const int i = r0 + lane;
+            double yi = (i <= r1) ? y[i - 1] - sj[lane] : 0.0;
+            const double rdi = (i <= r1) ? rd[i - 1] : 0.0;
+#pragma unroll
+            for (int jj = BS - 1; jj >= 0; --jj) {
+                if (jj < bw) {
+                    double xj = 0.0;
+                    if (lane == jj) {
+                        yi = yi * rdi;
+                        xj = yi;
+                    }
+                    xj = __shfl_sync(0xffffffffu, xj, jj);
+                    if (lane < jj) yi = dfma(-tri[lane][jj], xj, yi);  // U[r0 + lane, r0 + jj]
+                }
+            }
+            if (i <= r1) y[i - 1] = yi;
+        }
+        cons_sync();
+    }
+    if (bad) return;
+    for (int i = t; i < n; i += HCONS * 32) Y[(size_t)blockIdx.x * ldy + i] = y[i];
+}
+
+static cudaError_t run_zinv(ZArgs z, cudaStream_t st)
+{
+    const int nblk = (z.n + ZR - 1) / ZR, ntile = (z.m + ZC - 1) / ZC;
+    if ((size_t)nblk * ntile > (size_t)z.nflags) return cudaErrorInvalidValue;
+    cudaError_t e = cudaMemsetAsync(z.flags, 0, (size_t)nblk * ntile * sizeof(int), st);
+    if (e != cudaSuccess) return e;
+    static int maxgrid = 0;
+    if (maxgrid == 0) {
+        int dev = 0, sms = 0, per = 0;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, zl_kernel<false>, ZIT, 0);
+        maxgrid = sms * (per > 0 ? per : 1);
+    }
+    const int grid = min(nblk * ntile, maxgrid);
+    void* args[] = {&z};
+    return cudaLaunchCooperativeKernel((void*)zl_kernel<false>, dim3(grid), dim3(ZIT), args, 0, st);
+}
+
+// x <- D P L y: independent tasks (row block, 4 right-hand sides), no flags; the blocks of
+// the last rows (the most work) are handed out first.
+static cudaError_t run_zmul(const ZArgs& z, cudaStream_t st)
+{
+    const int nblk = (z.n + ZR - 1) / ZR, ntile = (z.m + ZC - 1) / ZC;
+    zl_kernel<true><<<nblk * ntile, ZIT, 0, st>>>(z);
+    return cudaGetLastError();
 }
 
 cudaError_t launch_ldiv(const LdivArgs& a, int nrhs, cudaStream_t st)
@@ -266,11 +527,25 @@ cudaError_t launch_ldiv(const LdivArgs& a, int nrhs, cudaStream_t st)
     z.perm = a.perm;
     z.scale = a.scale;
     z.iscale = a.iscale;
-    if (a.mode == 1) {  // applyZinv: x <- L^-1 P^-1 D^-1 x (in place)
-        z.src = a.X; z.lds = a.ldx; z.dst = a.X; z.ldd = a.ldx; z.m = nrhs; z.gather = 1;
-        return run_z(true, z, st);
+    z.flags = a.zflags;
+    z.nflags = a.nzflags;
+    z.err = a.err;
+    z.limit_ns = a.limit_ns;
+    z.tol = a.tol;
+    if (!a.Y || a.ycap <= 0 || !a.zflags || !a.err) return cudaErrorInvalidValue;
+    if (a.mode == 1) {  // applyZinv: x <- L^-1 P^-1 D^-1 x, through the scratch
+        for (int c0 = 0; c0 < nrhs; c0 += a.ycap) {
+            const int cnt = min(a.ycap, nrhs - c0);
+            z.src = a.X + (size_t)c0 * a.ldx; z.lds = a.ldx; z.dst = a.Y; z.ldd = a.n; z.m = cnt; z.gather = 1;
+            cudaError_t e = run_zinv(z, st);
+            if (e == cudaSuccess)
+                e = cudaMemcpy2DAsync(a.X + (size_t)c0 * a.ldx, (size_t)a.ldx * sizeof(double), a.Y,
+                                      (size_t)a.n * sizeof(double), (size_t)a.n * sizeof(double), cnt,
+                                      cudaMemcpyDeviceToDevice, st);
+            if (e != cudaSuccess) return e;
+        }
+        return cudaSuccess;
     }
-    if (!a.Y || a.ycap <= 0) return cudaErrorInvalidValue;
     if (a.mode == 2) {  // applyZ: x <- D P L x, through the scratch (CTAs split the rows)
         for (int c0 = 0; c0 < nrhs; c0 += a.ycap) {
             const int cnt = min(a.ycap, nrhs - c0);
@@ -279,7 +554,7 @@ cudaError_t launch_ldiv(const LdivArgs& a, int nrhs, cudaStream_t st)
                                               cudaMemcpyDeviceToDevice, st);
             if (e != cudaSuccess) return e;
             z.src = a.Y; z.lds = a.n; z.dst = a.X + (size_t)c0 * a.ldx; z.ldd = a.ldx; z.m = cnt; z.gather = 0;
-            e = run_z(false, z, st);
+            e = run_zmul(z, st);
             if (e != cudaSuccess) return e;
         }
         return cudaSuccess;
@@ -293,16 +568,35 @@ cudaError_t launch_ldiv(const LdivArgs& a, int nrhs, cudaStream_t st)
         if (e != cudaSuccess) return e;
         attr = hsm;
     }
+    // Gt through TMA: even n (16-byte row pitch and box origins) and room for >= 2 slots
+    const size_t vec = (size_t)a.n * 2 * sizeof(double) + (size_t)a.n + 16;
+    const int ns = (int)min((size_t)HB_MAXSLOTS, vec < 210 * 1024 ? (210 * 1024 - vec) / HB_BYTES : (size_t)0);
+    const size_t tsm = (size_t)ns * HB_BYTES + vec;
+    CUtensorMap tmG;
+    bool use_tma = (a.n % 2 == 0) && a.n >= 2 && ns >= 2 && a.nshifts > 0 &&
+                   make_tmap_2d(&tmG, a.Gt, a.ldg, a.nshifts * a.n, a.ldg, HB_ROWS, HB_COLS);
+    if (use_tma) {
+        static size_t tattr = 0;
+        if (tsm > tattr) {
+            if (cudaFuncSetAttribute(hess_tma_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)tsm) !=
+                cudaSuccess)
+                use_tma = false;
+            else
+                tattr = tsm;
+        }
+    }
     for (int c0 = 0; c0 < nrhs; c0 += a.ycap) {
         const int cnt = min(a.ycap, nrhs - c0);
         z.src = a.X + (size_t)c0 * a.ldx; z.lds = a.ldx; z.dst = a.Y; z.ldd = a.n; z.m = cnt; z.gather = 1;
-        cudaError_t e = run_z(true, z, st);
+        z.done = a.done ? a.done + c0 : nullptr;
+        cudaError_t e = run_zinv(z, st);
         if (e != cudaSuccess) return e;
-        hess_kernel<<<cnt, SOLVE_T, hsm, st>>>(a, a.Y, a.n, c0);
+        if (use_tma) hess_tma_kernel<<<cnt, HT, tsm, st>>>(a, a.Y, a.n, c0, ns, tmG);
+        else hess_kernel<<<cnt, SOLVE_T, hsm, st>>>(a, a.Y, a.n, c0);
         e = cudaGetLastError();
         if (e != cudaSuccess) return e;
         z.src = a.Y; z.lds = a.n; z.dst = a.X + (size_t)c0 * a.ldx; z.ldd = a.ldx; z.gather = 0;
-        e = run_z(false, z, st);
+        e = run_zmul(z, st);
         if (e != cudaSuccess) return e;
     }
     return cudaSuccess;
@@ -315,11 +609,13 @@ __global__ void __launch_bounds__(256) residual_kernel(int n, const double* __re
                                                        const double* __restrict__ B, int ldb,
                                                        const double* __restrict__ X, int ldx, double* __restrict__ R,
                                                        int ldr, int nrhs, int rhs_per_shift,
-                                                       const double* __restrict__ sig, const double* __restrict__ tau)
+                                                       const double* __restrict__ sig, const double* __restrict__ tau,
+                                                       const double* __restrict__ done, double tol)
 {
     __shared__ double sJ[RT_K][RT_M + 1];
     __shared__ double sX[RT_N][RT_K + 1];
     const int i0 = blockIdx.x * RT_M, c0 = blockIdx.y * RT_N;
+    if (tile_done(done, tol, c0, RT_N, nrhs)) return;  // converged columns keep their residual
     const int t = threadIdx.x;
     const int ti = t & 63, tc = t >> 6;  // 64 rows x 4 column pairs
     double acc0 = 0.0, acc1 = 0.0;
@@ -359,11 +655,11 @@ __global__ void __launch_bounds__(256) residual_kernel(int n, const double* __re
 
 cudaError_t launch_residual(int n, const double* J, int ldj, const double* B, int ldb, const double* X, int ldx,
                             double* R, int ldr, int nrhs, int rhs_per_shift, const double* sig, const double* tau,
-                            cudaStream_t st)
+                            cudaStream_t st, const double* done, double tol)
 {
     if (nrhs <= 0 || n <= 0) return cudaSuccess;
     dim3 grid((n + RT_M - 1) / RT_M, (nrhs + RT_N - 1) / RT_N);
-    residual_kernel<<<grid, 256, 0, st>>>(n, J, ldj, B, ldb, X, ldx, R, ldr, nrhs, rhs_per_shift, sig, tau);
+    residual_kernel<<<grid, 256, 0, st>>>(n, J, ldj, B, ldb, X, ldx, R, ldr, nrhs, rhs_per_shift, sig, tau, done, tol);
     return cudaGetLastError();
 }
 
