@@ -4,15 +4,17 @@
 //
 // One CTA per shift.  Element j of the pending row r (the not-yet-chosen candidate row,
 // F:2522-2527) lives in a register of thread (j-1) mod T for the whole elimination, so a
-// step costs one CTA barrier: the owner of element k+1 publishes it, every thread takes
-// the pivot decision of the next step from it.  Ht[j, k+1] (row k+1 of H) is prefetched
-// one step ahead.  Every operation is the reference's, in its order, with no fused
+// step costs one CTA barrier: the owner of element k+1 updates it first, takes the pivot
+// decision of step k+1 (the compare and the one division) and publishes it in shared
+// memory; every other thread only reads the decision.  Rows of H (Ht[j, k+1]) are requested D
+// steps before they are used (D = 4 up to n = 2048), into a register ring indexed at
+// compile time, so that a step does not wait for its loads.  Every operation is the reference's, in its order, with no fused
 // multiply-add, so Gt, swap, rdiag and info are bit-identical to the reference.
 #include "common.cuh"
 
 namespace lhl {
 
-template <int T, int E>
+template <int T, int E, int D>
 __global__ void __launch_bounds__(T) shift_lu_kernel(int n, const double* __restrict__ Ht, int ldh,
                                                      const double* __restrict__ sig, const double* __restrict__ tau_,
                                                      int s0, double* __restrict__ Gt_all, int ldg,
@@ -28,29 +30,35 @@ __global__ void __launch_bounds__(T) shift_lu_kernel(int n, const double* __rest
     const int t = threadIdx.x;
 
     __shared__ double s_next[2];  // r[k+1] after step k, double-buffered by step parity
+    __shared__ double s_l[2], s_a[2], s_b[2];  // the decision of step k (by parity)
+    __shared__ int s_sw[2];
     __shared__ int s_info;
 
+    // D rows of H in flight: the row for step k is requested at step k - D
     double r[E];
-    double h[E];
+    double hq[D][E];      // hq[d]: H row k+1 (Ht[j, k+1]) for the step k = d + 1 (mod D)
+    double hsub[E];       // Ht[j, j+1] = H[j+1, j]: the subdiagonal entry of the step this
+                          // thread decides (the owner of element j decides step j)
     // row 1 of G: r[j] = tau * Ht[j, 1], r[1] += sigma (F:2536-2539)
 #pragma unroll
     for (int e = 0; e < E; ++e) {
         const int j = 1 + t + e * T;
         r[e] = (j <= n) ? dmul(tau, M1(Ht, ldh, j, 1)) : 0.0;
         if (j == 1) r[e] = dadd(r[e], sigma);
-        h[e] = (j <= n && n >= 2) ? M1(Ht, ldh, j, 2) : 0.0;
+        hsub[e] = (j + 1 <= n) ? M1(Ht, ldh, j, j + 1) : 0.0;
     }
-    double hb = (n >= 2) ? M1(Ht, ldh, 1, 2) : 0.0;  // Ht[k, k+1] of the coming step
-    if (t == 0) {
-        s_next[1] = r[0];
-        s_info = 0;
+#pragma unroll
+    for (int d = 0; d < D; ++d) {
+        const int k = d + 1;  // step
+#pragma unroll
+        for (int e = 0; e < E; ++e) {
+            const int j = 1 + t + e * T;
+            hq[d][e] = (j <= n && k + 1 <= n) ? M1(Ht, ldh, j, k + 1) : 0.0;
+        }
     }
-    __syncthreads();
-
-    for (int k = 1; k <= n - 1; ++k) {
-        const double a = s_next[k & 1];
-        const double b = dmul(tau, hb);
-        hb = (k + 2 <= n) ? M1(Ht, ldh, k + 1, k + 2) : 0.0;
+    // the pivot decision of step k (F:2541-2556): |b| > |a| swaps; l = a/b, b/a, or 0
+    auto decide = [&](int k, double a, double hs) {
+        const double b = dmul(tau, hs);
         const bool sw = fabs(b) > fabs(a);
         double l;
         if (sw) {
@@ -60,45 +68,68 @@ __global__ void __launch_bounds__(T) shift_lu_kernel(int n, const double* __rest
         } else {
             l = b / a;
         }
-        if (t == 0) {
-            swp[k - 1] = sw ? 1 : 0;
-            M1(Gt, ldg, k, k) = sw ? b : a;
-            M1(Gt, ldg, k, k + 1) = l;
-            if (!sw && a == 0.0 && s_info == 0) s_info = k;
-        }
-        // prefetch Ht[j, k+2] for the next step
-        double hn[E];
+        s_l[k & 1] = l;
+        s_a[k & 1] = a;
+        s_b[k & 1] = b;
+        s_sw[k & 1] = sw ? 1 : 0;
+    };
+    if (t == 0) {
+        s_next[1] = r[0];
+        s_info = 0;
+        if (n >= 2) decide(1, r[0], hsub[0]);
+    }
+    __syncthreads();
+
+    for (int k0 = 1; k0 <= n - 1; k0 += D) {
 #pragma unroll
-        for (int e = 0; e < E; ++e) {
-            const int j = 1 + t + e * T;
-            hn[e] = (j >= k + 1 && j <= n && k + 2 <= n) ? M1(Ht, ldh, j, k + 2) : 0.0;
-        }
-#pragma unroll
-        for (int e = 0; e < E; ++e) {
-            const int j = 1 + t + e * T;
-            if (j >= k + 1 && j <= n) {
-                if (sw) {
-                    const double g = dmul(tau, h[e]);
-                    double gk = g;
-                    double rj = dsub(r[e], dmul(l, g));
-                    if (j == k + 1) {
-                        gk = dadd(g, sigma);              // Gt[k+1,k] += sigma
-                        rj = dsub(rj, dmul(l, sigma));    // r[k+1] -= l*sigma
-                    }
-                    M1(Gt, ldg, j, k) = gk;
-                    r[e] = rj;
-                } else {
-                    const double rj = r[e];
-                    M1(Gt, ldg, j, k) = rj;
-                    double rn = dsub(dmul(tau, h[e]), dmul(l, rj));
-                    if (j == k + 1) rn = dadd(rn, sigma); // r[k+1] += sigma
-                    r[e] = rn;
-                }
-                if (j == k + 1) s_next[(k + 1) & 1] = r[e];  // owner of element k+1
+        for (int d = 0; d < D; ++d) {
+            const int k = k0 + d;
+            if (k > n - 1) break;
+            const double l = s_l[k & 1];
+            const bool sw = s_sw[k & 1] != 0;
+            if (t == 0) {
+                const double a = s_a[k & 1], b = s_b[k & 1];
+                swp[k - 1] = sw ? 1 : 0;
+                M1(Gt, ldg, k, k) = sw ? b : a;
+                M1(Gt, ldg, k, k + 1) = l;
+                if (!sw && a == 0.0 && s_info == 0) s_info = k;
             }
-            h[e] = hn[e];
+#pragma unroll
+            for (int e = 0; e < E; ++e) {
+                const int j = 1 + t + e * T;
+                if (j >= k + 1 && j <= n) {
+                    if (sw) {
+                        const double g = dmul(tau, hq[d][e]);
+                        double gk = g;
+                        double rj = dsub(r[e], dmul(l, g));
+                        if (j == k + 1) {
+                            gk = dadd(g, sigma);              // Gt[k+1,k] += sigma
+                            rj = dsub(rj, dmul(l, sigma));    // r[k+1] -= l*sigma
+                        }
+                        M1(Gt, ldg, j, k) = gk;
+                        r[e] = rj;
+                    } else {
+                        const double rj = r[e];
+                        M1(Gt, ldg, j, k) = rj;
+                        double rn = dsub(dmul(tau, hq[d][e]), dmul(l, rj));
+                        if (j == k + 1) rn = dadd(rn, sigma); // r[k+1] += sigma
+                        r[e] = rn;
+                    }
+                    if (j == k + 1) {  // owner of element k+1: publish it and decide step k+1
+                        s_next[(k + 1) & 1] = r[e];
+                        if (k + 1 <= n - 1) decide(k + 1, r[e], hsub[e]);
+                    }
+                }
+            }
+            // request the row for step k + D into the slot just used
+            const int kf = k + D;
+#pragma unroll
+            for (int e = 0; e < E; ++e) {
+                const int j = 1 + t + e * T;
+                hq[d][e] = (j >= kf && j <= n && kf + 1 <= n) ? M1(Ht, ldh, j, kf + 1) : 0.0;
+            }
+            __syncthreads();
         }
-        __syncthreads();
     }
     // finish (F:2579-2594)
     if (t == 0) {
@@ -113,12 +144,12 @@ __global__ void __launch_bounds__(T) shift_lu_kernel(int n, const double* __rest
     for (int j = 1 + t; j <= n; j += T) rdiag[j - 1] = 1.0 / M1(Gt, ldg, j, j);
 }
 
-template <int T, int E>
+template <int T, int E, int D>
 static cudaError_t launch_shift_T(int n, const double* Ht, int ldh, const double* sig, const double* tau, int s0,
                                   int count, double* Gt, int ldg, uint8_t* swp, double* rd, int32_t* info,
                                   cudaStream_t st)
 {
-    shift_lu_kernel<T, E><<<count, T, 0, st>>>(n, Ht, ldh, sig, tau, s0, Gt, ldg, swp, rd, info);
+    shift_lu_kernel<T, E, D><<<count, T, 0, st>>>(n, Ht, ldh, sig, tau, s0, Gt, ldg, swp, rd, info);
     return cudaGetLastError();
 }
 
@@ -126,12 +157,12 @@ cudaError_t launch_shift_lu(int n, const double* Ht, int ldh, const double* sig,
                             double* Gt, int ldg, uint8_t* swp, double* rd, int32_t* info, cudaStream_t st)
 {
     if (count <= 0 || n <= 0) return cudaSuccess;
-    if (n <= 256) return launch_shift_T<256, 1>(n, Ht, ldh, sig, tau, s0, count, Gt, ldg, swp, rd, info, st);
-    if (n <= 1024) return launch_shift_T<512, 2>(n, Ht, ldh, sig, tau, s0, count, Gt, ldg, swp, rd, info, st);
-    if (n <= 2048) return launch_shift_T<512, 4>(n, Ht, ldh, sig, tau, s0, count, Gt, ldg, swp, rd, info, st);
-    if (n <= 4096) return launch_shift_T<512, 8>(n, Ht, ldh, sig, tau, s0, count, Gt, ldg, swp, rd, info, st);
-    if (n <= 8192) return launch_shift_T<1024, 8>(n, Ht, ldh, sig, tau, s0, count, Gt, ldg, swp, rd, info, st);
-    if (n <= 16384) return launch_shift_T<1024, 16>(n, Ht, ldh, sig, tau, s0, count, Gt, ldg, swp, rd, info, st);
+    if (n <= 256) return launch_shift_T<256, 1, 4>(n, Ht, ldh, sig, tau, s0, count, Gt, ldg, swp, rd, info, st);
+    if (n <= 1024) return launch_shift_T<512, 2, 4>(n, Ht, ldh, sig, tau, s0, count, Gt, ldg, swp, rd, info, st);
+    if (n <= 2048) return launch_shift_T<512, 4, 4>(n, Ht, ldh, sig, tau, s0, count, Gt, ldg, swp, rd, info, st);
+    if (n <= 4096) return launch_shift_T<512, 8, 2>(n, Ht, ldh, sig, tau, s0, count, Gt, ldg, swp, rd, info, st);
+    if (n <= 8192) return launch_shift_T<1024, 8, 1>(n, Ht, ldh, sig, tau, s0, count, Gt, ldg, swp, rd, info, st);
+    if (n <= 16384) return launch_shift_T<1024, 16, 1>(n, Ht, ldh, sig, tau, s0, count, Gt, ldg, swp, rd, info, st);
     return cudaErrorInvalidValue;
 }
 

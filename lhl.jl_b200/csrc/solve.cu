@@ -602,52 +602,74 @@ cudaError_t launch_ldiv(const LdivArgs& a, int nrhs, cudaStream_t st)
     return cudaSuccess;
 }
 
-// ---- residual r = b - (sigma_s I + tau_s J) x, one tile of 64 rows x 8 columns per CTA ----
-constexpr int RT_M = 64, RT_N = 8, RT_K = 32;
+// ---- residual r = b - (sigma_s I + tau_s J) x: tiles of 16 rows x 64 right-hand sides ----
+// 256 threads, thread (row r = t % 16, columns 4 (t / 16) .. +3); k in chunks of 64 through
+// shared memory, the next chunk prefetched into registers while the current one is used.
+constexpr int RM = 16, RN = 64, RK = 64, RTT = 256;
 
-__global__ void __launch_bounds__(256) residual_kernel(int n, const double* __restrict__ J, int ldj,
+__global__ void __launch_bounds__(RTT) residual_kernel(int n, const double* __restrict__ J, int ldj,
                                                        const double* __restrict__ B, int ldb,
                                                        const double* __restrict__ X, int ldx, double* __restrict__ R,
                                                        int ldr, int nrhs, int rhs_per_shift,
                                                        const double* __restrict__ sig, const double* __restrict__ tau,
                                                        const double* __restrict__ done, double tol)
 {
-    __shared__ double sJ[RT_K][RT_M + 1];
-    __shared__ double sX[RT_N][RT_K + 1];
-    const int i0 = blockIdx.x * RT_M, c0 = blockIdx.y * RT_N;
-    if (tile_done(done, tol, c0, RT_N, nrhs)) return;  // converged columns keep their residual
+    __shared__ double Js[RK][RM + 1];
+    __shared__ double Xs[RK][RN + 1];
+    const int i0 = blockIdx.x * RM, c0 = blockIdx.y * RN;
+    if (tile_done(done, tol, c0, RN, nrhs)) return;  // converged columns keep their residual
     const int t = threadIdx.x;
-    const int ti = t & 63, tc = t >> 6;  // 64 rows x 4 column pairs
-    double acc0 = 0.0, acc1 = 0.0;
-    for (int k0 = 0; k0 < n; k0 += RT_K) {
-        for (int e = t; e < RT_K * RT_M; e += 256) {
-            const int ii = e % RT_M, kk = e / RT_M;
+    const int r = t % RM, cg = t / RM;  // cg in 0..15
+    constexpr int JPER = RM * RK / RTT, XPER = RK * RN / RTT;  // 4 and 16
+    double jr[JPER], xr[XPER];
+    auto fetch = [&](int k0) {
+#pragma unroll
+        for (int u = 0; u < JPER; ++u) {
+            const int e = t + u * RTT;
+            const int ii = e % RM, kk = e / RM;  // J rows contiguous
             const int i = i0 + ii, k = k0 + kk;
-            sJ[kk][ii] = (i < n && k < n) ? J[(size_t)k * ldj + i] : 0.0;
+            jr[u] = (i < n && k < n) ? J[(size_t)k * ldj + i] : 0.0;
         }
-        for (int e = t; e < RT_K * RT_N; e += 256) {
-            const int kk = e % RT_K, cc = e / RT_K;
+#pragma unroll
+        for (int u = 0; u < XPER; ++u) {
+            const int e = t + u * RTT;
+            const int kk = e % RK, cc = e / RK;  // X columns contiguous
             const int k = k0 + kk, c = c0 + cc;
-            sX[cc][kk] = (k < n && c < nrhs) ? X[(size_t)c * ldx + k] : 0.0;
+            xr[u] = (k < n && c < nrhs) ? X[(size_t)c * ldx + k] : 0.0;
+        }
+    };
+    double acc[4] = {0.0, 0.0, 0.0, 0.0};
+    fetch(0);
+    for (int k0 = 0; k0 < n; k0 += RK) {
+#pragma unroll
+        for (int u = 0; u < JPER; ++u) {
+            const int e = t + u * RTT;
+            Js[e / RM][e % RM] = jr[u];
+        }
+#pragma unroll
+        for (int u = 0; u < XPER; ++u) {
+            const int e = t + u * RTT;
+            Xs[e % RK][e / RK] = xr[u];
         }
         __syncthreads();
-#pragma unroll 8
-        for (int kk = 0; kk < RT_K; ++kk) {
-            const double jv = sJ[kk][ti];
-            acc0 = dfma(jv, sX[2 * tc][kk], acc0);
-            acc1 = dfma(jv, sX[2 * tc + 1][kk], acc1);
+        if (k0 + RK < n) fetch(k0 + RK);
+#pragma unroll 16
+        for (int kk = 0; kk < RK; ++kk) {
+            const double jv = Js[kk][r];
+#pragma unroll
+            for (int q = 0; q < 4; ++q) acc[q] = dfma(jv, Xs[kk][cg * 4 + q], acc[q]);
         }
         __syncthreads();
     }
-    const int i = i0 + ti;
+    const int i = i0 + r;
     if (i < n) {
-        for (int q = 0; q < 2; ++q) {
-            const int c = c0 + 2 * tc + q;
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+            const int c = c0 + cg * 4 + q;
             if (c < nrhs) {
                 const int s = c / rhs_per_shift;
                 const double xv = X[(size_t)c * ldx + i];
-                const double jx = q == 0 ? acc0 : acc1;
-                R[(size_t)c * ldr + i] = B[(size_t)c * ldb + i] - (sig[s] * xv + tau[s] * jx);
+                R[(size_t)c * ldr + i] = B[(size_t)c * ldb + i] - (sig[s] * xv + tau[s] * acc[q]);
             }
         }
     }
@@ -658,8 +680,8 @@ cudaError_t launch_residual(int n, const double* J, int ldj, const double* B, in
                             cudaStream_t st, const double* done, double tol)
 {
     if (nrhs <= 0 || n <= 0) return cudaSuccess;
-    dim3 grid((n + RT_M - 1) / RT_M, (nrhs + RT_N - 1) / RT_N);
-    residual_kernel<<<grid, 256, 0, st>>>(n, J, ldj, B, ldb, X, ldx, R, ldr, nrhs, rhs_per_shift, sig, tau, done, tol);
+    dim3 grid((n + RM - 1) / RM, (nrhs + RN - 1) / RN);
+    residual_kernel<<<grid, RTT, 0, st>>>(n, J, ldj, B, ldb, X, ldx, R, ldr, nrhs, rhs_per_shift, sig, tau, done, tol);
     return cudaGetLastError();
 }
 
