@@ -23,8 +23,8 @@ struct lhl_ws_s {
     int nzflags;
     // mixed form (LHL_PREC_MIXED) only
     lhl::MixPlan mplan;
-    unsigned long long* mhdr;
-    float *mcval, *mcrow, *mgrows;
+    unsigned long long *mhdr, *mcval, *mcrow;
+    float* mgrows;
 };
 
 struct lhl_shift_s {
@@ -227,8 +227,13 @@ int lhl_reduce(lhl_ws_t ws, const double* dJ, int64_t ldj, int balance, void* st
     if (ws->precision == LHL_PREC_MIXED && n >= 3) {
         // balancing (FP64, the plain kernel's balance-only mode), then the FP32 reduction
         if (!balance) e = lhl::launch_fill_ones(ws->scale, ws->iscale, (int)n, st);
+        // exchange words are tagged with their step: clear the previous reduction's
         if (e == cudaSuccess)
             e = cudaMemsetAsync(ws->mhdr, 0, 2 * (size_t)ws->mplan.grid * sizeof(unsigned long long), st);
+        if (e == cudaSuccess) e = cudaMemsetAsync(ws->mcval, 0, 2 * (size_t)n * sizeof(unsigned long long), st);
+        if (e == cudaSuccess)
+            e = cudaMemsetAsync(ws->mcrow, 0,
+                                2 * (size_t)ws->mplan.grid * ws->mplan.ldr * sizeof(unsigned long long), st);
         if (e == cudaSuccess) e = lhl::launch_reduce(a, balance ? 1 : 0, 0, st);
         if (e != cudaSuccess) return LHL_ERR_CUDA;
         lhl::MixArgs m;

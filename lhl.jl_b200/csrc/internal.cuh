@@ -89,8 +89,8 @@ struct MixArgs {
     double* A;              // balanced J in, factors out (n x n, ld n)
     int64_t* ipiv;
     unsigned long long* hdr;  // 2 x grid: per CTA and step parity, value << 32 | step << 16 | row
-    float* cval;            // 2 x n column values by physical row
-    float* crow;            // 2 x grid x ldr candidate rows
+    unsigned long long* cval;  // 2 x n column values by physical row (tagged words)
+    unsigned long long* crow;  // 2 x grid x ldr candidate rows (tagged words)
     float* grows;           // n x ldr rows when they do not fit in shared memory
     int* err;
     unsigned long long limit_ns;

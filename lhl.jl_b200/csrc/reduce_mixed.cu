@@ -12,9 +12,11 @@
 //
 // Step k (1-based, k = 1..n-2), per CTA:
 //   wait   -- warp 0 polls until every CTA has published step k: a 64-bit header per CTA
-//             (step number, best candidate's logical row and signed column value) stored with
-//             release semantics after the CTA's rows' column-k values (cval) and the
-//             candidate's row (crow).  The poll uses acquire loads and is bounded in wall time.
+//             (step number, best candidate's logical row and signed column value), stored
+//             after the CTA's rows' column-k values (cval) and the candidate's row (crow).
+//             Every exchange word carries its step number, so no store waits for an earlier
+//             one to be acknowledged (no release fences): a reader re-reads a word whose tag
+//             is not yet the step's.  Polls and re-reads are bounded in wall time.
 //             Warp 0 then picks the pivot p (largest |value|, ties to the lowest logical row:
 //             the reference's first maximum, F:799-806) and swaps labels k+1 <-> p.
 //   load   -- swap columns k+1 <-> p in own rows; load the pivot row R from the winner's crow
@@ -23,27 +25,22 @@
 //             the row update A[i,:] -= l_i R):
 //                 c'_i = (A[i,k+1] - l_i R[k+1]) + A[i,k+2:n].l - l_i (R[k+2:n].l)
 //             with both dot products in FP64 (FP32 partial sums of at most 16 terms, added in
-//             FP64).  Warp 0 then publishes step k+1 while warps 1-7 apply the rank-1 row
-//             update to the other own rows; warp 0 updates the candidate row last and returns
-//             to polling.
+//             FP64).  Warp 0 then updates the candidate row and publishes it in the same pass,
+//             and returns to polling, while warps 1-15 apply the rank-1 row update to the
+//             other own rows.
 // At the end every CTA writes its rows, in FP64, to their logical positions of `factors`:
 // the same layout as the plain form (H in the upper Hessenberg part, multipliers below).
 #include "internal.cuh"
 
 namespace lhl {
 
-constexpr int MT = 256;
+constexpr int MT = 512;
 constexpr int MW = MT / 32;
 constexpr int MIX_FLUSH = 16;  // float4 iterations per lane before the FP32 partials go to FP64
 constexpr int MIX_RPC_MAX = 64;
 
-__device__ __forceinline__ void st_release_u64(unsigned long long* p, unsigned long long v)
-{
-    asm volatile("st.release.gpu.global.u64 [%0], %1;" ::"l"(p), "l"(v) : "memory");
-}
-
-// Polling load: relaxed, so that a lane's loads of several headers are in flight together;
-// the poll ends with one acquire fence.
+// Polling load: relaxed, so that a lane's loads of several headers are in flight together.
+// No acquire is needed: every word read after the poll carries its own step tag.
 __device__ __forceinline__ unsigned long long ld_relaxed_u64(const unsigned long long* p)
 {
     unsigned long long v;
@@ -51,7 +48,35 @@ __device__ __forceinline__ unsigned long long ld_relaxed_u64(const unsigned long
     return v;
 }
 
-__device__ __forceinline__ void fence_acq_rel_gpu() { asm volatile("fence.acq_rel.gpu;" ::: "memory"); }
+__device__ __forceinline__ void st_relaxed_u64(unsigned long long* p, unsigned long long v)
+{
+    asm volatile("st.relaxed.gpu.global.u64 [%0], %1;" ::"l"(p), "l"(v) : "memory");
+}
+
+// Exchange words carry their step: value bits << 32 | (step & 0xffff) << 16.  A reader that
+// has seen a CTA's header for step k may still see older words of that CTA (the stores are
+// not ordered), so it re-reads a word until its tag is k, bounded in wall time.
+__device__ __forceinline__ unsigned long long mix_tag(unsigned step, float v)
+{
+    return ((unsigned long long)__float_as_uint(v) << 32) | ((unsigned long long)(step & 0xffffu) << 16);
+}
+
+__device__ __forceinline__ float ld_tagged(const unsigned long long* p, unsigned step, unsigned long long limit_ns,
+                                           bool& ok)
+{
+    unsigned long long v = ld_relaxed_u64(p);
+    if (((unsigned)(v >> 16) & 0xffffu) != (step & 0xffffu)) {
+        const uint64_t t0 = globaltimer_ns();
+        do {
+            v = ld_relaxed_u64(p);
+            if (globaltimer_ns() - t0 > limit_ns) {
+                ok = false;
+                break;
+            }
+        } while (((unsigned)(v >> 16) & 0xffffu) != (step & 0xffffu));
+    }
+    return __uint_as_float((unsigned)(v >> 32));
+}
 
 // header word: value bits << 32 | (step & 0xffff) << 16 | logical row (0 = none)
 __device__ __forceinline__ unsigned long long mix_pack(unsigned int step, int idx, float val)
@@ -169,17 +194,20 @@ __global__ void __launch_bounds__(MT, 1) reduce_mixed_kernel(MixArgs a)
         for (int i = lane; i < nr; i += 32) {
             const int L = r0 + i + 1;
             const float v = rows[(size_t)i * ldr];
-            __stcg(&a.cval[(1 & 1) * n + r0 + i], v);
+            __stcg(&a.cval[(1 & 1) * n + r0 + i], mix_tag(1u, v));
             if (L >= 2 && mix_better(v, L, bv, bi)) { bv = v; bi = L; bl = i; }
         }
         warp_best(bv, bi, bl);
         if (bl >= 0) {
-            const float4* src = reinterpret_cast<const float4*>(rows + (size_t)bl * ldr);
-            float4* dst = reinterpret_cast<float4*>(a.crow + ((size_t)(1 & 1) * G + b) * ldr);
-            for (int g = lane; g < (ldr >> 2); g += 32) __stcg(&dst[g], src[g]);
+            const float2* src = reinterpret_cast<const float2*>(rows + (size_t)bl * ldr);
+            ulonglong2* dst = reinterpret_cast<ulonglong2*>(a.crow + ((size_t)(1 & 1) * G + b) * ldr);
+            for (int g = lane; g < (ldr >> 1); g += 32) {
+                const float2 x = src[g];
+                __stcg(&dst[g], make_ulonglong2(mix_tag(1u, x.x), mix_tag(1u, x.y)));
+            }
         }
         __syncwarp();
-        if (lane == 0) st_release_u64(&hdr[(1 & 1) * G + b], mix_pack(1u, bi, bv));
+        if (lane == 0) st_relaxed_u64(&hdr[(1 & 1) * G + b], mix_pack(1u, bi, bv));
     }
 
     const uint64_t t_start = globaltimer_ns();
@@ -233,7 +261,6 @@ __global__ void __launch_bounds__(MT, 1) reduce_mixed_kernel(MixArgs a)
                     if (__shfl_sync(0xffffffffu, bad, 0)) { ok = 0; break; }
                 }
             }
-            fence_acq_rel_gpu();  // the CTAs' column values and rows are read after this
             float bv = 0.f;
             int bi = 0, bs = -1;
             if (ok) {
@@ -282,29 +309,39 @@ __global__ void __launch_bounds__(MT, 1) reduce_mixed_kernel(MixArgs a)
                 ri[p - 1] = u;
             }
         {
-            const float* src = win >= 0 ? a.crow + ((size_t)par * G + win) * ldr : nullptr;
-            const float* cv = a.cval + (size_t)par * n;
+            const unsigned long long* src = win >= 0 ? a.crow + ((size_t)par * G + win) * ldr : nullptr;
+            const unsigned long long* cv = a.cval + (size_t)par * n;
+            bool ok = true;
             for (int base = 0; base < n; base += 4 * MT) {
-                float rv[4], cvv[4];
+                unsigned long long rv[4], cvv[4];
 #pragma unroll
                 for (int u = 0; u < 4; ++u) {
                     const int c = k + 1 + base + t + u * MT;  // logical column of R
                     const int sc = c == k + 1 ? p : (c == p ? k + 1 : c);
-                    rv[u] = (src && c <= n) ? __ldcg(&src[sc - 1]) : 0.f;
+                    rv[u] = (src && c <= n) ? ld_relaxed_u64(&src[sc - 1]) : mix_tag((unsigned)k, 0.f);
                     const int q = base + t + u * MT;
-                    cvv[u] = q < n ? __ldcg(&cv[q]) : 0.f;
+                    cvv[u] = q < n ? ld_relaxed_u64(&cv[q]) : mix_tag((unsigned)k, 0.f);
                 }
 #pragma unroll
                 for (int u = 0; u < 4; ++u) {
                     const int c = k + 1 + base + t + u * MT;
-                    if (c <= n) R[c - 1] = rv[u];
+                    const int sc = c == k + 1 ? p : (c == p ? k + 1 : c);
+                    const unsigned want = (unsigned)k & 0xffffu;
+                    float r = __uint_as_float((unsigned)(rv[u] >> 32));
+                    if (((unsigned)(rv[u] >> 16) & 0xffffu) != want) r = ld_tagged(&src[sc - 1], k, a.limit_ns, ok);
+                    if (c <= n) R[c - 1] = r;
                     const int q = base + t + u * MT;
                     if (q < n) {
                         const int j = lg[q];
-                        if (j >= k + 2) lv[j - 1] = piv != 0.f ? cvv[u] / piv : 0.f;
+                        if (j >= k + 2) {
+                            float cq = __uint_as_float((unsigned)(cvv[u] >> 32));
+                            if (((unsigned)(cvv[u] >> 16) & 0xffffu) != want) cq = ld_tagged(&cv[q], k, a.limit_ns, ok);
+                            lv[j - 1] = piv != 0.f ? cq / piv : 0.f;
+                        }
                     }
                 }
             }
+            if (!ok) atomicCAS(a.err, 0, (int)LHL_ERR_TIMEOUT);
         }
         __syncthreads();
         mark(1);
@@ -337,7 +374,7 @@ __global__ void __launch_bounds__(MT, 1) reduce_mixed_kernel(MixArgs a)
                 const float c32 = (float)cn;
                 ri[k] = c32;
                 s_li[i] = li;
-                if (k + 1 <= n - 2) __stcg(&a.cval[(size_t)np * n + r0 + i], c32);
+                if (k + 1 <= n - 2) __stcg(&a.cval[(size_t)np * n + r0 + i], mix_tag((unsigned)(k + 1), c32));
                 if (L >= k + 2 && mix_better(c32, L, bv, bi)) { bv = c32; bi = L; bl = i; }
             }
             warp_best(bv, bi, bl);
@@ -351,29 +388,30 @@ __global__ void __launch_bounds__(MT, 1) reduce_mixed_kernel(MixArgs a)
         mark(2);
         const int cl = s_cand;
         if (warp == 0) {
-            // ---- publish step k+1, then the candidate row's own row update ----
-            if (k + 1 <= n - 2) {
-                const int np = (k + 1) & 1;
-                if (cl >= 0) {
-                    const float4* rc = reinterpret_cast<const float4*>(rows + (size_t)cl * ldr);
-                    const float4* R4 = reinterpret_cast<const float4*>(R);
-                    float4* dst = reinterpret_cast<float4*>(a.crow + ((size_t)np * G + b) * ldr);
-                    const float li = s_li[cl];
-                    for (int g = ((k + 1) >> 2) + lane; g < (ldr >> 2); g += 32) {
-                        float4 x = rc[g];
-                        const float4 y = R4[g];
-                        x.x = fmaf(-li, y.x, x.x);
-                        x.y = fmaf(-li, y.y, x.y);
-                        x.z = fmaf(-li, y.z, x.z);
-                        x.w = fmaf(-li, y.w, x.w);
-                        __stcg(&dst[g], x);
-                    }
+            // ---- publish step k+1: the candidate row after this step's row update, written to
+            // the exchange and back into its own row in one pass ----
+            const int np = (k + 1) & 1;
+            const bool pub = k + 1 <= n - 2;
+            if (cl >= 0) {
+                float* rc = rows + (size_t)cl * ldr;
+                const float li = s_li[cl];
+                ulonglong2* dst = reinterpret_cast<ulonglong2*>(a.crow + ((size_t)np * G + b) * ldr);
+                const unsigned st = (unsigned)(k + 1);
+                for (int g = ((k + 1) >> 1) + lane; g < (ldr >> 1); g += 32) {
+                    const int c = 2 * g;  // 0-based columns c, c+1; only c >= k+1 change
+                    float x0 = rc[c], x1 = rc[c + 1];
+                    if (c >= k + 1) x0 = fmaf(-li, R[c], x0);
+                    x1 = fmaf(-li, R[c + 1], x1);  // c + 1 >= k + 1 always
+                    if (pub) __stcg(&dst[g], make_ulonglong2(mix_tag(st, x0), mix_tag(st, x1)));
+                    rc[c] = x0;
+                    rc[c + 1] = x1;
                 }
+            }
+            if (pub) {
                 __syncwarp();
-                if (lane == 0) st_release_u64(&hdr[np * G + b], mix_pack((unsigned)(k + 1), s_p, s_piv));
+                if (lane == 0) st_relaxed_u64(&hdr[np * G + b], mix_pack((unsigned)(k + 1), s_p, s_piv));
             }
             mark(3);
-            if (cl >= 0 && s_li[cl] != 0.f) mix_axpy(rows + (size_t)cl * ldr, R, s_li[cl], k + 1, ldr, lane);
         } else {
             // ---- rank-1 row update of the other own active rows ----
             for (int v = warp - 1; v < nr; v += MW - 1) {
