@@ -17,6 +17,7 @@ struct lhl_ws_s {
     unsigned int* bar;
     unsigned long long limit_ns;
     unsigned long long* ptimes;
+    double* linv;  // mixed form: inverses of L's 64 x 64 diagonal blocks
     double* ybuf;  // ldiv scratch: n x ycap right-hand sides
     int ycap;
     int* zflags;   // ldiv scratch: ready flags, ceil(n/64) x ceil(ycap/4)
@@ -30,6 +31,7 @@ struct lhl_ws_s {
 struct lhl_shift_s {
     int64_t n, nshifts, ldg;
     double *Gt, *rdiag, *sigma, *tau;
+    double* uinv;  // mixed form: inverses of U's 32 x 32 diagonal blocks (n / 32 blocks per shift)
     uint8_t* swap;
     int32_t* info;
 };
@@ -49,7 +51,7 @@ static void ws_free(lhl_ws_t w)
     if (!w) return;
     void* ptrs[] = {w->F, w->Ht, w->scale, w->iscale, w->B0, w->part, w->tab, w->cand_v, w->cand_s, w->buf2, w->tsnap,
                     w->bsum, w->bfac, w->ipiv, w->perm, w->iperm, w->cand_i, w->bflag, w->err, w->bar,
-                    w->ptimes, w->mhdr, w->mcval, w->mcrow, w->mgrows, w->ybuf, w->zflags};
+                    w->ptimes, w->mhdr, w->mcval, w->mcrow, w->mgrows, w->ybuf, w->zflags, w->linv};
     for (void* p : ptrs)
         if (p) cudaFree(p);
     delete w;
@@ -117,6 +119,7 @@ int lhl_ws_create(int64_t n, int precision, lhl_ws_t* out)
         A_(mcval, 2 * (size_t)n);
         A_(mcrow, 2 * g * ldr);
         A_(mgrows, w->mplan.smem_rows ? 1 : (size_t)n * ldr);
+        A_(linv, (size_t)((n + 63) / 64) * 64 * 64);
     }
 #undef A_
     if (e == cudaSuccess) e = cudaMemset(w->err, 0, 4 * sizeof(int));
@@ -249,6 +252,7 @@ int lhl_reduce(lhl_ws_t ws, const double* dJ, int64_t ldj, int balance, void* st
         m.limit_ns = ws->limit_ns;
         m.ptimes = ws->ptimes;
         e = lhl::launch_reduce_mixed(m, ws->mplan, st);
+        if (e == cudaSuccess) e = lhl::launch_linv((int)n, ws->F, (int)n, ws->linv, st);
         if (e != cudaSuccess) return LHL_ERR_CUDA;
         return cuda_status(lhl::launch_ht_perm((int)n, ws->F, ws->Ht, ws->ipiv, ws->perm, ws->iperm, st));
     }
@@ -286,6 +290,7 @@ int lhl_shift_create(int64_t n, int64_t nshifts, lhl_shift_t* out)
     if (e == cudaSuccess) e = dalloc(&s->tau, nshifts);
     if (e == cudaSuccess) e = dalloc(&s->swap, (size_t)n * nshifts);
     if (e == cudaSuccess) e = dalloc(&s->info, nshifts);
+    if (e == cudaSuccess) e = dalloc(&s->uinv, (size_t)((n + 31) / 32) * 32 * 32 * (size_t)nshifts);
     if (e == cudaSuccess) e = cudaMemset(s->Gt, 0, (gsz ? gsz : 1) * sizeof(double));
     if (e == cudaSuccess) e = cudaMemset(s->info, 0, nshifts * sizeof(int32_t));
     if (e == cudaSuccess) e = cudaMemset(s->sigma, 0, nshifts * sizeof(double));
@@ -301,7 +306,7 @@ int lhl_shift_create(int64_t n, int64_t nshifts, lhl_shift_t* out)
 int lhl_shift_destroy(lhl_shift_t s)
 {
     if (!s) return LHL_ERR_ARG;
-    void* ptrs[] = {s->Gt, s->rdiag, s->sigma, s->tau, s->swap, s->info};
+    void* ptrs[] = {s->Gt, s->rdiag, s->sigma, s->tau, s->swap, s->info, s->uinv};
     for (void* p : ptrs)
         if (p) cudaFree(p);
     delete s;
@@ -340,6 +345,8 @@ int lhl_shift_batched(lhl_shift_t sh, lhl_ws_t ws, int64_t s0, int64_t count, co
     if (e != cudaSuccess) return LHL_ERR_CUDA;
     e = lhl::launch_shift_lu((int)ws->n, ws->Ht, (int)ws->n, sh->sigma + s0, sh->tau + s0, (int)s0, (int)count,
                              sh->Gt, (int)sh->ldg, sh->swap, sh->rdiag, sh->info, st);
+    if (e == cudaSuccess && ws->precision == LHL_PREC_MIXED)
+        e = lhl::launch_uinv((int)ws->n, sh->Gt, (int)sh->ldg, sh->rdiag, (int)s0, (int)count, sh->uinv, st);
     return cuda_status(e);
 }
 
@@ -354,6 +361,8 @@ int lhl_shift(lhl_shift_t sh, lhl_ws_t ws, int64_t slot, double sigma, double ta
     if (e != cudaSuccess) return LHL_ERR_CUDA;
     e = lhl::launch_shift_lu((int)ws->n, ws->Ht, (int)ws->n, sh->sigma + slot, sh->tau + slot, (int)slot, 1,
                              sh->Gt, (int)sh->ldg, sh->swap, sh->rdiag, sh->info, st);
+    if (e == cudaSuccess && ws->precision == LHL_PREC_MIXED)
+        e = lhl::launch_uinv((int)ws->n, sh->Gt, (int)sh->ldg, sh->rdiag, (int)slot, 1, sh->uinv, st);
     return cuda_status(e);
 }
 
@@ -381,6 +390,7 @@ static int ldiv_common(lhl_shift_t sh, lhl_ws_t ws, double* dX, int64_t ldx, int
     a.rhs_per_shift = 1;
     a.Y = ws->ybuf;
     a.ycap = ws->ycap;
+    a.linv = ws->linv;  // null for the plain form
     a.zflags = ws->zflags;
     a.nzflags = ws->nzflags;
     a.err = ws->err;
@@ -392,6 +402,7 @@ static int ldiv_common(lhl_shift_t sh, lhl_ws_t ws, double* dX, int64_t ldx, int
         a.rdiag = sh->rdiag;
         a.rhs_per_shift = (int)rps;
         a.nshifts = (int)sh->nshifts;
+        a.uinv = ws->precision == LHL_PREC_MIXED ? sh->uinv : nullptr;
     }
     return cuda_status(lhl::launch_ldiv(a, (int)nrhs, st));
 }
@@ -482,6 +493,8 @@ int lhl_refine_tol(lhl_shift_t sh, lhl_ws_t ws, const double* dJ, int64_t ldj, c
         a.rdiag = sh->rdiag;
         a.rhs_per_shift = (int)rhs_per_shift;
         a.nshifts = (int)sh->nshifts;
+        a.uinv = ws->precision == LHL_PREC_MIXED ? sh->uinv : nullptr;
+        a.linv = ws->linv;
         a.done = dres;
         a.tol = tol;
         a.Y = ws->ybuf;

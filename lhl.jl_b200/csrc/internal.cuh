@@ -55,6 +55,8 @@ struct LdivArgs {
     double* Y;            // ldiv scratch: n x ycap (the workspace's)
     int ycap;
     int nshifts;          // shift slots in the batch at Gt (for the tensor map over all of them)
+    const double* uinv;   // mixed form: inverses of U's 32 x 32 diagonal blocks per shift, or null
+    const double* linv;   // mixed form: inverses of L's 64 x 64 diagonal blocks, or null
     int* zflags;          // ldiv scratch: ready flags of the blocked forward substitution
     int nzflags;
     int* err;             // bounded-wait status (the workspace's error word)
@@ -79,6 +81,7 @@ struct ZArgs {
     int nflags;
     const double* done;  // optional: a tile whose columns all have done[c] <= tol is skipped
     double tol;
+    const double* linv;  // zinv, mixed form: inverses of L's 64 x 64 diagonal blocks
     int* err;
     unsigned long long limit_ns;
 };
@@ -122,6 +125,9 @@ cudaError_t launch_shift_lu(int n, const double* Ht, int ldh, const double* sig,
                             double* Gt, int ldg, uint8_t* swp, double* rd, int32_t* info, cudaStream_t st);
 
 cudaError_t launch_ldiv(const LdivArgs& a, int nrhs, cudaStream_t st);
+cudaError_t launch_linv(int n, const double* F, int ldf, double* linv, cudaStream_t st);
+cudaError_t launch_uinv(int n, const double* Gt, int ldg, const double* rd, int s0, int count, double* uinv,
+                        cudaStream_t st);
 cudaError_t launch_residual(int n, const double* J, int ldj, const double* B, int ldb, const double* X, int ldx,
                             double* R, int ldr, int nrhs, int rhs_per_shift, const double* sig, const double* tau,
                             cudaStream_t st, const double* done = nullptr, double tol = 0.0);

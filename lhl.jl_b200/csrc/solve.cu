@@ -50,7 +50,7 @@ constexpr int ZC = 4;    // right-hand sides per task
 constexpr int ZIT = 256;
 
 template <bool MUL>
-__global__ void __launch_bounds__(ZIT) zl_kernel(ZArgs z)
+__global__ void __launch_bounds__(ZIT, 2) zl_kernel(ZArgs z)
 {
     __shared__ double Lt[ZR][ZR + 1];
     __shared__ double Ys[ZR][ZC];
@@ -78,14 +78,19 @@ __global__ void __launch_bounds__(ZIT) zl_kernel(ZArgs z)
         // L tiles are software-pipelined: tile j+1 is in registers while tile j is used
         constexpr int PER = ZR * ZR / ZIT;  // 16 entries per thread
         double lreg[PER];
+        const bool dinv = !MUL && z.linv != nullptr;  // mixed form: diagonal blocks by their inverses
         auto load_tile = [&](int j) {
 #pragma unroll
             for (int u = 0; u < PER; ++u) {
                 const int e = t + u * ZIT;
                 const int rr = e & (ZR - 1), qq = e >> 6;
                 const int gr = i * ZR + rr, q = j * ZR + qq;
-                // L[row][q] = F[(q-1) ldf + row] for 1 <= q <= n-2 and row >= q+1, else 0
-                lreg[u] = (gr < n && q >= 1 && q <= n - 2 && gr >= q + 1) ? z.F[(size_t)(q - 1) * z.ldf + gr] : 0.0;
+                if (dinv && j == i) {
+                    lreg[u] = z.linv[((size_t)i * ZR + rr) * ZR + qq];  // (L_ii)^-1, row-major
+                } else {
+                    // L[row][q] = F[(q-1) ldf + row] for 1 <= q <= n-2 and row >= q+1, else 0
+                    lreg[u] = (gr < n && q >= 1 && q <= n - 2 && gr >= q + 1) ? z.F[(size_t)(q - 1) * z.ldf + gr] : 0.0;
+                }
             }
         };
         load_tile(0);
@@ -135,6 +140,25 @@ __global__ void __launch_bounds__(ZIT) zl_kernel(ZArgs z)
                 if (MUL) acc += s0 + s1;
                 else acc -= s0 + s1;
                 __syncthreads();
+            } else if (dinv) {
+                // diagonal block: y_i = (L_ii)^-1 acc, a 64 x 64 product
+                Ys[r][jr] = acc;
+                __syncthreads();
+                double s0 = 0.0, s1 = 0.0, s2 = 0.0, s3 = 0.0;
+#pragma unroll 4
+                for (int qq = 0; qq < ZR; qq += 4) {
+                    s0 = dfma(Lt[r][qq], Ys[qq][jr], s0);
+                    s1 = dfma(Lt[r][qq + 1], Ys[qq + 1][jr], s1);
+                    s2 = dfma(Lt[r][qq + 2], Ys[qq + 2][jr], s2);
+                    s3 = dfma(Lt[r][qq + 3], Ys[qq + 3][jr], s3);
+                }
+                if (live) z.dst[(size_t)col * z.ldd + row] = (s0 + s1) + (s2 + s3);
+                __syncthreads();
+                if (t == 0) {
+                    __threadfence();
+                    asm volatile("st.release.gpu.global.s32 [%0], %1;" ::"l"(z.flags + (size_t)i * ntile + c), "r"(1)
+                                 : "memory");
+                }
             } else {
                 // diagonal block: unit lower solve, one warp per right-hand side
                 Ys[r][jr] = acc;
@@ -255,6 +279,96 @@ __global__ void __launch_bounds__(SOLVE_T) hess_kernel(LdivArgs a, double* Y, in
     for (int i = t; i < n; i += SOLVE_T) yg[i] = y[i];
 }
 
+// Mixed form: inverses of the unit lower 64 x 64 diagonal blocks of L (shift-independent,
+// formed once per reduction), so that the forward substitution's diagonal step is a
+// product.  One CTA of 64 threads per block; thread c forms column c by substitution on e_c.
+// Stored row-major: linv[(i * 64 + r) * 64 + c].
+__global__ void __launch_bounds__(ZR) linv_kernel(int n, const double* __restrict__ F, int ldf,
+                                                  double* __restrict__ linv)
+{
+    extern __shared__ double lsm[];
+    double(*T)[ZR + 1] = reinterpret_cast<double(*)[ZR + 1]>(lsm);
+    double(*X)[ZR + 1] = reinterpret_cast<double(*)[ZR + 1]>(lsm + ZR * (ZR + 1));
+    const int i = blockIdx.x, c = threadIdx.x;
+    for (int rr = 0; rr < ZR; ++rr) {  // T[rr][q] = L[row][col] strictly below the diagonal
+        const int gr = i * ZR + rr, q = i * ZR + c;
+        T[rr][c] = (gr < n && q >= 1 && q <= n - 2 && gr >= q + 1) ? F[(size_t)(q - 1) * ldf + gr] : 0.0;
+    }
+    __syncthreads();
+    for (int rr = 0; rr < ZR; ++rr) {
+        double acc = 0.0;
+        if (rr == c) acc = 1.0;
+        else if (rr > c)
+            for (int q = c; q < rr; ++q) acc = dfma(-T[rr][q], X[q][c], acc);
+        X[rr][c] = acc;
+    }
+    __syncthreads();
+    for (int rr = 0; rr < ZR; ++rr) linv[((size_t)i * ZR + rr) * ZR + c] = X[rr][c];
+}
+
+cudaError_t launch_linv(int n, const double* F, int ldf, double* linv, cudaStream_t st)
+{
+    if (n <= 0) return cudaSuccess;
+    const size_t smem = 2 * (size_t)ZR * (ZR + 1) * sizeof(double);
+    static bool attr = false;
+    if (!attr) {
+        cudaError_t e = cudaFuncSetAttribute(linv_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        if (e != cudaSuccess) return e;
+        attr = true;
+    }
+    linv_kernel<<<(n + ZR - 1) / ZR, ZR, smem, st>>>(n, F, ldf, linv);
+    return cudaGetLastError();
+}
+
+// Mixed form: inverses of the 32 x 32 diagonal blocks of each shift's U (the blocks of the
+// back substitution below: rows r0..r1, r1 = n - 32 b), so that the back substitution's
+// triangle step is a matrix-vector product instead of a 32-step recurrence.  One warp per
+// (shift, block); lane c forms column c of the inverse by substitution on e_c.  Stored
+// column by column: element (i, c) at uinv[((s * nblocks + b) * 32 + c) * 32 + i].  Not used by the plain form, whose
+// solves keep the backward-stable substitution.
+constexpr int UW = 2;  // warps (blocks) per CTA
+
+__global__ void __launch_bounds__(UW * 32) uinv_kernel(int n, const double* __restrict__ Gt_all, int ldg,
+                                                      const double* __restrict__ rd_all, int s0,
+                                                      double* __restrict__ uinv_all)
+{
+    __shared__ double T[UW][BS][BS + 1];
+    __shared__ double X[UW][BS][BS + 1];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int nblocks = (n + BS - 1) / BS;
+    const int b = blockIdx.x * UW + warp;
+    if (b >= nblocks) return;
+    const int s = s0 + blockIdx.y;
+    const double* Gt = Gt_all + (size_t)s * ldg * n;
+    const double* rd = rd_all + (size_t)s * n;
+    const int r1 = n - BS * b, r0 = max(r1 - (BS - 1), 1), bw = r1 - r0 + 1;
+    for (int i = 0; i < BS; ++i)  // T[i][j] = U[r0 + i, r0 + j] = Gt[r0 + j, r0 + i]
+        T[warp][i][lane] = (i < bw && lane < bw && lane >= i) ? M1(Gt, ldg, r0 + lane, r0 + i) : 0.0;
+    __syncwarp();
+    for (int i = BS - 1; i >= 0; --i) {
+        if (lane < bw && i <= lane) {
+            double acc = (i == lane) ? 1.0 : 0.0;
+            for (int j = i + 1; j <= lane; ++j) acc = dfma(-T[warp][i][j], X[warp][j][lane], acc);
+            X[warp][i][lane] = acc * rd[r0 + i - 1];
+        } else {
+            X[warp][i][lane] = 0.0;
+        }
+        __syncwarp();
+    }
+    double* out = uinv_all + ((size_t)blockIdx.y * nblocks + b) * BS * BS;  // column c at out + 32 c
+    for (int c = 0; c < BS; ++c) out[c * BS + lane] = X[warp][lane][c];
+}
+
+cudaError_t launch_uinv(int n, const double* Gt, int ldg, const double* rd, int s0, int count, double* uinv,
+                        cudaStream_t st)
+{
+    if (n <= 0 || count <= 0) return cudaSuccess;
+    const int nblocks = (n + BS - 1) / BS;
+    uinv_kernel<<<dim3((nblocks + UW - 1) / UW, count), UW * 32, 0, st>>>(n, Gt, ldg, rd, s0,
+                                                                       uinv + (size_t)s0 * nblocks * BS * BS);
+    return cudaGetLastError();
+}
+
 // The same Hessenberg solve with Gt streamed by TMA (even n): the back substitution's 32-row
 // blocks read their 32 columns of Gt (rows r0..n) as 128 x 32 boxes through a ring of `ns`
 // shared-memory slots.  Warp 16 is the producer: it requests boxes in consumption order as
@@ -359,6 +473,7 @@ __global__ void __launch_bounds__(HT) hess_tma_kernel(LdivArgs a, double* Y, int
 {
     extern __shared__ __align__(1024) double hsm[];
     __shared__ __align__(8) uint64_t full[HB_MAXSLOTS], empty[HB_MAXSLOTS];
+    __shared__ __align__(16) double Xs[BS * BS];  // mixed form: the current block's inverse
     __shared__ double tri[BS][BS + 1];
     __shared__ double sj[BS];
     __shared__ int s_bad;
@@ -427,6 +542,17 @@ __global__ void __launch_bounds__(HT) hess_tma_kernel(LdivArgs a, double* Y, int
         const int bw = r1 - r0 + 1;
         const int nk = (n - r0 + HB_ROWS) / HB_ROWS;
         double acc0 = 0.0, acc1 = 0.0;  // columns jj = warp and warp + 16
+        if (a.uinv && warp == 0) {  // mixed form: the block's inverse into shared memory, async
+            const char* X = reinterpret_cast<const char*>(a.uinv + ((size_t)s * nblocks + b) * BS * BS);
+#pragma unroll
+            for (int q = 0; q < BS * BS * 8 / 16 / 32; ++q) {
+                const int off = (q * 32 + lane) * 16;
+                asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(smem_u32(reinterpret_cast<char*>(Xs) + off)),
+                             "l"(X + off)
+                             : "memory");
+            }
+            asm volatile("cp.async.commit_group;" ::: "memory");
+        }
         for (int k = 0; k < nk; ++k, ++u) {
             const int slot = u % ns;
             if (!bad && !mbar_wait_ns(&full[slot], (uint32_t)((u / ns) & 1), a.limit_ns)) {
@@ -464,7 +590,23 @@ __global__ void __launch_bounds__(HT) hess_tma_kernel(LdivArgs a, double* Y, int
             if (warp + HCONS < bw) sj[warp + HCONS] = acc1;
         }
         cons_sync();
-        if (warp == 0) {
+        if (warp == 0 && a.uinv) {
+            // x_block = Ub^-1 (y_block - sums): a 32 x 32 matrix-vector product
+            const int i = r0 + lane;
+            const double rhs = (i <= r1) ? y[i - 1] - sj[lane] : 0.0;
+            asm volatile("cp.async.wait_all;" ::: "memory");
+            __syncwarp();
+            double p0 = 0.0, p1 = 0.0, p2 = 0.0, p3 = 0.0;
+#pragma unroll
+            for (int c = 0; c < BS; c += 4) {
+                p0 = dfma(Xs[c * BS + lane], __shfl_sync(0xffffffffu, rhs, c), p0);
+                p1 = dfma(Xs[(c + 1) * BS + lane], __shfl_sync(0xffffffffu, rhs, c + 1), p1);
+                p2 = dfma(Xs[(c + 2) * BS + lane], __shfl_sync(0xffffffffu, rhs, c + 2), p2);
+                p3 = dfma(Xs[(c + 3) * BS + lane], __shfl_sync(0xffffffffu, rhs, c + 3), p3);
+            }
+            __syncwarp();  // Xs is refilled at the next block's start
+            if (i <= r1) y[i - 1] = (p0 + p1) + (p2 + p3);
+        } else if (warp == 0) {
             const int i = r0 + lane;
             double yi = (i <= r1) ? y[i - 1] - sj[lane] : 0.0;
             const double rdi = (i <= r1) ? rd[i - 1] : 0.0;
@@ -532,6 +674,7 @@ cudaError_t launch_ldiv(const LdivArgs& a, int nrhs, cudaStream_t st)
     z.err = a.err;
     z.limit_ns = a.limit_ns;
     z.tol = a.tol;
+    z.linv = a.linv;
     if (!a.Y || a.ycap <= 0 || !a.zflags || !a.err) return cudaErrorInvalidValue;
     if (a.mode == 1) {  // applyZinv: x <- L^-1 P^-1 D^-1 x, through the scratch
         for (int c0 = 0; c0 < nrhs; c0 += a.ycap) {
@@ -605,8 +748,9 @@ cudaError_t launch_ldiv(const LdivArgs& a, int nrhs, cudaStream_t st)
 // ---- residual r = b - (sigma_s I + tau_s J) x: tiles of 16 rows x 64 right-hand sides ----
 // 256 threads, thread (row r = t % 16, columns 4 (t / 16) .. +3); k in chunks of 64 through
 // shared memory, the next chunk prefetched into registers while the current one is used.
-constexpr int RM = 16, RN = 64, RK = 64, RTT = 256;
+constexpr int RM = 16, RK = 64, RTT = 256;
 
+template <int CPT>  // columns per thread: tiles of 16 CPT right-hand sides
 __global__ void __launch_bounds__(RTT) residual_kernel(int n, const double* __restrict__ J, int ldj,
                                                        const double* __restrict__ B, int ldb,
                                                        const double* __restrict__ X, int ldx, double* __restrict__ R,
@@ -614,12 +758,13 @@ __global__ void __launch_bounds__(RTT) residual_kernel(int n, const double* __re
                                                        const double* __restrict__ sig, const double* __restrict__ tau,
                                                        const double* __restrict__ done, double tol)
 {
+    constexpr int RN = 16 * CPT;
     __shared__ double Js[RK][RM + 1];
     __shared__ double Xs[RK][RN + 1];
     const int i0 = blockIdx.x * RM, c0 = blockIdx.y * RN;
     if (tile_done(done, tol, c0, RN, nrhs)) return;  // converged columns keep their residual
     const int t = threadIdx.x;
-    const int r = t % RM, cg = t / RM;  // cg in 0..15
+    const int r = t % RM, cg = t / RM;  // cg in 0..15, columns cg*CPT ..
     constexpr int JPER = RM * RK / RTT, XPER = RK * RN / RTT;  // 4 and 16
     double jr[JPER], xr[XPER];
     auto fetch = [&](int k0) {
@@ -638,7 +783,9 @@ __global__ void __launch_bounds__(RTT) residual_kernel(int n, const double* __re
             xr[u] = (k < n && c < nrhs) ? X[(size_t)c * ldx + k] : 0.0;
         }
     };
-    double acc[4] = {0.0, 0.0, 0.0, 0.0};
+    double acc[CPT];
+#pragma unroll
+    for (int q = 0; q < CPT; ++q) acc[q] = 0.0;
     fetch(0);
     for (int k0 = 0; k0 < n; k0 += RK) {
 #pragma unroll
@@ -657,15 +804,15 @@ __global__ void __launch_bounds__(RTT) residual_kernel(int n, const double* __re
         for (int kk = 0; kk < RK; ++kk) {
             const double jv = Js[kk][r];
 #pragma unroll
-            for (int q = 0; q < 4; ++q) acc[q] = dfma(jv, Xs[kk][cg * 4 + q], acc[q]);
+            for (int q = 0; q < CPT; ++q) acc[q] = dfma(jv, Xs[kk][cg * CPT + q], acc[q]);
         }
         __syncthreads();
     }
     const int i = i0 + r;
     if (i < n) {
 #pragma unroll
-        for (int q = 0; q < 4; ++q) {
-            const int c = c0 + cg * 4 + q;
+        for (int q = 0; q < CPT; ++q) {
+            const int c = c0 + cg * CPT + q;
             if (c < nrhs) {
                 const int s = c / rhs_per_shift;
                 const double xv = X[(size_t)c * ldx + i];
@@ -680,8 +827,15 @@ cudaError_t launch_residual(int n, const double* J, int ldj, const double* B, in
                             cudaStream_t st, const double* done, double tol)
 {
     if (nrhs <= 0 || n <= 0) return cudaSuccess;
-    dim3 grid((n + RM - 1) / RM, (nrhs + RN - 1) / RN);
-    residual_kernel<<<grid, RTT, 0, st>>>(n, J, ldj, B, ldb, X, ldx, R, ldr, nrhs, rhs_per_shift, sig, tau, done, tol);
+    if (done) {  // refinement steps: narrow tiles, so that converged columns cost nothing
+        dim3 grid((n + RM - 1) / RM, (nrhs + 15) / 16);
+        residual_kernel<1><<<grid, RTT, 0, st>>>(n, J, ldj, B, ldb, X, ldx, R, ldr, nrhs, rhs_per_shift, sig, tau, done,
+                                                 tol);
+    } else {
+        dim3 grid((n + RM - 1) / RM, (nrhs + 63) / 64);
+        residual_kernel<4><<<grid, RTT, 0, st>>>(n, J, ldj, B, ldb, X, ldx, R, ldr, nrhs, rhs_per_shift, sig, tau, done,
+                                                 tol);
+    }
     return cudaGetLastError();
 }
 
