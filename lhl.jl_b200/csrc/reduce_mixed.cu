@@ -13,7 +13,8 @@
 // Step k (1-based, k = 1..n-2), per CTA:
 //   wait   -- warp 0 polls until every CTA has published step k: a 64-bit header per CTA
 //             (step number, best candidate's logical row and signed column value), stored
-//             after the CTA's rows' column-k values (cval) and the candidate's row (crow).
+//             after the CTA's rows' column-k values (cval) and before the candidate's row
+//             (crow), which is written while the header travels.
 //             Every exchange word carries its step number, so no store waits for an earlier
 //             one to be acknowledged (no release fences): a reader re-reads a word whose tag
 //             is not yet the step's.  Polls and re-reads are bounded in wall time.
@@ -212,7 +213,8 @@ __global__ void __launch_bounds__(MT, 1) reduce_mixed_kernel(MixArgs a)
 
     const uint64_t t_start = globaltimer_ns();
     // CTA 0's time per sub-phase, summed over steps (probe slots 0-4: wait and pivot choice,
-    // interchange and loads, dot products and new column, publication, row update)
+    // interchange and loads, dot products and new column, publication, row update; slots 5
+    // and 6 split the first and third: the poll alone, the dot products alone)
     unsigned long long* probe = (b == 0 && t == 0 && a.ptimes) ? a.ptimes + 8 : nullptr;
     uint64_t tp = t_start;
     auto mark = [&](int slot) {
@@ -260,6 +262,10 @@ __global__ void __launch_bounds__(MT, 1) reduce_mixed_kernel(MixArgs a)
                     }
                     if (__shfl_sync(0xffffffffu, bad, 0)) { ok = 0; break; }
                 }
+            }
+            if (probe) {  // the poll alone (slot 5)
+                const uint64_t now = globaltimer_ns();
+                probe[5] += now - tp;
             }
             float bv = 0.f;
             int bi = 0, bs = -1;
@@ -353,6 +359,10 @@ __global__ void __launch_bounds__(MT, 1) reduce_mixed_kernel(MixArgs a)
             if (lane == 0) s_dot[v] = d;
         }
         __syncthreads();
+        if (probe) {  // the dot products alone (slot 6)
+            const uint64_t now = globaltimer_ns();
+            probe[6] += now - tp;
+        }
         // warp 0: new column k+1 of own rows, multipliers into column k, the next candidate
         if (warp == 0) {
             float bv = 0.f;
@@ -382,6 +392,9 @@ __global__ void __launch_bounds__(MT, 1) reduce_mixed_kernel(MixArgs a)
                 s_cand = bl;
                 s_piv = bv;
                 s_p = bi;
+                // publish step k+1's header now: the candidate row follows below, and a reader
+                // re-reads any row word whose tag is not yet k+1
+                if (k + 1 <= n - 2) st_relaxed_u64(&hdr[np * G + b], mix_pack((unsigned)(k + 1), bi, bv));
             }
         }
         __syncthreads();
@@ -406,10 +419,6 @@ __global__ void __launch_bounds__(MT, 1) reduce_mixed_kernel(MixArgs a)
                     rc[c] = x0;
                     rc[c + 1] = x1;
                 }
-            }
-            if (pub) {
-                __syncwarp();
-                if (lane == 0) st_relaxed_u64(&hdr[np * G + b], mix_pack((unsigned)(k + 1), s_p, s_piv));
             }
             mark(3);
         } else {
