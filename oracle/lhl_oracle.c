@@ -942,3 +942,156 @@ int lhlo_num_threads(void)
     return 1;
 #endif
 }
+
+/* ------------------------------------------------------------------------------------ */
+/* Complex shifts on a real reduction (LHLShift{ComplexF64} on LHLWorkspace{Float64}).    */
+/* Shift LU: F:2529-2594 with TG = ComplexF64 (every complex product written out as        */
+/* Julia's Complex arithmetic: (ac - bd, ad + bc); complex x real scales both parts; the    */
+/* pivot magnitude is |re| + |im|, F:2519-2520).  Gt is planar: real parts in rows          */
+/* 1..n, imaginary parts in rows po+1..po+n of each column (F:117-129).  Division is the    */
+/* robust complex division of Baudin & Smith (2012), which Julia's Base uses for            */
+/* ComplexF64 (the reference calls `/` and `inv`, F:2548, F:2555, F:2590); rdiag =         */
+/* 1 / U[j,j] by the same division.  The planar solve is F:2146-2156 (gather into planes),  */
+/* the real L sweeps on each plane, F:2823-2910 (planar Hessenberg solve, here without the  */
+/* 4-row pipelining of its back substitution: the same sums in plain order), scatter.      */
+/* ------------------------------------------------------------------------------------ */
+typedef struct { double re, im; } cplx;
+
+static cplx c_mul(cplx a, cplx b) { cplx r = {a.re * b.re - a.im * b.im, a.re * b.im + a.im * b.re}; return r; }
+static cplx c_sub(cplx a, cplx b) { cplx r = {a.re - b.re, a.im - b.im}; return r; }
+static cplx c_add(cplx a, cplx b) { cplx r = {a.re + b.re, a.im + b.im}; return r; }
+static cplx c_scale(cplx a, double s) { cplx r = {a.re * s, a.im * s}; return r; }
+static double c_mag(cplx a) { return fabs(a.re) + fabs(a.im); }
+
+/* Baudin & Smith, "A robust complex division in Scilab" (2012), without its rescaling of  */
+/* operands near overflow/underflow (not reached by the tested inputs).                     */
+static double cdiv2(double a, double b, double c, double d, double r, double t)
+{
+    if (r != 0.0) {
+        double br = b * r;
+        return br != 0.0 ? (a + br) * t : a * t + (b * t) * r;
+    }
+    return (a + d * (b / c)) * t;
+}
+static cplx c_div(cplx x, cplx y)
+{
+    double a = x.re, b = x.im, c = y.re, d = y.im;
+    cplx q;
+    if (fabs(d) <= fabs(c)) {
+        double r = d / c, t = 1.0 / (c + d * r);
+        q.re = cdiv2(a, b, c, d, r, t);
+        q.im = cdiv2(b, -a, c, d, r, t);
+    } else {
+        double r = c / d, t = 1.0 / (d + c * r);
+        q.re = cdiv2(b, a, d, c, r, t);
+        q.im = -cdiv2(a, -b, d, c, r, t);
+    }
+    return q;
+}
+
+#define CG(G, ldg, po, i, c) ((cplx){M1(G, ldg, i, c), M1(G, ldg, (po) + (i), c)})
+#define CSET(G, ldg, po, i, c, v) do { cplx v_ = (v); M1(G, ldg, i, c) = v_.re; M1(G, ldg, (po) + (i), c) = v_.im; } while (0)
+
+int lhlo_shift_complex(int n, const double* Ht, int ldh, double sr, double si, double tr, double ti, double* Gt,
+                       int ldg, int po, uint8_t* swp, double* rdiag /* 2n interleaved */, double* rw /* 2n */)
+{
+    if (n == 0) return 0;
+    cplx sigma = {sr, si}, tau = {tr, ti};
+    cplx* r = (cplx*)rw;
+    for (int j = 1; j <= n; ++j) r[j - 1] = c_scale(tau, M1(Ht, ldh, j, 1));
+    r[0] = c_add(r[0], sigma);
+    int info = 0;
+    for (int k = 1; k <= n - 1; ++k) {
+        cplx a = r[k - 1];
+        cplx b = c_scale(tau, M1(Ht, ldh, k, k + 1));
+        if (c_mag(b) > c_mag(a)) {
+            swp[k - 1] = 1;
+            CSET(Gt, ldg, po, k, k, b);
+            cplx l = c_div(a, b);
+            CSET(Gt, ldg, po, k, k + 1, l);
+            for (int j = k + 1; j <= n; ++j) {
+                cplx g = c_scale(tau, M1(Ht, ldh, j, k + 1));
+                CSET(Gt, ldg, po, j, k, g);
+                r[j - 1] = c_sub(r[j - 1], c_mul(l, g));
+            }
+            CSET(Gt, ldg, po, k + 1, k, c_add(CG(Gt, ldg, po, k + 1, k), sigma));
+            r[k] = c_sub(r[k], c_mul(l, sigma));
+        } else {
+            swp[k - 1] = 0;
+            CSET(Gt, ldg, po, k, k, a);
+            cplx l;
+            if (a.re == 0.0 && a.im == 0.0) { if (info == 0) info = k; l.re = 0.0; l.im = 0.0; }
+            else l = c_div(b, a);
+            CSET(Gt, ldg, po, k, k + 1, l);
+            for (int j = k + 1; j <= n; ++j) {
+                cplx rj = r[j - 1];
+                CSET(Gt, ldg, po, j, k, rj);
+                r[j - 1] = c_sub(c_scale(tau, M1(Ht, ldh, j, k + 1)), c_mul(l, rj));
+            }
+            r[k] = c_add(r[k], sigma);
+        }
+    }
+    cplx rn = r[n - 1];
+    CSET(Gt, ldg, po, n, n, rn);
+    swp[n - 1] = 0;
+    if (rn.re == 0.0 && rn.im == 0.0 && info == 0) info = n;
+    cplx one = {1.0, 0.0};
+    for (int j = 1; j <= n; ++j) {
+        cplx q = c_div(one, CG(Gt, ldg, po, j, j));
+        rdiag[2 * (j - 1)] = q.re;
+        rdiag[2 * (j - 1) + 1] = q.im;
+    }
+    return info;
+}
+
+/* planar Hessenberg solve, F:2823-2910 (y: re plane y[0..n-1], im plane y[po..po+n-1]) */
+static void hess_solve_planar(int n, const double* Gt, int ldg, int po, const uint8_t* swp, const double* rd,
+                              double* y)
+{
+    for (int k = 1; k <= n - 1; ++k) {
+        int s = swp[k - 1];
+        cplx a = {y[k - 1], y[po + k - 1]}, b = {y[k], y[po + k]};
+        cplx xk = s ? b : a;
+        y[k - 1] = xk.re;
+        y[po + k - 1] = xk.im;
+        cplx v = c_sub(s ? a : b, c_mul(CG(Gt, ldg, po, k, k + 1), xk));
+        y[k] = v.re;
+        y[po + k] = v.im;
+    }
+    for (int j = n; j >= 1; --j) {
+        double sr = 0.0, si = 0.0;
+        for (int i = j + 1; i <= n; ++i) {
+            double xr = y[i - 1], xi = y[po + i - 1];
+            double gr = M1(Gt, ldg, i, j), gi = M1(Gt, ldg, po + i, j);
+            sr += gr * xr - gi * xi;
+            si += gr * xi + gi * xr;
+        }
+        cplx rj = {rd[2 * (j - 1)], rd[2 * (j - 1) + 1]};
+        cplx xj = c_mul(c_sub((cplx){y[j - 1], y[po + j - 1]}, (cplx){sr, si}), rj);
+        y[j - 1] = xj.re;
+        y[po + j - 1] = xj.im;
+    }
+}
+
+/* lhl_ldiv!(x, sh::LHLShift{ComplexF64}, ws::LHLWorkspace{Float64}), F:3080-3110.          */
+/* x: n complex (interleaved); y: 2 po doubles of scratch.                                  */
+void lhlo_ldiv_complex(int n, const double* F, int ldf, const int64_t* perm, const int64_t* iperm,
+                       const double* scale, const double* iscale, const double* Gt, int ldg, int po,
+                       const uint8_t* swp, const double* rdiag, double* x, double* y)
+{
+    for (int i = 1; i <= n; ++i) {
+        int64_t p = perm[i - 1];
+        y[i - 1] = x[2 * (p - 1)] * iscale[p - 1];
+        y[po + i - 1] = x[2 * (p - 1) + 1] * iscale[p - 1];
+    }
+    zinvsweep(n, F, ldf, y);
+    zinvsweep(n, F, ldf, y + po);
+    hess_solve_planar(n, Gt, ldg, po, swp, rdiag, y);
+    zsweep(n, F, ldf, y);
+    zsweep(n, F, ldf, y + po);
+    for (int i = 1; i <= n; ++i) {
+        int64_t p = iperm[i - 1];
+        x[2 * (i - 1)] = y[p - 1] * scale[i - 1];
+        x[2 * (i - 1) + 1] = y[po + p - 1] * scale[i - 1];
+    }
+}

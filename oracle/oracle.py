@@ -56,6 +56,9 @@ def lib():
         L.lhlo_shift_solve_batch.argtypes = [i, _dp, i, _dp, _dp, i, _iv, _iv, _dv, _dv, i, _dv, _dv,
                                              _dp, _dp, i, _i32]
         L.lhlo_shift_solve_batch.restype = i
+        L.lhlo_shift_complex.argtypes = [i, _dp, i, d, d, d, d, _dp, i, i, _u8, _dv, _dv]
+        L.lhlo_shift_complex.restype = i
+        L.lhlo_ldiv_complex.argtypes = [i, _dp, i, _iv, _iv, _dv, _dv, _dp, i, i, _u8, _dv, _dv, _dv]
         L.lhlo_num_threads.restype = i
         _lib = L
     return _lib
@@ -253,3 +256,78 @@ def reduce_blocked_ptr_raw(A, nb=16):
     ip = _ipiv_buf(n)
     lib().lhlo_reduce_blocked_ptr(n, A, max(n, 1), ip, nb)
     return A, ip[: max(n - 2, 0)].copy()
+
+
+def cpack(re, im):
+    """Complex array from its parts, keeping the signs of zeros (re + 1j*im does not)."""
+    z = np.empty(np.shape(re), dtype=np.complex128)
+    z.real = re
+    z.imag = im
+    return z
+
+
+def plane_offset(n: int) -> int:
+    """Rows per plane of a complex shift's planar Gt: n plus a zero pad of at least 4, even
+    (so that the imaginary plane starts on a 16-byte boundary)."""
+    po = n + 4
+    return po + (po & 1)
+
+
+class ShiftC:
+    """The outputs of ``lhl_shift!`` for a complex shift on a real reduction (LHLShift{ComplexF64}
+    on LHLWorkspace{Float64}): planar Gt (real parts rows 0..n-1, imaginary rows po..po+n-1)."""
+
+    def __init__(self, n):
+        self.n = n
+        self.po = plane_offset(n)
+        self.ldg = 2 * self.po
+        self.Gt = np.zeros((self.ldg, max(n, 1)), order="F")
+        self.swap = np.zeros(max(n, 1), dtype=np.uint8)
+        self.rdiag = np.zeros(max(n, 1), dtype=np.complex128)
+        self.info = 0
+        self.sigma = 0j
+        self.tau = 0j
+
+    def U(self):
+        n, po = self.n, self.po
+        G = self.Gt
+        Um = np.zeros((n, n), dtype=np.complex128)
+        for k in range(n):
+            Um[k, k:] = cpack(G[k:n, k], G[po + k:po + n, k])
+        return Um
+
+
+def shift_complex(R: Reduction, sigma, tau) -> ShiftC:
+    n = R.n
+    S = ShiftC(n)
+    w = np.zeros(2 * max(n, 1))
+    Ht = R.Ht if n > 0 else np.zeros((1, 1), order="F")
+    rd = np.zeros(2 * max(n, 1))
+    sigma, tau = complex(sigma), complex(tau)
+    S.info = int(lib().lhlo_shift_complex(n, Ht, max(n, 1), sigma.real, sigma.imag, tau.real, tau.imag, S.Gt,
+                                          S.ldg, S.po, S.swap, rd, w))
+    S.rdiag = cpack(rd[0::2][:max(n, 1)], rd[1::2][:max(n, 1)])
+    S.sigma, S.tau = sigma, tau
+    return S
+
+
+def ldiv_complex(R: Reduction, S: ShiftC, b):
+    x = np.array(b, dtype=np.complex128, copy=True)
+    xv = x.view(np.float64)
+    y = np.zeros(2 * S.po)
+    rd = np.empty(2 * max(R.n, 1))
+    rd[0::2] = S.rdiag.real
+    rd[1::2] = S.rdiag.imag
+    lib().lhlo_ldiv_complex(R.n, R.factors, max(R.n, 1), R.perm, R.iperm, R.scale, R.iscale, S.Gt, S.ldg, S.po,
+                            S.swap, rd, xv, y)
+    return x
+
+
+def refine_complex(R: Reduction, S: ShiftC, J, b, x, steps=1):
+    """lhl_refine!(x, sI + tJ, b, sh, ws, steps) (F:3144-3157) with the residual in numpy."""
+    W = S.sigma * np.eye(R.n) + S.tau * np.asarray(J)
+    x = np.array(x, dtype=np.complex128, copy=True)
+    for _ in range(steps):
+        r = b - W @ x
+        x = x + ldiv_complex(R, S, r)
+    return x

@@ -227,3 +227,131 @@ def test_batch_driver_matches_single():
         x = O.refine(R, S, J, B[:, s], x, 1)
         assert np.array_equal(x, X[:, s])
         assert info[s] == S.info
+
+
+# ---- complex shifts on a real reduction (test/core_tests.jl:214-233, :251-280) ----------
+
+def _cdiv(a, b):
+    """Baudin & Smith's robust complex division on (re, im) pairs, written independently of
+    the oracle's C code (the oracle's stand-in for Julia's ComplexF64 `/`)."""
+    (ar, ai), (c, d) = a, b
+
+    def two(a_, b_, c_, d_, r, t):
+        if r != 0.0:
+            br = b_ * r
+            return (a_ + br) * t if br != 0.0 else a_ * t + (b_ * t) * r
+        return (a_ + d_ * (b_ / c_)) * t
+
+    if abs(d) <= abs(c):
+        r = d / c
+        t = 1.0 / (c + d * r)
+        return two(ar, ai, c, d, r, t), two(ai, -ar, c, d, r, t)
+    r = c / d
+    t = 1.0 / (d + c * r)
+    return two(ai, ar, d, c, r, t), -two(ar, -ai, d, c, r, t)
+
+
+def shift_ref_complex(Ht, sigma, tau):
+    """Pure-Python restatement of the complex-on-real shift LU (F:2529-2594 with TG =
+    ComplexF64; `_lhl_shift_ref!` of test/core_tests.jl:119-171 on complex values): complex
+    products (ac - bd, ad + bc), complex x real scaling both parts, pivot magnitude
+    |re| + |im|.  Returns (U, l, swap, rdiag, info) as complex arrays."""
+    n = Ht.shape[0]
+    sr, si = sigma.real, sigma.imag
+    tr, ti = tau.real, tau.imag
+    mul = lambda a, b: (a[0] * b[0] - a[1] * b[1], a[0] * b[1] + a[1] * b[0])  # noqa: E731
+    sub = lambda a, b: (a[0] - b[0], a[1] - b[1])  # noqa: E731
+    add = lambda a, b: (a[0] + b[0], a[1] + b[1])  # noqa: E731
+    sc = lambda h: (tr * h, ti * h)  # noqa: E731
+    mag = lambda a: abs(a[0]) + abs(a[1])  # noqa: E731
+    r = [sc(Ht[j, 0]) for j in range(n)]
+    r[0] = add(r[0], (sr, si))
+    G = {}
+    swap = [0] * n
+    lv = []
+    info = 0
+    for k in range(n - 1):
+        a = r[k]
+        b = sc(Ht[k, k + 1])
+        if mag(b) > mag(a):
+            swap[k] = 1
+            G[(k, k)] = b
+            l = _cdiv(a, b)
+            for j in range(k + 1, n):
+                g = sc(Ht[j, k + 1])
+                G[(j, k)] = g
+                r[j] = sub(r[j], mul(l, g))
+            G[(k + 1, k)] = add(G[(k + 1, k)], (sr, si))
+            r[k + 1] = sub(r[k + 1], mul(l, (sr, si)))
+        else:
+            G[(k, k)] = a
+            if a == (0.0, 0.0):
+                info = info or (k + 1)
+                l = (0.0, 0.0)
+            else:
+                l = _cdiv(b, a)
+            for j in range(k + 1, n):
+                rj = r[j]
+                G[(j, k)] = rj
+                r[j] = sub(sc(Ht[j, k + 1]), mul(l, rj))
+            r[k + 1] = add(r[k + 1], (sr, si))
+        lv.append(l)
+    G[(n - 1, n - 1)] = r[n - 1]
+    if r[n - 1] == (0.0, 0.0) and info == 0:
+        info = n
+    U = O.cpack([G[(j, k)][0] for k in range(n) for j in range(k, n)], [G[(j, k)][1] for k in range(n) for j in range(k, n)])
+    q = [_cdiv((1.0, 0.0), G[(j, j)]) for j in range(n)]
+    rd = O.cpack([v[0] for v in q], [v[1] for v in q])
+    return U, O.cpack([v[0] for v in lv], [v[1] for v in lv]), np.array(swap, dtype=np.uint8), rd, info
+
+
+def cstate(S):
+    n, po, G = S.n, S.po, S.Gt
+    U = O.cpack([G[j, k] for k in range(n) for j in range(k, n)], [G[po + j, k] for k in range(n) for j in range(k, n)])
+    l = O.cpack([G[k, k + 1] for k in range(n - 1)], [G[po + k, k + 1] for k in range(n - 1)])
+    return U, l, S.swap[:n].copy(), S.rdiag[:n].copy(), S.info
+
+
+def cbits_equal(a, b):
+    a = np.ascontiguousarray(a, dtype=np.complex128)
+    b = np.ascontiguousarray(b, dtype=np.complex128)
+    return a.shape == b.shape and np.array_equal(a.view(np.int64), b.view(np.int64))
+
+
+@pytest.mark.filterwarnings("ignore::RuntimeWarning")  # the (0, 0) shift divides by zero, as in the reference
+@pytest.mark.parametrize("n", list(range(1, 25)) + [64, 65, 130])
+@pytest.mark.parametrize("tie", [False, True])
+def test_complex_shift_matches_restatement(n, tie):
+    """test/core_tests.jl:214-233: the complex-on-real shift LU, bit for bit against an
+    independent restatement, for the reference test's five shifts."""
+    g = rng(32 + n)
+    J = g.integers(-2, 3, (n, n)).astype(float) if tie else g.standard_normal((n, n))
+    R = O.reduce(J)
+    for s, t in ((0.4 + 0.7j, -1), (1, -0.1 + 0.2j), (0, 1j), (2j, 0), (0, 0)):
+        S = O.shift_complex(R, s, t)
+        U, l, sw, rd, info = shift_ref_complex(R.Ht, complex(s), complex(t))
+        Uo, lo, swo, rdo, infoo = cstate(S)
+        assert cbits_equal(U, Uo) and cbits_equal(l, lo) and np.array_equal(sw, swo)
+        assert info == infoo
+        if info == 0:
+            assert cbits_equal(rd, rdo)
+
+
+@pytest.mark.parametrize("n", [1, 2, 3, 5, 40, 129, 260, 600])
+def test_complex_shifts_on_a_real_reduction(n):
+    """test/core_tests.jl:251-280: solves against a dense complex LU (rtol 1e-9), and one
+    refinement step with the complex system matrix: bwd <= 2 bwd(x) + eps and < 50 eps."""
+    J = rng(n).standard_normal((n, n))
+    g = rng(n + 7)
+    b = g.standard_normal(n) + 1j * g.standard_normal(n)
+    R = O.reduce(J)
+    eps = np.finfo(float).eps
+    for s, t in ((0.4 + 0.7j, -1.0), (1.0, -0.05 + 0.3j), (0.0, 1j), (-3.0 + 2j, 2.0 - 1j), (1.0, -0.05)):
+        W = s * np.eye(n) + t * J
+        S = O.shift_complex(R, s, t)
+        x = O.ldiv_complex(R, S, b)
+        xr = np.linalg.solve(W, b)
+        assert np.linalg.norm(x - xr) <= 1e-9 * np.linalg.norm(xr)
+        y = O.refine_complex(R, S, J, b, x, 1)
+        assert O.bwd(W, y, b) <= 2 * O.bwd(W, x, b) + eps
+        assert O.bwd(W, y, b) < 50 * eps
