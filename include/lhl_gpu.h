@@ -63,6 +63,8 @@ typedef struct {
     int32_t* info;    /* first zero pivot, 0 if none (F:2450) */
     double* sigma;
     double* tau;
+    int64_t po;         /* complex shifts: rows per plane of the planar Gt */
+    int32_t is_complex; /* 1: LHLShift{ComplexF64} on a real reduction */
 } lhl_shift_view;
 
 /* ---- workspace ------------------------------------------------------------------ */
@@ -102,6 +104,23 @@ int lhl_shift_batched(lhl_shift_t sh, lhl_ws_t ws, int64_t s0, int64_t count, co
                       const double* dtau, void* stream);
 /* lhl_shift!(ws, sigma, tau) for one shift slot with host scalars. */
 int lhl_shift(lhl_shift_t sh, lhl_ws_t ws, int64_t slot, double sigma, double tau, void* stream);
+
+/* ---- complex shifts on a real reduction (LHLShift{ComplexF64} on LHLWorkspace{Float64}) ----
+ * LHLShift{Complex{T}}(n) (F:107-116, F:180-191): nshifts slots whose Gt is planar, (2 po) x n
+ * per slot with real parts in rows 1..n and imaginary parts in rows po+1..po+n (po in the
+ * view); rdiag, sigma and tau hold interleaved (re, im) pairs.  lhl_ldiv, lhl_refine,
+ * lhl_refine_tol and lhl_residual_norms given such a shift take interleaved complex dX / dB /
+ * dR (CuArray{ComplexF64} memory; leading dimensions counted in complex elements), and the
+ * solve is the reference's complex-on-real one (F:3080-3110). */
+int lhl_shift_create_complex(int64_t n, int64_t nshifts, lhl_shift_t* sh);
+/* lhl_shift!(sh, ws, sigma, tau) with complex sigma, tau (F:2456-2594 with TG = ComplexF64).
+ * A shift object made by lhl_shift_create takes only real shifts: LHL_ERR_ARG otherwise
+ * (F:2466-2472).  A real shift on a complex object is converted. */
+int lhl_shift_complex(lhl_shift_t sh, lhl_ws_t ws, int64_t slot, double sigma_re, double sigma_im, double tau_re,
+                      double tau_im, void* stream);
+/* Batched complex shifts: dsigma, dtau are count interleaved complex values on the device. */
+int lhl_shift_batched_complex(lhl_shift_t sh, lhl_ws_t ws, int64_t s0, int64_t count, const double* dsigma,
+                              const double* dtau, void* stream);
 
 /* ---- solves --------------------------------------------------------------------- */
 /* lhl_ldiv!(x, sh, ws) (F:3052-3068) for nrhs columns of dX (n x nrhs, leading dimension

@@ -32,6 +32,8 @@ struct lhl_shift_s {
     int64_t n, nshifts, ldg;
     double *Gt, *rdiag, *sigma, *tau;
     double* uinv;  // mixed form: inverses of U's 32 x 32 diagonal blocks (n / 32 blocks per shift)
+    int cplx;      // complex shifts: Gt planar (2 po rows), rdiag / sigma / tau interleaved complex
+    int64_t po;
     uint8_t* swap;
     int32_t* info;
 };
@@ -272,35 +274,46 @@ int lhl_reduce(lhl_ws_t ws, const double* dJ, int64_t ldj, int balance, void* st
     return cuda_status(e);
 }
 
-int lhl_shift_create(int64_t n, int64_t nshifts, lhl_shift_t* out)
+static int shift_create(int64_t n, int64_t nshifts, int cplx, lhl_shift_t* out)
 {
     if (!out) return LHL_ERR_ARG;
     *out = nullptr;
     if (n < 0 || n > 16384 || nshifts < 1) return LHL_ERR_DIM;
+    if (cplx && n > 8192) return LHL_ERR_DIM;
     lhl_shift_t s = new (std::nothrow) lhl_shift_s();
     if (!s) return LHL_ERR_ALLOC;
     memset(s, 0, sizeof(*s));
     s->n = n;
     s->nshifts = nshifts;
-    s->ldg = n + 4;
+    s->cplx = cplx;
+    s->po = (n + 4) + ((n + 4) & 1);   // rows per plane, even (16-byte aligned planes)
+    s->ldg = cplx ? 2 * s->po : n + 4;
+    const int P = cplx ? 2 : 1;
     const size_t gsz = (size_t)s->ldg * (size_t)n * (size_t)nshifts;
     cudaError_t e = dalloc(&s->Gt, gsz);
-    if (e == cudaSuccess) e = dalloc(&s->rdiag, (size_t)n * nshifts);
-    if (e == cudaSuccess) e = dalloc(&s->sigma, nshifts);
-    if (e == cudaSuccess) e = dalloc(&s->tau, nshifts);
+    if (e == cudaSuccess) e = dalloc(&s->rdiag, (size_t)P * n * nshifts);
+    if (e == cudaSuccess) e = dalloc(&s->sigma, (size_t)P * nshifts);
+    if (e == cudaSuccess) e = dalloc(&s->tau, (size_t)P * nshifts);
     if (e == cudaSuccess) e = dalloc(&s->swap, (size_t)n * nshifts);
     if (e == cudaSuccess) e = dalloc(&s->info, nshifts);
-    if (e == cudaSuccess) e = dalloc(&s->uinv, (size_t)((n + 31) / 32) * 32 * 32 * (size_t)nshifts);
+    if (e == cudaSuccess) e = dalloc(&s->uinv, cplx ? 1 : (size_t)((n + 31) / 32) * 32 * 32 * (size_t)nshifts);
     if (e == cudaSuccess) e = cudaMemset(s->Gt, 0, (gsz ? gsz : 1) * sizeof(double));
     if (e == cudaSuccess) e = cudaMemset(s->info, 0, nshifts * sizeof(int32_t));
-    if (e == cudaSuccess) e = cudaMemset(s->sigma, 0, nshifts * sizeof(double));
-    if (e == cudaSuccess) e = cudaMemset(s->tau, 0, nshifts * sizeof(double));
+    if (e == cudaSuccess) e = cudaMemset(s->sigma, 0, (size_t)P * nshifts * sizeof(double));
+    if (e == cudaSuccess) e = cudaMemset(s->tau, 0, (size_t)P * nshifts * sizeof(double));
     if (e != cudaSuccess) {
         lhl_shift_destroy(s);
         return e == cudaErrorMemoryAllocation ? LHL_ERR_ALLOC : LHL_ERR_CUDA;
     }
     *out = s;
     return LHL_OK;
+}
+
+int lhl_shift_create(int64_t n, int64_t nshifts, lhl_shift_t* out) { return shift_create(n, nshifts, 0, out); }
+
+int lhl_shift_create_complex(int64_t n, int64_t nshifts, lhl_shift_t* out)
+{
+    return shift_create(n, nshifts, 1, out);
 }
 
 int lhl_shift_destroy(lhl_shift_t s)
@@ -325,24 +338,19 @@ int lhl_shift_get_view(lhl_shift_t s, lhl_shift_view* v)
     v->info = s->info;
     v->sigma = s->sigma;
     v->tau = s->tau;
+    v->po = s->po;
+    v->is_complex = s->cplx;
     return LHL_OK;
 }
 
-int lhl_shift_batched(lhl_shift_t sh, lhl_ws_t ws, int64_t s0, int64_t count, const double* dsigma,
-                      const double* dtau, void* stream)
+static int shift_run(lhl_shift_t sh, lhl_ws_t ws, int64_t s0, int64_t count, cudaStream_t st)
 {
-    if (!sh || !ws) return LHL_ERR_ARG;
-    if (sh->n != ws->n) return LHL_ERR_DIM;
-    if (s0 < 0 || count < 0 || s0 + count > sh->nshifts) return LHL_ERR_DIM;
-    if (count == 0 || ws->n == 0) return LHL_OK;
-    if (!dsigma || !dtau) return LHL_ERR_ARG;
-    cudaStream_t st = (cudaStream_t)stream;
-    cudaError_t e = cudaSuccess;
-    if (dsigma != sh->sigma + s0)
-        e = cudaMemcpyAsync(sh->sigma + s0, dsigma, count * sizeof(double), cudaMemcpyDeviceToDevice, st);
-    if (e == cudaSuccess && dtau != sh->tau + s0)
-        e = cudaMemcpyAsync(sh->tau + s0, dtau, count * sizeof(double), cudaMemcpyDeviceToDevice, st);
-    if (e != cudaSuccess) return LHL_ERR_CUDA;
+    cudaError_t e;
+    if (sh->cplx) {
+        e = lhl::launch_shift_lu_cplx((int)ws->n, ws->Ht, (int)ws->n, sh->sigma + 2 * s0, sh->tau + 2 * s0, (int)s0,
+                                      (int)count, sh->Gt, (int)sh->ldg, (int)sh->po, sh->swap, sh->rdiag, sh->info, st);
+        return cuda_status(e);
+    }
     e = lhl::launch_shift_lu((int)ws->n, ws->Ht, (int)ws->n, sh->sigma + s0, sh->tau + s0, (int)s0, (int)count,
                              sh->Gt, (int)sh->ldg, sh->swap, sh->rdiag, sh->info, st);
     if (e == cudaSuccess && ws->precision == LHL_PREC_MIXED)
@@ -350,20 +358,81 @@ int lhl_shift_batched(lhl_shift_t sh, lhl_ws_t ws, int64_t s0, int64_t count, co
     return cuda_status(e);
 }
 
-int lhl_shift(lhl_shift_t sh, lhl_ws_t ws, int64_t slot, double sigma, double tau, void* stream)
+static int shift_args(lhl_shift_t sh, lhl_ws_t ws, int64_t s0, int64_t count)
 {
     if (!sh || !ws) return LHL_ERR_ARG;
     if (sh->n != ws->n) return LHL_ERR_DIM;
-    if (slot < 0 || slot >= sh->nshifts) return LHL_ERR_DIM;
+    if (s0 < 0 || count < 0 || s0 + count > sh->nshifts) return LHL_ERR_DIM;
+    return LHL_OK;
+}
+
+int lhl_shift_batched(lhl_shift_t sh, lhl_ws_t ws, int64_t s0, int64_t count, const double* dsigma,
+                      const double* dtau, void* stream)
+{
+    int rc = shift_args(sh, ws, s0, count);
+    if (rc != LHL_OK) return rc;
+    if (count == 0 || ws->n == 0) return LHL_OK;
+    if (!dsigma || !dtau) return LHL_ERR_ARG;
+    cudaStream_t st = (cudaStream_t)stream;
+    cudaError_t e = cudaSuccess;
+    if (sh->cplx) {  // real shifts on a complex LHLShift: converted (F:2474-2475)
+        e = lhl::launch_real_to_cplx(dsigma, sh->sigma + 2 * s0, (int)count, st);
+        if (e == cudaSuccess) e = lhl::launch_real_to_cplx(dtau, sh->tau + 2 * s0, (int)count, st);
+    } else {
+        if (dsigma != sh->sigma + s0)
+            e = cudaMemcpyAsync(sh->sigma + s0, dsigma, count * sizeof(double), cudaMemcpyDeviceToDevice, st);
+        if (e == cudaSuccess && dtau != sh->tau + s0)
+            e = cudaMemcpyAsync(sh->tau + s0, dtau, count * sizeof(double), cudaMemcpyDeviceToDevice, st);
+    }
+    if (e != cudaSuccess) return LHL_ERR_CUDA;
+    return shift_run(sh, ws, s0, count, st);
+}
+
+int lhl_shift_batched_complex(lhl_shift_t sh, lhl_ws_t ws, int64_t s0, int64_t count, const double* dsigma,
+                              const double* dtau, void* stream)
+{
+    int rc = shift_args(sh, ws, s0, count);
+    if (rc != LHL_OK) return rc;
+    if (!sh->cplx) return LHL_ERR_ARG;  // complex shifts need a complex LHLShift (F:2466-2472)
+    if (count == 0 || ws->n == 0) return LHL_OK;
+    if (!dsigma || !dtau) return LHL_ERR_ARG;
+    cudaStream_t st = (cudaStream_t)stream;
+    cudaError_t e = cudaSuccess;
+    if (dsigma != sh->sigma + 2 * s0)
+        e = cudaMemcpyAsync(sh->sigma + 2 * s0, dsigma, 2 * count * sizeof(double), cudaMemcpyDeviceToDevice, st);
+    if (e == cudaSuccess && dtau != sh->tau + 2 * s0)
+        e = cudaMemcpyAsync(sh->tau + 2 * s0, dtau, 2 * count * sizeof(double), cudaMemcpyDeviceToDevice, st);
+    if (e != cudaSuccess) return LHL_ERR_CUDA;
+    return shift_run(sh, ws, s0, count, st);
+}
+
+int lhl_shift_complex(lhl_shift_t sh, lhl_ws_t ws, int64_t slot, double sigma_re, double sigma_im, double tau_re,
+                      double tau_im, void* stream)
+{
+    int rc = shift_args(sh, ws, slot, 1);
+    if (rc != LHL_OK) return rc;
+    if (!sh->cplx) {
+        if (sigma_im != 0.0 || tau_im != 0.0) return LHL_ERR_ARG;  // F:2466-2472
+        return lhl_shift(sh, ws, slot, sigma_re, tau_re, stream);
+    }
+    if (ws->n == 0) return LHL_OK;
+    cudaStream_t st = (cudaStream_t)stream;
+    cudaError_t e = lhl::launch_set_pair(sh->sigma + 2 * slot, sh->sigma + 2 * slot + 1, sigma_re, sigma_im, st);
+    if (e == cudaSuccess) e = lhl::launch_set_pair(sh->tau + 2 * slot, sh->tau + 2 * slot + 1, tau_re, tau_im, st);
+    if (e != cudaSuccess) return LHL_ERR_CUDA;
+    return shift_run(sh, ws, slot, 1, st);
+}
+
+int lhl_shift(lhl_shift_t sh, lhl_ws_t ws, int64_t slot, double sigma, double tau, void* stream)
+{
+    int rc = shift_args(sh, ws, slot, 1);
+    if (rc != LHL_OK) return rc;
+    if (sh->cplx) return lhl_shift_complex(sh, ws, slot, sigma, 0.0, tau, 0.0, stream);
     if (ws->n == 0) return LHL_OK;
     cudaStream_t st = (cudaStream_t)stream;
     cudaError_t e = lhl::launch_set_pair(sh->sigma + slot, sh->tau + slot, sigma, tau, st);
     if (e != cudaSuccess) return LHL_ERR_CUDA;
-    e = lhl::launch_shift_lu((int)ws->n, ws->Ht, (int)ws->n, sh->sigma + slot, sh->tau + slot, (int)slot, 1,
-                             sh->Gt, (int)sh->ldg, sh->swap, sh->rdiag, sh->info, st);
-    if (e == cudaSuccess && ws->precision == LHL_PREC_MIXED)
-        e = lhl::launch_uinv((int)ws->n, sh->Gt, (int)sh->ldg, sh->rdiag, (int)slot, 1, sh->uinv, st);
-    return cuda_status(e);
+    return shift_run(sh, ws, slot, 1, st);
 }
 
 static int ldiv_common(lhl_shift_t sh, lhl_ws_t ws, double* dX, int64_t ldx, int64_t nrhs, int64_t rps, int mode,
@@ -402,7 +471,9 @@ static int ldiv_common(lhl_shift_t sh, lhl_ws_t ws, double* dX, int64_t ldx, int
         a.rdiag = sh->rdiag;
         a.rhs_per_shift = (int)rps;
         a.nshifts = (int)sh->nshifts;
-        a.uinv = ws->precision == LHL_PREC_MIXED ? sh->uinv : nullptr;
+        a.uinv = (ws->precision == LHL_PREC_MIXED && !sh->cplx) ? sh->uinv : nullptr;
+        a.cplx = sh->cplx;
+        a.po = (int)sh->po;
     }
     return cuda_status(lhl::launch_ldiv(a, (int)nrhs, st));
 }
@@ -428,6 +499,32 @@ int lhl_applyZinv(lhl_ws_t ws, double* dX, int64_t ldx, int64_t nrhs, void* stre
     return ldiv_common(nullptr, ws, dX, ldx, nrhs, 1, 1, (cudaStream_t)stream);
 }
 
+// residual, norms and update for real or complex (interleaved) right-hand sides
+static cudaError_t resid_any(lhl_shift_t sh, int64_t n, const double* dJ, int64_t ldj, const double* dB, int64_t ldb,
+                             const double* dX, int64_t ldx, double* dR, int64_t ldr, int64_t nrhs, int64_t rps,
+                             cudaStream_t st, const double* done, double tol)
+{
+    if (sh->cplx)
+        return lhl::launch_residual_cplx((int)n, dJ, (int)ldj, dB, (int)ldb, dX, (int)ldx, dR, (int)ldr, (int)nrhs,
+                                         (int)rps, sh->sigma, sh->tau, st, done, tol);
+    return lhl::launch_residual((int)n, dJ, (int)ldj, dB, (int)ldb, dX, (int)ldx, dR, (int)ldr, (int)nrhs, (int)rps,
+                                sh->sigma, sh->tau, st, done, tol);
+}
+
+static cudaError_t relres_any(lhl_shift_t sh, int64_t n, const double* dR, int64_t ldr, const double* dB,
+                              int64_t ldb, double* dres, int64_t nrhs, cudaStream_t st)
+{
+    const int P = sh->cplx ? 2 : 1;  // an interleaved complex column is a real vector of 2n
+    return lhl::launch_relres((int)(P * n), dR, (int)(P * ldr), dB, (int)(P * ldb), dres, (int)nrhs, st);
+}
+
+static cudaError_t axpy_any(lhl_shift_t sh, int64_t n, double* dX, int64_t ldx, const double* dR, int64_t ldr,
+                            int64_t nrhs, cudaStream_t st, const double* done, double tol)
+{
+    const int P = sh->cplx ? 2 : 1;
+    return lhl::launch_axpy_cols((int)(P * n), dX, (int)(P * ldx), dR, (int)(P * ldr), (int)nrhs, st, done, tol);
+}
+
 int lhl_refine(lhl_shift_t sh, lhl_ws_t ws, const double* dJ, int64_t ldj, const double* dB, int64_t ldb, double* dX,
                int64_t ldx, double* dR, int64_t nrhs, int64_t rhs_per_shift, int steps, void* stream)
 {
@@ -442,12 +539,11 @@ int lhl_refine(lhl_shift_t sh, lhl_ws_t ws, const double* dJ, int64_t ldj, const
     if ((nrhs + rhs_per_shift - 1) / rhs_per_shift > sh->nshifts) return LHL_ERR_DIM;
     cudaStream_t st = (cudaStream_t)stream;
     for (int s = 0; s < steps; ++s) {
-        cudaError_t e = lhl::launch_residual((int)n, dJ, (int)ldj, dB, (int)ldb, dX, (int)ldx, dR, (int)ldx, (int)nrhs,
-                                             (int)rhs_per_shift, sh->sigma, sh->tau, st);
+        cudaError_t e = resid_any(sh, n, dJ, ldj, dB, ldb, dX, ldx, dR, ldx, nrhs, rhs_per_shift, st, nullptr, 0.0);
         if (e != cudaSuccess) return LHL_ERR_CUDA;
         int rc = ldiv_common(sh, ws, dR, ldx, nrhs, rhs_per_shift, 0, st);
         if (rc != LHL_OK) return rc;
-        e = lhl::launch_axpy_cols((int)n, dX, (int)ldx, dR, (int)ldx, (int)nrhs, st);
+        e = axpy_any(sh, n, dX, ldx, dR, ldx, nrhs, st, nullptr, 0.0);
         if (e != cudaSuccess) return LHL_ERR_CUDA;
     }
     return LHL_OK;
@@ -470,9 +566,9 @@ int lhl_refine_tol(lhl_shift_t sh, lhl_ws_t ws, const double* dJ, int64_t ldj, c
     cudaStream_t st = (cudaStream_t)stream;
     for (int s = 0; s <= max_steps; ++s) {
         // step 0 computes every residual; later steps only those of unconverged columns
-        cudaError_t e = lhl::launch_residual((int)n, dJ, (int)ldj, dB, (int)ldb, dX, (int)ldx, dR, (int)ldx, (int)nrhs,
-                                             (int)rhs_per_shift, sh->sigma, sh->tau, st, s > 0 ? dres : nullptr, tol);
-        if (e == cudaSuccess) e = lhl::launch_relres((int)n, dR, (int)ldx, dB, (int)ldb, dres, (int)nrhs, st);
+        cudaError_t e = resid_any(sh, n, dJ, ldj, dB, ldb, dX, ldx, dR, ldx, nrhs, rhs_per_shift, st,
+                                  s > 0 ? dres : nullptr, tol);
+        if (e == cudaSuccess) e = relres_any(sh, n, dR, ldx, dB, ldb, dres, nrhs, st);
         if (e != cudaSuccess) return LHL_ERR_CUDA;
         if (s == max_steps) break;
         lhl::LdivArgs a;
@@ -493,7 +589,9 @@ int lhl_refine_tol(lhl_shift_t sh, lhl_ws_t ws, const double* dJ, int64_t ldj, c
         a.rdiag = sh->rdiag;
         a.rhs_per_shift = (int)rhs_per_shift;
         a.nshifts = (int)sh->nshifts;
-        a.uinv = ws->precision == LHL_PREC_MIXED ? sh->uinv : nullptr;
+        a.uinv = (ws->precision == LHL_PREC_MIXED && !sh->cplx) ? sh->uinv : nullptr;
+        a.cplx = sh->cplx;
+        a.po = (int)sh->po;
         a.linv = ws->linv;
         a.done = dres;
         a.tol = tol;
@@ -504,7 +602,7 @@ int lhl_refine_tol(lhl_shift_t sh, lhl_ws_t ws, const double* dJ, int64_t ldj, c
         a.err = ws->err;
         a.limit_ns = ws->limit_ns;
         e = lhl::launch_ldiv(a, (int)nrhs, st);
-        if (e == cudaSuccess) e = lhl::launch_axpy_cols((int)n, dX, (int)ldx, dR, (int)ldx, (int)nrhs, st, dres, tol);
+        if (e == cudaSuccess) e = axpy_any(sh, n, dX, ldx, dR, ldx, nrhs, st, dres, tol);
         if (e != cudaSuccess) return LHL_ERR_CUDA;
     }
     return LHL_OK;
@@ -523,10 +621,9 @@ int lhl_residual_norms(lhl_shift_t sh, const double* dJ, int64_t ldj, const doub
     if (ldj < n || ldb < n || ldx < n) return LHL_ERR_DIM;
     if ((nrhs + rhs_per_shift - 1) / rhs_per_shift > sh->nshifts) return LHL_ERR_DIM;
     cudaStream_t st = (cudaStream_t)stream;
-    cudaError_t e = lhl::launch_residual((int)n, dJ, (int)ldj, dB, (int)ldb, dX, (int)ldx, dR, (int)ldx, (int)nrhs,
-                                         (int)rhs_per_shift, sh->sigma, sh->tau, st);
+    cudaError_t e = resid_any(sh, n, dJ, ldj, dB, ldb, dX, ldx, dR, ldx, nrhs, rhs_per_shift, st, nullptr, 0.0);
     if (e != cudaSuccess) return LHL_ERR_CUDA;
-    return cuda_status(lhl::launch_relres((int)n, dR, (int)ldx, dB, (int)ldb, dres, (int)nrhs, st));
+    return cuda_status(relres_any(sh, n, dR, ldx, dB, ldb, dres, nrhs, st));
 }
 
 }  // extern "C"

@@ -1,0 +1,394 @@
+// complex.cu -- complex shifts on a real reduction (LHLShift{ComplexF64} on
+// LHLWorkspace{Float64}): the shift LU of G = sigma I + tau H with complex sigma, tau
+// (F:2529-2594 with TG = ComplexF64), its planar Hessenberg solve (F:2823-2910) and the
+// complex residual of lhl_refine! (F:3144-3157).  The L sweeps of the solve are the real
+// ones (solve.cu), applied to the two planes as two real right-hand sides.
+//
+// Layout: Gt is planar, (2 po) x n per shift: real parts in rows 1..n, imaginary parts in
+// rows po+1..po+n of each column (po = n + 4 rounded up to even).  rdiag, sigma, tau and
+// every complex vector of the C ABI are interleaved (re, im) pairs, as CuArray{ComplexF64}.
+//
+// Arithmetic is Julia's Complex arithmetic written out on the parts, every operation
+// rounded separately (no fused multiply-adds): (a+bi)(c+di) = (ac - bd) + (ad + bc)i,
+// complex x real scales both parts, the pivot magnitude is |re| + |im| (F:2519-2520).
+// Division is Baudin & Smith's robust complex division (the one Julia's Base uses for
+// ComplexF64, without its rescaling near overflow and underflow); rdiag = 1 / U[j,j] by the
+// same division.  The CPU oracle uses the same operations in the same order, so the device
+// shift LU is bit-identical to it.
+#include "internal.cuh"
+
+namespace lhl {
+
+struct dc {
+    double re, im;
+};
+
+__device__ __forceinline__ dc cmul(dc a, dc b)
+{
+    return {dsub(dmul(a.re, b.re), dmul(a.im, b.im)), dadd(dmul(a.re, b.im), dmul(a.im, b.re))};
+}
+__device__ __forceinline__ dc csub(dc a, dc b) { return {dsub(a.re, b.re), dsub(a.im, b.im)}; }
+__device__ __forceinline__ dc cadd(dc a, dc b) { return {dadd(a.re, b.re), dadd(a.im, b.im)}; }
+__device__ __forceinline__ dc cscale(dc a, double s) { return {dmul(a.re, s), dmul(a.im, s)}; }
+__device__ __forceinline__ double cmag(dc a) { return dadd(fabs(a.re), fabs(a.im)); }
+
+__device__ __forceinline__ double cdiv2(double a, double b, double c, double d, double r, double t)
+{
+    if (r != 0.0) {
+        const double br = dmul(b, r);
+        return br != 0.0 ? dmul(dadd(a, br), t) : dadd(dmul(a, t), dmul(dmul(b, t), r));
+    }
+    return dmul(dadd(a, dmul(d, __ddiv_rn(b, c))), t);
+}
+
+// Baudin & Smith, "A robust complex division in Scilab" (2012).
+__device__ __forceinline__ dc cdiv(dc x, dc y)
+{
+    const double a = x.re, b = x.im, c = y.re, d = y.im;
+    if (fabs(d) <= fabs(c)) {
+        const double r = __ddiv_rn(d, c), t = __ddiv_rn(1.0, dadd(c, dmul(d, r)));
+        return {cdiv2(a, b, c, d, r, t), cdiv2(b, -a, c, d, r, t)};
+    }
+    const double r = __ddiv_rn(c, d), t = __ddiv_rn(1.0, dadd(d, dmul(c, r)));
+    return {cdiv2(b, a, d, c, r, t), -cdiv2(a, -b, d, c, r, t)};
+}
+
+// ---- shift LU, one CTA per shift (the real kernel's structure, shift.cu) ----
+template <int T, int E>
+__global__ void __launch_bounds__(T) shift_lu_cplx_kernel(int n, const double* __restrict__ Ht, int ldh,
+                                                          const double* __restrict__ sig, const double* __restrict__ tau_,
+                                                          int s0, double* __restrict__ Gt_all, int ldg, int po,
+                                                          uint8_t* __restrict__ swap_all, double* __restrict__ rdiag_all,
+                                                          int32_t* __restrict__ info_all)
+{
+    const int s = s0 + blockIdx.x;
+    const dc sigma = {sig[2 * blockIdx.x], sig[2 * blockIdx.x + 1]};
+    const dc tau = {tau_[2 * blockIdx.x], tau_[2 * blockIdx.x + 1]};
+    double* Gt = Gt_all + (size_t)s * ldg * n;
+    uint8_t* swp = swap_all + (size_t)s * n;
+    double* rdiag = rdiag_all + (size_t)s * 2 * n;
+    const int t = threadIdx.x;
+    __shared__ dc s_next[2];
+    __shared__ dc s_l[2], s_a[2], s_b[2];
+    __shared__ int s_sw[2];
+    __shared__ int s_info;
+
+    dc r[E];
+    double h[E];     // Ht[j, k+1] for the current step
+    double hsub[E];  // Ht[j, j+1]: the subdiagonal of the step this thread decides
+#pragma unroll
+    for (int e = 0; e < E; ++e) {
+        const int j = 1 + t + e * T;
+        r[e] = (j <= n) ? cscale(tau, M1(Ht, ldh, j, 1)) : dc{0.0, 0.0};
+        if (j == 1) r[e] = cadd(r[e], sigma);
+        h[e] = (j <= n && n >= 2) ? M1(Ht, ldh, j, 2) : 0.0;
+        hsub[e] = (j + 1 <= n) ? M1(Ht, ldh, j, j + 1) : 0.0;
+    }
+    auto decide = [&](int k, dc a, double hs) {
+        const dc b = cscale(tau, hs);
+        const bool sw = cmag(b) > cmag(a);
+        dc l;
+        if (sw) l = cdiv(a, b);
+        else if (a.re == 0.0 && a.im == 0.0) l = {0.0, 0.0};
+        else l = cdiv(b, a);
+        s_l[k & 1] = l;
+        s_a[k & 1] = a;
+        s_b[k & 1] = b;
+        s_sw[k & 1] = sw ? 1 : 0;
+    };
+    if (t == 0) {
+        s_next[1] = r[0];
+        s_info = 0;
+        if (n >= 2) decide(1, r[0], hsub[0]);
+    }
+    __syncthreads();
+    for (int k = 1; k <= n - 1; ++k) {
+        const dc l = s_l[k & 1];
+        const bool sw = s_sw[k & 1] != 0;
+        if (t == 0) {
+            const dc a = s_a[k & 1], b = s_b[k & 1];
+            const dc d = sw ? b : a;
+            swp[k - 1] = sw ? 1 : 0;
+            M1(Gt, ldg, k, k) = d.re;
+            M1(Gt, ldg, po + k, k) = d.im;
+            M1(Gt, ldg, k, k + 1) = l.re;
+            M1(Gt, ldg, po + k, k + 1) = l.im;
+            if (!sw && a.re == 0.0 && a.im == 0.0 && s_info == 0) s_info = k;
+        }
+        double hn[E];
+#pragma unroll
+        for (int e = 0; e < E; ++e) {
+            const int j = 1 + t + e * T;
+            hn[e] = (j >= k + 1 && j <= n && k + 2 <= n) ? M1(Ht, ldh, j, k + 2) : 0.0;
+        }
+#pragma unroll
+        for (int e = 0; e < E; ++e) {
+            const int j = 1 + t + e * T;
+            if (j >= k + 1 && j <= n) {
+                dc gk;
+                if (sw) {
+                    const dc g = cscale(tau, h[e]);
+                    gk = g;
+                    dc rj = csub(r[e], cmul(l, g));
+                    if (j == k + 1) {
+                        gk = cadd(g, sigma);              // Gt[k+1,k] += sigma
+                        rj = csub(rj, cmul(l, sigma));    // r[k+1] -= l*sigma
+                    }
+                    r[e] = rj;
+                } else {
+                    const dc rj = r[e];
+                    gk = rj;
+                    dc rn = csub(cscale(tau, h[e]), cmul(l, rj));
+                    if (j == k + 1) rn = cadd(rn, sigma); // r[k+1] += sigma
+                    r[e] = rn;
+                }
+                M1(Gt, ldg, j, k) = gk.re;
+                M1(Gt, ldg, po + j, k) = gk.im;
+                if (j == k + 1) {  // owner of element k+1: publish it and decide step k+1
+                    s_next[(k + 1) & 1] = r[e];
+                    if (k + 1 <= n - 1) decide(k + 1, r[e], hsub[e]);
+                }
+            }
+            h[e] = hn[e];
+        }
+        __syncthreads();
+    }
+    if (t == 0) {  // finish (F:2579-2594)
+        const dc rn = s_next[n & 1];
+        M1(Gt, ldg, n, n) = rn.re;
+        M1(Gt, ldg, po + n, n) = rn.im;
+        swp[n - 1] = 0;
+        int info = s_info;
+        if (rn.re == 0.0 && rn.im == 0.0 && info == 0) info = n;
+        info_all[s] = info;
+    }
+    __syncthreads();
+    for (int j = 1 + t; j <= n; j += T) {
+        const dc q = cdiv(dc{1.0, 0.0}, dc{M1(Gt, ldg, j, j), M1(Gt, ldg, po + j, j)});
+        rdiag[2 * (j - 1)] = q.re;
+        rdiag[2 * (j - 1) + 1] = q.im;
+    }
+}
+
+cudaError_t launch_shift_lu_cplx(int n, const double* Ht, int ldh, const double* sig, const double* tau, int s0,
+                                 int count, double* Gt, int ldg, int po, uint8_t* swp, double* rd, int32_t* info,
+                                 cudaStream_t st)
+{
+    if (count <= 0 || n <= 0) return cudaSuccess;
+#define L_(T, E) shift_lu_cplx_kernel<T, E><<<count, T, 0, st>>>(n, Ht, ldh, sig, tau, s0, Gt, ldg, po, swp, rd, info)
+    if (n <= 256) L_(256, 1);
+    else if (n <= 1024) L_(512, 2);
+    else if (n <= 2048) L_(512, 4);
+    else if (n <= 4096) L_(512, 8);
+    else if (n <= 8192) L_(1024, 8);
+    else return cudaErrorInvalidValue;
+#undef L_
+    return cudaGetLastError();
+}
+
+// ---- planar Hessenberg solve, one CTA per complex right-hand side ----
+// Y holds each complex right-hand side as two real columns (real parts in column 2c,
+// imaginary parts in column 2c + 1, leading dimension ldy), as the L sweeps left them.
+constexpr int CT = 512;
+constexpr int CB = 32;
+
+__global__ void __launch_bounds__(CT) hess_cplx_kernel(int n, const double* __restrict__ Gt_all, int ldg, int po,
+                                                       const uint8_t* __restrict__ swap_all,
+                                                       const double* __restrict__ rdiag_all, double* Y, int ldy,
+                                                       int col0, int rhs_per_shift, const double* __restrict__ done,
+                                                       double tol)
+{
+    extern __shared__ double csm[];
+    const int cc = col0 + blockIdx.x;  // complex right-hand side
+    if (done && done[cc] <= tol) return;
+    const int n_ = n;
+    double* yr = csm;
+    double* yi = csm + n_;
+    __shared__ double tr_[CB][CB + 1], ti_[CB][CB + 1];
+    __shared__ double sjr[CB], sji[CB];
+    const int t = threadIdx.x, lane = t & 31, warp = t >> 5;
+    const int s = cc / rhs_per_shift;
+    const double* Gt = Gt_all + (size_t)s * ldg * n_;
+    const uint8_t* swp = swap_all + (size_t)s * n_;
+    const double* rd = rdiag_all + (size_t)s * 2 * n_;
+    double* Yr = Y + (size_t)(2 * blockIdx.x) * ldy;
+    double* Yi = Y + (size_t)(2 * blockIdx.x + 1) * ldy;
+    for (int i = t; i < n_; i += CT) {
+        yr[i] = Yr[i];
+        yi[i] = Yi[i];
+    }
+    __syncthreads();
+    if (t == 0 && n_ >= 2) {  // forward select-swap recurrence (F:2827-2838), complex multipliers
+        dc c = {yr[0], yi[0]};
+        for (int k = 1; k <= n_ - 1; ++k) {
+            const dc b = {yr[k], yi[k]};
+            const bool sw = swp[k - 1] != 0;
+            const dc xk = sw ? b : c;
+            yr[k - 1] = xk.re;
+            yi[k - 1] = xk.im;
+            const dc lk = {M1(Gt, ldg, k, k + 1), M1(Gt, ldg, po + k, k + 1)};
+            c = csub(sw ? c : b, cmul(lk, xk));
+        }
+        yr[n_ - 1] = c.re;
+        yi[n_ - 1] = c.im;
+    }
+    __syncthreads();
+    // back substitution in blocks of 32 rows from the bottom, left-looking: complex dot
+    // products with the contiguous columns of both planes of Gt, then a warp solves the block
+    const int nwarps = CT / 32;
+    for (int r1 = n_; r1 >= 1; r1 -= CB) {
+        const int r0 = max(r1 - CB + 1, 1);
+        const int bs = r1 - r0 + 1;
+        for (int jj = warp; jj < bs; jj += nwarps) {
+            const int j = r0 + jj;
+            const double* gr = Gt + (size_t)(j - 1) * ldg;  // real plane of column j = row j of U
+            const double* gi = gr + po;
+            if (r0 + lane <= r1) {
+                tr_[jj][lane] = gr[r0 + lane - 1];
+                ti_[jj][lane] = gi[r0 + lane - 1];
+            }
+            double ar = 0.0, ai = 0.0;
+            for (int i = r1 + 1 + lane; i <= n_; i += 32) {
+                const double xr = yr[i - 1], xi = yi[i - 1], g_r = gr[i - 1], g_i = gi[i - 1];
+                ar += g_r * xr - g_i * xi;
+                ai += g_r * xi + g_i * xr;
+            }
+            ar = warp_sum(ar);
+            ai = warp_sum(ai);
+            if (lane == 0) {
+                sjr[jj] = ar;
+                sji[jj] = ai;
+            }
+        }
+        __syncthreads();
+        if (warp == 0) {
+            const int i = r0 + lane;
+            dc yv = (i <= r1) ? csub(dc{yr[i - 1], yi[i - 1]}, dc{sjr[lane], sji[lane]}) : dc{0.0, 0.0};
+            const dc rdi = (i <= r1) ? dc{rd[2 * (i - 1)], rd[2 * (i - 1) + 1]} : dc{0.0, 0.0};
+            for (int j = r1; j >= r0; --j) {
+                dc xj = {0.0, 0.0};
+                if (i == j) {
+                    yv = cmul(yv, rdi);
+                    xj = yv;
+                }
+                xj.re = __shfl_sync(0xffffffffu, xj.re, j - r0);
+                xj.im = __shfl_sync(0xffffffffu, xj.im, j - r0);
+                if (i < j && i >= r0) {  // U[i, j] = Gt[j, i] (staged as tr_[i - r0][j - r0])
+                    const dc u = {tr_[lane][j - r0], ti_[lane][j - r0]};
+                    yv = csub(yv, cmul(u, xj));
+                }
+            }
+            if (i <= r1) {
+                yr[i - 1] = yv.re;
+                yi[i - 1] = yv.im;
+            }
+        }
+        __syncthreads();
+    }
+    for (int i = t; i < n_; i += CT) {
+        Yr[i] = yr[i];
+        Yi[i] = yi[i];
+    }
+}
+
+cudaError_t launch_hess_cplx(int n, const double* Gt, int ldg, int po, const uint8_t* swp, const double* rd,
+                             double* Y, int ldy, int col0, int count, int rhs_per_shift, const double* done,
+                             double tol, cudaStream_t st)
+{
+    if (count <= 0 || n <= 0) return cudaSuccess;
+    const size_t smem = (size_t)2 * n * sizeof(double);
+    if (smem > 150 * 1024) return cudaErrorInvalidValue;
+    static size_t attr = 0;
+    if (smem > 32 * 1024 && smem > attr) {
+        cudaError_t e = cudaFuncSetAttribute(hess_cplx_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        if (e != cudaSuccess) return e;
+        attr = smem;
+    }
+    hess_cplx_kernel<<<count, CT, smem, st>>>(n, Gt, ldg, po, swp, rd, Y, ldy, col0, rhs_per_shift, done, tol);
+    return cudaGetLastError();
+}
+
+// ---- complex residual r = b - (sigma_s x + tau_s J x), J real; b, x, r interleaved complex ----
+// Tiles of 16 rows x 8 complex right-hand sides (16 real columns), one complex column pair
+// per thread; k in chunks of 64 through shared memory.
+constexpr int QM = 16, QC = 8, QK = 64, QT = 128;
+
+__global__ void __launch_bounds__(QT) residual_cplx_kernel(int n, const double* __restrict__ J, int ldj,
+                                                            const double* __restrict__ B, int ldb,
+                                                            const double* __restrict__ X, int ldx,
+                                                            double* __restrict__ R, int ldr, int nrhs,
+                                                            int rhs_per_shift, const double* __restrict__ sig,
+                                                            const double* __restrict__ tau,
+                                                            const double* __restrict__ done, double tol)
+{
+    __shared__ double Js[QK][QM + 1];
+    __shared__ double Xs[QK][2 * QC + 1];
+    const int i0 = blockIdx.x * QM, c0 = blockIdx.y * QC;
+    if (done) {
+        bool all = true;
+        for (int c = c0; c < c0 + QC && c < nrhs; ++c) all = all && (done[c] <= tol);
+        if (all) return;
+    }
+    const int t = threadIdx.x;
+    const int r = t % QM, cq = t / QM;  // cq in 0..7: complex column c0 + cq
+    double ar = 0.0, ai = 0.0;
+    for (int k0 = 0; k0 < n; k0 += QK) {
+        for (int e = t; e < QM * QK; e += QT) {
+            const int ii = e % QM, kk = e / QM;
+            const int i = i0 + ii, k = k0 + kk;
+            Js[kk][ii] = (i < n && k < n) ? J[(size_t)k * ldj + i] : 0.0;
+        }
+        for (int e = t; e < QK * 2 * QC; e += QT) {
+            const int kk = e % QK, cp = e / QK;  // cp = 2 (column) + part
+            const int k = k0 + kk, c = c0 + (cp >> 1);
+            Xs[kk][cp] = (k < n && c < nrhs) ? X[2 * ((size_t)c * ldx + k) + (cp & 1)] : 0.0;
+        }
+        __syncthreads();
+#pragma unroll 8
+        for (int kk = 0; kk < QK; ++kk) {
+            const double jv = Js[kk][r];
+            ar = dfma(jv, Xs[kk][2 * cq], ar);
+            ai = dfma(jv, Xs[kk][2 * cq + 1], ai);
+        }
+        __syncthreads();
+    }
+    const int i = i0 + r, c = c0 + cq;
+    if (i < n && c < nrhs) {
+        const int s = c / rhs_per_shift;
+        const dc sg = {sig[2 * s], sig[2 * s + 1]}, tu = {tau[2 * s], tau[2 * s + 1]};
+        const dc xv = {X[2 * ((size_t)c * ldx + i)], X[2 * ((size_t)c * ldx + i) + 1]};
+        const dc bv = {B[2 * ((size_t)c * ldb + i)], B[2 * ((size_t)c * ldb + i) + 1]};
+        const dc w = cadd(cmul(sg, xv), cmul(tu, dc{ar, ai}));
+        R[2 * ((size_t)c * ldr + i)] = bv.re - w.re;
+        R[2 * ((size_t)c * ldr + i) + 1] = bv.im - w.im;
+    }
+}
+
+cudaError_t launch_residual_cplx(int n, const double* J, int ldj, const double* B, int ldb, const double* X, int ldx,
+                                 double* R, int ldr, int nrhs, int rhs_per_shift, const double* sig, const double* tau,
+                                 cudaStream_t st, const double* done, double tol)
+{
+    if (nrhs <= 0 || n <= 0) return cudaSuccess;
+    dim3 grid((n + QM - 1) / QM, (nrhs + QC - 1) / QC);
+    residual_cplx_kernel<<<grid, QT, 0, st>>>(n, J, ldj, B, ldb, X, ldx, R, ldr, nrhs, rhs_per_shift, sig, tau, done,
+                                              tol);
+    return cudaGetLastError();
+}
+
+__global__ void real_to_cplx_kernel(const double* __restrict__ re, double* __restrict__ out, int count)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < count) {
+        out[2 * i] = re[i];
+        out[2 * i + 1] = 0.0;
+    }
+}
+
+cudaError_t launch_real_to_cplx(const double* re, double* out, int count, cudaStream_t st)
+{
+    if (count <= 0) return cudaSuccess;
+    real_to_cplx_kernel<<<(count + 255) / 256, 256, 0, st>>>(re, out, count);
+    return cudaGetLastError();
+}
+
+}  // namespace lhl

@@ -57,6 +57,8 @@ struct LdivArgs {
     int nshifts;          // shift slots in the batch at Gt (for the tensor map over all of them)
     const double* uinv;   // mixed form: inverses of U's 32 x 32 diagonal blocks per shift, or null
     const double* linv;   // mixed form: inverses of L's 64 x 64 diagonal blocks, or null
+    int cplx;             // complex shift: Gt planar (po rows per plane), rdiag and X interleaved complex
+    int po;
     int* zflags;          // ldiv scratch: ready flags of the blocked forward substitution
     int nzflags;
     int* err;             // bounded-wait status (the workspace's error word)
@@ -82,6 +84,8 @@ struct ZArgs {
     const double* done;  // optional: a tile whose columns all have done[c] <= tol is skipped
     double tol;
     const double* linv;  // zinv, mixed form: inverses of L's 64 x 64 diagonal blocks
+    int cplx;            // gather source / scatter destination interleaved complex (column c: part
+                         // c & 1 of complex column c >> 1)
     int* err;
     unsigned long long limit_ns;
 };
@@ -126,6 +130,17 @@ cudaError_t launch_shift_lu(int n, const double* Ht, int ldh, const double* sig,
 
 cudaError_t launch_ldiv(const LdivArgs& a, int nrhs, cudaStream_t st);
 cudaError_t launch_linv(int n, const double* F, int ldf, double* linv, cudaStream_t st);
+// complex shifts on a real reduction (complex.cu)
+cudaError_t launch_shift_lu_cplx(int n, const double* Ht, int ldh, const double* sig, const double* tau, int s0,
+                                 int count, double* Gt, int ldg, int po, uint8_t* swp, double* rd, int32_t* info,
+                                 cudaStream_t st);
+cudaError_t launch_hess_cplx(int n, const double* Gt, int ldg, int po, const uint8_t* swp, const double* rd,
+                             double* Y, int ldy, int col0, int count, int rhs_per_shift, const double* done,
+                             double tol, cudaStream_t st);
+cudaError_t launch_residual_cplx(int n, const double* J, int ldj, const double* B, int ldb, const double* X, int ldx,
+                                 double* R, int ldr, int nrhs, int rhs_per_shift, const double* sig, const double* tau,
+                                 cudaStream_t st, const double* done = nullptr, double tol = 0.0);
+cudaError_t launch_real_to_cplx(const double* re, double* out, int count, cudaStream_t st);
 cudaError_t launch_uinv(int n, const double* Gt, int ldg, const double* rd, int s0, int count, double* uinv,
                         cudaStream_t st);
 cudaError_t launch_residual(int n, const double* J, int ldj, const double* B, int ldb, const double* X, int ldx,

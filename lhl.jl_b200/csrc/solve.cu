@@ -25,12 +25,13 @@ constexpr int BS = 32;
 
 constexpr int ZT = 512;
 
-// true when every column c0..c0+cnt-1 (< m) is marked converged
-__device__ __forceinline__ bool tile_done(const double* done, double tol, int c0, int cnt, int m)
+// true when every column c0..c0+cnt-1 (< m) is marked converged; with cs = 1 the columns
+// are the two parts of complex right-hand sides and done[] is indexed by c >> 1
+__device__ __forceinline__ bool tile_done(const double* done, double tol, int c0, int cnt, int m, int cs = 0)
 {
     if (!done) return false;
     for (int c = c0; c < c0 + cnt && c < m; ++c)
-        if (!(done[c] <= tol)) return false;
+        if (!(done[c >> cs] <= tol)) return false;
     return true;
 }
 
@@ -62,17 +63,19 @@ __global__ void __launch_bounds__(ZIT, 2) zl_kernel(ZArgs z)
     for (int task = blockIdx.x; task < nblk * ntile; task += gridDim.x) {
         const int ib = task / ntile, c = task - ib * ntile;
         const int i = MUL ? nblk - 1 - ib : ib;  // L y: the longest rows first
-        if (tile_done(z.done, z.tol, c * ZC, ZC, m)) continue;  // all of its tasks skip alike
+        if (tile_done(z.done, z.tol, c * ZC, ZC, m, z.cplx)) continue;  // all of its tasks skip alike
         const int row = i * ZR + r, col = c * ZC + jr;
         const bool live = row < n && col < m;
         double acc = 0.0;
         if (live) {
-            const double* x = z.src + (size_t)col * z.lds;
-            if (!MUL && z.gather) {
+            if (!MUL && z.gather && z.cplx) {  // part col & 1 of interleaved complex column col >> 1
                 const int64_t p = z.perm[row];
-                acc = x[p - 1] * z.iscale[p - 1];
+                acc = z.src[2 * ((size_t)(col >> 1) * z.lds + (p - 1)) + (col & 1)] * z.iscale[p - 1];
+            } else if (!MUL && z.gather) {
+                const int64_t p = z.perm[row];
+                acc = z.src[(size_t)col * z.lds + (p - 1)] * z.iscale[p - 1];
             } else {
-                acc = x[row];
+                acc = z.src[(size_t)col * z.lds + row];
             }
         }
         // L tiles are software-pipelined: tile j+1 is in registers while tile j is used
@@ -184,7 +187,8 @@ __global__ void __launch_bounds__(ZIT, 2) zl_kernel(ZArgs z)
         }
         if (MUL && live) {  // x[perm[row]] = (L y)[row] * scale[perm[row]]
             const int64_t p = z.perm[row];
-            z.dst[(size_t)col * z.ldd + (p - 1)] = acc * z.scale[p - 1];
+            if (z.cplx) z.dst[2 * ((size_t)(col >> 1) * z.ldd + (p - 1)) + (col & 1)] = acc * z.scale[p - 1];
+            else z.dst[(size_t)col * z.ldd + (p - 1)] = acc * z.scale[p - 1];
         }
     }
 }
@@ -676,6 +680,27 @@ cudaError_t launch_ldiv(const LdivArgs& a, int nrhs, cudaStream_t st)
     z.tol = a.tol;
     z.linv = a.linv;
     if (!a.Y || a.ycap <= 0 || !a.zflags || !a.err) return cudaErrorInvalidValue;
+    if (a.mode == 0 && a.cplx) {
+        // complex shift on a real reduction: each complex right-hand side is two real columns
+        // of Y (its planes) for the L sweeps (F:3092-3104)
+        const int chunk = a.ycap / 2;
+        for (int c0 = 0; c0 < nrhs; c0 += chunk) {
+            const int cnt = min(chunk, nrhs - c0);
+            z.cplx = 1;
+            z.src = a.X + 2 * (size_t)c0 * a.ldx; z.lds = a.ldx; z.dst = a.Y; z.ldd = a.n; z.m = 2 * cnt;
+            z.gather = 1;
+            z.done = a.done ? a.done + c0 : nullptr;
+            cudaError_t e = run_zinv(z, st);
+            if (e == cudaSuccess)
+                e = launch_hess_cplx(a.n, a.Gt, a.ldg, a.po, a.swp, a.rdiag, a.Y, a.n, c0, cnt, a.rhs_per_shift,
+                                     a.done, a.tol, st);
+            if (e != cudaSuccess) return e;
+            z.src = a.Y; z.lds = a.n; z.dst = a.X + 2 * (size_t)c0 * a.ldx; z.ldd = a.ldx; z.gather = 0;
+            e = run_zmul(z, st);
+            if (e != cudaSuccess) return e;
+        }
+        return cudaSuccess;
+    }
     if (a.mode == 1) {  // applyZinv: x <- L^-1 P^-1 D^-1 x, through the scratch
         for (int c0 = 0; c0 < nrhs; c0 += a.ycap) {
             const int cnt = min(a.ycap, nrhs - c0);

@@ -53,7 +53,7 @@ class _WsView(C.Structure):
 class _ShView(C.Structure):
     _fields_ = [("n", C.c_int64), ("nshifts", C.c_int64), ("ldg", C.c_int64), ("Gt", C.c_void_p),
                 ("swap", C.c_void_p), ("rdiag", C.c_void_p), ("info", C.c_void_p), ("sigma", C.c_void_p),
-                ("tau", C.c_void_p)]
+                ("tau", C.c_void_p), ("po", C.c_int64), ("is_complex", C.c_int32)]
 
 
 def _load():
@@ -75,6 +75,9 @@ def _load():
         "lhl_shift_get_view": [vp, C.POINTER(_ShView)],
         "lhl_shift_batched": [vp, vp, i64, i64, vp, vp, vp],
         "lhl_shift": [vp, vp, i64, d, d, vp],
+        "lhl_shift_create_complex": [i64, i64, C.POINTER(vp)],
+        "lhl_shift_complex": [vp, vp, i64, d, d, d, d, vp],
+        "lhl_shift_batched_complex": [vp, vp, i64, i64, vp, vp, vp],
         "lhl_ldiv": [vp, vp, vp, i64, i64, i64, vp],
         "lhl_refine": [vp, vp, vp, i64, vp, i64, vp, i64, vp, i64, i64, i32, vp],
         "lhl_refine_tol": [vp, vp, vp, i64, vp, i64, vp, i64, vp, vp, i64, i64, d, i32, vp],
@@ -142,30 +145,40 @@ def _colmajor(M: torch.Tensor) -> torch.Tensor:
     return M.t().contiguous().t()
 
 
-def _require_cuda_f64(x: torch.Tensor, name: str):
+def _require_cuda_f64(x: torch.Tensor, name: str, cplx: bool = False):
     if not isinstance(x, torch.Tensor) or not x.is_cuda:
         raise ArgumentError(f"{name} must be a CUDA tensor")
-    if x.dtype != torch.float64:
+    want = torch.complex128 if cplx else torch.float64
+    if x.dtype != want:
+        if cplx:
+            raise ArgumentError(f"{name} must be complex128: a real vector cannot hold the solution of a "
+                                "complex shift (F:3084-3085)")
         raise ArgumentError(f"{name} must be float64 (complex shifts need an LHLShift built for them)")
 
 
 class LHLShift:
-    """``LHLShift{Float64}(n)``: a batch of ``nshifts`` shift slots (src/LHLFactorization.jl:84-116)."""
+    """``LHLShift{Float64}(n)`` or, with ``complex=True``, ``LHLShift{ComplexF64}(n)`` on a real
+    reduction: a batch of ``nshifts`` shift slots (src/LHLFactorization.jl:84-116).  A complex
+    shift object's Gt is planar: (2 po) x n per slot, real parts in rows 0..n-1, imaginary
+    parts in rows po..po+n-1."""
 
-    def __init__(self, n, nshifts: int = 1):
+    def __init__(self, n, nshifts: int = 1, complex: bool = False):
         if isinstance(n, LHLWorkspace):
             n = n.n
         self._h = C.c_void_p()
-        _check(_lib.lhl_shift_create(int(n), int(nshifts), C.byref(self._h)), "LHLShift")
+        create = _lib.lhl_shift_create_complex if complex else _lib.lhl_shift_create
+        _check(create(int(n), int(nshifts), C.byref(self._h)), "LHLShift")
         self.n = int(n)
         self.nshifts = int(nshifts)
         v = _ShView()
         _check(_lib.lhl_shift_get_view(self._h, C.byref(v)))
         self._v = v
+        self.is_complex = bool(v.is_complex)
+        self.po = int(v.po)
 
     def __del__(self):
         h = getattr(self, "_h", None)
-        if h is not None and h.value:
+        if h is not None and h.value and _lib is not None:
             _lib.lhl_shift_destroy(h)
             self._h = None
 
@@ -182,6 +195,8 @@ class LHLShift:
         return _view(self._v.swap + slot * self.n, (self.n,), "|u1")
 
     def rdiag(self, slot: int = 0) -> torch.Tensor:
+        if self.is_complex:
+            return torch.view_as_complex(_view(self._v.rdiag + 16 * slot * self.n, (self.n, 2)))
         return _view(self._v.rdiag + 8 * slot * self.n, (self.n,))
 
     @property
@@ -190,10 +205,14 @@ class LHLShift:
 
     @property
     def sigma_all(self) -> torch.Tensor:
+        if self.is_complex:
+            return torch.view_as_complex(_view(self._v.sigma, (self.nshifts, 2)))
         return _view(self._v.sigma, (self.nshifts,))
 
     @property
     def tau_all(self) -> torch.Tensor:
+        if self.is_complex:
+            return torch.view_as_complex(_view(self._v.tau, (self.nshifts, 2)))
         return _view(self._v.tau, (self.nshifts,))
 
     @property
@@ -203,11 +222,13 @@ class LHLShift:
 
     @property
     def σ(self):
-        return float(self.sigma_all[0].item())
+        v = self.sigma_all[0].item()
+        return v if self.is_complex else float(v)
 
     @property
     def τ(self):
-        return float(self.tau_all[0].item())
+        v = self.tau_all[0].item()
+        return v if self.is_complex else float(v)
 
 
 class LHLWorkspace:
@@ -218,15 +239,17 @@ class LHLWorkspace:
 
     _SHIFT_FIELDS = ("Gt", "rdiag", "swap", "info", "σ", "τ")
 
-    def __init__(self, n: int, precision: int = LHL_PREC_FP64):
+    def __init__(self, n: int, precision: int = LHL_PREC_FP64, shift_complex: bool = False):
         self._h = C.c_void_p()
         _check(_lib.lhl_ws_create(int(n), int(precision), C.byref(self._h)), "LHLWorkspace")
         self.n = int(n)
         self.precision = precision
+        self.shift_complex = bool(shift_complex)
         v = _WsView()
         _check(_lib.lhl_ws_get_view(self._h, C.byref(v)))
         self._v = v
-        self.shift = LHLShift(self.n, 1)
+        # ws.shift: LHLShift{Float64}, or LHLShift{ComplexF64} for shift = Complex{T} (F:164-178)
+        self.shift = LHLShift(self.n, 1, complex=self.shift_complex)
         self.reduced = False
 
     def __del__(self):
@@ -312,19 +335,20 @@ def lhl_reduce_(ws: LHLWorkspace, J: torch.Tensor, balance: bool, thread=True, s
 
 
 def lhl(J: torch.Tensor, balance: bool = True, thread=True, precision: int = LHL_PREC_FP64,
-        stream=None) -> LHLWorkspace:
-    """``lhl(J; balance=true)`` (F:3179): allocate a workspace and reduce J into it."""
+        shift_complex: bool = False, stream=None) -> LHLWorkspace:
+    """``lhl(J; balance=true, shift=...)`` (F:3179): allocate a workspace and reduce J into it;
+    ``shift_complex=True`` is ``shift = ComplexF64`` (complex shifts on the real reduction)."""
     _require_cuda_f64(J, "J")
     if J.dim() != 2 or J.shape[0] != J.shape[1]:
         raise DimensionMismatch(f"matrix is not square: dimensions are {tuple(J.shape)}")
-    ws = LHLWorkspace(J.shape[0], precision)
+    ws = LHLWorkspace(J.shape[0], precision, shift_complex)
     return lhl_reduce_(ws, J, balance, thread, stream)
 
 
 def lhl_(ws: LHLWorkspace, J: torch.Tensor, balance: bool = True, thread=True, stream=None) -> LHLWorkspace:
     """``lhl!(ws, J; balance)`` (F:3192).  A workspace of another order is rebuilt in place."""
     if J.shape[0] != ws.n:
-        new = LHLWorkspace(J.shape[0], ws.precision)
+        new = LHLWorkspace(J.shape[0], ws.precision, ws.shift_complex)
         ws.__dict__.update({k: v for k, v in new.__dict__.items()})
         new._h = None
     return lhl_reduce_(ws, J, balance, thread, stream)
@@ -343,20 +367,36 @@ def _shift_args(a):
 def lhl_shift_(*args, slot: int = 0, stream=None):
     """``lhl_shift!(ws, sigma, tau)`` / ``lhl_shift!(sh, ws, sigma, tau)`` (F:2456-2489)."""
     sh, ws, sigma, tau, ret = _shift_args(args)
+    if sh.n != ws.n:
+        raise DimensionMismatch(f"the LHLShift is {sh.n}x{sh.n}, the workspace {ws.n}x{ws.n}")
+    if sh.is_complex:
+        sigma, tau = complex(sigma), complex(tau)
+        _check(_lib.lhl_shift_complex(sh._h, ws._h, int(slot), sigma.real, sigma.imag, tau.real, tau.imag,
+                                      _stream(stream)), "lhl_shift")
+        return ret
     for v in (sigma, tau):
         if isinstance(v, complex) and v.imag != 0:
             raise ArgumentError(f"complex shift ({sigma}, {tau}) on a real LHLShift")
     sigma = float(sigma.real if isinstance(sigma, complex) else sigma)
     tau = float(tau.real if isinstance(tau, complex) else tau)
-    if sh.n != ws.n:
-        raise DimensionMismatch(f"the LHLShift is {sh.n}x{sh.n}, the workspace {ws.n}x{ws.n}")
     _check(_lib.lhl_shift(sh._h, ws._h, int(slot), sigma, tau, _stream(stream)), "lhl_shift")
     return ret
 
 
 def lhl_shift_batched_(sh: LHLShift, ws: LHLWorkspace, sigmas: torch.Tensor, taus: torch.Tensor, s0: int = 0,
                        stream=None) -> LHLShift:
-    """Load len(sigmas) shifts into slots s0.. of ``sh`` in one launch (device arrays)."""
+    """Load len(sigmas) shifts into slots s0.. of ``sh`` in one launch (device arrays; complex128
+    arrays for complex shifts, which need a complex ``sh``)."""
+    if sigmas.is_complex() or taus.is_complex():
+        if not sh.is_complex:
+            raise ArgumentError("complex shifts on a real LHLShift")
+        sigmas = sigmas.to(torch.complex128).contiguous()
+        taus = taus.to(torch.complex128).contiguous()
+        if sigmas.numel() != taus.numel():
+            raise DimensionMismatch("sigmas and taus differ in length")
+        _check(_lib.lhl_shift_batched_complex(sh._h, ws._h, int(s0), sigmas.numel(), C.c_void_p(sigmas.data_ptr()),
+                                              C.c_void_p(taus.data_ptr()), _stream(stream)), "lhl_shift_batched")
+        return sh
     _require_cuda_f64(sigmas, "sigmas")
     _require_cuda_f64(taus, "taus")
     sigmas = sigmas.contiguous()
@@ -392,9 +432,9 @@ def lhl_ldiv_(x: torch.Tensor, *args, rhs_per_shift: int = 1, stream=None) -> to
         sh = ws.shift
     else:
         sh, ws = args
-    if x.is_complex():
+    if x.is_complex() and not sh.is_complex:
         raise ArgumentError("a complex right-hand side needs an LHLShift built for complex shifts")
-    _require_cuda_f64(x, "x")
+    _require_cuda_f64(x, "x", sh.is_complex)
     if sh.n != ws.n:
         raise DimensionMismatch(f"the LHLShift is {sh.n}x{sh.n}, the workspace {ws.n}x{ws.n}")
     xx, k, ld = _as_cols(x, ws.n)
@@ -419,16 +459,17 @@ def lhl_refine_(x: torch.Tensor, J: torch.Tensor, b: torch.Tensor, *args, steps:
         raise TypeError("lhl_refine_(x, J, b, ws, steps) or (x, J, b, sh, ws, steps)")
     if steps <= 0:
         return x
-    for t, nm in ((x, "x"), (J, "J"), (b, "b")):
-        _require_cuda_f64(t, nm)
+    _require_cuda_f64(J, "J")
+    for t, nm in ((x, "x"), (b, "b")):
+        _require_cuda_f64(t, nm, sh.is_complex)
     n = ws.n
     xx, k, ldx = _as_cols(x, n)
     bb, kb, ldb = _as_cols(b, n)
     if kb != k:
         raise DimensionMismatch("x and b differ in column count")
     Jc = _colmajor(J)
-    R = torch.empty((n, k), dtype=torch.float64, device=x.device).t().contiguous().t() if k > 1 else \
-        torch.empty(n, dtype=torch.float64, device=x.device)
+    dt = torch.complex128 if sh.is_complex else torch.float64
+    R = torch.empty((k, n), dtype=dt, device=x.device).t() if k > 1 else torch.empty(n, dtype=dt, device=x.device)
     ldr = n
     if ldx != ldr:
         raise ArgumentError("x must have leading dimension n")
@@ -445,8 +486,9 @@ def lhl_refine_tol_(x: torch.Tensor, J: torch.Tensor, b: torch.Tensor, sh: LHLSh
     ``lhl_refine!`` (F:3144-3157); columns already at relative residual <= tol are skipped on
     the device.  Returns the per-column final relative residuals (device tensor); x is updated
     in place.  `R` (n x k scratch) and `res` (k) may be passed to avoid allocation."""
-    for t, nm in ((x, "x"), (J, "J"), (b, "b")):
-        _require_cuda_f64(t, nm)
+    _require_cuda_f64(J, "J")
+    for t, nm in ((x, "x"), (b, "b")):
+        _require_cuda_f64(t, nm, sh.is_complex)
     n = ws.n
     xx, k, ldx = _as_cols(x, n)
     bb, kb, ldb = _as_cols(b, n)
@@ -456,7 +498,7 @@ def lhl_refine_tol_(x: torch.Tensor, J: torch.Tensor, b: torch.Tensor, sh: LHLSh
         raise ArgumentError("x must have leading dimension n")
     Jc = _colmajor(J)
     if R is None:
-        R = torch.empty((k, n), dtype=torch.float64, device=x.device)
+        R = torch.empty((k, n), dtype=torch.complex128 if sh.is_complex else torch.float64, device=x.device)
     if res is None:
         res = torch.empty(k, dtype=torch.float64, device=x.device)
     if R.numel() < n * k or res.numel() < k:
@@ -475,7 +517,7 @@ def residual_norms(sh: LHLShift, J: torch.Tensor, b: torch.Tensor, x: torch.Tens
     xx, k, ldx = _as_cols(x, n)
     bb, _, ldb = _as_cols(b, n)
     Jc = _colmajor(J)
-    R = torch.empty((k, n), dtype=torch.float64, device=x.device)
+    R = torch.empty((k, n), dtype=torch.complex128 if sh.is_complex else torch.float64, device=x.device)
     out = torch.empty(k, dtype=torch.float64, device=x.device)
     _check(_lib.lhl_residual_norms(sh._h, C.c_void_p(Jc.data_ptr()), max(Jc.stride(1), n), C.c_void_p(bb.data_ptr()),
                                    ldb, C.c_void_p(xx.data_ptr()), ldx, C.c_void_p(R.data_ptr()),

@@ -1,0 +1,164 @@
+"""Complex shifts on a real reduction (LHLShift{ComplexF64} on LHLWorkspace{Float64}) on the
+device, through the C ABI: the shift LU bit for bit against the oracle (planar Gt, swap,
+rdiag, info), solves against a dense complex LU and the oracle (test/core_tests.jl:251-280),
+refinement to 1e-10 on a resolvent sweep shaped like config 5, and the reference's errors."""
+import numpy as np
+import pytest
+
+from oracle import oracle as O
+
+pytestmark = pytest.mark.gpu
+
+SHIFTS = ((0.4 + 0.7j, -1.0), (1.0, -0.1 + 0.2j), (0.0, 1j), (2j, 0.0), (-3.0 + 2j, 2.0 - 1j))
+
+
+def _mods():
+    import torch
+    import lhl_gpu as G
+    return torch, G
+
+
+def dev(a):
+    torch, _ = _mods()
+    return torch.as_tensor(np.asfortranarray(a)).cuda()
+
+
+def host(t):
+    return t.detach().cpu().numpy()
+
+
+def rng(seed):
+    return np.random.default_rng(seed)
+
+
+def bits_equal(a, b):
+    a = np.ascontiguousarray(a)
+    b = np.ascontiguousarray(b)
+    return a.shape == b.shape and a.dtype == b.dtype and np.array_equal(a.view(np.uint8), b.view(np.uint8))
+
+
+@pytest.mark.parametrize("n", list(range(1, 34)) + [63, 64, 65, 255, 256, 257, 511, 512, 513, 1024, 2048])
+@pytest.mark.parametrize("tie", [False, True])
+def test_complex_shift_bitexact(n, tie):
+    """The device shift LU (planar Gt, swap, rdiag, info) is bit-identical to the oracle's."""
+    torch, G = _mods()
+    g = rng(32 + n)
+    J = g.integers(-2, 3, (n, n)).astype(float) if tie else g.standard_normal((n, n))
+    R = O.reduce(J)
+    ws = G.lhl(dev(J), shift_complex=True)
+    for s, t in SHIFTS + ((0.0, 0.0),):
+        G.lhl_shift_(ws, s, t)
+        So = O.shift_complex(R, s, t)
+        sh = ws.shift
+        assert sh.po == So.po
+        Gt = host(sh.Gt())
+        torch.cuda.synchronize()
+        # every entry the elimination writes: rows k..n of column k and row k of column k+1, both planes
+        for k in range(n):
+            for off in (0, sh.po):
+                assert bits_equal(Gt[off + k:off + n, k], So.Gt[off + k:off + n, k]), (s, t, k)
+                if k + 1 < n:
+                    assert bits_equal(Gt[off + k, k + 1:k + 2], So.Gt[off + k, k + 1:k + 2])
+        assert np.array_equal(host(sh.swap())[:n], So.swap[:n])
+        assert sh.info == So.info
+        if So.info == 0:
+            assert bits_equal(host(sh.rdiag()), So.rdiag[:n])
+
+
+@pytest.mark.parametrize("n", [1, 2, 3, 5, 40, 129, 260, 600])
+def test_complex_solves(n):
+    """test/core_tests.jl:251-280 on the device: solves against a dense complex LU (rtol 1e-9) and
+    the oracle's, and one refinement step: bwd <= 2 bwd(x) + eps and < 50 eps."""
+    torch, G = _mods()
+    J = rng(n).standard_normal((n, n))
+    g = rng(n + 7)
+    b = g.standard_normal(n) + 1j * g.standard_normal(n)
+    R = O.reduce(J)
+    Jd = dev(J)
+    ws = G.lhl(Jd, shift_complex=True)
+    eps = np.finfo(float).eps
+    for s, t in ((0.4 + 0.7j, -1.0), (1.0, -0.05 + 0.3j), (0.0, 1j), (-3.0 + 2j, 2.0 - 1j), (1.0, -0.05)):
+        W = s * np.eye(n) + t * J
+        G.lhl_shift_(ws, s, t)
+        x = G.lhl_ldiv_(dev(b), ws)
+        xh = host(x)
+        xr = np.linalg.solve(W, b)
+        assert np.linalg.norm(xh - xr) <= 1e-9 * np.linalg.norm(xr)
+        xo = O.ldiv_complex(R, O.shift_complex(R, s, t), b)
+        assert np.linalg.norm(xh - xo) <= 1e-9 * np.linalg.norm(xo)
+        y = host(G.lhl_refine_(x.clone(), Jd, dev(b), ws, 1))
+        assert O.bwd(W, y, b) <= 2 * O.bwd(W, xh, b) + eps
+        assert O.bwd(W, y, b) < 50 * eps
+
+
+@pytest.mark.parametrize("n", [60, 700])
+def test_complex_batched_matches_single(n):
+    torch, G = _mods()
+    J = rng(3 + n).standard_normal((n, n))
+    ws = G.lhl(dev(J), shift_complex=True)
+    sig = np.array([0.5 + 1j, -1.0 + 3j, 0.2j, 2.0])
+    tau = np.array([-1.0, -1.0 + 0.1j, 1.0, -0.5j])
+    sh = G.LHLShift(n, 4, complex=True)
+    G.lhl_shift_batched_(sh, ws, dev(sig), dev(tau))
+    B = rng(4).standard_normal((n, 8)) + 1j * rng(5).standard_normal((n, 8))
+    X = dev(B)
+    G.lhl_ldiv_(X, sh, ws, rhs_per_shift=2)
+    Xh = host(X)
+    for s in range(4):
+        G.lhl_shift_(ws, sig[s], tau[s])
+        assert bits_equal(host(ws.shift.Gt()), host(sh.Gt(s)))
+        for r in range(2):
+            x1 = host(G.lhl_ldiv_(dev(B[:, 2 * s + r]), ws))
+            assert bits_equal(x1, Xh[:, 2 * s + r])
+
+
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_resolvent_sweep_reaches_1e10(precision):
+    """Config 5's shape at n = 1024: J ~ N(0,1)/sqrt(n), complex shifts s = a + ib with a in
+    [-2, 0], b in [0, 10], (sigma, tau) = (s, -1), four complex N(0,1) right-hand sides per
+    shift, refined to relative residual <= 1e-10 in both forms."""
+    torch, G = _mods()
+    n, S, Rr = 1024, 8, 4
+    J = rng(10).standard_normal((n, n)) / np.sqrt(n)
+    g = rng(11)
+    s = g.uniform(-2.0, 0.0, S) + 1j * g.uniform(0.0, 10.0, S)
+    g2 = rng(12)
+    B = g2.standard_normal((n, S * Rr)) + 1j * g2.standard_normal((n, S * Rr))
+    Jd = dev(J)
+    prec = G.LHL_PREC_MIXED if precision == "mixed" else G.LHL_PREC_FP64
+    ws = G.lhl(Jd, precision=prec, shift_complex=True)
+    ws.check()
+    sh = G.LHLShift(n, S, complex=True)
+    G.lhl_shift_batched_(sh, ws, dev(s), dev(-np.ones(S, dtype=complex)))
+    Bd = dev(B)
+    X = Bd.clone()
+    G.lhl_ldiv_(X, sh, ws, rhs_per_shift=Rr)
+    res = host(G.lhl_refine_tol_(X, Jd, Bd, sh, ws, tol=1e-10, max_steps=16, rhs_per_shift=Rr))
+    assert (res <= 1e-10).all(), res
+    Xh = host(X)
+    for c in (0, S * Rr - 1):
+        W = s[c // Rr] * np.eye(n) - J
+        assert np.linalg.norm(B[:, c] - W @ Xh[:, c]) <= 1.0001e-10 * np.linalg.norm(B[:, c])
+
+
+def test_complex_errors_mirror_the_reference():
+    torch, G = _mods()
+    n = 6
+    J = rng(1).standard_normal((n, n))
+    ws = G.lhl(dev(J))
+    with pytest.raises(G.ArgumentError):  # complex shift on a real LHLShift (F:2466-2472)
+        G.lhl_shift_(ws, 1.0, -0.3j)
+    G.lhl_shift_(ws, 1.0, -0.3)
+    with pytest.raises(G.ArgumentError):  # complex x with a real shift
+        G.lhl_ldiv_(dev(np.ones(n) + 0j), ws)
+    wc = G.lhl(dev(J), shift_complex=True)
+    G.lhl_shift_(wc, 1.0 + 1j, -0.3)
+    with pytest.raises(G.ArgumentError):  # a real x cannot hold a complex shift's solution (F:3084-3085)
+        G.lhl_ldiv_(dev(np.ones(n)), wc)
+    x = dev(np.ones(n) + 0j)
+    assert G.lhl_ldiv_(x, wc) is x
+    # a real shift on a complex LHLShift is converted (F:2474-2475)
+    G.lhl_shift_(wc, 2.0, -0.5)
+    Wr = 2.0 * np.eye(n) - 0.5 * J
+    b = rng(2).standard_normal(n) + 0j
+    assert np.allclose(host(G.lhl_ldiv_(dev(b), wc)), np.linalg.solve(Wr, b), rtol=1e-10, atol=1e-12)
