@@ -155,6 +155,47 @@ int lhl_residual_norms(lhl_shift_t sh, const double* dJ, int64_t ldj, const doub
 int lhl_applyZ(lhl_ws_t ws, double* dX, int64_t ldx, int64_t nrhs, void* stream);
 int lhl_applyZinv(lhl_ws_t ws, double* dX, int64_t ldx, int64_t nrhs, void* stream);
 
+/* ---- batches of independent matrices of uneven order -------------------------------- */
+/* Many Jacobians J_m (order n_m <= 499: the reference's unblocked path) with S shifts each,
+ * in one launch per phase.  Packed column-major storage:
+ *   J_m, factors_m, Ht_m at sum_{l<m} n_l^2 (leading dimension n_m);
+ *   ipiv/perm/iperm/scale/iscale of matrix m at sum_{l<m} n_l;
+ *   shift s of matrix m: Gt at sum_{l<m} S (n_l+4) n_l + s (n_m+4) n_m (leading dimension
+ *   n_m+4), swap and rdiag at S sum_{l<m} n_l + s n_m, info/sigma/tau at m S + s;
+ *   right-hand side r of shift s of matrix m (lhl_solve_batched): column s R + r of the
+ *   n_m x (S R) block at S R sum_{l<m} n_l.
+ * Results per matrix are those of lhl_reduce (bit-identical) and lhl_shift. */
+typedef struct lhl_batch_s* lhl_batch_t;
+typedef struct {
+    int64_t count, shifts, total_n, total_nn, total_g;
+    double* factors;
+    double* Ht;
+    int64_t* ipiv;
+    int64_t* perm;
+    int64_t* iperm;
+    double* scale;
+    double* iscale;
+    double* Gt;
+    uint8_t* swap;
+    double* rdiag;
+    int32_t* info;
+    double* sigma;
+    double* tau;
+} lhl_batch_view;
+int lhl_batch_create(int64_t count, const int64_t* ns, int64_t shifts_per_matrix, lhl_batch_t* batch);
+int lhl_batch_destroy(lhl_batch_t batch);
+int lhl_batch_get_view(lhl_batch_t batch, lhl_batch_view* view);
+/* lhl_reduce!(ws_m, J_m, balance) for every m: one CTA per matrix (F:355-390, F:466-501). */
+int lhl_reduce_batched(lhl_batch_t batch, const double* dJ, int balance, void* stream);
+/* lhl_shift! of all count x S shifts (dsigma, dtau: count S values, matrix-major): one CTA per shift. */
+int lhl_shift_batched_all(lhl_batch_t batch, const double* dsigma, const double* dtau, void* stream);
+/* x = W^-1 b for every right-hand side (lhl_ldiv!, F:3052-3068), then lhl_refine! (F:3144-3157)
+ * with W = sigma I + tau J_m from the caller's dJ until ||b - W x|| / ||b|| <= tol or max_steps
+ * refinement steps: one CTA per right-hand side, everything on chip, one launch.  dres
+ * (count S R, optional) receives every final relative residual. */
+int lhl_solve_batched(lhl_batch_t batch, const double* dJ, const double* dB, double* dX, int64_t rhs_per_shift,
+                      double tol, int max_steps, double* dres, void* stream);
+
 /* ---- reduction without device allocation ------------------------------------------ */
 /* No counterpart in the reference (which allocates its workspace in Julia).  For callers
  * that cannot call cudaMalloc -- a host that owns a fixed device-memory budget, a Julia

@@ -38,6 +38,17 @@ struct lhl_shift_s {
     int32_t* info;
 };
 
+struct lhl_batch_s {
+    int64_t count, S, total_n, total_nn, total_g;
+    int64_t* ns_host;
+    int *d_n;
+    int64_t *d_off2, *d_off1, *d_offg;
+    double *F, *Ht, *scale, *iscale, *Gt, *rdiag, *sigma, *tau;
+    int64_t *ipiv, *perm, *iperm;
+    uint8_t* swap;
+    int32_t* info;
+};
+
 static int cuda_status(cudaError_t e) { return e == cudaSuccess ? LHL_OK : LHL_ERR_CUDA; }
 
 template <class T>
@@ -624,6 +635,168 @@ int lhl_residual_norms(lhl_shift_t sh, const double* dJ, int64_t ldj, const doub
     cudaError_t e = resid_any(sh, n, dJ, ldj, dB, ldb, dX, ldx, dR, ldx, nrhs, rhs_per_shift, st, nullptr, 0.0);
     if (e != cudaSuccess) return LHL_ERR_CUDA;
     return cuda_status(relres_any(sh, n, dR, ldx, dB, ldb, dres, nrhs, st));
+}
+
+
+// ---- batches of independent matrices of uneven order ----
+static lhl::BatchDesc batch_desc(lhl_batch_t b)
+{
+    lhl::BatchDesc d;
+    d.count = (int)b->count;
+    d.S = (int)b->S;
+    d.n = b->d_n;
+    d.off2 = b->d_off2;
+    d.off1 = b->d_off1;
+    d.offg = b->d_offg;
+    d.F = b->F;
+    d.Ht = b->Ht;
+    d.ipiv = b->ipiv;
+    d.perm = b->perm;
+    d.iperm = b->iperm;
+    d.scale = b->scale;
+    d.iscale = b->iscale;
+    d.Gt = b->Gt;
+    d.swap = b->swap;
+    d.rdiag = b->rdiag;
+    d.info = b->info;
+    return d;
+}
+
+int lhl_batch_destroy(lhl_batch_t b)
+{
+    if (!b) return LHL_ERR_ARG;
+    void* ptrs[] = {b->d_n, b->d_off2, b->d_off1, b->d_offg, b->F, b->Ht, b->scale, b->iscale, b->Gt, b->rdiag,
+                    b->sigma, b->tau, b->ipiv, b->perm, b->iperm, b->swap, b->info};
+    for (void* p : ptrs)
+        if (p) cudaFree(p);
+    free(b->ns_host);
+    delete b;
+    return LHL_OK;
+}
+
+int lhl_batch_create(int64_t count, const int64_t* ns, int64_t shifts_per_matrix, lhl_batch_t* out)
+{
+    if (!out || !ns) return LHL_ERR_ARG;
+    *out = nullptr;
+    if (count < 1 || shifts_per_matrix < 1 || count * shifts_per_matrix > (1ll << 30)) return LHL_ERR_DIM;
+    for (int64_t m = 0; m < count; ++m)
+        if (ns[m] < 1 || ns[m] > lhl::BATCH_NMAX) return LHL_ERR_DIM;
+    lhl_batch_t b = new (std::nothrow) lhl_batch_s();
+    if (!b) return LHL_ERR_ALLOC;
+    memset(b, 0, sizeof(*b));
+    b->count = count;
+    b->S = shifts_per_matrix;
+    b->ns_host = (int64_t*)malloc(count * sizeof(int64_t));
+    int* hn = (int*)malloc(count * sizeof(int));
+    int64_t* h2 = (int64_t*)malloc(count * sizeof(int64_t));
+    int64_t* h1 = (int64_t*)malloc(count * sizeof(int64_t));
+    int64_t* hg = (int64_t*)malloc(count * sizeof(int64_t));
+    if (!b->ns_host || !hn || !h2 || !h1 || !hg) {
+        free(hn); free(h2); free(h1); free(hg);
+        lhl_batch_destroy(b);
+        return LHL_ERR_ALLOC;
+    }
+    int64_t o2 = 0, o1 = 0, og = 0;
+    for (int64_t m = 0; m < count; ++m) {
+        const int64_t n = ns[m];
+        b->ns_host[m] = n;
+        hn[m] = (int)n;
+        h2[m] = o2;
+        h1[m] = o1;
+        hg[m] = og;
+        o2 += n * n;
+        o1 += n;
+        og += b->S * (n + 4) * n;
+    }
+    b->total_nn = o2;
+    b->total_n = o1;
+    b->total_g = og;
+    const int64_t S = b->S;
+    cudaError_t e = cudaSuccess;
+#define A_(p, cnt) if (e == cudaSuccess) e = dalloc(&b->p, (size_t)(cnt))
+    A_(d_n, count);
+    A_(d_off2, count);
+    A_(d_off1, count);
+    A_(d_offg, count);
+    A_(F, o2);
+    A_(Ht, o2);
+    A_(scale, o1);
+    A_(iscale, o1);
+    A_(ipiv, o1);
+    A_(perm, o1);
+    A_(iperm, o1);
+    A_(Gt, og);
+    A_(rdiag, S * o1);
+    A_(swap, S * o1);
+    A_(info, S * count);
+    A_(sigma, S * count);
+    A_(tau, S * count);
+#undef A_
+    if (e == cudaSuccess) e = cudaMemcpy(b->d_n, hn, count * sizeof(int), cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) e = cudaMemcpy(b->d_off2, h2, count * sizeof(int64_t), cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) e = cudaMemcpy(b->d_off1, h1, count * sizeof(int64_t), cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) e = cudaMemcpy(b->d_offg, hg, count * sizeof(int64_t), cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) e = cudaMemset(b->Gt, 0, (og ? og : 1) * sizeof(double));
+    free(hn); free(h2); free(h1); free(hg);
+    if (e != cudaSuccess) {
+        lhl_batch_destroy(b);
+        return e == cudaErrorMemoryAllocation ? LHL_ERR_ALLOC : LHL_ERR_CUDA;
+    }
+    *out = b;
+    return LHL_OK;
+}
+
+int lhl_batch_get_view(lhl_batch_t b, lhl_batch_view* v)
+{
+    if (!b || !v) return LHL_ERR_ARG;
+    v->count = b->count;
+    v->shifts = b->S;
+    v->total_n = b->total_n;
+    v->total_nn = b->total_nn;
+    v->total_g = b->total_g;
+    v->factors = b->F;
+    v->Ht = b->Ht;
+    v->ipiv = b->ipiv;
+    v->perm = b->perm;
+    v->iperm = b->iperm;
+    v->scale = b->scale;
+    v->iscale = b->iscale;
+    v->Gt = b->Gt;
+    v->swap = b->swap;
+    v->rdiag = b->rdiag;
+    v->info = b->info;
+    v->sigma = b->sigma;
+    v->tau = b->tau;
+    return LHL_OK;
+}
+
+int lhl_reduce_batched(lhl_batch_t b, const double* dJ, int balance, void* stream)
+{
+    if (!b || !dJ) return LHL_ERR_ARG;
+    return cuda_status(lhl::launch_reduce_batch(batch_desc(b), dJ, balance ? 1 : 0, (cudaStream_t)stream));
+}
+
+int lhl_shift_batched_all(lhl_batch_t b, const double* dsigma, const double* dtau, void* stream)
+{
+    if (!b || !dsigma || !dtau) return LHL_ERR_ARG;
+    cudaStream_t st = (cudaStream_t)stream;
+    const size_t cnt = (size_t)b->S * b->count;
+    cudaError_t e = cudaSuccess;
+    if (dsigma != b->sigma) e = cudaMemcpyAsync(b->sigma, dsigma, cnt * sizeof(double), cudaMemcpyDeviceToDevice, st);
+    if (e == cudaSuccess && dtau != b->tau)
+        e = cudaMemcpyAsync(b->tau, dtau, cnt * sizeof(double), cudaMemcpyDeviceToDevice, st);
+    if (e == cudaSuccess) e = lhl::launch_shift_lu_batch(batch_desc(b), b->sigma, b->tau, st);
+    return cuda_status(e);
+}
+
+int lhl_solve_batched(lhl_batch_t b, const double* dJ, const double* dB, double* dX, int64_t rhs_per_shift, double tol,
+                      int max_steps, double* dres, void* stream)
+{
+    if (!b || !dJ || !dB || !dX) return LHL_ERR_ARG;
+    if (rhs_per_shift < 1 || max_steps < 0 || !(tol >= 0.0)) return LHL_ERR_ARG;
+    if (b->count * b->S * rhs_per_shift > (1ll << 31) - 1) return LHL_ERR_DIM;
+    return cuda_status(lhl::launch_solve_batch(batch_desc(b), dJ, dB, dX, (int)rhs_per_shift, b->sigma, b->tau, tol,
+                                               max_steps, dres, (cudaStream_t)stream));
 }
 
 }  // extern "C"

@@ -65,6 +65,28 @@ struct LdivArgs {
     unsigned long long limit_ns;
 };
 
+// Many independent matrices of uneven order (lhl_reduce_batched, batch.cu): matrix m has order
+// n[m] <= 512 and S shifts; its arrays start at the prefix offsets below.
+struct BatchDesc {
+    int count, S;
+    const int* n;
+    const int64_t* off2;  // sum of n^2 over earlier matrices: J, factors, Ht
+    const int64_t* off1;  // sum of n: ipiv, perm, iperm, scale, iscale; x S for swap, rdiag
+    const int64_t* offg;  // sum of S (n + 4) n: Gt
+    double* F;
+    double* Ht;
+    int64_t* ipiv;
+    int64_t* perm;
+    int64_t* iperm;
+    double* scale;
+    double* iscale;
+    double* Gt;
+    uint8_t* swap;
+    double* rdiag;
+    int32_t* info;
+};
+constexpr int BATCH_NMAX = 499;  // the reference reduces n < 500 unblocked (F:398-402)
+
 // One L sweep over a tile of right-hand sides (see solve.cu).
 struct ZArgs {
     int n;
@@ -130,6 +152,12 @@ cudaError_t launch_shift_lu(int n, const double* Ht, int ldh, const double* sig,
 
 cudaError_t launch_ldiv(const LdivArgs& a, int nrhs, cudaStream_t st);
 cudaError_t launch_linv(int n, const double* F, int ldf, double* linv, cudaStream_t st);
+// batches of independent matrices (batch.cu, shift.cu, solve.cu)
+cudaError_t launch_reduce_batch(const BatchDesc& d, const double* J, int balance, cudaStream_t st);
+cudaError_t launch_shift_lu_batch(const BatchDesc& d, const double* sig, const double* tau, cudaStream_t st);
+cudaError_t launch_solve_batch(const BatchDesc& d, const double* J, const double* B, double* X, int R,
+                               const double* sig, const double* tau, double tol, int max_steps, double* res,
+                               cudaStream_t st);
 // complex shifts on a real reduction (complex.cu)
 cudaError_t launch_shift_lu_cplx(int n, const double* Ht, int ldh, const double* sig, const double* tau, int s0,
                                  int count, double* Gt, int ldg, int po, uint8_t* swp, double* rd, int32_t* info,

@@ -10,23 +10,16 @@
 // steps before they are used (D = 4 up to n = 2048), into a register ring indexed at
 // compile time, so that a step does not wait for its loads.  Every operation is the reference's, in its order, with no fused
 // multiply-add, so Gt, swap, rdiag and info are bit-identical to the reference.
-#include "common.cuh"
+#include "internal.cuh"
 
 namespace lhl {
 
+// The elimination of one shift; every thread of the CTA calls it (T threads).
 template <int T, int E, int D>
-__global__ void __launch_bounds__(T) shift_lu_kernel(int n, const double* __restrict__ Ht, int ldh,
-                                                     const double* __restrict__ sig, const double* __restrict__ tau_,
-                                                     int s0, double* __restrict__ Gt_all, int ldg,
-                                                     uint8_t* __restrict__ swap_all, double* __restrict__ rdiag_all,
-                                                     int32_t* __restrict__ info_all)
+__device__ __forceinline__ void shift_lu_body(int n, const double* __restrict__ Ht, int ldh, double sigma, double tau,
+                                              double* __restrict__ Gt, int ldg, uint8_t* __restrict__ swp,
+                                              double* __restrict__ rdiag, int32_t* __restrict__ info_out)
 {
-    const int s = s0 + blockIdx.x;
-    const double sigma = sig[blockIdx.x];
-    const double tau = tau_[blockIdx.x];
-    double* Gt = Gt_all + (size_t)s * ldg * n;
-    uint8_t* swp = swap_all + (size_t)s * n;
-    double* rdiag = rdiag_all + (size_t)s * n;
     const int t = threadIdx.x;
 
     __shared__ double s_next[2];  // r[k+1] after step k, double-buffered by step parity
@@ -138,10 +131,43 @@ __global__ void __launch_bounds__(T) shift_lu_kernel(int n, const double* __rest
         swp[n - 1] = 0;
         int info = s_info;
         if (rn == 0.0 && info == 0) info = n;
-        info_all[s] = info;
+        *info_out = info;
     }
     __syncthreads();
     for (int j = 1 + t; j <= n; j += T) rdiag[j - 1] = 1.0 / M1(Gt, ldg, j, j);
+}
+
+template <int T, int E, int D>
+__global__ void __launch_bounds__(T) shift_lu_kernel(int n, const double* __restrict__ Ht, int ldh,
+                                                     const double* __restrict__ sig, const double* __restrict__ tau_,
+                                                     int s0, double* __restrict__ Gt_all, int ldg,
+                                                     uint8_t* __restrict__ swap_all, double* __restrict__ rdiag_all,
+                                                     int32_t* __restrict__ info_all)
+{
+    const int s = s0 + blockIdx.x;
+    shift_lu_body<T, E, D>(n, Ht, ldh, sig[blockIdx.x], tau_[blockIdx.x], Gt_all + (size_t)s * ldg * n, ldg,
+                           swap_all + (size_t)s * n, rdiag_all + (size_t)s * n, info_all + s);
+}
+
+// Many independent matrices (lhl_shift_batched_all): CTA b takes shift b % S of matrix b / S;
+// the matrix's order and offsets come from the batch descriptor.
+__global__ void __launch_bounds__(256) shift_lu_batch_kernel(BatchDesc d, const double* __restrict__ sig,
+                                                             const double* __restrict__ tau)
+{
+    const int m = blockIdx.x / d.S, s = blockIdx.x - m * d.S;
+    const int n = d.n[m];
+    if (n <= 0) return;
+    const size_t ms = (size_t)m * d.S + s;
+    shift_lu_body<256, 2, 2>(n, d.Ht + d.off2[m], n, sig[ms], tau[ms], d.Gt + d.offg[m] + (size_t)s * (n + 4) * n,
+                             n + 4, d.swap + d.S * d.off1[m] + (size_t)s * n, d.rdiag + d.S * d.off1[m] + (size_t)s * n,
+                             d.info + ms);
+}
+
+cudaError_t launch_shift_lu_batch(const BatchDesc& d, const double* sig, const double* tau, cudaStream_t st)
+{
+    if (d.count <= 0 || d.S <= 0) return cudaSuccess;
+    shift_lu_batch_kernel<<<d.count * d.S, 256, 0, st>>>(d, sig, tau);
+    return cudaGetLastError();
 }
 
 template <int T, int E, int D>

@@ -634,6 +634,149 @@ __global__ void __launch_bounds__(HT) hess_tma_kernel(LdivArgs a, double* Y, int
     for (int i = t; i < n; i += HCONS * 32) Y[(size_t)blockIdx.x * ldy + i] = y[i];
 }
 
+// ---- batches of small independent matrices: one CTA per (matrix, shift, right-hand side),
+// the solve and its refinement entirely on chip (lhl_solve_batched) ----
+// y <- L^-1 y, blocked by 32: the block's triangle staged in shared memory and solved by one
+// warp with shuffles, then every thread applies the block to its rows.
+__device__ void small_lsolve(int n, const double* __restrict__ F, double* y)
+{
+    __shared__ double tri[BS][BS + 1];
+    const int t = threadIdx.x, lane = t & 31, warp = t >> 5;
+    for (int c0 = 2; c0 <= n - 1; c0 += BS) {
+        const int cb = min(c0 + BS - 1, n - 1), bw = cb - c0 + 1;
+        for (int e = t; e < BS * BS; e += SOLVE_T) {
+            const int r = e & 31, q = e >> 5;  // L[c0 + r, c0 + q] = F[c0 + r, c0 + q - 1]
+            if (q < bw && r < bw && r > q) tri[r][q] = M1(F, n, c0 + r, c0 + q - 1);
+        }
+        __syncthreads();
+        if (warp == 0) {
+            double yr = lane < bw ? y[c0 + lane - 1] : 0.0;
+            for (int q = 0; q < bw - 1; ++q) {
+                const double xq = __shfl_sync(0xffffffffu, yr, q);
+                if (lane > q && lane < bw) yr = dfma(-tri[lane][q], xq, yr);
+            }
+            if (lane < bw) y[c0 + lane - 1] = yr;
+        }
+        __syncthreads();
+        for (int i = cb + 1 + t; i <= n; i += SOLVE_T) {
+            double v = y[i - 1];
+            for (int q = 0; q < bw; ++q) v = dfma(-M1(F, n, i, c0 + q - 1), y[c0 + q - 1], v);
+            y[i - 1] = v;
+        }
+        __syncthreads();
+    }
+}
+
+// y <- L y (original y on the right): (L y)[i] = y[i] + sum_{c=2}^{i-1} L[i,c] y[c]
+__device__ void small_lmul(int n, const double* __restrict__ F, double* y, double* y2)
+{
+    const int t = threadIdx.x;
+    for (int i = 1 + t; i <= n; i += SOLVE_T) {
+        double v = y[i - 1];
+        for (int c = 2; c <= i - 1; ++c) v = dfma(M1(F, n, i, c - 1), y[c - 1], v);
+        y2[i - 1] = v;
+    }
+    __syncthreads();
+    for (int i = t; i < n; i += SOLVE_T) y[i] = y2[i];
+    __syncthreads();
+}
+
+__device__ double block_sum(double v, double* red)
+{
+    const int t = threadIdx.x;
+    v = warp_sum(v);
+    __syncthreads();
+    if ((t & 31) == 0) red[t >> 5] = v;
+    __syncthreads();
+    double s = 0.0;
+    for (int w = 0; w < SOLVE_T / 32; ++w) s += red[w];
+    return s;
+}
+
+__global__ void __launch_bounds__(SOLVE_T) solve_batch_kernel(BatchDesc d, const double* __restrict__ J,
+                                                              const double* __restrict__ B, double* __restrict__ X,
+                                                              int R, const double* __restrict__ sig,
+                                                              const double* __restrict__ tau, double tol,
+                                                              int max_steps, double* __restrict__ res)
+{
+    const int SR = d.S * R;
+    const int m = blockIdx.x / SR, q = blockIdx.x - m * SR, s = q / R;
+    const int n = d.n[m];
+    if (n <= 0) return;
+    __shared__ double xs[512], rs[512], ys[512], ys2[512];
+    __shared__ uint8_t ssw[512];
+    __shared__ double red[SOLVE_T / 32];
+    const int t = threadIdx.x;
+    const double* Jm = J + d.off2[m];
+    const double* F = d.F + d.off2[m];
+    const int64_t* perm = d.perm + d.off1[m];
+    const int64_t* iperm = d.iperm + d.off1[m];
+    const double* sc = d.scale + d.off1[m];
+    const double* isc = d.iscale + d.off1[m];
+    const int ldg = n + 4;
+    const double* Gt = d.Gt + d.offg[m] + (size_t)s * ldg * n;
+    const uint8_t* swp = d.swap + (size_t)d.S * d.off1[m] + (size_t)s * n;
+    const double* rd = d.rdiag + (size_t)d.S * d.off1[m] + (size_t)s * n;
+    const double sigma = sig[(size_t)m * d.S + s], tauv = tau[(size_t)m * d.S + s];
+    const double* b = B + (size_t)SR * d.off1[m] + (size_t)q * n;
+    double* x = X + (size_t)SR * d.off1[m] + (size_t)q * n;
+    LdivArgs la;
+    la.n = n;
+    la.ldg = ldg;
+    // v <- W^-1 v in place (F:3052-3068)
+    auto solve = [&](double* v) {
+        for (int i = t; i < n; i += SOLVE_T) {
+            const int64_t p = perm[i];
+            ys[i] = v[p - 1] * isc[p - 1];
+        }
+        __syncthreads();
+        small_lsolve(n, F, ys);
+        hess_solve(la, Gt, swp, rd, ys, ys2, ssw);
+        small_lmul(n, F, ys, ys2);
+        for (int i = t; i < n; i += SOLVE_T) v[i] = ys[iperm[i] - 1] * sc[i];
+        __syncthreads();
+    };
+    double bb = 0.0;
+    for (int i = t; i < n; i += SOLVE_T) {
+        const double v = b[i];
+        xs[i] = v;
+        bb = dfma(v, v, bb);
+    }
+    const double bnorm = sqrt(block_sum(bb, red));
+    __syncthreads();
+    solve(xs);  // x = W^-1 b
+    double rel = 0.0;
+    for (int it = 0; it <= max_steps; ++it) {
+        // r = b - (sigma x + tau J x), FP64 with the caller's J
+        double rr = 0.0;
+        for (int i = t; i < n; i += SOLVE_T) {
+            double acc = 0.0;
+            for (int j = 0; j < n; ++j) acc = dfma(Jm[(size_t)j * n + i], xs[j], acc);
+            const double r = b[i] - (sigma * xs[i] + tauv * acc);
+            rs[i] = r;
+            rr = dfma(r, r, rr);
+        }
+        const double rn = sqrt(block_sum(rr, red));
+        rel = bnorm > 0.0 ? rn / bnorm : rn;
+        if (rel <= tol || it == max_steps) break;
+        __syncthreads();
+        solve(rs);
+        for (int i = t; i < n; i += SOLVE_T) xs[i] += rs[i];
+        __syncthreads();
+    }
+    for (int i = t; i < n; i += SOLVE_T) x[i] = xs[i];
+    if (t == 0 && res) res[blockIdx.x] = rel;
+}
+
+cudaError_t launch_solve_batch(const BatchDesc& d, const double* J, const double* B, double* X, int R,
+                               const double* sig, const double* tau, double tol, int max_steps, double* res,
+                               cudaStream_t st)
+{
+    if (d.count <= 0 || d.S <= 0 || R <= 0) return cudaSuccess;
+    solve_batch_kernel<<<d.count * d.S * R, SOLVE_T, 0, st>>>(d, J, B, X, R, sig, tau, tol, max_steps, res);
+    return cudaGetLastError();
+}
+
 static cudaError_t run_zinv(ZArgs z, cudaStream_t st)
 {
     const int nblk = (z.n + ZR - 1) / ZR, ntile = (z.m + ZC - 1) / ZC;

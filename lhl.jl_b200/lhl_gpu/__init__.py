@@ -24,6 +24,7 @@ from __future__ import annotations
 import ctypes as C
 import os
 
+import numpy as np
 import torch
 
 _HERE = os.path.dirname(os.path.abspath(__file__))
@@ -76,6 +77,12 @@ def _load():
         "lhl_shift_batched": [vp, vp, i64, i64, vp, vp, vp],
         "lhl_shift": [vp, vp, i64, d, d, vp],
         "lhl_shift_create_complex": [i64, i64, C.POINTER(vp)],
+        "lhl_batch_create": [i64, vp, i64, C.POINTER(vp)],
+        "lhl_batch_destroy": [vp],
+        "lhl_batch_get_view": [vp, vp],
+        "lhl_reduce_batched": [vp, vp, i32, vp],
+        "lhl_shift_batched_all": [vp, vp, vp, vp],
+        "lhl_solve_batched": [vp, vp, vp, vp, i64, d, i32, vp, vp],
         "lhl_shift_complex": [vp, vp, i64, d, d, d, d, vp],
         "lhl_shift_batched_complex": [vp, vp, i64, i64, vp, vp, vp],
         "lhl_ldiv": [vp, vp, vp, i64, i64, i64, vp],
@@ -117,6 +124,14 @@ def _check(rc, what=""):
 def _stream(stream=None):
     s = stream if stream is not None else torch.cuda.current_stream()
     return C.c_void_p(s.cuda_stream)
+
+
+class _BatchView(C.Structure):
+    _fields_ = [("count", C.c_int64), ("shifts", C.c_int64), ("total_n", C.c_int64), ("total_nn", C.c_int64),
+                ("total_g", C.c_int64), ("factors", C.c_void_p), ("Ht", C.c_void_p), ("ipiv", C.c_void_p),
+                ("perm", C.c_void_p), ("iperm", C.c_void_p), ("scale", C.c_void_p), ("iscale", C.c_void_p),
+                ("Gt", C.c_void_p), ("swap", C.c_void_p), ("rdiag", C.c_void_p), ("info", C.c_void_p),
+                ("sigma", C.c_void_p), ("tau", C.c_void_p)]
 
 
 class _DevArray:
@@ -542,11 +557,129 @@ def applyZinv_(x: torch.Tensor, ws: LHLWorkspace, stream=None) -> torch.Tensor:
     return x
 
 
+class LHLBatch:
+    """Many independent real matrices of uneven order (n <= 512) with ``shifts`` shifts each:
+    the batched form of ``lhl``, ``lhl_shift!``, ``lhl_ldiv!`` and ``lhl_refine!`` (one launch
+    per phase; see lhl_batch_create in include/lhl_gpu.h for the packed layout)."""
+
+    def __init__(self, ns, shifts: int):
+        self.ns = np.asarray(ns, dtype=np.int64)
+        self.count = int(self.ns.size)
+        self.S = int(shifts)
+        self._h = C.c_void_p()
+        nsc = np.ascontiguousarray(self.ns)
+        _check(_lib.lhl_batch_create(self.count, C.c_void_p(nsc.ctypes.data), self.S, C.byref(self._h)), "LHLBatch")
+        v = _BatchView()
+        _check(_lib.lhl_batch_get_view(self._h, C.byref(v)))
+        self._v = v
+        self.off2 = np.concatenate([[0], np.cumsum(self.ns * self.ns)])
+        self.off1 = np.concatenate([[0], np.cumsum(self.ns)])
+        self.offg = np.concatenate([[0], np.cumsum(self.S * (self.ns + 4) * self.ns)])
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        if h is not None and h.value and _lib is not None:
+            _lib.lhl_batch_destroy(h)
+            self._h = None
+
+    # packing of host data
+    def pack_matrices(self, mats) -> np.ndarray:
+        return np.concatenate([np.asarray(A, dtype=np.float64).ravel(order="F") for A in mats])
+
+    def pack_rhs(self, blocks) -> np.ndarray:
+        """blocks[m]: n_m x (S R), column s R + r is right-hand side r of shift s."""
+        return np.concatenate([np.asarray(X, dtype=np.float64).ravel(order="F") for X in blocks])
+
+    def unpack_rhs(self, packed, R: int):
+        out = []
+        o = 0
+        for n in self.ns:
+            k = int(n) * self.S * R
+            out.append(np.asarray(packed[o:o + k]).reshape((self.S * R, int(n))).T)
+            o += k
+        return out
+
+    # device views of matrix m (and shift s)
+    def factors(self, m: int) -> torch.Tensor:
+        n = int(self.ns[m])
+        return _view(self._v.factors + 8 * int(self.off2[m]), (n, n), strides=(8, 8 * n))
+
+    def Ht(self, m: int) -> torch.Tensor:
+        n = int(self.ns[m])
+        return _view(self._v.Ht + 8 * int(self.off2[m]), (n, n), strides=(8, 8 * n))
+
+    def ipiv(self, m: int) -> torch.Tensor:
+        n = int(self.ns[m])
+        return _view(self._v.ipiv + 8 * int(self.off1[m]), (max(n - 2, 0),), "<i8")
+
+    def scale(self, m: int) -> torch.Tensor:
+        return _view(self._v.scale + 8 * int(self.off1[m]), (int(self.ns[m]),))
+
+    def perm(self, m: int) -> torch.Tensor:
+        return _view(self._v.perm + 8 * int(self.off1[m]), (int(self.ns[m]),), "<i8")
+
+    def Gt(self, m: int, s: int) -> torch.Tensor:
+        n = int(self.ns[m])
+        base = self._v.Gt + 8 * (int(self.offg[m]) + s * (n + 4) * n)
+        return _view(base, (n + 4, n), strides=(8, 8 * (n + 4)))
+
+    def rdiag(self, m: int, s: int) -> torch.Tensor:
+        n = int(self.ns[m])
+        return _view(self._v.rdiag + 8 * (self.S * int(self.off1[m]) + s * n), (n,))
+
+    def swap(self, m: int, s: int) -> torch.Tensor:
+        n = int(self.ns[m])
+        return _view(self._v.swap + (self.S * int(self.off1[m]) + s * n), (n,), "|u1")
+
+    @property
+    def info(self) -> torch.Tensor:
+        return _view(self._v.info, (self.count * self.S,), "<i4")
+
+
+def lhl_reduce_batched_(b: LHLBatch, J: torch.Tensor, balance: bool = True, stream=None) -> LHLBatch:
+    """lhl_reduce! of every matrix of the batch (J: packed, see LHLBatch.pack_matrices)."""
+    _require_cuda_f64(J, "J")
+    if J.numel() != int(b.off2[-1]):
+        raise DimensionMismatch("packed J has the wrong length")
+    _check(_lib.lhl_reduce_batched(b._h, C.c_void_p(J.data_ptr()), int(bool(balance)), _stream(stream)),
+           "lhl_reduce_batched")
+    return b
+
+
+def lhl_shift_batched_all_(b: LHLBatch, sigmas: torch.Tensor, taus: torch.Tensor, stream=None) -> LHLBatch:
+    """lhl_shift! of every (matrix, shift): sigmas, taus have count x S entries, matrix-major."""
+    for t, nm in ((sigmas, "sigmas"), (taus, "taus")):
+        _require_cuda_f64(t, nm)
+        if t.numel() != b.count * b.S:
+            raise DimensionMismatch(f"{nm} must have count x shifts entries")
+    sigmas, taus = sigmas.contiguous(), taus.contiguous()
+    _check(_lib.lhl_shift_batched_all(b._h, C.c_void_p(sigmas.data_ptr()), C.c_void_p(taus.data_ptr()),
+                                      _stream(stream)), "lhl_shift_batched_all")
+    return b
+
+
+def lhl_solve_batched_(b: LHLBatch, J: torch.Tensor, B: torch.Tensor, X: torch.Tensor, rhs_per_shift: int,
+                       tol: float = 1e-10, max_steps: int = 8, res: torch.Tensor = None, stream=None) -> torch.Tensor:
+    """Every right-hand side solved and refined to `tol` on chip (lhl_solve_batched); returns
+    the final relative residuals (count x S x R)."""
+    for t, nm in ((J, "J"), (B, "B"), (X, "X")):
+        _require_cuda_f64(t, nm)
+    k = b.count * b.S * int(rhs_per_shift)
+    if B.numel() != int(b.off1[-1]) * b.S * int(rhs_per_shift) or X.numel() != B.numel():
+        raise DimensionMismatch("packed B / X have the wrong length")
+    if res is None:
+        res = torch.empty(k, dtype=torch.float64, device=B.device)
+    _check(_lib.lhl_solve_batched(b._h, C.c_void_p(J.data_ptr()), C.c_void_p(B.data_ptr()),
+                                  C.c_void_p(X.data_ptr()), int(rhs_per_shift), float(tol), int(max_steps),
+                                  C.c_void_p(res.data_ptr()), _stream(stream)), "lhl_solve_batched")
+    return res
+
+
 def version() -> str:
     return _lib.lhl_version().decode()
 
 
 __all__ = ["LHLWorkspace", "LHLShift", "lhl", "lhl_", "lhl_reduce_", "lhl_shift_", "lhl_shift_batched_",
-           "lhl_refine_tol_",
+           "lhl_refine_tol_", "LHLBatch", "lhl_reduce_batched_", "lhl_shift_batched_all_", "lhl_solve_batched_",
            "lhl_ldiv_", "lhl_refine_", "applyZ_", "applyZinv_", "residual_norms", "ArgumentError",
            "DimensionMismatch", "LHLDeviceError", "LHL_PREC_FP64", "LHL_PREC_MIXED", "version", "lib"]
