@@ -173,6 +173,7 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--cpu-baseline-steps", type=int, default=1)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-c4", action="store_true", help="skip the batched config-4 measurement")
     args = ap.parse_args()
     world, rank, local = dist_setup(args.gpus)
 
@@ -317,6 +318,43 @@ def main():
     h2d = Jh.numel() * 8 + Bh.numel() * 8 + sh_h.numel() * 8
     d2h = Xh.numel() * 8
 
+    # ---- config 4: 4096 independent Jacobians of uneven order, batched (FP64) ----
+    c4 = None
+    if not args.no_c4:
+        cfg4 = configs.config4()
+        ns4 = [int(v) for v in cfg4["ns"]]
+        S4, R4 = 8, 4
+        bt = G.LHLBatch(ns4, S4)
+        J4 = torch.as_tensor(bt.pack_matrices(cfg4["mats"])).to(dev)
+        B4 = torch.as_tensor(bt.pack_rhs([X[:, :S4 * R4] for X in cfg4["rhs"]])).to(dev)
+        X4 = torch.empty_like(B4)
+        sg4 = torch.as_tensor(cfg4["sigma"].ravel()).to(dev)
+        ta4 = torch.as_tensor(cfg4["tau"].ravel()).to(dev)
+        res4 = torch.empty(len(ns4) * S4 * R4, dtype=torch.float64, device=dev)
+
+        def c4_step():
+            G.lhl_reduce_batched_(bt, J4, True)
+            G.lhl_shift_batched_all_(bt, sg4, ta4)
+            G.lhl_solve_batched_(bt, J4, B4, X4, R4, tol=TOL, max_steps=6, res=res4)
+
+        for _ in range(3):
+            c4_step()
+        torch.cuda.synchronize()
+        c4_ms = time_events(stream, c4_step, max(3, min(args.steps, 5)), flush)
+        r4 = res4.cpu().numpy()
+        assert (r4 <= TOL).all(), f"config 4 residual above {TOL}: {r4.max()}"
+        c4 = {"workload": "c4: 4096 J, n uniform [16,256], N(0,1) - 5I; 8 shifts (1,-g) g log-uniform "
+                          "[1e-3,1e-1]; 4 RHS/shift; reduction + shift LUs + solves refined to 1e-10, "
+                          "three launches, FP64 (plain form)",
+              "value": len(ns4) * S4 * R4 / (c4_ms * 1e-3), "unit": UNIT, "ms_per_step": c4_ms,
+              "phases_ms": {"reduce_batched": time_events(stream, lambda: G.lhl_reduce_batched_(bt, J4, True), 3,
+                                                          flush),
+                            "shift_batched_all": time_events(stream, lambda: G.lhl_shift_batched_all_(bt, sg4, ta4),
+                                                             3, flush),
+                            "solve_batched": time_events(stream, lambda: G.lhl_solve_batched_(
+                                bt, J4, B4, X4, R4, tol=TOL, max_steps=6, res=res4), 3, flush)},
+              "max_rel_residual": float(r4.max())}
+
     # ---- max over ranks ----
     vals = torch.tensor([ms_mixed, ms_plain, e2e_ms], dtype=torch.float64, device=dev)
     if pg:
@@ -355,6 +393,7 @@ def main():
                 "cpu_baseline": cpu,
                 "e2e": {"value": world * S / (e2e_ms * 1e-3), "unit": UNIT, "h2d_bytes_per_step": h2d,
                         "d2h_bytes_per_step": d2h, "ms_per_step": e2e_ms},
+                "batched_c4": c4,
                 "gpu_launches": mixed.launches() * args.steps,
                 "clocks": clk_mixed}
         print(json.dumps(line), flush=True)
