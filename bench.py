@@ -128,9 +128,11 @@ def time_events(stream, fn, reps, flush):
 
 
 class Form:
-    """One form of the path on the device: the workspace, the shift batch and one step."""
+    """One form of the path on the device: the workspace, the shift batch and one step.
+    refine = ("fixed", max_steps): lhl_refine_tol; ("gmres", max_cycles, restart): lhl_refine_gmres
+    with the host stopping once every column is at the tolerance."""
 
-    def __init__(self, G, torch, precision, n, S, dev, max_steps):
+    def __init__(self, G, torch, precision, n, S, dev, refine):
         self.G, self.torch = G, torch
         self.precision = precision
         self.ws = G.LHLWorkspace(n, precision)
@@ -138,7 +140,7 @@ class Form:
         self.X = torch.empty((S, n), dtype=torch.float64, device=dev).t()
         self.Rs = torch.empty((S, n), dtype=torch.float64, device=dev)
         self.res = torch.empty(S, dtype=torch.float64, device=dev)
-        self.max_steps = max_steps
+        self.refine = refine
 
     def reduce(self, Jd):
         self.G.lhl_reduce_(self.ws, Jd, True)
@@ -148,21 +150,38 @@ class Form:
         G.lhl_shift_batched_(self.sh, self.ws, sig, tau)
         self.X.copy_(Bd)
         G.lhl_ldiv_(self.X, self.sh, self.ws)
-        G.lhl_refine_tol_(self.X, Jd, Bd, self.sh, self.ws, tol=TOL, max_steps=self.max_steps, R=self.Rs,
-                          res=self.res)
+        if self.refine[0] == "gmres":
+            G.lhl_refine_gmres_(self.X, Jd, Bd, self.sh, self.ws, tol=TOL, max_cycles=self.refine[1],
+                                restart=self.refine[2], host_check=True, R=self.Rs, res=self.res)
+        else:
+            G.lhl_refine_tol_(self.X, Jd, Bd, self.sh, self.ws, tol=TOL, max_steps=self.refine[1], R=self.Rs,
+                              res=self.res)
 
     def step(self, Jd, Bd, sig, tau):
         self.reduce(Jd)
         self.chain(Jd, Bd, sig, tau)
 
-    def launches(self):
-        red = 5 if self.precision == self.G.LHL_PREC_MIXED else 4   # init, [balance,] coop, Ht, perm
-        return red + 1 + 1 + 4 * self.max_steps + 2                 # shift LU, ldiv, refinement steps, final check
+
+def count_launches(torch, fn):
+    """Kernels of this library launched by one call of fn, counted from the CUDA activity
+    trace of an untimed run (torch.profiler); None where the trace is unavailable."""
+    try:
+        from torch.profiler import ProfilerActivity, profile
+        torch.cuda.synchronize()
+        with profile(activities=[ProfilerActivity.CUDA]) as prof:
+            fn()
+            torch.cuda.synchronize()
+        names = [e.name for e in prof.events() if e.device_type == torch.autograd.DeviceType.CUDA]
+        ours = [nm for nm in names if "lhl::" in nm]
+        return len(ours) if ours else None
+    except Exception:  # pragma: no cover - profiler missing on the box
+        return None
 
 
 TOL = 1e-10
-MIXED_MAX_STEPS = 16
-PLAIN_MAX_STEPS = 2
+MIXED_REFINE = ("gmres", 4, 3)   # GMRES(3), at most 4 cycles
+PLAIN_REFINE = ("fixed", 2)
+FIXED_POINT_REPLAY_STEPS = 16
 
 
 def main():
@@ -225,8 +244,8 @@ def main():
     sig = torch.as_tensor(cfg["sigma"]).to(dev)
     tau = torch.as_tensor(cfg["tau"]).to(dev)
     flush = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.float32, device=dev)
-    mixed = Form(G, torch, G.LHL_PREC_MIXED, n, S, dev, MIXED_MAX_STEPS)
-    plain = Form(G, torch, G.LHL_PREC_FP64, n, S, dev, PLAIN_MAX_STEPS)
+    mixed = Form(G, torch, G.LHL_PREC_MIXED, n, S, dev, MIXED_REFINE)
+    plain = Form(G, torch, G.LHL_PREC_FP64, n, S, dev, PLAIN_REFINE)
 
     def timed(form):
         for _ in range(max(args.warmup, 3)):
@@ -266,17 +285,32 @@ def main():
 
     ph_mixed = phases(mixed)
     ph_plain = phases(plain)
-    # refinement steps the mixed form needed (per column), from a fixed-step replay on the host side
+    # what the mixed form's refinement needed: fixed-point steps per column (a replay of
+    # lhl_refine_tol with growing step counts) against GMRES-IR cycles
     G.lhl_shift_batched_(mixed.sh, mixed.ws, sig, tau)
     X0 = Bd.clone()
     G.lhl_ldiv_(X0, mixed.sh, mixed.ws)
     need = np.full(S, -1)
-    for st in range(MIXED_MAX_STEPS + 1):
+    for st in range(FIXED_POINT_REPLAY_STEPS + 1):
         Xs = X0.clone()
         r = G.lhl_refine_tol_(Xs, Jd, Bd, mixed.sh, mixed.ws, tol=0.0, max_steps=st).cpu().numpy()
         need[(need < 0) & (r <= TOL)] = st
         if (need >= 0).all():
             break
+    gm_cycles = None
+    for cyc in range(1, MIXED_REFINE[1] + 1):
+        Xs = X0.clone()
+        r = G.lhl_refine_gmres_(Xs, Jd, Bd, mixed.sh, mixed.ws, tol=TOL, max_cycles=cyc,
+                                restart=MIXED_REFINE[2]).cpu().numpy()
+        if (r <= TOL).all():
+            gm_cycles = cyc
+            break
+    fixed_chain_ms = time_events(stream, lambda: (G.lhl_shift_batched_(mixed.sh, mixed.ws, sig, tau),
+                                                  mixed.X.copy_(Bd), G.lhl_ldiv_(mixed.X, mixed.sh, mixed.ws),
+                                                  G.lhl_refine_tol_(mixed.X, Jd, Bd, mixed.sh, mixed.ws, tol=TOL,
+                                                                    max_steps=FIXED_POINT_REPLAY_STEPS, R=mixed.Rs,
+                                                                    res=mixed.res)), 3, flush)
+    launches = count_launches(torch, lambda: mixed.step(Jd, Bd, sig, tau))
 
     # ---- roofline of the dominant kernel: the mixed reduction ----
     alg_bytes = 4.0 * (n ** 3) / 3.0 + 16.0 * n * n   # FP32 GEMV stream (4 n^3/3) + J in, factors out (FP64)
@@ -384,8 +418,13 @@ def main():
                 "excluding_reduction": {"mixed": S / (ph_mixed["chain"] * 1e-3), "plain": S / (ph_plain["chain"] * 1e-3),
                                         "unit": UNIT, "note": "S*R / T(shift + solve + refine), reduction excluded"},
                 "phases_ms": ph_mixed, "max_rel_residual": res_mixed,
-                "refine_steps_needed": {"max": int(need.max()), "mean": float(need.mean()),
-                                        "histogram": {int(k): int((need == k).sum()) for k in np.unique(need)}},
+                "refinement": {"method": f"GMRES-IR: GMRES({MIXED_REFINE[2]}) cycles left-preconditioned by the "
+                                         f"shift's factorisation, host check per cycle",
+                               "gmres_cycles_needed": gm_cycles,
+                               "fixed_point_steps_needed": {
+                                   "max": int(need.max()), "mean": float(need.mean()),
+                                   "histogram": {int(k): int((need == k).sum()) for k in np.unique(need)}},
+                               "chain_ms_with_fixed_point": fixed_chain_ms},
                 "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                              "frac": achieved / peak, "traffic": traffic, "peak_kind": peak_kind,
                              "kernel": "lhl_reduce, mixed form (balance + FP32 ELMHES, cooperative launches)",
@@ -394,7 +433,7 @@ def main():
                 "e2e": {"value": world * S / (e2e_ms * 1e-3), "unit": UNIT, "h2d_bytes_per_step": h2d,
                         "d2h_bytes_per_step": d2h, "ms_per_step": e2e_ms},
                 "batched_c4": c4,
-                "gpu_launches": mixed.launches() * args.steps,
+                "gpu_launches": launches * args.steps if launches is not None else None,
                 "clocks": clk_mixed}
         print(json.dumps(line), flush=True)
     if pg:

@@ -146,6 +146,24 @@ int lhl_refine_tol(lhl_shift_t sh, lhl_ws_t ws, const double* dJ, int64_t ldj, c
                    double* dX, int64_t ldx, double* dR, double* dres, int64_t nrhs, int64_t rhs_per_shift, double tol,
                    int max_steps, void* stream);
 
+/* Refinement by GMRES-IR, for where lhl_refine!'s fixed-point iteration (F:3144-3157)
+ * contracts slowly (the mixed form near a shift where sigma I + tau J is close to singular).
+ * Starting from the solution in dX, each cycle computes r = b - A x for every column whose
+ * relative residual is above tol, then up to `restart` steps of GMRES on A d = r
+ * left-preconditioned by the shift's factorisation (each step one lhl_ldiv and one product
+ * with A), stopping a column's cycle once its estimated residual is below 0.1 tol, and
+ * x += d.  At most max_cycles cycles; columns at or below tol are left alone.  On return
+ * dres holds every column's final relative residual, as for lhl_refine_tol.
+ * host_check = 1: the host reads dres after each cycle (a stream synchronisation) and stops
+ * once every column is at or below tol; 0: max_cycles cycles are launched without a host
+ * round trip (finished columns skip their work), which a CUDA graph can capture.
+ * 1 <= restart <= 32.  The Krylov basis, nrhs (restart + 1) n doubles, is kept in the
+ * workspace: allocated by the first call that needs it, reused after.  Real shifts only
+ * (LHL_ERR_ARG for a complex shift batch). */
+int lhl_refine_gmres(lhl_shift_t sh, lhl_ws_t ws, const double* dJ, int64_t ldj, const double* dB, int64_t ldb,
+                     double* dX, int64_t ldx, double* dR, double* dres, int64_t nrhs, int64_t rhs_per_shift,
+                     double tol, int max_cycles, int restart, int host_check, void* stream);
+
 /* Relative residuals ||b - (sigma I + tau J) x||_2 / ||b||_2 per column into dres (nrhs). */
 int lhl_residual_norms(lhl_shift_t sh, const double* dJ, int64_t ldj, const double* dB, int64_t ldb,
                        const double* dX, int64_t ldx, double* dR, double* dres, int64_t nrhs,

@@ -26,6 +26,9 @@ struct lhl_ws_s {
     lhl::MixPlan mplan;
     unsigned long long *mhdr, *mcval, *mcrow;
     float* mgrows;
+    // lhl_refine_gmres: Krylov bases, per-column state and activity, host copy of dres
+    double *gmV, *gmS, *gmA, *gmH;
+    size_t gmV_cap, gmS_cap, gmA_cap, gmH_cap;
 };
 
 struct lhl_shift_s {
@@ -64,9 +67,10 @@ static void ws_free(lhl_ws_t w)
     if (!w) return;
     void* ptrs[] = {w->F, w->Ht, w->scale, w->iscale, w->B0, w->part, w->tab, w->cand_v, w->cand_s, w->buf2, w->tsnap,
                     w->bsum, w->bfac, w->ipiv, w->perm, w->iperm, w->cand_i, w->bflag, w->err, w->bar,
-                    w->ptimes, w->mhdr, w->mcval, w->mcrow, w->mgrows, w->ybuf, w->zflags, w->linv};
+                    w->ptimes, w->mhdr, w->mcval, w->mcrow, w->mgrows, w->ybuf, w->zflags, w->linv, w->gmV, w->gmS, w->gmA};
     for (void* p : ptrs)
         if (p) cudaFree(p);
+    if (w->gmH) cudaFreeHost(w->gmH);
     delete w;
 }
 
@@ -560,20 +564,68 @@ int lhl_refine(lhl_shift_t sh, lhl_ws_t ws, const double* dJ, int64_t ldj, const
     return LHL_OK;
 }
 
-int lhl_refine_tol(lhl_shift_t sh, lhl_ws_t ws, const double* dJ, int64_t ldj, const double* dB, int64_t ldb,
-                   double* dX, int64_t ldx, double* dR, double* dres, int64_t nrhs, int64_t rhs_per_shift, double tol,
-                   int max_steps, void* stream)
+// lhl_ldiv's arguments for the refinement loops: R in place, columns with done[c] <= tol skipped
+static lhl::LdivArgs refine_ldiv_args(lhl_shift_t sh, lhl_ws_t ws, double* dR, int64_t ldr, int64_t rps,
+                                      const double* done, double tol)
+{
+    lhl::LdivArgs a;
+    memset(&a, 0, sizeof(a));
+    a.n = (int)ws->n;
+    a.F = ws->F;
+    a.ldf = (int)ws->n;
+    a.perm = ws->perm;
+    a.iperm = ws->iperm;
+    a.scale = ws->scale;
+    a.iscale = ws->iscale;
+    a.X = dR;
+    a.ldx = (int)ldr;
+    a.mode = 0;
+    a.Gt = sh->Gt;
+    a.ldg = (int)sh->ldg;
+    a.swp = sh->swap;
+    a.rdiag = sh->rdiag;
+    a.rhs_per_shift = (int)rps;
+    a.nshifts = (int)sh->nshifts;
+    a.uinv = (ws->precision == LHL_PREC_MIXED && !sh->cplx) ? sh->uinv : nullptr;
+    a.cplx = sh->cplx;
+    a.po = (int)sh->po;
+    a.linv = ws->linv;
+    a.done = done;
+    a.tol = tol;
+    a.Y = ws->ybuf;
+    a.ycap = ws->ycap;
+    a.zflags = ws->zflags;
+    a.nzflags = ws->nzflags;
+    a.err = ws->err;
+    a.limit_ns = ws->limit_ns;
+    return a;
+}
+
+static int refine_args_check(lhl_shift_t sh, lhl_ws_t ws, const double* dJ, int64_t ldj, const double* dB,
+                             int64_t ldb, const double* dX, int64_t ldx, const double* dR, const double* dres,
+                             int64_t nrhs, int64_t rhs_per_shift, double tol, bool bad_count)
 {
     if (!sh || !ws) return LHL_ERR_ARG;
     const int64_t n = ws->n;
     if (sh->n != n) return LHL_ERR_DIM;
-    if (rhs_per_shift < 1 || max_steps < 0 || !(tol >= 0.0)) return LHL_ERR_ARG;
+    if (rhs_per_shift < 1 || bad_count || !(tol >= 0.0)) return LHL_ERR_ARG;
     if (nrhs < 0) return LHL_ERR_DIM;
     if (nrhs == 0 || n == 0) return LHL_OK;
     if (!dJ || !dB || !dX || !dR || !dres) return LHL_ERR_ARG;
     if (ldj < n || ldb < n || ldx < n) return LHL_ERR_DIM;
     if ((nrhs + rhs_per_shift - 1) / rhs_per_shift > sh->nshifts) return LHL_ERR_DIM;
     if (n > 8192) return LHL_ERR_DIM;
+    return LHL_OK;
+}
+
+int lhl_refine_tol(lhl_shift_t sh, lhl_ws_t ws, const double* dJ, int64_t ldj, const double* dB, int64_t ldb,
+                   double* dX, int64_t ldx, double* dR, double* dres, int64_t nrhs, int64_t rhs_per_shift, double tol,
+                   int max_steps, void* stream)
+{
+    const int chk =
+        refine_args_check(sh, ws, dJ, ldj, dB, ldb, dX, ldx, dR, dres, nrhs, rhs_per_shift, tol, max_steps < 0);
+    if (chk != LHL_OK || nrhs == 0 || ws->n == 0) return chk;
+    const int64_t n = ws->n;
     cudaStream_t st = (cudaStream_t)stream;
     for (int s = 0; s <= max_steps; ++s) {
         // step 0 computes every residual; later steps only those of unconverged columns
@@ -582,38 +634,72 @@ int lhl_refine_tol(lhl_shift_t sh, lhl_ws_t ws, const double* dJ, int64_t ldj, c
         if (e == cudaSuccess) e = relres_any(sh, n, dR, ldx, dB, ldb, dres, nrhs, st);
         if (e != cudaSuccess) return LHL_ERR_CUDA;
         if (s == max_steps) break;
-        lhl::LdivArgs a;
-        memset(&a, 0, sizeof(a));
-        a.n = (int)n;
-        a.F = ws->F;
-        a.ldf = (int)n;
-        a.perm = ws->perm;
-        a.iperm = ws->iperm;
-        a.scale = ws->scale;
-        a.iscale = ws->iscale;
-        a.X = dR;
-        a.ldx = (int)ldx;
-        a.mode = 0;
-        a.Gt = sh->Gt;
-        a.ldg = (int)sh->ldg;
-        a.swp = sh->swap;
-        a.rdiag = sh->rdiag;
-        a.rhs_per_shift = (int)rhs_per_shift;
-        a.nshifts = (int)sh->nshifts;
-        a.uinv = (ws->precision == LHL_PREC_MIXED && !sh->cplx) ? sh->uinv : nullptr;
-        a.cplx = sh->cplx;
-        a.po = (int)sh->po;
-        a.linv = ws->linv;
-        a.done = dres;
-        a.tol = tol;
-        a.Y = ws->ybuf;
-        a.ycap = ws->ycap;
-        a.zflags = ws->zflags;
-        a.nzflags = ws->nzflags;
-        a.err = ws->err;
-        a.limit_ns = ws->limit_ns;
-        e = lhl::launch_ldiv(a, (int)nrhs, st);
+        e = lhl::launch_ldiv(refine_ldiv_args(sh, ws, dR, ldx, rhs_per_shift, dres, tol), (int)nrhs, st);
         if (e == cudaSuccess) e = axpy_any(sh, n, dX, ldx, dR, ldx, nrhs, st, dres, tol);
+        if (e != cudaSuccess) return LHL_ERR_CUDA;
+    }
+    return LHL_OK;
+}
+
+// grow-only device buffer of the workspace
+static cudaError_t ws_grow(double** p, size_t* cap, size_t need)
+{
+    if (*cap >= need && *p) return cudaSuccess;
+    if (*p) cudaFree(*p);
+    *p = nullptr;
+    *cap = 0;
+    cudaError_t e = cudaMalloc((void**)p, need * sizeof(double));
+    if (e == cudaSuccess) *cap = need;
+    return e;
+}
+
+int lhl_refine_gmres(lhl_shift_t sh, lhl_ws_t ws, const double* dJ, int64_t ldj, const double* dB, int64_t ldb,
+                     double* dX, int64_t ldx, double* dR, double* dres, int64_t nrhs, int64_t rhs_per_shift,
+                     double tol, int max_cycles, int restart, int host_check, void* stream)
+{
+    const int chk = refine_args_check(sh, ws, dJ, ldj, dB, ldb, dX, ldx, dR, dres, nrhs, rhs_per_shift, tol,
+                                      max_cycles < 0 || restart < 1 || restart > 32);
+    if (chk != LHL_OK || nrhs == 0 || ws->n == 0) return chk;
+    if (sh->cplx) return LHL_ERR_ARG;
+    const int n = (int)ws->n, m = restart, nr = (int)nrhs;
+    cudaStream_t st = (cudaStream_t)stream;
+    cudaError_t e = ws_grow(&ws->gmV, &ws->gmV_cap, (size_t)nr * (m + 1) * n);
+    if (e == cudaSuccess) e = ws_grow(&ws->gmS, &ws->gmS_cap, (size_t)nr * lhl::gm_state_doubles(m));
+    if (e == cudaSuccess) e = ws_grow(&ws->gmA, &ws->gmA_cap, (size_t)nr);
+    if (e == cudaSuccess && host_check && (ws->gmH_cap < (size_t)nr || !ws->gmH)) {
+        if (ws->gmH) cudaFreeHost(ws->gmH);
+        ws->gmH = nullptr;
+        ws->gmH_cap = 0;
+        e = cudaHostAlloc((void**)&ws->gmH, (size_t)nr * sizeof(double), cudaHostAllocDefault);
+        if (e == cudaSuccess) ws->gmH_cap = (size_t)nr;
+    }
+    if (e != cudaSuccess) return LHL_ERR_ALLOC;
+    const int ldv = (m + 1) * n;  // column c's vector i at gmV + c ldv + i n
+    for (int cyc = 0; cyc <= max_cycles; ++cyc) {
+        e = lhl::launch_residual(n, dJ, (int)ldj, dB, (int)ldb, dX, (int)ldx, dR, (int)ldx, nr, (int)rhs_per_shift,
+                                 sh->sigma, sh->tau, st, cyc > 0 ? dres : nullptr, tol);
+        if (e == cudaSuccess) e = lhl::launch_relres(n, dR, (int)ldx, dB, (int)ldb, dres, nr, st);
+        if (e != cudaSuccess) return LHL_ERR_CUDA;
+        if (cyc == max_cycles) break;
+        if (host_check) {
+            e = cudaMemcpyAsync(ws->gmH, dres, (size_t)nr * sizeof(double), cudaMemcpyDeviceToHost, st);
+            if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+            if (e != cudaSuccess) return LHL_ERR_CUDA;
+            bool all = true;
+            for (int c = 0; c < nr && all; ++c) all = ws->gmH[c] <= tol;
+            if (all) break;
+        }
+        // z = W~^-1 r for the unconverged columns, then the cycle's Arnoldi steps
+        e = lhl::launch_ldiv(refine_ldiv_args(sh, ws, dR, ldx, rhs_per_shift, dres, tol), nr, st);
+        if (e == cudaSuccess) e = lhl::launch_gm_begin(n, m, dR, (int)ldx, ws->gmV, ws->gmS, ws->gmA, dres, tol, nr, st);
+        for (int j = 0; j < m && e == cudaSuccess; ++j) {
+            e = lhl::launch_residual(n, dJ, (int)ldj, nullptr, 0, ws->gmV + (size_t)j * n, ldv, dR, (int)ldx, nr,
+                                     (int)rhs_per_shift, sh->sigma, sh->tau, st, ws->gmA, 0.5);
+            if (e == cudaSuccess)
+                e = lhl::launch_ldiv(refine_ldiv_args(sh, ws, dR, ldx, rhs_per_shift, ws->gmA, 0.5), nr, st);
+            if (e == cudaSuccess) e = lhl::launch_gm_arnoldi(n, m, j, dR, (int)ldx, ws->gmV, ws->gmS, ws->gmA, nr, st);
+        }
+        if (e == cudaSuccess) e = lhl::launch_gm_update(n, m, dX, (int)ldx, ws->gmV, ws->gmS, nr, st);
         if (e != cudaSuccess) return LHL_ERR_CUDA;
     }
     return LHL_OK;

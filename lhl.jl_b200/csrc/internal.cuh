@@ -179,4 +179,13 @@ cudaError_t launch_axpy_cols(int n, double* X, int ldx, const double* R, int ldr
 cudaError_t launch_relres(int n, const double* R, int ldr, const double* B, int ldb, double* out, int nrhs,
                           cudaStream_t st);
 
+// GMRES-IR (gmres.cu)
+size_t gm_state_doubles(int m);
+cudaError_t launch_gm_begin(int n, int m, const double* R, int ldr, double* V, double* S, double* act,
+                            const double* res, double tol, int nrhs, cudaStream_t st);
+cudaError_t launch_gm_arnoldi(int n, int m, int j, double* R, int ldr, double* V, double* S, double* act, int nrhs,
+                              cudaStream_t st);
+cudaError_t launch_gm_update(int n, int m, double* X, int ldx, const double* V, const double* S, int nrhs,
+                             cudaStream_t st);
+
 }  // namespace lhl

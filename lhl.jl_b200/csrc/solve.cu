@@ -984,7 +984,8 @@ __global__ void __launch_bounds__(RTT) residual_kernel(int n, const double* __re
             if (c < nrhs) {
                 const int s = c / rhs_per_shift;
                 const double xv = X[(size_t)c * ldx + i];
-                R[(size_t)c * ldr + i] = B[(size_t)c * ldb + i] - (sig[s] * xv + tau[s] * acc[q]);
+                const double bv = B ? B[(size_t)c * ldb + i] : 0.0;  // no B: R = -W X
+                R[(size_t)c * ldr + i] = bv - (sig[s] * xv + tau[s] * acc[q]);
             }
         }
     }

@@ -88,6 +88,7 @@ def _load():
         "lhl_ldiv": [vp, vp, vp, i64, i64, i64, vp],
         "lhl_refine": [vp, vp, vp, i64, vp, i64, vp, i64, vp, i64, i64, i32, vp],
         "lhl_refine_tol": [vp, vp, vp, i64, vp, i64, vp, i64, vp, vp, i64, i64, d, i32, vp],
+        "lhl_refine_gmres": [vp, vp, vp, i64, vp, i64, vp, i64, vp, vp, i64, i64, d, i32, i32, i32, vp],
         "lhl_residual_norms": [vp, vp, i64, vp, i64, vp, i64, vp, vp, i64, i64, vp],
         "lhl_applyZ": [vp, vp, i64, i64, vp],
         "lhl_applyZinv": [vp, vp, i64, i64, vp],
@@ -269,7 +270,7 @@ class LHLWorkspace:
 
     def __del__(self):
         h = getattr(self, "_h", None)
-        if h is not None and h.value:
+        if h is not None and h.value and _lib is not None:
             _lib.lhl_ws_destroy(h)
             self._h = None
 
@@ -433,7 +434,7 @@ def _as_cols(x: torch.Tensor, n: int):
     if x.dim() == 2:
         if x.shape[0] != n:
             raise DimensionMismatch(f"x has {x.shape[0]} rows, the workspace is {n}x{n}")
-        if x.stride(0) != 1 and x.shape[1] > 1:
+        if x.stride(0) != 1 and x.shape[1] > 1 and n > 1:  # one row: only the column stride counts
             raise ArgumentError("x must be column-major (stride (1, ld))")
         return x, x.shape[1], max(x.stride(1), n) if x.shape[1] > 1 else n
     raise DimensionMismatch("x must be a vector or an (n, k) block")
@@ -522,6 +523,41 @@ def lhl_refine_tol_(x: torch.Tensor, J: torch.Tensor, b: torch.Tensor, sh: LHLSh
                                C.c_void_p(bb.data_ptr()), ldb, C.c_void_p(xx.data_ptr()), ldx,
                                C.c_void_p(R.data_ptr()), C.c_void_p(res.data_ptr()), k, int(rhs_per_shift),
                                float(tol), int(max_steps), _stream(stream)), "lhl_refine_tol")
+    return res
+
+
+def lhl_refine_gmres_(x: torch.Tensor, J: torch.Tensor, b: torch.Tensor, sh: LHLShift, ws: LHLWorkspace,
+                      tol: float = 1e-10, max_cycles: int = 4, restart: int = 8, rhs_per_shift: int = 1,
+                      host_check: bool = True, R: torch.Tensor = None, res: torch.Tensor = None,
+                      stream=None) -> torch.Tensor:
+    """Refinement by GMRES-IR (lhl_refine_gmres of the C ABI): up to `max_cycles` cycles of
+    GMRES(`restart`) on the correction equation, left-preconditioned by the shift's
+    factorisation, for every column above relative residual `tol`.  Returns the per-column
+    final relative residuals (device tensor); x is updated in place.  Real shifts only."""
+    _require_cuda_f64(J, "J")
+    if sh.is_complex:
+        raise ArgumentError("lhl_refine_gmres takes real shifts only")
+    for t, nm in ((x, "x"), (b, "b")):
+        _require_cuda_f64(t, nm)
+    n = ws.n
+    xx, k, ldx = _as_cols(x, n)
+    bb, kb, ldb = _as_cols(b, n)
+    if kb != k:
+        raise DimensionMismatch("x and b differ in column count")
+    if ldx != n:
+        raise ArgumentError("x must have leading dimension n")
+    Jc = _colmajor(J)
+    if R is None:
+        R = torch.empty((k, n), dtype=torch.float64, device=x.device)
+    if res is None:
+        res = torch.empty(k, dtype=torch.float64, device=x.device)
+    if R.numel() < n * k or res.numel() < k:
+        raise DimensionMismatch("scratch too small")
+    _check(_lib.lhl_refine_gmres(sh._h, ws._h, C.c_void_p(Jc.data_ptr()), max(Jc.stride(1), n),
+                                 C.c_void_p(bb.data_ptr()), ldb, C.c_void_p(xx.data_ptr()), ldx,
+                                 C.c_void_p(R.data_ptr()), C.c_void_p(res.data_ptr()), k, int(rhs_per_shift),
+                                 float(tol), int(max_cycles), int(restart), int(bool(host_check)),
+                                 _stream(stream)), "lhl_refine_gmres")
     return res
 
 
@@ -680,6 +716,6 @@ def version() -> str:
 
 
 __all__ = ["LHLWorkspace", "LHLShift", "lhl", "lhl_", "lhl_reduce_", "lhl_shift_", "lhl_shift_batched_",
-           "lhl_refine_tol_", "LHLBatch", "lhl_reduce_batched_", "lhl_shift_batched_all_", "lhl_solve_batched_",
+           "lhl_refine_tol_", "lhl_refine_gmres_", "LHLBatch", "lhl_reduce_batched_", "lhl_shift_batched_all_", "lhl_solve_batched_",
            "lhl_ldiv_", "lhl_refine_", "applyZ_", "applyZinv_", "residual_norms", "ArgumentError",
            "DimensionMismatch", "LHLDeviceError", "LHL_PREC_FP64", "LHL_PREC_MIXED", "version", "lib"]

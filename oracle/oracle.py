@@ -331,3 +331,66 @@ def refine_complex(R: Reduction, S: ShiftC, J, b, x, steps=1):
         r = b - W @ x
         x = x + ldiv_complex(R, S, r)
     return x
+
+
+def gmres_ir(matvec, precond, b, x, tol, max_cycles=4, restart=8):
+    """GMRES-IR for one column, the algorithm lhl_refine_gmres runs on the device: restarted
+    GMRES (Saad and Schultz, 1986: Arnoldi with Givens rotations) on the correction equation
+    W d = r, left-preconditioned by the factorisation (Carson and Higham, 2017), here with
+    classical Gram-Schmidt applied twice.  A cycle starts while ||r|| / ||b|| > tol; its Arnoldi
+    steps stop once |g_{j+1}| / beta <= min(0.5, 0.1 tol / (||r|| / ||b||)), at a breakdown, or
+    after `restart` steps.  Returns (x, relative residual, preconditioner applications)."""
+    b = np.asarray(b, dtype=np.float64)
+    x = np.array(x, dtype=np.float64, copy=True)
+    nb = np.linalg.norm(b)
+    m = restart
+    napply = 0
+    rel = np.inf
+    for cyc in range(max_cycles + 1):
+        r = b - matvec(x)
+        rel = np.linalg.norm(r) / nb if nb > 0 else np.linalg.norm(r)
+        if cyc == max_cycles or not rel > tol:
+            break
+        z = precond(r)
+        napply += 1
+        beta = np.linalg.norm(z)
+        if not (beta > 0 and np.isfinite(beta)):
+            break
+        eta = min(0.5, 0.1 * tol / rel)
+        V = [z / beta]
+        Hr = np.zeros((m, m))
+        cs = np.zeros(m)
+        sn = np.zeros(m)
+        g = np.zeros(m + 1)
+        g[0] = beta
+        jd = 0
+        for j in range(m):
+            w = precond(matvec(V[j]))
+            napply += 1
+            h1 = np.array([v @ w for v in V])
+            w = w - sum(h * v for h, v in zip(h1, V))
+            h2 = np.array([v @ w for v in V])
+            w = w - sum(h * v for h, v in zip(h2, V))
+            hn = np.linalg.norm(w)
+            V.append(w / hn if hn > 0 and np.isfinite(hn) else np.zeros_like(w))
+            hc = np.concatenate([h1 + h2, [hn]])
+            for i in range(j):
+                a_, b_ = hc[i], hc[i + 1]
+                hc[i] = cs[i] * a_ + sn[i] * b_
+                hc[i + 1] = -sn[i] * a_ + cs[i] * b_
+            rr = np.hypot(hc[j], hc[j + 1])
+            cs[j], sn[j] = (hc[j] / rr, hc[j + 1] / rr) if rr > 0 else (1.0, 0.0)
+            Hr[:j, j] = hc[:j]
+            Hr[j, j] = rr
+            g[j + 1] = -sn[j] * g[j]
+            g[j] = cs[j] * g[j]
+            jd = j + 1
+            est = abs(g[j + 1]) / beta
+            if not est > eta or not hn > 0 or not np.isfinite(est):
+                break
+        y = np.zeros(jd)
+        for i in range(jd - 1, -1, -1):
+            v = g[i] - Hr[i, i + 1:jd] @ y[i + 1:jd]
+            y[i] = v / Hr[i, i] if Hr[i, i] != 0 else 0.0
+        x = x + sum(y[i] * V[i] for i in range(jd))
+    return x, rel, napply
