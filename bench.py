@@ -193,6 +193,8 @@ def main():
     ap.add_argument("--cpu-baseline-steps", type=int, default=1)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-c4", action="store_true", help="skip the batched config-4 measurement")
+    ap.add_argument("--no-launch-count", action="store_true",
+                    help="skip the profiler-based kernel count (for runs under ncu)")
     args = ap.parse_args()
     world, rank, local = dist_setup(args.gpus)
 
@@ -310,7 +312,7 @@ def main():
                                                   G.lhl_refine_tol_(mixed.X, Jd, Bd, mixed.sh, mixed.ws, tol=TOL,
                                                                     max_steps=FIXED_POINT_REPLAY_STEPS, R=mixed.Rs,
                                                                     res=mixed.res)), 3, flush)
-    launches = count_launches(torch, lambda: mixed.step(Jd, Bd, sig, tau))
+    launches = None if args.no_launch_count else count_launches(torch, lambda: mixed.step(Jd, Bd, sig, tau))
 
     # ---- roofline of the dominant kernel: the mixed reduction ----
     alg_bytes = 4.0 * (n ** 3) / 3.0 + 16.0 * n * n   # FP32 GEMV stream (4 n^3/3) + J in, factors out (FP64)

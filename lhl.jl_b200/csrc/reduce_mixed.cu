@@ -26,9 +26,9 @@
 //             the row update A[i,:] -= l_i R):
 //                 c'_i = (A[i,k+1] - l_i R[k+1]) + A[i,k+2:n].l - l_i (R[k+2:n].l)
 //             with both dot products in FP64 (FP32 partial sums of at most 16 terms, added in
-//             FP64).  Warp 0 then updates the candidate row and publishes it in the same pass,
-//             and returns to polling, while warps 1-15 apply the rank-1 row update to the
-//             other own rows.
+//             FP64).  Warp 0 publishes the next step's header and returns to polling, while
+//             warps 1-15 update the candidate row and publish it in the same pass, then apply
+//             the rank-1 row update to the other own rows.
 // At the end every CTA writes its rows, in FP64, to their logical positions of `factors`:
 // the same layout as the plain form (H in the upper Hessenberg part, multipliers below).
 #include "internal.cuh"
@@ -97,12 +97,16 @@ __device__ __forceinline__ bool mix_better(float v, int i, float bv, int bi)
 
 __device__ __forceinline__ void warp_best(float& bv, int& bi, int& bl)
 {
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) {
-        const float ov = __shfl_xor_sync(0xffffffffu, bv, o);
-        const int oi = __shfl_xor_sync(0xffffffffu, bi, o), ol = __shfl_xor_sync(0xffffffffu, bl, o);
-        if (mix_better(ov, oi, bv, bi)) { bv = ov; bi = oi; bl = ol; }
-    }
+    // the same order as mix_better as a key: |v| (its bits order like unsigned integers), plus one
+    // so that a zero candidate beats "none" (key 0); then the lowest row among the largest keys
+    const unsigned key = bi == 0 ? 0u : __float_as_uint(fabsf(bv)) + 1u;
+    const unsigned m = __reduce_max_sync(0xffffffffu, key);
+    const unsigned lo = __reduce_min_sync(0xffffffffu, key == m ? (unsigned)bi : 0xffffffffu);
+    const unsigned who = __ballot_sync(0xffffffffu, key == m && (unsigned)bi == lo);
+    const int src = __ffs(who) - 1;
+    bv = __shfl_sync(0xffffffffu, bv, src);
+    bi = __shfl_sync(0xffffffffu, bi, src);
+    bl = __shfl_sync(0xffffffffu, bl, src);
 }
 
 // x[c0..ldr) . l[c0..ldr) with FP64 accumulation of FP32 partials (warp-collective; pads of
@@ -212,9 +216,10 @@ __global__ void __launch_bounds__(MT, 1) reduce_mixed_kernel(MixArgs a)
     }
 
     const uint64_t t_start = globaltimer_ns();
-    // CTA 0's time per sub-phase, summed over steps (probe slots 0-4: wait and pivot choice,
-    // interchange and loads, dot products and new column, publication, row update; slots 5
-    // and 6 split the first and third: the poll alone, the dot products alone)
+    // CTA 0's time per sub-phase on warp 0, summed over steps (probe slots 0-2: wait and pivot
+    // choice, interchange and loads, dot products and new column; slot 4: from there to the next
+    // wait; slots 5 and 6 split slots 0 and 2: the poll alone, the dot products alone.  Slot 3
+    // is unused: warps 1-15 publish the candidate row)
     unsigned long long* probe = (b == 0 && t == 0 && a.ptimes) ? a.ptimes + 8 : nullptr;
     uint64_t tp = t_start;
     auto mark = [&](int slot) {
@@ -400,9 +405,10 @@ __global__ void __launch_bounds__(MT, 1) reduce_mixed_kernel(MixArgs a)
         __syncthreads();
         mark(2);
         const int cl = s_cand;
-        if (warp == 0) {
+        if (warp != 0) {
             // ---- publish step k+1: the candidate row after this step's row update, written to
-            // the exchange and back into its own row in one pass ----
+            // the exchange and back into its own row in one pass, by warps 1-15 (warp 0 is
+            // already polling for step k+1) ----
             const int np = (k + 1) & 1;
             const bool pub = k + 1 <= n - 2;
             if (cl >= 0) {
@@ -410,7 +416,7 @@ __global__ void __launch_bounds__(MT, 1) reduce_mixed_kernel(MixArgs a)
                 const float li = s_li[cl];
                 ulonglong2* dst = reinterpret_cast<ulonglong2*>(a.crow + ((size_t)np * G + b) * ldr);
                 const unsigned st = (unsigned)(k + 1);
-                for (int g = ((k + 1) >> 1) + lane; g < (ldr >> 1); g += 32) {
+                for (int g = ((k + 1) >> 1) + (t - 32); g < (ldr >> 1); g += MT - 32) {
                     const int c = 2 * g;  // 0-based columns c, c+1; only c >= k+1 change
                     float x0 = rc[c], x1 = rc[c + 1];
                     if (c >= k + 1) x0 = fmaf(-li, R[c], x0);
@@ -420,8 +426,6 @@ __global__ void __launch_bounds__(MT, 1) reduce_mixed_kernel(MixArgs a)
                     rc[c + 1] = x1;
                 }
             }
-            mark(3);
-        } else {
             // ---- rank-1 row update of the other own active rows ----
             for (int v = warp - 1; v < nr; v += MW - 1) {
                 const float li = s_li[v];

@@ -46,7 +46,12 @@ def main():
             b.record()
             torch.cuda.synchronize()
             ws.check()
-            print(f"reduce n={n} {args.precision} rep={r} ms={a.elapsed_time(b):.3f}", flush=True)
+            line = f"reduce n={n} {args.precision} rep={r} ms={a.elapsed_time(b):.3f}"
+            if args.precision == "mixed":  # CTA 0's sub-phase times, summed over the steps (ms)
+                p = [int(v) for v in ws.probe_ns()]
+                names = ("wait+choice", "loads", "dots+column", "publish", "rowop", "poll", "dots")
+                line += " " + " ".join(f"{nm}={p[i] / 1e6:.2f}" for i, nm in enumerate(names))
+            print(line, flush=True)
         return
     S = args.shifts
     G.lhl_reduce_(ws, J, True)
