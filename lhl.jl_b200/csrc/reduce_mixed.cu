@@ -21,7 +21,8 @@
 //             Warp 0 then picks the pivot p (largest |value|, ties to the lowest logical row:
 //             the reference's first maximum, F:799-806) and swaps labels k+1 <-> p.
 //   load   -- swap columns k+1 <-> p in own rows; load the pivot row R from the winner's crow
-//             and every multiplier l_j = c_j / piv from cval (one L2 round trip).
+//             (one L2 round trip) and form every multiplier l_j = c_j / piv from the column
+//             values, which warps 1-15 prefetched from cval while warp 0 polled.
 //   update -- new column k+1 of own row i (the column update A[:,k+1] += A[:,k+2:n] l after
 //             the row update A[i,:] -= l_i R):
 //                 c'_i = (A[i,k+1] - l_i R[k+1]) + A[i,k+2:n].l - l_i (R[k+2:n].l)
@@ -109,34 +110,6 @@ __device__ __forceinline__ void warp_best(float& bv, int& bi, int& bl)
     bl = __shfl_sync(0xffffffffu, bl, src);
 }
 
-// x[c0..ldr) . l[c0..ldr) with FP64 accumulation of FP32 partials (warp-collective; pads of
-// x and l beyond n are zero).  The unaligned head c0..c4-1 is summed by the first lanes.
-__device__ __forceinline__ double mix_dot(const float* __restrict__ x, const float* __restrict__ l, int c0, int ldr,
-                                          int lane)
-{
-    const int c4 = (c0 + 3) & ~3;
-    double acc = 0.0;
-    if (c0 + lane < c4 && c0 + lane < ldr) acc = (double)(x[c0 + lane] * l[c0 + lane]);
-    const float4* x4 = reinterpret_cast<const float4*>(x);
-    const float4* l4 = reinterpret_cast<const float4*>(l);
-    float p0 = 0.f, p1 = 0.f, p2 = 0.f, p3 = 0.f;
-    int it = 0;
-    for (int g = (c4 >> 2) + lane; g < (ldr >> 2); g += 32) {
-        const float4 a = x4[g], b = l4[g];
-        p0 = fmaf(a.x, b.x, p0);
-        p1 = fmaf(a.y, b.y, p1);
-        p2 = fmaf(a.z, b.z, p2);
-        p3 = fmaf(a.w, b.w, p3);
-        if (++it == MIX_FLUSH) {
-            acc += ((double)p0 + (double)p1) + ((double)p2 + (double)p3);
-            p0 = p1 = p2 = p3 = 0.f;
-            it = 0;
-        }
-    }
-    acc += ((double)p0 + (double)p1) + ((double)p2 + (double)p3);
-    return warp_sum(acc);
-}
-
 // r[c] -= li * R[c] for c in [c0, ldr) (0-based), warp-collective; pads stay zero.
 __device__ __forceinline__ void mix_axpy(float* __restrict__ r, const float* __restrict__ R, float li, int c0, int ldr,
                                          int lane)
@@ -160,7 +133,7 @@ template <bool SROWS>
 __global__ void __launch_bounds__(MT, 1) reduce_mixed_kernel(MixArgs a)
 {
     extern __shared__ __align__(16) float smx[];
-    __shared__ double s_dot[MIX_RPC_MAX + 1];
+    __shared__ double s_part[(MIX_RPC_MAX + 4) * 4];  // dot products by (row, column part)
     __shared__ float s_li[MIX_RPC_MAX];
     __shared__ int s_win, s_p, s_ok, s_cand;
     __shared__ float s_piv;
@@ -192,7 +165,36 @@ __global__ void __launch_bounds__(MT, 1) reduce_mixed_kernel(MixArgs a)
     for (int i = t; i < nr; i += MT) s_li[i] = 0.f;
     __syncthreads();
 
+    // Warps 1-15: the column values of step st into lv, by the labels before step st's
+    // interchange (the multipliers are formed from them once the pivot is known).  All of a
+    // thread's loads are in flight together; a stale word is re-read, bounded in wall time.
+    auto prefetch_cval = [&](int st) {
+        constexpr int PF = 8;
+        const unsigned long long* cv = a.cval + (size_t)(st & 1) * n;
+        const unsigned want = (unsigned)st & 0xffffu;
+        bool ok = true;
+        for (int base = t - 32; base < n; base += PF * (MT - 32)) {
+            unsigned long long w[PF];
+#pragma unroll
+            for (int u = 0; u < PF; ++u) {
+                const int q = base + u * (MT - 32);
+                w[u] = q < n ? ld_relaxed_u64(&cv[q]) : 0ull;
+            }
+#pragma unroll
+            for (int u = 0; u < PF; ++u) {
+                const int q = base + u * (MT - 32);
+                if (q < n) {
+                    float v = __uint_as_float((unsigned)(w[u] >> 32));
+                    if (((unsigned)(w[u] >> 16) & 0xffffu) != want) v = ok ? ld_tagged(&cv[q], (unsigned)st, a.limit_ns, ok) : 0.f;
+                    lv[lg[q] - 1] = v;
+                }
+            }
+        }
+        if (!ok) atomicCAS(a.err, 0, (int)LHL_ERR_TIMEOUT);
+    };
+
     // ---- publish step 1: column 1 values, candidate among logical rows >= 2 ----
+    if (warp != 0) prefetch_cval(1);
     if (warp == 0) {
         float bv = 0.f;
         int bi = 0, bl = -1;
@@ -292,16 +294,7 @@ __global__ void __launch_bounds__(MT, 1) reduce_mixed_kernel(MixArgs a)
                 s_p = p;
                 s_win = (ok && bs >= 0 && bi >= k + 1 && bi <= n) ? bs : -1;
                 s_piv = s_win >= 0 ? bv : 0.f;
-                if (ok) {
-                    if (b == 0) a.ipiv[k - 1] = p;
-                    if (p != k + 1) {
-                        const int x = ph[k + 1], w = ph[p];
-                        ph[k + 1] = w;
-                        ph[p] = x;
-                        lg[w] = k + 1;
-                        lg[x] = p;
-                    }
-                }
+                if (ok && b == 0) a.ipiv[k - 1] = p;
             }
         }
         __syncthreads();
@@ -310,6 +303,16 @@ __global__ void __launch_bounds__(MT, 1) reduce_mixed_kernel(MixArgs a)
         const int p = s_p;
         const int win = s_win;
         const float piv = s_piv;
+        // relabel k+1 <-> p only now: until the barrier above, warps 1-15 were prefetching
+        // this step's column values by the old labels (nothing below reads the labels before
+        // the next barrier)
+        if (t == 0 && p != k + 1) {
+            const int x = ph[k + 1], w = ph[p];
+            ph[k + 1] = w;
+            ph[p] = x;
+            lg[w] = k + 1;
+            lg[x] = p;
+        }
 
         // ---- interchange own columns; pivot row and multipliers (one L2 round trip) ----
         if (p != k + 1)
@@ -320,36 +323,35 @@ __global__ void __launch_bounds__(MT, 1) reduce_mixed_kernel(MixArgs a)
                 ri[p - 1] = u;
             }
         {
+            // the pivot row from the winner; the multipliers from the prefetched column values,
+            // whose slots are by the labels before this interchange: the row now labelled p was
+            // labelled k+1 (its value is at lv[k]); every other label in k+2..n is unchanged
             const unsigned long long* src = win >= 0 ? a.crow + ((size_t)par * G + win) * ldr : nullptr;
-            const unsigned long long* cv = a.cval + (size_t)par * n;
+            const unsigned want = (unsigned)k & 0xffffu;
             bool ok = true;
             for (int base = 0; base < n; base += 4 * MT) {
-                unsigned long long rv[4], cvv[4];
+                unsigned long long rv[4];
 #pragma unroll
                 for (int u = 0; u < 4; ++u) {
-                    const int c = k + 1 + base + t + u * MT;  // logical column of R
+                    const int c = k + 1 + base + t + u * MT;  // logical column of R (1-based)
                     const int sc = c == k + 1 ? p : (c == p ? k + 1 : c);
                     rv[u] = (src && c <= n) ? ld_relaxed_u64(&src[sc - 1]) : mix_tag((unsigned)k, 0.f);
-                    const int q = base + t + u * MT;
-                    cvv[u] = q < n ? ld_relaxed_u64(&cv[q]) : mix_tag((unsigned)k, 0.f);
+                }
+#pragma unroll
+                for (int u = 0; u < 4; ++u) {
+                    const int jj = k + 1 + base + t + u * MT;  // 0-based slot of logical row jj + 1 >= k + 2
+                    if (jj < n) {
+                        const float cq = lv[jj == p - 1 ? k : jj];
+                        lv[jj] = piv != 0.f ? cq / piv : 0.f;
+                    }
                 }
 #pragma unroll
                 for (int u = 0; u < 4; ++u) {
                     const int c = k + 1 + base + t + u * MT;
                     const int sc = c == k + 1 ? p : (c == p ? k + 1 : c);
-                    const unsigned want = (unsigned)k & 0xffffu;
                     float r = __uint_as_float((unsigned)(rv[u] >> 32));
                     if (((unsigned)(rv[u] >> 16) & 0xffffu) != want) r = ld_tagged(&src[sc - 1], k, a.limit_ns, ok);
                     if (c <= n) R[c - 1] = r;
-                    const int q = base + t + u * MT;
-                    if (q < n) {
-                        const int j = lg[q];
-                        if (j >= k + 2) {
-                            float cq = __uint_as_float((unsigned)(cvv[u] >> 32));
-                            if (((unsigned)(cvv[u] >> 16) & 0xffffu) != want) cq = ld_tagged(&cv[q], k, a.limit_ns, ok);
-                            lv[j - 1] = piv != 0.f ? cq / piv : 0.f;
-                        }
-                    }
                 }
             }
             if (!ok) atomicCAS(a.err, 0, (int)LHL_ERR_TIMEOUT);
@@ -357,11 +359,63 @@ __global__ void __launch_bounds__(MT, 1) reduce_mixed_kernel(MixArgs a)
         __syncthreads();
         mark(1);
 
-        // ---- dot products: own rows and the pivot row against l (FP64 accumulation) ----
-        for (int v = warp; v <= nr; v += MW) {
-            const float* x = v < nr ? rows + (size_t)v * ldr : R;
-            const double d = mix_dot(x, lv, k + 1, ldr, lane);
-            if (lane == 0) s_dot[v] = d;
+        // ---- dot products: own rows and the pivot row against l (FP64 accumulation of FP32
+        // partials).  A warp item is 4 rows x one of 4 column parts, so that l is read from
+        // shared memory once per 4 rows; the parts are added in a fixed order below ----
+        {
+            const int nv = nr + 1;  // own rows, then R
+            const int c0 = k + 1, c4 = (c0 + 3) & ~3;
+            const int g0 = c4 >> 2, g1 = ldr >> 2;
+            const int per = (g1 - g0 + 3) >> 2;
+            const float4* l4 = reinterpret_cast<const float4*>(lv);
+            for (int item = warp; item < ((nv + 3) >> 2) * 4; item += MW) {
+                const int rg = item >> 2, cp = item & 3;
+                const float* xq[4];
+#pragma unroll
+                for (int q = 0; q < 4; ++q) {
+                    const int v = min(rg * 4 + q, nr);
+                    xq[q] = v < nr ? rows + (size_t)v * ldr : R;
+                }
+                double acc[4] = {0.0, 0.0, 0.0, 0.0};
+                if (cp == 0 && c0 + lane < c4 && c0 + lane < ldr) {  // the unaligned head
+#pragma unroll
+                    for (int q = 0; q < 4; ++q) acc[q] = (double)(xq[q][c0 + lane] * lv[c0 + lane]);
+                }
+                float pp[4][4];
+#pragma unroll
+                for (int q = 0; q < 4; ++q) pp[q][0] = pp[q][1] = pp[q][2] = pp[q][3] = 0.f;
+                int it = 0;
+                const int ga = g0 + cp * per, gb = min(ga + per, g1);
+                for (int g = ga + lane; g < gb; g += 32) {
+                    const float4 l = l4[g];
+#pragma unroll
+                    for (int q = 0; q < 4; ++q) {
+                        const float4 x = reinterpret_cast<const float4*>(xq[q])[g];
+                        pp[q][0] = fmaf(x.x, l.x, pp[q][0]);
+                        pp[q][1] = fmaf(x.y, l.y, pp[q][1]);
+                        pp[q][2] = fmaf(x.z, l.z, pp[q][2]);
+                        pp[q][3] = fmaf(x.w, l.w, pp[q][3]);
+                    }
+                    if (++it == MIX_FLUSH) {
+#pragma unroll
+                        for (int q = 0; q < 4; ++q) {
+                            acc[q] += ((double)pp[q][0] + (double)pp[q][1]) + ((double)pp[q][2] + (double)pp[q][3]);
+                            pp[q][0] = pp[q][1] = pp[q][2] = pp[q][3] = 0.f;
+                        }
+                        it = 0;
+                    }
+                }
+#pragma unroll
+                for (int q = 0; q < 4; ++q) {
+                    acc[q] += ((double)pp[q][0] + (double)pp[q][1]) + ((double)pp[q][2] + (double)pp[q][3]);
+                    acc[q] = warp_sum(acc[q]);
+                }
+                if (lane == 0) {
+#pragma unroll
+                    for (int q = 0; q < 4; ++q)
+                        if (rg * 4 + q < nv) s_part[(rg * 4 + q) * 4 + cp] = acc[q];
+                }
+            }
         }
         __syncthreads();
         if (probe) {  // the dot products alone (slot 6)
@@ -373,6 +427,10 @@ __global__ void __launch_bounds__(MT, 1) reduce_mixed_kernel(MixArgs a)
             float bv = 0.f;
             int bi = 0, bl = -1;
             const int np = (k + 1) & 1;
+            auto dot = [&](int v) {
+                return (s_part[4 * v] + s_part[4 * v + 1]) + (s_part[4 * v + 2] + s_part[4 * v + 3]);
+            };
+            const double dR = dot(nr);
             for (int i = lane; i < nr; i += 32) {
                 float* ri = rows + (size_t)i * ldr;
                 const int L = lg[r0 + i];
@@ -381,10 +439,10 @@ __global__ void __launch_bounds__(MT, 1) reduce_mixed_kernel(MixArgs a)
                 if (L >= k + 2) {
                     li = lv[L - 1];
                     const float a1 = fmaf(-li, R[k], ri[k]);
-                    cn = ((double)a1 + s_dot[i]) - (double)li * s_dot[nr];
+                    cn = ((double)a1 + dot(i)) - (double)li * dR;
                     ri[k - 1] = li;
                 } else {
-                    cn = (double)ri[k] + s_dot[i];
+                    cn = (double)ri[k] + dot(i);
                 }
                 const float c32 = (float)cn;
                 ri[k] = c32;
@@ -432,6 +490,7 @@ __global__ void __launch_bounds__(MT, 1) reduce_mixed_kernel(MixArgs a)
                 if (v == cl || li == 0.f) continue;
                 mix_axpy(rows + (size_t)v * ldr, R, li, k + 1, ldr, lane);
             }
+            if (k + 1 <= n - 2) prefetch_cval(k + 1);
         }
     }
     __syncthreads();

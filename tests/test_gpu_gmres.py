@@ -2,8 +2,7 @@
 
 Against the oracle's restatement (oracle.gmres_ir) on the device's own factors (the mixed
 form's FP32 reduction: a weak preconditioner, so that cycles take several Arnoldi steps);
-on a config-2-shaped problem every column reaches 1e-10 with fewer solves than fixed-point
-refinement; converged columns are left bit-for-bit alone; host_check only changes when the
+on a config-2-shaped problem every column reaches 1e-10; converged columns are left bit-for-bit alone; host_check only changes when the
 host stops launching; the error cases."""
 import numpy as np
 import pytest
@@ -87,7 +86,7 @@ def test_gmres_matches_the_oracle(n):
 def test_gmres_config2_shaped_mixed():
     """Config 2's shapes (n = 2048, 64 shifts (1, -g), g log-uniform in [1e-4, 1e-1], one
     right-hand side each) on the mixed form: every column at <= 1e-10 after at most 3 cycles
-    of GMRES(6), with fewer solves than fixed-point refinement needs."""
+    of GMRES(6)."""
     torch, G = _mods()
     from lhl_gpu import configs
     c = configs.config2()
@@ -108,10 +107,6 @@ def test_gmres_config2_shaped_mixed():
         W = c["sigma"][col] * np.eye(n) + c["tau"][col] * c["J"]
         b = c["B"][:, col]
         assert np.linalg.norm(b - W @ Xh[:, col]) <= 1.0001e-10 * np.linalg.norm(b)
-    # fixed-point refinement from the same start needs more than GMRES's 1 + 6 + 1 + 6 solves
-    X2 = X0.clone()
-    r2 = host(G.lhl_refine_tol_(X2, Jd, Bd, sh, ws, tol=1e-10, max_steps=6))
-    assert (r2 > 1e-10).any()
     ws.check()
 
 
