@@ -84,6 +84,10 @@ int lhl_ws_check(lhl_ws_t ws, void* stream);
 int lhl_ws_phase_ns(lhl_ws_t ws, uint64_t* out8, void* stream);
 /* Finer device timers of the last reduction, per sub-phase of one CTA (16 slots). */
 int lhl_ws_probe_ns(lhl_ws_t ws, uint64_t* out16, void* stream);
+/* Profiling hook: on = 1 makes the reductions of this workspace record the timers that
+ * lhl_ws_phase_ns and lhl_ws_probe_ns read (off by default: the timer reads and their
+ * accumulation lengthen CTA 0's per-step path; with them off both read zeros). */
+int lhl_ws_set_probes(lhl_ws_t ws, int on);
 /* Test hook: the wall-time limit of every grid-barrier wait of this workspace's kernels. */
 int lhl_ws_set_barrier_limit_ns(lhl_ws_t ws, uint64_t limit_ns);
 

@@ -29,6 +29,7 @@ struct lhl_ws_s {
     // lhl_refine_gmres: Krylov bases, per-column state and activity, host copy of dres
     double *gmV, *gmS, *gmA, *gmH;
     size_t gmV_cap, gmS_cap, gmA_cap, gmH_cap;
+    int probes;  // device timers in the reduction kernels (lhl_ws_set_probes)
 };
 
 struct lhl_shift_s {
@@ -207,6 +208,13 @@ int lhl_ws_probe_ns(lhl_ws_t ws, uint64_t* out16, void* stream)
     return cuda_status(e);
 }
 
+int lhl_ws_set_probes(lhl_ws_t ws, int on)
+{
+    if (!ws) return LHL_ERR_ARG;
+    ws->probes = on ? 1 : 0;
+    return LHL_OK;
+}
+
 int lhl_reduce(lhl_ws_t ws, const double* dJ, int64_t ldj, int balance, void* stream)
 {
     if (!ws || (!dJ && ws->n > 0)) return LHL_ERR_ARG;
@@ -242,7 +250,7 @@ int lhl_reduce(lhl_ws_t ws, const double* dJ, int64_t ldj, int balance, void* st
     a.bar = ws->bar;
     a.err = ws->err;
     a.limit_ns = ws->limit_ns;
-    a.ptimes = ws->ptimes;
+    a.ptimes = ws->probes ? ws->ptimes : nullptr;
     a.use_tma = (n % 2 == 0) ? 1 : 0;
     if (ws->precision == LHL_PREC_MIXED && n >= 3) {
         // balancing (FP64, the plain kernel's balance-only mode), then the FP32 reduction
@@ -267,7 +275,7 @@ int lhl_reduce(lhl_ws_t ws, const double* dJ, int64_t ldj, int balance, void* st
         m.grows = ws->mgrows;
         m.err = ws->err;
         m.limit_ns = ws->limit_ns;
-        m.ptimes = ws->ptimes;
+        m.ptimes = ws->probes ? ws->ptimes : nullptr;
         e = lhl::launch_reduce_mixed(m, ws->mplan, st);
         if (e == cudaSuccess) e = lhl::launch_linv((int)n, ws->F, (int)n, ws->linv, st);
         if (e != cudaSuccess) return LHL_ERR_CUDA;

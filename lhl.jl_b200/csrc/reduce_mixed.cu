@@ -406,15 +406,20 @@ __global__ void __launch_bounds__(MT, 1) reduce_mixed_kernel(MixArgs a)
                     }
                 }
 #pragma unroll
-                for (int q = 0; q < 4; ++q) {
+                for (int q = 0; q < 4; ++q)
                     acc[q] += ((double)pp[q][0] + (double)pp[q][1]) + ((double)pp[q][2] + (double)pp[q][3]);
-                    acc[q] = warp_sum(acc[q]);
-                }
-                if (lane == 0) {
-#pragma unroll
-                    for (int q = 0; q < 4; ++q)
-                        if (rg * 4 + q < nv) s_part[(rg * 4 + q) * 4 + cp] = acc[q];
-                }
+                // the four sums over the warp in six shuffles: halves of the lanes keep two of the
+                // values, quarters one; lanes 8q .. 8q+7 end with row q's sum
+                const bool h16 = lane & 16, h8 = lane & 8;
+                const double e0 = __shfl_xor_sync(0xffffffffu, h16 ? acc[0] : acc[2], 16);
+                const double e1 = __shfl_xor_sync(0xffffffffu, h16 ? acc[1] : acc[3], 16);
+                const double k0 = (h16 ? acc[2] : acc[0]) + e0, k1 = (h16 ? acc[3] : acc[1]) + e1;
+                double sum = (h8 ? k1 : k0) + __shfl_xor_sync(0xffffffffu, h8 ? k0 : k1, 8);
+                sum += __shfl_xor_sync(0xffffffffu, sum, 4);
+                sum += __shfl_xor_sync(0xffffffffu, sum, 2);
+                sum += __shfl_xor_sync(0xffffffffu, sum, 1);
+                const int q = lane >> 3;
+                if ((lane & 7) == 0 && rg * 4 + q < nv) s_part[(rg * 4 + q) * 4 + cp] = sum;
             }
         }
         __syncthreads();

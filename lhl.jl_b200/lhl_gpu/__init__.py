@@ -71,6 +71,7 @@ def _load():
         "lhl_reduce": [vp, vp, i64, i32, vp],
         "lhl_ws_phase_ns": [vp, C.POINTER(C.c_uint64), vp],
         "lhl_ws_probe_ns": [vp, C.POINTER(C.c_uint64), vp],
+        "lhl_ws_set_probes": [vp, i32],
         "lhl_shift_create": [i64, i64, C.POINTER(vp)],
         "lhl_shift_destroy": [vp],
         "lhl_shift_get_view": [vp, C.POINTER(_ShView)],
@@ -328,6 +329,10 @@ class LHLWorkspace:
         buf = (C.c_uint64 * 16)()
         _check(_lib.lhl_ws_probe_ns(self._h, buf, _stream(stream)), "probe_ns")
         return list(buf)
+
+    def set_probes(self, on: bool = True):
+        """Record the reduction's device timers (phase_ns, probe_ns); off by default."""
+        _check(_lib.lhl_ws_set_probes(self._h, int(bool(on))), "set_probes")
 
     def set_barrier_limit_ns(self, ns: int):
         _check(_lib.lhl_ws_set_barrier_limit_ns(self._h, int(ns)))

@@ -32,11 +32,14 @@ def main():
     ap.add_argument("--reps", type=int, default=3)
     ap.add_argument("--seed", type=int, default=2)
     ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed"])
+    ap.add_argument("--probes", action="store_true", help="record and print the reduction's device timers")
     args = ap.parse_args()
     n = args.n
     rng = np.random.default_rng(args.seed)
     J = torch.as_tensor(np.asfortranarray(rng.standard_normal((n, n)))).cuda()
     ws = G.LHLWorkspace(n, G.LHL_PREC_MIXED if args.precision == "mixed" else G.LHL_PREC_FP64)
+    if args.probes:
+        ws.set_probes(True)
     ev = lambda: torch.cuda.Event(enable_timing=True)  # noqa: E731
     if args.what == "reduce":
         for r in range(args.reps):
@@ -47,7 +50,7 @@ def main():
             torch.cuda.synchronize()
             ws.check()
             line = f"reduce n={n} {args.precision} rep={r} ms={a.elapsed_time(b):.3f}"
-            if args.precision == "mixed":  # CTA 0's sub-phase times, summed over the steps (ms)
+            if args.precision == "mixed" and args.probes:  # CTA 0's sub-phase times, summed over the steps (ms)
                 p = [int(v) for v in ws.probe_ns()]
                 names = ("wait+choice", "loads", "dots+column", "publish", "rowop", "poll", "dots")
                 line += " " + " ".join(f"{nm}={p[i] / 1e6:.2f}" for i, nm in enumerate(names))
