@@ -1,0 +1,97 @@
+"""Multi-GPU sharding of the path, one process per GPU over torch.distributed.
+
+A single reduction does not shard (every ELMHES step needs a global pivot decision), so each
+rank that needs a Jacobian reduces it itself.  What shards (the reference's own units of
+independent work are the shift, F:2456-2461, and the Jacobian, F:3179):
+
+* shifts of one J: every rank reduces J (or holds its own copy of the factors), runs the
+  shift LUs, solves and refinement for a contiguous slice of the shifts, and the solution
+  columns are gathered in shift order (`shift_slice`, `gather_columns`, `sharded_chain`);
+* independent Jacobians (batches of matrices of uneven order): a partition balanced by the
+  O(n^3) reduction cost (`jacobian_partition`); no exchange at all.
+
+The collectives are plain torch.distributed calls, NCCL over NVLink for CUDA tensors and
+gloo for CPU tensors, so the host logic runs the same in CPU tests.
+"""
+from __future__ import annotations
+
+import heapq
+
+import torch
+
+
+def shift_slice(S: int, rank: int, world: int):
+    """(s0, count) of rank's contiguous slice of S shifts; counts differ by at most one and
+    lower ranks take the larger ones."""
+    if world < 1 or not 0 <= rank < world or S < 0:
+        raise ValueError("bad shard arguments")
+    base, extra = divmod(S, world)
+    count = base + (1 if rank < extra else 0)
+    s0 = rank * base + min(rank, extra)
+    return s0, count
+
+
+def jacobian_partition(ns, world: int):
+    """Assign matrices of orders ns to `world` ranks, balancing the sum of n^3 (the reduction's
+    cost; the shift and solve work, n^2 per shift, follows it).  Longest-processing-time first:
+    matrices in decreasing order, each to the least-loaded rank (ties to the lowest rank).
+    Returns one sorted index list per rank."""
+    if world < 1:
+        raise ValueError("world must be >= 1")
+    heap = [(0, r) for r in range(world)]
+    parts = [[] for _ in range(world)]
+    for i in sorted(range(len(ns)), key=lambda i: (-int(ns[i]), i)):
+        load, r = heapq.heappop(heap)
+        parts[r].append(i)
+        heapq.heappush(heap, (load + int(ns[i]) ** 3, r))
+    return [sorted(p) for p in parts]
+
+
+def gather_columns(X_local: torch.Tensor, S: int, rhs_per_shift: int, group=None) -> torch.Tensor:
+    """All ranks' solution columns in shift order: rank r holds the (n, count_r * R) block of
+    its shift slice (`shift_slice`).  The blocks are padded to the largest slice for one
+    all_gather and trimmed after.  Returns the (n, S * R) block on every rank."""
+    import torch.distributed as dist
+    world = dist.get_world_size(group)
+    n = X_local.shape[0]
+    R = rhs_per_shift
+    cmax = shift_slice(S, 0, world)[1] * R
+    buf = torch.zeros((cmax, n), dtype=X_local.dtype, device=X_local.device)
+    if X_local.shape[1]:
+        buf[: X_local.shape[1]] = X_local.t()
+    out = [torch.empty_like(buf) for _ in range(world)]
+    dist.all_gather(out, buf, group=group)
+    cols = [out[r][: shift_slice(S, r, world)[1] * R] for r in range(world)]
+    return torch.cat(cols, 0).t()
+
+
+def sharded_chain(G, ws, J: torch.Tensor, B: torch.Tensor, sigmas: torch.Tensor, taus: torch.Tensor,
+                  rhs_per_shift: int = 1, tol: float = 1e-10, refine: str = "gmres", group=None):
+    """The per-shift chain on this rank's slice of the shifts of an already reduced workspace:
+    shift LUs, solves, refinement to `tol` (GMRES-IR or fixed-point), then the gather.
+    B holds all S * R right-hand sides; returns (X with every rank's columns, this rank's
+    relative residuals)."""
+    import torch.distributed as dist
+    world = dist.get_world_size(group)
+    rank = dist.get_rank(group)
+    S = sigmas.numel()
+    R = rhs_per_shift
+    s0, cnt = shift_slice(S, rank, world)
+    n = ws.n
+    if cnt == 0:
+        X_local = torch.empty((n, 0), dtype=B.dtype, device=B.device)
+        res = torch.empty(0, dtype=torch.float64, device=B.device)
+    else:
+        sh = G.LHLShift(n, cnt)
+        G.lhl_shift_batched_(sh, ws, sigmas[s0:s0 + cnt].contiguous(), taus[s0:s0 + cnt].contiguous())
+        Bl = B[:, s0 * R:(s0 + cnt) * R]
+        X_local = torch.empty((cnt * R, n), dtype=B.dtype, device=B.device).t()
+        X_local.copy_(Bl)
+        G.lhl_ldiv_(X_local, sh, ws, rhs_per_shift=R)
+        Bc = torch.empty_like(X_local)
+        Bc.copy_(Bl)
+        if refine == "gmres":
+            res = G.lhl_refine_gmres_(X_local, J, Bc, sh, ws, tol=tol, rhs_per_shift=R)
+        else:
+            res = G.lhl_refine_tol_(X_local, J, Bc, sh, ws, tol=tol, rhs_per_shift=R)
+    return gather_columns(X_local, S, R, group), res
