@@ -46,6 +46,9 @@ def main():
     ap.add_argument("--reps", type=int, default=2)
     ap.add_argument("--chunk", type=int, default=16)
     ap.add_argument("--forms", default="plain,mixed")
+    ap.add_argument("--steps", type=int, default=4, help="plain form: fixed-point steps at most")
+    ap.add_argument("--cycles", type=int, default=4, help="mixed form: GMRES-IR cycles at most")
+    ap.add_argument("--restart", type=int, default=3, help="mixed form: Arnoldi steps per cycle")
     args = ap.parse_args()
     c = load(args.config)
     n = c["n"]
@@ -81,10 +84,10 @@ def main():
                 Xc.copy_(Bc)
                 G.lhl_ldiv_(Xc, sh, ws, rhs_per_shift=R)
                 if use_gmres:
-                    G.lhl_refine_gmres_(Xc, Jd, Bc, sh, ws, tol=TOL, max_cycles=4, restart=3, rhs_per_shift=R,
+                    G.lhl_refine_gmres_(Xc, Jd, Bc, sh, ws, tol=TOL, max_cycles=args.cycles, restart=args.restart, rhs_per_shift=R,
                                         R=Rs, res=res_all[s0 * R:(s0 + cnt) * R])
                 else:
-                    G.lhl_refine_tol_(Xc, Jd, Bc, sh, ws, tol=TOL, max_steps=16 if form == "mixed" else 4,
+                    G.lhl_refine_tol_(Xc, Jd, Bc, sh, ws, tol=TOL, max_steps=16 if form == "mixed" else args.steps,
                                       rhs_per_shift=R, R=Rs, res=res_all[s0 * R:(s0 + cnt) * R])
             ev[2].record(stream)
             torch.cuda.synchronize()
@@ -102,8 +105,11 @@ def main():
         print(json.dumps({"config": args.config, "form": form, "n": n, "shifts": S, "rhs_per_shift": R,
                           "complex_shifts": bool(cplx), "solves_per_s": S * R / (ms * 1e-3), "ms_per_step": ms,
                           "reduce_ms": red, "chain_ms": ms - red, "max_rel_residual": float(res.max()),
-                          "all_at_tol": bool((res <= TOL).all()),
-                          "refinement": "GMRES-IR" if use_gmres else "fixed-point"}), flush=True)
+                          "all_at_tol": bool((res <= TOL).all()), "n_at_tol": int((res <= TOL).sum()),
+                          "median_rel_residual": float(np.median(res)),
+                          "refinement": (f"GMRES-IR, GMRES({args.restart}) x {args.cycles}" if use_gmres
+                                         else f"fixed-point, {16 if form == 'mixed' else args.steps} steps at most")}),
+              flush=True)
         del ws, sh, X, Rs
         torch.cuda.empty_cache()
 
