@@ -329,6 +329,15 @@ def main():
                                                                     res=mixed.res)), 3, flush)
     launches = None if args.no_launch_count else count_launches(torch, lambda: mixed.step(Jd, Bd, sig, tau))
 
+    # ---- whole-step lower bound: the compulsory HBM bytes of each phase at the measured copy
+    # bandwidth (every phase here is HBM- or latency-bound; none is tensor-core work):
+    # reduction 4n^3/3 (FP32 GEMV stream) + 16n^2; shift LUs 4n^2 (Ht, shared) + S 4n^2 (Gt);
+    # one solve pass S 4n^2 (Gt) + 8n^2 (L, shared); one residual pass 8n^2 (J, shared)
+    def step_lower_ms(peak_gbs):
+        b = (4.0 * n ** 3 / 3 + 16.0 * n * n) + (4.0 * n * n + S * 4.0 * n * n) \
+            + (S * 4.0 * n * n + 8.0 * n * n) + 8.0 * n * n
+        return b / (peak_gbs * 1e9) * 1e3
+
     # ---- roofline of the dominant kernel: the mixed reduction ----
     alg_bytes = 4.0 * (n ** 3) / 3.0 + 16.0 * n * n   # FP32 GEMV stream (4 n^3/3) + J in, factors out (FP64)
     peak, peak_kind = peaks()
@@ -452,6 +461,10 @@ def main():
                              "frac": achieved / peak, "traffic": traffic, "peak_kind": peak_kind,
                              "kernel": "lhl_reduce, mixed form (balance + FP32 ELMHES, cooperative launches)",
                              "algorithmic_bytes": alg_bytes},
+                "roofline_step": {"t_lower_ms": step_lower_ms(peak), "t_measured_ms": ms_mixed,
+                                  "frac": step_lower_ms(peak) / ms_mixed,
+                                  "counts": "reduction + all shift LUs + one solve pass + one residual pass, "
+                                            "compulsory HBM bytes at the measured copy bandwidth"},
                 "cpu_baseline": cpu,
                 "e2e": {"value": world * S / (e2e_ms * 1e-3), "unit": UNIT, "h2d_bytes_per_step": h2d,
                         "d2h_bytes_per_step": d2h, "ms_per_step": e2e_ms},

@@ -162,8 +162,10 @@ int lhl_refine_tol(lhl_shift_t sh, lhl_ws_t ws, const double* dJ, int64_t ldj, c
  * once every column is at or below tol; 0: max_cycles cycles are launched without a host
  * round trip (finished columns skip their work), which a CUDA graph can capture.
  * 1 <= restart <= 32.  The Krylov basis, nrhs (restart + 1) n doubles, is kept in the
- * workspace: allocated by the first call that needs it, reused after.  Real shifts only
- * (LHL_ERR_ARG for a complex shift batch). */
+ * workspace: allocated by the first call that needs it, reused after.  With a complex shift
+ * batch, dX / dB / dR are interleaved complex (as for lhl_refine_tol) and GMRES runs on the
+ * realified system: each interleaved column is a real vector of 2n, the real inner product is
+ * Re<v, w>, and the basis takes 2n doubles per vector. */
 int lhl_refine_gmres(lhl_shift_t sh, lhl_ws_t ws, const double* dJ, int64_t ldj, const double* dB, int64_t ldb,
                      double* dX, int64_t ldx, double* dR, double* dres, int64_t nrhs, int64_t rhs_per_shift,
                      double tol, int max_cycles, int restart, int host_check, void* stream);

@@ -668,10 +668,13 @@ int lhl_refine_gmres(lhl_shift_t sh, lhl_ws_t ws, const double* dJ, int64_t ldj,
     const int chk = refine_args_check(sh, ws, dJ, ldj, dB, ldb, dX, ldx, dR, dres, nrhs, rhs_per_shift, tol,
                                       max_cycles < 0 || restart < 1 || restart > 32);
     if (chk != LHL_OK || nrhs == 0 || ws->n == 0) return chk;
-    if (sh->cplx) return LHL_ERR_ARG;
-    const int n = (int)ws->n, m = restart, nr = (int)nrhs;
+    // Complex shifts: GMRES on the realified system.  An interleaved complex column of n
+    // entries is a real vector of 2n; the product with W and the preconditioner are real-linear
+    // maps of it, and the real inner product is Re<v, w>.  The Arnoldi kernels run on 2n reals.
+    const int P = sh->cplx ? 2 : 1;
+    const int n = (int)ws->n, ne = P * n, m = restart, nr = (int)nrhs;
     cudaStream_t st = (cudaStream_t)stream;
-    cudaError_t e = ws_grow(&ws->gmV, &ws->gmV_cap, (size_t)nr * (m + 1) * n);
+    cudaError_t e = ws_grow(&ws->gmV, &ws->gmV_cap, (size_t)nr * (m + 1) * ne);
     if (e == cudaSuccess) e = ws_grow(&ws->gmS, &ws->gmS_cap, (size_t)nr * lhl::gm_state_doubles(m));
     if (e == cudaSuccess) e = ws_grow(&ws->gmA, &ws->gmA_cap, (size_t)nr);
     if (e == cudaSuccess && host_check && (ws->gmH_cap < (size_t)nr || !ws->gmH)) {
@@ -682,11 +685,11 @@ int lhl_refine_gmres(lhl_shift_t sh, lhl_ws_t ws, const double* dJ, int64_t ldj,
         if (e == cudaSuccess) ws->gmH_cap = (size_t)nr;
     }
     if (e != cudaSuccess) return LHL_ERR_ALLOC;
-    const int ldv = (m + 1) * n;  // column c's vector i at gmV + c ldv + i n
+    const int ldv = (m + 1) * n;  // in (complex) elements: column c's vector i at gmV + P (c ldv + i n)
     for (int cyc = 0; cyc <= max_cycles; ++cyc) {
-        e = lhl::launch_residual(n, dJ, (int)ldj, dB, (int)ldb, dX, (int)ldx, dR, (int)ldx, nr, (int)rhs_per_shift,
-                                 sh->sigma, sh->tau, st, cyc > 0 ? dres : nullptr, tol);
-        if (e == cudaSuccess) e = lhl::launch_relres(n, dR, (int)ldx, dB, (int)ldb, dres, nr, st);
+        e = resid_any(sh, n, dJ, ldj, dB, ldb, dX, ldx, dR, ldx, nrhs, rhs_per_shift, st, cyc > 0 ? dres : nullptr,
+                      tol);
+        if (e == cudaSuccess) e = relres_any(sh, n, dR, ldx, dB, ldb, dres, nrhs, st);
         if (e != cudaSuccess) return LHL_ERR_CUDA;
         if (cyc == max_cycles) break;
         if (host_check) {
@@ -699,15 +702,17 @@ int lhl_refine_gmres(lhl_shift_t sh, lhl_ws_t ws, const double* dJ, int64_t ldj,
         }
         // z = W~^-1 r for the unconverged columns, then the cycle's Arnoldi steps
         e = lhl::launch_ldiv(refine_ldiv_args(sh, ws, dR, ldx, rhs_per_shift, dres, tol), nr, st);
-        if (e == cudaSuccess) e = lhl::launch_gm_begin(n, m, dR, (int)ldx, ws->gmV, ws->gmS, ws->gmA, dres, tol, nr, st);
+        if (e == cudaSuccess)
+            e = lhl::launch_gm_begin(ne, m, dR, (int)(P * ldx), ws->gmV, ws->gmS, ws->gmA, dres, tol, nr, st);
         for (int j = 0; j < m && e == cudaSuccess; ++j) {
-            e = lhl::launch_residual(n, dJ, (int)ldj, nullptr, 0, ws->gmV + (size_t)j * n, ldv, dR, (int)ldx, nr,
-                                     (int)rhs_per_shift, sh->sigma, sh->tau, st, ws->gmA, 0.5);
+            e = resid_any(sh, n, dJ, ldj, nullptr, 0, ws->gmV + (size_t)P * j * n, ldv, dR, ldx, nrhs,
+                          rhs_per_shift, st, ws->gmA, 0.5);
             if (e == cudaSuccess)
                 e = lhl::launch_ldiv(refine_ldiv_args(sh, ws, dR, ldx, rhs_per_shift, ws->gmA, 0.5), nr, st);
-            if (e == cudaSuccess) e = lhl::launch_gm_arnoldi(n, m, j, dR, (int)ldx, ws->gmV, ws->gmS, ws->gmA, nr, st);
+            if (e == cudaSuccess)
+                e = lhl::launch_gm_arnoldi(ne, m, j, dR, (int)(P * ldx), ws->gmV, ws->gmS, ws->gmA, nr, st);
         }
-        if (e == cudaSuccess) e = lhl::launch_gm_update(n, m, dX, (int)ldx, ws->gmV, ws->gmS, nr, st);
+        if (e == cudaSuccess) e = lhl::launch_gm_update(ne, m, dX, (int)(P * ldx), ws->gmV, ws->gmS, nr, st);
         if (e != cudaSuccess) return LHL_ERR_CUDA;
     }
     return LHL_OK;

@@ -357,7 +357,7 @@ __global__ void __launch_bounds__(QT) residual_cplx_kernel(int n, const double* 
         const int s = c / rhs_per_shift;
         const dc sg = {sig[2 * s], sig[2 * s + 1]}, tu = {tau[2 * s], tau[2 * s + 1]};
         const dc xv = {X[2 * ((size_t)c * ldx + i)], X[2 * ((size_t)c * ldx + i) + 1]};
-        const dc bv = {B[2 * ((size_t)c * ldb + i)], B[2 * ((size_t)c * ldb + i) + 1]};
+        const dc bv = B ? dc{B[2 * ((size_t)c * ldb + i)], B[2 * ((size_t)c * ldb + i) + 1]} : dc{0.0, 0.0};  // no B: -W X
         const dc w = cadd(cmul(sg, xv), cmul(tu, dc{ar, ai}));
         R[2 * ((size_t)c * ldr + i)] = bv.re - w.re;
         R[2 * ((size_t)c * ldr + i) + 1] = bv.im - w.im;

@@ -73,6 +73,10 @@ __device__ __forceinline__ void shift_lu_body(int n, const double* __restrict__ 
     }
     __syncthreads();
 
+    // running column pointers, so that a step computes no 64-bit addresses: this thread's
+    // element e of Gt column k is gcol[e * T], of Ht column k + D + 1 (the prefetch) hcol[e * T]
+    double* gcol = Gt + t;
+    const double* hcol = Ht + (size_t)(D + 1) * ldh + t;
     for (int k0 = 1; k0 <= n - 1; k0 += D) {
 #pragma unroll
         for (int d = 0; d < D; ++d) {
@@ -99,11 +103,11 @@ __device__ __forceinline__ void shift_lu_body(int n, const double* __restrict__ 
                             gk = dadd(g, sigma);              // Gt[k+1,k] += sigma
                             rj = dsub(rj, dmul(l, sigma));    // r[k+1] -= l*sigma
                         }
-                        M1(Gt, ldg, j, k) = gk;
+                        gcol[e * T] = gk;
                         r[e] = rj;
                     } else {
                         const double rj = r[e];
-                        M1(Gt, ldg, j, k) = rj;
+                        gcol[e * T] = rj;
                         double rn = dsub(dmul(tau, hq[d][e]), dmul(l, rj));
                         if (j == k + 1) rn = dadd(rn, sigma); // r[k+1] += sigma
                         r[e] = rn;
@@ -119,8 +123,10 @@ __device__ __forceinline__ void shift_lu_body(int n, const double* __restrict__ 
 #pragma unroll
             for (int e = 0; e < E; ++e) {
                 const int j = 1 + t + e * T;
-                hq[d][e] = (j >= kf && j <= n && kf + 1 <= n) ? M1(Ht, ldh, j, kf + 1) : 0.0;
+                hq[d][e] = (j >= kf && j <= n && kf + 1 <= n) ? hcol[e * T] : 0.0;
             }
+            gcol += ldg;
+            hcol += ldh;
             __syncthreads();
         }
     }

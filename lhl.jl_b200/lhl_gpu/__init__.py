@@ -538,12 +538,11 @@ def lhl_refine_gmres_(x: torch.Tensor, J: torch.Tensor, b: torch.Tensor, sh: LHL
     """Refinement by GMRES-IR (lhl_refine_gmres of the C ABI): up to `max_cycles` cycles of
     GMRES(`restart`) on the correction equation, left-preconditioned by the shift's
     factorisation, for every column above relative residual `tol`.  Returns the per-column
-    final relative residuals (device tensor); x is updated in place.  Real shifts only."""
+    final relative residuals (device tensor); x is updated in place.  For complex shifts x and b
+    are complex128 and GMRES runs on the realified system."""
     _require_cuda_f64(J, "J")
-    if sh.is_complex:
-        raise ArgumentError("lhl_refine_gmres takes real shifts only")
     for t, nm in ((x, "x"), (b, "b")):
-        _require_cuda_f64(t, nm)
+        _require_cuda_f64(t, nm, sh.is_complex)
     n = ws.n
     xx, k, ldx = _as_cols(x, n)
     bb, kb, ldb = _as_cols(b, n)
@@ -553,7 +552,7 @@ def lhl_refine_gmres_(x: torch.Tensor, J: torch.Tensor, b: torch.Tensor, sh: LHL
         raise ArgumentError("x must have leading dimension n")
     Jc = _colmajor(J)
     if R is None:
-        R = torch.empty((k, n), dtype=torch.float64, device=x.device)
+        R = torch.empty((k, n), dtype=torch.complex128 if sh.is_complex else torch.float64, device=x.device)
     if res is None:
         res = torch.empty(k, dtype=torch.float64, device=x.device)
     if R.numel() < n * k or res.numel() < k:

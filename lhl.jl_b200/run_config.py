@@ -3,8 +3,8 @@
     python lhl.jl_b200/run_config.py --config c1|c3|c5 [--reps 2] [--chunk 16]
 
 One step = the reduction, every shift LU, every solve and refinement until each solve is at
-relative residual <= 1e-10 (plain form: fixed-point lhl_refine_tol; mixed form: GMRES-IR for
-real shifts, fixed-point for complex ones).  Shifts are processed in chunks of `--chunk`
+relative residual <= 1e-10 (plain form: fixed-point lhl_refine_tol; mixed form: GMRES-IR,
+on the realified system for complex shifts).  Shifts are processed in chunks of `--chunk`
 (config 5's complex Gt is 1.07 GB per shift at n = 8192).  Inputs are the seeded synthetic
 configurations of lhl_gpu.configs; device-resident; CUDA-event times; one JSON line per form.
 """
@@ -69,7 +69,7 @@ def main():
         X = torch.empty((chunk * R, n), dtype=dt, device="cuda").t()
         Rs = torch.empty((chunk * R, n), dtype=dt, device="cuda")
         res_all = torch.empty(S * R, dtype=torch.float64, device="cuda")
-        use_gmres = form == "mixed" and not cplx
+        use_gmres = form == "mixed"
 
         def step(times=None):
             ev = [torch.cuda.Event(enable_timing=True) for _ in range(3)]

@@ -339,7 +339,19 @@ def gmres_ir(matvec, precond, b, x, tol, max_cycles=4, restart=8):
     W d = r, left-preconditioned by the factorisation (Carson and Higham, 2017), here with
     classical Gram-Schmidt applied twice.  A cycle starts while ||r|| / ||b|| > tol; its Arnoldi
     steps stop once |g_{j+1}| / beta <= min(0.5, 0.1 tol / (||r|| / ||b||)), at a breakdown, or
-    after `restart` steps.  Returns (x, relative residual, preconditioner applications)."""
+    after `restart` steps.  Returns (x, relative residual, preconditioner applications).
+    Complex b / x: the same real algorithm on the realified system (an interleaved complex
+    vector of n entries is a real vector of 2n; the real inner product is Re<v, w>)."""
+    if np.iscomplexobj(b) or np.iscomplexobj(x):
+        def to_r(v):
+            return np.ascontiguousarray(v, dtype=np.complex128).view(np.float64)
+
+        def to_c(v):
+            return np.ascontiguousarray(v, dtype=np.float64).view(np.complex128)
+
+        xr, rel, k = gmres_ir(lambda v: to_r(matvec(to_c(v))), lambda v: to_r(precond(to_c(v))), to_r(b),
+                              to_r(x), tol, max_cycles, restart)
+        return to_c(xr), rel, k
     b = np.asarray(b, dtype=np.float64)
     x = np.array(x, dtype=np.float64, copy=True)
     nb = np.linalg.norm(b)

@@ -3,7 +3,8 @@
 Against the oracle's restatement (oracle.gmres_ir) on the device's own factors (the mixed
 form's FP32 reduction: a weak preconditioner, so that cycles take several Arnoldi steps);
 on a config-2-shaped problem every column reaches 1e-10; converged columns are left bit-for-bit alone; host_check only changes when the
-host stops launching; the error cases."""
+host stops launching; complex shifts (GMRES on the realified system) against the oracle and
+on a config-5-shaped sweep; the error cases."""
 import numpy as np
 import pytest
 
@@ -173,8 +174,68 @@ def test_gmres_errors():
         G.lhl_refine_gmres_(X, Jd, dev(B[:, :1]), sh, ws)
     with pytest.raises(G.DimensionMismatch):  # 3 columns, one per shift, 2 shifts
         G.lhl_refine_gmres_(dev(np.ones((n, 3))), Jd, dev(np.ones((n, 3))), sh, ws)
+    with pytest.raises(G.ArgumentError):  # complex vectors with a real shift batch
+        G.lhl_refine_gmres_(dev(np.ones(n) + 0j), Jd, dev(np.ones(n) + 0j), sh, ws)
     wc = G.lhl(Jd, shift_complex=True)
     shc = G.LHLShift(n, 1, complex=True)
     G.lhl_shift_batched_(shc, wc, dev(np.array([1.0 + 1j])), dev(np.array([-0.1 + 0j])))
-    with pytest.raises(G.ArgumentError):
-        G.lhl_refine_gmres_(dev(np.ones(n) + 0j), Jd, dev(np.ones(n) + 0j), shc, wc)
+    with pytest.raises(G.ArgumentError):  # a real x cannot hold a complex shift's solution
+        G.lhl_refine_gmres_(dev(np.ones(n)), Jd, dev(np.ones(n)), shc, wc)
+
+
+def cplx_problem(n, S, rps, seed, precision):
+    """Config 5's form: J ~ N(0,1)/sqrt(n), shifts (s, -1) with s = a + ib, a in [-2, 0],
+    b in [0, 10], complex N(0,1) right-hand sides."""
+    torch, G = _mods()
+    J = rng(seed).standard_normal((n, n)) / np.sqrt(n)
+    g = rng(seed + 1)
+    s = g.uniform(-2.0, 0.0, S) + 1j * g.uniform(0.0, 10.0, S)
+    Jd = dev(J)
+    ws = G.lhl(Jd, precision=precision, shift_complex=True)
+    ws.check()
+    sh = G.LHLShift(n, S, complex=True)
+    G.lhl_shift_batched_(sh, ws, dev(s), dev(-np.ones(S, dtype=complex)))
+    g2 = rng(seed + 2)
+    B = g2.standard_normal((n, S * rps)) + 1j * g2.standard_normal((n, S * rps))
+    return J, s, Jd, ws, sh, B
+
+
+@pytest.mark.parametrize("n", [3, 129, 600])
+def test_gmres_complex_matches_the_oracle(n):
+    """Complex shifts: one cycle of 3 Arnoldi steps of the realified GMRES from x = 0, on the
+    mixed form's factors, against oracle.gmres_ir with the same factors and shift LUs."""
+    torch, G = _mods()
+    S, rps = 2, 2
+    J, s, Jd, ws, sh, B = cplx_problem(n, S, rps, 40 + n, G.LHL_PREC_MIXED)
+    X = dev(np.zeros((n, S * rps), dtype=complex))
+    res = host(G.lhl_refine_gmres_(X, Jd, dev(B), sh, ws, tol=0.0, max_cycles=1, restart=3,
+                                   rhs_per_shift=rps))
+    Xh = host(X)
+    R = as_oracle(ws)
+    for c in range(S * rps):
+        W = s[c // rps] * np.eye(n) - J
+        So = O.shift_complex(R, s[c // rps], -1.0)
+        xo, relo, _ = O.gmres_ir(lambda v: W @ v, lambda v: O.ldiv_complex(R, So, v), B[:, c],
+                                 np.zeros(n, dtype=complex), 0.0, max_cycles=1, restart=3)
+        assert np.linalg.norm(Xh[:, c] - xo) <= 1e-8 * np.linalg.norm(xo), c
+        rh = np.linalg.norm(B[:, c] - W @ Xh[:, c]) / np.linalg.norm(B[:, c])
+        assert abs(res[c] - rh) <= 1e-3 * rh + 1e-12, (c, res[c], rh)
+
+
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_gmres_complex_resolvent_sweep(precision):
+    """Config 5's shape at n = 1024 (8 complex shifts x 4 right-hand sides): every column at
+    <= 1e-10 by GMRES-IR, checked again on the host."""
+    torch, G = _mods()
+    n, S, rps = 1024, 8, 4
+    prec = G.LHL_PREC_MIXED if precision == "mixed" else G.LHL_PREC_FP64
+    J, s, Jd, ws, sh, B = cplx_problem(n, S, rps, 10, prec)
+    Bd = dev(B)
+    X = Bd.clone()
+    G.lhl_ldiv_(X, sh, ws, rhs_per_shift=rps)
+    res = host(G.lhl_refine_gmres_(X, Jd, Bd, sh, ws, tol=1e-10, max_cycles=4, restart=6, rhs_per_shift=rps))
+    assert (res <= 1e-10).all(), res.max()
+    Xh = host(X)
+    for c in (0, S * rps - 1):
+        W = s[c // rps] * np.eye(n) - J
+        assert np.linalg.norm(B[:, c] - W @ Xh[:, c]) <= 1.0001e-10 * np.linalg.norm(B[:, c])

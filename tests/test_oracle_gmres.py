@@ -79,3 +79,25 @@ def test_gmres_ir_short_restarts_still_converge(restart):
     W, b, mv, pc = weak_case(150, 4, 1e-4, 0.9)
     x, rel, _ = O.gmres_ir(mv, pc, b, pc(b), 1e-10, max_cycles=30, restart=restart)
     assert rel <= 1e-10
+
+
+def test_gmres_ir_complex_realified():
+    """Complex shifts on a real reduction: the realified GMRES-IR reaches the tolerance from a
+    perturbed preconditioner (the factors of J + 1e-3 E) on a complex shift near an eigenvalue."""
+    n = 160
+    g0 = rng(7)
+    J = g0.standard_normal((n, n)) / np.sqrt(n)
+    E = g0.standard_normal((n, n)) / np.sqrt(n)
+    ev = np.linalg.eigvals(J)
+    s = ev[np.argmax(np.abs(ev.imag))] + 0.02  # close to an eigenvalue: W nearly singular
+    W = s * np.eye(n) - J
+    Rp = O.reduce(J + 1e-3 * E)
+    Sp = O.shift_complex(Rp, s, -1.0)
+    b = g0.standard_normal(n) + 1j * g0.standard_normal(n)
+    mv = lambda v: W @ v  # noqa: E731
+    pc = lambda v: O.ldiv_complex(Rp, Sp, v)  # noqa: E731
+    x0 = pc(b)
+    x, rel, napply = O.gmres_ir(mv, pc, b, x0, 1e-10, max_cycles=8, restart=8)
+    assert rel <= 1e-10
+    assert np.linalg.norm(b - W @ x) <= 1.0001e-10 * np.linalg.norm(b)
+    assert napply <= 8
