@@ -3,8 +3,8 @@
     python lhl.jl_b200/run_config.py --config c1|c3|c5 [--reps 2] [--chunk 16]
 
 One step = the reduction, every shift LU, every solve and refinement until each solve is at
-relative residual <= 1e-10 (plain form: fixed-point lhl_refine_tol; mixed form: GMRES-IR,
-on the realified system for complex shifts).  Shifts are processed in chunks of `--chunk`
+relative residual <= 1e-10 (plain form: fixed-point lhl_refine_tol; mixed form: GMRES-IR for
+real shifts, fixed-point for complex ones unless --gmres-complex).  Shifts are processed in chunks of `--chunk`
 (config 5's complex Gt is 1.07 GB per shift at n = 8192).  Inputs are the seeded synthetic
 configurations of lhl_gpu.configs; device-resident; CUDA-event times; one JSON line per form.
 """
@@ -49,6 +49,7 @@ def main():
     ap.add_argument("--steps", type=int, default=4, help="plain form: fixed-point steps at most")
     ap.add_argument("--cycles", type=int, default=4, help="mixed form: GMRES-IR cycles at most")
     ap.add_argument("--restart", type=int, default=3, help="mixed form: Arnoldi steps per cycle")
+    ap.add_argument("--gmres-complex", action="store_true", help="mixed form, complex shifts: GMRES-IR too")
     args = ap.parse_args()
     c = load(args.config)
     n = c["n"]
@@ -69,7 +70,10 @@ def main():
         X = torch.empty((chunk * R, n), dtype=dt, device="cuda").t()
         Rs = torch.empty((chunk * R, n), dtype=dt, device="cuda")
         res_all = torch.empty(S * R, dtype=torch.float64, device="cuda")
-        use_gmres = form == "mixed"
+        # GMRES-IR pays where a few columns converge slowly (config 2's mixed form).  Where every
+        # column converges in a few fixed-point steps and solves are costly (config 5's complex
+        # shifts), its extra solve per cycle loses: 436 against 571 solves/s there.
+        use_gmres = form == "mixed" and not (cplx and not args.gmres_complex)
 
         def step(times=None):
             ev = [torch.cuda.Event(enable_timing=True) for _ in range(3)]
