@@ -40,6 +40,7 @@ constexpr int MT = 512;
 constexpr int MW = MT / 32;
 constexpr int MIX_FLUSH = 16;  // float4 iterations per lane before the FP32 partials go to FP64
 constexpr int MIX_RPC_MAX = 64;
+constexpr unsigned MIX_POLL_GAP_NS = 300;  // offset of the second header-poll stream
 
 // Polling load: relaxed, so that a lane's loads of several headers are in flight together.
 // No acquire is needed: every word read after the poll carries its own step tag.
@@ -247,18 +248,36 @@ __global__ void __launch_bounds__(MT, 1) reduce_mixed_kernel(MixArgs a)
             const uint64_t t0 = globaltimer_ns();
             unsigned spins = 0;
             int ok = 1;
-            for (;;) {
+            // two streams of header loads, the second started about half an L2 round trip after
+            // the first, each re-issued as soon as its data is in: a header is seen about half
+            // a round trip sooner than by one stream of samples
+            unsigned long long wa[5] = {0, 0, 0, 0, 0}, wc[5] = {0, 0, 0, 0, 0};
+            auto issue = [&](unsigned long long (&w)[5]) {
 #pragma unroll
                 for (int qq = 0; qq < 5; ++qq) {
                     const int s = lane + 32 * qq;
-                    if (s < G && ((pending >> qq) & 1u)) {
-                        const unsigned long long v = ld_relaxed_u64(&H[s]);
-                        hv[qq] = v;
-                        if (((unsigned)(v >> 16) & 0xffffu) == want) pending &= ~(1u << qq);
-                    }
+                    if (s < G && ((pending >> qq) & 1u)) w[qq] = ld_relaxed_u64(&H[s]);
                 }
+            };
+            auto absorb = [&](const unsigned long long (&w)[5]) {
+#pragma unroll
+                for (int qq = 0; qq < 5; ++qq)
+                    if (((pending >> qq) & 1u) && ((unsigned)(w[qq] >> 16) & 0xffffu) == want) {
+                        hv[qq] = w[qq];
+                        pending &= ~(1u << qq);
+                    }
+            };
+            issue(wa);
+            __nanosleep(MIX_POLL_GAP_NS);
+            issue(wc);
+            for (;;) {
+                absorb(wa);
                 if (__all_sync(0xffffffffu, pending == 0)) break;
-                if ((++spins & 15u) == 0) {
+                issue(wa);
+                absorb(wc);
+                if (__all_sync(0xffffffffu, pending == 0)) break;
+                issue(wc);
+                if (((spins += 2) & 15u) == 0) {
                     int bad = 0;
                     if (lane == 0) {
                         if (ld_acquire_i32(a.err) != 0) bad = 1;
