@@ -96,6 +96,15 @@ int lhl_ws_set_barrier_limit_ns(lhl_ws_t ws, uint64_t limit_ns);
  * dJ (n x n, leading dimension ldj) is not modified. */
 int lhl_reduce(lhl_ws_t ws, const double* dJ, int64_t ldj, int balance, void* stream);
 
+/* Loads a saved reduction into a workspace of the same order and precision, in place of
+ * lhl_reduce: device-to-device copies of the arrays of lhl_ws_view (dfactors and dHt n x n,
+ * ld n; dipiv n-2; dperm, diperm, dscale, discale n), then, for the mixed form, the inverses
+ * of L's diagonal blocks that its solves use.  With the arrays of an earlier lhl_reduce, the
+ * workspace then shifts and solves exactly as it did.  No counterpart in the reference, whose
+ * workspaces live only in a Julia session. */
+int lhl_ws_import(lhl_ws_t ws, const double* dfactors, const double* dHt, const int64_t* dipiv, const int64_t* dperm,
+                  const int64_t* diperm, const double* dscale, const double* discale, void* stream);
+
 /* ---- shifts --------------------------------------------------------------------- */
 /* A batch of nshifts LHLShift{Float64}(n) objects (F:107-116). */
 int lhl_shift_create(int64_t n, int64_t nshifts, lhl_shift_t* sh);

@@ -297,6 +297,30 @@ int lhl_reduce(lhl_ws_t ws, const double* dJ, int64_t ldj, int balance, void* st
     return cuda_status(e);
 }
 
+int lhl_ws_import(lhl_ws_t ws, const double* dfactors, const double* dHt, const int64_t* dipiv, const int64_t* dperm,
+                  const int64_t* diperm, const double* dscale, const double* discale, void* stream)
+{
+    if (!ws) return LHL_ERR_ARG;
+    const int64_t n = ws->n;
+    if (n == 0) return LHL_OK;
+    if (!dfactors || !dHt || !dperm || !diperm || !dscale || !discale || (n > 2 && !dipiv)) return LHL_ERR_ARG;
+    cudaStream_t st = (cudaStream_t)stream;
+    const size_t nn = (size_t)n * (size_t)n;
+    cudaError_t e = cudaMemcpyAsync(ws->F, dfactors, nn * sizeof(double), cudaMemcpyDeviceToDevice, st);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(ws->Ht, dHt, nn * sizeof(double), cudaMemcpyDeviceToDevice, st);
+    if (e == cudaSuccess && n > 2)
+        e = cudaMemcpyAsync(ws->ipiv, dipiv, (size_t)(n - 2) * sizeof(int64_t), cudaMemcpyDeviceToDevice, st);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(ws->perm, dperm, (size_t)n * sizeof(int64_t), cudaMemcpyDeviceToDevice, st);
+    if (e == cudaSuccess)
+        e = cudaMemcpyAsync(ws->iperm, diperm, (size_t)n * sizeof(int64_t), cudaMemcpyDeviceToDevice, st);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(ws->scale, dscale, (size_t)n * sizeof(double), cudaMemcpyDeviceToDevice, st);
+    if (e == cudaSuccess)
+        e = cudaMemcpyAsync(ws->iscale, discale, (size_t)n * sizeof(double), cudaMemcpyDeviceToDevice, st);
+    if (e == cudaSuccess && ws->precision == LHL_PREC_MIXED && n >= 3)
+        e = lhl::launch_linv((int)n, ws->F, (int)n, ws->linv, st);
+    return cuda_status(e);
+}
+
 static int shift_create(int64_t n, int64_t nshifts, int cplx, lhl_shift_t* out)
 {
     if (!out) return LHL_ERR_ARG;

@@ -72,6 +72,7 @@ def _load():
         "lhl_ws_phase_ns": [vp, C.POINTER(C.c_uint64), vp],
         "lhl_ws_probe_ns": [vp, C.POINTER(C.c_uint64), vp],
         "lhl_ws_set_probes": [vp, i32],
+        "lhl_ws_import": [vp, vp, vp, vp, vp, vp, vp, vp, vp],
         "lhl_shift_create": [i64, i64, C.POINTER(vp)],
         "lhl_shift_destroy": [vp],
         "lhl_shift_get_view": [vp, C.POINTER(_ShView)],
@@ -329,6 +330,34 @@ class LHLWorkspace:
         buf = (C.c_uint64 * 16)()
         _check(_lib.lhl_ws_probe_ns(self._h, buf, _stream(stream)), "probe_ns")
         return list(buf)
+
+    def save(self, path: str, stream=None):
+        """Write the reduction (factors, Ht, ipiv, perm, iperm, scale, iscale) and the
+        workspace's order and precision to an .npz file; `load` restores it."""
+        if not self.reduced:
+            raise ArgumentError("the workspace holds no reduction")
+        torch.cuda.current_stream().synchronize() if stream is None else stream.synchronize()
+        np.savez(path, n=self.n, precision=self.precision, shift_complex=self.shift_complex,
+                 factors=self.factors.cpu().numpy(), Ht=self.Ht.cpu().numpy(), ipiv=self.ipiv.cpu().numpy(),
+                 perm=self.perm.cpu().numpy(), iperm=self.iperm.cpu().numpy(), scale=self.scale.cpu().numpy(),
+                 iscale=self.iscale.cpu().numpy())
+
+    @classmethod
+    def load(cls, path: str, stream=None) -> "LHLWorkspace":
+        """A workspace holding the reduction saved by `save` (lhl_ws_import of the C ABI)."""
+        d = np.load(path)
+        ws = cls(int(d["n"]), int(d["precision"]), bool(d["shift_complex"]))
+        n = ws.n
+        dev = {k: torch.as_tensor(np.ascontiguousarray(d[k])).cuda() for k in ("ipiv", "perm", "iperm", "scale", "iscale")}
+        if n:
+            for k in ("factors", "Ht"):  # (n, n) matrices, column-major on the device
+                dev[k] = _colmajor(torch.as_tensor(np.asarray(d[k])).cuda())
+            _check(_lib.lhl_ws_import(ws._h, *[C.c_void_p(dev[k].data_ptr()) for k in
+                                               ("factors", "Ht", "ipiv", "perm", "iperm", "scale", "iscale")],
+                                      _stream(stream)), "lhl_ws_import")
+            (stream or torch.cuda.current_stream()).synchronize()
+        ws.reduced = True
+        return ws
 
     def set_probes(self, on: bool = True):
         """Record the reduction's device timers (phase_ns, probe_ns); off by default."""
