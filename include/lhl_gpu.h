@@ -105,6 +105,27 @@ int lhl_reduce(lhl_ws_t ws, const double* dJ, int64_t ldj, int balance, void* st
 int lhl_ws_import(lhl_ws_t ws, const double* dfactors, const double* dHt, const int64_t* dipiv, const int64_t* dperm,
                   const int64_t* diperm, const double* dscale, const double* discale, void* stream);
 
+/* ---- element type Float32 (LHLWorkspace{Float32}, F:703-705) ------------------------
+ * lhl_ws_create_f32 makes a workspace whose element type is Float32.  Its arrays keep FP64
+ * storage holding float values, so every view, shift object and solve entry point of this
+ * header applies unchanged:
+ *   - J is rounded to float on the way in (lhl_reduce) or taken as float (lhl_reduce_f32);
+ *   - the reduction runs in FP64 (plain) or as the mixed form, and its factors and Ht are
+ *     then rounded to float;
+ *   - the shift LU (lhl_shift, lhl_shift_batched) runs in float arithmetic with sigma and tau
+ *     rounded to float, as LHLShift{Float32} does (F:2529-2594 with T = Float32);
+ *   - solves take FP64 vectors (lhl_ldiv) or float ones (lhl_ldiv_f32, widened, solved in
+ *     FP64 with the float factors, rounded back).
+ * Complex shifts on a Float32 workspace are LHL_ERR_ARG. */
+int lhl_ws_create_f32(int64_t n, int precision, lhl_ws_t* ws);
+/* lhl_reduce!(ws, J, balance) with J Float32 (dJ n x n, ld ldj, float).  On a Float64
+ * workspace the float values are taken exactly, as the reference converts them. */
+int lhl_reduce_f32(lhl_ws_t ws, const float* dJ, int64_t ldj, int balance, void* stream);
+/* lhl_ldiv!(x, sh, ws) for float right-hand sides (dX n x nrhs, ld ldx, float), in place.
+ * The widened copy lives in a workspace buffer, allocated by the first call that needs it. */
+int lhl_ldiv_f32(lhl_shift_t sh, lhl_ws_t ws, float* dX, int64_t ldx, int64_t nrhs, int64_t rhs_per_shift,
+                 void* stream);
+
 /* ---- shifts --------------------------------------------------------------------- */
 /* A batch of nshifts LHLShift{Float64}(n) objects (F:107-116). */
 int lhl_shift_create(int64_t n, int64_t nshifts, lhl_shift_t* sh);

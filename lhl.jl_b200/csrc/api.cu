@@ -30,6 +30,9 @@ struct lhl_ws_s {
     double *gmV, *gmS, *gmA, *gmH;
     size_t gmV_cap, gmS_cap, gmA_cap, gmH_cap;
     int probes;  // device timers in the reduction kernels (lhl_ws_set_probes)
+    int f32;     // LHLWorkspace{Float32}: float values in the FP64 arrays, float shift arithmetic
+    double* f32x;  // lhl_ldiv_f32: widened right-hand sides (grow-only)
+    size_t f32x_cap;
 };
 
 struct lhl_shift_s {
@@ -68,7 +71,7 @@ static void ws_free(lhl_ws_t w)
     if (!w) return;
     void* ptrs[] = {w->F, w->Ht, w->scale, w->iscale, w->B0, w->part, w->tab, w->cand_v, w->cand_s, w->buf2, w->tsnap,
                     w->bsum, w->bfac, w->ipiv, w->perm, w->iperm, w->cand_i, w->bflag, w->err, w->bar,
-                    w->ptimes, w->mhdr, w->mcval, w->mcrow, w->mgrows, w->ybuf, w->zflags, w->linv, w->gmV, w->gmS, w->gmA};
+                    w->ptimes, w->mhdr, w->mcval, w->mcrow, w->mgrows, w->ybuf, w->zflags, w->linv, w->gmV, w->gmS, w->gmA, w->f32x};
     for (void* p : ptrs)
         if (p) cudaFree(p);
     if (w->gmH) cudaFreeHost(w->gmH);
@@ -151,6 +154,13 @@ int lhl_ws_create(int64_t n, int precision, lhl_ws_t* out)
     return LHL_OK;
 }
 
+int lhl_ws_create_f32(int64_t n, int precision, lhl_ws_t* out)
+{
+    const int rc = lhl_ws_create(n, precision, out);
+    if (rc == LHL_OK) (*out)->f32 = 1;
+    return rc;
+}
+
 int lhl_ws_destroy(lhl_ws_t ws)
 {
     if (!ws) return LHL_ERR_ARG;
@@ -215,6 +225,18 @@ int lhl_ws_set_probes(lhl_ws_t ws, int on)
     return LHL_OK;
 }
 
+// The reduction of the matrix already copied into ws->F (the entry points below load it).
+static int reduce_loaded(lhl_ws_t ws, int balance, cudaStream_t st);
+
+// Float32 workspace: the reduction's factors and Ht rounded to float values, in place
+static int round_reduction_f32(lhl_ws_t ws, cudaStream_t st)
+{
+    const int n = (int)ws->n;
+    cudaError_t e = lhl::launch_round_f32(ws->F, n, ws->F, n, n, n, st);
+    if (e == cudaSuccess) e = lhl::launch_round_f32(ws->Ht, n, ws->Ht, n, n, n, st);
+    return cuda_status(e);
+}
+
 int lhl_reduce(lhl_ws_t ws, const double* dJ, int64_t ldj, int balance, void* stream)
 {
     if (!ws || (!dJ && ws->n > 0)) return LHL_ERR_ARG;
@@ -222,8 +244,32 @@ int lhl_reduce(lhl_ws_t ws, const double* dJ, int64_t ldj, int balance, void* st
     if (ldj < n || ldj < 1) return LHL_ERR_DIM;
     if (n == 0) return LHL_OK;
     cudaStream_t st = (cudaStream_t)stream;
-    cudaError_t e = cudaMemcpy2DAsync(ws->F, n * sizeof(double), dJ, ldj * sizeof(double), n * sizeof(double), n,
-                                      cudaMemcpyDeviceToDevice, st);
+    cudaError_t e = ws->f32 ? lhl::launch_round_f32(dJ, (int)ldj, ws->F, (int)n, (int)n, (int)n, st)  // J -> Float32
+                            : cudaMemcpy2DAsync(ws->F, n * sizeof(double), dJ, ldj * sizeof(double), n * sizeof(double),
+                                                n, cudaMemcpyDeviceToDevice, st);
+    if (e != cudaSuccess) return LHL_ERR_CUDA;
+    int rc = reduce_loaded(ws, balance, st);
+    if (rc == LHL_OK && ws->f32) rc = round_reduction_f32(ws, st);
+    return rc;
+}
+
+int lhl_reduce_f32(lhl_ws_t ws, const float* dJ, int64_t ldj, int balance, void* stream)
+{
+    if (!ws || (!dJ && ws->n > 0)) return LHL_ERR_ARG;
+    const int64_t n = ws->n;
+    if (ldj < n || ldj < 1) return LHL_ERR_DIM;
+    if (n == 0) return LHL_OK;
+    cudaStream_t st = (cudaStream_t)stream;
+    if (lhl::launch_f32_to_f64(dJ, (int)ldj, ws->F, (int)n, (int)n, (int)n, st) != cudaSuccess) return LHL_ERR_CUDA;
+    int rc = reduce_loaded(ws, balance, st);
+    if (rc == LHL_OK && ws->f32) rc = round_reduction_f32(ws, st);
+    return rc;
+}
+
+static int reduce_loaded(lhl_ws_t ws, int balance, cudaStream_t st)
+{
+    const int64_t n = ws->n;
+    cudaError_t e = cudaSuccess;
     if (e == cudaSuccess) e = cudaMemsetAsync(ws->bar, 0, sizeof(unsigned int), st);
     if (e == cudaSuccess) e = cudaMemsetAsync(ws->err, 0, sizeof(int), st);
     if (e == cudaSuccess) e = cudaMemsetAsync(ws->ptimes, 0, 24 * sizeof(unsigned long long), st);
@@ -393,13 +439,14 @@ int lhl_shift_get_view(lhl_shift_t s, lhl_shift_view* v)
 static int shift_run(lhl_shift_t sh, lhl_ws_t ws, int64_t s0, int64_t count, cudaStream_t st)
 {
     cudaError_t e;
+    if (sh->cplx && ws->f32) return LHL_ERR_ARG;  // complex shifts need a Float64 workspace
     if (sh->cplx) {
         e = lhl::launch_shift_lu_cplx((int)ws->n, ws->Ht, (int)ws->n, sh->sigma + 2 * s0, sh->tau + 2 * s0, (int)s0,
                                       (int)count, sh->Gt, (int)sh->ldg, (int)sh->po, sh->swap, sh->rdiag, sh->info, st);
         return cuda_status(e);
     }
     e = lhl::launch_shift_lu((int)ws->n, ws->Ht, (int)ws->n, sh->sigma + s0, sh->tau + s0, (int)s0, (int)count,
-                             sh->Gt, (int)sh->ldg, sh->swap, sh->rdiag, sh->info, st);
+                             sh->Gt, (int)sh->ldg, sh->swap, sh->rdiag, sh->info, st, ws->f32);
     if (e == cudaSuccess && ws->precision == LHL_PREC_MIXED)
         e = lhl::launch_uinv((int)ws->n, sh->Gt, (int)sh->ldg, sh->rdiag, (int)s0, (int)count, sh->uinv, st);
     return cuda_status(e);
@@ -532,6 +579,35 @@ int lhl_ldiv(lhl_shift_t sh, lhl_ws_t ws, double* dX, int64_t ldx, int64_t nrhs,
     if (rhs_per_shift < 1) return LHL_ERR_ARG;
     if (nrhs > 0 && (nrhs + rhs_per_shift - 1) / rhs_per_shift > sh->nshifts) return LHL_ERR_DIM;
     return ldiv_common(sh, ws, dX, ldx, nrhs, rhs_per_shift, 0, (cudaStream_t)stream);
+}
+
+int lhl_ldiv_f32(lhl_shift_t sh, lhl_ws_t ws, float* dX, int64_t ldx, int64_t nrhs, int64_t rhs_per_shift,
+                 void* stream)
+{
+    if (!sh || !ws) return LHL_ERR_ARG;
+    if (sh->cplx) return LHL_ERR_ARG;
+    if (sh->n != ws->n) return LHL_ERR_DIM;
+    if (rhs_per_shift < 1) return LHL_ERR_ARG;
+    if (nrhs < 0) return LHL_ERR_DIM;
+    if (nrhs > 0 && (nrhs + rhs_per_shift - 1) / rhs_per_shift > sh->nshifts) return LHL_ERR_DIM;
+    const int64_t n = ws->n;
+    if (nrhs == 0 || n == 0) return LHL_OK;
+    if (!dX) return LHL_ERR_ARG;
+    if (ldx < n) return LHL_ERR_DIM;
+    cudaStream_t st = (cudaStream_t)stream;
+    const size_t need = (size_t)n * (size_t)nrhs;
+    if (ws->f32x_cap < need || !ws->f32x) {
+        if (ws->f32x) cudaFree(ws->f32x);
+        ws->f32x = nullptr;
+        ws->f32x_cap = 0;
+        if (cudaMalloc((void**)&ws->f32x, need * sizeof(double)) != cudaSuccess) return LHL_ERR_ALLOC;
+        ws->f32x_cap = need;
+    }
+    if (lhl::launch_f32_to_f64(dX, (int)ldx, ws->f32x, (int)n, (int)n, (int)nrhs, st) != cudaSuccess)
+        return LHL_ERR_CUDA;
+    const int rc = ldiv_common(sh, ws, ws->f32x, n, nrhs, rhs_per_shift, 0, st);
+    if (rc != LHL_OK) return rc;
+    return cuda_status(lhl::launch_f64_to_f32(ws->f32x, (int)n, dX, (int)ldx, (int)n, (int)nrhs, st));
 }
 
 int lhl_applyZ(lhl_ws_t ws, double* dX, int64_t ldx, int64_t nrhs, void* stream)

@@ -147,8 +147,10 @@ size_t stepTabBytes();
 bool make_tmap_2d(void* tmap, const double* base, int rows, int cols, int ld, int box_r, int box_c);
 int reduce_grid_size();
 
+// f32 = 1: the elimination in float arithmetic (LHLWorkspace{Float32}); Ht holds float values
 cudaError_t launch_shift_lu(int n, const double* Ht, int ldh, const double* sig, const double* tau, int s0, int count,
-                            double* Gt, int ldg, uint8_t* swp, double* rd, int32_t* info, cudaStream_t st);
+                            double* Gt, int ldg, uint8_t* swp, double* rd, int32_t* info, cudaStream_t st,
+                            int f32 = 0);
 
 cudaError_t launch_ldiv(const LdivArgs& a, int nrhs, cudaStream_t st);
 cudaError_t launch_linv(int n, const double* F, int ldf, double* linv, cudaStream_t st);
@@ -178,6 +180,11 @@ cudaError_t launch_axpy_cols(int n, double* X, int ldx, const double* R, int ldr
                              const double* done = nullptr, double tol = 0.0);
 cudaError_t launch_relres(int n, const double* R, int ldr, const double* B, int ldb, double* out, int nrhs,
                           cudaStream_t st);
+
+// Float32 workspaces (f32.cu): column-major block conversions
+cudaError_t launch_f32_to_f64(const float* src, int lds, double* dst, int ldd, int rows, int cols, cudaStream_t st);
+cudaError_t launch_round_f32(const double* src, int lds, double* dst, int ldd, int rows, int cols, cudaStream_t st);
+cudaError_t launch_f64_to_f32(const double* src, int lds, float* dst, int ldd, int rows, int cols, cudaStream_t st);
 
 // GMRES-IR (gmres.cu)
 size_t gm_state_doubles(int m);

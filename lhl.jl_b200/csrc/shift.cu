@@ -14,31 +14,43 @@
 
 namespace lhl {
 
+// Rounded operations of the elimination's arithmetic type V: double (LHLWorkspace{Float64}) or
+// float (LHLWorkspace{Float32}: Ht, sigma and tau hold float values, every operation rounds to
+// float, and Gt / rdiag receive float values in double storage).  No fused multiply-add.
+__device__ __forceinline__ double vmul(double a, double b) { return __dmul_rn(a, b); }
+__device__ __forceinline__ double vadd(double a, double b) { return __dadd_rn(a, b); }
+__device__ __forceinline__ double vsub(double a, double b) { return __dsub_rn(a, b); }
+__device__ __forceinline__ float vmul(float a, float b) { return __fmul_rn(a, b); }
+__device__ __forceinline__ float vadd(float a, float b) { return __fadd_rn(a, b); }
+__device__ __forceinline__ float vsub(float a, float b) { return __fsub_rn(a, b); }
+
 // The elimination of one shift; every thread of the CTA calls it (T threads).
-template <int T, int E, int D>
-__device__ __forceinline__ void shift_lu_body(int n, const double* __restrict__ Ht, int ldh, double sigma, double tau,
-                                              double* __restrict__ Gt, int ldg, uint8_t* __restrict__ swp,
-                                              double* __restrict__ rdiag, int32_t* __restrict__ info_out)
+template <int T, int E, int D, class V = double>
+__device__ __forceinline__ void shift_lu_body(int n, const double* __restrict__ Ht, int ldh, double sigma_in,
+                                              double tau_in, double* __restrict__ Gt, int ldg,
+                                              uint8_t* __restrict__ swp, double* __restrict__ rdiag,
+                                              int32_t* __restrict__ info_out)
 {
     const int t = threadIdx.x;
+    const V sigma = (V)sigma_in, tau = (V)tau_in;
 
-    __shared__ double s_next[2];  // r[k+1] after step k, double-buffered by step parity
-    __shared__ double s_l[2], s_a[2], s_b[2];  // the decision of step k (by parity)
+    __shared__ V s_next[2];  // r[k+1] after step k, double-buffered by step parity
+    __shared__ V s_l[2], s_a[2], s_b[2];  // the decision of step k (by parity)
     __shared__ int s_sw[2];
     __shared__ int s_info;
 
     // D rows of H in flight: the row for step k is requested at step k - D
-    double r[E];
-    double hq[D][E];      // hq[d]: H row k+1 (Ht[j, k+1]) for the step k = d + 1 (mod D)
-    double hsub[E];       // Ht[j, j+1] = H[j+1, j]: the subdiagonal entry of the step this
+    V r[E];
+    V hq[D][E];           // hq[d]: H row k+1 (Ht[j, k+1]) for the step k = d + 1 (mod D)
+    V hsub[E];            // Ht[j, j+1] = H[j+1, j]: the subdiagonal entry of the step this
                           // thread decides (the owner of element j decides step j)
     // row 1 of G: r[j] = tau * Ht[j, 1], r[1] += sigma (F:2536-2539)
 #pragma unroll
     for (int e = 0; e < E; ++e) {
         const int j = 1 + t + e * T;
-        r[e] = (j <= n) ? dmul(tau, M1(Ht, ldh, j, 1)) : 0.0;
-        if (j == 1) r[e] = dadd(r[e], sigma);
-        hsub[e] = (j + 1 <= n) ? M1(Ht, ldh, j, j + 1) : 0.0;
+        r[e] = (j <= n) ? vmul(tau, (V)M1(Ht, ldh, j, 1)) : (V)0;
+        if (j == 1) r[e] = vadd(r[e], sigma);
+        hsub[e] = (j + 1 <= n) ? (V)M1(Ht, ldh, j, j + 1) : (V)0;
     }
 #pragma unroll
     for (int d = 0; d < D; ++d) {
@@ -46,18 +58,18 @@ __device__ __forceinline__ void shift_lu_body(int n, const double* __restrict__ 
 #pragma unroll
         for (int e = 0; e < E; ++e) {
             const int j = 1 + t + e * T;
-            hq[d][e] = (j <= n && k + 1 <= n) ? M1(Ht, ldh, j, k + 1) : 0.0;
+            hq[d][e] = (j <= n && k + 1 <= n) ? (V)M1(Ht, ldh, j, k + 1) : (V)0;
         }
     }
     // the pivot decision of step k (F:2541-2556): |b| > |a| swaps; l = a/b, b/a, or 0
-    auto decide = [&](int k, double a, double hs) {
-        const double b = dmul(tau, hs);
+    auto decide = [&](int k, V a, V hs) {
+        const V b = vmul(tau, hs);
         const bool sw = fabs(b) > fabs(a);
-        double l;
+        V l;
         if (sw) {
             l = a / b;
-        } else if (a == 0.0) {
-            l = 0.0;
+        } else if (a == (V)0) {
+            l = (V)0;
         } else {
             l = b / a;
         }
@@ -82,34 +94,34 @@ __device__ __forceinline__ void shift_lu_body(int n, const double* __restrict__ 
         for (int d = 0; d < D; ++d) {
             const int k = k0 + d;
             if (k > n - 1) break;
-            const double l = s_l[k & 1];
+            const V l = s_l[k & 1];
             const bool sw = s_sw[k & 1] != 0;
             if (t == 0) {
-                const double a = s_a[k & 1], b = s_b[k & 1];
+                const V a = s_a[k & 1], b = s_b[k & 1];
                 swp[k - 1] = sw ? 1 : 0;
                 M1(Gt, ldg, k, k) = sw ? b : a;
                 M1(Gt, ldg, k, k + 1) = l;
-                if (!sw && a == 0.0 && s_info == 0) s_info = k;
+                if (!sw && a == (V)0 && s_info == 0) s_info = k;
             }
 #pragma unroll
             for (int e = 0; e < E; ++e) {
                 const int j = 1 + t + e * T;
                 if (j >= k + 1 && j <= n) {
                     if (sw) {
-                        const double g = dmul(tau, hq[d][e]);
-                        double gk = g;
-                        double rj = dsub(r[e], dmul(l, g));
+                        const V g = vmul(tau, hq[d][e]);
+                        V gk = g;
+                        V rj = vsub(r[e], vmul(l, g));
                         if (j == k + 1) {
-                            gk = dadd(g, sigma);              // Gt[k+1,k] += sigma
-                            rj = dsub(rj, dmul(l, sigma));    // r[k+1] -= l*sigma
+                            gk = vadd(g, sigma);              // Gt[k+1,k] += sigma
+                            rj = vsub(rj, vmul(l, sigma));    // r[k+1] -= l*sigma
                         }
                         gcol[e * T] = gk;
                         r[e] = rj;
                     } else {
-                        const double rj = r[e];
+                        const V rj = r[e];
                         gcol[e * T] = rj;
-                        double rn = dsub(dmul(tau, hq[d][e]), dmul(l, rj));
-                        if (j == k + 1) rn = dadd(rn, sigma); // r[k+1] += sigma
+                        V rn = vsub(vmul(tau, hq[d][e]), vmul(l, rj));
+                        if (j == k + 1) rn = vadd(rn, sigma); // r[k+1] += sigma
                         r[e] = rn;
                     }
                     if (j == k + 1) {  // owner of element k+1: publish it and decide step k+1
@@ -123,7 +135,7 @@ __device__ __forceinline__ void shift_lu_body(int n, const double* __restrict__ 
 #pragma unroll
             for (int e = 0; e < E; ++e) {
                 const int j = 1 + t + e * T;
-                hq[d][e] = (j >= kf && j <= n && kf + 1 <= n) ? hcol[e * T] : 0.0;
+                hq[d][e] = (j >= kf && j <= n && kf + 1 <= n) ? (V)hcol[e * T] : (V)0;
             }
             gcol += ldg;
             hcol += ldh;
@@ -132,18 +144,18 @@ __device__ __forceinline__ void shift_lu_body(int n, const double* __restrict__ 
     }
     // finish (F:2579-2594)
     if (t == 0) {
-        const double rn = s_next[n & 1];
+        const V rn = s_next[n & 1];
         M1(Gt, ldg, n, n) = rn;
         swp[n - 1] = 0;
         int info = s_info;
-        if (rn == 0.0 && info == 0) info = n;
+        if (rn == (V)0 && info == 0) info = n;
         *info_out = info;
     }
     __syncthreads();
-    for (int j = 1 + t; j <= n; j += T) rdiag[j - 1] = 1.0 / M1(Gt, ldg, j, j);
+    for (int j = 1 + t; j <= n; j += T) rdiag[j - 1] = (V)1 / (V)M1(Gt, ldg, j, j);
 }
 
-template <int T, int E, int D>
+template <int T, int E, int D, class V = double>
 __global__ void __launch_bounds__(T) shift_lu_kernel(int n, const double* __restrict__ Ht, int ldh,
                                                      const double* __restrict__ sig, const double* __restrict__ tau_,
                                                      int s0, double* __restrict__ Gt_all, int ldg,
@@ -151,7 +163,7 @@ __global__ void __launch_bounds__(T) shift_lu_kernel(int n, const double* __rest
                                                      int32_t* __restrict__ info_all)
 {
     const int s = s0 + blockIdx.x;
-    shift_lu_body<T, E, D>(n, Ht, ldh, sig[blockIdx.x], tau_[blockIdx.x], Gt_all + (size_t)s * ldg * n, ldg,
+    shift_lu_body<T, E, D, V>(n, Ht, ldh, sig[blockIdx.x], tau_[blockIdx.x], Gt_all + (size_t)s * ldg * n, ldg,
                            swap_all + (size_t)s * n, rdiag_all + (size_t)s * n, info_all + s);
 }
 
@@ -179,22 +191,23 @@ cudaError_t launch_shift_lu_batch(const BatchDesc& d, const double* sig, const d
 template <int T, int E, int D>
 static cudaError_t launch_shift_T(int n, const double* Ht, int ldh, const double* sig, const double* tau, int s0,
                                   int count, double* Gt, int ldg, uint8_t* swp, double* rd, int32_t* info,
-                                  cudaStream_t st)
+                                  cudaStream_t st, int f32)
 {
-    shift_lu_kernel<T, E, D><<<count, T, 0, st>>>(n, Ht, ldh, sig, tau, s0, Gt, ldg, swp, rd, info);
+    if (f32) shift_lu_kernel<T, E, D, float><<<count, T, 0, st>>>(n, Ht, ldh, sig, tau, s0, Gt, ldg, swp, rd, info);
+    else shift_lu_kernel<T, E, D, double><<<count, T, 0, st>>>(n, Ht, ldh, sig, tau, s0, Gt, ldg, swp, rd, info);
     return cudaGetLastError();
 }
 
 cudaError_t launch_shift_lu(int n, const double* Ht, int ldh, const double* sig, const double* tau, int s0, int count,
-                            double* Gt, int ldg, uint8_t* swp, double* rd, int32_t* info, cudaStream_t st)
+                            double* Gt, int ldg, uint8_t* swp, double* rd, int32_t* info, cudaStream_t st, int f32)
 {
     if (count <= 0 || n <= 0) return cudaSuccess;
-    if (n <= 256) return launch_shift_T<256, 1, 4>(n, Ht, ldh, sig, tau, s0, count, Gt, ldg, swp, rd, info, st);
-    if (n <= 1024) return launch_shift_T<512, 2, 4>(n, Ht, ldh, sig, tau, s0, count, Gt, ldg, swp, rd, info, st);
-    if (n <= 2048) return launch_shift_T<512, 4, 4>(n, Ht, ldh, sig, tau, s0, count, Gt, ldg, swp, rd, info, st);
-    if (n <= 4096) return launch_shift_T<512, 8, 2>(n, Ht, ldh, sig, tau, s0, count, Gt, ldg, swp, rd, info, st);
-    if (n <= 8192) return launch_shift_T<1024, 8, 1>(n, Ht, ldh, sig, tau, s0, count, Gt, ldg, swp, rd, info, st);
-    if (n <= 16384) return launch_shift_T<1024, 16, 1>(n, Ht, ldh, sig, tau, s0, count, Gt, ldg, swp, rd, info, st);
+    if (n <= 256) return launch_shift_T<256, 1, 4>(n, Ht, ldh, sig, tau, s0, count, Gt, ldg, swp, rd, info, st, f32);
+    if (n <= 1024) return launch_shift_T<512, 2, 4>(n, Ht, ldh, sig, tau, s0, count, Gt, ldg, swp, rd, info, st, f32);
+    if (n <= 2048) return launch_shift_T<512, 4, 4>(n, Ht, ldh, sig, tau, s0, count, Gt, ldg, swp, rd, info, st, f32);
+    if (n <= 4096) return launch_shift_T<512, 8, 2>(n, Ht, ldh, sig, tau, s0, count, Gt, ldg, swp, rd, info, st, f32);
+    if (n <= 8192) return launch_shift_T<1024, 8, 1>(n, Ht, ldh, sig, tau, s0, count, Gt, ldg, swp, rd, info, st, f32);
+    if (n <= 16384) return launch_shift_T<1024, 16, 1>(n, Ht, ldh, sig, tau, s0, count, Gt, ldg, swp, rd, info, st, f32);
     return cudaErrorInvalidValue;
 }
 

@@ -73,6 +73,9 @@ def _load():
         "lhl_ws_probe_ns": [vp, C.POINTER(C.c_uint64), vp],
         "lhl_ws_set_probes": [vp, i32],
         "lhl_ws_import": [vp, vp, vp, vp, vp, vp, vp, vp, vp],
+        "lhl_ws_create_f32": [i64, i32, C.POINTER(vp)],
+        "lhl_reduce_f32": [vp, vp, i64, i32, vp],
+        "lhl_ldiv_f32": [vp, vp, vp, i64, i64, i64, vp],
         "lhl_shift_create": [i64, i64, C.POINTER(vp)],
         "lhl_shift_destroy": [vp],
         "lhl_shift_get_view": [vp, C.POINTER(_ShView)],
@@ -174,6 +177,13 @@ def _require_cuda_f64(x: torch.Tensor, name: str, cplx: bool = False):
         raise ArgumentError(f"{name} must be float64 (complex shifts need an LHLShift built for them)")
 
 
+def _require_cuda_real(x: torch.Tensor, name: str):
+    if not isinstance(x, torch.Tensor) or not x.is_cuda:
+        raise ArgumentError(f"{name} must be a CUDA tensor")
+    if x.dtype not in (torch.float64, torch.float32):
+        raise ArgumentError(f"{name} must be float64 or float32")
+
+
 class LHLShift:
     """``LHLShift{Float64}(n)`` or, with ``complex=True``, ``LHLShift{ComplexF64}(n)`` on a real
     reduction: a batch of ``nshifts`` shift slots (src/LHLFactorization.jl:84-116).  A complex
@@ -257,9 +267,18 @@ class LHLWorkspace:
 
     _SHIFT_FIELDS = ("Gt", "rdiag", "swap", "info", "σ", "τ")
 
-    def __init__(self, n: int, precision: int = LHL_PREC_FP64, shift_complex: bool = False):
+    def __init__(self, n: int, precision: int = LHL_PREC_FP64, shift_complex: bool = False,
+                 dtype: torch.dtype = torch.float64):
         self._h = C.c_void_p()
-        _check(_lib.lhl_ws_create(int(n), int(precision), C.byref(self._h)), "LHLWorkspace")
+        if dtype == torch.float32:  # LHLWorkspace{Float32}
+            if shift_complex:
+                raise ArgumentError("complex shifts need a Float64 workspace")
+            _check(_lib.lhl_ws_create_f32(int(n), int(precision), C.byref(self._h)), "LHLWorkspace")
+        elif dtype == torch.float64:
+            _check(_lib.lhl_ws_create(int(n), int(precision), C.byref(self._h)), "LHLWorkspace")
+        else:
+            raise ArgumentError(f"element type {dtype} is not supported (float64 or float32)")
+        self.dtype = dtype
         self.n = int(n)
         self.precision = precision
         self.shift_complex = bool(shift_complex)
@@ -338,6 +357,7 @@ class LHLWorkspace:
             raise ArgumentError("the workspace holds no reduction")
         torch.cuda.current_stream().synchronize() if stream is None else stream.synchronize()
         np.savez(path, n=self.n, precision=self.precision, shift_complex=self.shift_complex,
+                 f32=self.dtype == torch.float32,
                  factors=self.factors.cpu().numpy(), Ht=self.Ht.cpu().numpy(), ipiv=self.ipiv.cpu().numpy(),
                  perm=self.perm.cpu().numpy(), iperm=self.iperm.cpu().numpy(), scale=self.scale.cpu().numpy(),
                  iscale=self.iscale.cpu().numpy())
@@ -346,7 +366,8 @@ class LHLWorkspace:
     def load(cls, path: str, stream=None) -> "LHLWorkspace":
         """A workspace holding the reduction saved by `save` (lhl_ws_import of the C ABI)."""
         d = np.load(path)
-        ws = cls(int(d["n"]), int(d["precision"]), bool(d["shift_complex"]))
+        ws = cls(int(d["n"]), int(d["precision"]), bool(d["shift_complex"]),
+                 dtype=torch.float32 if ("f32" in d and bool(d["f32"])) else torch.float64)
         n = ws.n
         dev = {k: torch.as_tensor(np.ascontiguousarray(d[k])).cuda() for k in ("ipiv", "perm", "iperm", "scale", "iscale")}
         if n:
@@ -371,14 +392,18 @@ class LHLWorkspace:
 def lhl_reduce_(ws: LHLWorkspace, J: torch.Tensor, balance: bool, thread=True, stream=None) -> LHLWorkspace:
     """``lhl_reduce!(ws, J, balance)`` (F:355).  J is not modified.  The workspace must have
     been built for J's order (the device workspace does not resize in place)."""
-    _require_cuda_f64(J, "J")
+    if isinstance(J, torch.Tensor) and J.dtype == torch.float32:
+        _require_cuda_real(J, "J")
+    else:
+        _require_cuda_f64(J, "J")
     if J.dim() != 2 or J.shape[0] != J.shape[1]:
         raise DimensionMismatch(f"matrix is not square: dimensions are {tuple(J.shape)}")
     if J.shape[0] != ws.n:
         raise DimensionMismatch(f"J is {J.shape[0]}x{J.shape[0]}, the workspace is {ws.n}x{ws.n}")
     Jc = _colmajor(J)
     ld = max(Jc.stride(1), 1)
-    _check(_lib.lhl_reduce(ws._h, C.c_void_p(Jc.data_ptr()), ld, int(bool(balance)), _stream(stream)), "lhl_reduce")
+    fn = _lib.lhl_reduce_f32 if Jc.dtype == torch.float32 else _lib.lhl_reduce
+    _check(fn(ws._h, C.c_void_p(Jc.data_ptr()), ld, int(bool(balance)), _stream(stream)), "lhl_reduce")
     ws.reduced = True
     ws._J_keepalive = Jc
     return ws
@@ -388,10 +413,10 @@ def lhl(J: torch.Tensor, balance: bool = True, thread=True, precision: int = LHL
         shift_complex: bool = False, stream=None) -> LHLWorkspace:
     """``lhl(J; balance=true, shift=...)`` (F:3179): allocate a workspace and reduce J into it;
     ``shift_complex=True`` is ``shift = ComplexF64`` (complex shifts on the real reduction)."""
-    _require_cuda_f64(J, "J")
+    _require_cuda_real(J, "J")
     if J.dim() != 2 or J.shape[0] != J.shape[1]:
         raise DimensionMismatch(f"matrix is not square: dimensions are {tuple(J.shape)}")
-    ws = LHLWorkspace(J.shape[0], precision, shift_complex)
+    ws = LHLWorkspace(J.shape[0], precision, shift_complex, dtype=J.dtype)
     return lhl_reduce_(ws, J, balance, thread, stream)
 
 
@@ -484,12 +509,16 @@ def lhl_ldiv_(x: torch.Tensor, *args, rhs_per_shift: int = 1, stream=None) -> to
         sh, ws = args
     if x.is_complex() and not sh.is_complex:
         raise ArgumentError("a complex right-hand side needs an LHLShift built for complex shifts")
-    _require_cuda_f64(x, "x", sh.is_complex)
+    if x.dtype == torch.float32 and not sh.is_complex:  # float vectors: widened, solved, rounded back
+        _require_cuda_real(x, "x")
+        fn = _lib.lhl_ldiv_f32
+    else:
+        _require_cuda_f64(x, "x", sh.is_complex)
+        fn = _lib.lhl_ldiv
     if sh.n != ws.n:
         raise DimensionMismatch(f"the LHLShift is {sh.n}x{sh.n}, the workspace {ws.n}x{ws.n}")
     xx, k, ld = _as_cols(x, ws.n)
-    _check(_lib.lhl_ldiv(sh._h, ws._h, C.c_void_p(xx.data_ptr()), ld, k, int(rhs_per_shift), _stream(stream)),
-           "lhl_ldiv")
+    _check(fn(sh._h, ws._h, C.c_void_p(xx.data_ptr()), ld, k, int(rhs_per_shift), _stream(stream)), "lhl_ldiv")
     return x
 
 

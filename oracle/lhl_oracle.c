@@ -723,6 +723,56 @@ int lhlo_shift(int n, const double* Ht, int ldh, double sigma, double tau, doubl
     return info;
 }
 
+/* lhl_shift! for LHLWorkspace{Float32} (F:2529-2594 with T = Float32): the same steps in
+ * float arithmetic, sigma and tau rounded to float first (T(sigma), T(tau)).  Ht holds float
+ * values in double storage; Gt and rdiag receive float values in double storage. */
+int lhlo_shift_f32(int n, const double* Ht, int ldh, double sigma_d, double tau_d, double* Gt, int ldg,
+                   uint8_t* swp, double* rdiag, double* rw /* work, n */)
+{
+    if (n == 0) return 0;
+    const float sigma = (float)sigma_d, tau = (float)tau_d;
+    float* r = (float*)rw;
+    for (int j = 1; j <= n; ++j) r[j - 1] = tau * (float)M1(Ht, ldh, j, 1);
+    r[0] = r[0] + sigma;
+    int info = 0;
+    for (int k = 1; k <= n - 1; ++k) {
+        float a = r[k - 1];
+        float b = tau * (float)M1(Ht, ldh, k, k + 1);
+        if (fabsf(b) > fabsf(a)) {
+            swp[k - 1] = 1;
+            M1(Gt, ldg, k, k) = b;
+            float l = a / b;
+            M1(Gt, ldg, k, k + 1) = l;
+            for (int j = k + 1; j <= n; ++j) {
+                float g = tau * (float)M1(Ht, ldh, j, k + 1);
+                M1(Gt, ldg, j, k) = g;
+                r[j - 1] = r[j - 1] - l * g;
+            }
+            M1(Gt, ldg, k + 1, k) = (float)M1(Gt, ldg, k + 1, k) + sigma;
+            r[k] = r[k] - l * sigma;
+        } else {
+            swp[k - 1] = 0;
+            M1(Gt, ldg, k, k) = a;
+            float l;
+            if (a == 0.0f) { if (info == 0) info = k; l = 0.0f; }
+            else l = b / a;
+            M1(Gt, ldg, k, k + 1) = l;
+            for (int j = k + 1; j <= n; ++j) {
+                float rj = r[j - 1];
+                M1(Gt, ldg, j, k) = rj;
+                r[j - 1] = tau * (float)M1(Ht, ldh, j, k + 1) - l * rj;
+            }
+            r[k] = r[k] + sigma;
+        }
+    }
+    float rn = r[n - 1];
+    M1(Gt, ldg, n, n) = rn;
+    swp[n - 1] = 0;
+    if (rn == 0.0f && info == 0) info = n;
+    for (int j = 1; j <= n; ++j) rdiag[j - 1] = 1.0f / (float)M1(Gt, ldg, j, j);
+    return info;
+}
+
 /* ------------------------------------------------------------------------------------ */
 /* Solves.  L (the multipliers) is read from the factors F: L[i,k] = F[i,k], i >= k+2.    */
 /* Sweeps follow the Float64 padded-buffer kernels (F:2265-2434: fused multiply-adds in a */

@@ -48,6 +48,8 @@ def lib():
         L.lhlo_reduce.restype = i
         L.lhlo_shift.argtypes = [i, _dp, i, d, d, _dp, i, _u8, _dv, _dv]
         L.lhlo_shift.restype = i
+        L.lhlo_shift_f32.argtypes = [i, _dp, i, d, d, _dp, i, _u8, _dv, _dv]
+        L.lhlo_shift_f32.restype = i
         L.lhlo_ldiv.argtypes = [i, _dp, i, _iv, _iv, _dv, _dv, _dp, i, _u8, _dv, _dv, _dv]
         L.lhlo_applyZ.argtypes = [i, _dp, i, _iv, _dv, _dv, _dv]
         L.lhlo_applyZinv.argtypes = [i, _dp, i, _iv, _dv, _dv, _dv]
@@ -192,6 +194,19 @@ def shift(R: Reduction, sigma, tau) -> Shift:
     Ht = R.Ht if n > 0 else np.zeros((1, 1), order="F")
     S.info = int(lib().lhlo_shift(n, Ht, max(n, 1), float(sigma), float(tau), S.Gt, S.ldg, S.swap, S.rdiag, w))
     S.sigma, S.tau = float(sigma), float(tau)
+    return S
+
+
+def shift_f32(Ht, sigma, tau) -> Shift:
+    """lhl_shift! of an LHLWorkspace{Float32} on the n x n Ht (float values; any float dtype),
+    in float arithmetic (lhlo_shift_f32)."""
+    Ht = np.asfortranarray(np.asarray(Ht, dtype=np.float32), dtype=np.float64)
+    n = Ht.shape[0]
+    S = Shift(n)
+    w = np.zeros(max(n, 1))
+    H = Ht if n > 0 else np.zeros((1, 1), order="F")
+    S.info = int(lib().lhlo_shift_f32(n, H, max(n, 1), float(sigma), float(tau), S.Gt, S.ldg, S.swap, S.rdiag, w))
+    S.sigma, S.tau = float(np.float32(sigma)), float(np.float32(tau))
     return S
 
 

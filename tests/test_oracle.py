@@ -86,11 +86,12 @@ def test_blocked_small_panels(n):
 
 # test/core_tests.jl:115-212 -- the shift LU against the test file's own reference
 def shift_ref(Ht, sigma, tau):
-    """Pure-Python restatement of `_lhl_shift_ref!` (test/core_tests.jl:119-171)."""
+    """Pure-Python restatement of `_lhl_shift_ref!` (test/core_tests.jl:119-171).  With a
+    float32 Ht and np.float32 sigma, tau every operation rounds to float32 (T = Float32)."""
     n = Ht.shape[0]
-    Gt = np.zeros((n, n))
+    Gt = np.zeros((n, n), dtype=Ht.dtype)
     swap = np.zeros(n, dtype=bool)
-    rdiag = np.zeros(n)
+    rdiag = np.zeros(n, dtype=Ht.dtype)
     r = np.array([tau * Ht[j, 0] for j in range(n)])
     r[0] += sigma
     info = 0
@@ -355,3 +356,29 @@ def test_complex_shifts_on_a_real_reduction(n):
         y = O.refine_complex(R, S, J, b, x, 1)
         assert O.bwd(W, y, b) <= 2 * O.bwd(W, x, b) + eps
         assert O.bwd(W, y, b) < 50 * eps
+
+
+SHIFTS_REF = ((1.0, -0.1), (0.0, 1.0), (1.0, -3.0), (2.0, 0.0), (0.0, 0.0))
+
+
+@pytest.mark.parametrize("n", list(range(1, 34)) + [64, 130, 257])
+@pytest.mark.parametrize("tie", [False, True])
+def test_shift_f32_matches_restatement(n, tie):
+    """LHLWorkspace{Float32}'s shift LU (test/core_tests.jl:192-203 with T = Float32): the
+    oracle's float restatement against the pure-Python one run in numpy float32, bit for bit,
+    on upper Hessenberg matrices (random, and with ties and zeros)."""
+    g = rng(900 + n)
+    H = g.integers(-2, 3, (n, n)) if tie else g.standard_normal((n, n))
+    H = np.triu(H.astype(np.float32), -1)
+    Ht = np.asfortranarray(H.T)
+    for s, t in SHIFTS_REF:
+        U, l, sw, rd, info = shift_ref(Ht, np.float32(s), np.float32(t))
+        S = O.shift_f32(Ht, s, t)
+        Uo, lo, swo, rdo, infoo = S.state()
+        assert info == infoo, (s, t)
+        assert np.array_equal(np.asarray(swo, dtype=bool), sw)
+        for a, b in ((U, Uo), (l, lo), (rd, rdo)):
+            a32 = np.asarray(a, dtype=np.float32)
+            b32 = np.asarray(b).astype(np.float32)
+            assert np.array_equal(b32.astype(np.float64), np.asarray(b)), "not float values"
+            assert np.array_equal(a32.view(np.int32), b32.view(np.int32)), (s, t)
