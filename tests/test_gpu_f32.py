@@ -92,7 +92,7 @@ def test_f32_solves(n, precision):
     assert bwd < 50 * EPS32, bwd
     # a block of float right-hand sides, and FP64 vectors on the same workspace
     B = rng(n + 8).standard_normal((n, 3)).astype(np.float32)
-    X = host(G.lhl_ldiv_(dev(B), ws))
+    X = host(G.lhl_ldiv_(dev(B), ws, rhs_per_shift=3))
     for c in range(3):
         xc = np.linalg.solve(W.astype(np.float64), B[:, c].astype(np.float64))
         assert np.linalg.norm(X[:, c] - xc) <= 1e-3 * np.linalg.norm(xc)
