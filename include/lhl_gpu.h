@@ -186,10 +186,12 @@ int lhl_refine_tol(lhl_shift_t sh, lhl_ws_t ws, const double* dJ, int64_t ldj, c
  * relative residual is above tol, then up to `restart` steps of GMRES on A d = r
  * left-preconditioned by the shift's factorisation (each step one lhl_ldiv and one product
  * with A), stopping a column's cycle once its estimated residual is below 0.1 tol, and
- * x += d.  At most max_cycles cycles; columns at or below tol are left alone.  On return
- * dres holds every column's final relative residual, as for lhl_refine_tol.
- * host_check = 1: the host reads dres after each cycle (a stream synchronisation) and stops
- * once every column is at or below tol; 0: max_cycles cycles are launched without a host
+ * x += d.  At most max_cycles cycles; columns at or below tol are left alone, and so is a
+ * column whose residual did not at least halve over its last cycle (it is at the accuracy this
+ * preconditioner and FP64 allow for that shift; its last iterate stays).  On return dres holds
+ * every column's final relative residual, as for lhl_refine_tol.
+ * host_check = 1: the host reads which columns still refine after each cycle (a stream
+ * synchronisation) and stops once none does; 0: max_cycles cycles are launched without a host
  * round trip (finished columns skip their work), which a CUDA graph can capture.
  * 1 <= restart <= 32.  The Krylov basis, nrhs (restart + 1) n doubles, is kept in the
  * workspace: allocated by the first call that needs it, reused after.  With a complex shift

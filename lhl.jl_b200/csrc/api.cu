@@ -27,8 +27,8 @@ struct lhl_ws_s {
     unsigned long long *mhdr, *mcval, *mcrow;
     float* mgrows;
     // lhl_refine_gmres: Krylov bases, per-column state and activity, host copy of dres
-    double *gmV, *gmS, *gmA, *gmH;
-    size_t gmV_cap, gmS_cap, gmA_cap, gmH_cap;
+    double *gmV, *gmS, *gmA, *gmH, *gmP;
+    size_t gmV_cap, gmS_cap, gmA_cap, gmH_cap, gmP_cap;
     int probes;  // device timers in the reduction kernels (lhl_ws_set_probes)
     int f32;     // LHLWorkspace{Float32}: float values in the FP64 arrays, float shift arithmetic
     double* f32x;  // lhl_ldiv_f32: widened right-hand sides (grow-only)
@@ -71,7 +71,7 @@ static void ws_free(lhl_ws_t w)
     if (!w) return;
     void* ptrs[] = {w->F, w->Ht, w->scale, w->iscale, w->B0, w->part, w->tab, w->cand_v, w->cand_s, w->buf2, w->tsnap,
                     w->bsum, w->bfac, w->ipiv, w->perm, w->iperm, w->cand_i, w->bflag, w->err, w->bar,
-                    w->ptimes, w->mhdr, w->mcval, w->mcrow, w->mgrows, w->ybuf, w->zflags, w->linv, w->gmV, w->gmS, w->gmA, w->f32x};
+                    w->ptimes, w->mhdr, w->mcval, w->mcrow, w->mgrows, w->ybuf, w->zflags, w->linv, w->gmV, w->gmS, w->gmA, w->f32x, w->gmP};
     for (void* p : ptrs)
         if (p) cudaFree(p);
     if (w->gmH) cudaFreeHost(w->gmH);
@@ -777,6 +777,7 @@ int lhl_refine_gmres(lhl_shift_t sh, lhl_ws_t ws, const double* dJ, int64_t ldj,
     cudaError_t e = ws_grow(&ws->gmV, &ws->gmV_cap, (size_t)nr * (m + 1) * ne);
     if (e == cudaSuccess) e = ws_grow(&ws->gmS, &ws->gmS_cap, (size_t)nr * lhl::gm_state_doubles(m));
     if (e == cudaSuccess) e = ws_grow(&ws->gmA, &ws->gmA_cap, (size_t)nr);
+    if (e == cudaSuccess) e = ws_grow(&ws->gmP, &ws->gmP_cap, (size_t)nr);
     if (e == cudaSuccess && host_check && (ws->gmH_cap < (size_t)nr || !ws->gmH)) {
         if (ws->gmH) cudaFreeHost(ws->gmH);
         ws->gmH = nullptr;
@@ -792,16 +793,19 @@ int lhl_refine_gmres(lhl_shift_t sh, lhl_ws_t ws, const double* dJ, int64_t ldj,
         if (e == cudaSuccess) e = relres_any(sh, n, dR, ldx, dB, ldb, dres, nrhs, st);
         if (e != cudaSuccess) return LHL_ERR_CUDA;
         if (cyc == max_cycles) break;
+        // the columns that take this cycle: above tol and not stagnated
+        e = lhl::launch_gm_mark(dres, ws->gmP, ws->gmA, tol, cyc == 0, nr, st);
+        if (e != cudaSuccess) return LHL_ERR_CUDA;
         if (host_check) {
-            e = cudaMemcpyAsync(ws->gmH, dres, (size_t)nr * sizeof(double), cudaMemcpyDeviceToHost, st);
+            e = cudaMemcpyAsync(ws->gmH, ws->gmA, (size_t)nr * sizeof(double), cudaMemcpyDeviceToHost, st);
             if (e == cudaSuccess) e = cudaStreamSynchronize(st);
             if (e != cudaSuccess) return LHL_ERR_CUDA;
-            bool all = true;
-            for (int c = 0; c < nr && all; ++c) all = ws->gmH[c] <= tol;
-            if (all) break;
+            bool none = true;
+            for (int c = 0; c < nr && none; ++c) none = !(ws->gmH[c] > 0.5);
+            if (none) break;
         }
-        // z = W~^-1 r for the unconverged columns, then the cycle's Arnoldi steps
-        e = lhl::launch_ldiv(refine_ldiv_args(sh, ws, dR, ldx, rhs_per_shift, dres, tol), nr, st);
+        // z = W~^-1 r for those columns, then the cycle's Arnoldi steps
+        e = lhl::launch_ldiv(refine_ldiv_args(sh, ws, dR, ldx, rhs_per_shift, ws->gmA, 0.5), nr, st);
         if (e == cudaSuccess)
             e = lhl::launch_gm_begin(ne, m, dR, (int)(P * ldx), ws->gmV, ws->gmS, ws->gmA, dres, tol, nr, st);
         for (int j = 0; j < m && e == cudaSuccess; ++j) {

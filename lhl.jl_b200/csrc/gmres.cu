@@ -5,6 +5,7 @@
 //
 // Per cycle, for every column whose relative residual is still above tol:
 //   r = b - W x                    (residual kernel, FP64)
+//   the columns that take the cycle: above tol, and not stagnated (gm_mark_kernel)
 //   z = W~^-1 r                    (lhl_ldiv's kernels)
 //   v0 = z / beta, g = beta e1     (gm_begin_kernel)
 //   for j = 0 .. m-1, while the column is active:
@@ -43,8 +44,31 @@ __device__ __forceinline__ double block_sum_gm(double v, double* red)
     return s;
 }
 
-// Starts a cycle.  z = W~^-1 r is in R's column c.  Columns at or below tol (and NaN
-// residuals) sit the cycle out.
+// Which columns take the next cycle: those above tol (not NaN) whose relative residual at
+// least halved over the last cycle.  One that did not is at its attainable accuracy (its FP64
+// floor for this shift, or the limit of the preconditioner): it is marked (prev < 0) and sits
+// out every later cycle, keeping its last iterate.
+__global__ void gm_mark_kernel(const double* __restrict__ res, double* __restrict__ prev, double* __restrict__ act,
+                               double tol, int first, int nrhs)
+{
+    const int c = blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= nrhs) return;
+    const double rc = res[c];
+    bool go = rc > tol;
+    if (first) {
+        prev[c] = rc;
+    } else if (prev[c] < 0.0) {
+        go = false;
+    } else if (go && !(rc <= 0.5 * prev[c])) {
+        prev[c] = -1.0;
+        go = false;
+    } else {
+        prev[c] = rc;
+    }
+    act[c] = go ? 1.0 : 0.0;
+}
+
+// Starts a cycle for the columns gm_mark_kernel chose.  z = W~^-1 r is in R's column c.
 __global__ void __launch_bounds__(GT) gm_begin_kernel(int n, int m, const double* __restrict__ R, int ldr,
                                                       double* __restrict__ V, double* __restrict__ S,
                                                       double* __restrict__ act, const double* __restrict__ res,
@@ -54,11 +78,8 @@ __global__ void __launch_bounds__(GT) gm_begin_kernel(int n, int m, const double
     const int c = blockIdx.x;
     double* st = S + (size_t)c * gm_state_size(m);
     const double rc = res[c];
-    if (!(rc > tol)) {
-        if (threadIdx.x == 0) {
-            act[c] = 0.0;
-            st[2] = 0.0;
-        }
+    if (!(act[c] > 0.5)) {
+        if (threadIdx.x == 0) st[2] = 0.0;
         return;
     }
     const double* z = R + (size_t)c * ldr;
@@ -189,6 +210,14 @@ __global__ void __launch_bounds__(GT) gm_update_kernel(int n, int m, double* __r
 }
 
 size_t gm_state_doubles(int m) { return (size_t)gm_state_size(m); }
+
+cudaError_t launch_gm_mark(const double* res, double* prev, double* act, double tol, int first, int nrhs,
+                           cudaStream_t st)
+{
+    if (nrhs <= 0) return cudaSuccess;
+    gm_mark_kernel<<<(nrhs + 127) / 128, 128, 0, st>>>(res, prev, act, tol, first, nrhs);
+    return cudaGetLastError();
+}
 
 cudaError_t launch_gm_begin(int n, int m, const double* R, int ldr, double* V, double* S, double* act,
                             const double* res, double tol, int nrhs, cudaStream_t st)

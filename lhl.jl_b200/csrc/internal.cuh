@@ -188,6 +188,8 @@ cudaError_t launch_f64_to_f32(const double* src, int lds, float* dst, int ldd, i
 
 // GMRES-IR (gmres.cu)
 size_t gm_state_doubles(int m);
+cudaError_t launch_gm_mark(const double* res, double* prev, double* act, double tol, int first, int nrhs,
+                           cudaStream_t st);
 cudaError_t launch_gm_begin(int n, int m, const double* R, int ldr, double* V, double* S, double* act,
                             const double* res, double tol, int nrhs, cudaStream_t st);
 cudaError_t launch_gm_arnoldi(int n, int m, int j, double* R, int ldr, double* V, double* S, double* act, int nrhs,

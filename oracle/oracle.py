@@ -354,7 +354,8 @@ def gmres_ir(matvec, precond, b, x, tol, max_cycles=4, restart=8):
     W d = r, left-preconditioned by the factorisation (Carson and Higham, 2017), here with
     classical Gram-Schmidt applied twice.  A cycle starts while ||r|| / ||b|| > tol; its Arnoldi
     steps stop once |g_{j+1}| / beta <= min(0.5, 0.1 tol / (||r|| / ||b||)), at a breakdown, or
-    after `restart` steps.  Returns (x, relative residual, preconditioner applications).
+    after `restart` steps.  No new cycle starts once a cycle failed to halve the residual (the
+    attainable accuracy).  Returns (x, relative residual, preconditioner applications).
     Complex b / x: the same real algorithm on the realified system (an interleaved complex
     vector of n entries is a real vector of 2n; the real inner product is Re<v, w>)."""
     if np.iscomplexobj(b) or np.iscomplexobj(x):
@@ -373,11 +374,15 @@ def gmres_ir(matvec, precond, b, x, tol, max_cycles=4, restart=8):
     m = restart
     napply = 0
     rel = np.inf
+    prev = None
     for cyc in range(max_cycles + 1):
         r = b - matvec(x)
         rel = np.linalg.norm(r) / nb if nb > 0 else np.linalg.norm(r)
         if cyc == max_cycles or not rel > tol:
             break
+        if prev is not None and not rel <= 0.5 * prev:
+            break  # stagnated: the residual did not halve over the last cycle
+        prev = rel
         z = precond(r)
         napply += 1
         beta = np.linalg.norm(z)

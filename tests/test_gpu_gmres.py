@@ -239,3 +239,24 @@ def test_gmres_complex_resolvent_sweep(precision):
     for c in (0, S * rps - 1):
         W = s[c // rps] * np.eye(n) - J
         assert np.linalg.norm(B[:, c] - W @ Xh[:, c]) <= 1.0001e-10 * np.linalg.norm(B[:, c])
+
+
+def test_gmres_stagnated_columns_stop():
+    """tol below FP64's reach: every column stops refining once a cycle fails to halve its
+    residual, so 12 and 40 allowed cycles give bit-identical results, with or without the host
+    check, at a residual near the FP64 floor."""
+    torch, G = _mods()
+    n, S = 600, 4
+    J, g, Jd, ws, sh, B = problem(n, S, 1, 21, G.LHL_PREC_MIXED)
+    Bd = dev(B)
+    X0 = Bd.clone()
+    G.lhl_ldiv_(X0, sh, ws)
+    outs = []
+    for cyc, hc in ((12, True), (40, True), (40, False)):
+        X = X0.clone()
+        r = host(G.lhl_refine_gmres_(X, Jd, Bd, sh, ws, tol=1e-30, max_cycles=cyc, restart=4, host_check=hc))
+        outs.append((host(X), r))
+    for X, r in outs[1:]:
+        assert np.array_equal(X.view(np.int64), outs[0][0].view(np.int64))
+        assert np.array_equal(r.view(np.int64), outs[0][1].view(np.int64))
+    assert (outs[0][1] < 1e-12).all()

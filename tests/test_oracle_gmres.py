@@ -101,3 +101,12 @@ def test_gmres_ir_complex_realified():
     assert rel <= 1e-10
     assert np.linalg.norm(b - W @ x) <= 1.0001e-10 * np.linalg.norm(b)
     assert napply <= 8
+
+
+def test_gmres_ir_stops_at_its_attainable_accuracy():
+    """With a tolerance below FP64's reach the cycles stop once one fails to halve the
+    residual, far before max_cycles."""
+    W, b, mv, pc = weak_case(150, 4, 1e-4, 0.9)
+    x, rel, napply = O.gmres_ir(mv, pc, b, pc(b), 1e-30, max_cycles=40, restart=4)
+    assert rel < 1e-12
+    assert napply <= 6 * (1 + 4), napply
