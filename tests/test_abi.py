@@ -51,6 +51,22 @@ def test_null_handles_rejected_on_host():
     assert L.lhl_ws_create(4, 7, ctypes.byref(h)) == 1         # ArgumentError: precision
     L.lhl_ldiv.argtypes = [vp, vp, vp, ctypes.c_int64, ctypes.c_int64, ctypes.c_int64, vp]
     assert L.lhl_ldiv(vp(0), vp(0), vp(0), 1, 1, 1, vp(0)) == 1
+    # the later entry points refuse null handles the same way, before any device call
+    i64, i32, d = ctypes.c_int64, ctypes.c_int, ctypes.c_double
+    L.lhl_ldiv_f32.argtypes = [vp, vp, vp, i64, i64, i64, vp]
+    assert L.lhl_ldiv_f32(vp(0), vp(0), vp(0), 1, 1, 1, vp(0)) == 1
+    L.lhl_reduce_f32.argtypes = [vp, vp, i64, i32, vp]
+    assert L.lhl_reduce_f32(vp(0), vp(0), 1, 1, vp(0)) == 1
+    L.lhl_ws_import.argtypes = [vp] * 9
+    assert L.lhl_ws_import(*([vp(0)] * 9)) == 1
+    L.lhl_ws_set_probes.argtypes = [vp, i32]
+    assert L.lhl_ws_set_probes(vp(0), 1) == 1
+    L.lhl_ws_create_f32.argtypes = [i64, i32, ctypes.POINTER(vp)]
+    assert L.lhl_ws_create_f32(-1, 0, ctypes.byref(h)) == 2
+    assert L.lhl_ws_create_f32(4, 7, ctypes.byref(h)) == 1
+    L.lhl_refine_gmres.argtypes = [vp, vp, vp, i64, vp, i64, vp, i64, vp, vp, i64, i64, d, i32, i32, i32, vp]
+    assert L.lhl_refine_gmres(vp(0), vp(0), vp(0), 1, vp(0), 1, vp(0), 1, vp(0), vp(0), 1, 1, 1e-10, 1, 3, 1,
+                              vp(0)) == 1
 
 
 def test_configs_are_seeded_and_shaped():
