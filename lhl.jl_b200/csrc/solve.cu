@@ -693,7 +693,7 @@ __device__ double block_sum(double v, double* red)
     return s;
 }
 
-__global__ void __launch_bounds__(SOLVE_T) solve_batch_kernel(BatchDesc d, const double* __restrict__ J,
+__global__ void __launch_bounds__(SOLVE_T, 2) solve_batch_kernel(BatchDesc d, const double* __restrict__ J,
                                                               const double* __restrict__ B, double* __restrict__ X,
                                                               int R, const double* __restrict__ sig,
                                                               const double* __restrict__ tau, double tol,
