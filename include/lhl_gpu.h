@@ -126,6 +126,24 @@ int lhl_reduce_f32(lhl_ws_t ws, const float* dJ, int64_t ldj, int balance, void*
 int lhl_ldiv_f32(lhl_shift_t sh, lhl_ws_t ws, float* dX, int64_t ldx, int64_t nrhs, int64_t rhs_per_shift,
                  void* stream);
 
+/* ---- element type ComplexF64 (LHLWorkspace{ComplexF64}, test/core_tests.jl:241-249) -----
+ * lhl_ws_create_c128 makes a workspace for a complex J (FP64 form only; n <= 8192, else
+ * LHL_ERR_DIM).  Its factors and Ht (lhl_ws_view) are n x n interleaved complex (re, im
+ * pairs, ld n), scale / iscale real; lhl_ws_import takes arrays of that layout.  Replaces
+ * lhl_reduce!(ws, J, balance) for complex T (F:355-390; balancing F:299-340 and the pivot
+ * search F:470-477 on the modulus |z|; the unblocked ELMHES with the generic sweep F:466-538
+ * at every n, the path the reference takes below n = 768).  Its shifts are complex: only a
+ * shift object made by lhl_shift_create_complex serves it (LHL_ERR_ARG otherwise, F:2463-2465),
+ * through lhl_shift_complex / lhl_shift_batched_complex (real sigma, tau are converted).
+ * lhl_ldiv, lhl_applyZ, lhl_applyZinv, lhl_refine, lhl_refine_tol, lhl_refine_gmres and
+ * lhl_residual_norms take interleaved complex vectors and, for the refinements, a complex dJ
+ * (n x n interleaved, ld ldj complex elements); the solve is applyZinv!, the planar Hessenberg
+ * solve, applyZ! (F:3111-3121).  lhl_reduce and lhl_reduce_f32 on it are LHL_ERR_ARG. */
+int lhl_ws_create_c128(int64_t n, lhl_ws_t* ws);
+/* lhl_reduce!(ws, J, balance) for a complex J (dJ n x n interleaved complex, ld ldj complex
+ * elements); a workspace not made by lhl_ws_create_c128 is LHL_ERR_ARG. */
+int lhl_reduce_c128(lhl_ws_t ws, const double* dJ, int64_t ldj, int balance, void* stream);
+
 /* ---- shifts --------------------------------------------------------------------- */
 /* A batch of nshifts LHLShift{Float64}(n) objects (F:107-116). */
 int lhl_shift_create(int64_t n, int64_t nshifts, lhl_shift_t* sh);

@@ -33,6 +33,7 @@ struct lhl_ws_s {
     int f32;     // LHLWorkspace{Float32}: float values in the FP64 arrays, float shift arithmetic
     double* f32x;  // lhl_ldiv_f32: widened right-hand sides (grow-only)
     size_t f32x_cap;
+    int cj;        // LHLWorkspace{ComplexF64}: F, Ht, buf2 interleaved complex (cplxj.cu)
 };
 
 struct lhl_shift_s {
@@ -43,6 +44,7 @@ struct lhl_shift_s {
     int64_t po;
     uint8_t* swap;
     int32_t* info;
+    int cj;        // the slots were last loaded from a complex reduction: residuals take a complex J
 };
 
 struct lhl_batch_s {
@@ -161,6 +163,52 @@ int lhl_ws_create_f32(int64_t n, int precision, lhl_ws_t* out)
     return rc;
 }
 
+int lhl_ws_create_c128(int64_t n, lhl_ws_t* out)
+{
+    if (!out) return LHL_ERR_ARG;
+    *out = nullptr;
+    if (n < 0 || n > lhl::CJ_NMAX) return LHL_ERR_DIM;
+    lhl_ws_t w = new (std::nothrow) lhl_ws_s();
+    if (!w) return LHL_ERR_ALLOC;
+    memset(w, 0, sizeof(*w));
+    w->n = n;
+    w->precision = LHL_PREC_FP64;
+    w->cj = 1;
+    w->grid = lhl::cj_grid_size((int)n);
+    w->limit_ns = 2000000000ull;
+    const size_t nn = (size_t)n * (size_t)n;
+    cudaError_t e = cudaSuccess;
+#define A_(p, cnt) if (e == cudaSuccess) e = dalloc(&w->p, (cnt))
+    A_(F, 2 * nn);
+    A_(Ht, 2 * nn);
+    A_(buf2, 2 * nn);
+    A_(scale, n);
+    A_(iscale, n);
+    A_(bsum, 2 * (size_t)n);
+    A_(bfac, n);
+    A_(ipiv, n > 2 ? n - 2 : 1);
+    A_(perm, n);
+    A_(iperm, n);
+    A_(cand_v, w->grid);
+    A_(cand_i, w->grid);
+    A_(bflag, 4);
+    A_(err, 4);
+    A_(bar, 4);
+    A_(ptimes, 24);
+    w->ycap = 256;
+    A_(ybuf, (size_t)n * w->ycap);
+#undef A_
+    if (e == cudaSuccess) e = cudaMemset(w->err, 0, 4 * sizeof(int));
+    if (e == cudaSuccess) e = cudaMemset(w->ptimes, 0, 24 * sizeof(unsigned long long));
+    if (e == cudaSuccess) e = cudaMemset(w->Ht, 0, (nn ? 2 * nn : 1) * sizeof(double));
+    if (e != cudaSuccess) {
+        ws_free(w);
+        return e == cudaErrorMemoryAllocation ? LHL_ERR_ALLOC : LHL_ERR_CUDA;
+    }
+    *out = w;
+    return LHL_OK;
+}
+
 int lhl_ws_destroy(lhl_ws_t ws)
 {
     if (!ws) return LHL_ERR_ARG;
@@ -240,6 +288,7 @@ static int round_reduction_f32(lhl_ws_t ws, cudaStream_t st)
 int lhl_reduce(lhl_ws_t ws, const double* dJ, int64_t ldj, int balance, void* stream)
 {
     if (!ws || (!dJ && ws->n > 0)) return LHL_ERR_ARG;
+    if (ws->cj) return LHL_ERR_ARG;  // a complex workspace takes a complex J (lhl_reduce_c128)
     const int64_t n = ws->n;
     if (ldj < n || ldj < 1) return LHL_ERR_DIM;
     if (n == 0) return LHL_OK;
@@ -256,6 +305,7 @@ int lhl_reduce(lhl_ws_t ws, const double* dJ, int64_t ldj, int balance, void* st
 int lhl_reduce_f32(lhl_ws_t ws, const float* dJ, int64_t ldj, int balance, void* stream)
 {
     if (!ws || (!dJ && ws->n > 0)) return LHL_ERR_ARG;
+    if (ws->cj) return LHL_ERR_ARG;
     const int64_t n = ws->n;
     if (ldj < n || ldj < 1) return LHL_ERR_DIM;
     if (n == 0) return LHL_OK;
@@ -264,6 +314,42 @@ int lhl_reduce_f32(lhl_ws_t ws, const float* dJ, int64_t ldj, int balance, void*
     int rc = reduce_loaded(ws, balance, st);
     if (rc == LHL_OK && ws->f32) rc = round_reduction_f32(ws, st);
     return rc;
+}
+
+int lhl_reduce_c128(lhl_ws_t ws, const double* dJ, int64_t ldj, int balance, void* stream)
+{
+    if (!ws || (!dJ && ws->n > 0)) return LHL_ERR_ARG;
+    if (!ws->cj) return LHL_ERR_ARG;  // a complex J needs a workspace made by lhl_ws_create_c128
+    const int64_t n = ws->n;
+    if (ldj < n || ldj < 1) return LHL_ERR_DIM;
+    if (n == 0) return LHL_OK;
+    cudaStream_t st = (cudaStream_t)stream;
+    cudaError_t e = cudaMemcpy2DAsync(ws->F, n * 2 * sizeof(double), dJ, ldj * 2 * sizeof(double),
+                                      n * 2 * sizeof(double), n, cudaMemcpyDeviceToDevice, st);
+    if (e == cudaSuccess) e = cudaMemsetAsync(ws->bar, 0, sizeof(unsigned int), st);
+    if (e == cudaSuccess) e = cudaMemsetAsync(ws->err, 0, sizeof(int), st);
+    if (e == cudaSuccess && !balance) e = lhl::launch_fill_ones(ws->scale, ws->iscale, (int)n, st);
+    if (e != cudaSuccess) return LHL_ERR_CUDA;
+    lhl::CjArgs a;
+    memset(&a, 0, sizeof(a));
+    a.n = (int)n;
+    a.A = ws->F;
+    a.B = ws->buf2;
+    a.Ht = ws->Ht;
+    a.ipiv = ws->ipiv;
+    a.perm = ws->perm;
+    a.iperm = ws->iperm;
+    a.scale = ws->scale;
+    a.iscale = ws->iscale;
+    a.bsum = ws->bsum;
+    a.bfac = ws->bfac;
+    a.bflag = ws->bflag;
+    a.cand_v = ws->cand_v;
+    a.cand_i = ws->cand_i;
+    a.bar = ws->bar;
+    a.err = ws->err;
+    a.limit_ns = ws->limit_ns;
+    return cuda_status(lhl::launch_reduce_cj(a, balance ? 1 : 0, st));
 }
 
 static int reduce_loaded(lhl_ws_t ws, int balance, cudaStream_t st)
@@ -351,7 +437,7 @@ int lhl_ws_import(lhl_ws_t ws, const double* dfactors, const double* dHt, const 
     if (n == 0) return LHL_OK;
     if (!dfactors || !dHt || !dperm || !diperm || !dscale || !discale || (n > 2 && !dipiv)) return LHL_ERR_ARG;
     cudaStream_t st = (cudaStream_t)stream;
-    const size_t nn = (size_t)n * (size_t)n;
+    const size_t nn = (size_t)n * (size_t)n * (ws->cj ? 2 : 1);  // complex reduction: interleaved pairs
     cudaError_t e = cudaMemcpyAsync(ws->F, dfactors, nn * sizeof(double), cudaMemcpyDeviceToDevice, st);
     if (e == cudaSuccess) e = cudaMemcpyAsync(ws->Ht, dHt, nn * sizeof(double), cudaMemcpyDeviceToDevice, st);
     if (e == cudaSuccess && n > 2)
@@ -440,9 +526,11 @@ static int shift_run(lhl_shift_t sh, lhl_ws_t ws, int64_t s0, int64_t count, cud
 {
     cudaError_t e;
     if (sh->cplx && ws->f32) return LHL_ERR_ARG;  // complex shifts need a Float64 workspace
+    sh->cj = ws->cj;
     if (sh->cplx) {
         e = lhl::launch_shift_lu_cplx((int)ws->n, ws->Ht, (int)ws->n, sh->sigma + 2 * s0, sh->tau + 2 * s0, (int)s0,
-                                      (int)count, sh->Gt, (int)sh->ldg, (int)sh->po, sh->swap, sh->rdiag, sh->info, st);
+                                      (int)count, sh->Gt, (int)sh->ldg, (int)sh->po, sh->swap, sh->rdiag, sh->info, st,
+                                      ws->cj);
         return cuda_status(e);
     }
     e = lhl::launch_shift_lu((int)ws->n, ws->Ht, (int)ws->n, sh->sigma + s0, sh->tau + s0, (int)s0, (int)count,
@@ -455,6 +543,7 @@ static int shift_run(lhl_shift_t sh, lhl_ws_t ws, int64_t s0, int64_t count, cud
 static int shift_args(lhl_shift_t sh, lhl_ws_t ws, int64_t s0, int64_t count)
 {
     if (!sh || !ws) return LHL_ERR_ARG;
+    if (ws->cj && !sh->cplx) return LHL_ERR_ARG;  // an LHLShift{Float64} cannot serve a ComplexF64 workspace (F:2463-2465)
     if (sh->n != ws->n) return LHL_ERR_DIM;
     if (s0 < 0 || count < 0 || s0 + count > sh->nshifts) return LHL_ERR_DIM;
     return LHL_OK;
@@ -538,9 +627,11 @@ static int ldiv_common(lhl_shift_t sh, lhl_ws_t ws, double* dX, int64_t ldx, int
     if (!dX) return LHL_ERR_ARG;
     if (ldx < n) return LHL_ERR_DIM;
     if (n > 8192) return LHL_ERR_DIM;
+    if (ws->cj && sh && !sh->cplx) return LHL_ERR_ARG;
     lhl::LdivArgs a;
     memset(&a, 0, sizeof(a));
     a.n = (int)n;
+    a.cj = ws->cj;
     a.F = ws->F;
     a.ldf = (int)n;
     a.perm = ws->perm;
@@ -627,6 +718,9 @@ static cudaError_t resid_any(lhl_shift_t sh, int64_t n, const double* dJ, int64_
                              const double* dX, int64_t ldx, double* dR, int64_t ldr, int64_t nrhs, int64_t rps,
                              cudaStream_t st, const double* done, double tol)
 {
+    if (sh->cplx && sh->cj)  // complex J (the slots came from a complex reduction)
+        return lhl::launch_residual_cj((int)n, dJ, (int)ldj, dB, (int)ldb, dX, (int)ldx, dR, (int)ldr, (int)nrhs,
+                                       (int)rps, sh->sigma, sh->tau, st, done, tol);
     if (sh->cplx)
         return lhl::launch_residual_cplx((int)n, dJ, (int)ldj, dB, (int)ldb, dX, (int)ldx, dR, (int)ldr, (int)nrhs,
                                          (int)rps, sh->sigma, sh->tau, st, done, tol);
@@ -652,6 +746,7 @@ int lhl_refine(lhl_shift_t sh, lhl_ws_t ws, const double* dJ, int64_t ldj, const
                int64_t ldx, double* dR, int64_t nrhs, int64_t rhs_per_shift, int steps, void* stream)
 {
     if (!sh || !ws) return LHL_ERR_ARG;
+    if (ws->cj && !sh->cplx) return LHL_ERR_ARG;
     const int64_t n = ws->n;
     if (sh->n != n) return LHL_ERR_DIM;
     if (rhs_per_shift < 1 || steps < 0) return LHL_ERR_ARG;
@@ -679,6 +774,7 @@ static lhl::LdivArgs refine_ldiv_args(lhl_shift_t sh, lhl_ws_t ws, double* dR, i
     lhl::LdivArgs a;
     memset(&a, 0, sizeof(a));
     a.n = (int)ws->n;
+    a.cj = ws->cj;
     a.F = ws->F;
     a.ldf = (int)ws->n;
     a.perm = ws->perm;
@@ -714,6 +810,7 @@ static int refine_args_check(lhl_shift_t sh, lhl_ws_t ws, const double* dJ, int6
                              int64_t nrhs, int64_t rhs_per_shift, double tol, bool bad_count)
 {
     if (!sh || !ws) return LHL_ERR_ARG;
+    if (ws->cj && !sh->cplx) return LHL_ERR_ARG;
     const int64_t n = ws->n;
     if (sh->n != n) return LHL_ERR_DIM;
     if (rhs_per_shift < 1 || bad_count || !(tol >= 0.0)) return LHL_ERR_ARG;

@@ -109,6 +109,20 @@ __device__ __forceinline__ void warp_argmax(double& a, int& ia)
     }
 }
 
+// Balancing decision for one index (F:313-327): the power-of-two factor f that brings the
+// column and row norms c, r within a factor 2, and whether it reduces c + r below 0.95 of
+// its value.  The loops are bounded by the exponent range.
+__device__ __forceinline__ bool balance_decide(double c, double r, double& f)
+{
+    if (c == 0.0 || r == 0.0) return false;
+    f = 1.0;
+    const double s = c + r;
+    int guard = 0;
+    while (c < r / 2.0 && guard < 4200) { c *= 2.0; r /= 2.0; f *= 2.0; ++guard; }
+    while (c >= 2.0 * r && guard < 8400) { c /= 2.0; r *= 2.0; f /= 2.0; ++guard; }
+    return c + r < 0.95 * s;
+}
+
 }  // namespace lhl
 
 // ---- TMA (cp.async.bulk.tensor) and mbarrier helpers -------------------------------------

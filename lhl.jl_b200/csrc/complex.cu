@@ -15,46 +15,24 @@
 // ComplexF64, without its rescaling near overflow and underflow); rdiag = 1 / U[j,j] by the
 // same division.  The CPU oracle uses the same operations in the same order, so the device
 // shift LU is bit-identical to it.
+#include "cplx.cuh"
 #include "internal.cuh"
 
 namespace lhl {
 
-struct dc {
-    double re, im;
-};
-
-__device__ __forceinline__ dc cmul(dc a, dc b)
-{
-    return {dsub(dmul(a.re, b.re), dmul(a.im, b.im)), dadd(dmul(a.re, b.im), dmul(a.im, b.re))};
-}
-__device__ __forceinline__ dc csub(dc a, dc b) { return {dsub(a.re, b.re), dsub(a.im, b.im)}; }
-__device__ __forceinline__ dc cadd(dc a, dc b) { return {dadd(a.re, b.re), dadd(a.im, b.im)}; }
-__device__ __forceinline__ dc cscale(dc a, double s) { return {dmul(a.re, s), dmul(a.im, s)}; }
-__device__ __forceinline__ double cmag(dc a) { return dadd(fabs(a.re), fabs(a.im)); }
-
-__device__ __forceinline__ double cdiv2(double a, double b, double c, double d, double r, double t)
-{
-    if (r != 0.0) {
-        const double br = dmul(b, r);
-        return br != 0.0 ? dmul(dadd(a, br), t) : dadd(dmul(a, t), dmul(dmul(b, t), r));
-    }
-    return dmul(dadd(a, dmul(d, __ddiv_rn(b, c))), t);
-}
-
-// Baudin & Smith, "A robust complex division in Scilab" (2012).
-__device__ __forceinline__ dc cdiv(dc x, dc y)
-{
-    const double a = x.re, b = x.im, c = y.re, d = y.im;
-    if (fabs(d) <= fabs(c)) {
-        const double r = __ddiv_rn(d, c), t = __ddiv_rn(1.0, dadd(c, dmul(d, r)));
-        return {cdiv2(a, b, c, d, r, t), cdiv2(b, -a, c, d, r, t)};
-    }
-    const double r = __ddiv_rn(c, d), t = __ddiv_rn(1.0, dadd(d, dmul(c, r)));
-    return {cdiv2(b, a, d, c, r, t), -cdiv2(a, -b, d, c, r, t)};
-}
-
 // ---- shift LU, one CTA per shift (the real kernel's structure, shift.cu) ----
-template <int T, int E>
+// HV = double: complex shifts on a real Ht; HV = dc: a complex reduction's Ht (interleaved).
+__device__ __forceinline__ void ht_load(const double* Ht, int ldh, int j, int k, double& v) { v = M1(Ht, ldh, j, k); }
+__device__ __forceinline__ void ht_load(const double* Ht, int ldh, int j, int k, dc& v)
+{
+    const double2 w = reinterpret_cast<const double2*>(Ht)[(size_t)(k - 1) * ldh + (j - 1)];
+    v = {w.x, w.y};
+}
+template <class HV> __device__ __forceinline__ HV hzero();
+template <> __device__ __forceinline__ double hzero<double>() { return 0.0; }
+template <> __device__ __forceinline__ dc hzero<dc>() { return {0.0, 0.0}; }
+
+template <int T, int E, class HV>
 __global__ void __launch_bounds__(T) shift_lu_cplx_kernel(int n, const double* __restrict__ Ht, int ldh,
                                                           const double* __restrict__ sig, const double* __restrict__ tau_,
                                                           int s0, double* __restrict__ Gt_all, int ldg, int po,
@@ -74,18 +52,22 @@ __global__ void __launch_bounds__(T) shift_lu_cplx_kernel(int n, const double* _
     __shared__ int s_info;
 
     dc r[E];
-    double h[E];     // Ht[j, k+1] for the current step
-    double hsub[E];  // Ht[j, j+1]: the subdiagonal of the step this thread decides
+    HV h[E];     // Ht[j, k+1] for the current step
+    HV hsub[E];  // Ht[j, j+1]: the subdiagonal of the step this thread decides
 #pragma unroll
     for (int e = 0; e < E; ++e) {
         const int j = 1 + t + e * T;
-        r[e] = (j <= n) ? cscale(tau, M1(Ht, ldh, j, 1)) : dc{0.0, 0.0};
+        HV h1 = hzero<HV>();
+        if (j <= n) ht_load(Ht, ldh, j, 1, h1);
+        r[e] = (j <= n) ? tmul(tau, h1) : dc{0.0, 0.0};
         if (j == 1) r[e] = cadd(r[e], sigma);
-        h[e] = (j <= n && n >= 2) ? M1(Ht, ldh, j, 2) : 0.0;
-        hsub[e] = (j + 1 <= n) ? M1(Ht, ldh, j, j + 1) : 0.0;
+        h[e] = hzero<HV>();
+        if (j <= n && n >= 2) ht_load(Ht, ldh, j, 2, h[e]);
+        hsub[e] = hzero<HV>();
+        if (j + 1 <= n) ht_load(Ht, ldh, j, j + 1, hsub[e]);
     }
-    auto decide = [&](int k, dc a, double hs) {
-        const dc b = cscale(tau, hs);
+    auto decide = [&](int k, dc a, HV hs) {
+        const dc b = tmul(tau, hs);
         const bool sw = cmag(b) > cmag(a);
         dc l;
         if (sw) l = cdiv(a, b);
@@ -115,11 +97,12 @@ __global__ void __launch_bounds__(T) shift_lu_cplx_kernel(int n, const double* _
             M1(Gt, ldg, po + k, k + 1) = l.im;
             if (!sw && a.re == 0.0 && a.im == 0.0 && s_info == 0) s_info = k;
         }
-        double hn[E];
+        HV hn[E];
 #pragma unroll
         for (int e = 0; e < E; ++e) {
             const int j = 1 + t + e * T;
-            hn[e] = (j >= k + 1 && j <= n && k + 2 <= n) ? M1(Ht, ldh, j, k + 2) : 0.0;
+            hn[e] = hzero<HV>();
+            if (j >= k + 1 && j <= n && k + 2 <= n) ht_load(Ht, ldh, j, k + 2, hn[e]);
         }
 #pragma unroll
         for (int e = 0; e < E; ++e) {
@@ -127,7 +110,7 @@ __global__ void __launch_bounds__(T) shift_lu_cplx_kernel(int n, const double* _
             if (j >= k + 1 && j <= n) {
                 dc gk;
                 if (sw) {
-                    const dc g = cscale(tau, h[e]);
+                    const dc g = tmul(tau, h[e]);
                     gk = g;
                     dc rj = csub(r[e], cmul(l, g));
                     if (j == k + 1) {
@@ -138,7 +121,7 @@ __global__ void __launch_bounds__(T) shift_lu_cplx_kernel(int n, const double* _
                 } else {
                     const dc rj = r[e];
                     gk = rj;
-                    dc rn = csub(cscale(tau, h[e]), cmul(l, rj));
+                    dc rn = csub(tmul(tau, h[e]), cmul(l, rj));
                     if (j == k + 1) rn = cadd(rn, sigma); // r[k+1] += sigma
                     r[e] = rn;
                 }
@@ -172,10 +155,17 @@ __global__ void __launch_bounds__(T) shift_lu_cplx_kernel(int n, const double* _
 
 cudaError_t launch_shift_lu_cplx(int n, const double* Ht, int ldh, const double* sig, const double* tau, int s0,
                                  int count, double* Gt, int ldg, int po, uint8_t* swp, double* rd, int32_t* info,
-                                 cudaStream_t st)
+                                 cudaStream_t st, int ht_complex)
 {
     if (count <= 0 || n <= 0) return cudaSuccess;
-#define L_(T, E) shift_lu_cplx_kernel<T, E><<<count, T, 0, st>>>(n, Ht, ldh, sig, tau, s0, Gt, ldg, po, swp, rd, info)
+#define L_(T, E)                                                                                                  \
+    do {                                                                                                          \
+        if (ht_complex)                                                                                           \
+            shift_lu_cplx_kernel<T, E, dc><<<count, T, 0, st>>>(n, Ht, ldh, sig, tau, s0, Gt, ldg, po, swp, rd, info); \
+        else                                                                                                      \
+            shift_lu_cplx_kernel<T, E, double><<<count, T, 0, st>>>(n, Ht, ldh, sig, tau, s0, Gt, ldg, po, swp, rd,  \
+                                                                    info);                                        \
+    } while (0)
     if (n <= 256) L_(256, 1);
     else if (n <= 1024) L_(512, 2);
     else if (n <= 2048) L_(512, 4);

@@ -1,0 +1,615 @@
+// cplxj.cu -- LHLWorkspace{ComplexF64}: the reduction of a complex J and the solves on it.
+//
+//   * balancing (F:299-340) with the complex modulus |z| = hypot(re, im) (cplx.cuh);
+//   * the unblocked ELMHES reduction (F:466-501) with the generic paired sweep (F:508-538),
+//     the path the reference takes for ComplexF64 below _lhl_block_min = 768 (F:703-705);
+//     at and above 768 the reference switches to its blocked form, whose pivots are the
+//     unblocked ones and whose factors agree with them to rounding (test/threading.jl:58-79);
+//     this build keeps the unblocked order at every n;
+//   * Ht = H transposed (F:2005-2061) and perm / iperm (F:376-387);
+//   * lhl_ldiv! on the complex reduction (F:3111-3121): applyZinv! (gather with the real
+//     iscale, the generic L^-1 sweep F:2151-2195), the planar Hessenberg solve (complex.cu),
+//     applyZ! (the generic L sweep F:2199-2243, scatter with scale);
+//   * the residual of lhl_refine! with a complex J (F:3144-3157).
+//
+// Layout: J, factors and Ht are n x n interleaved complex (re, im pairs, leading dimension n),
+// as a CuArray{ComplexF64}; scale and iscale are real.  The complex shift LU on the complex
+// Ht is complex.cu's kernel with a complex Ht.
+//
+// The reduction is one cooperative launch, one thread per row, double-buffered like the real
+// unblocked kernel (reduce.cu): step k reads the matrix of step k-1 with rows and columns
+// k+1 <-> p swapped on the fly and writes the other buffer, so a step needs one grid barrier
+// (the pivot search).  Every element sees the reference's complex operations in its order.
+#include "cplx.cuh"
+#include "internal.cuh"
+
+namespace lhl {
+
+constexpr int CJT = 256;
+constexpr int CJW = CJT / 32;
+
+__device__ __forceinline__ dc ldc(const double* A, int ld, int i, int j)
+{
+    const double2 w = reinterpret_cast<const double2*>(A)[(size_t)(j - 1) * ld + (i - 1)];
+    return {w.x, w.y};
+}
+__device__ __forceinline__ void stc(double* A, int ld, int i, int j, dc v)
+{
+    reinterpret_cast<double2*>(A)[(size_t)(j - 1) * ld + (i - 1)] = make_double2(v.re, v.im);
+}
+
+// every CTA reads all CTA candidates and reduces them (first max)
+__device__ __forceinline__ void cj_combine(const CjArgs& a, int* s_p, double* s_red, int* s_redi)
+{
+    const int t = threadIdx.x;
+    double v = 0.0;
+    int vi = 0;
+    for (int c = t; c < (int)gridDim.x; c += CJT) {
+        const int ci = ((volatile int*)a.cand_i)[c];
+        const double cv = ((volatile double*)a.cand_v)[c];
+        argmax_combine(v, vi, cv, ci);
+    }
+    warp_argmax(v, vi);
+    if ((t & 31) == 0) {
+        s_red[t >> 5] = v;
+        s_redi[t >> 5] = vi;
+    }
+    __syncthreads();
+    if (t == 0) {
+        double bv = 0.0;
+        int bi = 0;
+        for (int w = 0; w < CJW; ++w) argmax_combine(bv, bi, s_red[w], s_redi[w]);
+        *s_p = bi;
+    }
+    __syncthreads();
+}
+
+__device__ __forceinline__ void cj_publish(const CjArgs& a, double v, int vi, double* s_red, int* s_redi)
+{
+    warp_argmax(v, vi);
+    const int t = threadIdx.x;
+    if ((t & 31) == 0) {
+        s_red[t >> 5] = v;
+        s_redi[t >> 5] = vi;
+    }
+    __syncthreads();
+    if (t == 0) {
+        double bv = 0.0;
+        int bi = 0;
+        for (int w = 0; w < CJW; ++w) argmax_combine(bv, bi, s_red[w], s_redi[w]);
+        a.cand_v[blockIdx.x] = bv;
+        a.cand_i[blockIdx.x] = bi;
+    }
+    __syncthreads();
+}
+
+// Balancing (F:299-340), organised as the real kernel's: per sweep (1) every index's
+// column and row sums of moduli without the diagonal, each summed in the reference's order
+// by one thread; (2) CTA 0 walks i = 1..n in order taking the reference's decision, the
+// sums of later indices patched for an index that scales; (3) all CTAs apply the sweep's
+// power-of-two factors (exact on both parts).
+__device__ bool cj_balance(const CjArgs& a, GridBarrier& gb)
+{
+    const int n = a.n;
+    double* A = a.A;
+    const int gt = blockIdx.x * CJT + threadIdx.x;
+    const int gsz = gridDim.x * CJT;
+    for (int i = gt; i < n; i += gsz) {
+        a.scale[i] = 1.0;
+        a.iscale[i] = 1.0;
+    }
+    __shared__ int s_first;
+    __shared__ double s_f;
+    for (int sweep = 0; sweep < 20; ++sweep) {
+        for (int i = 1 + gt; i <= n; i += gsz) {
+            double c = 0.0, r = 0.0;
+            for (int j = 1; j <= n; ++j) {
+                if (j == i) continue;
+                c = dadd(c, cabs_h(ldc(A, n, j, i)));
+                r = dadd(r, cabs_h(ldc(A, n, i, j)));
+            }
+            a.bsum[i - 1] = c;
+            a.bsum[n + i - 1] = r;
+            a.bfac[i - 1] = 1.0;
+        }
+        if (gt == 0) a.bflag[0] = 0;
+        if (!gb.sync()) return false;
+        if (blockIdx.x == 0) {
+            int base = 1;
+            while (base <= n) {
+                if (threadIdx.x == 0) s_first = 0x7fffffff;
+                __syncthreads();
+                const int i = base + threadIdx.x;
+                double f = 1.0;
+                if (i <= n && balance_decide(a.bsum[i - 1], a.bsum[n + i - 1], f)) atomicMin(&s_first, i);
+                __syncthreads();
+                const int si = s_first;
+                if (si == 0x7fffffff) {
+                    base += CJT;
+                    continue;
+                }
+                if (i == si) {
+                    s_f = f;
+                    a.bflag[0] = 1;
+                }
+                __syncthreads();
+                const double fs = s_f;
+                for (int m = si + 1 + threadIdx.x; m <= n; m += CJT) {
+                    const double vr = cabs_h(ldc(A, n, si, m));
+                    const double vc = cabs_h(ldc(A, n, m, si));
+                    a.bsum[m - 1] = (a.bsum[m - 1] - vr) + vr / fs;
+                    a.bsum[n + m - 1] = (a.bsum[n + m - 1] - vc) + vc * fs;
+                }
+                if (threadIdx.x == 0) {
+                    a.bfac[si - 1] = fs;
+                    a.scale[si - 1] *= fs;
+                    a.iscale[si - 1] /= fs;
+                }
+                __syncthreads();
+                base = si + 1;
+            }
+        }
+        if (!gb.sync()) return false;
+        const int scaled = ((volatile int*)a.bflag)[0];
+        if (!scaled) break;
+        for (size_t e = gt; e < (size_t)n * n; e += gsz) {
+            const int i = (int)(e % n), j = (int)(e / n);
+            const double fi = a.bfac[i], fj = a.bfac[j];
+            if (fi != 1.0 || fj != 1.0) {
+                A[2 * e] = (A[2 * e] / fi) * fj;
+                A[2 * e + 1] = (A[2 * e + 1] / fi) * fj;
+            }
+        }
+        if (!gb.sync()) return false;
+    }
+    return true;
+}
+
+// Unblocked ELMHES with the generic paired sweep (F:466-538), one thread per row.
+__device__ bool cj_unblocked(const CjArgs& a, GridBarrier& gb, dc* s_l)
+{
+    const int n = a.n;
+    double* buf[2] = {a.A, a.B};
+    __shared__ double s_red[CJW];
+    __shared__ int s_redi[CJW];
+    __shared__ int s_p;
+    const int gt = blockIdx.x * CJT + threadIdx.x;
+    const int i = gt + 1;  // this thread's row
+    {
+        double v = 0.0;
+        int vi = 0;
+        if (i >= 2 && i <= n) { v = cabs_h(ldc(a.A, n, i, 1)); vi = i; }
+        cj_publish(a, v, vi, s_red, s_redi);
+    }
+    if (!gb.sync()) return false;
+    for (int k = 1; k <= n - 2; ++k) {
+        const double* R = buf[(k - 1) & 1];
+        double* W = buf[k & 1];
+        cj_combine(a, &s_p, s_red, s_redi);
+        const int p = (s_p >= k + 1 && s_p <= n) ? s_p : k + 1;
+        if (gt == 0) a.ipiv[k - 1] = p;
+        auto sw = [&](int r) { return r == k + 1 ? p : (r == p ? k + 1 : r); };
+        const dc piv = ldc(R, n, p, k);
+        const bool pz = ciszero(piv);
+        // multipliers l_j = A'[j,k] / piv (F:489-491), j = k+2..n
+        for (int j = k + 2 + threadIdx.x; j <= n; j += CJT) {
+            const dc v = ldc(R, n, sw(j), k);
+            s_l[j - 1] = pz ? v : cdiv(v, piv);
+        }
+        __syncthreads();
+        double cand = 0.0;
+        int candi = 0;
+        if (i <= n) {
+            const int si = sw(i);
+            dc ck = ldc(R, n, si, k);
+            if (!pz && i >= k + 2) ck = s_l[i - 1];
+            stc(W, n, i, k, ck);
+            dc ck1 = ldc(R, n, si, p);
+            if (pz) {
+                // step skipped (F:488): rows and columns still carry the interchange
+                for (int j = k + 2; j <= n; ++j) stc(W, n, i, j, ldc(R, n, si, sw(j)));
+                stc(W, n, i, k + 1, ck1);
+            } else {
+                const dc pk = ldc(R, n, p, p);
+                const bool low = i >= k + 2;
+                const dc li = low ? s_l[i - 1] : dc{0.0, 0.0};
+                if (low && !ciszero(pk)) ck1 = csub(ck1, cmul(li, pk));  // F:492-496
+                int j = k + 2;
+                while (j + 1 <= n) {  // column pairs (F:515-528)
+                    const int sj = sw(j), sj1 = sw(j + 1);
+                    dc v0 = ldc(R, n, si, sj), v1 = ldc(R, n, si, sj1);
+                    if (low) {
+                        v0 = csub(v0, cmul(li, ldc(R, n, p, sj)));
+                        v1 = csub(v1, cmul(li, ldc(R, n, p, sj1)));
+                    }
+                    stc(W, n, i, j, v0);
+                    stc(W, n, i, j + 1, v1);
+                    ck1 = cadd(ck1, cadd(cmul(s_l[j - 1], v0), cmul(s_l[j], v1)));
+                    j += 2;
+                }
+                if (j <= n) {  // last single column (F:529-536)
+                    const int sj = sw(j);
+                    dc v0 = ldc(R, n, si, sj);
+                    if (low) v0 = csub(v0, cmul(li, ldc(R, n, p, sj)));
+                    stc(W, n, i, j, v0);
+                    ck1 = cadd(ck1, cmul(s_l[j - 1], v0));
+                }
+                stc(W, n, i, k + 1, ck1);
+            }
+            if (i >= k + 2) { cand = cabs_h(ck1); candi = i; }
+        }
+        cj_publish(a, cand, candi, s_red, s_redi);
+        if (!gb.sync()) return false;
+    }
+    return true;
+}
+
+__global__ void __launch_bounds__(CJT, 1) cj_reduce_kernel(CjArgs a, int balance)
+{
+    extern __shared__ double2 cj_dyn[];
+    GridBarrier gb{a.bar, a.err, a.limit_ns, 0, nullptr};
+    if (balance && !cj_balance(a, gb)) return;
+    if (a.n >= 3) cj_unblocked(a, gb, reinterpret_cast<dc*>(cj_dyn));
+}
+
+__global__ void cj_init_kernel(int n, int64_t* ipiv, double* cand_v, int* cand_i, int ncand)
+{
+    for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < n - 2; k += gridDim.x * blockDim.x) ipiv[k] = k + 2;
+    for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < ncand; c += gridDim.x * blockDim.x) {
+        cand_v[c] = 0.0;
+        cand_i[c] = 0;
+    }
+}
+
+// Final assembly: column j from buffer j&1 (columns n-1, n from the last step's buffer) with
+// the interchanges of steps j+1..n-2 applied (F:480-485).  One CTA per column.
+__global__ void __launch_bounds__(CJT) cj_assemble_kernel(int n, double* A, const double* B2, const int64_t* ipiv)
+{
+    extern __shared__ double2 col[];
+    const int j = blockIdx.x + 1;
+    if (j > n) return;
+    const double* src;
+    int from;
+    if (j <= n - 2) {
+        src = (j & 1) ? B2 : A;
+        from = j + 1;
+    } else {
+        const int kl = n - 2;
+        src = (kl >= 1 && (kl & 1)) ? B2 : A;
+        from = n - 1;
+    }
+    const double2* s2 = reinterpret_cast<const double2*>(src) + (size_t)(j - 1) * n;
+    for (int i = threadIdx.x; i < n; i += CJT) col[i] = s2[i];
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        for (int k = from; k <= n - 2; ++k) {
+            const int p = (int)ipiv[k - 1];
+            if (p > k + 1 && p <= n) {
+                const double2 t = col[k];
+                col[k] = col[p - 1];
+                col[p - 1] = t;
+            }
+        }
+    }
+    __syncthreads();
+    double2* d2 = reinterpret_cast<double2*>(A) + (size_t)(j - 1) * n;
+    for (int i = threadIdx.x; i < n; i += CJT) d2[i] = col[i];
+}
+
+// Ht[j,i] = A[i,j] for i <= j+1, zero elsewhere (F:2005-2061); 32 x 32 tiles.
+__global__ void cj_ht_kernel(int n, const double* __restrict__ A, double* __restrict__ Ht)
+{
+    __shared__ double2 tile[32][33];
+    const double2* A2 = reinterpret_cast<const double2*>(A);
+    double2* H2 = reinterpret_cast<double2*>(Ht);
+    const int bi = blockIdx.y * 32, bj = blockIdx.x * 32;
+    for (int r = threadIdx.y; r < 32; r += blockDim.y) {
+        const int i = bi + threadIdx.x, j = bj + r;
+        tile[r][threadIdx.x] = (i < n && j < n) ? A2[(size_t)j * n + i] : make_double2(0.0, 0.0);
+    }
+    __syncthreads();
+    for (int r = threadIdx.y; r < 32; r += blockDim.y) {
+        const int i = bi + r, j = bj + threadIdx.x;
+        if (i < n && j < n) H2[(size_t)i * n + j] = (i <= j + 1) ? tile[threadIdx.x][r] : make_double2(0.0, 0.0);
+    }
+}
+
+int cj_grid_size(int n)
+{
+    const int g = (n + CJT - 1) / CJT;
+    return g < 1 ? 1 : g;
+}
+
+size_t cj_smem(int n) { return (size_t)(n > 0 ? n : 1) * sizeof(double2); }
+
+cudaError_t launch_reduce_cj(CjArgs a, int balance, cudaStream_t st)
+{
+    const int n = a.n;
+    if (n <= 0) return cudaSuccess;
+    if (n > CJ_NMAX) return cudaErrorInvalidValue;
+    const int grid = cj_grid_size(n);
+    const size_t smem = cj_smem(n);
+    static size_t attr_r = 0, attr_a = 0;
+    cudaError_t e = cudaSuccess;
+    if (smem > 48 * 1024 && smem > attr_r) {
+        e = cudaFuncSetAttribute(cj_reduce_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        if (e != cudaSuccess) return e;
+        attr_r = smem;
+    }
+    if (smem > 48 * 1024 && smem > attr_a) {
+        e = cudaFuncSetAttribute(cj_assemble_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        if (e != cudaSuccess) return e;
+        attr_a = smem;
+    }
+    cj_init_kernel<<<16, 256, 0, st>>>(n, a.ipiv, a.cand_v, a.cand_i, grid);
+    e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+    int bal = balance;
+    void* args[] = {&a, &bal};
+    e = cudaLaunchCooperativeKernel((void*)cj_reduce_kernel, dim3(grid), dim3(CJT), args, smem, st);
+    if (e != cudaSuccess) return e;
+    if (n >= 3) {
+        cj_assemble_kernel<<<n, CJT, smem, st>>>(n, a.A, a.B, a.ipiv);
+        e = cudaGetLastError();
+        if (e != cudaSuccess) return e;
+    }
+    dim3 hg((n + 31) / 32, (n + 31) / 32);
+    cj_ht_kernel<<<hg, dim3(32, 8), 0, st>>>(n, a.A, a.Ht);
+    e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+    return launch_perm(n, a.ipiv, a.perm, a.iperm, st);
+}
+
+// ---- solves ------------------------------------------------------------------------
+// One CTA per complex right-hand side; the vector lives in shared memory.  L[i,k] =
+// factors[i,k] (i >= k+2), read as the packed Lp of the reference holds it (F:407-464).
+
+// y <- L^-1 y, the generic sweep F:2151-2195: groups of four steps (a serial head triangle,
+// then rows k+5:n take all four columns at once as (L1 x1 + L2 x2) + (L3 x3 + L4 x4)), then
+// single steps.
+__device__ void cj_fwd(int n, const double* F, dc* y)
+{
+    const int t = threadIdx.x;
+    const int G = (n - 2 > 0 ? n - 2 : 0) >> 2;
+    for (int g = 1; g <= G; ++g) {
+        const int k = 4 * g - 3;
+        if (t == 0) {
+            const dc x1 = y[k];
+            const dc x2 = csub(y[k + 1], cmul(ldc(F, n, k + 2, k), x1));
+            y[k + 1] = x2;
+            const dc x3 = csub(y[k + 2], cadd(cmul(ldc(F, n, k + 3, k), x1), cmul(ldc(F, n, k + 3, k + 1), x2)));
+            y[k + 2] = x3;
+            const dc x4 = csub(y[k + 3], cadd(cadd(cmul(ldc(F, n, k + 4, k), x1), cmul(ldc(F, n, k + 4, k + 1), x2)),
+                                              cmul(ldc(F, n, k + 4, k + 2), x3)));
+            y[k + 3] = x4;
+        }
+        __syncthreads();
+        const dc x1 = y[k], x2 = y[k + 1], x3 = y[k + 2], x4 = y[k + 3];
+        for (int i = k + 5 + t; i <= n; i += CJT) {
+            const dc s = cadd(cadd(cmul(ldc(F, n, i, k), x1), cmul(ldc(F, n, i, k + 1), x2)),
+                              cadd(cmul(ldc(F, n, i, k + 2), x3), cmul(ldc(F, n, i, k + 3), x4)));
+            y[i - 1] = csub(y[i - 1], s);
+        }
+        __syncthreads();
+    }
+    for (int k = 4 * G + 1; k <= n - 2; ++k) {
+        const dc xk = y[k];
+        for (int i = k + 2 + t; i <= n; i += CJT) y[i - 1] = csub(y[i - 1], cmul(ldc(F, n, i, k), xk));
+        __syncthreads();
+    }
+}
+
+// y <- L y, the generic sweep F:2199-2243: single steps in reverse, then groups in reverse;
+// a group reads its four values first (step k+c touches rows k+c+2:n only).
+__device__ void cj_bwd(int n, const double* F, dc* y)
+{
+    const int t = threadIdx.x;
+    const int G = (n - 2 > 0 ? n - 2 : 0) >> 2;
+    for (int k = n - 2; k >= 4 * G + 1; --k) {
+        const dc xk = y[k];
+        for (int i = k + 2 + t; i <= n; i += CJT) y[i - 1] = cadd(y[i - 1], cmul(ldc(F, n, i, k), xk));
+        __syncthreads();
+    }
+    for (int g = G; g >= 1; --g) {
+        const int k = 4 * g - 3;
+        const dc x1 = y[k], x2 = y[k + 1], x3 = y[k + 2], x4 = y[k + 3];
+        __syncthreads();
+        if (t == 0) {
+            y[k + 1] = cadd(x2, cmul(ldc(F, n, k + 2, k), x1));
+            y[k + 2] = cadd(x3, cadd(cmul(ldc(F, n, k + 3, k), x1), cmul(ldc(F, n, k + 3, k + 1), x2)));
+            y[k + 3] = cadd(x4, cadd(cadd(cmul(ldc(F, n, k + 4, k), x1), cmul(ldc(F, n, k + 4, k + 1), x2)),
+                                     cmul(ldc(F, n, k + 4, k + 2), x3)));
+        }
+        for (int i = k + 5 + t; i <= n; i += CJT) {
+            const dc s = cadd(cadd(cmul(ldc(F, n, i, k), x1), cmul(ldc(F, n, i, k + 1), x2)),
+                              cadd(cmul(ldc(F, n, i, k + 2), x3), cmul(ldc(F, n, i, k + 3), x4)));
+            y[i - 1] = cadd(y[i - 1], s);
+        }
+        __syncthreads();
+    }
+}
+
+// applyZinv! (F:2104-2112): y = P^-1 D^-1 x (F:2130-2140), y <- L^-1 y.  Column c = col0 +
+// blockIdx.x of X (interleaved, ld ldx complex); out to X itself, or (planar != 0) to columns
+// 2 b, 2 b + 1 of Y (ld ldy) as two planes for the Hessenberg solve.
+__global__ void __launch_bounds__(CJT) cj_zinv_kernel(int n, const double* __restrict__ F,
+                                                       const int64_t* __restrict__ perm,
+                                                       const double* __restrict__ iscale, double* X, int ldx,
+                                                       int col0, double* Y, int ldy, int planar,
+                                                       const double* __restrict__ done, double tol)
+{
+    extern __shared__ double2 yv[];
+    dc* y = reinterpret_cast<dc*>(yv);
+    const int b = blockIdx.x, c = col0 + b;
+    if (done && done[c] <= tol) return;
+    double2* x2 = reinterpret_cast<double2*>(X) + (size_t)c * ldx;
+    for (int i = threadIdx.x; i < n; i += CJT) {
+        const int p = (int)perm[i] - 1;
+        const double2 v = x2[p];
+        const double s = iscale[p];
+        y[i] = {dmul(v.x, s), dmul(v.y, s)};
+    }
+    __syncthreads();
+    cj_fwd(n, F, y);
+    __syncthreads();
+    if (planar) {
+        double* yr = Y + (size_t)(2 * b) * ldy;
+        double* yi = yr + ldy;
+        for (int i = threadIdx.x; i < n; i += CJT) {
+            yr[i] = y[i].re;
+            yi[i] = y[i].im;
+        }
+    } else {
+        for (int i = threadIdx.x; i < n; i += CJT) x2[i] = make_double2(y[i].re, y[i].im);
+    }
+}
+
+// applyZ! (F:2069-2082): y <- L y, x = D P y (x[i] = y[iperm[i]] * scale[i]).  In from X
+// itself, or (planar != 0) from the planes in columns 2 b, 2 b + 1 of Y.
+__global__ void __launch_bounds__(CJT) cj_z_kernel(int n, const double* __restrict__ F,
+                                                    const int64_t* __restrict__ iperm,
+                                                    const double* __restrict__ scale, double* X, int ldx, int col0,
+                                                    const double* Y, int ldy, int planar,
+                                                    const double* __restrict__ done, double tol)
+{
+    extern __shared__ double2 yv[];
+    dc* y = reinterpret_cast<dc*>(yv);
+    const int b = blockIdx.x, c = col0 + b;
+    if (done && done[c] <= tol) return;
+    double2* x2 = reinterpret_cast<double2*>(X) + (size_t)c * ldx;
+    if (planar) {
+        const double* yr = Y + (size_t)(2 * b) * ldy;
+        const double* yi = yr + ldy;
+        for (int i = threadIdx.x; i < n; i += CJT) y[i] = {yr[i], yi[i]};
+    } else {
+        for (int i = threadIdx.x; i < n; i += CJT) y[i] = {x2[i].x, x2[i].y};
+    }
+    __syncthreads();
+    cj_bwd(n, F, y);
+    __syncthreads();
+    for (int i = threadIdx.x; i < n; i += CJT) {
+        const dc v = y[(int)iperm[i] - 1];
+        const double s = scale[i];
+        x2[i] = make_double2(dmul(v.re, s), dmul(v.im, s));
+    }
+}
+
+cudaError_t launch_ldiv_cj(const LdivArgs& a, int nrhs, cudaStream_t st)
+{
+    const int n = a.n;
+    if (nrhs <= 0 || n <= 0) return cudaSuccess;
+    if (n > CJ_NMAX || !a.Y || a.ycap < 2) return cudaErrorInvalidValue;
+    const size_t smem = cj_smem(n);
+    static size_t attr_zi = 0, attr_z = 0;
+    cudaError_t e = cudaSuccess;
+    if (smem > 48 * 1024 && smem > attr_zi) {
+        e = cudaFuncSetAttribute(cj_zinv_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        if (e != cudaSuccess) return e;
+        attr_zi = smem;
+    }
+    if (smem > 48 * 1024 && smem > attr_z) {
+        e = cudaFuncSetAttribute(cj_z_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        if (e != cudaSuccess) return e;
+        attr_z = smem;
+    }
+    if (a.mode == 1) {  // applyZinv!
+        cj_zinv_kernel<<<nrhs, CJT, smem, st>>>(n, a.F, a.perm, a.iscale, a.X, a.ldx, 0, nullptr, 0, 0, a.done, a.tol);
+        return cudaGetLastError();
+    }
+    if (a.mode == 2) {  // applyZ!
+        cj_z_kernel<<<nrhs, CJT, smem, st>>>(n, a.F, a.iperm, a.scale, a.X, a.ldx, 0, nullptr, 0, 0, a.done, a.tol);
+        return cudaGetLastError();
+    }
+    // lhl_ldiv! (F:3111-3121): applyZinv!, planar Hessenberg solve, applyZ!
+    const int chunk = a.ycap / 2;
+    for (int c0 = 0; c0 < nrhs; c0 += chunk) {
+        const int cnt = min(chunk, nrhs - c0);
+        cj_zinv_kernel<<<cnt, CJT, smem, st>>>(n, a.F, a.perm, a.iscale, a.X, a.ldx, c0, a.Y, n, 1, a.done, a.tol);
+        e = cudaGetLastError();
+        if (e == cudaSuccess)
+            e = launch_hess_cplx(n, a.Gt, a.ldg, a.po, a.swp, a.rdiag, a.Y, n, c0, cnt, a.rhs_per_shift, a.done,
+                                 a.tol, st);
+        if (e == cudaSuccess) {
+            cj_z_kernel<<<cnt, CJT, smem, st>>>(n, a.F, a.iperm, a.scale, a.X, a.ldx, c0, a.Y, n, 1, a.done, a.tol);
+            e = cudaGetLastError();
+        }
+        if (e != cudaSuccess) return e;
+    }
+    return cudaSuccess;
+}
+
+// ---- residual r = b - (sigma_s x + tau_s J x), J complex; b, x, r interleaved complex ----
+// Tiles of 16 rows x 8 complex right-hand sides, k in chunks of 32 through shared memory.
+constexpr int RM = 16, RC = 8, RK = 32, RTT = 128;
+
+__global__ void __launch_bounds__(RTT) cj_residual_kernel(int n, const double* __restrict__ J, int ldj,
+                                                          const double* __restrict__ B, int ldb,
+                                                          const double* __restrict__ X, int ldx,
+                                                          double* __restrict__ R, int ldr, int nrhs,
+                                                          int rhs_per_shift, const double* __restrict__ sig,
+                                                          const double* __restrict__ tau,
+                                                          const double* __restrict__ done, double tol)
+{
+    __shared__ double2 Js[RK][RM + 1];
+    __shared__ double2 Xs[RK][RC + 1];
+    const int i0 = blockIdx.x * RM, c0 = blockIdx.y * RC;
+    if (done) {
+        bool all = true;
+        for (int c = c0; c < c0 + RC && c < nrhs; ++c) all = all && (done[c] <= tol);
+        if (all) return;
+    }
+    const double2* J2 = reinterpret_cast<const double2*>(J);
+    const double2* X2 = reinterpret_cast<const double2*>(X);
+    const int t = threadIdx.x;
+    const int r = t % RM, cq = t / RM;
+    double ar = 0.0, ai = 0.0;
+    for (int k0 = 0; k0 < n; k0 += RK) {
+        for (int e = t; e < RM * RK; e += RTT) {
+            const int ii = e % RM, kk = e / RM;
+            const int i = i0 + ii, k = k0 + kk;
+            Js[kk][ii] = (i < n && k < n) ? J2[(size_t)k * ldj + i] : make_double2(0.0, 0.0);
+        }
+        for (int e = t; e < RK * RC; e += RTT) {
+            const int kk = e % RK, cc = e / RK;
+            const int k = k0 + kk, c = c0 + cc;
+            Xs[kk][cc] = (k < n && c < nrhs) ? X2[(size_t)c * ldx + k] : make_double2(0.0, 0.0);
+        }
+        __syncthreads();
+#pragma unroll 8
+        for (int kk = 0; kk < RK; ++kk) {
+            const double2 jv = Js[kk][r], xv = Xs[kk][cq];
+            ar = dfma(jv.x, xv.x, ar);
+            ar = dfma(-jv.y, xv.y, ar);
+            ai = dfma(jv.x, xv.y, ai);
+            ai = dfma(jv.y, xv.x, ai);
+        }
+        __syncthreads();
+    }
+    const int i = i0 + r, c = c0 + cq;
+    if (i < n && c < nrhs) {
+        const int s = c / rhs_per_shift;
+        const dc sg = {sig[2 * s], sig[2 * s + 1]}, tu = {tau[2 * s], tau[2 * s + 1]};
+        const double2 xw = X2[(size_t)c * ldx + i];
+        const dc xv = {xw.x, xw.y};
+        dc bv = {0.0, 0.0};  // no B: -W X
+        if (B) {
+            const double2 bw = reinterpret_cast<const double2*>(B)[(size_t)c * ldb + i];
+            bv = {bw.x, bw.y};
+        }
+        const dc w = cadd(cmul(sg, xv), cmul(tu, dc{ar, ai}));
+        reinterpret_cast<double2*>(R)[(size_t)c * ldr + i] = make_double2(bv.re - w.re, bv.im - w.im);
+    }
+}
+
+cudaError_t launch_residual_cj(int n, const double* J, int ldj, const double* B, int ldb, const double* X, int ldx,
+                               double* R, int ldr, int nrhs, int rhs_per_shift, const double* sig, const double* tau,
+                               cudaStream_t st, const double* done, double tol)
+{
+    if (nrhs <= 0 || n <= 0) return cudaSuccess;
+    dim3 grid((n + RM - 1) / RM, (nrhs + RC - 1) / RC);
+    cj_residual_kernel<<<grid, RTT, 0, st>>>(n, J, ldj, B, ldb, X, ldx, R, ldr, nrhs, rhs_per_shift, sig, tau, done,
+                                             tol);
+    return cudaGetLastError();
+}
+
+}  // namespace lhl

@@ -63,6 +63,7 @@ struct LdivArgs {
     int nzflags;
     int* err;             // bounded-wait status (the workspace's error word)
     unsigned long long limit_ns;
+    int cj;               // complex reduction (LHLWorkspace{ComplexF64}): F interleaved complex (cplxj.cu)
 };
 
 // Many independent matrices of uneven order (lhl_reduce_batched, batch.cu): matrix m has order
@@ -161,9 +162,10 @@ cudaError_t launch_solve_batch(const BatchDesc& d, const double* J, const double
                                const double* sig, const double* tau, double tol, int max_steps, double* res,
                                cudaStream_t st);
 // complex shifts on a real reduction (complex.cu)
+// ht_complex = 1: Ht of a complex reduction (interleaved complex, ld ldh complex elements)
 cudaError_t launch_shift_lu_cplx(int n, const double* Ht, int ldh, const double* sig, const double* tau, int s0,
                                  int count, double* Gt, int ldg, int po, uint8_t* swp, double* rd, int32_t* info,
-                                 cudaStream_t st);
+                                 cudaStream_t st, int ht_complex = 0);
 cudaError_t launch_hess_cplx(int n, const double* Gt, int ldg, int po, const uint8_t* swp, const double* rd,
                              double* Y, int ldy, int col0, int count, int rhs_per_shift, const double* done,
                              double tol, cudaStream_t st);
@@ -180,6 +182,37 @@ cudaError_t launch_axpy_cols(int n, double* X, int ldx, const double* R, int ldr
                              const double* done = nullptr, double tol = 0.0);
 cudaError_t launch_relres(int n, const double* R, int ldr, const double* B, int ldb, double* out, int nrhs,
                           cudaStream_t st);
+
+// perm from ipiv and its inverse (reduce.cu)
+cudaError_t launch_perm(int n, const int64_t* ipiv, int64_t* perm, int64_t* iperm, cudaStream_t st);
+
+// Complex J, LHLWorkspace{ComplexF64} (cplxj.cu).  A, B, Ht: n x n interleaved complex, ld n.
+struct CjArgs {
+    int n;
+    double* A;        // J in (balanced in place), factors out
+    double* B;        // second step buffer
+    double* Ht;
+    int64_t* ipiv;
+    int64_t* perm;
+    int64_t* iperm;
+    double* scale;
+    double* iscale;
+    double* bsum;     // 2n
+    double* bfac;     // n
+    int* bflag;
+    double* cand_v;   // per-CTA pivot candidates (cj_grid_size(n) of them)
+    int* cand_i;
+    unsigned int* bar;
+    int* err;
+    unsigned long long limit_ns;
+};
+constexpr int CJ_NMAX = 8192;
+int cj_grid_size(int n);
+cudaError_t launch_reduce_cj(CjArgs a, int balance, cudaStream_t st);
+cudaError_t launch_ldiv_cj(const LdivArgs& a, int nrhs, cudaStream_t st);
+cudaError_t launch_residual_cj(int n, const double* J, int ldj, const double* B, int ldb, const double* X, int ldx,
+                               double* R, int ldr, int nrhs, int rhs_per_shift, const double* sig, const double* tau,
+                               cudaStream_t st, const double* done = nullptr, double tol = 0.0);
 
 // Float32 workspaces (f32.cu): column-major block conversions
 cudaError_t launch_f32_to_f64(const float* src, int lds, double* dst, int ldd, int rows, int cols, cudaStream_t st);

@@ -118,17 +118,6 @@ __device__ __forceinline__ void publish_candidate(const RedArgs& a, double v, in
 // (exact).  The decision of an index after an in-sweep scaling therefore reads a patched
 // sum, which differs from a fresh sequential sum by rounding only.
 // ---------------------------------------------------------------------------------
-__device__ __forceinline__ bool balance_decide(double c, double r, double& f)
-{
-    if (c == 0.0 || r == 0.0) return false;
-    f = 1.0;
-    const double s = c + r;
-    int guard = 0;
-    while (c < r / 2.0 && guard < 4200) { c *= 2.0; r /= 2.0; f *= 2.0; ++guard; }
-    while (c >= 2.0 * r && guard < 8400) { c /= 2.0; r *= 2.0; f /= 2.0; ++guard; }
-    return c + r < 0.95 * s;
-}
-
 __device__ bool balance_phase(const RedArgs& a, GridBarrier& gb)
 {
     const int n = a.n;
@@ -1398,6 +1387,13 @@ cudaError_t launch_ht_perm(int n, const double* A, double* Ht, const int64_t* ip
     ht_fill_kernel<<<grid, dim3(32, 8), 0, st>>>(n, A, Ht);
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return e;
+    perm_kernel<<<1, 256, sizeof(int) * (size_t)n, st>>>(n, ipiv, perm, iperm);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_perm(int n, const int64_t* ipiv, int64_t* perm, int64_t* iperm, cudaStream_t st)
+{
+    if (n <= 0) return cudaSuccess;
     perm_kernel<<<1, 256, sizeof(int) * (size_t)n, st>>>(n, ipiv, perm, iperm);
     return cudaGetLastError();
 }

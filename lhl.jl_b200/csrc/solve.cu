@@ -808,6 +808,7 @@ static cudaError_t run_zmul(const ZArgs& z, cudaStream_t st)
 cudaError_t launch_ldiv(const LdivArgs& a, int nrhs, cudaStream_t st)
 {
     if (nrhs <= 0 || a.n <= 0) return cudaSuccess;
+    if (a.cj) return launch_ldiv_cj(a, nrhs, st);  // complex reduction: complex L (cplxj.cu)
     ZArgs z;
     memset(&z, 0, sizeof(z));
     z.n = a.n;

@@ -76,6 +76,8 @@ def _load():
         "lhl_ws_create_f32": [i64, i32, C.POINTER(vp)],
         "lhl_reduce_f32": [vp, vp, i64, i32, vp],
         "lhl_ldiv_f32": [vp, vp, vp, i64, i64, i64, vp],
+        "lhl_ws_create_c128": [i64, C.POINTER(vp)],
+        "lhl_reduce_c128": [vp, vp, i64, i32, vp],
         "lhl_shift_create": [i64, i64, C.POINTER(vp)],
         "lhl_shift_destroy": [vp],
         "lhl_shift_get_view": [vp, C.POINTER(_ShView)],
@@ -153,7 +155,7 @@ class _DevArray:
 def _view(ptr, shape, typestr="<f8", strides=None):
     if any(s == 0 for s in shape):
         return torch.empty(shape, dtype={"<f8": torch.float64, "<i8": torch.int64, "|u1": torch.uint8,
-                                         "<i4": torch.int32}[typestr], device="cuda")
+                                         "<i4": torch.int32, "<c16": torch.complex128}[typestr], device="cuda")
     return torch.as_tensor(_DevArray(ptr, shape, typestr, strides), device="cuda")
 
 
@@ -260,7 +262,9 @@ class LHLShift:
 
 
 class LHLWorkspace:
-    """``LHLWorkspace{Float64}(n)`` on the device (src/LHLFactorization.jl:144-178).
+    """``LHLWorkspace{T}(n)`` on the device (src/LHLFactorization.jl:144-178), T = Float64
+    (``dtype=torch.float64``), Float32 or ComplexF64 (``dtype=torch.complex128``: a complex J,
+    whose shifts are complex; its factors and Ht are complex128 views).
 
     Holds the reduction and, in ``.shift``, one shift slot (the reference's ``ws.shift``);
     the shift fields are forwarded as in the reference (F:182-191)."""
@@ -276,8 +280,13 @@ class LHLWorkspace:
             _check(_lib.lhl_ws_create_f32(int(n), int(precision), C.byref(self._h)), "LHLWorkspace")
         elif dtype == torch.float64:
             _check(_lib.lhl_ws_create(int(n), int(precision), C.byref(self._h)), "LHLWorkspace")
+        elif dtype == torch.complex128:  # LHLWorkspace{ComplexF64}: shift type ComplexF64 (F:164-169)
+            if precision != LHL_PREC_FP64:
+                raise ArgumentError("a ComplexF64 workspace has the FP64 form only")
+            _check(_lib.lhl_ws_create_c128(int(n), C.byref(self._h)), "LHLWorkspace")
+            shift_complex = True
         else:
-            raise ArgumentError(f"element type {dtype} is not supported (float64 or float32)")
+            raise ArgumentError(f"element type {dtype} is not supported (float64, float32 or complex128)")
         self.dtype = dtype
         self.n = int(n)
         self.precision = precision
@@ -306,11 +315,15 @@ class LHLWorkspace:
     @property
     def factors(self) -> torch.Tensor:
         n = self.n
+        if self.dtype == torch.complex128:
+            return _view(self._v.factors, (n, n), "<c16", strides=(16, 16 * n))
         return _view(self._v.factors, (n, n), strides=(8, 8 * n))
 
     @property
     def Ht(self) -> torch.Tensor:
         n = self.n
+        if self.dtype == torch.complex128:
+            return _view(self._v.Ht, (n, n), "<c16", strides=(16, 16 * n))
         return _view(self._v.Ht, (n, n), strides=(8, 8 * n))
 
     @property
@@ -357,7 +370,7 @@ class LHLWorkspace:
             raise ArgumentError("the workspace holds no reduction")
         torch.cuda.current_stream().synchronize() if stream is None else stream.synchronize()
         np.savez(path, n=self.n, precision=self.precision, shift_complex=self.shift_complex,
-                 f32=self.dtype == torch.float32,
+                 f32=self.dtype == torch.float32, c128=self.dtype == torch.complex128,
                  factors=self.factors.cpu().numpy(), Ht=self.Ht.cpu().numpy(), ipiv=self.ipiv.cpu().numpy(),
                  perm=self.perm.cpu().numpy(), iperm=self.iperm.cpu().numpy(), scale=self.scale.cpu().numpy(),
                  iscale=self.iscale.cpu().numpy())
@@ -366,8 +379,12 @@ class LHLWorkspace:
     def load(cls, path: str, stream=None) -> "LHLWorkspace":
         """A workspace holding the reduction saved by `save` (lhl_ws_import of the C ABI)."""
         d = np.load(path)
-        ws = cls(int(d["n"]), int(d["precision"]), bool(d["shift_complex"]),
-                 dtype=torch.float32 if ("f32" in d and bool(d["f32"])) else torch.float64)
+        dt = torch.float64
+        if "f32" in d and bool(d["f32"]):
+            dt = torch.float32
+        elif "c128" in d and bool(d["c128"]):
+            dt = torch.complex128
+        ws = cls(int(d["n"]), int(d["precision"]), bool(d["shift_complex"]), dtype=dt)
         n = ws.n
         dev = {k: torch.as_tensor(np.ascontiguousarray(d[k])).cuda() for k in ("ipiv", "perm", "iperm", "scale", "iscale")}
         if n:
@@ -392,7 +409,9 @@ class LHLWorkspace:
 def lhl_reduce_(ws: LHLWorkspace, J: torch.Tensor, balance: bool, thread=True, stream=None) -> LHLWorkspace:
     """``lhl_reduce!(ws, J, balance)`` (F:355).  J is not modified.  The workspace must have
     been built for J's order (the device workspace does not resize in place)."""
-    if isinstance(J, torch.Tensor) and J.dtype == torch.float32:
+    if ws.dtype == torch.complex128:
+        _require_cuda_f64(J, "J", True)
+    elif isinstance(J, torch.Tensor) and J.dtype == torch.float32:
         _require_cuda_real(J, "J")
     else:
         _require_cuda_f64(J, "J")
@@ -403,6 +422,8 @@ def lhl_reduce_(ws: LHLWorkspace, J: torch.Tensor, balance: bool, thread=True, s
     Jc = _colmajor(J)
     ld = max(Jc.stride(1), 1)
     fn = _lib.lhl_reduce_f32 if Jc.dtype == torch.float32 else _lib.lhl_reduce
+    if Jc.dtype == torch.complex128:
+        fn = _lib.lhl_reduce_c128
     _check(fn(ws._h, C.c_void_p(Jc.data_ptr()), ld, int(bool(balance)), _stream(stream)), "lhl_reduce")
     ws.reduced = True
     ws._J_keepalive = Jc
@@ -412,8 +433,12 @@ def lhl_reduce_(ws: LHLWorkspace, J: torch.Tensor, balance: bool, thread=True, s
 def lhl(J: torch.Tensor, balance: bool = True, thread=True, precision: int = LHL_PREC_FP64,
         shift_complex: bool = False, stream=None) -> LHLWorkspace:
     """``lhl(J; balance=true, shift=...)`` (F:3179): allocate a workspace and reduce J into it;
-    ``shift_complex=True`` is ``shift = ComplexF64`` (complex shifts on the real reduction)."""
-    _require_cuda_real(J, "J")
+    ``shift_complex=True`` is ``shift = ComplexF64`` (complex shifts on the real reduction); a
+    complex128 J makes an ``LHLWorkspace{ComplexF64}``."""
+    if isinstance(J, torch.Tensor) and J.dtype == torch.complex128:
+        _require_cuda_f64(J, "J", True)
+    else:
+        _require_cuda_real(J, "J")
     if J.dim() != 2 or J.shape[0] != J.shape[1]:
         raise DimensionMismatch(f"matrix is not square: dimensions are {tuple(J.shape)}")
     ws = LHLWorkspace(J.shape[0], precision, shift_complex, dtype=J.dtype)
@@ -423,7 +448,7 @@ def lhl(J: torch.Tensor, balance: bool = True, thread=True, precision: int = LHL
 def lhl_(ws: LHLWorkspace, J: torch.Tensor, balance: bool = True, thread=True, stream=None) -> LHLWorkspace:
     """``lhl!(ws, J; balance)`` (F:3192).  A workspace of another order is rebuilt in place."""
     if J.shape[0] != ws.n:
-        new = LHLWorkspace(J.shape[0], ws.precision, ws.shift_complex)
+        new = LHLWorkspace(J.shape[0], ws.precision, ws.shift_complex, dtype=ws.dtype)
         ws.__dict__.update({k: v for k, v in new.__dict__.items()})
         new._h = None
     return lhl_reduce_(ws, J, balance, thread, stream)
@@ -538,7 +563,7 @@ def lhl_refine_(x: torch.Tensor, J: torch.Tensor, b: torch.Tensor, *args, steps:
         raise TypeError("lhl_refine_(x, J, b, ws, steps) or (x, J, b, sh, ws, steps)")
     if steps <= 0:
         return x
-    _require_cuda_f64(J, "J")
+    _require_cuda_f64(J, "J", ws.dtype == torch.complex128)
     for t, nm in ((x, "x"), (b, "b")):
         _require_cuda_f64(t, nm, sh.is_complex)
     n = ws.n
@@ -565,7 +590,7 @@ def lhl_refine_tol_(x: torch.Tensor, J: torch.Tensor, b: torch.Tensor, sh: LHLSh
     ``lhl_refine!`` (F:3144-3157); columns already at relative residual <= tol are skipped on
     the device.  Returns the per-column final relative residuals (device tensor); x is updated
     in place.  `R` (n x k scratch) and `res` (k) may be passed to avoid allocation."""
-    _require_cuda_f64(J, "J")
+    _require_cuda_f64(J, "J", ws.dtype == torch.complex128)
     for t, nm in ((x, "x"), (b, "b")):
         _require_cuda_f64(t, nm, sh.is_complex)
     n = ws.n
@@ -598,7 +623,7 @@ def lhl_refine_gmres_(x: torch.Tensor, J: torch.Tensor, b: torch.Tensor, sh: LHL
     factorisation, for every column above relative residual `tol`.  Returns the per-column
     final relative residuals (device tensor); x is updated in place.  For complex shifts x and b
     are complex128 and GMRES runs on the realified system."""
-    _require_cuda_f64(J, "J")
+    _require_cuda_f64(J, "J", ws.dtype == torch.complex128)
     for t, nm in ((x, "x"), (b, "b")):
         _require_cuda_f64(t, nm, sh.is_complex)
     n = ws.n
@@ -625,7 +650,8 @@ def lhl_refine_gmres_(x: torch.Tensor, J: torch.Tensor, b: torch.Tensor, sh: LHL
 
 def residual_norms(sh: LHLShift, J: torch.Tensor, b: torch.Tensor, x: torch.Tensor, rhs_per_shift: int = 1,
                    stream=None) -> torch.Tensor:
-    """||b - (sigma I + tau J) x||_2 / ||b||_2 per column, on the device."""
+    """||b - (sigma I + tau J) x||_2 / ||b||_2 per column, on the device (J complex128 when the
+    slots were loaded from a complex reduction)."""
     n = sh.n
     xx, k, ldx = _as_cols(x, n)
     bb, _, ldb = _as_cols(b, n)
@@ -641,7 +667,7 @@ def residual_norms(sh: LHLShift, J: torch.Tensor, b: torch.Tensor, x: torch.Tens
 
 def applyZ_(x: torch.Tensor, ws: LHLWorkspace, stream=None) -> torch.Tensor:
     """``applyZ!(x, ws)``: x <- Z x (F:2069)."""
-    _require_cuda_f64(x, "x")
+    _require_cuda_f64(x, "x", ws.dtype == torch.complex128)
     xx, k, ld = _as_cols(x, ws.n)
     _check(_lib.lhl_applyZ(ws._h, C.c_void_p(xx.data_ptr()), ld, k, _stream(stream)), "applyZ")
     return x
@@ -649,7 +675,7 @@ def applyZ_(x: torch.Tensor, ws: LHLWorkspace, stream=None) -> torch.Tensor:
 
 def applyZinv_(x: torch.Tensor, ws: LHLWorkspace, stream=None) -> torch.Tensor:
     """``applyZinv!(x, ws)``: x <- Z^-1 x (F:2104)."""
-    _require_cuda_f64(x, "x")
+    _require_cuda_f64(x, "x", ws.dtype == torch.complex128)
     xx, k, ld = _as_cols(x, ws.n)
     _check(_lib.lhl_applyZinv(ws._h, C.c_void_p(xx.data_ptr()), ld, k, _stream(stream)), "applyZinv")
     return x

@@ -1145,3 +1145,289 @@ void lhlo_ldiv_complex(int n, const double* F, int ldf, const int64_t* perm, con
         x[2 * (i - 1) + 1] = y[po + p - 1] * scale[i - 1];
     }
 }
+
+/* ------------------------------------------------------------------------------------ */
+/* A complex J (LHLWorkspace{ComplexF64}).  J, F and Ht are interleaved complex (re, im    */
+/* pairs), column-major.  The reference runs the generic Julia code with T = ComplexF64:    */
+/* balancing F:299-340 and the pivot search F:470-477 on abs(z) = hypot(re, im); the        */
+/* unblocked ELMHES F:466-501 with the generic paired sweep F:508-538 (the SIMD variants are */
+/* Float32/Float64 only, F:547); below _lhl_block_min(ComplexF64) = 768 (F:703-705) that is  */
+/* the reference's own path, at and above it the reference's blocked form has the same       */
+/* pivots and factors equal to rounding (test/threading.jl:58-79).  Solves: applyZinv!      */
+/* (gather, generic L^-1 sweep F:2151-2195), planar Hessenberg solve (F:2823-2910), applyZ! */
+/* (generic L sweep F:2199-2243, scatter), as lhl_ldiv! does for a complex workspace         */
+/* (F:3111-3121).                                                                            */
+/* ------------------------------------------------------------------------------------ */
+#define CM1(A, ld, i, j) (((cplx*)(A))[(size_t)((j) - 1) * (size_t)(ld) + (size_t)((i) - 1)])
+
+/* |z| = hypot(re, im).  Borges, "An improved algorithm for hypot(a, b)" (arXiv:1904.09481,  */
+/* 2019): sqrt of a fused x^2 + y^2 and one fused correction step, operands first scaled by  */
+/* a power of two when very large or very small.  The device library computes the same      */
+/* steps (IEEE sqrt and division, exact fma), so the two agree bit for bit.                  */
+static double c_abs(cplx z)
+{
+    double ax = fabs(z.re), ay = fabs(z.im);
+    if (isinf(ax) || isinf(ay)) return INFINITY;
+    if (isnan(ax) || isnan(ay)) return ax + ay;
+    double x = fmax(ax, ay), y = fmin(ax, ay);
+    if (y == 0.0) return x;
+    double s = 1.0;
+    if (x > 0x1p+500) { x *= 0x1p-600; y *= 0x1p-600; s = 0x1p+600; }
+    else if (x < 0x1p-500) { x *= 0x1p+600; y *= 0x1p+600; s = 0x1p-600; }
+    double h = sqrt(fma(x, x, y * y));
+    double h2 = h * h, x2 = x * x;
+    double c = (fma(-y, y, h2 - x2) + fma(h, h, -h2)) - fma(x, x, -x2);
+    h = h - c / (2.0 * h);
+    return h * s;
+}
+
+double lhlo_cabs(double re, double im) { cplx z = {re, im}; return c_abs(z); }
+
+static int c_iszero(cplx a) { return a.re == 0.0 && a.im == 0.0; }
+static void cswap(cplx* a, cplx* b) { cplx t = *a; *a = *b; *b = t; }
+
+/* F:299-340 with T = ComplexF64: the norms sum abs(z), the factors are real powers of two. */
+static void cbalance(int n, double* A, int ld, double* d, double* isc)
+{
+    for (int i = 1; i <= n; ++i) { d[i - 1] = 1.0; isc[i - 1] = 1.0; }
+    for (int sweep = 0; sweep < 20; ++sweep) {
+        int converged = 1;
+        for (int i = 1; i <= n; ++i) {
+            double c = 0.0, r = 0.0;
+            for (int j = 1; j <= n; ++j) {
+                if (j == i) continue;
+                c += c_abs(CM1(A, ld, j, i));
+                r += c_abs(CM1(A, ld, i, j));
+            }
+            if (c == 0.0 || r == 0.0) continue;
+            double f = 1.0;
+            double s = c + r;
+            while (c < r / 2.0) { c *= 2.0; r /= 2.0; f *= 2.0; }
+            while (c >= 2.0 * r) { c /= 2.0; r *= 2.0; f /= 2.0; }
+            if (c + r < 0.95 * s) {
+                converged = 0;
+                d[i - 1] *= f;
+                isc[i - 1] /= f;
+                for (int j = 1; j <= n; ++j) {
+                    CM1(A, ld, i, j).re /= f;
+                    CM1(A, ld, i, j).im /= f;
+                    CM1(A, ld, j, i).re *= f;
+                    CM1(A, ld, j, i).im *= f;
+                }
+            }
+        }
+        if (converged) break;
+    }
+}
+
+/* F:466-501 and the generic paired sweep F:508-538, T = ComplexF64. */
+static void creduce_unblocked(int n, double* A, int ld, int64_t* ipiv)
+{
+    for (int k = 1; k <= n - 2; ++k) {
+        int p = k + 1;
+        double amax = c_abs(CM1(A, ld, k + 1, k));
+        for (int i = k + 2; i <= n; ++i) {
+            double a = c_abs(CM1(A, ld, i, k));
+            if (a > amax) { amax = a; p = i; }
+        }
+        ipiv[k - 1] = p;
+        if (p != k + 1) {
+            for (int j = 1; j <= n; ++j) cswap(&CM1(A, ld, k + 1, j), &CM1(A, ld, p, j));
+            for (int i = 1; i <= n; ++i) cswap(&CM1(A, ld, i, k + 1), &CM1(A, ld, i, p));
+        }
+        cplx piv = CM1(A, ld, k + 1, k);
+        if (c_iszero(piv)) continue;
+        for (int i = k + 2; i <= n; ++i) CM1(A, ld, i, k) = c_div(CM1(A, ld, i, k), piv);
+        cplx pk = CM1(A, ld, k + 1, k + 1);
+        if (!c_iszero(pk))
+            for (int i = k + 2; i <= n; ++i) CM1(A, ld, i, k + 1) = c_sub(CM1(A, ld, i, k + 1), c_mul(CM1(A, ld, i, k), pk));
+        int j = k + 2;
+        while (j + 1 <= n) {
+            cplx pj = CM1(A, ld, k + 1, j), pj1 = CM1(A, ld, k + 1, j + 1);
+            for (int i = k + 2; i <= n; ++i) {
+                cplx l = CM1(A, ld, i, k);
+                CM1(A, ld, i, j) = c_sub(CM1(A, ld, i, j), c_mul(l, pj));
+                CM1(A, ld, i, j + 1) = c_sub(CM1(A, ld, i, j + 1), c_mul(l, pj1));
+            }
+            cplx vj = CM1(A, ld, j, k), vj1 = CM1(A, ld, j + 1, k);
+            for (int i = 1; i <= n; ++i)
+                CM1(A, ld, i, k + 1) = c_add(CM1(A, ld, i, k + 1),
+                                             c_add(c_mul(vj, CM1(A, ld, i, j)), c_mul(vj1, CM1(A, ld, i, j + 1))));
+            j += 2;
+        }
+        if (j <= n) {
+            cplx pj = CM1(A, ld, k + 1, j);
+            for (int i = k + 2; i <= n; ++i) CM1(A, ld, i, j) = c_sub(CM1(A, ld, i, j), c_mul(CM1(A, ld, i, k), pj));
+            cplx vj = CM1(A, ld, j, k);
+            for (int i = 1; i <= n; ++i) CM1(A, ld, i, k + 1) = c_add(CM1(A, ld, i, k + 1), c_mul(vj, CM1(A, ld, i, j)));
+        }
+    }
+}
+
+/* lhl_reduce! for a complex J (F:355-405): copy, balance, unblocked reduction, Ht fill     */
+/* (Ht[j,i] = H[i,j] for i <= j+1, zero elsewhere), perm / iperm.                            */
+int lhlo_reduce_c128(int n, const double* J, int ldj, int balance, double* F, int ldf, int64_t* ipiv, double* scale,
+                     double* iscale, int64_t* perm, int64_t* iperm, double* Ht)
+{
+    if (n < 0 || ldj < n || ldf < n) return -1;
+    for (int j = 1; j <= n; ++j)
+        for (int i = 1; i <= n; ++i) CM1(F, ldf, i, j) = CM1(J, ldj, i, j);
+    if (balance) cbalance(n, F, ldf, scale, iscale);
+    else for (int i = 0; i < n; ++i) { scale[i] = 1.0; iscale[i] = 1.0; }
+    creduce_unblocked(n, F, ldf, ipiv);
+    if (Ht) {
+        memset(Ht, 0, sizeof(double) * 2 * (size_t)n * (size_t)n);
+        for (int i = 1; i <= n; ++i)
+            for (int j = (i - 1 > 1 ? i - 1 : 1); j <= n; ++j) CM1(Ht, n, j, i) = CM1(F, ldf, i, j);
+    }
+    for (int i = 1; i <= n; ++i) perm[i - 1] = i;
+    for (int k = 1; k <= n - 2; ++k) {
+        int64_t p = ipiv[k - 1];
+        int64_t t = perm[k]; perm[k] = perm[p - 1]; perm[p - 1] = t;
+    }
+    for (int i = 1; i <= n; ++i) iperm[perm[i - 1] - 1] = i;
+    return 0;
+}
+
+/* The shift LU of lhlo_shift_complex with tau * Ht[j,k] a complex product (Ht complex). */
+int lhlo_shift_c128(int n, const double* Ht, int ldh, double sr, double si, double tr, double ti, double* Gt, int ldg,
+                    int po, uint8_t* swp, double* rdiag /* 2n interleaved */, double* rw /* 2n */)
+{
+    if (n == 0) return 0;
+    cplx sigma = {sr, si}, tau = {tr, ti};
+    cplx* r = (cplx*)rw;
+    for (int j = 1; j <= n; ++j) r[j - 1] = c_mul(tau, CM1(Ht, ldh, j, 1));
+    r[0] = c_add(r[0], sigma);
+    int info = 0;
+    for (int k = 1; k <= n - 1; ++k) {
+        cplx a = r[k - 1];
+        cplx b = c_mul(tau, CM1(Ht, ldh, k, k + 1));
+        if (c_mag(b) > c_mag(a)) {
+            swp[k - 1] = 1;
+            CSET(Gt, ldg, po, k, k, b);
+            cplx l = c_div(a, b);
+            CSET(Gt, ldg, po, k, k + 1, l);
+            for (int j = k + 1; j <= n; ++j) {
+                cplx g = c_mul(tau, CM1(Ht, ldh, j, k + 1));
+                CSET(Gt, ldg, po, j, k, g);
+                r[j - 1] = c_sub(r[j - 1], c_mul(l, g));
+            }
+            CSET(Gt, ldg, po, k + 1, k, c_add(CG(Gt, ldg, po, k + 1, k), sigma));
+            r[k] = c_sub(r[k], c_mul(l, sigma));
+        } else {
+            swp[k - 1] = 0;
+            CSET(Gt, ldg, po, k, k, a);
+            cplx l;
+            if (c_iszero(a)) { if (info == 0) info = k; l.re = 0.0; l.im = 0.0; }
+            else l = c_div(b, a);
+            CSET(Gt, ldg, po, k, k + 1, l);
+            for (int j = k + 1; j <= n; ++j) {
+                cplx rj = r[j - 1];
+                CSET(Gt, ldg, po, j, k, rj);
+                r[j - 1] = c_sub(c_mul(tau, CM1(Ht, ldh, j, k + 1)), c_mul(l, rj));
+            }
+            r[k] = c_add(r[k], sigma);
+        }
+    }
+    cplx rn = r[n - 1];
+    CSET(Gt, ldg, po, n, n, rn);
+    swp[n - 1] = 0;
+    if (c_iszero(rn) && info == 0) info = n;
+    cplx one = {1.0, 0.0};
+    for (int j = 1; j <= n; ++j) {
+        cplx q = c_div(one, CG(Gt, ldg, po, j, j));
+        rdiag[2 * (j - 1)] = q.re;
+        rdiag[2 * (j - 1) + 1] = q.im;
+    }
+    return info;
+}
+
+/* x <- L^-1 x, the generic sweep F:2151-2195 (L[i,k] = F[i,k], i >= k+2): groups of four
+ * steps with a serial head triangle, rows k+5:n as (L1 x1 + L2 x2) + (L3 x3 + L4 x4). */
+static void czinvsweep(int n, const double* F, int ldf, cplx* x)
+{
+    int G = (n - 2 > 0 ? n - 2 : 0) >> 2;
+    for (int g = 1; g <= G; ++g) {
+        int k = 4 * g - 3;
+        cplx x1 = x[k];
+        cplx x2 = c_sub(x[k + 1], c_mul(CM1(F, ldf, k + 2, k), x1));
+        x[k + 1] = x2;
+        cplx x3 = c_sub(x[k + 2], c_add(c_mul(CM1(F, ldf, k + 3, k), x1), c_mul(CM1(F, ldf, k + 3, k + 1), x2)));
+        x[k + 2] = x3;
+        cplx x4 = c_sub(x[k + 3], c_add(c_add(c_mul(CM1(F, ldf, k + 4, k), x1), c_mul(CM1(F, ldf, k + 4, k + 1), x2)),
+                                        c_mul(CM1(F, ldf, k + 4, k + 2), x3)));
+        x[k + 3] = x4;
+        for (int i = k + 5; i <= n; ++i) {
+            cplx s = c_add(c_add(c_mul(CM1(F, ldf, i, k), x1), c_mul(CM1(F, ldf, i, k + 1), x2)),
+                           c_add(c_mul(CM1(F, ldf, i, k + 2), x3), c_mul(CM1(F, ldf, i, k + 3), x4)));
+            x[i - 1] = c_sub(x[i - 1], s);
+        }
+    }
+    for (int k = 4 * G + 1; k <= n - 2; ++k) {
+        cplx xk = x[k];
+        for (int i = k + 2; i <= n; ++i) x[i - 1] = c_sub(x[i - 1], c_mul(CM1(F, ldf, i, k), xk));
+    }
+}
+
+/* x <- L x, the generic sweep F:2199-2243: single steps in reverse, then groups in reverse,
+ * each reading its four values first. */
+static void czsweep(int n, const double* F, int ldf, cplx* x)
+{
+    int G = (n - 2 > 0 ? n - 2 : 0) >> 2;
+    for (int k = n - 2; k >= 4 * G + 1; --k) {
+        cplx xk = x[k];
+        for (int i = k + 2; i <= n; ++i) x[i - 1] = c_add(x[i - 1], c_mul(CM1(F, ldf, i, k), xk));
+    }
+    for (int g = G; g >= 1; --g) {
+        int k = 4 * g - 3;
+        cplx x1 = x[k], x2 = x[k + 1], x3 = x[k + 2], x4 = x[k + 3];
+        x[k + 1] = c_add(x2, c_mul(CM1(F, ldf, k + 2, k), x1));
+        x[k + 2] = c_add(x3, c_add(c_mul(CM1(F, ldf, k + 3, k), x1), c_mul(CM1(F, ldf, k + 3, k + 1), x2)));
+        x[k + 3] = c_add(x4, c_add(c_add(c_mul(CM1(F, ldf, k + 4, k), x1), c_mul(CM1(F, ldf, k + 4, k + 1), x2)),
+                                   c_mul(CM1(F, ldf, k + 4, k + 2), x3)));
+        for (int i = k + 5; i <= n; ++i) {
+            cplx s = c_add(c_add(c_mul(CM1(F, ldf, i, k), x1), c_mul(CM1(F, ldf, i, k + 1), x2)),
+                           c_add(c_mul(CM1(F, ldf, i, k + 2), x3), c_mul(CM1(F, ldf, i, k + 3), x4)));
+            x[i - 1] = c_add(x[i - 1], s);
+        }
+    }
+}
+
+/* applyZinv! (F:2104-2112) and applyZ! (F:2069-2082) for a complex reduction; x n complex. */
+void lhlo_applyZinv_c128(int n, const double* F, int ldf, const int64_t* perm, const double* iscale, double* x)
+{
+    cplx* xv = (cplx*)x;
+    cplx* w = (cplx*)malloc(sizeof(cplx) * (size_t)(n > 0 ? n : 1));
+    for (int i = 1; i <= n; ++i) {
+        int64_t p = perm[i - 1];
+        w[i - 1] = c_scale(xv[p - 1], iscale[p - 1]);
+    }
+    czinvsweep(n, F, ldf, w);
+    for (int i = 0; i < n; ++i) xv[i] = w[i];
+    free(w);
+}
+
+void lhlo_applyZ_c128(int n, const double* F, int ldf, const int64_t* iperm, const double* scale, double* x)
+{
+    cplx* xv = (cplx*)x;
+    cplx* w = (cplx*)malloc(sizeof(cplx) * (size_t)(n > 0 ? n : 1));
+    for (int i = 0; i < n; ++i) w[i] = xv[i];
+    czsweep(n, F, ldf, w);
+    for (int i = 1; i <= n; ++i) xv[i - 1] = c_scale(w[iperm[i - 1] - 1], scale[i - 1]);
+    free(w);
+}
+
+/* lhl_ldiv!(x, sh, ws) on a complex reduction (F:3111-3121): applyZinv!, the planar        */
+/* Hessenberg solve, applyZ!.  y: 2 po doubles of scratch.                                   */
+void lhlo_ldiv_c128(int n, const double* F, int ldf, const int64_t* perm, const int64_t* iperm, const double* scale,
+                    const double* iscale, const double* Gt, int ldg, int po, const uint8_t* swp, const double* rdiag,
+                    double* x, double* y)
+{
+    cplx* xv = (cplx*)x;
+    lhlo_applyZinv_c128(n, F, ldf, perm, iscale, x);
+    for (int i = 0; i < n; ++i) { y[i] = xv[i].re; y[po + i] = xv[i].im; }
+    for (int i = n; i < po; ++i) { y[i] = 0.0; y[po + i] = 0.0; }
+    hess_solve_planar(n, Gt, ldg, po, swp, rdiag, y);
+    for (int i = 0; i < n; ++i) { xv[i].re = y[i]; xv[i].im = y[po + i]; }
+    lhlo_applyZ_c128(n, F, ldf, iperm, scale, x);
+}

@@ -61,6 +61,15 @@ def lib():
         L.lhlo_shift_complex.argtypes = [i, _dp, i, d, d, d, d, _dp, i, i, _u8, _dv, _dv]
         L.lhlo_shift_complex.restype = i
         L.lhlo_ldiv_complex.argtypes = [i, _dp, i, _iv, _iv, _dv, _dv, _dp, i, i, _u8, _dv, _dv, _dv]
+        L.lhlo_cabs.argtypes = [d, d]
+        L.lhlo_cabs.restype = d
+        L.lhlo_reduce_c128.argtypes = [i, _dv, i, i, _dv, i, _iv, _dv, _dv, _iv, _iv, _dv]
+        L.lhlo_reduce_c128.restype = i
+        L.lhlo_shift_c128.argtypes = [i, _dv, i, d, d, d, d, _dp, i, i, _u8, _dv, _dv]
+        L.lhlo_shift_c128.restype = i
+        L.lhlo_applyZinv_c128.argtypes = [i, _dv, i, _iv, _dv, _dv]
+        L.lhlo_applyZ_c128.argtypes = [i, _dv, i, _iv, _dv, _dv]
+        L.lhlo_ldiv_c128.argtypes = [i, _dv, i, _iv, _iv, _dv, _dv, _dp, i, i, _u8, _dv, _dv, _dv]
         L.lhlo_num_threads.restype = i
         _lib = L
     return _lib
@@ -426,3 +435,115 @@ def gmres_ir(matvec, precond, b, x, tol, max_cycles=4, restart=8):
             y[i] = v / Hr[i, i] if Hr[i, i] != 0 else 0.0
         x = x + sum(y[i] * V[i] for i in range(jd))
     return x, rel, napply
+
+
+# ---------------------------------------------------------------------------------------------
+# A complex J (LHLWorkspace{ComplexF64}): lhlo_reduce_c128 and friends in lhl_oracle.c.
+# Complex matrices cross as complex128 arrays (interleaved pairs), column-major.
+# ---------------------------------------------------------------------------------------------
+def _cflat(a):
+    """The interleaved float64 view of a Fortran-ordered complex128 array."""
+    return np.asfortranarray(a, dtype=np.complex128).ravel(order="F").view(np.float64)
+
+
+class ReductionC(Reduction):
+    """The outputs of ``lhl_reduce!`` for a complex J: complex factors and Ht, real scale."""
+
+    @property
+    def L(self):
+        n = self.n
+        Lm = np.eye(n, dtype=np.complex128)
+        for k in range(n - 2):
+            Lm[k + 2:, k + 1] = self.factors[k + 2:, k]
+        return Lm
+
+    def Z(self):
+        n = self.n
+        Zm = np.eye(n, dtype=np.complex128, order="F")
+        for j in range(n):
+            Zm[:, j] = apply_z_c128(self, Zm[:, j].copy())
+        return Zm
+
+    def Zinv(self):
+        n = self.n
+        Zm = np.eye(n, dtype=np.complex128, order="F")
+        for j in range(n):
+            Zm[:, j] = apply_zinv_c128(self, Zm[:, j].copy())
+        return Zm
+
+
+def cabs(z) -> float:
+    """abs(z) of the complex reduction (the hypot algorithm the oracle and the device share)."""
+    z = complex(z)
+    return float(lib().lhlo_cabs(z.real, z.imag))
+
+
+def reduce_c128(J, balance=True) -> ReductionC:
+    """``lhl(J; balance)`` for a complex J (unblocked ELMHES at every n)."""
+    J = np.asfortranarray(J, dtype=np.complex128)
+    n = J.shape[0]
+    R = ReductionC(n)
+    m = max(n, 1)
+    Jf = _cflat(J) if n > 0 else np.zeros(2)
+    F = np.zeros(2 * m * m)
+    Ht = np.zeros(2 * m * m)
+    ip = _ipiv_buf(n)
+    sc, isc = np.ones(m), np.ones(m)
+    pm, ipm = np.zeros(m, dtype=np.int64), np.zeros(m, dtype=np.int64)
+    rc = lib().lhlo_reduce_c128(n, Jf, m, int(balance), F, m, ip, sc, isc, pm, ipm, Ht)
+    assert rc == 0
+    R.factors = F.view(np.complex128).reshape((m, m), order="F")[:n, :n].copy(order="F")
+    R.Ht = Ht.view(np.complex128).reshape((m, m), order="F")[:n, :n].copy(order="F")
+    R.ipiv = ip[: max(n - 2, 0)].copy()
+    R.scale, R.iscale = sc[:n].copy(), isc[:n].copy()
+    R.perm, R.iperm = pm[:n].copy(), ipm[:n].copy()
+    return R
+
+
+def shift_c128(R: ReductionC, sigma, tau) -> ShiftC:
+    """``lhl_shift!(ws, sigma, tau)`` on a complex reduction (planar Gt, as ShiftC)."""
+    n = R.n
+    S = ShiftC(n)
+    w = np.zeros(2 * max(n, 1))
+    Ht = _cflat(R.Ht) if n > 0 else np.zeros(2)
+    rd = np.zeros(2 * max(n, 1))
+    sigma, tau = complex(sigma), complex(tau)
+    S.info = int(lib().lhlo_shift_c128(n, Ht, max(n, 1), sigma.real, sigma.imag, tau.real, tau.imag, S.Gt, S.ldg,
+                                       S.po, S.swap, rd, w))
+    S.rdiag = cpack(rd[0::2][:max(n, 1)], rd[1::2][:max(n, 1)])
+    S.sigma, S.tau = sigma, tau
+    return S
+
+
+def apply_zinv_c128(R: ReductionC, x):
+    x = np.array(x, dtype=np.complex128, copy=True)
+    lib().lhlo_applyZinv_c128(R.n, _cflat(R.factors) if R.n else np.zeros(2), max(R.n, 1), R.perm, R.iscale,
+                              x.view(np.float64))
+    return x
+
+
+def apply_z_c128(R: ReductionC, x):
+    x = np.array(x, dtype=np.complex128, copy=True)
+    lib().lhlo_applyZ_c128(R.n, _cflat(R.factors) if R.n else np.zeros(2), max(R.n, 1), R.iperm, R.scale,
+                           x.view(np.float64))
+    return x
+
+
+def ldiv_c128(R: ReductionC, S: ShiftC, b):
+    x = np.array(b, dtype=np.complex128, copy=True)
+    y = np.zeros(2 * S.po)
+    rd = np.empty(2 * max(R.n, 1))
+    rd[0::2] = S.rdiag.real
+    rd[1::2] = S.rdiag.imag
+    lib().lhlo_ldiv_c128(R.n, _cflat(R.factors) if R.n else np.zeros(2), max(R.n, 1), R.perm, R.iperm, R.scale,
+                         R.iscale, S.Gt, S.ldg, S.po, S.swap, rd, x.view(np.float64), y)
+    return x
+
+
+def refine_c128(R: ReductionC, S: ShiftC, J, b, x, steps=1):
+    """lhl_refine!(x, sI + tJ, b, sh, ws, steps) on a complex reduction, residual in numpy."""
+    W = S.sigma * np.eye(R.n) + S.tau * np.asarray(J, dtype=np.complex128)
+    x = np.array(x, dtype=np.complex128, copy=True)
+    for _ in range(steps):
+        x = x + ldiv_c128(R, S, b - W @ x)
+    return x

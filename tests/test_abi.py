@@ -67,6 +67,13 @@ def test_null_handles_rejected_on_host():
     L.lhl_refine_gmres.argtypes = [vp, vp, vp, i64, vp, i64, vp, i64, vp, vp, i64, i64, d, i32, i32, i32, vp]
     assert L.lhl_refine_gmres(vp(0), vp(0), vp(0), 1, vp(0), 1, vp(0), 1, vp(0), vp(0), 1, 1, 1e-10, 1, 3, 1,
                               vp(0)) == 1
+    # LHLWorkspace{ComplexF64}: order checked on the host, null handles refused
+    L.lhl_ws_create_c128.argtypes = [i64, ctypes.POINTER(vp)]
+    assert L.lhl_ws_create_c128(-1, ctypes.byref(h)) == 2
+    assert L.lhl_ws_create_c128(8193, ctypes.byref(h)) == 2
+    assert L.lhl_ws_create_c128(4, None) == 1
+    L.lhl_reduce_c128.argtypes = [vp, vp, i64, i32, vp]
+    assert L.lhl_reduce_c128(vp(0), vp(0), 1, 1, vp(0)) == 1
 
 
 def test_configs_are_seeded_and_shaped():

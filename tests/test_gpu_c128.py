@@ -1,0 +1,247 @@
+"""A complex J (LHLWorkspace{ComplexF64}) on the device through the C ABI: the reduction
+(ipiv, factors, Ht, scale, perm) and the shift LU (planar Gt, swap, rdiag, info) bit for bit
+against the oracle, applyZ! / applyZinv! bit for bit, solves against the oracle and a dense
+solve (test/core_tests.jl:241-249), the complex reduction of a real J against complex shifts
+on the real reduction (:251-280), refinement with the complex W, save / load, and the
+reference's errors."""
+import numpy as np
+import pytest
+
+from oracle import oracle as O
+
+pytestmark = pytest.mark.gpu
+
+SHIFTS = ((0.4 + 0.7j, -1.0), (1.0, -0.05 + 0.3j), (0.0, 1j), (-3.0 + 2j, 2.0 - 1j), (1.0, -0.05))
+
+
+def _mods():
+    import torch
+    import lhl_gpu as G
+    return torch, G
+
+
+def dev(a):
+    torch, _ = _mods()
+    return torch.as_tensor(np.asfortranarray(a)).cuda()
+
+
+def host(t):
+    return t.detach().cpu().numpy()
+
+
+def crandn(g, *shape):
+    return g.standard_normal(shape) + 1j * g.standard_normal(shape)
+
+
+def bits_equal(a, b):
+    a = np.ascontiguousarray(a)
+    b = np.ascontiguousarray(b)
+    return a.shape == b.shape and a.dtype == b.dtype and np.array_equal(a.view(np.uint8), b.view(np.uint8))
+
+
+def bwd(W, x, b):
+    r = b - W @ x
+    return np.abs(r).max() / (np.abs(W).sum(axis=1).max() * np.abs(x).max() + np.abs(b).max())
+
+
+def matrix(n, kind, seed):
+    g = np.random.default_rng(seed)
+    if kind == "tie":  # Gaussian integers: many equal moduli
+        return (g.integers(-2, 3, (n, n)) + 1j * g.integers(-2, 3, (n, n))).astype(np.complex128)
+    if kind == "graded":  # rows and columns over ten orders of magnitude: balancing scales
+        d = 10.0 ** np.linspace(-5, 5, n)
+        return (crandn(g, n, n) * d[:, None]) / d[None, :]
+    return crandn(g, n, n)
+
+
+@pytest.mark.parametrize("n", list(range(1, 18)) + [31, 64, 65, 129, 256, 300, 600])
+@pytest.mark.parametrize("kind", ["randn", "tie", "graded"])
+@pytest.mark.parametrize("balance", [True, False])
+def test_complex_reduction_bitexact(n, kind, balance):
+    torch, G = _mods()
+    J = matrix(n, kind, 100 + n)
+    R = O.reduce_c128(J, balance)
+    ws = G.lhl(dev(J), balance=balance)
+    assert ws.dtype == torch.complex128 and ws.shift.is_complex
+    torch.cuda.synchronize()
+    ws.check()
+    assert np.array_equal(host(ws.ipiv), R.ipiv)
+    assert bits_equal(host(ws.scale), R.scale)
+    assert bits_equal(host(ws.factors), R.factors)
+    assert bits_equal(host(ws.Ht), R.Ht)
+    assert np.array_equal(host(ws.perm), R.perm) and np.array_equal(host(ws.iperm), R.iperm)
+
+
+@pytest.mark.parametrize("n", [1, 2, 3, 5, 16, 33, 128, 129, 257, 600])
+def test_complex_shift_and_z_bitexact(n):
+    """The shift LU on the complex Ht and the two Z applications are the oracle's operations in
+    the oracle's order; the solve differs from it only in the back substitution's summation
+    order (tolerance 1e-12)."""
+    torch, G = _mods()
+    g = np.random.default_rng(7 * n)
+    J = crandn(g, n, n)
+    R = O.reduce_c128(J)
+    ws = G.lhl(dev(J))
+    b = crandn(g, n)
+    for s, t in SHIFTS + ((0.0, 0.0),):
+        G.lhl_shift_(ws, s, t)
+        So = O.shift_c128(R, s, t)
+        sh = ws.shift
+        Gt = host(sh.Gt())
+        assert sh.info == So.info
+        assert bits_equal(host(sh.swap())[:n], So.swap[:n])
+        assert bits_equal(host(sh.rdiag())[:n], So.rdiag[:n])
+        for k in range(n):
+            for off in (0, sh.po):
+                assert bits_equal(Gt[off + k:off + n, k], So.Gt[off + k:off + n, k]), (s, t, k)
+        if So.info:
+            continue
+        x = host(G.lhl_ldiv_(dev(b), ws))
+        xo = O.ldiv_c128(R, So, b)
+        assert np.linalg.norm(x - xo) <= 1e-12 * np.linalg.norm(xo)
+    for fn_dev, fn_o in ((G.applyZ_, O.apply_z_c128), (G.applyZinv_, O.apply_zinv_c128)):
+        X = crandn(g, n, 3)
+        Xd = dev(X)
+        fn_dev(Xd, ws)
+        for c in range(3):
+            assert bits_equal(host(Xd)[:, c], fn_o(R, X[:, c]))
+
+
+def test_complex_solve_matches_dense():
+    """test/core_tests.jl:241-249: n = 30, gamma = 0.2 + 0.3i."""
+    torch, G = _mods()
+    g = np.random.default_rng(13)
+    n = 30
+    J = crandn(g, n, n)
+    b = crandn(g, n)
+    gam = 0.2 + 0.3j
+    ws = G.lhl(dev(J))
+    G.lhl_shift_(ws, 1, -gam)
+    x = host(G.lhl_ldiv_(dev(b), ws))
+    xr = np.linalg.solve(np.eye(n) - gam * J, b)
+    assert np.linalg.norm(x - xr) <= 1e-9 * np.linalg.norm(xr)
+
+
+@pytest.mark.parametrize("n", [1, 2, 3, 5, 40, 129, 260, 600])
+def test_complex_reduction_vs_complex_shifts_on_real(n):
+    """test/core_tests.jl:251-280 on the device: ws = lhl(J; shift = ComplexF64), wf =
+    lhl(complex.(J)); x == xf to 1e-9, both against the dense solve, one refinement step with
+    the complex W (through the complex J) under 50 eps."""
+    torch, G = _mods()
+    g = np.random.default_rng(n)
+    J = g.standard_normal((n, n))
+    b = crandn(np.random.default_rng(n + 7), n)
+    ws = G.lhl(dev(J), shift_complex=True)
+    wf = G.lhl(dev(J.astype(np.complex128)))
+    assert np.array_equal(host(ws.ipiv), host(wf.ipiv))
+    Jc = dev(J.astype(np.complex128))
+    eps = np.finfo(float).eps
+    for s, t in SHIFTS:
+        W = s * np.eye(n) + t * J
+        G.lhl_shift_(ws, s, t)
+        G.lhl_shift_(wf, s, t)
+        x = host(G.lhl_ldiv_(dev(b), ws))
+        xf_d = G.lhl_ldiv_(dev(b), wf)
+        xf = host(xf_d)
+        xd = np.linalg.solve(W, b)
+        assert np.linalg.norm(x - xd) <= 1e-9 * np.linalg.norm(xd)
+        assert np.linalg.norm(x - xf) <= 1e-9 * np.linalg.norm(x)
+        G.lhl_refine_(xf_d, Jc, dev(b), wf, 1)
+        y = host(xf_d)
+        assert bwd(W, y, b) <= 2 * bwd(W, xf, b) + eps
+        assert bwd(W, y, b) < 50 * eps
+
+
+def test_complex_refinement_to_tolerance_and_gmres():
+    """Several shifts and right-hand sides per shift on one complex reduction: fixed-point
+    refinement to a tolerance and GMRES-IR both reach 1e-12, the residuals checked on the host."""
+    torch, G = _mods()
+    g = np.random.default_rng(3)
+    n, S, rps = 200, 4, 3
+    J = crandn(g, n, n) / np.sqrt(n)
+    ws = G.LHLWorkspace(n, dtype=torch.complex128)
+    G.lhl_reduce_(ws, dev(J), True)
+    sh = G.LHLShift(n, S, complex=True)
+    sig = torch.tensor(1.0 + 0.3j * np.arange(S), dtype=torch.complex128).cuda()
+    tau = torch.tensor(-0.5 + 0.1j * np.arange(S), dtype=torch.complex128).cuda()
+    G.lhl_shift_batched_(sh, ws, sig, tau)
+    B = crandn(g, n, S * rps)
+    Jd, Bd = dev(J), dev(B)
+    for how in ("tol", "gmres"):
+        X = torch.zeros((S * rps, n), dtype=torch.complex128, device="cuda").t()
+        X.copy_(Bd)
+        G.lhl_ldiv_(X, sh, ws, rhs_per_shift=rps)
+        if how == "tol":
+            res = G.lhl_refine_tol_(X, Jd, Bd, sh, ws, tol=1e-12, max_steps=6, rhs_per_shift=rps)
+        else:
+            res = G.lhl_refine_gmres_(X, Jd, Bd, sh, ws, tol=1e-12, max_cycles=4, restart=4, rhs_per_shift=rps)
+        Xh = host(X)
+        sg, tu = host(sig), host(tau)
+        for c in range(S * rps):
+            s = c // rps
+            W = sg[s] * np.eye(n) + tu[s] * J
+            rel = np.linalg.norm(B[:, c] - W @ Xh[:, c]) / np.linalg.norm(B[:, c])
+            assert rel <= 1e-12, (how, c, rel)
+        assert float(host(res).max()) <= 1e-12
+
+
+def test_complex_above_block_threshold():
+    """n = 1000 (>= 768, where the reference would switch to its blocked form): the unblocked
+    order still reconstructs J and solves to 1e-9."""
+    torch, G = _mods()
+    g = np.random.default_rng(1000)
+    n = 1000
+    J = crandn(g, n, n)
+    ws = G.lhl(dev(J))
+    H = np.triu(host(ws.factors), -1)
+    Zi = dev(np.eye(n, dtype=np.complex128))
+    G.applyZinv_(Zi, ws)
+    Z = dev(np.eye(n, dtype=np.complex128))
+    G.applyZ_(Z, ws)
+    Zh, Zih = host(Z), host(Zi)
+    assert np.linalg.norm(Zh @ H @ Zih - J) <= 1e-9 * np.linalg.norm(J)
+    assert np.abs(np.tril(host(ws.factors), -2)).max() <= 1.0
+    b = crandn(g, n)
+    G.lhl_shift_(ws, 1, -0.01 + 0.02j)
+    x = host(G.lhl_ldiv_(dev(b), ws))
+    xr = np.linalg.solve(np.eye(n) - (0.01 - 0.02j) * J, b)
+    assert np.linalg.norm(x - xr) <= 1e-9 * np.linalg.norm(xr)
+
+
+def test_complex_save_load(tmp_path):
+    torch, G = _mods()
+    g = np.random.default_rng(4)
+    n = 77
+    J = crandn(g, n, n)
+    ws = G.lhl(dev(J))
+    b = crandn(g, n)
+    G.lhl_shift_(ws, 1, -0.1j)
+    x = host(G.lhl_ldiv_(dev(b), ws))
+    p = str(tmp_path / "ws.npz")
+    ws.save(p)
+    w2 = G.LHLWorkspace.load(p)
+    assert w2.dtype == torch.complex128
+    G.lhl_shift_(w2, 1, -0.1j)
+    assert bits_equal(host(G.lhl_ldiv_(dev(b), w2)), x)
+
+
+def test_complex_workspace_errors():
+    torch, G = _mods()
+    n = 6
+    J = crandn(np.random.default_rng(0), n, n)
+    ws = G.lhl(dev(J))
+    with pytest.raises(G.ArgumentError):  # a real J on a complex workspace
+        G.lhl_reduce_(ws, dev(J.real.copy()), True)
+    with pytest.raises(G.ArgumentError):  # an LHLShift{Float64} cannot serve it (F:2463-2465)
+        G.lhl_shift_(G.LHLShift(n, 1), ws, 1.0, -0.5)
+    with pytest.raises(G.ArgumentError):  # a real x cannot hold the solution
+        G.lhl_ldiv_(dev(np.ones(n)), ws)
+    with pytest.raises(G.ArgumentError):  # the mixed form is real only
+        G.LHLWorkspace(n, G.LHL_PREC_MIXED, dtype=torch.complex128)
+    with pytest.raises(G.ArgumentError):  # a complex J on a real workspace
+        G.lhl_reduce_(G.LHLWorkspace(n), dev(J), True)
+    with pytest.raises(G.DimensionMismatch):
+        G.lhl_ldiv_(dev(np.ones(n + 1, dtype=np.complex128)), ws)
+    # real shifts are converted on a complex shift object
+    G.lhl_shift_(ws, 2.0, -0.5)
+    assert ws.shift.info == 0

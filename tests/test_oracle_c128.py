@@ -1,0 +1,120 @@
+"""The oracle's complex J (LHLWorkspace{ComplexF64}) against the reference's own relations,
+on CPU: the reduction reconstructs J with |l| <= 1 (test/core_tests.jl:5-21 with a complex
+J), solves match a dense solve (:241-249), the complex reduction of a real J matches the
+complex-shift-on-real path (:251-280: x == xf, refinement backward error), and a complex
+reduction of a real J takes the real reduction's pivots.  The reference's matrices come from
+Julia's MersenneTwister, which is not reproduced here: these are the same families from
+numpy's seeded generator."""
+import math
+
+import numpy as np
+import pytest
+
+from oracle import oracle as O
+
+SHIFTS = ((0.4 + 0.7j, -1.0), (1.0, -0.05 + 0.3j), (0.0, 1j), (-3.0 + 2j, 2.0 - 1j), (1.0, -0.05))
+
+
+def crandn(g, *shape):
+    return g.standard_normal(shape) + 1j * g.standard_normal(shape)
+
+
+def bwd(W, x, b):
+    """test/core_tests.jl:3: ||b - W x||_inf / (||W||_inf ||x||_inf + ||b||_inf)."""
+    r = b - W @ x
+    return np.abs(r).max() / (np.abs(W).sum(axis=1).max() * np.abs(x).max() + np.abs(b).max())
+
+
+def test_modulus_is_hypot():
+    """abs(z) of the complex path is hypot(re, im): the restated algorithm agrees with the C
+    library's hypot bit for bit on a wide sample, and handles zeros, huge and tiny parts."""
+    g = np.random.default_rng(1)
+    z = g.standard_normal((5000, 2)) * np.exp(g.uniform(-300, 300, (5000, 1)))
+    for a, b in z:
+        assert O.cabs(complex(a, b)) == math.hypot(a, b)
+    assert O.cabs(0j) == 0.0
+    assert O.cabs(3 + 4j) == 5.0
+    assert O.cabs(complex(-2.0, 0.0)) == 2.0
+    assert O.cabs(complex(1e308, 1e308)) == math.hypot(1e308, 1e308)
+    assert O.cabs(complex(5e-324, 5e-324)) == math.hypot(5e-324, 5e-324)
+    assert math.isinf(O.cabs(complex(math.inf, math.nan)))
+
+
+@pytest.mark.parametrize("n", [1, 2, 3, 4, 17, 80, 128, 200])
+@pytest.mark.parametrize("balance", [True, False])
+def test_complex_reduction_reconstructs_J(n, balance):
+    g = np.random.default_rng(n)
+    J = crandn(g, n, n)
+    R = O.reduce_c128(J, balance)
+    Z, Zi = R.Z(), R.Zinv()
+    H = np.triu(R.factors, -1)
+    assert np.allclose(Z @ Zi, np.eye(n), rtol=0, atol=1e-10)
+    assert np.linalg.norm(Z @ H @ Zi - J) <= 1e-10 * np.linalg.norm(J)
+    assert np.all(np.abs(np.tril(R.factors, -2)) <= 1.0)
+    # balancing factors are powers of two and scale * iscale == 1 exactly
+    assert np.all(np.frexp(R.scale)[0] == 0.5)
+    assert np.all(R.scale * R.iscale == 1.0)
+    # Ht holds H transposed, zero below its subdiagonal band
+    assert np.array_equal(R.Ht, H.T)
+
+
+def test_complex_solve_matches_dense():
+    """test/core_tests.jl:241-249: n = 30, gamma = 0.2 + 0.3i, lhl_shift!(ws, 1, -gamma)."""
+    g = np.random.default_rng(13)
+    n = 30
+    J = crandn(g, n, n)
+    b = crandn(g, n)
+    gam = 0.2 + 0.3j
+    R = O.reduce_c128(J)
+    S = O.shift_c128(R, 1, -gam)
+    x = O.ldiv_c128(R, S, b)
+    xr = np.linalg.solve(np.eye(n) - gam * J, b)
+    assert np.linalg.norm(x - xr) <= 1e-9 * np.linalg.norm(xr)
+
+
+@pytest.mark.parametrize("n", [1, 2, 3, 5, 40, 129])
+def test_complex_reduction_of_real_J_matches_complex_shifts(n):
+    """test/core_tests.jl:251-280: a real J with complex shifts (ws) against the complex
+    reduction of complex.(J) (wf): the two solves agree to 1e-9, both match the dense solve,
+    and one refinement step with the complex W brings the backward error under 50 eps."""
+    g = np.random.default_rng(n)
+    J = g.standard_normal((n, n))
+    b = crandn(np.random.default_rng(n + 7), n)
+    Rr = O.reduce(J)
+    Rc = O.reduce_c128(J.astype(np.complex128))
+    assert np.array_equal(Rr.ipiv, Rc.ipiv)
+    eps = np.finfo(float).eps
+    for s, t in SHIFTS:
+        W = s * np.eye(n) + t * J
+        x = O.ldiv_complex(Rr, O.shift_complex(Rr, s, t), b)
+        Sf = O.shift_c128(Rc, s, t)
+        xf = O.ldiv_c128(Rc, Sf, b)
+        xd = np.linalg.solve(W, b)
+        assert np.linalg.norm(x - xd) <= 1e-9 * np.linalg.norm(xd)
+        assert np.linalg.norm(x - xf) <= 1e-9 * np.linalg.norm(x)
+        y = O.refine_c128(Rc, Sf, J, b, xf, 1)
+        assert bwd(W, y, b) <= 2 * bwd(W, xf, b) + eps
+        assert bwd(W, y, b) < 50 * eps
+
+
+def test_complex_singular_shift_reports_info():
+    """A zero pivot is reported in info, not raised (test/core_tests.jl:235-239)."""
+    R = O.reduce_c128(np.array([[1.0, 0.0], [0.0, 2.0]], dtype=np.complex128))
+    S = O.shift_c128(R, 1, -1.0)
+    assert S.info != 0
+    S = O.shift_c128(R, 1j, 1.0)
+    assert S.info == 0
+
+
+def test_complex_tie_matrix_pivots_first_max():
+    """Gaussian-integer matrices have many equal moduli: the pivot is the first maximum (the
+    strict > scan of F:470-477), so the complex reduction of an integer J equals the real one's
+    pivots, and a rotated copy (J * i) has the same pivots (|i z| = |z| exactly)."""
+    g = np.random.default_rng(5)
+    for n in (9, 33, 64):
+        J = g.integers(-2, 3, (n, n)).astype(float)
+        Rr = O.reduce(J)
+        Rc = O.reduce_c128(J.astype(np.complex128))
+        Ri = O.reduce_c128(1j * J.astype(np.complex128))
+        assert np.array_equal(Rr.ipiv, Rc.ipiv)
+        assert np.array_equal(Rc.ipiv, Ri.ipiv)
