@@ -152,6 +152,33 @@ def test_complex_reduction_vs_complex_shifts_on_real(n):
         assert bwd(W, y, b) < 50 * eps
 
 
+@pytest.mark.parametrize("n", [1, 2, 3, 5, 40, 129])
+def test_complex_shifts_forward_error_within_10x_of_complex_reduction(n):
+    """test/core_tests.jl:264-268 on the device: err(x) <= 10 err(xf) + 100 eps against a
+    high-precision solution (FP64 solves corrected by extended-precision residuals)."""
+    torch, G = _mods()
+    g = np.random.default_rng(n)
+    J = g.standard_normal((n, n))
+    b = crandn(np.random.default_rng(n + 7), n)
+    ws = G.lhl(dev(J), shift_complex=True)
+    wf = G.lhl(dev(J.astype(np.complex128)))
+    L = np.clongdouble
+    eps = np.finfo(float).eps
+    for s, t in SHIFTS:
+        W64 = s * np.eye(n) + t * J
+        WL = L(s) * np.eye(n, dtype=L) + L(t) * J.astype(L)
+        xr = np.linalg.solve(W64, b).astype(L)
+        for _ in range(6):
+            xr = xr + np.linalg.solve(W64, (b.astype(L) - WL @ xr).astype(np.complex128)).astype(L)
+        G.lhl_shift_(ws, s, t)
+        G.lhl_shift_(wf, s, t)
+        x = host(G.lhl_ldiv_(dev(b), ws)).astype(L)
+        xf = host(G.lhl_ldiv_(dev(b), wf)).astype(L)
+        ex = float(np.linalg.norm(x - xr) / np.linalg.norm(xr))
+        ef = float(np.linalg.norm(xf - xr) / np.linalg.norm(xr))
+        assert ex <= 10 * ef + 100 * eps, (s, t, ex, ef)
+
+
 def test_complex_refinement_to_tolerance_and_gmres():
     """Several shifts and right-hand sides per shift on one complex reduction: fixed-point
     refinement to a tolerance and GMRES-IR both reach 1e-12, the residuals checked on the host."""

@@ -97,6 +97,43 @@ def test_complex_reduction_of_real_J_matches_complex_shifts(n):
         assert bwd(W, y, b) < 50 * eps
 
 
+def xref_extended(J, s, t, b, iters=6):
+    """The solution of (s I + t J) x = b to far below FP64 rounding: FP64 solves corrected by
+    residuals computed in 80-bit extended precision (the reference's test uses BigFloat at 128
+    bits, test/core_tests.jl:264-268; extended precision resolves errors down to ~1e-18 here)."""
+    n = J.shape[0]
+    L = np.clongdouble
+    W64 = s * np.eye(n) + t * J
+    WL = L(s) * np.eye(n, dtype=L) + L(t) * J.astype(L)
+    bL = b.astype(L)
+    x = np.linalg.solve(W64, b).astype(L)
+    for _ in range(iters):
+        r = bL - WL @ x
+        x = x + np.linalg.solve(W64, r.astype(np.complex128)).astype(L)
+    return x
+
+
+def ferr(v, xref):
+    return float(np.linalg.norm(v.astype(np.clongdouble) - xref) / np.linalg.norm(xref))
+
+
+@pytest.mark.parametrize("n", [1, 2, 3, 5, 40, 129])
+def test_complex_shifts_forward_error_within_10x_of_complex_reduction(n):
+    """test/core_tests.jl:264-268: the forward error of complex shifts on a real reduction is
+    at most 10 x the complex reduction's (+ 100 eps), against a high-precision solution."""
+    g = np.random.default_rng(n)
+    J = g.standard_normal((n, n))
+    b = crandn(np.random.default_rng(n + 7), n)
+    Rr = O.reduce(J)
+    Rc = O.reduce_c128(J.astype(np.complex128))
+    eps = np.finfo(float).eps
+    for s, t in SHIFTS:
+        xr = xref_extended(J, s, t, b)
+        x = O.ldiv_complex(Rr, O.shift_complex(Rr, s, t), b)
+        xf = O.ldiv_c128(Rc, O.shift_c128(Rc, s, t), b)
+        assert ferr(x, xr) <= 10 * ferr(xf, xr) + 100 * eps, (s, t, ferr(x, xr), ferr(xf, xr))
+
+
 def test_complex_singular_shift_reports_info():
     """A zero pivot is reported in info, not raised (test/core_tests.jl:235-239)."""
     R = O.reduce_c128(np.array([[1.0, 0.0], [0.0, 2.0]], dtype=np.complex128))
