@@ -191,8 +191,8 @@ class Shift:
         """(U, l, swap, rdiag, info) exactly as test/core_tests.jl:173-190 extracts it."""
         n = self.n
         G = self.Gt
-        U = np.array([G[j, k] for k in range(n) for j in range(k, n)])
-        l = np.array([G[k, k + 1] for k in range(n - 1)])
+        U = G[:n, :n].T[np.triu_indices(n)]  # G[j, k] for k = 0.., j = k.. (column order)
+        l = G[np.arange(n - 1), np.arange(1, n)]
         return U, l, self.swap[:n].copy(), self.rdiag[:n].copy(), self.info
 
 

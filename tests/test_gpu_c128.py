@@ -72,6 +72,35 @@ def test_complex_reduction_bitexact(n, kind, balance):
     assert np.array_equal(host(ws.perm), R.perm) and np.array_equal(host(ws.iperm), R.iperm)
 
 
+@pytest.mark.parametrize("n", list(range(1, 121)) + [511, 512, 520])
+@pytest.mark.parametrize("tie", [False, True])
+def test_c128_shift_bitexact_reference_orders(n, tie):
+    """test/core_tests.jl:192-201 for T = ComplexF64 at its orders (1:120, 511, 512, 520): the
+    device shift LU on a complex Ht, bit for bit against the oracle (itself pinned to the
+    independent restatement in tests/test_oracle.py), the reference test's five shifts;
+    tie matrices are rand(-2:2) promoted to complex."""
+    torch, G = _mods()
+    g = np.random.default_rng(31 + n + 1000 * tie)
+    J = g.integers(-2, 3, (n, n)).astype(np.complex128) if tie else crandn(g, n, n)
+    R = O.reduce_c128(J)
+    ws = G.LHLWorkspace(n, dtype=torch.complex128)
+    ws.Ht.copy_(dev(R.Ht))
+    for s, t in ((1, -0.1), (0, 1), (1, -3), (2, 0), (0, 0)):
+        with np.errstate(divide="ignore", invalid="ignore"):
+            So = O.shift_c128(R, s, t)
+        G.lhl_shift_(ws, s, t)
+        sh = ws.shift
+        Gt = host(sh.Gt())
+        po = sh.po
+        assert sh.info == So.info
+        assert bits_equal(host(sh.swap())[:n], So.swap[:n])
+        for off in (0, po):
+            assert bits_equal(Gt[off:off + n, :n].T[np.triu_indices(n)], So.Gt[off:off + n, :n].T[np.triu_indices(n)])
+            assert bits_equal(Gt[off + np.arange(n - 1), np.arange(1, n)], So.Gt[off + np.arange(n - 1), np.arange(1, n)])
+        if So.info == 0:
+            assert bits_equal(host(sh.rdiag())[:n], So.rdiag[:n])
+
+
 @pytest.mark.parametrize("n", [1, 2, 3, 5, 16, 33, 128, 129, 257, 600])
 def test_complex_shift_and_z_bitexact(n):
     """The shift LU on the complex Ht and the two Z applications are the oracle's operations in

@@ -37,7 +37,7 @@ def bits_equal(a, b):
     return a.shape == b.shape and a.dtype == b.dtype and np.array_equal(a.view(np.uint8), b.view(np.uint8))
 
 
-@pytest.mark.parametrize("n", list(range(1, 34)) + [63, 64, 65, 255, 256, 257, 511, 512, 513, 1024, 2048])
+@pytest.mark.parametrize("n", list(range(1, 101)) + [255, 256, 257, 511, 512, 513, 520, 700, 1024, 2048])
 @pytest.mark.parametrize("tie", [False, True])
 def test_complex_shift_bitexact(n, tie):
     """The device shift LU (planar Gt, swap, rdiag, info) is bit-identical to the oracle's."""

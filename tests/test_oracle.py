@@ -253,17 +253,21 @@ def _cdiv(a, b):
 
 
 def shift_ref_complex(Ht, sigma, tau):
-    """Pure-Python restatement of the complex-on-real shift LU (F:2529-2594 with TG =
-    ComplexF64; `_lhl_shift_ref!` of test/core_tests.jl:119-171 on complex values): complex
-    products (ac - bd, ad + bc), complex x real scaling both parts, pivot magnitude
-    |re| + |im|.  Returns (U, l, swap, rdiag, info) as complex arrays."""
+    """Pure-Python restatement of the complex shift LU (F:2529-2594 with TG = ComplexF64;
+    `_lhl_shift_ref!` of test/core_tests.jl:119-171 on complex values): complex products
+    (ac - bd, ad + bc), tau times a real Ht entry scaling both parts (a shift on a real
+    reduction) or a complex product (a complex reduction's Ht), pivot magnitude |re| + |im|.
+    Returns (U, l, swap, rdiag, info) as complex arrays."""
     n = Ht.shape[0]
     sr, si = sigma.real, sigma.imag
     tr, ti = tau.real, tau.imag
     mul = lambda a, b: (a[0] * b[0] - a[1] * b[1], a[0] * b[1] + a[1] * b[0])  # noqa: E731
     sub = lambda a, b: (a[0] - b[0], a[1] - b[1])  # noqa: E731
     add = lambda a, b: (a[0] + b[0], a[1] + b[1])  # noqa: E731
-    sc = lambda h: (tr * h, ti * h)  # noqa: E731
+    if np.iscomplexobj(Ht):
+        sc = lambda h: mul((tr, ti), (h.real, h.imag))  # noqa: E731
+    else:
+        sc = lambda h: (tr * h, ti * h)  # noqa: E731
     mag = lambda a: abs(a[0]) + abs(a[1])  # noqa: E731
     r = [sc(Ht[j, 0]) for j in range(n)]
     r[0] = add(r[0], (sr, si))
@@ -317,6 +321,29 @@ def cbits_equal(a, b):
     a = np.ascontiguousarray(a, dtype=np.complex128)
     b = np.ascontiguousarray(b, dtype=np.complex128)
     return a.shape == b.shape and np.array_equal(a.view(np.int64), b.view(np.int64))
+
+
+@pytest.mark.filterwarnings("ignore::RuntimeWarning")  # the (0, 0) shift divides by zero, as in the reference
+@pytest.mark.parametrize("n", list(range(1, 41)) + [64, 65, 130])
+@pytest.mark.parametrize("tie", [False, True])
+def test_c128_shift_matches_restatement(n, tie):
+    """test/core_tests.jl:192-201 for T = ComplexF64: the shift LU of a complex reduction (complex
+    Ht), bit for bit against the independent restatement, over the reference test's shifts;
+    tie matrices are rand(-2:2) promoted to complex, as the test's tie_matrix does."""
+    g = rng(31 + n)
+    if tie:
+        J = g.integers(-2, 3, (n, n)).astype(np.complex128)
+    else:
+        J = g.standard_normal((n, n)) + 1j * g.standard_normal((n, n))
+    R = O.reduce_c128(J)
+    for s, t in ((1, -0.1), (0, 1), (1, -3), (2, 0), (0, 0)):
+        S = O.shift_c128(R, s, t)
+        U, l, sw, rd, info = shift_ref_complex(R.Ht, complex(s), complex(t))
+        Uo, lo, swo, rdo, infoo = cstate(S)
+        assert cbits_equal(U, Uo) and cbits_equal(l, lo) and np.array_equal(sw, swo)
+        assert info == infoo
+        if info == 0:
+            assert cbits_equal(rd, rdo)
 
 
 @pytest.mark.filterwarnings("ignore::RuntimeWarning")  # the (0, 0) shift divides by zero, as in the reference
