@@ -1141,20 +1141,33 @@ __device__ bool blocked_phase(const RedArgs& a, GridBarrier& gb, PanelSh& S, uin
 #pragma unroll
                     for (int s = 0; s < NBMAX; ++s) Lr[s] = (act && s < nbp) ? -M1(A, n, i, k0 + s) : 0.0;
                     const int cend = min(kb + 2 + tj * 32 + 31, n);
-#pragma unroll 4
-                    for (int c = kb + 2 + tj * 32; c <= cend; ++c) {
-                        const double* U = A + (size_t)(c - 1) * n + k0;  // rows k0+1..kb+1
-                        const double uv = (lane < nbp) ? U[lane] : 0.0;
-                        double us[NBMAX];
+                    // 16 columns per round: their U rows (lane s holds U[s]) and this lane's
+                    // elements are all requested before the first chain starts
+                    for (int cb = kb + 2 + tj * 32; cb <= cend; cb += 16) {
+                        const int ncol = min(16, cend - cb + 1);
+                        double uc[16], vc[16];
 #pragma unroll
-                        for (int s = 0; s < NBMAX; ++s) us[s] = __shfl_sync(0xffffffffu, uv, s);  // all lanes
-                        if (act) {
-                            double v = M1(A, n, i, c);
+                        for (int u = 0; u < 16; ++u) {
+                            const int c = cb + u;
+                            uc[u] = (u < ncol && lane < nbp) ? A[(size_t)(c - 1) * n + k0 + lane] : 0.0;  // rows k0+1..kb+1
+                            vc[u] = (u < ncol && act) ? M1(A, n, i, c) : 0.0;
+                        }
 #pragma unroll
-                            for (int s = 0; s < NBMAX; ++s)
-                                if (s < nbp) v = dfma(Lr[s], us[s], v);
-                            M1(A, n, i, c) = v;
-                            if (more && c >= k0n + 1 && c <= kbn + 1) a.B0[(size_t)(c - k0n - 1) * n + (i - 1)] = v;
+                        for (int u = 0; u < 16; ++u) {
+                            if (u < ncol) {
+                                const int c = cb + u;
+                                double v = vc[u];
+#pragma unroll
+                                for (int s = 0; s < NBMAX; ++s) {
+                                    const double us = __shfl_sync(0xffffffffu, uc[u], s);  // all lanes
+                                    if (s < nbp) v = dfma(Lr[s], us, v);
+                                }
+                                if (act) {
+                                    M1(A, n, i, c) = v;
+                                    if (more && c >= k0n + 1 && c <= kbn + 1)
+                                        a.B0[(size_t)(c - k0n - 1) * n + (i - 1)] = v;
+                                }
+                            }
                         }
                     }
                 } else {
@@ -1181,28 +1194,37 @@ __device__ bool blocked_phase(const RedArgs& a, GridBarrier& gb, PanelSh& S, uin
                         }
                         acc[q] = v;
                     }
-                    // one fma chain per element over j = kb+2..n, in order; loads in batches of 8
+                    // one fma chain per element over j = kb+2..n, in order, in chunks of 32 j: the
+                    // chunk's multipliers A[j, k0+c0q+q] come in one coalesced load per column
+                    // (lane u holds row j0+u) and reach every lane by shuffle; each lane issues its
+                    // row's 32 loads of the chunk together
                     const int c0q = cg * 4;
                     const int nq = min(4, nbp - c0q);
-                    int j = kb + 2;
-                    for (; j + 7 <= n; j += 8) {
-                        double av[8], lv[8][4];
+                    for (int j0 = kb + 2; j0 <= n; j0 += 32) {
+                        const int jl = j0 + lane;
+                        double lq[4];
 #pragma unroll
-                        for (int u = 0; u < 8; ++u) {
-                            av[u] = M1(A, n, ii, j + u);
+                        for (int q = 0; q < 4; ++q) lq[q] = (q < nq && jl <= n) ? M1(A, n, jl, k0 + c0q + q) : 0.0;
+                        const int cnt = min(32, n - j0 + 1);
+                        if (cnt == 32) {
+                            double av[32];
 #pragma unroll
-                            for (int q = 0; q < 4; ++q) lv[u][q] = (q < nq) ? M1(A, n, j + u, k0 + c0q + q) : 0.0;
+                            for (int u = 0; u < 32; ++u) av[u] = M1(A, n, ii, j0 + u);
+#pragma unroll
+                            for (int u = 0; u < 32; ++u)
+#pragma unroll
+                                for (int q = 0; q < 4; ++q)
+                                    acc[q] = dfma(av[u], __shfl_sync(0xffffffffu, lq[q], u), acc[q]);
+                        } else {
+                            for (int u = 0; u < cnt; ++u) {
+                                const double aij = M1(A, n, ii, j0 + u);
+#pragma unroll
+                                for (int q = 0; q < 4; ++q) {
+                                    const double l = __shfl_sync(0xffffffffu, lq[q], u);
+                                    if (q < nq) acc[q] = dfma(aij, l, acc[q]);
+                                }
+                            }
                         }
-#pragma unroll
-                        for (int u = 0; u < 8; ++u)
-#pragma unroll
-                            for (int q = 0; q < 4; ++q) acc[q] = dfma(av[u], lv[u][q], acc[q]);
-                    }
-                    for (; j <= n; ++j) {
-                        const double aij = M1(A, n, ii, j);
-#pragma unroll
-                        for (int q = 0; q < 4; ++q)
-                            if (q < nq) acc[q] = dfma(aij, M1(A, n, j, k0 + c0q + q), acc[q]);
                     }
                     if (act) {
 #pragma unroll

@@ -54,6 +54,8 @@ def main():
                 p = [int(v) for v in ws.probe_ns()]
                 names = ("wait+choice", "loads", "dots+column", "publish", "rowop", "poll", "dots")
                 line += " " + " ".join(f"{nm}={p[i] / 1e6:.2f}" for i, nm in enumerate(names))
+            if args.precision == "fp64" and args.probes:  # the plain reduction's phase timers (ms)
+                line += " " + " ".join(f"{k}={v / 1e6:.2f}" for k, v in ws.phase_ns().items())
             print(line, flush=True)
         return
     S = args.shifts
