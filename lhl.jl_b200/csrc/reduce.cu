@@ -882,26 +882,51 @@ __device__ void panel_row(const RedArgs& a, const PanelSh& S, int k0, int kb, in
 // pre-sweep value it receives after the whole sequence (F:1344-1379, F:1395-1415).
 __device__ void build_swap_map(const RedArgs& a, PanelSh& S, int k0, int kb)
 {
-    if (threadIdx.x == 0) {
+    // warp 0 replays the panel's interchanges on the list of rows they touch: entry q (in
+    // order of first appearance) lives in lane q % 32, slot q / 32, as (row, row whose value
+    // it ends with); a lookup is one ballot per slot
+    if (threadIdx.x < 32) {
+        const int lane = threadIdx.x;
+        int row0 = 0, row1 = 0, val0 = 0, val1 = 0;
         int nsr = 0;
-        int val[2 * NBMAX + 2];
-        auto find = [&](int r) {
-            for (int q = 0; q < nsr; ++q)
-                if (S.srow[q] == r) return q;
-            S.srow[nsr] = r;
-            val[nsr] = r;
-            return nsr++;
+        auto find = [&](int r) -> int {
+            const unsigned m0 = __ballot_sync(0xffffffffu, lane < nsr && row0 == r);
+            const unsigned m1 = __ballot_sync(0xffffffffu, lane + 32 < nsr && row1 == r);
+            if (m0) return __ffs(m0) - 1;
+            if (m1) return 32 + __ffs(m1) - 1;
+            const int q = nsr++;
+            if (q < 32) {
+                if (lane == q) { row0 = r; val0 = r; }
+            } else if (lane == q - 32) {
+                row1 = r;
+                val1 = r;
+            }
+            return q;
         };
         for (int k = k0; k <= kb; ++k) {
             const int p = S.ipv[k - k0];
             if (p <= k + 1 || p > a.n) continue;
             const int s1 = find(k + 1), s2 = find(p);
-            const int t = val[s1];
-            val[s1] = val[s2];
-            val[s2] = t;
+            const int v1 = __shfl_sync(0xffffffffu, s1 < 32 ? val0 : val1, s1 & 31);
+            const int v2 = __shfl_sync(0xffffffffu, s2 < 32 ? val0 : val1, s2 & 31);
+            if (lane == (s1 & 31)) {
+                if (s1 < 32) val0 = v2;
+                else val1 = v2;
+            }
+            if (lane == (s2 & 31)) {
+                if (s2 < 32) val0 = v1;
+                else val1 = v1;
+            }
         }
-        for (int q = 0; q < nsr; ++q) S.ssrc[q] = val[q];
-        S.nsr = nsr;
+        if (lane < nsr) {
+            S.srow[lane] = row0;
+            S.ssrc[lane] = val0;
+        }
+        if (lane + 32 < nsr) {
+            S.srow[lane + 32] = row1;
+            S.ssrc[lane + 32] = val1;
+        }
+        if (lane == 0) S.nsr = nsr;
     }
     __syncthreads();
 }
@@ -910,13 +935,20 @@ __device__ void build_swap_map(const RedArgs& a, PanelSh& S, int k0, int kb)
 __device__ void build_trsm_inverse(const RedArgs& a, PanelSh& S, int k0, int kb)
 {
     const int nbp = kb - k0 + 1;   // S.tri[r-1][s-1] = M[r,s] = A[k0+r, k0+s-1], r > s
-    const int q = threadIdx.x + 1;  // column q of P
+    const int q = threadIdx.x + 1;  // column q of P, kept in registers while it is built
     if (threadIdx.x < nbp) {
-        for (int r = 1; r <= nbp; ++r) {
-            if (r <= q) { S.Pm[r - 1][q - 1] = 0.0; continue; }
-            double acc = -S.tri[r - 1][q - 1];
-            for (int s = q + 1; s <= r - 1; ++s) acc = dsub(acc, dmul(S.tri[r - 1][s - 1], S.Pm[s - 1][q - 1]));
-            S.Pm[r - 1][q - 1] = acc;
+        double pc[NBMAX];
+#pragma unroll
+        for (int r = 1; r <= NBMAX; ++r) {
+            double acc = 0.0;
+            if (r <= nbp && r > q) {
+                acc = -S.tri[r - 1][q - 1];
+#pragma unroll
+                for (int s = 2; s <= NBMAX - 1; ++s)
+                    if (s >= q + 1 && s <= r - 1) acc = dsub(acc, dmul(S.tri[r - 1][s - 1], pc[s - 1]));
+            }
+            pc[r - 1] = acc;
+            if (r <= nbp) S.Pm[r - 1][q - 1] = acc;
         }
     }
     __syncthreads();

@@ -56,6 +56,11 @@ def main():
                 line += " " + " ".join(f"{nm}={p[i] / 1e6:.2f}" for i, nm in enumerate(names))
             if args.precision == "fp64" and args.probes:  # the plain reduction's phase timers (ms)
                 line += " " + " ".join(f"{k}={v / 1e6:.2f}" for k, v in ws.phase_ns().items())
+                # finer probes (reduce.cu's tprobe slots): 0-4 the row phase of the last CTA with
+                # rows (start, partials staged, row work, candidate published, barrier), 5 and 6 CTA
+                # 0's pivot combine and step table, 7 CTA 1's GEMV tasks, 8 CTA 0's phase A to its end
+                p = [int(v) for v in ws.probe_ns()]
+                line += " probes=" + ",".join(f"{p[i] / 1e6:.2f}" for i in range(9))
             print(line, flush=True)
         return
     S = args.shifts
