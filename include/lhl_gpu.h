@@ -220,6 +220,21 @@ int lhl_refine_gmres(lhl_shift_t sh, lhl_ws_t ws, const double* dJ, int64_t ldj,
                      double* dX, int64_t ldx, double* dR, double* dres, int64_t nrhs, int64_t rhs_per_shift,
                      double tol, int max_cycles, int restart, int host_check, void* stream);
 
+/* lhl_refine!(x, A, b, sh, ws, steps) (F:3144-3157) with the caller's system matrix A, as the
+ * reference takes it (dA, n x n, ld lda; its tests pass Matrix(W)): r = b - A x, ldiv by shift
+ * slot `slot` of sh, x += r, for every one of the nrhs columns.  A need not be sigma I + tau J:
+ * the refinement converges to A^-1 b wherever the slot's factorisation is close enough to A
+ * (a mass matrix M other than a multiple of I in W = J - M / gamma, say).  Tolerance, dres and
+ * the step count as for lhl_refine_tol (tol = 0: exactly max_steps steps, the reference's
+ * lhl_refine!); the _gmres form refines as lhl_refine_gmres.  With a complex shift object A,
+ * dB, dX and dR are interleaved complex. */
+int lhl_refine_system(lhl_shift_t sh, lhl_ws_t ws, int64_t slot, const double* dA, int64_t lda, const double* dB,
+                      int64_t ldb, double* dX, int64_t ldx, double* dR, double* dres, int64_t nrhs, double tol,
+                      int max_steps, void* stream);
+int lhl_refine_system_gmres(lhl_shift_t sh, lhl_ws_t ws, int64_t slot, const double* dA, int64_t lda,
+                            const double* dB, int64_t ldb, double* dX, int64_t ldx, double* dR, double* dres,
+                            int64_t nrhs, double tol, int max_cycles, int restart, int host_check, void* stream);
+
 /* Relative residuals ||b - (sigma I + tau J) x||_2 / ||b||_2 per column into dres (nrhs). */
 int lhl_residual_norms(lhl_shift_t sh, const double* dJ, int64_t ldj, const double* dB, int64_t ldb,
                        const double* dX, int64_t ldx, double* dR, double* dres, int64_t nrhs,

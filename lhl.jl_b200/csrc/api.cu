@@ -919,6 +919,56 @@ int lhl_refine_gmres(lhl_shift_t sh, lhl_ws_t ws, const double* dJ, int64_t ldj,
     return LHL_OK;
 }
 
+// (sigma, tau) = (0, 1) as real values and as interleaved complex pairs: a shift view with these
+// makes the residual kernels apply the caller's system matrix A itself, r = b - A x.
+__device__ double g_system_shift[4] = {0.0, 0.0, 1.0, 0.0};
+
+// One slot of a shift object as a shift batch of its own whose residuals take a system matrix:
+// the slot's factorisation (Gt, swap, rdiag, U block inverses) and (sigma, tau) = (0, 1).  A
+// complex shift's system matrix is complex (the complex-J residual).
+static int system_view(lhl_shift_t sh, int64_t slot, lhl_shift_s* v)
+{
+    if (!sh) return LHL_ERR_ARG;
+    if (slot < 0 || slot >= sh->nshifts) return LHL_ERR_DIM;
+    void* u = nullptr;
+    if (cudaGetSymbolAddress(&u, g_system_shift) != cudaSuccess) return LHL_ERR_CUDA;
+    *v = *sh;
+    const size_t n = (size_t)sh->n;
+    const size_t P = sh->cplx ? 2 : 1;
+    v->Gt = sh->Gt + (size_t)slot * (size_t)sh->ldg * n;
+    v->swap = sh->swap + (size_t)slot * n;
+    v->rdiag = sh->rdiag + (size_t)slot * P * n;
+    if (!sh->cplx) v->uinv = sh->uinv + (size_t)slot * ((n + 31) / 32) * 32 * 32;
+    v->info = sh->info + slot;
+    v->sigma = (double*)u;
+    v->tau = (double*)u + 2;
+    v->nshifts = 1;
+    v->cj = sh->cplx;
+    return LHL_OK;
+}
+
+int lhl_refine_system(lhl_shift_t sh, lhl_ws_t ws, int64_t slot, const double* dA, int64_t lda, const double* dB,
+                      int64_t ldb, double* dX, int64_t ldx, double* dR, double* dres, int64_t nrhs, double tol,
+                      int max_steps, void* stream)
+{
+    lhl_shift_s v;
+    const int rc = system_view(sh, slot, &v);
+    if (rc != LHL_OK) return rc;
+    return lhl_refine_tol(&v, ws, dA, lda, dB, ldb, dX, ldx, dR, dres, nrhs, nrhs > 0 ? nrhs : 1, tol, max_steps,
+                          stream);
+}
+
+int lhl_refine_system_gmres(lhl_shift_t sh, lhl_ws_t ws, int64_t slot, const double* dA, int64_t lda,
+                            const double* dB, int64_t ldb, double* dX, int64_t ldx, double* dR, double* dres,
+                            int64_t nrhs, double tol, int max_cycles, int restart, int host_check, void* stream)
+{
+    lhl_shift_s v;
+    const int rc = system_view(sh, slot, &v);
+    if (rc != LHL_OK) return rc;
+    return lhl_refine_gmres(&v, ws, dA, lda, dB, ldb, dX, ldx, dR, dres, nrhs, nrhs > 0 ? nrhs : 1, tol, max_cycles,
+                            restart, host_check, stream);
+}
+
 int lhl_residual_norms(lhl_shift_t sh, const double* dJ, int64_t ldj, const double* dB, int64_t ldb,
                        const double* dX, int64_t ldx, double* dR, double* dres, int64_t nrhs, int64_t rhs_per_shift,
                        void* stream)

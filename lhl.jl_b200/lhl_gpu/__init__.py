@@ -77,6 +77,8 @@ def _load():
         "lhl_reduce_f32": [vp, vp, i64, i32, vp],
         "lhl_ldiv_f32": [vp, vp, vp, i64, i64, i64, vp],
         "lhl_ws_create_c128": [i64, C.POINTER(vp)],
+        "lhl_refine_system": [vp, vp, i64, vp, i64, vp, i64, vp, i64, vp, vp, i64, d, i32, vp],
+        "lhl_refine_system_gmres": [vp, vp, i64, vp, i64, vp, i64, vp, i64, vp, vp, i64, d, i32, i32, i32, vp],
         "lhl_reduce_c128": [vp, vp, i64, i32, vp],
         "lhl_shift_create": [i64, i64, C.POINTER(vp)],
         "lhl_shift_destroy": [vp],
@@ -646,6 +648,56 @@ def lhl_refine_gmres_(x: torch.Tensor, J: torch.Tensor, b: torch.Tensor, sh: LHL
                                  float(tol), int(max_cycles), int(restart), int(bool(host_check)),
                                  _stream(stream)), "lhl_refine_gmres")
     return res
+
+
+def lhl_refine_system_(x: torch.Tensor, A: torch.Tensor, b: torch.Tensor, *args, slot: int = 0, tol: float = 0.0,
+                       gmres: bool = False, restart: int = 8, host_check: bool = True, R: torch.Tensor = None,
+                       res: torch.Tensor = None, stream=None) -> torch.Tensor:
+    """``lhl_refine!(x, A, b, ws, steps)`` / ``lhl_refine!(x, A, b, sh, ws, steps)`` (F:3144-3157)
+    with the caller's system matrix A, as the reference takes it: r = b - A x, lhl_ldiv! by shift
+    slot ``slot``, x += r, ``steps`` times (tol = 0); with tol > 0 a column stops once its relative
+    residual is <= tol (at most ``steps`` steps), and with ``gmres=True`` the steps are GMRES-IR
+    cycles of GMRES(restart).  A may differ from sigma I + tau J (a mass matrix in W = J - M/gamma):
+    the refinement converges to A^-1 b where the slot's factorisation is close enough to A.  Every
+    column of x uses the same slot.  Returns x; ``res`` (if given) receives the final relative
+    residuals."""
+    if len(args) == 2:
+        ws, steps = args
+        sh = ws.shift
+    elif len(args) == 3:
+        sh, ws, steps = args
+    else:
+        raise TypeError("lhl_refine_system_(x, A, b, ws, steps) or (x, A, b, sh, ws, steps)")
+    cplx = sh.is_complex
+    _require_cuda_f64(A, "A", cplx)
+    for t, nm in ((x, "x"), (b, "b")):
+        _require_cuda_f64(t, nm, cplx)
+    n = ws.n
+    if A.dim() != 2 or tuple(A.shape) != (n, n):
+        raise DimensionMismatch(f"A is {tuple(A.shape)}, the workspace is {n}x{n}")
+    xx, k, ldx = _as_cols(x, n)
+    bb, kb, ldb = _as_cols(b, n)
+    if kb != k:
+        raise DimensionMismatch("x and b differ in column count")
+    if ldx != n:
+        raise ArgumentError("x must have leading dimension n")
+    Ac = _colmajor(A)
+    dt = torch.complex128 if cplx else torch.float64
+    if R is None:
+        R = torch.empty((k, n), dtype=dt, device=x.device)
+    if res is None:
+        res = torch.empty(k, dtype=torch.float64, device=x.device)
+    if R.numel() < n * k or res.numel() < k:
+        raise DimensionMismatch("scratch too small")
+    ptrs = (C.c_void_p(Ac.data_ptr()), max(Ac.stride(1), n), C.c_void_p(bb.data_ptr()), ldb,
+            C.c_void_p(xx.data_ptr()), ldx, C.c_void_p(R.data_ptr()), C.c_void_p(res.data_ptr()), k, float(tol))
+    if gmres:
+        _check(_lib.lhl_refine_system_gmres(sh._h, ws._h, int(slot), *ptrs, int(steps), int(restart),
+                                            int(bool(host_check)), _stream(stream)), "lhl_refine_system_gmres")
+    else:
+        _check(_lib.lhl_refine_system(sh._h, ws._h, int(slot), *ptrs, int(steps), _stream(stream)),
+               "lhl_refine_system")
+    return x
 
 
 def residual_norms(sh: LHLShift, J: torch.Tensor, b: torch.Tensor, x: torch.Tensor, rhs_per_shift: int = 1,

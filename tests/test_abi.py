@@ -74,6 +74,12 @@ def test_null_handles_rejected_on_host():
     assert L.lhl_ws_create_c128(4, None) == 1
     L.lhl_reduce_c128.argtypes = [vp, vp, i64, i32, vp]
     assert L.lhl_reduce_c128(vp(0), vp(0), 1, 1, vp(0)) == 1
+    # refinement with the caller's system matrix
+    L.lhl_refine_system.argtypes = [vp, vp, i64, vp, i64, vp, i64, vp, i64, vp, vp, i64, d, i32, vp]
+    assert L.lhl_refine_system(vp(0), vp(0), 0, vp(0), 1, vp(0), 1, vp(0), 1, vp(0), vp(0), 1, 0.0, 1, vp(0)) == 1
+    L.lhl_refine_system_gmres.argtypes = [vp, vp, i64, vp, i64, vp, i64, vp, i64, vp, vp, i64, d, i32, i32, i32, vp]
+    assert L.lhl_refine_system_gmres(vp(0), vp(0), 0, vp(0), 1, vp(0), 1, vp(0), 1, vp(0), vp(0), 1, 0.0, 1, 3, 1,
+                                     vp(0)) == 1
 
 
 def test_configs_are_seeded_and_shaped():
