@@ -162,9 +162,31 @@ __global__ void __launch_bounds__(BT) reduce_batch_kernel(BatchDesc d, const dou
             double ck1 = M1(A, n, i, k + 1);
             if (!generic) {
                 double s = 0.0;
-                for (int j = k + 2; j <= n; ++j) {
+                const bool low = i >= k + 2;
+                int j = k + 2;
+                // eight columns at a time: the block's loads (this row, the pivot row, column k;
+                // none of them is stored this step) are issued before its stores
+                for (; j + 7 <= n; j += 8) {
+                    double v[8], pr[8], lk[8];
+#pragma unroll
+                    for (int u = 0; u < 8; ++u) {
+                        v[u] = M1(A, n, i, j + u);
+                        pr[u] = low ? M1(A, n, k + 1, j + u) : 0.0;
+                        lk[u] = M1(A, n, j + u, k);
+                    }
+#pragma unroll
+                    for (int u = 0; u < 8; ++u) {
+                        double x = v[u];
+                        if (low) {
+                            x = dfma(li, -pr[u], x);
+                            M1(A, n, i, j + u) = x;
+                        }
+                        s = dfma(lk[u], x, s);
+                    }
+                }
+                for (; j <= n; ++j) {
                     double v = M1(A, n, i, j);
-                    if (i >= k + 2) {
+                    if (low) {
                         v = dfma(li, -M1(A, n, k + 1, j), v);
                         M1(A, n, i, j) = v;
                     }

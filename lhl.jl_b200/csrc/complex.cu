@@ -289,7 +289,7 @@ cudaError_t launch_hess_cplx(int n, const double* Gt, int ldg, int po, const uin
     const size_t smem = (size_t)2 * n * sizeof(double);
     if (smem > 150 * 1024) return cudaErrorInvalidValue;
     static size_t attr = 0;
-    if (smem > 32 * 1024 && smem > attr) {
+    if (smem > attr) {  // opt in for any size: the static tiles (17 KB) come on top of it
         cudaError_t e = cudaFuncSetAttribute(hess_cplx_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
         if (e != cudaSuccess) return e;
         attr = smem;

@@ -16,10 +16,11 @@
 // as a CuArray{ComplexF64}; scale and iscale are real.  The complex shift LU on the complex
 // Ht is complex.cu's kernel with a complex Ht.
 //
-// The reduction is one cooperative launch, one thread per row, double-buffered like the real
-// unblocked kernel (reduce.cu): step k reads the matrix of step k-1 with rows and columns
-// k+1 <-> p swapped on the fly and writes the other buffer, so a step needs one grid barrier
-// (the pivot search).  Every element sees the reference's complex operations in its order.
+// The reduction is one cooperative launch, one thread per row (rows by warps, spread over up to
+// one CTA per SM), double-buffered like the real unblocked kernel (reduce.cu): step k reads the
+// matrix of step k-1 with rows and columns k+1 <-> p swapped on the fly and writes the other
+// buffer, so a step needs one grid barrier (the pivot search).  Every element sees the
+// reference's complex operations in its order.
 #include "cplx.cuh"
 #include "internal.cuh"
 
@@ -174,7 +175,9 @@ __device__ bool cj_unblocked(const CjArgs& a, GridBarrier& gb, dc* s_l)
     __shared__ int s_redi[CJW];
     __shared__ int s_p;
     const int gt = blockIdx.x * CJT + threadIdx.x;
-    const int i = gt + 1;  // this thread's row
+    // rows by warps spread over the CTAs (global warp w = local warp * grid + CTA holds rows
+    // 32 w + 1 .. 32 w + 32), so that every SM streams a share of the matrix each step
+    const int i = 32 * ((threadIdx.x >> 5) * (int)gridDim.x + (int)blockIdx.x) + (threadIdx.x & 31) + 1;
     {
         double v = 0.0;
         int vi = 0;
@@ -215,6 +218,28 @@ __device__ bool cj_unblocked(const CjArgs& a, GridBarrier& gb, dc* s_l)
                 const dc li = low ? s_l[i - 1] : dc{0.0, 0.0};
                 if (low && !ciszero(pk)) ck1 = csub(ck1, cmul(li, pk));  // F:492-496
                 int j = k + 2;
+                // eight column pairs at a time: every load of the block is issued before its
+                // stores (a store to W could otherwise hold back the next load from R)
+                for (; j + 15 <= n; j += 16) {
+                    dc v[16], pr[16];
+#pragma unroll
+                    for (int u = 0; u < 16; ++u) {
+                        const int sj = sw(j + u);
+                        v[u] = ldc(R, n, si, sj);
+                        pr[u] = low ? ldc(R, n, p, sj) : dc{0.0, 0.0};
+                    }
+#pragma unroll
+                    for (int u = 0; u < 16; u += 2) {
+                        dc v0 = v[u], v1 = v[u + 1];
+                        if (low) {
+                            v0 = csub(v0, cmul(li, pr[u]));
+                            v1 = csub(v1, cmul(li, pr[u + 1]));
+                        }
+                        stc(W, n, i, j + u, v0);
+                        stc(W, n, i, j + u + 1, v1);
+                        ck1 = cadd(ck1, cadd(cmul(s_l[j + u - 1], v0), cmul(s_l[j + u], v1)));
+                    }
+                }
                 while (j + 1 <= n) {  // column pairs (F:515-528)
                     const int sj = sw(j), sj1 = sw(j + 1);
                     dc v0 = ldc(R, n, si, sj), v1 = ldc(R, n, si, sj1);
@@ -314,10 +339,21 @@ __global__ void cj_ht_kernel(int n, const double* __restrict__ A, double* __rest
     }
 }
 
+// one CTA per SM at most, at least one warp of rows per CTA; together they hold >= n rows
 int cj_grid_size(int n)
 {
-    const int g = (n + CJT - 1) / CJT;
-    return g < 1 ? 1 : g;
+    static int sms = 0;
+    if (sms == 0) {
+        int dev = 0;
+        if (cudaGetDevice(&dev) != cudaSuccess ||
+            cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || sms <= 0)
+            sms = 1;
+    }
+    const int warps = (n + 31) / 32;
+    int g = warps < sms ? warps : sms;
+    if (g < 1) g = 1;
+    while ((long long)g * CJT < n) ++g;  // 8 warps per CTA must cover n rows
+    return g;
 }
 
 size_t cj_smem(int n) { return (size_t)(n > 0 ? n : 1) * sizeof(double2); }
@@ -331,12 +367,12 @@ cudaError_t launch_reduce_cj(CjArgs a, int balance, cudaStream_t st)
     const size_t smem = cj_smem(n);
     static size_t attr_r = 0, attr_a = 0;
     cudaError_t e = cudaSuccess;
-    if (smem > 48 * 1024 && smem > attr_r) {
+    if (smem > attr_r) {
         e = cudaFuncSetAttribute(cj_reduce_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
         if (e != cudaSuccess) return e;
         attr_r = smem;
     }
-    if (smem > 48 * 1024 && smem > attr_a) {
+    if (smem > attr_a) {
         e = cudaFuncSetAttribute(cj_assemble_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
         if (e != cudaSuccess) return e;
         attr_a = smem;
@@ -502,12 +538,12 @@ cudaError_t launch_ldiv_cj(const LdivArgs& a, int nrhs, cudaStream_t st)
     const size_t smem = cj_smem(n);
     static size_t attr_zi = 0, attr_z = 0;
     cudaError_t e = cudaSuccess;
-    if (smem > 48 * 1024 && smem > attr_zi) {
+    if (smem > attr_zi) {
         e = cudaFuncSetAttribute(cj_zinv_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
         if (e != cudaSuccess) return e;
         attr_zi = smem;
     }
-    if (smem > 48 * 1024 && smem > attr_z) {
+    if (smem > attr_z) {
         e = cudaFuncSetAttribute(cj_z_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
         if (e != cudaSuccess) return e;
         attr_z = smem;

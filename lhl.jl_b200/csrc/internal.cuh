@@ -132,7 +132,7 @@ struct MixPlan {
     size_t smem;
 };
 
-constexpr size_t MIX_SMEM_MAX = 227 * 1024 - 2048;  // dynamic part; the kernel's static shared arrays use < 1 KB
+constexpr size_t MIX_SMEM_MAX = 227 * 1024 - 4096;  // dynamic part; the kernel's static shared arrays use 2.4 KB
 void mixed_plan(int n, int sms, MixPlan* pl);
 cudaError_t launch_reduce_mixed(MixArgs a, const MixPlan& pl, cudaStream_t st);
 

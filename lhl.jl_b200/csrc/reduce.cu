@@ -229,7 +229,9 @@ __device__ bool unblocked_phase(const RedArgs& a, GridBarrier& gb)
     __shared__ int s_redi[RW];
     __shared__ int s_p;
     const int gt = blockIdx.x * RT + threadIdx.x;
-    const int i = gt + 1;  // this thread's row
+    // this thread's row: rows by warps spread over the CTAs (global warp w = local warp * grid +
+    // CTA holds rows 32 w + 1 .. 32 w + 32), so that many SMs stream the matrix each step
+    const int i = 32 * ((threadIdx.x >> 5) * (int)gridDim.x + (int)blockIdx.x) + (threadIdx.x & 31) + 1;
     const bool generic = n < 8;
 
     // candidates for column 1
@@ -272,10 +274,30 @@ __device__ bool unblocked_phase(const RedArgs& a, GridBarrier& gb)
                 if (pk != 0.0 && i >= k + 2) ck1 = dsub(ck1, dmul(li, pk));
                 if (!generic) {
                     double s = 0.0;
-                    for (int j = k + 2; j <= n; ++j) {
+                    const bool low = i >= k + 2;
+                    int j = k + 2;
+                    // sixteen columns at a time: every load of the block is issued before its
+                    // stores (a store to W could otherwise hold back the next load from R)
+                    for (; j + 15 <= n; j += 16) {
+                        double v[16], pr[16];
+#pragma unroll
+                        for (int u = 0; u < 16; ++u) {
+                            const int sj = sw(j + u);
+                            v[u] = M1(R, n, si, sj);
+                            pr[u] = low ? M1(R, n, p, sj) : 0.0;
+                        }
+#pragma unroll
+                        for (int u = 0; u < 16; ++u) {
+                            double x = v[u];
+                            if (low) x = dfma(li, -pr[u], x);
+                            M1(W, n, i, j + u) = x;
+                            s = dfma(s_l[j + u - 1], x, s);
+                        }
+                    }
+                    for (; j <= n; ++j) {
                         const int sj = sw(j);
                         double v = M1(R, n, si, sj);
-                        if (i >= k + 2) v = dfma(li, -M1(R, n, p, sj), v);
+                        if (low) v = dfma(li, -M1(R, n, p, sj), v);
                         M1(W, n, i, j) = v;
                         s = dfma(s_l[j - 1], v, s);
                     }

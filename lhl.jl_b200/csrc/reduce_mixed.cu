@@ -552,7 +552,7 @@ cudaError_t launch_reduce_mixed(MixArgs a, const MixPlan& pl, cudaStream_t st)
     a.ldr = pl.ldr;
     static size_t attr[2] = {0, 0};
     const void* fn = pl.smem_rows ? (const void*)reduce_mixed_kernel<true> : (const void*)reduce_mixed_kernel<false>;
-    if (pl.smem > 48 * 1024 && pl.smem > attr[pl.smem_rows]) {
+    if (pl.smem > attr[pl.smem_rows]) {
         cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)pl.smem);
         if (e != cudaSuccess) return e;
         attr[pl.smem_rows] = pl.smem;

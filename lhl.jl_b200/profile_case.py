@@ -32,12 +32,19 @@ def main():
     ap.add_argument("--reps", type=int, default=3)
     ap.add_argument("--seed", type=int, default=2)
     ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed"])
+    ap.add_argument("--complex-j", action="store_true", help="a complex J (LHLWorkspace{ComplexF64})")
     ap.add_argument("--probes", action="store_true", help="record and print the reduction's device timers")
     args = ap.parse_args()
     n = args.n
     rng = np.random.default_rng(args.seed)
-    J = torch.as_tensor(np.asfortranarray(rng.standard_normal((n, n)))).cuda()
-    ws = G.LHLWorkspace(n, G.LHL_PREC_MIXED if args.precision == "mixed" else G.LHL_PREC_FP64)
+    Jh = rng.standard_normal((n, n))
+    if args.complex_j:
+        Jh = Jh + 1j * rng.standard_normal((n, n))
+    J = torch.as_tensor(np.asfortranarray(Jh)).cuda()
+    if args.complex_j:
+        ws = G.LHLWorkspace(n, dtype=torch.complex128)
+    else:
+        ws = G.LHLWorkspace(n, G.LHL_PREC_MIXED if args.precision == "mixed" else G.LHL_PREC_FP64)
     if args.probes:
         ws.set_probes(True)
     ev = lambda: torch.cuda.Event(enable_timing=True)  # noqa: E731
@@ -49,12 +56,13 @@ def main():
             b.record()
             torch.cuda.synchronize()
             ws.check()
-            line = f"reduce n={n} {args.precision} rep={r} ms={a.elapsed_time(b):.3f}"
+            form = "complex-J" if args.complex_j else args.precision
+            line = f"reduce n={n} {form} rep={r} ms={a.elapsed_time(b):.3f}"
             if args.precision == "mixed" and args.probes:  # CTA 0's sub-phase times, summed over the steps (ms)
                 p = [int(v) for v in ws.probe_ns()]
                 names = ("wait+choice", "loads", "dots+column", "publish", "rowop", "poll", "dots")
                 line += " " + " ".join(f"{nm}={p[i] / 1e6:.2f}" for i, nm in enumerate(names))
-            if args.precision == "fp64" and args.probes:  # the plain reduction's phase timers (ms)
+            if args.precision == "fp64" and args.probes and not args.complex_j:  # plain reduction's phase timers (ms)
                 line += " " + " ".join(f"{k}={v / 1e6:.2f}" for k, v in ws.phase_ns().items())
                 # finer probes (reduce.cu's tprobe slots): 0-4 the row phase of the last CTA with
                 # rows (start, partials staged, row work, candidate published, barrier), 5 and 6 CTA
@@ -65,10 +73,14 @@ def main():
         return
     S = args.shifts
     G.lhl_reduce_(ws, J, True)
-    sh = G.LHLShift(n, S)
+    sh = G.LHLShift(n, S, complex=args.complex_j)
     sig = torch.ones(S, dtype=torch.float64, device="cuda")
     tau = torch.as_tensor(-(10.0 ** rng.uniform(-4, -1, S))).cuda()
-    B = torch.as_tensor(np.asfortranarray(rng.standard_normal((n, S)))).cuda()
+    Bh = rng.standard_normal((n, S))
+    if args.complex_j:
+        sig, tau = sig.to(torch.complex128), tau.to(torch.complex128)
+        Bh = Bh + 1j * rng.standard_normal((n, S))
+    B = torch.as_tensor(np.asfortranarray(Bh)).cuda()
     X = torch.empty_like(B)
     for r in range(args.reps):
         a, b = ev(), ev()
