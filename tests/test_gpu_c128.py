@@ -301,3 +301,23 @@ def test_complex_workspace_errors():
     # real shifts are converted on a complex shift object
     G.lhl_shift_(ws, 2.0, -0.5)
     assert ws.shift.info == 0
+
+
+@pytest.mark.parametrize("complex_j", [False, True])
+def test_complex_solves_at_2048(complex_j):
+    """n = 2048: the planar Hessenberg solve's dynamic shared memory is exactly 32 KB there, which
+    with its static tiles passes the 48 KB default; complex shifts on a real J and a complex J
+    both solve against a dense solve to 1e-9."""
+    torch, G = _mods()
+    n = 2048
+    g = np.random.default_rng(2048)
+    J = g.standard_normal((n, n)) / np.sqrt(n)
+    if complex_j:
+        J = J + 1j * g.standard_normal((n, n)) / np.sqrt(n)
+    b = crandn(g, n)
+    ws = G.lhl(dev(J)) if complex_j else G.lhl(dev(J), shift_complex=True)
+    s, t = 1.0, -0.3 + 0.2j
+    G.lhl_shift_(ws, s, t)
+    x = host(G.lhl_ldiv_(dev(b), ws))
+    xr = np.linalg.solve(s * np.eye(n) + t * J, b)
+    assert np.linalg.norm(x - xr) <= 1e-9 * np.linalg.norm(xr)
