@@ -195,12 +195,13 @@ __global__ void __launch_bounds__(ZIT, 2) zl_kernel(ZArgs z)
 
 // Hessenberg solve with the shift's LU (F:2746-2816): forward select-swap steps, then
 // U x = y with U[k,j] = Gt[j,k] (j >= k) and rdiag = 1 / U[k,k].
+template <int NT = SOLVE_T>
 __device__ void hess_solve(const LdivArgs& a, const double* Gt, const uint8_t* swp, const double* rd, double* y,
                            double* sm, uint8_t* ssw)
 {
     const int n = a.n;
     const int t = threadIdx.x, lane = t & 31, warp = t >> 5;
-    for (int k = 1 + t; k <= n - 1; k += SOLVE_T) {
+    for (int k = 1 + t; k <= n - 1; k += NT) {
         sm[k - 1] = M1(Gt, a.ldg, k, k + 1);
         ssw[k - 1] = swp[k - 1];
     }
@@ -224,7 +225,7 @@ __device__ void hess_solve(const LdivArgs& a, const double* Gt, const uint8_t* s
     // the 32 x 32 triangle from there.
     __shared__ double tri[BS][BS + 1];
     double* sj = sm;  // block partial sums (the multiplier copy in sm is no longer needed)
-    const int nwarps = SOLVE_T / 32;
+    const int nwarps = NT / 32;
     for (int r1 = n; r1 >= 1; r1 -= BS) {
         const int r0 = max(r1 - BS + 1, 1);
         const int bs = r1 - r0 + 1;
@@ -638,13 +639,14 @@ __global__ void __launch_bounds__(HT) hess_tma_kernel(LdivArgs a, double* Y, int
 // the solve and its refinement entirely on chip (lhl_solve_batched) ----
 // y <- L^-1 y, blocked by 32: the block's triangle staged in shared memory and solved by one
 // warp with shuffles, then every thread applies the block to its rows.
+template <int NT>
 __device__ void small_lsolve(int n, const double* __restrict__ F, double* y)
 {
     __shared__ double tri[BS][BS + 1];
     const int t = threadIdx.x, lane = t & 31, warp = t >> 5;
     for (int c0 = 2; c0 <= n - 1; c0 += BS) {
         const int cb = min(c0 + BS - 1, n - 1), bw = cb - c0 + 1;
-        for (int e = t; e < BS * BS; e += SOLVE_T) {
+        for (int e = t; e < BS * BS; e += NT) {
             const int r = e & 31, q = e >> 5;  // L[c0 + r, c0 + q] = F[c0 + r, c0 + q - 1]
             if (q < bw && r < bw && r > q) tri[r][q] = M1(F, n, c0 + r, c0 + q - 1);
         }
@@ -658,7 +660,7 @@ __device__ void small_lsolve(int n, const double* __restrict__ F, double* y)
             if (lane < bw) y[c0 + lane - 1] = yr;
         }
         __syncthreads();
-        for (int i = cb + 1 + t; i <= n; i += SOLVE_T) {
+        for (int i = cb + 1 + t; i <= n; i += NT) {
             double v = y[i - 1];
             for (int q = 0; q < bw; ++q) v = dfma(-M1(F, n, i, c0 + q - 1), y[c0 + q - 1], v);
             y[i - 1] = v;
@@ -668,19 +670,21 @@ __device__ void small_lsolve(int n, const double* __restrict__ F, double* y)
 }
 
 // y <- L y (original y on the right): (L y)[i] = y[i] + sum_{c=2}^{i-1} L[i,c] y[c]
+template <int NT>
 __device__ void small_lmul(int n, const double* __restrict__ F, double* y, double* y2)
 {
     const int t = threadIdx.x;
-    for (int i = 1 + t; i <= n; i += SOLVE_T) {
+    for (int i = 1 + t; i <= n; i += NT) {
         double v = y[i - 1];
         for (int c = 2; c <= i - 1; ++c) v = dfma(M1(F, n, i, c - 1), y[c - 1], v);
         y2[i - 1] = v;
     }
     __syncthreads();
-    for (int i = t; i < n; i += SOLVE_T) y[i] = y2[i];
+    for (int i = t; i < n; i += NT) y[i] = y2[i];
     __syncthreads();
 }
 
+template <int NT>
 __device__ double block_sum(double v, double* red)
 {
     const int t = threadIdx.x;
@@ -689,11 +693,15 @@ __device__ double block_sum(double v, double* red)
     if ((t & 31) == 0) red[t >> 5] = v;
     __syncthreads();
     double s = 0.0;
-    for (int w = 0; w < SOLVE_T / 32; ++w) s += red[w];
+    for (int w = 0; w < NT / 32; ++w) s += red[w];
     return s;
 }
 
-__global__ void __launch_bounds__(SOLVE_T, 2) solve_batch_kernel(BatchDesc d, const double* __restrict__ J,
+// threads per CTA of the batched solve: one per row of a matrix of order <= 256 (most of config
+// 4), four CTAs per SM within the 64-register cap
+constexpr int SB_T = 256;
+
+__global__ void __launch_bounds__(SB_T, 4) solve_batch_kernel(BatchDesc d, const double* __restrict__ J,
                                                               const double* __restrict__ B, double* __restrict__ X,
                                                               int R, const double* __restrict__ sig,
                                                               const double* __restrict__ tau, double tol,
@@ -705,7 +713,7 @@ __global__ void __launch_bounds__(SOLVE_T, 2) solve_batch_kernel(BatchDesc d, co
     if (n <= 0) return;
     __shared__ double xs[512], rs[512], ys[512], ys2[512];
     __shared__ uint8_t ssw[512];
-    __shared__ double red[SOLVE_T / 32];
+    __shared__ double red[SB_T / 32];
     const int t = threadIdx.x;
     const double* Jm = J + d.off2[m];
     const double* F = d.F + d.off2[m];
@@ -725,46 +733,46 @@ __global__ void __launch_bounds__(SOLVE_T, 2) solve_batch_kernel(BatchDesc d, co
     la.ldg = ldg;
     // v <- W^-1 v in place (F:3052-3068)
     auto solve = [&](double* v) {
-        for (int i = t; i < n; i += SOLVE_T) {
+        for (int i = t; i < n; i += SB_T) {
             const int64_t p = perm[i];
             ys[i] = v[p - 1] * isc[p - 1];
         }
         __syncthreads();
-        small_lsolve(n, F, ys);
-        hess_solve(la, Gt, swp, rd, ys, ys2, ssw);
-        small_lmul(n, F, ys, ys2);
-        for (int i = t; i < n; i += SOLVE_T) v[i] = ys[iperm[i] - 1] * sc[i];
+        small_lsolve<SB_T>(n, F, ys);
+        hess_solve<SB_T>(la, Gt, swp, rd, ys, ys2, ssw);
+        small_lmul<SB_T>(n, F, ys, ys2);
+        for (int i = t; i < n; i += SB_T) v[i] = ys[iperm[i] - 1] * sc[i];
         __syncthreads();
     };
     double bb = 0.0;
-    for (int i = t; i < n; i += SOLVE_T) {
+    for (int i = t; i < n; i += SB_T) {
         const double v = b[i];
         xs[i] = v;
         bb = dfma(v, v, bb);
     }
-    const double bnorm = sqrt(block_sum(bb, red));
+    const double bnorm = sqrt(block_sum<SB_T>(bb, red));
     __syncthreads();
     solve(xs);  // x = W^-1 b
     double rel = 0.0;
     for (int it = 0; it <= max_steps; ++it) {
         // r = b - (sigma x + tau J x), FP64 with the caller's J
         double rr = 0.0;
-        for (int i = t; i < n; i += SOLVE_T) {
+        for (int i = t; i < n; i += SB_T) {
             double acc = 0.0;
             for (int j = 0; j < n; ++j) acc = dfma(Jm[(size_t)j * n + i], xs[j], acc);
             const double r = b[i] - (sigma * xs[i] + tauv * acc);
             rs[i] = r;
             rr = dfma(r, r, rr);
         }
-        const double rn = sqrt(block_sum(rr, red));
+        const double rn = sqrt(block_sum<SB_T>(rr, red));
         rel = bnorm > 0.0 ? rn / bnorm : rn;
         if (rel <= tol || it == max_steps) break;
         __syncthreads();
         solve(rs);
-        for (int i = t; i < n; i += SOLVE_T) xs[i] += rs[i];
+        for (int i = t; i < n; i += SB_T) xs[i] += rs[i];
         __syncthreads();
     }
-    for (int i = t; i < n; i += SOLVE_T) x[i] = xs[i];
+    for (int i = t; i < n; i += SB_T) x[i] = xs[i];
     if (t == 0 && res) res[blockIdx.x] = rel;
 }
 
@@ -773,7 +781,7 @@ cudaError_t launch_solve_batch(const BatchDesc& d, const double* J, const double
                                cudaStream_t st)
 {
     if (d.count <= 0 || d.S <= 0 || R <= 0) return cudaSuccess;
-    solve_batch_kernel<<<d.count * d.S * R, SOLVE_T, 0, st>>>(d, J, B, X, R, sig, tau, tol, max_steps, res);
+    solve_batch_kernel<<<d.count * d.S * R, SB_T, 0, st>>>(d, J, B, X, R, sig, tau, tol, max_steps, res);
     return cudaGetLastError();
 }
 
