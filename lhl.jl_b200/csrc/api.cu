@@ -401,6 +401,8 @@ static int reduce_loaded(lhl_ws_t ws, int balance, cudaStream_t st)
         m.n = (int)n;
         m.A = ws->F;
         m.ipiv = ws->ipiv;
+        m.perm = ws->perm;
+        m.iperm = ws->iperm;
         m.hdr = ws->mhdr;
         m.cval = ws->mcval;
         m.crow = ws->mcrow;
@@ -408,10 +410,10 @@ static int reduce_loaded(lhl_ws_t ws, int balance, cudaStream_t st)
         m.err = ws->err;
         m.limit_ns = ws->limit_ns;
         m.ptimes = ws->probes ? ws->ptimes : nullptr;
-        e = lhl::launch_reduce_mixed(m, ws->mplan, st);
+        e = lhl::launch_reduce_mixed(m, ws->mplan, st);  // writes perm / iperm too
         if (e == cudaSuccess) e = lhl::launch_linv((int)n, ws->F, (int)n, ws->linv, st);
         if (e != cudaSuccess) return LHL_ERR_CUDA;
-        return cuda_status(lhl::launch_ht_perm((int)n, ws->F, ws->Ht, ws->ipiv, ws->perm, ws->iperm, st));
+        return cuda_status(lhl::launch_ht_fill((int)n, ws->F, ws->Ht, st));
     }
     const int mode = n <= 2 ? 0 : (n < 500 ? 1 : 2);
     if (!balance) {

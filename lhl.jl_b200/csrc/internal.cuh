@@ -118,6 +118,8 @@ struct MixArgs {
     int n, rpc, ldr;        // order, rows per CTA, row pitch (floats)
     double* A;              // balanced J in, factors out (n x n, ld n)
     int64_t* ipiv;
+    int64_t* perm;          // out: perm and iperm (1-based), from the final row labels
+    int64_t* iperm;
     unsigned long long* hdr;  // 2 x grid: per CTA and step parity, value << 32 | step << 16 | row
     unsigned long long* cval;  // 2 x n column values by physical row (tagged words)
     unsigned long long* crow;  // 2 x grid x ldr candidate rows (tagged words)
@@ -140,6 +142,7 @@ cudaError_t launch_reduce(RedArgs a, int balance, int mode, cudaStream_t st);
 cudaError_t launch_unblocked_assemble(int n, double* A, const double* B2, const int64_t* ipiv, cudaStream_t st);
 cudaError_t launch_ht_perm(int n, const double* A, double* Ht, const int64_t* ipiv, int64_t* perm, int64_t* iperm,
                            cudaStream_t st);
+cudaError_t launch_ht_fill(int n, const double* A, double* Ht, cudaStream_t st);
 cudaError_t launch_fill_ones(double* a, double* b, int n, cudaStream_t st);
 cudaError_t launch_set_pair(double* a, double* b, double va, double vb, cudaStream_t st);
 size_t stepTabBytes();

@@ -1467,6 +1467,14 @@ cudaError_t launch_ht_perm(int n, const double* A, double* Ht, const int64_t* ip
     return cudaGetLastError();
 }
 
+cudaError_t launch_ht_fill(int n, const double* A, double* Ht, cudaStream_t st)
+{
+    if (n <= 0) return cudaSuccess;
+    dim3 grid((n + 31) / 32, (n + 31) / 32);
+    ht_fill_kernel<<<grid, dim3(32, 8), 0, st>>>(n, A, Ht);
+    return cudaGetLastError();
+}
+
 cudaError_t launch_perm(int n, const int64_t* ipiv, int64_t* perm, int64_t* iperm, cudaStream_t st)
 {
     if (n <= 0) return cudaSuccess;

@@ -31,7 +31,8 @@
 //             warps 1-15 update the candidate row and publish it in the same pass, then apply
 //             the rank-1 row update to the other own rows.
 // At the end every CTA writes its rows, in FP64, to their logical positions of `factors`:
-// the same layout as the plain form (H in the upper Hessenberg part, multipliers below).
+// the same layout as the plain form (H in the upper Hessenberg part, multipliers below); CTA 0
+// also writes perm and iperm, read off its final labels.
 #include "internal.cuh"
 
 namespace lhl {
@@ -525,6 +526,13 @@ __global__ void __launch_bounds__(MT, 1) reduce_mixed_kernel(MixArgs a)
         const int i = e % nr, c = e / nr;
         a.A[(size_t)c * n + (lg[r0 + i] - 1)] = (double)rows[(size_t)i * ldr + c];
     }
+    // ---- perm / iperm (F:376-387) from the final labels: the labels went through the same
+    // interchanges k+1 <-> p, so logical position L holds original row ph[L] + 1 ----
+    if (b == 0)
+        for (int q = t; q < n; q += MT) {
+            a.perm[q] = ph[q + 1] + 1;
+            a.iperm[q] = lg[q];
+        }
 }
 
 static size_t mixed_fixed_smem(int ldr) { return (size_t)ldr * 4 * sizeof(float) + 16 * sizeof(float); }

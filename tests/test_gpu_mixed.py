@@ -60,6 +60,15 @@ def check_similarity(ws, J):
     R = as_oracle(ws)
     ip = R.ipiv
     assert all(k + 2 <= ip[k] <= n for k in range(n - 2)), ip
+    # perm / iperm (written by the reduction kernel from its row labels) are ipiv's (F:376-387)
+    perm = np.arange(1, n + 1)
+    for k in range(n - 2):
+        p = int(ip[k])
+        perm[k + 1], perm[p - 1] = perm[p - 1], perm[k + 1]
+    assert np.array_equal(R.perm, perm)
+    iperm = np.empty(n, dtype=np.int64)
+    iperm[perm - 1] = np.arange(1, n + 1)
+    assert np.array_equal(R.iperm, iperm)
     F = R.factors
     if n > 2:
         assert np.abs(np.tril(F, -2)).max() <= 1.0 + 4 * EPS32
