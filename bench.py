@@ -229,11 +229,12 @@ def main():
             return
         from oracle import oracle as O
         threads = O.num_threads()
-        times, _ = cpu_reference_run(cfg, max(args.steps, 1), 0, threads)
+        warm = max(args.warmup, 0)
+        times, _ = cpu_reference_run(cfg, max(args.steps, 1), warm, threads)
         sec = float(np.mean(times))
         val = S / sec
         line = {"impl": "reference", "metric": METRIC, "value": val, "unit": UNIT, "n_gpus": args.gpus,
-                "steps": len(times), "warmup": 0, "ms_per_step": sec * 1e3, "higher_is_better": True,
+                "steps": len(times), "warmup": warm, "ms_per_step": sec * 1e3, "higher_is_better": True,
                 "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (numpy PCG64 seeds 2,3,4)",
                 "config": config,
                 "cpu_baseline": {"value": val, "unit": UNIT, "cores": threads, "kind": "port",
