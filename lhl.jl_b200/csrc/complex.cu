@@ -33,7 +33,7 @@ template <> __device__ __forceinline__ double hzero<double>() { return 0.0; }
 template <> __device__ __forceinline__ dc hzero<dc>() { return {0.0, 0.0}; }
 
 template <int T, int E, class HV>
-__global__ void __launch_bounds__(T) shift_lu_cplx_kernel(int n, const double* __restrict__ Ht, int ldh,
+__global__ void __launch_bounds__(T, 1) shift_lu_cplx_kernel(int n, const double* __restrict__ Ht, int ldh,
                                                           const double* __restrict__ sig, const double* __restrict__ tau_,
                                                           int s0, double* __restrict__ Gt_all, int ldg, int po,
                                                           uint8_t* __restrict__ swap_all, double* __restrict__ rdiag_all,

@@ -162,3 +162,35 @@ def test_complex_errors_mirror_the_reference():
     Wr = 2.0 * np.eye(n) - 0.5 * J
     b = rng(2).standard_normal(n) + 0j
     assert np.allclose(host(G.lhl_ldiv_(dev(b), wc)), np.linalg.solve(Wr, b), rtol=1e-10, atol=1e-12)
+
+
+@pytest.mark.parametrize("n", [4099, 8192])
+@pytest.mark.parametrize("complex_ht", [False, True])
+def test_complex_shift_bitexact_large(n, complex_ht):
+    """The 1024-thread complex shift LU (4096 < n <= 8192, config 5's size) on a random upper
+    Hessenberg H placed straight into a workspace's Ht: bit for bit against the oracle."""
+    torch, G = _mods()
+    g = rng(n)
+    H = np.triu(g.standard_normal((n, n)), -1)
+    if complex_ht:
+        H = H + 1j * np.triu(g.standard_normal((n, n)), -1)
+    Ht = np.asfortranarray(H.T)
+    if complex_ht:
+        ws = G.LHLWorkspace(n, dtype=torch.complex128)
+    else:
+        ws = G.LHLWorkspace(n, shift_complex=True)
+    ws.Ht.copy_(dev(Ht))
+    R = O.ReductionC(n) if complex_ht else O.Reduction(n)
+    R.Ht = Ht
+    s, t = 0.4 + 0.7j, -1.0 + 0.1j
+    G.lhl_shift_(ws, s, t)
+    So = O.shift_c128(R, s, t) if complex_ht else O.shift_complex(R, s, t)
+    sh = ws.shift
+    Gt = host(sh.Gt())
+    assert sh.info == So.info
+    iu = np.triu_indices(n)
+    for off in (0, sh.po):
+        assert bits_equal(Gt[off:off + n, :n].T[iu], So.Gt[off:off + n, :n].T[iu])
+        assert bits_equal(Gt[off + np.arange(n - 1), np.arange(1, n)], So.Gt[off + np.arange(n - 1), np.arange(1, n)])
+    assert np.array_equal(host(sh.swap())[:n], So.swap[:n])
+    assert bits_equal(host(sh.rdiag()), So.rdiag[:n])
