@@ -701,7 +701,7 @@ __device__ void gemv_tma64(const RedArgs& a, const void* tmA, uint64_t* bars, do
                 const bool act = i >= k0 + 1 && i <= n;
                 const bool psub = pulled && p >= ga && p <= gb;
                 const double bval = (psub && act) ? sub[i - 1] : 0.0;
-                if (!mbar_wait(&bars[s], (ph >> s) & 1u, 1u << 22)) atomicCAS(a.err, 0, (int)LHL_ERR_TIMEOUT);
+                if (!mbar_wait_ns(&bars[s], (ph >> s) & 1u, a.limit_ns)) atomicCAS(a.err, 0, (int)LHL_ERR_TIMEOUT);
                 const double* tl = tiles + (size_t)s * 4096 + r;
                 auto TV = [&](int j) -> double { return (psub && j == p) ? bval : tl[(j - ga) * 64]; };
                 auto LV = [&](int j) -> double {
@@ -1109,7 +1109,7 @@ __device__ bool blocked_phase(const RedArgs& a, GridBarrier& gb, PanelSh& S, uin
                     double sacc = 0.0;
                     const int r = threadIdx.x;
                     for (int s = 0; s < PBOX_SLOTS && s * PBOX_G < P; ++s) {
-                        if (!mbar_wait(&bars[s], (ph >> s) & 1u, 1u << 22)) atomicCAS(a.err, 0, (int)LHL_ERR_TIMEOUT);
+                        if (!mbar_wait_ns(&bars[s], (ph >> s) & 1u, a.limit_ns)) atomicCAS(a.err, 0, (int)LHL_ERR_TIMEOUT);
                         const double* pb = tiles + (size_t)s * RT * PBOX_G;
                         const int gend = min(P - s * PBOX_G, PBOX_G);
                         for (int gg = 0; gg < gend; ++gg) {
