@@ -29,6 +29,14 @@ constexpr int TILE64_BYTES = 64 * 64 * 8;
 constexpr int PBOX_G = 32;     // groups per TMA box of GEMV partials (phase B)
 constexpr int PBOX_BYTES = RT * PBOX_G * 8;
 constexpr int PBOX_SLOTS = 2;
+// A TMA wait gives up after the workspace's wall-time limit, but never sooner than this: a copy
+// in flight completes in microseconds, so a short limit (the tests of the timeout path use 1 ns)
+// still ends the kernel at a grid barrier with no copy in flight into its shared memory.
+constexpr unsigned long long TMA_WAIT_FLOOR_NS = 100000000ull;
+__device__ __forceinline__ unsigned long long tma_wait_ns(const RedArgs& a)
+{
+    return a.limit_ns > TMA_WAIT_FLOOR_NS ? a.limit_ns : TMA_WAIT_FLOOR_NS;
+}
 
 
 // ---------------------------------------------------------------------------------
@@ -701,7 +709,7 @@ __device__ void gemv_tma64(const RedArgs& a, const void* tmA, uint64_t* bars, do
                 const bool act = i >= k0 + 1 && i <= n;
                 const bool psub = pulled && p >= ga && p <= gb;
                 const double bval = (psub && act) ? sub[i - 1] : 0.0;
-                if (!mbar_wait_ns(&bars[s], (ph >> s) & 1u, a.limit_ns)) atomicCAS(a.err, 0, (int)LHL_ERR_TIMEOUT);
+                if (!mbar_wait_ns(&bars[s], (ph >> s) & 1u, tma_wait_ns(a))) atomicCAS(a.err, 0, (int)LHL_ERR_TIMEOUT);
                 const double* tl = tiles + (size_t)s * 4096 + r;
                 auto TV = [&](int j) -> double { return (psub && j == p) ? bval : tl[(j - ga) * 64]; };
                 auto LV = [&](int j) -> double {
@@ -1109,7 +1117,7 @@ __device__ bool blocked_phase(const RedArgs& a, GridBarrier& gb, PanelSh& S, uin
                     double sacc = 0.0;
                     const int r = threadIdx.x;
                     for (int s = 0; s < PBOX_SLOTS && s * PBOX_G < P; ++s) {
-                        if (!mbar_wait_ns(&bars[s], (ph >> s) & 1u, a.limit_ns)) atomicCAS(a.err, 0, (int)LHL_ERR_TIMEOUT);
+                        if (!mbar_wait_ns(&bars[s], (ph >> s) & 1u, tma_wait_ns(a))) atomicCAS(a.err, 0, (int)LHL_ERR_TIMEOUT);
                         const double* pb = tiles + (size_t)s * RT * PBOX_G;
                         const int gend = min(P - s * PBOX_G, PBOX_G);
                         for (int gg = 0; gg < gend; ++gg) {
