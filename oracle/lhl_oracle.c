@@ -53,8 +53,11 @@ void lhlo_balance(int n, double* A, int ld, double* d, double* isc)
             if (c == 0.0 || r == 0.0) continue;
             double f = 1.0;
             double s = c + r;
-            while (c < r / 2.0) { c *= 2.0; r /= 2.0; f *= 2.0; }
-            while (c >= 2.0 * r) { c /= 2.0; r *= 2.0; f /= 2.0; }
+            /* the device's bounds: never reached by finite norms (at most ~2100 steps), they end
+             * the loops where the reference's would not (an infinite norm keeps c >= 2r true) */
+            int guard = 0;
+            while (c < r / 2.0 && guard < 4200) { c *= 2.0; r /= 2.0; f *= 2.0; ++guard; }
+            while (c >= 2.0 * r && guard < 8400) { c /= 2.0; r *= 2.0; f /= 2.0; ++guard; }
             if (c + r < 0.95 * s) {
                 converged = 0;
                 d[i - 1] *= f;
@@ -1202,8 +1205,9 @@ static void cbalance(int n, double* A, int ld, double* d, double* isc)
             if (c == 0.0 || r == 0.0) continue;
             double f = 1.0;
             double s = c + r;
-            while (c < r / 2.0) { c *= 2.0; r /= 2.0; f *= 2.0; }
-            while (c >= 2.0 * r) { c /= 2.0; r *= 2.0; f /= 2.0; }
+            int guard = 0;  /* the device's bounds (see lhlo_balance) */
+            while (c < r / 2.0 && guard < 4200) { c *= 2.0; r /= 2.0; f *= 2.0; ++guard; }
+            while (c >= 2.0 * r && guard < 8400) { c /= 2.0; r *= 2.0; f /= 2.0; ++guard; }
             if (c + r < 0.95 * s) {
                 converged = 0;
                 d[i - 1] *= f;

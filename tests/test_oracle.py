@@ -409,3 +409,19 @@ def test_shift_f32_matches_restatement(n, tie):
             b32 = np.asarray(b).astype(np.float32)
             assert np.array_equal(b32.astype(np.float64), np.asarray(b)), "not float values"
             assert np.array_equal(a32.view(np.int32), b32.view(np.int32)), (s, t)
+
+
+def test_balancing_ends_on_an_infinite_norm():
+    """An infinite entry: the reference's balancing loops never end (c = r = Inf keeps c >= 2r true,
+    F:313-320); the oracle carries the device's bounds on them, which finite norms never reach, and
+    decides "no scaling" for such an index.  Pivots stay valid row indices and the NaNs propagate."""
+    n = 40
+    J = rng(7).standard_normal((n, n))
+    J[n - 3, 3] = np.inf
+    J[5, 7] = np.nan
+    R = O.reduce(J)
+    assert all(k + 2 <= R.ipiv[k] <= n for k in range(n - 2))
+    assert np.isnan(R.factors).any()
+    assert np.all(R.scale * R.iscale == 1.0)
+    C = O.reduce_c128(J.astype(np.complex128))
+    assert all(k + 2 <= C.ipiv[k] <= n for k in range(n - 2))
