@@ -70,7 +70,8 @@ def sharded_chain(G, ws, J: torch.Tensor, B: torch.Tensor, sigmas: torch.Tensor,
     """The per-shift chain on this rank's slice of the shifts of an already reduced workspace:
     shift LUs, solves, refinement to `tol` (GMRES-IR or fixed-point), then the gather.
     B holds all S * R right-hand sides; returns (X with every rank's columns, this rank's
-    relative residuals)."""
+    relative residuals).  Complex shifts (complex sigmas or taus, on a real reduction) and a
+    complex J's workspace take a complex shift object and complex right-hand sides."""
     import torch.distributed as dist
     world = dist.get_world_size(group)
     rank = dist.get_rank(group)
@@ -82,7 +83,8 @@ def sharded_chain(G, ws, J: torch.Tensor, B: torch.Tensor, sigmas: torch.Tensor,
         X_local = torch.empty((n, 0), dtype=B.dtype, device=B.device)
         res = torch.empty(0, dtype=torch.float64, device=B.device)
     else:
-        sh = G.LHLShift(n, cnt)
+        cplx = sigmas.is_complex() or taus.is_complex() or getattr(ws, "dtype", None) == torch.complex128
+        sh = G.LHLShift(n, cnt, complex=cplx)
         G.lhl_shift_batched_(sh, ws, sigmas[s0:s0 + cnt].contiguous(), taus[s0:s0 + cnt].contiguous())
         Bl = B[:, s0 * R:(s0 + cnt) * R]
         X_local = torch.empty((cnt * R, n), dtype=B.dtype, device=B.device).t()

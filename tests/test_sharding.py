@@ -53,8 +53,12 @@ def _worker(rank, world, port, q):
         # the rank's columns hold their global column index in every row
         X = torch.arange(s0 * R, (s0 + cnt) * R, dtype=torch.float64).repeat(n, 1)
         full = SH.gather_columns(X, S, R)
+        # complex columns (complex shifts, a complex J): the same gather, imaginary part -index
+        Xc = torch.complex(X, -X)
+        fullc = SH.gather_columns(Xc, S, R)
         t = bench.max_over_ranks([1.0 + rank, 5.0 - rank], "cpu", dist)
-        q.put((rank, full.numpy().tolist(), t))
+        q.put((rank, full.numpy().tolist(), t, fullc.real.numpy().tolist(), fullc.imag.numpy().tolist(),
+               str(fullc.dtype)))
     finally:
         dist.destroy_process_group()
 
@@ -71,6 +75,8 @@ def test_two_ranks_gather_and_max_over_ranks():
         p.join(timeout=60)
         assert p.exitcode == 0
     want = np.tile(np.arange(10.0), (7, 1))
-    for rank, full, t in out:
+    for rank, full, t, cre, cim, cdt in out:
         assert np.array_equal(np.array(full), want), rank
         assert t == [2.0, 5.0]
+        assert cdt == "torch.complex128"
+        assert np.array_equal(np.array(cre), want) and np.array_equal(np.array(cim), -want), rank
