@@ -441,6 +441,11 @@ __device__ __forceinline__ int warp_combine(const RedArgs& a, double& pivs)
         const double sb = __shfl_xor_sync(0xffffffffu, sv, o);
         if (ib != 0 && (vi == 0 || b > v || (b == v && ib < vi))) { v = b; vi = ib; sv = sb; }
     }
+    // lane 0's result for every lane: with NaN candidates the comparison is no total order, and
+    // the butterfly could leave lanes with different winners (and the threads of a CTA with
+    // different branches around its barriers); lane 0 computes the same in every warp and CTA
+    vi = __shfl_sync(0xffffffffu, vi, 0);
+    sv = __shfl_sync(0xffffffffu, sv, 0);
     pivs = sv;
     return vi;
 }
