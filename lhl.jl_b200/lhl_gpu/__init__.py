@@ -32,6 +32,8 @@ _LIB_PATH = os.path.join(os.path.dirname(_HERE), "liblhl_gpu.so")
 
 LHL_OK, LHL_ERR_ARG, LHL_ERR_DIM, LHL_ERR_CUDA, LHL_ERR_TIMEOUT, LHL_ERR_ALLOC = range(6)
 LHL_PREC_FP64, LHL_PREC_MIXED = 0, 1
+# the arrays a reduction leaves in a workspace, in lhl_ws_import's argument order
+REDUCTION_ARRAYS = ("factors", "Ht", "ipiv", "perm", "iperm", "scale", "iscale")
 
 
 class ArgumentError(ValueError):
@@ -290,6 +292,7 @@ class LHLWorkspace:
         else:
             raise ArgumentError(f"element type {dtype} is not supported (float64, float32 or complex128)")
         self.dtype = dtype
+        self.device = torch.device("cuda", torch.cuda.current_device())  # where its arrays live
         self.n = int(n)
         self.precision = precision
         self.shift_complex = bool(shift_complex)
@@ -387,17 +390,38 @@ class LHLWorkspace:
         elif "c128" in d and bool(d["c128"]):
             dt = torch.complex128
         ws = cls(int(d["n"]), int(d["precision"]), bool(d["shift_complex"]), dtype=dt)
-        n = ws.n
-        dev = {k: torch.as_tensor(np.ascontiguousarray(d[k])).cuda() for k in ("ipiv", "perm", "iperm", "scale", "iscale")}
-        if n:
-            for k in ("factors", "Ht"):  # (n, n) matrices, column-major on the device
-                dev[k] = _colmajor(torch.as_tensor(np.asarray(d[k])).cuda())
-            _check(_lib.lhl_ws_import(ws._h, *[C.c_void_p(dev[k].data_ptr()) for k in
-                                               ("factors", "Ht", "ipiv", "perm", "iperm", "scale", "iscale")],
-                                      _stream(stream)), "lhl_ws_import")
-            (stream or torch.cuda.current_stream()).synchronize()
-        ws.reduced = True
+        ws.import_arrays({k: torch.as_tensor(np.asarray(d[k])).cuda() for k in REDUCTION_ARRAYS}, stream)
+        (stream or torch.cuda.current_stream()).synchronize()
         return ws
+
+    def import_arrays(self, arrays, stream=None) -> "LHLWorkspace":
+        """Take a reduction made elsewhere (lhl_ws_import of the C ABI): `arrays` maps the names
+        of REDUCTION_ARRAYS to CUDA tensors, factors and Ht (n, n) of the workspace's element
+        storage (complex128 for a complex J, float64 otherwise), ipiv (n-2), perm and iperm (n)
+        int64, scale and iscale (n) float64.  Copies are taken on the stream; the arrays may be
+        released once it has passed them."""
+        n = self.n
+        mat = torch.complex128 if self.dtype == torch.complex128 else torch.float64
+        want = {"factors": (mat, (n, n)), "Ht": (mat, (n, n)), "ipiv": (torch.int64, (max(n - 2, 0),)),
+                "perm": (torch.int64, (n,)), "iperm": (torch.int64, (n,)), "scale": (torch.float64, (n,)),
+                "iscale": (torch.float64, (n,))}
+        dev = {}
+        for k in REDUCTION_ARRAYS:
+            t = arrays[k]
+            dt, shape = want[k]
+            if not isinstance(t, torch.Tensor) or not t.is_cuda or t.dtype != dt:
+                raise ArgumentError(f"{k} must be a CUDA {dt} tensor")
+            if tuple(t.shape) != shape:
+                raise DimensionMismatch(f"{k} has shape {tuple(t.shape)}, expected {shape}")
+            if t.dim() == 2:  # column-major with leading dimension n
+                dev[k] = t if (t.stride(0) == 1 and t.stride(1) == n) else t.t().contiguous().t()
+            else:
+                dev[k] = t.contiguous()
+        if n:
+            _check(_lib.lhl_ws_import(self._h, *[C.c_void_p(dev[k].data_ptr()) for k in REDUCTION_ARRAYS],
+                                      _stream(stream)), "lhl_ws_import")
+        self.reduced = True
+        return self
 
     def set_probes(self, on: bool = True):
         """Record the reduction's device timers (phase_ns, probe_ns); off by default."""

@@ -65,6 +65,89 @@ def gather_columns(X_local: torch.Tensor, S: int, rhs_per_shift: int, group=None
     return torch.cat(cols, 0).t()
 
 
+_REDUCTION_ARRAYS = ("factors", "Ht", "ipiv", "perm", "iperm", "scale", "iscale")
+
+
+def reduction_layout(n: int, complex_j: bool = False):
+    """(name, 8-byte words) of each array of a reduction of order n, in the packed order:
+    factors and Ht column-major (interleaved re, im for a complex J), ipiv (n-2), perm and
+    iperm int64, scale and iscale float64."""
+    nn = n * n * (2 if complex_j else 1)
+    words = {"factors": nn, "Ht": nn, "ipiv": max(n - 2, 0), "perm": n, "iperm": n, "scale": n, "iscale": n}
+    return [(k, words[k]) for k in _REDUCTION_ARRAYS]
+
+
+def pack_reduction(arrays, n: int, complex_j: bool = False) -> torch.Tensor:
+    """One float64 buffer holding the arrays of a reduction (names and shapes as
+    LHLWorkspace.import_arrays takes them) in `reduction_layout` order; the int64 arrays are
+    carried bit for bit."""
+    parts = []
+    for k, _ in reduction_layout(n, complex_j):
+        t = arrays[k]
+        if t.dim() == 2:  # column-major flat: rows of the transpose
+            t = t.t().contiguous()
+            t = torch.view_as_real(t) if t.is_complex() else t
+        parts.append(t.contiguous().reshape(-1).view(torch.float64))
+    return torch.cat(parts) if parts else torch.empty(0, dtype=torch.float64)
+
+
+def unpack_reduction(buf: torch.Tensor, n: int, complex_j: bool = False):
+    """The arrays of `pack_reduction`'s buffer as views of it: factors and Ht (n, n)
+    column-major (complex128 for a complex J), ipiv, perm, iperm int64, scale, iscale."""
+    out, o = {}, 0
+    for k, w in reduction_layout(n, complex_j):
+        seg = buf[o:o + w]
+        o += w
+        if k in ("factors", "Ht"):
+            m = torch.view_as_complex(seg.view(n, n, 2)) if complex_j else seg.view(n, n)
+            out[k] = m.t()
+        elif k in ("ipiv", "perm", "iperm"):
+            out[k] = seg.view(torch.int64)
+        else:
+            out[k] = seg
+    if o != buf.numel():
+        raise ValueError(f"buffer of {buf.numel()} words for a reduction of {o}")
+    return out
+
+
+def broadcast_reduction(ws, src: int = 0, group=None):
+    """Share one rank's reduction with every rank of the group, in place of reducing J on
+    each: rank `src` (a global rank, as torch.distributed.broadcast takes it) holds the
+    reduction; the others' workspaces, of the same order, element type and form, import it
+    (lhl_ws_import).  One collective of 8 n^2 (16 n^2 for a complex J) bytes plus small
+    arrays.  A header broadcast and a flag reduction first make every rank raise together
+    when a workspace differs, so that no rank waits in the data broadcast alone."""
+    import torch.distributed as dist
+    cj = ws.dtype == torch.complex128
+    codes = {torch.float64: 0, torch.float32: 1, torch.complex128: 2}
+    dev = ws.device
+    me = dist.get_rank()
+    mine = torch.tensor([ws.n, int(ws.precision), codes[ws.dtype], int(bool(ws.reduced))],
+                        dtype=torch.int64, device=dev)
+    head = mine.clone()
+    dist.broadcast(head, src, group=group)
+    bad = 0
+    if me == src:
+        bad = 0 if ws.reduced else 1
+    elif not torch.equal(head[:3], mine[:3]):
+        bad = 2
+    flag = torch.tensor([bad], dtype=torch.int64, device=dev)
+    dist.all_reduce(flag, op=dist.ReduceOp.MAX, group=group)
+    if int(flag.item()) == 1:
+        raise ValueError(f"rank {src} holds no reduction to broadcast")
+    if int(flag.item()) == 2:
+        raise ValueError(f"workspaces differ from rank {src}'s (order, form, element type {head.tolist()[:3]})")
+    words = sum(w for _, w in reduction_layout(ws.n, cj))
+    if me == src:
+        buf = pack_reduction({k: getattr(ws, k) for k in _REDUCTION_ARRAYS}, ws.n, cj)
+    else:
+        buf = torch.empty(words, dtype=torch.float64, device=dev)
+    dist.broadcast(buf, src, group=group)
+    if me != src:
+        ws.import_arrays(unpack_reduction(buf, ws.n, cj))
+    return ws
+
+
 def sharded_chain(G, ws, J: torch.Tensor, B: torch.Tensor, sigmas: torch.Tensor, taus: torch.Tensor,
                   rhs_per_shift: int = 1, tol: float = 1e-10, refine: str = "gmres", group=None):
     """The per-shift chain on this rank's slice of the shifts of an already reduced workspace:
