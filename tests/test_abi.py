@@ -82,6 +82,38 @@ def test_null_handles_rejected_on_host():
                                      vp(0)) == 1
 
 
+def handle_functions():
+    """(name, ctypes argument types) of every declared entry point whose first argument is a
+    workspace, shift object or batch handle, read from the header."""
+    src = re.sub(r"/\*.*?\*/", "", open(HEADER).read(), flags=re.S)
+    scalars = {"int64_t": ctypes.c_int64, "int": ctypes.c_int, "double": ctypes.c_double,
+               "uint64_t": ctypes.c_uint64}
+    out = []
+    for name, params in re.findall(r"\bint\s+(lhl_\w+)\s*\(([^)]*)\)\s*;", src):
+        params = [p.strip() for p in params.split(",")]
+        if params[0].split()[0] not in ("lhl_ws_t", "lhl_shift_t", "lhl_batch_t"):
+            continue
+        types = []
+        for p in params:
+            ty = p.replace("const ", "").split()[0]
+            types.append(ctypes.c_void_p if ("*" in p or ty.startswith("lhl_")) else scalars[ty])
+        out.append((name, types))
+    return out
+
+
+def test_every_handle_entry_point_refuses_a_null_handle():
+    """LHL_ERR_ARG from every call on a null handle, other arguments zero or one, before any
+    device call (the library is loaded here without a GPU)."""
+    L = ctypes.CDLL(LIB)
+    fns = handle_functions()
+    assert len(fns) >= 30
+    for name, types in fns:
+        f = getattr(L, name)
+        f.argtypes = types
+        args = [None if t is ctypes.c_void_p else t(0.0 if t is ctypes.c_double else 1) for t in types]
+        assert f(*args) == 1, name
+
+
 def test_configs_are_seeded_and_shaped():
     import sys
     sys.path.insert(0, os.path.join(REPO, "lhl.jl_b200"))
