@@ -114,6 +114,32 @@ def test_every_handle_entry_point_refuses_a_null_handle():
         assert f(*args) == 1, name
 
 
+def test_creators_check_sizes_and_pointers_on_host():
+    """Shift objects, batches and the allocation-free reduction: DimensionMismatch for bad
+    orders, counts or leading dimensions, ArgumentError for null pointers, before any device
+    call."""
+    C = ctypes
+    L = C.CDLL(LIB)
+    vp, i64, i32 = C.c_void_p, C.c_int64, C.c_int
+    h = vp()
+    for name in ("lhl_shift_create", "lhl_shift_create_complex"):
+        f = getattr(L, name)
+        f.argtypes = [i64, i64, C.POINTER(vp)]
+        assert f(-1, 1, C.byref(h)) == 2 and f(4, -1, C.byref(h)) == 2 and f(4, 1, None) == 1, name
+    L.lhl_batch_create.argtypes = [i64, vp, i64, C.POINTER(vp)]
+    ok_ns = (i64 * 2)(4, 5)
+    assert L.lhl_batch_create(2, C.cast((i64 * 2)(4, -3), vp), 1, C.byref(h)) == 2
+    assert L.lhl_batch_create(2, C.cast(ok_ns, vp), -1, C.byref(h)) == 2
+    assert L.lhl_batch_create(0, C.cast(ok_ns, vp), 1, C.byref(h)) == 2
+    assert L.lhl_batch_create(2, None, 1, C.byref(h)) == 1
+    assert L.lhl_batch_create(2, C.cast(ok_ns, vp), 1, None) == 1
+    L.lhl_reduce_noalloc.argtypes = [i64, vp, i64, i32] + [vp] * 8
+    assert L.lhl_reduce_noalloc(-1, None, 1, 1, *([None] * 8)) == 2
+    assert L.lhl_reduce_noalloc(8, None, 8, 1, *([None] * 8)) == 1
+    assert L.lhl_reduce_noalloc(8, 1, 4, 1, *([1] * 7), None) == 2      # ldj < n
+    assert L.lhl_reduce_noalloc(2000, 1, 2000, 1, *([1] * 7), None) == 2  # above its order limit
+
+
 def test_configs_are_seeded_and_shaped():
     import sys
     sys.path.insert(0, os.path.join(REPO, "lhl.jl_b200"))
