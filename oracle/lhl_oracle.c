@@ -1268,17 +1268,198 @@ static void creduce_unblocked(int n, double* A, int ld, int64_t* ipiv)
     }
 }
 
-/* lhl_reduce! for a complex J (F:355-405): copy, balance, unblocked reduction, Ht fill     */
-/* (Ht[j,i] = H[i,j] for i <= j+1, zero elsewhere), perm / iperm.                            */
-int lhlo_reduce_c128(int n, const double* J, int ldj, int balance, double* F, int ldf, int64_t* ipiv, double* scale,
-                     double* iscale, int64_t* perm, int64_t* iperm, double* Ht)
+/* ------------------------------------------------------------------------------------ */
+/* Blocked reduction for a complex J: the generic path the reference takes for ComplexF64  */
+/* at n >= 768 (F:398-399, F:705), restated with Julia's Complex arithmetic (products      */
+/* (ac - bd, ad + bc), no fused operations, robust division, pivot on the modulus):        */
+/* driver F:765-783; panel steps F:787-850; interchanges F:857-890; row swap sweep        */
+/* F:1336-1342; GEMV F:1418-1440; TRSM F:1917-1927; GEMM F:1676-1689 (b = sgn * B          */
+/* element, sgn = -one(T) = (-1, -0) or one(T) = (1, 0)); top GEMM F:1588-1607 with its    */
+/* fix-up F:1598-1606; deferred swaps F:1383-1393.                                         */
+/* ------------------------------------------------------------------------------------ */
+
+/* w[r0:r1] = sum_{j=c0}^{c1} A[j,k] * A[r0:r1, j] from w = 0, four columns per pass.      */
+static void cgemv_cols(cplx* w, const double* A, int ld, int k, int r0, int r1, int c0, int c1)
 {
-    if (n < 0 || ldj < n || ldf < n) return -1;
+#pragma omp parallel for schedule(static) if (r1 - r0 >= 512)
+    for (int i = r0; i <= r1; ++i) {
+        cplx acc = {0.0, 0.0};
+        int j = c0;
+        while (j + 3 <= c1) {
+            cplx l1 = CM1(A, ld, j, k), l2 = CM1(A, ld, j + 1, k), l3 = CM1(A, ld, j + 2, k),
+                 l4 = CM1(A, ld, j + 3, k);
+            acc = c_add(acc, c_add(c_add(c_mul(l1, CM1(A, ld, i, j)), c_mul(l2, CM1(A, ld, i, j + 1))),
+                                   c_add(c_mul(l3, CM1(A, ld, i, j + 2)), c_mul(l4, CM1(A, ld, i, j + 3)))));
+            j += 4;
+        }
+        while (j <= c1) {
+            cplx lj = CM1(A, ld, j, k);
+            if (!c_iszero(lj)) acc = c_add(acc, c_mul(lj, CM1(A, ld, i, j)));
+            j += 1;
+        }
+        w[i - 1] = acc;
+    }
+}
+
+/* A[i0:i1, c0:c1] += A[i0:i1, j0:j1] * (sgn * A[r0:r0+K-1, cB:cB+(c1-c0)]). */
+static void cgemm_generic(double* A, int ld, int i0, int i1, int j0, int j1, int r0, int cB, int c0, int c1,
+                          cplx sgn)
+{
+    if (i1 < i0 || j1 < j0 || c1 < c0) return;
+#pragma omp parallel for schedule(static) if ((long)(c1 - c0 + 1) * (i1 - i0 + 1) >= 65536)
+    for (int c = c0; c <= c1; ++c) {
+        for (int j = j0; j <= j1; ++j) {
+            int jj = j - j0 + 1;
+            cplx b = c_mul(sgn, CM1(A, ld, r0 + jj - 1, cB + c - c0));
+            if (c_iszero(b)) continue;
+            for (int i = i0; i <= i1; ++i) CM1(A, ld, i, c) = c_add(CM1(A, ld, i, c), c_mul(CM1(A, ld, i, j), b));
+        }
+    }
+}
+
+static void cstep_swaps(int n, double* A, int ld, double* B0, int ldb, const int64_t* ipiv, int k0, int kb, int k,
+                        int p)
+{
+    for (int j = k0; j <= kb + 1; ++j) {
+        if (j == k) continue;
+        cswap(&CM1(A, ld, k + 1, j), &CM1(A, ld, p, j));
+    }
+    if (p <= kb + 1) {
+        for (int i = 1; i <= n; ++i) {
+            cswap(&CM1(A, ld, i, k + 1), &CM1(A, ld, i, p));
+            cswap(&CM1(B0, ldb, i, k + 1 - k0), &CM1(B0, ldb, i, p - k0));
+        }
+    } else {
+        for (int i = 1; i <= n; ++i) {
+            cplx t = CM1(A, ld, i, p);
+            CM1(A, ld, i, p) = CM1(B0, ldb, i, k + 1 - k0);
+            CM1(B0, ldb, i, k + 1 - k0) = t;
+            CM1(A, ld, i, k + 1) = t;
+        }
+        for (int kk = k0; kk <= k; ++kk) {
+            int q = (int)ipiv[kk - 1];
+            if (q != kk + 1) cswap(&CM1(A, ld, kk + 1, k + 1), &CM1(A, ld, q, k + 1));
+        }
+        for (int kk = k0; kk <= k - 1; ++kk) {
+            cplx x = CM1(A, ld, kk + 1, k + 1);
+            if (c_iszero(x)) continue;
+            for (int i = kk + 2; i <= n; ++i)
+                CM1(A, ld, i, k + 1) = c_sub(CM1(A, ld, i, k + 1), c_mul(CM1(A, ld, i, kk), x));
+        }
+    }
+}
+
+static void cpanel_steps(int n, double* A, int ld, int64_t* ipiv, double* B0, int ldb, cplx* w, int k0, int kb)
+{
+    for (int j = k0 + 1; j <= kb + 1; ++j)
+        for (int i = 1; i <= n; ++i) CM1(B0, ldb, i, j - k0) = CM1(A, ld, i, j);
+    for (int k = k0; k <= kb; ++k) {
+        int p = k + 1;
+        double amax = c_abs(CM1(A, ld, k + 1, k));
+        for (int i = k + 2; i <= n; ++i) {
+            double a = c_abs(CM1(A, ld, i, k));
+            if (a > amax) { amax = a; p = i; }
+        }
+        ipiv[k - 1] = p;
+        if (p != k + 1) {
+            cswap(&CM1(A, ld, k + 1, k), &CM1(A, ld, p, k));
+            cstep_swaps(n, A, ld, B0, ldb, ipiv, k0, kb, k, p);
+        }
+        cplx piv = CM1(A, ld, k + 1, k);
+        if (c_iszero(piv)) continue;
+        for (int i = k + 2; i <= n; ++i) CM1(A, ld, i, k) = c_div(CM1(A, ld, i, k), piv);
+        for (int j = k + 1; j <= kb + 1; ++j) {
+            cplx pj = CM1(A, ld, k + 1, j);
+            if (c_iszero(pj)) continue;
+            for (int i = k + 2; i <= n; ++i) CM1(A, ld, i, j) = c_sub(CM1(A, ld, i, j), c_mul(CM1(A, ld, i, k), pj));
+        }
+        for (int j = k + 2; j <= kb + 1; ++j) {
+            cplx vj = CM1(A, ld, j, k);
+            if (c_iszero(vj)) continue;
+            for (int i = k0 + 1; i <= n; ++i)
+                CM1(A, ld, i, k + 1) = c_add(CM1(A, ld, i, k + 1), c_mul(vj, CM1(A, ld, i, j)));
+        }
+        if (!(kb + 2 <= n)) continue;
+        cgemv_cols(w, A, ld, k, k0 + 1, n, kb + 2, n);
+        for (int kk = k0; kk <= k; ++kk) {
+            int q = (int)ipiv[kk - 1];
+            if (q != kk + 1) cswap(&w[kk], &w[q - 1]);
+        }
+        for (int kk = k0; kk <= k; ++kk) {
+            cplx x = w[kk];
+            if (c_iszero(x)) continue;
+            for (int i = kk + 2; i <= n; ++i) w[i - 1] = c_sub(w[i - 1], c_mul(CM1(A, ld, i, kk), x));
+        }
+        for (int i = k0 + 1; i <= n; ++i) CM1(A, ld, i, k + 1) = c_add(CM1(A, ld, i, k + 1), w[i - 1]);
+    }
+}
+
+static void creduce_blocked(int n, double* A, int ld, int64_t* ipiv, int nb)
+{
+    if (n < 3) return;
+    const cplx minus_one = {-1.0, -0.0}, one = {1.0, 0.0};
+    int ldb = n;
+    double* B0 = (double*)malloc(sizeof(cplx) * (size_t)n * (size_t)(nb + 1));
+    cplx* w = (cplx*)malloc(sizeof(cplx) * (size_t)n);
+    for (int k0 = 1; k0 <= n - 2; k0 += nb) {
+        int kb = k0 + nb - 1 < n - 2 ? k0 + nb - 1 : n - 2;
+        cpanel_steps(n, A, ld, ipiv, B0, ldb, w, k0, kb);
+        if (kb + 2 <= n) {
+#pragma omp parallel for schedule(static) if (n >= 512)
+            for (int c = kb + 2; c <= n; ++c)
+                for (int k = k0; k <= kb; ++k) {
+                    int p = (int)ipiv[k - 1];
+                    if (p != k + 1) cswap(&CM1(A, ld, k + 1, c), &CM1(A, ld, p, c));
+                }
+#pragma omp parallel for schedule(static) if (n >= 512)
+            for (int c = kb + 2; c <= n; ++c)
+                for (int k = k0; k <= kb; ++k) {
+                    cplx x = CM1(A, ld, k + 1, c);
+                    if (c_iszero(x)) continue;
+                    for (int i = k + 2; i <= kb + 1; ++i)
+                        CM1(A, ld, i, c) = c_sub(CM1(A, ld, i, c), c_mul(CM1(A, ld, i, k), x));
+                }
+            cgemm_generic(A, ld, kb + 2, n, k0, kb, k0 + 1, kb + 2, kb + 2, n, minus_one);
+        }
+        for (int k = k0; k <= kb; ++k)
+            for (int j = k + 2; j <= kb + 1; ++j) {
+                cplx vj = CM1(A, ld, j, k);
+                if (c_iszero(vj)) continue;
+                for (int i = 1; i <= k0; ++i)
+                    CM1(A, ld, i, k + 1) = c_add(CM1(A, ld, i, k + 1), c_mul(vj, CM1(A, ld, i, j)));
+            }
+        for (int kk = kb + 2; kk <= n; kk += nb) {
+            int ke = kk + nb - 1 < n ? kk + nb - 1 : n;
+            cgemm_generic(A, ld, 1, k0, kk, ke, kk, k0, k0 + 1, kb + 1, one);
+        }
+    }
+    for (int k0 = 1; k0 <= n - 2; k0 += nb) {
+        int kb = k0 + nb - 1 < n - 2 ? k0 + nb - 1 : n - 2;
+        for (int c = k0; c <= kb; ++c)
+            for (int k = kb + 1; k <= n - 2; ++k) {
+                int p = (int)ipiv[k - 1];
+                if (p != k + 1) cswap(&CM1(A, ld, k + 1, c), &CM1(A, ld, p, c));
+            }
+    }
+    free(B0);
+    free(w);
+}
+
+/* lhl_reduce! for a complex J (F:355-405): copy, balance, reduction, Ht fill               */
+/* (Ht[j,i] = H[i,j] for i <= j+1, zero elsewhere), perm / iperm.                            */
+/* path 0: the unblocked order at every n (the device's); 1: the generic blocked order     */
+/* (panels of nb); 2: the reference's choice, blocked with nb = 16 iff n >= 768 (F:398).    */
+int lhlo_reduce_c128_path(int n, const double* J, int ldj, int balance, double* F, int ldf, int64_t* ipiv,
+                          double* scale, double* iscale, int64_t* perm, int64_t* iperm, double* Ht, int path, int nb)
+{
+    if (n < 0 || ldj < n || ldf < n || path < 0 || path > 2 || nb < 1) return -1;
     for (int j = 1; j <= n; ++j)
         for (int i = 1; i <= n; ++i) CM1(F, ldf, i, j) = CM1(J, ldj, i, j);
     if (balance) cbalance(n, F, ldf, scale, iscale);
     else for (int i = 0; i < n; ++i) { scale[i] = 1.0; iscale[i] = 1.0; }
-    creduce_unblocked(n, F, ldf, ipiv);
+    if (path == 2) { path = n >= 768 ? 1 : 0; nb = 16; }
+    if (path == 1) creduce_blocked(n, F, ldf, ipiv, nb);
+    else creduce_unblocked(n, F, ldf, ipiv);
     if (Ht) {
         memset(Ht, 0, sizeof(double) * 2 * (size_t)n * (size_t)n);
         for (int i = 1; i <= n; ++i)
@@ -1291,6 +1472,12 @@ int lhlo_reduce_c128(int n, const double* J, int ldj, int balance, double* F, in
     }
     for (int i = 1; i <= n; ++i) iperm[perm[i - 1] - 1] = i;
     return 0;
+}
+
+int lhlo_reduce_c128(int n, const double* J, int ldj, int balance, double* F, int ldf, int64_t* ipiv, double* scale,
+                     double* iscale, int64_t* perm, int64_t* iperm, double* Ht)
+{
+    return lhlo_reduce_c128_path(n, J, ldj, balance, F, ldf, ipiv, scale, iscale, perm, iperm, Ht, 0, 16);
 }
 
 /* The shift LU of lhlo_shift_complex with tau * Ht[j,k] a complex product (Ht complex). */

@@ -65,6 +65,8 @@ def lib():
         L.lhlo_cabs.restype = d
         L.lhlo_reduce_c128.argtypes = [i, _dv, i, i, _dv, i, _iv, _dv, _dv, _iv, _iv, _dv]
         L.lhlo_reduce_c128.restype = i
+        L.lhlo_reduce_c128_path.argtypes = [i, _dv, i, i, _dv, i, _iv, _dv, _dv, _iv, _iv, _dv, i, i]
+        L.lhlo_reduce_c128_path.restype = i
         L.lhlo_shift_c128.argtypes = [i, _dv, i, d, d, d, d, _dp, i, i, _u8, _dv, _dv]
         L.lhlo_shift_c128.restype = i
         L.lhlo_applyZinv_c128.argtypes = [i, _dv, i, _iv, _dv, _dv]
@@ -478,8 +480,10 @@ def cabs(z) -> float:
     return float(lib().lhlo_cabs(z.real, z.imag))
 
 
-def reduce_c128(J, balance=True) -> ReductionC:
-    """``lhl(J; balance)`` for a complex J (unblocked ELMHES at every n)."""
+def reduce_c128(J, balance=True, path=0, nb=16) -> ReductionC:
+    """``lhl(J; balance)`` for a complex J.  path 0: the unblocked ELMHES at every n (the
+    device's order); 1: the generic blocked order with panels of nb; 2: the reference's
+    choice, blocked (nb = 16) iff n >= 768 (F:398, F:705)."""
     J = np.asfortranarray(J, dtype=np.complex128)
     n = J.shape[0]
     R = ReductionC(n)
@@ -490,7 +494,7 @@ def reduce_c128(J, balance=True) -> ReductionC:
     ip = _ipiv_buf(n)
     sc, isc = np.ones(m), np.ones(m)
     pm, ipm = np.zeros(m, dtype=np.int64), np.zeros(m, dtype=np.int64)
-    rc = lib().lhlo_reduce_c128(n, Jf, m, int(balance), F, m, ip, sc, isc, pm, ipm, Ht)
+    rc = lib().lhlo_reduce_c128_path(n, Jf, m, int(balance), F, m, ip, sc, isc, pm, ipm, Ht, int(path), int(nb))
     assert rc == 0
     R.factors = F.view(np.complex128).reshape((m, m), order="F")[:n, :n].copy(order="F")
     R.Ht = Ht.view(np.complex128).reshape((m, m), order="F")[:n, :n].copy(order="F")

@@ -155,3 +155,62 @@ def test_complex_tie_matrix_pivots_first_max():
         Ri = O.reduce_c128(1j * J.astype(np.complex128))
         assert np.array_equal(Rr.ipiv, Rc.ipiv)
         assert np.array_equal(Rc.ipiv, Ri.ipiv)
+
+
+# The reference's blocked generic reduction, which it runs for a complex J at n >= 768
+# (src/LHLFactorization.jl:398, :705): the blocked order restated in the oracle (path 1).
+@pytest.mark.parametrize("nb", [1, 3, 16])
+@pytest.mark.parametrize("n", [3, 4, 17, 80, 200])
+def test_complex_blocked_reconstructs_J(n, nb):
+    g = np.random.default_rng(n + 7 * nb)
+    J = crandn(g, n, n)
+    R = O.reduce_c128(J, True, path=1, nb=nb)
+    Z, Zi = R.Z(), R.Zinv()
+    H = np.triu(R.factors, -1)
+    assert np.linalg.norm(Z @ H @ Zi - J) <= 1e-10 * np.linalg.norm(J)
+    assert np.all(np.abs(np.tril(R.factors, -2)) <= 1.0)
+    assert np.array_equal(R.Ht, H.T)
+
+
+@pytest.mark.parametrize("kind", ["randn", "tie"])
+@pytest.mark.parametrize("n", [5, 40, 100, 300])
+def test_complex_blocked_pivots_match_unblocked(n, kind):
+    """test/threading.jl:58-79 and test/core_tests.jl:61-92 with a complex J: the blocked and
+    unblocked orders take the same pivots, and their factors differ by at most 100 n eps ||F||."""
+    g = np.random.default_rng(n)
+    if kind == "tie":
+        J = (g.integers(-2, 3, (n, n)) + 1j * g.integers(-2, 3, (n, n))).astype(np.complex128)
+    else:
+        J = crandn(g, n, n)
+    U = O.reduce_c128(J, True, path=0)
+    for nb in (2, 16):
+        B = O.reduce_c128(J, True, path=1, nb=nb)
+        assert np.array_equal(U.ipiv, B.ipiv), nb
+        assert np.array_equal(U.scale, B.scale)
+        assert np.linalg.norm(B.factors - U.factors) <= 100 * n * np.finfo(float).eps * np.linalg.norm(U.factors)
+
+
+def _same_bits(a, b):
+    return np.array_equal(np.ascontiguousarray(a).view(np.uint8), np.ascontiguousarray(b).view(np.uint8))
+
+
+def test_reference_order_above_768_against_the_device_order():
+    """The reference's choice (path 2) is the unblocked order below n = 768 and the blocked one
+    (nb = 16) from 768 on.  The device runs the unblocked order at every n, bit for bit with
+    path 0; at n = 800 its pivots equal the reference order's and H and L lie within
+    100 n eps of it (measured: about 1e-11 relative)."""
+    g = np.random.default_rng(800)
+    J = crandn(g, 767, 767) / math.sqrt(767)
+    a, b = O.reduce_c128(J, path=2), O.reduce_c128(J, path=0)
+    assert _same_bits(a.factors, b.factors)
+    n = 800
+    J = crandn(g, n, n) / math.sqrt(n)
+    ref = O.reduce_c128(J, path=2)
+    blk = O.reduce_c128(J, path=1, nb=16)
+    assert _same_bits(ref.factors, blk.factors)
+    dev_order = O.reduce_c128(J, path=0)
+    assert np.array_equal(ref.ipiv, dev_order.ipiv)
+    tol = 100 * n * np.finfo(float).eps
+    for part in (lambda F: np.triu(F, -1), lambda F: np.tril(F, -2)):
+        Fr, Fd = part(ref.factors), part(dev_order.factors)
+        assert np.linalg.norm(Fd - Fr) <= tol * np.linalg.norm(Fr)
