@@ -216,6 +216,25 @@ class LHLShift:
             _lib.lhl_shift_destroy(h)
             self._h = None
 
+    def _resize(self, n: int) -> "LHLShift":
+        """``_lhl_resize!(sh, n)`` (F:277-292): the same slots and shift type at order n; the
+        slots' factorisations are dropped.  The device object is replaced."""
+        n = int(n)
+        if n == self.n:
+            return self
+        h = C.c_void_p()
+        create = _lib.lhl_shift_create_complex if self.is_complex else _lib.lhl_shift_create
+        _check(create(n, self.nshifts, C.byref(h)), "LHLShift")
+        old, self._h = self._h, h
+        if old is not None and old.value:
+            _lib.lhl_shift_destroy(old)
+        v = _ShView()
+        _check(_lib.lhl_shift_get_view(self._h, C.byref(v)))
+        self._v = v
+        self.n = n
+        self.po = int(v.po)
+        return self
+
     @property
     def ldg(self):
         return int(self._v.ldg)
@@ -308,6 +327,30 @@ class LHLWorkspace:
         if h is not None and h.value and _lib is not None:
             _lib.lhl_ws_destroy(h)
             self._h = None
+
+    def _resize(self, n: int) -> "LHLWorkspace":
+        """``_lhl_resize!(ws, n)`` (F:256-275): a workspace of order n in place of this one, with
+        the same form, element type and shift type; the reduction is dropped and ``ws.shift``
+        takes the new order.  The device workspace is replaced; probe and wait-limit settings
+        carry over."""
+        n = int(n)
+        if n == self.n:
+            return self
+        new = LHLWorkspace(n, self.precision, self.shift_complex, dtype=self.dtype)
+        old, self._h = self._h, new._h
+        new._h = None  # the handle now belongs to self
+        if old is not None and old.value:
+            _lib.lhl_ws_destroy(old)
+        self._v = new._v
+        self.n = n
+        self.shift = new.shift
+        self.reduced = False
+        self.__dict__.pop("_J_keepalive", None)
+        if self.__dict__.get("_probes"):
+            _check(_lib.lhl_ws_set_probes(self._h, 1), "set_probes")
+        if self.__dict__.get("_limit_ns") is not None:
+            _check(_lib.lhl_ws_set_barrier_limit_ns(self._h, int(self._limit_ns)))
+        return self
 
     def __getattr__(self, name):
         if name in LHLWorkspace._SHIFT_FIELDS:
@@ -426,15 +469,17 @@ class LHLWorkspace:
     def set_probes(self, on: bool = True):
         """Record the reduction's device timers (phase_ns, probe_ns); off by default."""
         _check(_lib.lhl_ws_set_probes(self._h, int(bool(on))), "set_probes")
+        self._probes = bool(on)
 
     def set_barrier_limit_ns(self, ns: int):
         _check(_lib.lhl_ws_set_barrier_limit_ns(self._h, int(ns)))
+        self._limit_ns = int(ns)
 
 
 # ---------------------------------------------------------------------------------------
 def lhl_reduce_(ws: LHLWorkspace, J: torch.Tensor, balance: bool, thread=True, stream=None) -> LHLWorkspace:
-    """``lhl_reduce!(ws, J, balance)`` (F:355).  J is not modified.  The workspace must have
-    been built for J's order (the device workspace does not resize in place)."""
+    """``lhl_reduce!(ws, J, balance)`` (F:355).  J is not modified.  A workspace of another
+    order is resized to J's first, as the reference does (F:357)."""
     if ws.dtype == torch.complex128:
         _require_cuda_f64(J, "J", True)
     elif isinstance(J, torch.Tensor) and J.dtype == torch.float32:
@@ -443,8 +488,7 @@ def lhl_reduce_(ws: LHLWorkspace, J: torch.Tensor, balance: bool, thread=True, s
         _require_cuda_f64(J, "J")
     if J.dim() != 2 or J.shape[0] != J.shape[1]:
         raise DimensionMismatch(f"matrix is not square: dimensions are {tuple(J.shape)}")
-    if J.shape[0] != ws.n:
-        raise DimensionMismatch(f"J is {J.shape[0]}x{J.shape[0]}, the workspace is {ws.n}x{ws.n}")
+    ws._resize(J.shape[0])
     Jc = _colmajor(J)
     ld = max(Jc.stride(1), 1)
     fn = _lib.lhl_reduce_f32 if Jc.dtype == torch.float32 else _lib.lhl_reduce
@@ -472,11 +516,7 @@ def lhl(J: torch.Tensor, balance: bool = True, thread=True, precision: int = LHL
 
 
 def lhl_(ws: LHLWorkspace, J: torch.Tensor, balance: bool = True, thread=True, stream=None) -> LHLWorkspace:
-    """``lhl!(ws, J; balance)`` (F:3192).  A workspace of another order is rebuilt in place."""
-    if J.shape[0] != ws.n:
-        new = LHLWorkspace(J.shape[0], ws.precision, ws.shift_complex, dtype=ws.dtype)
-        ws.__dict__.update({k: v for k, v in new.__dict__.items()})
-        new._h = None
+    """``lhl!(ws, J; balance)`` (F:3192).  A workspace of another order is resized in place."""
     return lhl_reduce_(ws, J, balance, thread, stream)
 
 
@@ -493,16 +533,18 @@ def _shift_args(a):
 def lhl_shift_(*args, slot: int = 0, stream=None):
     """``lhl_shift!(ws, sigma, tau)`` / ``lhl_shift!(sh, ws, sigma, tau)`` (F:2456-2489)."""
     sh, ws, sigma, tau, ret = _shift_args(args)
-    if sh.n != ws.n:
-        raise DimensionMismatch(f"the LHLShift is {sh.n}x{sh.n}, the workspace {ws.n}x{ws.n}")
+    if ws.dtype == torch.complex128 and not sh.is_complex:
+        raise ArgumentError("an LHLShift{Float64} cannot serve a workspace of element type ComplexF64")
+    if not sh.is_complex:
+        for v in (sigma, tau):
+            if isinstance(v, complex) and v.imag != 0:
+                raise ArgumentError(f"complex shift ({sigma}, {tau}) on a real LHLShift")
+    sh._resize(ws.n)  # _lhl_resize!(sh, n), F:2476
     if sh.is_complex:
         sigma, tau = complex(sigma), complex(tau)
         _check(_lib.lhl_shift_complex(sh._h, ws._h, int(slot), sigma.real, sigma.imag, tau.real, tau.imag,
                                       _stream(stream)), "lhl_shift")
         return ret
-    for v in (sigma, tau):
-        if isinstance(v, complex) and v.imag != 0:
-            raise ArgumentError(f"complex shift ({sigma}, {tau}) on a real LHLShift")
     sigma = float(sigma.real if isinstance(sigma, complex) else sigma)
     tau = float(tau.real if isinstance(tau, complex) else tau)
     _check(_lib.lhl_shift(sh._h, ws._h, int(slot), sigma, tau, _stream(stream)), "lhl_shift")

@@ -230,6 +230,29 @@ def test_errors_mirror_the_reference():
     assert G.lhl_ldiv_(x, ws) is x
 
 
+def test_workspace_and_shift_resize_like_the_reference():
+    """test/core_tests.jl:107-112: lhl! onto a workspace of another order resizes it; :306-310:
+    lhl_shift! resizes a shift object to the workspace.  Both then solve like fresh objects."""
+    torch, G = _mods()
+    n = 40
+    ws = G.lhl(dev(rng(4).standard_normal((n, n))))
+    J3 = rng(6).standard_normal((2 * n, 2 * n))
+    assert G.lhl_(ws, dev(J3)) is ws and ws.n == 2 * n and ws.shift.n == 2 * n
+    R = O.reduce(J3)
+    assert np.array_equal(host(ws.ipiv), R.ipiv) and bits_equal(host(ws.factors), R.factors)
+    b3 = rng(7).standard_normal(2 * n)
+    G.lhl_shift_(ws, 1.0, -0.3)
+    x = host(G.lhl_ldiv_(dev(b3), ws))
+    xr = np.linalg.solve(np.eye(2 * n) - 0.3 * J3, b3)
+    assert np.linalg.norm(x - xr) <= 1e-9 * np.linalg.norm(xr)  # isapprox, rtol = 1e-9
+    sh = G.LHLShift(n, 1, complex=True)
+    assert G.lhl_shift_(sh, ws, 1.0, -0.3j) is sh and sh.n == 2 * n
+    b2 = rng(8).standard_normal(2 * n) + 1j * rng(9).standard_normal(2 * n)
+    xc = host(G.lhl_ldiv_(dev(b2), sh, ws))
+    xr = np.linalg.solve(np.eye(2 * n) - 0.3j * J3, b2)
+    assert np.linalg.norm(xc - xr) <= 1e-9 * np.linalg.norm(xr)
+
+
 def test_barrier_timeout_reports_and_recovers():
     """A grid-barrier wait limit of 1 ns expires: the reduction returns LHL_ERR_TIMEOUT
     instead of hanging, and the same workspace then reduces correctly."""
