@@ -253,6 +253,58 @@ def test_workspace_and_shift_resize_like_the_reference():
     assert np.linalg.norm(xc - xr) <= 1e-9 * np.linalg.norm(xr)
 
 
+def _wilkinson(n):
+    J = -np.tril(np.ones((n, n)), -1) + np.eye(n)
+    J[:, n - 1] = 1.0
+    return J
+
+
+@pytest.mark.parametrize("family", ["randn", "wilkinson", "graded"])
+def test_pivoting_is_what_makes_it_work(family):
+    """test/core_tests.jl:337-363 on the device: |l| <= 1 + eps on the families that break an
+    unpivoted reduction, and one refinement step with the caller's W takes the reference's
+    backward error below 1e-13 (the oracle reaches about 1e-16 on these)."""
+    torch, G = _mods()
+    n = 100
+    if family == "randn":
+        J = rng(1).standard_normal((n, n))
+    elif family == "wilkinson":
+        J = _wilkinson(n)
+    else:
+        J = np.diag(10.0 ** np.linspace(-8, 8, n)) @ rng(3).standard_normal((n, n)) @ \
+            np.diag(10.0 ** np.linspace(8, -8, n))
+    b = rng(42).standard_normal(n)
+    ws = G.lhl(dev(J))
+    assert np.abs(np.tril(host(ws.factors), -2)).max() <= 1 + np.finfo(float).eps
+    for g in (1e-3, 1.0, 1e3):
+        G.lhl_shift_(ws, 1.0, -g)
+        if ws.info != 0:
+            continue
+        W = np.eye(n) - g * J
+        x = G.lhl_ldiv_(dev(b), ws)
+        G.lhl_refine_system_(x, dev(W), dev(b), ws, 1)
+        assert O.bwd(W, host(x), b) < 1e-13, (family, g)
+
+
+def test_refinement_recovers_backward_error_where_kappa_Z_is_enormous():
+    """test/core_tests.jl:365-380 on the device: strictly upper triangular J with a 1e-8 corner,
+    every pivot near zero; one refinement step does not lose and ends below 1e-13 (the oracle:
+    6.5e-12 raw, 2.8e-17 refined)."""
+    torch, G = _mods()
+    n = 60
+    J = np.triu(rng(17).standard_normal((n, n)), 1)
+    J[n - 1, 0] = 1e-8
+    b = rng(18).standard_normal(n)
+    W = np.eye(n) - 0.5 * J
+    ws = G.lhl(dev(J))
+    G.lhl_shift_(ws, 1.0, -0.5)
+    raw = G.lhl_ldiv_(dev(b), ws)
+    refined = raw.clone()
+    G.lhl_refine_system_(refined, dev(W), dev(b), ws, 1)
+    assert O.bwd(W, host(refined), b) <= O.bwd(W, host(raw), b)
+    assert O.bwd(W, host(refined), b) < 1e-13
+
+
 def test_barrier_timeout_reports_and_recovers():
     """A grid-barrier wait limit of 1 ns expires: the reduction returns LHL_ERR_TIMEOUT
     instead of hanging, and the same workspace then reduces correctly."""
