@@ -151,20 +151,22 @@ def _bcast_worker(rank, world, port, q, case):
         dist.destroy_process_group()
 
 
+@pytest.mark.parametrize("world", [2, 3])
 @pytest.mark.parametrize("case", ["real", "complex", "order", "unreduced"])
-def test_two_ranks_broadcast_reduction(case):
+def test_ranks_broadcast_reduction(case, world):
+    """Rank 1 holds the reduction; with three ranks a receiver sits on each side of it."""
     ctx = mp.get_context("spawn")
     q = ctx.Queue()
     port = _free_port()
-    procs = [ctx.Process(target=_bcast_worker, args=(r, 2, port, q, case)) for r in range(2)]
+    procs = [ctx.Process(target=_bcast_worker, args=(r, world, port, q, case)) for r in range(world)]
     for p in procs:
         p.start()
     out = dict((r, (s, v)) for r, s, v in (q.get(timeout=120) for _ in procs))
     for p in procs:
         p.join(timeout=60)
         assert p.exitcode == 0
-    if case in ("order", "unreduced"):  # both ranks raise, neither waits in the data broadcast
-        assert out[0][0] == "raised" and out[1][0] == "raised", out
+    if case in ("order", "unreduced"):  # every rank raises, none waits in the data broadcast
+        assert all(out[r][0] == "raised" for r in range(world)), out
         return
-    assert out[0][0] == "ok" and out[1][0] == "ok"
-    assert out[0][1] == out[1][1]
+    assert all(out[r][0] == "ok" for r in range(world))
+    assert all(out[r][1] == out[1][1] for r in range(world))
