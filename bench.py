@@ -142,6 +142,37 @@ def time_events(stream, fn, reps, flush):
     return float(np.mean(out))
 
 
+def cpu_config_sample(name, shifts_sample):
+    """The oracle on a bounded sample of configuration c1, c3 or c5: the full reduction once,
+    then `shifts_sample` of its shifts (c1: all three), each with its right-hand sides solved and
+    refined by one step.  Returns (seconds for the whole step, scaled from the sample by the
+    shift count; solves per step; a description of the sample)."""
+    from oracle import oracle as O
+    from lhl_gpu import configs
+    c = {"c1": configs.config1, "c3": configs.config3, "c5": configs.config5}[name]()
+    J, sig, tau = c["J"], np.asarray(c["sigma"]), np.asarray(c["tau"])
+    n, S, R = J.shape[0], len(sig), int(c.get("nrhs", 1))
+    k = S if name == "c1" else max(1, min(shifts_sample, S))
+    t0 = time.perf_counter()
+    Rd = O.reduce(J)
+    t_red = time.perf_counter() - t0
+    t0 = time.perf_counter()
+    if np.iscomplexobj(sig) or np.iscomplexobj(tau):
+        g = np.random.default_rng(12)
+        for s in range(k):
+            Sh = O.shift_complex(Rd, sig[s], tau[s])
+            for _ in range(R):
+                b = g.standard_normal(n) + 1j * g.standard_normal(n)
+                x = O.ldiv_complex(Rd, Sh, b)
+                x = x + O.ldiv_complex(Rd, Sh, b - (sig[s] * x + tau[s] * (J @ x)))
+    else:
+        O.shift_solve_batch(Rd, J, sig[:k], tau[:k], np.asfortranarray(c["B"][:, :k]), steps=1)
+    t_sh = time.perf_counter() - t0
+    desc = (f"{name}: FP64 reduction of n = {n} once ({t_red:.2f} s), then {k} of {S} shifts with {R} right-hand "
+            f"side(s) each, shift LU + solve + 1 refinement step ({t_sh:.2f} s), scaled to {S} shifts")
+    return t_red + t_sh * S / k, S * R, desc
+
+
 class Form:
     """One form of the path on the device: the workspace, the shift batch and one step.
     refine = ("fixed", max_steps): lhl_refine_tol; ("gmres", max_cycles, restart): lhl_refine_gmres
@@ -210,6 +241,10 @@ def main():
     ap.add_argument("--no-c4", action="store_true", help="skip the batched config-4 measurement")
     ap.add_argument("--no-launch-count", action="store_true",
                     help="skip the profiler-based kernel count (for runs under ncu)")
+    ap.add_argument("--cpu-config", choices=["c1", "c3", "c5"],
+                    help="with --impl reference: time the oracle on a bounded sample of this configuration "
+                         "instead (thread count from OMP_NUM_THREADS; set OPENBLAS_NUM_THREADS alike)")
+    ap.add_argument("--cpu-shifts", type=int, default=4, help="--cpu-config: shifts in the sample")
     args = ap.parse_args()
     world, rank, local = dist_setup(args.gpus)
 
@@ -223,6 +258,18 @@ def main():
               "form": "mixed: FP32 reduction (FP64-accumulated column updates), FP64 balancing, shift LU, solves, "
                       "residuals and refinement",
               "l2": "flushed between timed steps (256 MiB write)", "replicas": world}
+
+    if args.impl == "reference" and args.cpu_config:
+        if rank != 0:
+            return
+        from oracle import oracle as O
+        sec, units, desc = cpu_config_sample(args.cpu_config, args.cpu_shifts)
+        val = units / sec
+        print(json.dumps({"impl": "reference", "metric": METRIC, "value": val, "unit": UNIT, "ms_per_step": sec * 1e3,
+                          "higher_is_better": True, "dtype": "f64", "config": {"workload": args.cpu_config},
+                          "cpu_baseline": {"value": val, "unit": UNIT, "cores": O.num_threads(), "kind": "port",
+                                           "sample": desc + "; oracle C restatement, OpenMP"}}), flush=True)
+        return
 
     if args.impl == "reference":
         if rank != 0:
