@@ -164,7 +164,8 @@ def cpu_config_sample(name, shifts_sample):
             for _ in range(R):
                 b = g.standard_normal(n) + 1j * g.standard_normal(n)
                 x = O.ldiv_complex(Rd, Sh, b)
-                x = x + O.ldiv_complex(Rd, Sh, b - (sig[s] * x + tau[s] * (J @ x)))
+                Jx = J @ x.real + 1j * (J @ x.imag)  # a real J: no complex copy of it
+                x = x + O.ldiv_complex(Rd, Sh, b - (sig[s] * x + tau[s] * Jx))
     else:
         O.shift_solve_batch(Rd, J, sig[:k], tau[:k], np.asfortranarray(c["B"][:, :k]), steps=1)
     t_sh = time.perf_counter() - t0
