@@ -295,11 +295,21 @@ int lhl_solve_batched(lhl_batch_t batch, const double* dJ, const double* dB, dou
  * array of the library (about 2.5 MB, present on every GPU that loads it until exit).
  * n <= LHL_NOALLOC_NMAX, else LHL_ERR_DIM.  The first call on a device resolves the array's
  * device address (make it before any stream capture).  All calls share the array: calls
- * whose work overlaps on the GPU race.  Allocates nothing. */
+ * whose work overlaps on the GPU race.  dJ must not overlap dfactors or dHt (LHL_ERR_ARG).
+ * Allocates nothing. */
 #define LHL_NOALLOC_NMAX 1024
 int lhl_reduce_noalloc(int64_t n, const double* dJ, int64_t ldj, int balance, double* dfactors, double* dHt,
                        int64_t* dipiv, int64_t* dperm, int64_t* diperm, double* dscale, double* discale,
                        void* stream);
+/* Waits for the stream, then reports a device-side error that the last lhl_reduce_noalloc on
+ * the current device recorded in the static array (LHL_ERR_TIMEOUT from a bounded wait) and
+ * clears it; LHL_OK otherwise.  The counterpart of lhl_ws_check for the allocation-free call:
+ * without it a reduction cut short by a wait limit would look successful.  The next
+ * lhl_reduce_noalloc clears the word, so check before it.  Allocates nothing. */
+int lhl_reduce_noalloc_check(void* stream);
+/* Test hook: the wall-time limit of every bounded wait of later lhl_reduce_noalloc calls in
+ * this process (0 restores the default of 2 s). */
+int lhl_reduce_noalloc_set_barrier_limit_ns(uint64_t limit_ns);
 
 /* Library build identification (for loaders that check they bound the right .so). */
 const char* lhl_version(void);

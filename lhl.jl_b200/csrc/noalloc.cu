@@ -20,6 +20,12 @@
 //  - The array keeps the last call's contents; each call clears what must start at zero
 //    (the grid-barrier counter, the error flag) with cudaMemsetAsync, which allocates
 //    nothing.
+//  - A bounded wait that expires inside the reduction leaves LHL_ERR_TIMEOUT in the array's
+//    error word; lhl_reduce_noalloc_check reads it back (and clears it) once the stream is
+//    done, as lhl_ws_check does for a workspace.  Read it before the next call, which
+//    clears it.
+//  - dJ must not overlap the outputs: the first thing a call queues is the copy of J into
+//    dfactors.
 // No cudaMalloc, cudaFree or allocating library routine is called on this path.
 #include <string.h>
 
@@ -46,6 +52,36 @@ static __device__ __align__(256) double g_noalloc_scratch[NDOUBLE];
 
 constexpr int MAXDEV = 64;
 static double* g_scratch_ptr[MAXDEV];  // device address of g_noalloc_scratch, per device
+constexpr size_t ERR_OFFSET_BYTES = OFF_INTS * sizeof(double) + (NCAND + 4) * sizeof(int);
+constexpr unsigned long long DEFAULT_LIMIT_NS = 2000000000ull;
+static unsigned long long g_limit_ns = DEFAULT_LIMIT_NS;  // every bounded wait of these calls
+
+// The device address of the scratch array on the current device, looked up once per device.
+static double* scratch_base(int* status)
+{
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= MAXDEV) {
+        *status = LHL_ERR_CUDA;
+        return nullptr;
+    }
+    if (!g_scratch_ptr[dev]) {
+        void* p = nullptr;
+        if (cudaGetSymbolAddress(&p, g_noalloc_scratch) != cudaSuccess || !p) {
+            *status = LHL_ERR_CUDA;
+            return nullptr;
+        }
+        g_scratch_ptr[dev] = (double*)p;
+    }
+    *status = LHL_OK;
+    return g_scratch_ptr[dev];
+}
+
+static bool overlaps(const void* a, size_t abytes, const void* b, size_t bbytes)
+{
+    const char* x = (const char*)a;
+    const char* y = (const char*)b;
+    return x < y + bbytes && y < x + abytes;
+}
 
 }  // namespace
 
@@ -58,14 +94,17 @@ extern "C" int lhl_reduce_noalloc(int64_t n, const double* dJ, int64_t ldj, int 
     if (n == 0) return LHL_OK;
     if (!dJ || !dfactors || !dHt || !dperm || !diperm || !dscale || !discale || (n > 2 && !dipiv)) return LHL_ERR_ARG;
     if (ldj < n) return LHL_ERR_DIM;
-    int dev = 0;
-    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= MAXDEV) return LHL_ERR_CUDA;
-    if (!g_scratch_ptr[dev]) {
-        void* p = nullptr;
-        if (cudaGetSymbolAddress(&p, g_noalloc_scratch) != cudaSuccess || !p) return LHL_ERR_CUDA;
-        g_scratch_ptr[dev] = (double*)p;
-    }
-    double* base = g_scratch_ptr[dev];
+    // J is read while dfactors is written: the caller's J may share no byte with an output
+    const size_t jbytes = ((size_t)(ldj) * (size_t)(n - 1) + (size_t)n) * sizeof(double);
+    const size_t nnbytes = (size_t)n * (size_t)n * sizeof(double);
+    if (overlaps(dJ, jbytes, dfactors, nnbytes) || overlaps(dJ, jbytes, dHt, nnbytes) ||
+        overlaps(dfactors, nnbytes, dHt, nnbytes))
+        return LHL_ERR_ARG;
+    // the fixed scratch must hold this build's grid and step table; checked before any work is queued
+    if (lhl::reduce_grid_size() > NCAND || lhl::stepTabBytes() > 512 * sizeof(double)) return LHL_ERR_CUDA;
+    int status = LHL_OK;
+    double* base = scratch_base(&status);
+    if (!base) return status;
     int* ints = (int*)(base + OFF_INTS);
     cudaStream_t st = (cudaStream_t)stream;
 
@@ -96,9 +135,8 @@ extern "C" int lhl_reduce_noalloc(int64_t n, const double* dJ, int64_t ldj, int 
     a.bar = (unsigned int*)(ints + NCAND + 8);
     a.scale = dscale;
     a.iscale = discale;
-    a.limit_ns = 2000000000ull;
+    a.limit_ns = g_limit_ns;
     a.ptimes = nullptr;
-    if (lhl::reduce_grid_size() > NCAND || lhl::stepTabBytes() > 512 * sizeof(double)) return LHL_ERR_CUDA;
     a.use_tma = (n % 2 == 0) ? 1 : 0;
     const int mode = n <= 2 ? 0 : (n < 500 ? 1 : 2);
     if (!balance) {
@@ -113,4 +151,31 @@ extern "C" int lhl_reduce_noalloc(int64_t n, const double* dJ, int64_t ldj, int 
     }
     e = lhl::launch_ht_perm((int)n, dfactors, dHt, dipiv, dperm, diperm, st);
     return e == cudaSuccess ? LHL_OK : LHL_ERR_CUDA;
+}
+
+extern "C" int lhl_reduce_noalloc_check(void* stream)
+{
+    int status = LHL_OK;
+    double* base = scratch_base(&status);
+    if (!base) return status;
+    cudaStream_t st = (cudaStream_t)stream;
+    if (cudaStreamSynchronize(st) != cudaSuccess) return LHL_ERR_CUDA;
+    int err = 0;
+    // a copy out of the static array into the caller's stack: no allocation
+    if (cudaMemcpyFromSymbol(&err, g_noalloc_scratch, sizeof(int), ERR_OFFSET_BYTES, cudaMemcpyDeviceToHost) !=
+        cudaSuccess)
+        return LHL_ERR_CUDA;
+    if (err) {
+        const int zero = 0;
+        if (cudaMemcpyToSymbol(g_noalloc_scratch, &zero, sizeof(int), ERR_OFFSET_BYTES, cudaMemcpyHostToDevice) !=
+            cudaSuccess)
+            return LHL_ERR_CUDA;
+    }
+    return err ? err : LHL_OK;
+}
+
+extern "C" int lhl_reduce_noalloc_set_barrier_limit_ns(uint64_t limit_ns)
+{
+    g_limit_ns = limit_ns ? (unsigned long long)limit_ns : DEFAULT_LIMIT_NS;
+    return LHL_OK;
 }

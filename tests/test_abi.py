@@ -138,6 +138,9 @@ def test_creators_check_sizes_and_pointers_on_host():
     assert L.lhl_reduce_noalloc(8, None, 8, 1, *([None] * 8)) == 1
     assert L.lhl_reduce_noalloc(8, 1, 4, 1, *([1] * 7), None) == 2      # ldj < n
     assert L.lhl_reduce_noalloc(2000, 1, 2000, 1, *([1] * 7), None) == 2  # above its order limit
+    # J sharing bytes with factors (or factors with Ht) is refused before anything is queued
+    assert L.lhl_reduce_noalloc(8, 4096, 8, 1, 4096 + 8, 1 << 20, 1, 1, 1, 1, 1, None) == 1
+    assert L.lhl_reduce_noalloc(8, 4096, 8, 1, 1 << 20, (1 << 20) + 64, 1, 1, 1, 1, 1, None) == 1
 
 
 def test_configs_are_seeded_and_shaped():
