@@ -1,22 +1,29 @@
 """Benchmark: shifted solves per second on one B200 (LHLFactorization.jl's hot path).
 
-Workload (config 2): J 2048x2048 FP64 N(0,1); 64 shifts (1, -g), g log-uniform in
-[1e-4, 1e-1]; one N(0,1) right-hand side per shift.  One step = the whole path on one
-batch: reduction J = Z H Z^-1, 64 shift LUs, 64 solves, then FP64 refinement until every
-solve is at <= 1e-10 relative residual (lhl_refine_tol; the final residuals are checked
-after the timed region).  value = 64 solves / step time of the mixed form (FP32 reduction);
-the plain FP64 form (bit-identical to the reference's operation order) is timed the same
-way and reported beside it, with the ratio.
+Headline workload, config 5 (the largest configuration; the one whose stated form is the mixed
+one): a real J 8192 x 8192 FP64 with iid N(0,1)/sqrt(n) entries; 128 complex shifts
+s = a + ib, a ~ U[-2, 0], b ~ U[0, 10], (sigma, tau) = (s, -1); 32 complex N(0,1) right-hand
+sides per shift.  One step = the whole path on one batch: the reduction J = Z H Z^-1, the 128
+complex shift LUs, the 4096 complex solves, then FP64 refinement until every solve is at
+<= 1e-10 relative residual (lhl_refine_tol; the final residuals are checked after the timed
+region).  value = 4096 solves / step time of the mixed form (FP32 reduction); the plain FP64
+form (bit-identical to the reference's operation order) is timed the same way and reported
+beside it, with the ratio.  Configurations 1, 2 and 3 (both forms) and the batched config 4
+are reported as extra fields of the same line.
 
-    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--config c5|c2|c3|c1]
 
-N > 1 runs independent replicas, one per GPU (the reduction of one J does not shard);
-value is the aggregate.  --impl reference times the CPU restatement of the reference
-algorithm (the oracle, all host threads) on the same workload.
+N > 1 runs independent replicas, one per GPU (one reduction does not shard); value is the
+aggregate.  --impl reference times the oracle (the CPU restatement of the reference's
+algorithm, all host threads) on a bounded sample of the same workload; it never loads the
+CUDA library.  --case runs one phase of one configuration alone (the small cases that the ncu
+summaries under profiles/ were captured on).
 """
 from __future__ import annotations
 
 import argparse
+import concurrent.futures as cf
+import importlib.util
 import json
 import os
 import subprocess
@@ -35,6 +42,8 @@ import numpy as np  # noqa: E402
 METRIC = "shifted solves/sec at 1e-10 rel. residual: mixed/batched vs plain FP64, 1 B200"
 UNIT = "solves/s"
 L2_FLUSH_BYTES = 256 << 20
+TOL = 1e-10
+EPS = float(np.finfo(float).eps)
 
 
 def peaks():
@@ -45,6 +54,15 @@ def peaks():
         return float(d["hbm_gbs"]), "measured"
     except Exception:
         return 6650.0, "fallback"
+
+
+def load_configs():
+    """lhl_gpu/configs.py by its path: the seeded input generator, without importing the
+    package (whose import loads the CUDA library; the reference arm must not)."""
+    spec = importlib.util.spec_from_file_location("lhl_configs", os.path.join(PKG, "lhl_gpu", "configs.py"))
+    m = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(m)
+    return m
 
 
 class ClockSampler:
@@ -113,26 +131,119 @@ def whole_job_rate(world, units_per_rank, ms_per_step):
     return world * units_per_rank / (ms_per_step * 1e-3)
 
 
-def cpu_reference_run(cfg, steps, warmup, threads_note):
-    """The oracle (CPU restatement) on one full step of the workload; returns seconds per step."""
-    from oracle import oracle as O
-    times = []
-    X = None
-    for it in range(warmup + steps):
-        t0 = time.perf_counter()
-        R = O.reduce(cfg["J"])
-        X, info = O.shift_solve_batch(R, cfg["J"], cfg["sigma"], cfg["tau"], cfg["B"], steps=cfg["steps"])
-        t1 = time.perf_counter()
-        if it >= warmup:
-            times.append(t1 - t0)
-    return times, X
+# ---------------------------------------------------------------------------------------
+# Workloads: the seeded configurations and how each form refines them
+
+DESCR = {
+    "c1": "c1: J 400x400 FP64 N(0,1), 3 shifts (1,-g) g in {0.01,0.013,0.021}, 1 RHS/shift",
+    "c2": "c2: J 2048x2048 FP64 N(0,1), 64 shifts (1,-g) g log-uniform [1e-4,1e-1], 1 RHS/shift",
+    "c3": "c3: stiff J 4096x4096 = Q diag(-lam) Q^-1 + 0.01 N(0,1), lam log-uniform [1,1e4]; 256 shifts "
+          "(-1/(dt g), 1), dt g log-uniform [1e-5,1e-2]; 1 RHS/shift",
+    "c5": "c5: real J 8192x8192 FP64 N(0,1)/sqrt(n); 128 complex shifts (s,-1), s = a+ib, a~U[-2,0], b~U[0,10]; "
+          "32 complex RHS/shift (4096 complex solves)",
+}
+# refinement per (configuration, form): ("fixed", max steps) = lhl_refine_tol;
+# ("gmres", max cycles, restart) = lhl_refine_gmres with a host check per cycle
+REFINE = {
+    ("c1", "mixed"): ("gmres", 4, 3), ("c1", "plain"): ("fixed", 2),
+    ("c2", "mixed"): ("gmres", 4, 3), ("c2", "plain"): ("fixed", 2),
+    ("c3", "mixed"): ("gmres", 12, 8), ("c3", "plain"): ("fixed", 4),
+    ("c5", "mixed"): ("fixed", 16), ("c5", "plain"): ("fixed", 4),
+}
 
 
-def time_events(stream, fn, reps, flush):
+def workload(name, cfgs):
+    c = {"c1": cfgs.config1, "c2": cfgs.config2, "c3": cfgs.config3, "c5": cfgs.config5}[name]()
+    w = {"name": name, "n": int(c["J"].shape[0]), "J": c["J"], "sigma": np.asarray(c["sigma"]),
+         "tau": np.asarray(c["tau"])}
+    w["S"] = len(w["sigma"])
+    w["cplx"] = bool(np.iscomplexobj(w["sigma"]))
+    if name == "c5":
+        g = c["rng"]
+        n, S, R = c["n"], len(c["sigma"]), c["nrhs"]
+        re = g.standard_normal((n, S * R))
+        im = g.standard_normal((n, S * R))
+        B = np.empty((n, S * R), dtype=np.complex128, order="F")
+        B.real = re
+        B.imag = im
+        w["B"], w["R"] = B, R
+        w["tau"] = w["tau"].astype(np.complex128)
+    else:
+        w["B"], w["R"] = np.asfortranarray(c["B"]), 1
+    fx = os.path.join(REPO, "tests", "golden", f"config_{name}.npz")
+    w["fixture"] = dict(np.load(fx)) if os.path.exists(fx) else None
+    return w
+
+
+def forward_errors(w, X):
+    """Forward error of the sampled columns against the oracle's refined FP64 solutions
+    (tests/golden/config_<c>.npz); None where no fixture exists."""
+    fx = w["fixture"]
+    if fx is None:
+        return None
+    out = []
+    for i, col in enumerate(fx["rhs_columns"]):
+        x = X[:, int(col)].cpu().numpy()
+        xr = fx["x_ref"][:, i]
+        out.append(float(np.linalg.norm(x - xr) / np.linalg.norm(xr)))
+    return {"max": max(out), "columns": [int(v) for v in fx["rhs_columns"]], "values": out,
+            "against": "the oracle's FP64 solution refined by two steps (tests/golden)"}
+
+
+class Form:
+    """One form of the path on the device for workload w: workspace, the shift object (shared
+    between forms when given), solution and residual scratch, and one step."""
+
+    def __init__(self, G, torch, w, form, dev, sh=None):
+        self.G, self.torch, self.w, self.form = G, torch, w, form
+        n, S, R = w["n"], w["S"], w["R"]
+        dt = torch.complex128 if w["cplx"] else torch.float64
+        self.ws = G.LHLWorkspace(n, G.LHL_PREC_MIXED if form == "mixed" else G.LHL_PREC_FP64,
+                                 shift_complex=w["cplx"])
+        self.sh = sh if sh is not None else G.LHLShift(n, S, complex=w["cplx"])
+        self.X = torch.empty((S * R, n), dtype=dt, device=dev).t()
+        self.Rs = torch.empty((S * R, n), dtype=dt, device=dev)
+        self.res = torch.empty(S * R, dtype=torch.float64, device=dev)
+        self.refine = REFINE[(w["name"], form)]
+
+    def reduce(self, Jd):
+        self.G.lhl_reduce_(self.ws, Jd, True)
+
+    def shift(self, sig, tau):
+        self.G.lhl_shift_batched_(self.sh, self.ws, sig, tau)
+
+    def solve(self, Bd):
+        self.X.copy_(Bd)
+        self.G.lhl_ldiv_(self.X, self.sh, self.ws, rhs_per_shift=self.w["R"])
+
+    def refine_(self, Jd, Bd):
+        G, R = self.G, self.w["R"]
+        if self.refine[0] == "gmres":
+            G.lhl_refine_gmres_(self.X, Jd, Bd, self.sh, self.ws, tol=TOL, max_cycles=self.refine[1],
+                                restart=self.refine[2], rhs_per_shift=R, host_check=True, R=self.Rs, res=self.res)
+        else:
+            G.lhl_refine_tol_(self.X, Jd, Bd, self.sh, self.ws, tol=TOL, max_steps=self.refine[1],
+                              rhs_per_shift=R, R=self.Rs, res=self.res)
+
+    def chain(self, Jd, Bd, sig, tau):
+        self.shift(sig, tau)
+        self.solve(Bd)
+        self.refine_(Jd, Bd)
+
+    def step(self, Jd, Bd, sig, tau):
+        self.reduce(Jd)
+        self.chain(Jd, Bd, sig, tau)
+
+    def describe_refine(self):
+        r = self.refine
+        return (f"GMRES-IR: GMRES({r[2]}) x {r[1]} cycles at most, host check per cycle" if r[0] == "gmres"
+                else f"fixed-point lhl_refine_tol, {r[1]} steps at most")
+
+
+def time_events(torch, stream, fn, reps, flush):
     out = []
     for k in range(reps):
         flush.fill_(float(k))
-        import torch
         a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         a.record(stream)
         fn()
@@ -142,71 +253,199 @@ def time_events(stream, fn, reps, flush):
     return float(np.mean(out))
 
 
-def cpu_config_sample(name, shifts_sample):
-    """The oracle on a bounded sample of configuration c1, c3 or c5: the full reduction once,
-    then `shifts_sample` of its shifts (c1: all three), each with its right-hand sides solved and
-    refined by one step.  Returns (seconds for the whole step, scaled from the sample by the
-    shift count; solves per step; a description of the sample)."""
-    from oracle import oracle as O
-    from lhl_gpu import configs
-    c = {"c1": configs.config1, "c3": configs.config3, "c5": configs.config5}[name]()
-    J, sig, tau = c["J"], np.asarray(c["sigma"]), np.asarray(c["tau"])
-    n, S, R = J.shape[0], len(sig), int(c.get("nrhs", 1))
-    k = S if name == "c1" else max(1, min(shifts_sample, S))
-    t0 = time.perf_counter()
-    Rd = O.reduce(J)
-    t_red = time.perf_counter() - t0
-    t0 = time.perf_counter()
-    if np.iscomplexobj(sig) or np.iscomplexobj(tau):
-        g = np.random.default_rng(12)
-        for s in range(k):
-            Sh = O.shift_complex(Rd, sig[s], tau[s])
-            for _ in range(R):
-                b = g.standard_normal(n) + 1j * g.standard_normal(n)
-                x = O.ldiv_complex(Rd, Sh, b)
-                Jx = J @ x.real + 1j * (J @ x.imag)  # a real J: no complex copy of it
-                x = x + O.ldiv_complex(Rd, Sh, b - (sig[s] * x + tau[s] * Jx))
-    else:
-        O.shift_solve_batch(Rd, J, sig[:k], tau[:k], np.asfortranarray(c["B"][:, :k]), steps=1)
-    t_sh = time.perf_counter() - t0
-    desc = (f"{name}: FP64 reduction of n = {n} once ({t_red:.2f} s), then {k} of {S} shifts with {R} right-hand "
-            f"side(s) each, shift LU + solve + 1 refinement step ({t_sh:.2f} s), scaled to {S} shifts")
-    return t_red + t_sh * S / k, S * R, desc
+def timed_steps(torch, form, dev_in, steps, warmup, flush, stream, pg=None, clocks=None):
+    """warmup untimed steps, then `steps` steps each bracketed by CUDA events on the launching
+    stream (L2 flushed before each); returns (mean ms, clock summary)."""
+    Jd, Bd, sig, tau = dev_in
+    for _ in range(warmup):
+        form.step(Jd, Bd, sig, tau)
+    torch.cuda.synchronize()
+    form.ws.check()
+    evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(steps)]
+    if pg:
+        pg.barrier()
+    torch.cuda.synchronize()
+    with ClockSampler(clocks if clocks is not None else 0) as clk:
+        for k in range(steps):
+            flush.fill_(float(k))
+            evs[k][0].record(stream)
+            form.step(Jd, Bd, sig, tau)
+            evs[k][1].record(stream)
+        torch.cuda.synchronize()
+    if pg:
+        pg.barrier()
+    form.ws.check()
+    return float(np.mean([a.elapsed_time(b) for a, b in evs])), clk.summary()
 
 
-class Form:
-    """One form of the path on the device: the workspace, the shift batch and one step.
-    refine = ("fixed", max_steps): lhl_refine_tol; ("gmres", max_cycles, restart): lhl_refine_gmres
-    with the host stopping once every column is at the tolerance."""
+def floor_counts(w, form):
+    """Config 3: FP64's attainable relative residual eps (|sigma| + |tau| ||J||_1) ||x|| / ||b||
+    per solve, and how many solves are at 1e-10, or else at their floor (within 10x)."""
+    J1 = float(np.abs(w["J"]).sum(axis=0).max())
+    X = form.X.cpu().numpy()
+    res = form.res.cpu().numpy()
+    B = w["B"]
+    fl = np.array([EPS * (abs(w["sigma"][c]) + abs(w["tau"][c]) * J1) * np.linalg.norm(X[:, c])
+                   / np.linalg.norm(B[:, c]) for c in range(X.shape[1])])
+    at_tol = res <= TOL
+    floor_limited = (~at_tol) & (fl > TOL / 10) & (res <= 10 * fl)
+    return {"at_1e-10": int(at_tol.sum()), "floor_limited": int(floor_limited.sum()),
+            "neither": int((~at_tol & ~floor_limited).sum()), "max_floor": float(fl.max()),
+            "max_rel_residual": float(res.max()),
+            "note": "a solve above 1e-10 whose FP64 floor eps ||W||_1 ||x|| / ||b|| exceeds 1e-11 and whose residual "
+                    "is within 10x of that floor counts as floor_limited"}
 
-    def __init__(self, G, torch, precision, n, S, dev, refine):
-        self.G, self.torch = G, torch
-        self.precision = precision
-        self.ws = G.LHLWorkspace(n, precision)
-        self.sh = G.LHLShift(n, S)
-        self.X = torch.empty((S, n), dtype=torch.float64, device=dev).t()
-        self.Rs = torch.empty((S, n), dtype=torch.float64, device=dev)
-        self.res = torch.empty(S, dtype=torch.float64, device=dev)
-        self.refine = refine
 
-    def reduce(self, Jd):
-        self.G.lhl_reduce_(self.ws, Jd, True)
-
-    def chain(self, Jd, Bd, sig, tau):
-        G = self.G
-        G.lhl_shift_batched_(self.sh, self.ws, sig, tau)
-        self.X.copy_(Bd)
-        G.lhl_ldiv_(self.X, self.sh, self.ws)
-        if self.refine[0] == "gmres":
-            G.lhl_refine_gmres_(self.X, Jd, Bd, self.sh, self.ws, tol=TOL, max_cycles=self.refine[1],
-                                restart=self.refine[2], host_check=True, R=self.Rs, res=self.res)
+def config_extra(G, torch, name, cfgs, dev, stream, flush, steps):
+    """Both forms of configuration `name` (c1, c2, c3) timed over `steps` steps after one warm-up."""
+    w = workload(name, cfgs)
+    Jd = torch.as_tensor(w["J"]).to(dev)
+    Bd = torch.as_tensor(w["B"]).to(dev)
+    sig = torch.as_tensor(w["sigma"]).to(dev)
+    tau = torch.as_tensor(w["tau"]).to(dev)
+    sh = G.LHLShift(w["n"], w["S"], complex=w["cplx"])
+    out = {"workload": DESCR[name], "steps": steps, "warmup": 1}
+    X_plain = None
+    for fm in ("mixed", "plain"):
+        f = Form(G, torch, w, fm, dev, sh)
+        ms, _ = timed_steps(torch, f, (Jd, Bd, sig, tau), steps, 1, flush, stream)
+        red = time_events(torch, stream, lambda: f.reduce(Jd), 2, flush)
+        res = f.res.cpu().numpy()
+        d = {"value": w["S"] * w["R"] / (ms * 1e-3), "unit": UNIT, "ms_per_step": ms, "reduce_ms": red,
+             "chain_ms": ms - red, "max_rel_residual": float(res.max()), "n_at_1e-10": int((res <= TOL).sum()),
+             "solves": int(res.size), "refinement": f.describe_refine()}
+        fe = forward_errors(w, f.X)
+        if fe is not None:
+            d["forward_error"] = fe
+        if name == "c3":
+            d["floor"] = floor_counts(w, f)
+        if fm == "plain":
+            X_plain = f.X.clone()
         else:
-            G.lhl_refine_tol_(self.X, Jd, Bd, self.sh, self.ws, tol=TOL, max_steps=self.refine[1], R=self.Rs,
-                              res=self.res)
+            X_mixed = f.X.clone()
+        out[fm] = d
+        del f
+    out["mixed_vs_plain"] = out["mixed"]["value"] / out["plain"]["value"]
+    if out["mixed"].get("forward_error") is None:
+        e = torch.linalg.vector_norm(X_mixed - X_plain, dim=0) / torch.linalg.vector_norm(X_plain, dim=0)
+        out["mixed"]["forward_error_vs_plain"] = {"max": float(e.max()), "median": float(e.median()),
+                                                  "against": "the plain form's refined FP64 solution"}
+    del sh
+    torch.cuda.empty_cache()
+    return out
 
-    def step(self, Jd, Bd, sig, tau):
-        self.reduce(Jd)
-        self.chain(Jd, Bd, sig, tau)
+
+# ---------------------------------------------------------------------------------------
+# CPU baseline: the oracle (C restatement of the reference's Float64 path, OpenMP reduction;
+# the per-right-hand-side solves of a shift spread over host threads), on a bounded sample
+
+def _sub_workload(w, sel):
+    """Workload w restricted to the shifts `sel` (same J, so the cached reduction serves it)."""
+    R = w["R"]
+    sub = dict(w)
+    sub["sigma"], sub["tau"], sub["S"] = w["sigma"][sel], w["tau"][sel], len(sel)
+    sub["B"] = np.asfortranarray(np.concatenate([w["B"][:, s * R:(s + 1) * R] for s in sel], axis=1))
+    return sub
+
+
+def _oracle_reduce(w):
+    """The oracle's FP64 reduction of w's J (OpenMP), kept for the chains that follow; seconds."""
+    from oracle import oracle as O
+    t0 = time.perf_counter()
+    _RED_CACHE["key"] = id(w["J"])
+    _RED_CACHE["R"] = O.reduce(w["J"])
+    return time.perf_counter() - t0
+
+
+def _chain_only(w, threads):
+    """The oracle's per-shift chain for every shift of w, on the reduction _oracle_reduce kept:
+    shift LU, every right-hand side solved (spread over host threads; ctypes releases the GIL),
+    one lhl_refine! step with the residual J X as one BLAS product over the shift's vectors."""
+    from oracle import oracle as O
+    assert _RED_CACHE.get("key") == id(w["J"]), "reduce first"
+    Rd = _RED_CACHE["R"]
+    pool = _POOL.setdefault(threads, cf.ThreadPoolExecutor(max_workers=threads))
+    J, R = w["J"], w["R"]
+    for s in range(w["S"]):
+        cols = slice(s * R, (s + 1) * R)
+        if w["cplx"]:
+            Sh = O.shift_complex(Rd, w["sigma"][s], w["tau"][s])
+            solve = lambda b: O.ldiv_complex(Rd, Sh, b)  # noqa: E731
+        else:
+            Sh = O.shift(Rd, w["sigma"][s], w["tau"][s])
+            solve = lambda b: O.ldiv(Rd, Sh, b)  # noqa: E731
+        Bs = w["B"][:, cols]
+        X = np.stack(list(pool.map(solve, [Bs[:, i] for i in range(Bs.shape[1])])), axis=1)
+        JX = (J @ X.real + 1j * (J @ X.imag)) if w["cplx"] else J @ X
+        Rr = Bs - (w["sigma"][s] * X + w["tau"][s] * JX)
+        X = X + np.stack(list(pool.map(solve, [Rr[:, i] for i in range(Rr.shape[1])])), axis=1)
+
+
+_RED_CACHE = {}
+_POOL = {}
+
+
+def cpu_sample(w, shifts, threads):
+    """The oracle on a bounded sample of workload w: the full FP64 reduction once, then `shifts`
+    of its shifts spread over the set, each with its whole chain (_chain_only).  Returns (seconds
+    of the whole step scaled from the sample by the shift count, reduction seconds, seconds per
+    shift, a description)."""
+    n, S, R = w["n"], w["S"], w["R"]
+    t_red = _oracle_reduce(w)
+    idx = np.linspace(0, S - 1, shifts).round().astype(int) if shifts < S else np.arange(S)
+    t0 = time.perf_counter()
+    _chain_only(_sub_workload(w, list(idx)), threads)
+    t_sh = (time.perf_counter() - t0) / len(idx)
+    desc = (f"{w['name']}: the oracle's FP64 reduction of n = {n} once ({t_red:.2f} s, OpenMP), then {len(idx)} of "
+            f"{S} shifts, each: shift LU, {R} solve(s) over {threads} host threads, one refinement step (BLAS "
+            f"residual) ({t_sh:.2f} s per shift); step time = reduction + per-shift time x {S}")
+    return t_red + t_sh * S, t_red, t_sh, desc
+
+
+def host_threads():
+    try:
+        return len(os.sched_getaffinity(0))
+    except Exception:
+        return os.cpu_count() or 1
+
+
+def reference_arm(args, cfgs, rank):
+    """--impl reference: the oracle on the box's host cores, bounded: the reduction once, then
+    each of warmup + steps steps one shift's whole chain (--cpu-shifts shifts per step, cycling
+    through the set); the step time reported is the reduction plus the mean per-shift time times
+    the shift count.  Never imports the CUDA library."""
+    if rank != 0:
+        return
+    from oracle import oracle as O
+    name = args.config
+    w = workload(name, cfgs)
+    threads = host_threads()
+    per_step = max(1, args.cpu_shifts)
+    S = w["S"]
+    t_red = _oracle_reduce(w)
+    shift_times = []
+    for it in range(args.warmup + args.steps):
+        s0 = (it * per_step) % S
+        sub = _sub_workload(w, [(s0 + j) % S for j in range(per_step)])
+        t1 = time.perf_counter()
+        _chain_only(sub, threads)
+        if it >= args.warmup:
+            shift_times.append((time.perf_counter() - t1) / per_step)
+    t_sh = float(np.mean(shift_times))
+    sec = t_red + t_sh * S
+    val = S * w["R"] / sec
+    sample = (f"{name}: oracle (C restatement of the reference's Float64 path; the reference is Julia, absent on "
+              f"this box): FP64 reduction of n = {w['n']} once ({t_red:.2f} s, OpenMP, {O.num_threads()} threads); "
+              f"each of the {args.steps} timed steps ({args.warmup} untimed first) = {per_step} shift(s) with shift "
+              f"LU, {w['R']} solve(s) over {threads} threads and one refinement step ({t_sh:.3f} s per shift); "
+              f"step time = reduction + mean shift time x {S} shifts")
+    line = {"impl": "reference", "metric": METRIC, "value": val, "unit": UNIT, "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": sec * 1e3, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (numpy PCG64 seeds)",
+            "config": {"workload": DESCR[name], "n": w["n"], "shifts": S, "rhs_per_shift": w["R"]},
+            "cpu_baseline": {"value": val, "unit": UNIT, "cores": threads, "kind": "port", "sample": sample},
+            "e2e": {"value": val, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
 
 
 def count_launches(torch, fn):
@@ -225,10 +464,8 @@ def count_launches(torch, fn):
         return None
 
 
-TOL = 1e-10
-MIXED_REFINE = ("gmres", 4, 3)   # GMRES(3), at most 4 cycles
-PLAIN_REFINE = ("fixed", 2)
-FIXED_POINT_REPLAY_STEPS = 16
+PLAIN_STEPS_MAX = 5
+E2E_STEPS_MAX = 10
 
 
 def main():
@@ -237,60 +474,25 @@ def main():
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--cpu-baseline-steps", type=int, default=1)
+    ap.add_argument("--config", default="c5", choices=["c5", "c2", "c3", "c1"],
+                    help="headline workload (default config 5)")
+    ap.add_argument("--cpu-shifts", type=int, default=1, help="CPU sample: shifts per sampled step")
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--no-c4", action="store_true", help="skip the batched config-4 measurement")
+    ap.add_argument("--no-extras", action="store_true", help="skip configurations 1-3 and 4 beside the headline")
     ap.add_argument("--no-launch-count", action="store_true",
                     help="skip the profiler-based kernel count (for runs under ncu)")
-    ap.add_argument("--cpu-config", choices=["c1", "c3", "c5"],
-                    help="with --impl reference: time the oracle on a bounded sample of this configuration "
-                         "instead (thread count from OMP_NUM_THREADS; set OPENBLAS_NUM_THREADS alike)")
-    ap.add_argument("--cpu-shifts", type=int, default=4, help="--cpu-config: shifts in the sample")
+    ap.add_argument("--case", choices=["reduce", "shift", "ldiv", "step"],
+                    help="run one phase of --config's --form alone, --reps times (profiling cases)")
+    ap.add_argument("--form", default="mixed", choices=["mixed", "plain"])
+    ap.add_argument("--reps", type=int, default=2)
+    ap.add_argument("--shifts", type=int, default=0, help="--case: use only the first SHIFTS shifts")
     args = ap.parse_args()
+    args.warmup = max(args.warmup, 3) if args.case is None else args.warmup
     world, rank, local = dist_setup(args.gpus)
-
-    from lhl_gpu import configs
-    cfg = configs.config2()
-    n, S = cfg["n"], len(cfg["sigma"])
-    config = {"workload": "c2: J 2048x2048 FP64 N(0,1), 64 shifts (1,-g) g log-uniform [1e-4,1e-1], 1 RHS/shift; "
-                          "one step = reduction + 64 shift LUs + 64 solves + refinement until every solve is at "
-                          "<= 1e-10 relative residual",
-              "n": n, "shifts": S, "rhs_per_shift": 1, "tolerance": TOL,
-              "form": "mixed: FP32 reduction (FP64-accumulated column updates), FP64 balancing, shift LU, solves, "
-                      "residuals and refinement",
-              "l2": "flushed between timed steps (256 MiB write)", "replicas": world}
-
-    if args.impl == "reference" and args.cpu_config:
-        if rank != 0:
-            return
-        from oracle import oracle as O
-        sec, units, desc = cpu_config_sample(args.cpu_config, args.cpu_shifts)
-        val = units / sec
-        print(json.dumps({"impl": "reference", "metric": METRIC, "value": val, "unit": UNIT, "ms_per_step": sec * 1e3,
-                          "higher_is_better": True, "dtype": "f64", "config": {"workload": args.cpu_config},
-                          "cpu_baseline": {"value": val, "unit": UNIT, "cores": O.num_threads(), "kind": "port",
-                                           "sample": desc + "; oracle C restatement, OpenMP"}}), flush=True)
-        return
+    cfgs = load_configs()
 
     if args.impl == "reference":
-        if rank != 0:
-            return
-        from oracle import oracle as O
-        threads = O.num_threads()
-        warm = max(args.warmup, 0)
-        times, _ = cpu_reference_run(cfg, max(args.steps, 1), warm, threads)
-        sec = float(np.mean(times))
-        val = S / sec
-        line = {"impl": "reference", "metric": METRIC, "value": val, "unit": UNIT, "n_gpus": args.gpus,
-                "steps": len(times), "warmup": warm, "ms_per_step": sec * 1e3, "higher_is_better": True,
-                "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (numpy PCG64 seeds 2,3,4)",
-                "config": config,
-                "cpu_baseline": {"value": val, "unit": UNIT, "cores": threads, "kind": "port",
-                                 "sample": f"{len(times)} full step(s) of the workload (FP64 reduction + 64 shift "
-                                           f"LUs + solves + 1 refinement): oracle C restatement, OpenMP"},
-                "e2e": {"value": val, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
-        print(json.dumps(line), flush=True)
-        return
+        return reference_arm(args, cfgs, rank)
 
     import torch
     import lhl_gpu as G
@@ -303,118 +505,89 @@ def main():
         pg = dist
     dev = torch.device("cuda", local)
     stream = torch.cuda.current_stream()
-
-    # ---- device-resident inputs ----
-    Jd = torch.as_tensor(cfg["J"]).to(dev)              # column-major (strides 1, n)
-    Bd = torch.as_tensor(cfg["B"]).to(dev)
-    sig = torch.as_tensor(cfg["sigma"]).to(dev)
-    tau = torch.as_tensor(cfg["tau"]).to(dev)
     flush = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.float32, device=dev)
-    mixed = Form(G, torch, G.LHL_PREC_MIXED, n, S, dev, MIXED_REFINE)
-    plain = Form(G, torch, G.LHL_PREC_FP64, n, S, dev, PLAIN_REFINE)
 
-    def timed(form):
-        for _ in range(max(args.warmup, 3)):
-            form.step(Jd, Bd, sig, tau)
-        torch.cuda.synchronize()
-        form.ws.check()
-        evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
-        if pg:
-            pg.barrier()
-        torch.cuda.synchronize()
-        with ClockSampler(local) as clk:
-            for k in range(args.steps):
-                flush.fill_(float(k))
-                evs[k][0].record(stream)
-                form.step(Jd, Bd, sig, tau)
-                evs[k][1].record(stream)
-            torch.cuda.synchronize()
-        if pg:
-            pg.barrier()
-        form.ws.check()
-        ms = float(np.mean([a.elapsed_time(b) for a, b in evs]))
-        # every solve of the timed work is at <= 1e-10 (final residuals from the refinement)
-        res = form.res.cpu().numpy()
-        assert (res <= TOL).all(), f"residual above {TOL}: {res.max()}"
-        return ms, clk.summary(), float(res.max())
+    w = workload(args.config, cfgs)
+    if args.case is not None and args.shifts:
+        k = args.shifts
+        w["S"], w["sigma"], w["tau"] = k, w["sigma"][:k], w["tau"][:k]
+        w["B"] = np.asfortranarray(w["B"][:, :k * w["R"]])
+    n, S, R = w["n"], w["S"], w["R"]
+    Jd = torch.as_tensor(w["J"]).to(dev)
+    Bd = torch.as_tensor(w["B"]).to(dev)
+    sig = torch.as_tensor(w["sigma"]).to(dev)
+    tau = torch.as_tensor(w["tau"]).to(dev)
+    dev_in = (Jd, Bd, sig, tau)
 
-    ms_mixed, clk_mixed, res_mixed = timed(mixed)
-    ms_plain, clk_plain, res_plain = timed(plain)
+    if args.case is not None:  # one phase alone (profiling)
+        f = Form(G, torch, w, args.form, dev)
+        f.step(Jd, Bd, sig, tau)
+        torch.cuda.synchronize()
+        fn = {"reduce": lambda: f.reduce(Jd), "shift": lambda: f.shift(sig, tau), "ldiv": lambda: f.solve(Bd),
+              "step": lambda: f.step(Jd, Bd, sig, tau)}[args.case]
+        ms = time_events(torch, stream, fn, max(args.reps, 1), flush)
+        f.ws.check()
+        print(json.dumps({"case": args.case, "config": args.config, "form": args.form, "n": n, "shifts": S,
+                          "rhs_per_shift": R, "ms": ms}), flush=True)
+        return
+
+    sh = G.LHLShift(n, S, complex=w["cplx"])
+    mixed = Form(G, torch, w, "mixed", dev, sh)
+    plain = Form(G, torch, w, "plain", dev, sh)
+    ms_mixed, clk_mixed = timed_steps(torch, mixed, dev_in, args.steps, args.warmup, flush, stream, pg, local)
+    res_mixed = mixed.res.cpu().numpy()
+    fe_mixed = forward_errors(w, mixed.X)
+    steps_plain = min(args.steps, PLAIN_STEPS_MAX)
+    ms_plain, clk_plain = timed_steps(torch, plain, dev_in, steps_plain, 1, flush, stream, pg, local)
+    res_plain = plain.res.cpu().numpy()
+    fe_plain = forward_errors(w, plain.X)
+    if args.config != "c3":
+        assert (res_mixed <= TOL).all(), f"mixed residual above {TOL}: {res_mixed.max()}"
+        assert (res_plain <= TOL).all(), f"plain residual above {TOL}: {res_plain.max()}"
 
     # ---- phases, each timed alone with events on the launching stream ----
-    def phases(form):
-        ph = {"reduce": time_events(stream, lambda: form.reduce(Jd), 5, flush),
-              "chain": time_events(stream, lambda: form.chain(Jd, Bd, sig, tau), 3, flush)}
-        ph["shift"] = time_events(stream, lambda: G.lhl_shift_batched_(form.sh, form.ws, sig, tau), 3, flush)
-        ph["ldiv"] = time_events(stream, lambda: G.lhl_ldiv_(form.X, form.sh, form.ws), 3, flush)
+    def phases(f):
+        reps = 2 if n >= 4096 else 3
+        ph = {"reduce": time_events(torch, stream, lambda: f.reduce(Jd), reps, flush),
+              "shift": time_events(torch, stream, lambda: f.shift(sig, tau), reps, flush),
+              "ldiv": time_events(torch, stream, lambda: f.solve(Bd), reps, flush)}
+        f.step(Jd, Bd, sig, tau)
+        ph["refine"] = time_events(torch, stream, lambda: (f.solve(Bd), f.refine_(Jd, Bd)), reps, flush) - ph["ldiv"]
         return ph
 
     ph_mixed = phases(mixed)
     ph_plain = phases(plain)
-    # what the mixed form's refinement needed: fixed-point steps per column (a replay of
-    # lhl_refine_tol with growing step counts) against GMRES-IR cycles
-    G.lhl_shift_batched_(mixed.sh, mixed.ws, sig, tau)
-    X0 = Bd.clone()
-    G.lhl_ldiv_(X0, mixed.sh, mixed.ws)
-    need = np.full(S, -1)
-    for st in range(FIXED_POINT_REPLAY_STEPS + 1):
-        Xs = X0.clone()
-        r = G.lhl_refine_tol_(Xs, Jd, Bd, mixed.sh, mixed.ws, tol=0.0, max_steps=st).cpu().numpy()
-        need[(need < 0) & (r <= TOL)] = st
-        if (need >= 0).all():
-            break
-    gm_cycles = None
-    for cyc in range(1, MIXED_REFINE[1] + 1):
-        Xs = X0.clone()
-        r = G.lhl_refine_gmres_(Xs, Jd, Bd, mixed.sh, mixed.ws, tol=TOL, max_cycles=cyc,
-                                restart=MIXED_REFINE[2]).cpu().numpy()
-        if (r <= TOL).all():
-            gm_cycles = cyc
-            break
-    fixed_chain_ms = time_events(stream, lambda: (G.lhl_shift_batched_(mixed.sh, mixed.ws, sig, tau),
-                                                  mixed.X.copy_(Bd), G.lhl_ldiv_(mixed.X, mixed.sh, mixed.ws),
-                                                  G.lhl_refine_tol_(mixed.X, Jd, Bd, mixed.sh, mixed.ws, tol=TOL,
-                                                                    max_steps=FIXED_POINT_REPLAY_STEPS, R=mixed.Rs,
-                                                                    res=mixed.res)), 3, flush)
     launches = None if args.no_launch_count else count_launches(torch, lambda: mixed.step(Jd, Bd, sig, tau))
 
-    # ---- whole-step lower bound: the compulsory HBM bytes of each phase at the measured copy
-    # bandwidth (every phase here is HBM- or latency-bound; none is tensor-core work):
-    # reduction 4n^3/3 (FP32 GEMV stream) + 16n^2; shift LUs 4n^2 (Ht, shared) + S 4n^2 (Gt);
-    # one solve pass S 4n^2 (Gt) + 8n^2 (L, shared); one residual pass 8n^2 (J, shared)
-    def step_lower_ms(peak_gbs):
-        b = (4.0 * n ** 3 / 3 + 16.0 * n * n) + (4.0 * n * n + S * 4.0 * n * n) \
-            + (S * 4.0 * n * n + 8.0 * n * n) + 8.0 * n * n
-        return b / (peak_gbs * 1e9) * 1e3
-
-    # ---- roofline of the dominant kernel: the mixed reduction ----
-    alg_bytes = 4.0 * (n ** 3) / 3.0 + 16.0 * n * n   # FP32 GEMV stream (4 n^3/3) + J in, factors out (FP64)
+    # ---- roofline of the dominant kernel: the mixed form's reduction (its launches alone) ----
+    # algorithmic bytes: the FP32 GEMV stream 4 n^3 / 3 (every step re-reads the trailing block)
+    # + 16 n^2 (J in, factors and Ht out in FP64)
+    alg_bytes = 4.0 * n ** 3 / 3.0 + 16.0 * n * n
     peak, peak_kind = peaks()
     red = ph_mixed["reduce"]
     achieved = alg_bytes / (red * 1e-3) / 1e9
     traffic = None
-    tp = os.path.join(REPO, "profiles", "reduce_mixed_kernel_c2_n2048.md")
+    tp = os.path.join(REPO, "profiles", f"reduce_mixed_{args.config}.md")
     if os.path.exists(tp):
         for line in open(tp):
             if line.startswith("dram_bytes_per_launch:"):
                 traffic = float(line.split(":")[1])
 
     # ---- end to end through the public API: host buffers, copies inside the timed region ----
-    def pinned_colmajor(a):
-        t = torch.empty((a.shape[1], a.shape[0]), dtype=torch.float64, pin_memory=True).t()
+    def pinned(a):
+        t = torch.empty((a.shape[1], a.shape[0]), dtype=torch.from_numpy(a[:1, :1].copy()).dtype,
+                        pin_memory=True).t()
         t.copy_(torch.as_tensor(a))
         return t
 
-    Jh = pinned_colmajor(cfg["J"])
-    Bh = pinned_colmajor(cfg["B"])
-    sh_h = torch.as_tensor(np.stack([cfg["sigma"], cfg["tau"]])).pin_memory()
-    Xh = torch.empty((S, n), dtype=torch.float64, pin_memory=True).t()
-    # Two device input slots: a Jacobian stream is served double-buffered, the copy of step t+1's
-    # inputs (on a copy stream) overlapping step t's work.  Every step still copies its own J, B
-    # and shifts from pinned host memory and reads its solutions back, all inside the timed region;
-    # the L2 flush is inside it too.
-    slots = [(torch.empty_like(Jd), torch.empty_like(Bd), torch.empty((2, S), dtype=torch.float64, device=dev))
-             for _ in range(2)]
+    Jh = pinned(w["J"])
+    Bh = pinned(w["B"])
+    sh_h = torch.as_tensor(np.stack([w["sigma"], w["tau"]]).astype(w["B"].dtype if w["cplx"] else np.float64)).pin_memory()
+    Xh = torch.empty((S * R, n), dtype=mixed.X.dtype, pin_memory=True).t()
+    # Two device input slots: a stream of Jacobians is served double-buffered, the copy of step
+    # t+1's inputs (on a copy stream) overlapping step t's work.  Every step still copies its own
+    # J, B and shifts from pinned host memory and reads its solutions back, inside the timed region.
+    slots = [(torch.empty_like(Jd), torch.empty_like(Bd), torch.empty_like(sh_h, device=dev)) for _ in range(2)]
     copy_stream = torch.cuda.Stream()
     ready = [torch.cuda.Event() for _ in range(2)]
     freed = [torch.cuda.Event() for _ in range(2)]
@@ -429,8 +602,6 @@ def main():
             ready[s].record(copy_stream)
 
     def e2e_run(K):
-        """K steps: the first step's copy, then per step t: the copy of step t+1 issued, the wait
-        for step t's inputs, the L2 flush, the step, the read-back of X."""
         for s in range(2):
             freed[s].record(stream)
         load_inputs(0)
@@ -445,116 +616,134 @@ def main():
             freed[s].record(stream)
             Xh.copy_(mixed.X, non_blocking=True)
 
-    e2e_run(2)
+    e2e_steps = min(args.steps, E2E_STEPS_MAX)
+    e2e_run(1)
     torch.cuda.synchronize()
     ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     ev0.record(stream)
-    e2e_run(args.steps)
+    e2e_run(e2e_steps)
     ev1.record(stream)
     torch.cuda.synchronize()
-    e2e_ms = ev0.elapsed_time(ev1) / args.steps
-    h2d = Jh.numel() * 8 + Bh.numel() * 8 + sh_h.numel() * 8
-    d2h = Xh.numel() * 8
+    e2e_ms = ev0.elapsed_time(ev1) / e2e_steps
+    h2d = Jh.numel() * Jh.element_size() + Bh.numel() * Bh.element_size() + sh_h.numel() * sh_h.element_size()
+    d2h = Xh.numel() * Xh.element_size()
+    e2e_res = G.residual_norms(sh, Jd, Bd, torch.as_tensor(Xh.numpy()).to(dev).t().contiguous().t(),
+                               rhs_per_shift=R).cpu().numpy() if w["cplx"] else None
+    del slots, Jh, Bh, Xh
 
-    # ---- config 4: 4096 independent Jacobians of uneven order, batched (FP64) ----
-    c4 = None
-    if not args.no_c4:
-        from lhl_gpu.sharding import jacobian_partition
-        cfg4 = configs.config4()
-        total4 = len(cfg4["ns"])
-        mine = jacobian_partition([int(v) for v in cfg4["ns"]], world)[rank]  # all of them on one GPU
-        ns4 = [int(cfg4["ns"][i]) for i in mine]
-        S4, R4 = 8, 4
-        bt = G.LHLBatch(ns4, S4)
-        J4 = torch.as_tensor(bt.pack_matrices([cfg4["mats"][i] for i in mine])).to(dev)
-        B4 = torch.as_tensor(bt.pack_rhs([cfg4["rhs"][i][:, :S4 * R4] for i in mine])).to(dev)
-        X4 = torch.empty_like(B4)
-        sg4 = torch.as_tensor(cfg4["sigma"][mine].ravel()).to(dev)
-        ta4 = torch.as_tensor(cfg4["tau"][mine].ravel()).to(dev)
-        res4 = torch.empty(len(ns4) * S4 * R4, dtype=torch.float64, device=dev)
+    # ---- extras: the other configurations (both forms) and the batched config 4 ----
+    extras = {}
+    if not args.no_extras:
+        del mixed, plain, sh
+        torch.cuda.empty_cache()
+        for nm, st in (("c1", 3), ("c2", 3), ("c3", 2)):
+            if nm != args.config:
+                extras[nm] = config_extra(G, torch, nm, cfgs, dev, stream, flush, st)
+        extras["c4"] = batched_c4(G, torch, cfgs, dev, stream, flush, world, rank)
 
-        def c4_step():
-            G.lhl_reduce_batched_(bt, J4, True)
-            G.lhl_shift_batched_all_(bt, sg4, ta4)
-            G.lhl_solve_batched_(bt, J4, B4, X4, R4, tol=TOL, max_steps=6, res=res4)
-
-        for _ in range(3):
-            c4_step()
-        torch.cuda.synchronize()
-        c4_ms = time_events(stream, c4_step, max(3, min(args.steps, 5)), flush)
-        r4 = res4.cpu().numpy()
-        assert (r4 <= TOL).all(), f"config 4 residual above {TOL}: {r4.max()}"
-        c4 = {"workload": "c4: 4096 J, n uniform [16,256], N(0,1) - 5I; 8 shifts (1,-g) g log-uniform "
-                          "[1e-3,1e-1]; 4 RHS/shift; reduction + shift LUs + solves refined to 1e-10, "
-                          "three launches, FP64 (plain form)",
-              "value": None, "unit": UNIT, "ms_per_step": None, "ranks": world,
-              "partition": "matrices balanced across ranks by n^3 (lhl_gpu.sharding.jacobian_partition)",
-              "phases_ms": {"reduce_batched": time_events(stream, lambda: G.lhl_reduce_batched_(bt, J4, True), 3,
-                                                          flush),
-                            "shift_batched_all": time_events(stream, lambda: G.lhl_shift_batched_all_(bt, sg4, ta4),
-                                                             3, flush),
-                            "solve_batched": time_events(stream, lambda: G.lhl_solve_batched_(
-                                bt, J4, B4, X4, R4, tol=TOL, max_steps=6, res=res4), 3, flush)},
-              "max_rel_residual": float(r4.max()), "_ms": c4_ms}
-
-    # ---- max over ranks ----
-    ms_mixed, ms_plain, e2e_ms, c4_max = max_over_ranks(
-        [ms_mixed, ms_plain, e2e_ms, c4["_ms"] if c4 else 0.0], dev, pg)
-    if c4:
-        c4.pop("_ms")
-        c4["ms_per_step"] = c4_max
-        c4["value"] = total4 * S4 * R4 / (c4_max * 1e-3)
-    value = whole_job_rate(world, S, ms_mixed)
-    plain_value = whole_job_rate(world, S, ms_plain)
+    ms_mixed, ms_plain, e2e_ms = max_over_ranks([ms_mixed, ms_plain, e2e_ms], dev, pg)
+    value = whole_job_rate(world, S * R, ms_mixed)
+    plain_value = whole_job_rate(world, S * R, ms_plain)
 
     if rank == 0:
         cpu = None
-        if not args.no_cpu_baseline:
-            from oracle import oracle as O
-            times, Xc = cpu_reference_run(cfg, args.cpu_baseline_steps, 0, None)
-            sec = float(np.mean(times))
-            cpu = {"value": S / sec, "unit": UNIT, "cores": O.num_threads(), "kind": "port",
-                   "sample": f"{len(times)} full step(s) (FP64 reduction + 64 shift LUs + solves + 1 refinement), "
-                             f"oracle C restatement with OpenMP, {sec:.2f} s/step"}
+        if not args.no_cpu_baseline and world == 1:
+            threads = host_threads()
+            sec, t_red, t_sh, desc = cpu_sample(w, max(1, args.cpu_shifts), threads)
+            cpu = {"value": S * R / sec, "unit": UNIT, "cores": threads, "kind": "port",
+                   "sample": desc + "; oracle C restatement (the reference is Julia, absent on this box)"}
         line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
-                "warmup": max(args.warmup, 3), "ms_per_step": ms_mixed, "higher_is_better": True, "scaling": "weak",
+                "warmup": args.warmup, "ms_per_step": ms_mixed, "higher_is_better": True, "scaling": "weak",
                 "vs_baseline": None, "dtype": "f64 (mixed form: f32 reduction)",
-                "data": "synthetic (numpy PCG64 seeds 2,3,4)", "config": config,
-                "plain_fp64": {"value": plain_value, "unit": UNIT, "ms_per_step": ms_plain,
-                               "max_rel_residual": res_plain, "phases_ms": ph_plain,
+                "data": "synthetic (numpy PCG64 seeds; no public dataset)",
+                "config": {"workload": DESCR[args.config] + "; one step = reduction + every shift LU + every solve "
+                                                             "+ refinement until every solve is at <= 1e-10",
+                           "n": n, "shifts": S, "rhs_per_shift": R, "tolerance": TOL,
+                           "form": "mixed: FP32 reduction, FP64 balancing, shift LUs, solves, residuals and "
+                                   "refinement", "l2": "flushed between timed steps (256 MiB write)",
+                           "replicas": world},
+                "max_rel_residual": float(res_mixed.max()), "forward_error": fe_mixed,
+                "refinement": mixed_refine_desc(args.config),
+                "plain_fp64": {"value": plain_value, "unit": UNIT, "ms_per_step": ms_plain, "steps": steps_plain,
+                               "warmup": 1, "max_rel_residual": float(res_plain.max()), "forward_error": fe_plain,
+                               "phases_ms": ph_plain, "refinement": plain_refine_desc(args.config),
                                "form": "plain: FP64 throughout, bit-identical reduction and shift LUs",
                                "clocks": clk_plain},
                 "mixed_vs_plain": value / plain_value,
-                "excluding_reduction": {"mixed": S / (ph_mixed["chain"] * 1e-3), "plain": S / (ph_plain["chain"] * 1e-3),
-                                        "unit": UNIT, "note": "S*R / T(shift + solve + refine), reduction excluded"},
-                "phases_ms": ph_mixed, "max_rel_residual": res_mixed,
-                "refinement": {"method": f"GMRES-IR: GMRES({MIXED_REFINE[2]}) cycles left-preconditioned by the "
-                                         f"shift's factorisation, host check per cycle",
-                               "gmres_cycles_needed": gm_cycles,
-                               "fixed_point_steps_needed": {
-                                   "max": int(need.max()), "mean": float(need.mean()),
-                                   "histogram": {int(k): int((need == k).sum()) for k in np.unique(need)}},
-                               "chain_ms_with_fixed_point": fixed_chain_ms},
+                "phases_ms": ph_mixed,
+                "excluding_reduction": {"mixed": S * R / ((ms_mixed - ph_mixed["reduce"]) * 1e-3),
+                                        "plain": S * R / ((ms_plain - ph_plain["reduce"]) * 1e-3), "unit": UNIT,
+                                        "note": "S*R / T(shift + solve + refine), reduction excluded"},
                 "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                              "frac": achieved / peak, "traffic": traffic, "peak_kind": peak_kind,
-                             "kernel": "lhl_reduce, mixed form (balance + FP32 ELMHES, cooperative launches)",
-                             "algorithmic_bytes": alg_bytes},
-                "roofline_step": {"t_lower_ms": step_lower_ms(peak), "t_measured_ms": ms_mixed,
-                                  "frac": step_lower_ms(peak) / ms_mixed,
-                                  "counts": "reduction + all shift LUs + one solve pass + one residual pass, "
-                                            "compulsory HBM bytes at the measured copy bandwidth"},
+                             "kernel": "lhl_reduce, mixed form (its launches alone)",
+                             "algorithmic_bytes": alg_bytes,
+                             "algorithmic": "4 n^3 / 3 (FP32 GEMV stream) + 16 n^2 (J in, factors and Ht out)"},
                 "cpu_baseline": cpu,
-                "e2e": {"value": world * S / (e2e_ms * 1e-3), "unit": UNIT, "h2d_bytes_per_step": h2d,
-                        "d2h_bytes_per_step": d2h, "ms_per_step": e2e_ms,
-                        "timing": "K steps in one event-timed region through the public API: per step the "
-                                  "pinned host->device copy of J, B and the shifts (double-buffered: step "
-                                  "t+1's copy overlaps step t), the L2 flush, the step, the read-back of X"},
-                "batched_c4": c4,
+                "e2e": {"value": world * S * R / (e2e_ms * 1e-3), "unit": UNIT, "h2d_bytes_per_step": h2d,
+                        "d2h_bytes_per_step": d2h, "ms_per_step": e2e_ms, "steps": e2e_steps,
+                        "max_rel_residual": float(e2e_res.max()) if e2e_res is not None else None,
+                        "timing": "K steps in one event-timed region through the public API: per step the pinned "
+                                  "host->device copy of J, B and the shifts (double-buffered: step t+1's copy "
+                                  "overlaps step t), the L2 flush, the step, the read-back of X"},
+                "extras": extras,
                 "gpu_launches": launches * args.steps if launches is not None else None,
                 "clocks": clk_mixed}
         print(json.dumps(line), flush=True)
     if pg:
         pg.destroy_process_group()
+
+
+def mixed_refine_desc(name):
+    r = REFINE[(name, "mixed")]
+    return (f"GMRES-IR, GMRES({r[2]}) x {r[1]} cycles at most" if r[0] == "gmres"
+            else f"fixed-point lhl_refine_tol, {r[1]} steps at most")
+
+
+def plain_refine_desc(name):
+    r = REFINE[(name, "plain")]
+    return f"fixed-point lhl_refine_tol, {r[1]} steps at most"
+
+
+def batched_c4(G, torch, cfgs, dev, stream, flush, world, rank):
+    """Config 4: 4096 independent Jacobians of uneven order, batched (FP64), this rank's share."""
+    from lhl_gpu.sharding import jacobian_partition
+    cfg4 = cfgs.config4()
+    total4 = len(cfg4["ns"])
+    mine = jacobian_partition([int(v) for v in cfg4["ns"]], world)[rank]
+    ns4 = [int(cfg4["ns"][i]) for i in mine]
+    S4, R4 = 8, 4
+    bt = G.LHLBatch(ns4, S4)
+    J4 = torch.as_tensor(bt.pack_matrices([cfg4["mats"][i] for i in mine])).to(dev)
+    B4 = torch.as_tensor(bt.pack_rhs([cfg4["rhs"][i][:, :S4 * R4] for i in mine])).to(dev)
+    X4 = torch.empty_like(B4)
+    sg4 = torch.as_tensor(cfg4["sigma"][mine].ravel()).to(dev)
+    ta4 = torch.as_tensor(cfg4["tau"][mine].ravel()).to(dev)
+    res4 = torch.empty(len(ns4) * S4 * R4, dtype=torch.float64, device=dev)
+
+    def c4_step():
+        G.lhl_reduce_batched_(bt, J4, True)
+        G.lhl_shift_batched_all_(bt, sg4, ta4)
+        G.lhl_solve_batched_(bt, J4, B4, X4, R4, tol=TOL, max_steps=6, res=res4)
+
+    for _ in range(3):
+        c4_step()
+    torch.cuda.synchronize()
+    c4_ms = time_events(torch, stream, c4_step, 5, flush)
+    r4 = res4.cpu().numpy()
+    assert (r4 <= TOL).all(), f"config 4 residual above {TOL}: {r4.max()}"
+    return {"workload": "c4: 4096 J, n uniform [16,256], N(0,1) - 5I; 8 shifts (1,-g) g log-uniform [1e-3,1e-1]; "
+                        "4 RHS/shift; reduction + shift LUs + solves refined to 1e-10, three launches, FP64",
+            "value": len(ns4) * S4 * R4 / (c4_ms * 1e-3) * world, "unit": UNIT, "ms_per_step": c4_ms,
+            "matrices": total4, "partition": "matrices balanced across ranks by n^3 (lhl_gpu.sharding)",
+            "phases_ms": {"reduce_batched": time_events(torch, stream, lambda: G.lhl_reduce_batched_(bt, J4, True),
+                                                        3, flush),
+                          "shift_batched_all": time_events(torch, stream, lambda: G.lhl_shift_batched_all_(bt, sg4,
+                                                                                                          ta4),
+                                                           3, flush),
+                          "solve_batched": time_events(torch, stream, lambda: G.lhl_solve_batched_(
+                              bt, J4, B4, X4, R4, tol=TOL, max_steps=6, res=res4), 3, flush)},
+            "max_rel_residual": float(r4.max())}
 
 
 if __name__ == "__main__":

@@ -620,6 +620,39 @@ int lhl_shift(lhl_shift_t sh, lhl_ws_t ws, int64_t slot, double sigma, double ta
     return shift_run(sh, ws, slot, 1, st);
 }
 
+// Complex shifts with many right-hand sides: the solve scratch Y (n x ycap real columns) grows
+// so that one pass of the solve kernels covers every right-hand side (each complex one is two
+// real columns), up to 1 GiB; the multi-right-hand-side Hessenberg solve then has every
+// shift's group of vectors in one launch.  Grow-only; a failed allocation keeps the old buffer
+// (the solve then runs in chunks of it).  cudaFree waits for work in flight on the old one.
+static void ws_grow_y(lhl_ws_t ws, lhl_shift_t sh, int64_t nrhs)
+{
+    if (!sh || !sh->cplx || ws->cj || ws->n <= 0) return;
+    const int64_t want = 2 * nrhs;
+    if (want <= ws->ycap) return;
+    const int64_t cap_max = (int64_t)((1ull << 30) / (8ull * (uint64_t)ws->n));
+    const int64_t cap = want < cap_max ? want : cap_max;
+    if (cap <= ws->ycap) return;
+    const int64_t nflags = ((ws->n + 63) / 64) * ((cap + 3) / 4);
+    double* y = nullptr;
+    int* f = nullptr;
+    if (cudaMalloc((void**)&y, (size_t)ws->n * (size_t)cap * sizeof(double)) != cudaSuccess) {
+        cudaGetLastError();
+        return;
+    }
+    if (cudaMalloc((void**)&f, (size_t)nflags * sizeof(int)) != cudaSuccess) {
+        cudaGetLastError();
+        cudaFree(y);
+        return;
+    }
+    cudaFree(ws->ybuf);
+    cudaFree(ws->zflags);
+    ws->ybuf = y;
+    ws->zflags = f;
+    ws->ycap = (int)cap;
+    ws->nzflags = (int)nflags;
+}
+
 static int ldiv_common(lhl_shift_t sh, lhl_ws_t ws, double* dX, int64_t ldx, int64_t nrhs, int64_t rps, int mode,
                        cudaStream_t st)
 {
@@ -630,6 +663,7 @@ static int ldiv_common(lhl_shift_t sh, lhl_ws_t ws, double* dX, int64_t ldx, int
     if (ldx < n) return LHL_ERR_DIM;
     if (n > 8192) return LHL_ERR_DIM;
     if (ws->cj && sh && !sh->cplx) return LHL_ERR_ARG;
+    if (mode == 0) ws_grow_y(ws, sh, nrhs);
     lhl::LdivArgs a;
     memset(&a, 0, sizeof(a));
     a.n = (int)n;
@@ -771,8 +805,9 @@ int lhl_refine(lhl_shift_t sh, lhl_ws_t ws, const double* dJ, int64_t ldj, const
 
 // lhl_ldiv's arguments for the refinement loops: R in place, columns with done[c] <= tol skipped
 static lhl::LdivArgs refine_ldiv_args(lhl_shift_t sh, lhl_ws_t ws, double* dR, int64_t ldr, int64_t rps,
-                                      const double* done, double tol)
+                                      const double* done, double tol, int64_t nrhs)
 {
+    ws_grow_y(ws, sh, nrhs);
     lhl::LdivArgs a;
     memset(&a, 0, sizeof(a));
     a.n = (int)ws->n;
@@ -841,7 +876,7 @@ int lhl_refine_tol(lhl_shift_t sh, lhl_ws_t ws, const double* dJ, int64_t ldj, c
         if (e == cudaSuccess) e = relres_any(sh, n, dR, ldx, dB, ldb, dres, nrhs, st);
         if (e != cudaSuccess) return LHL_ERR_CUDA;
         if (s == max_steps) break;
-        e = lhl::launch_ldiv(refine_ldiv_args(sh, ws, dR, ldx, rhs_per_shift, dres, tol), (int)nrhs, st);
+        e = lhl::launch_ldiv(refine_ldiv_args(sh, ws, dR, ldx, rhs_per_shift, dres, tol, nrhs), (int)nrhs, st);
         if (e == cudaSuccess) e = axpy_any(sh, n, dX, ldx, dR, ldx, nrhs, st, dres, tol);
         if (e != cudaSuccess) return LHL_ERR_CUDA;
     }
@@ -904,14 +939,14 @@ int lhl_refine_gmres(lhl_shift_t sh, lhl_ws_t ws, const double* dJ, int64_t ldj,
             if (none) break;
         }
         // z = W~^-1 r for those columns, then the cycle's Arnoldi steps
-        e = lhl::launch_ldiv(refine_ldiv_args(sh, ws, dR, ldx, rhs_per_shift, ws->gmA, 0.5), nr, st);
+        e = lhl::launch_ldiv(refine_ldiv_args(sh, ws, dR, ldx, rhs_per_shift, ws->gmA, 0.5, nr), nr, st);
         if (e == cudaSuccess)
             e = lhl::launch_gm_begin(ne, m, dR, (int)(P * ldx), ws->gmV, ws->gmS, ws->gmA, dres, tol, nr, st);
         for (int j = 0; j < m && e == cudaSuccess; ++j) {
             e = resid_any(sh, n, dJ, ldj, nullptr, 0, ws->gmV + (size_t)P * j * n, ldv, dR, ldx, nrhs,
                           rhs_per_shift, st, ws->gmA, 0.5);
             if (e == cudaSuccess)
-                e = lhl::launch_ldiv(refine_ldiv_args(sh, ws, dR, ldx, rhs_per_shift, ws->gmA, 0.5), nr, st);
+                e = lhl::launch_ldiv(refine_ldiv_args(sh, ws, dR, ldx, rhs_per_shift, ws->gmA, 0.5, nr), nr, st);
             if (e == cudaSuccess)
                 e = lhl::launch_gm_arnoldi(ne, m, j, dR, (int)(P * ldx), ws->gmV, ws->gmS, ws->gmA, nr, st);
         }

@@ -298,6 +298,262 @@ cudaError_t launch_hess_cplx(int n, const double* Gt, int ldg, int po, const uin
     return cudaGetLastError();
 }
 
+// ---- planar Hessenberg solve of several right-hand sides of one shift per CTA ----
+// The same solve as hess_cplx_kernel (F:2823-2884) for a group of up to MG complex
+// right-hand sides that share a shift, so that the shift's Gt (0.5 GB per plane pair at
+// n = 8192) is streamed once per group instead of once per right-hand side.  The vectors stay
+// in the scratch Y (global memory, L2-resident); the CTA works on them in place:
+//   1. the forward select-swap recurrence (F:2827-2838), one thread per right-hand side, on
+//      chunks of 32 steps staged in shared memory by the whole CTA;
+//   2. the back substitution in blocks of 32 rows from the bottom, left-looking: for block b
+//      the products U[b, j] x[j] over the solved rows j below it are a small complex GEMM
+//      (32 rows x MG right-hand sides x K), K in chunks of 64 staged by cp.async (double
+//      buffered), each thread a 4 x 4 complex register tile over one of 16 interleaved K
+//      slices, the slices summed by half-warp shuffles; then one warp per right-hand side
+//      solves the 32 x 32 triangle with rdiag (shuffles, as the one-vector kernel does).
+// Results agree with the one-vector kernel to rounding (the summation order differs).
+constexpr int MG = 8;        // complex right-hand sides per CTA
+constexpr int MT = 256;      // threads
+constexpr int MRB = 32;      // rows per back-substitution block
+constexpr int MKC = 64;      // K chunk
+constexpr int MUP = MKC + 1; // padded row pitch of the staged U tile
+constexpr int MXP = MG + 1;  // padded pitch of the staged x tile
+constexpr int MFC = 32;      // forward-recurrence chunk (steps)
+struct MrhsSmem {
+    double U[2][2][MRB][MUP];    // [stage][plane][row][k]
+    double X[2][2][MKC][MXP];    // [stage][part][k][rhs]
+    double T[2][MRB][MRB + 1];   // diagonal block U_bb: [plane][row][col]
+    double D[2][MRB][MXP];       // block sums: [part][row][rhs]
+    double F[2][MFC + 1][MG];    // forward recurrence: y chunk [part][step][rhs]
+    double FL[2][MFC];           // forward recurrence: multipliers l_k [part][step]
+    unsigned char FS[MFC];       // forward recurrence: swaps
+};
+
+// 8-byte asynchronous copy global -> shared; a masked copy reads nothing (source size 0, the
+// destination is zero-filled) and is given `base`, a valid address, as its source
+__device__ __forceinline__ void cp_async8(double* dst, const double* src, bool valid, const double* base)
+{
+    const unsigned d = (unsigned)__cvta_generic_to_shared(dst);
+    const int sz = valid ? 8 : 0;
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;" ::"r"(d), "l"(valid ? src : base), "r"(sz)
+                 : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+template <int N> __device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory"); }
+
+__global__ void __launch_bounds__(MT, 2) hess_cplx_mrhs_kernel(int n, const double* __restrict__ Gt_all, int ldg,
+                                                               int po, const uint8_t* __restrict__ swap_all,
+                                                               const double* __restrict__ rdiag_all, double* Y,
+                                                               int ldy, int col0, int count, int rhs_per_shift,
+                                                               int s_first, int groups_per_shift,
+                                                               const double* __restrict__ done, double tol)
+{
+    extern __shared__ __align__(16) unsigned char mrhs_raw[];
+    MrhsSmem& sm = *reinterpret_cast<MrhsSmem*>(mrhs_raw);
+    const int s = s_first + blockIdx.x / groups_per_shift;
+    const int g = blockIdx.x % groups_per_shift;
+    // this CTA's complex right-hand sides: [c_lo, c_hi) of the chunk (global indices)
+    const int c_lo = max(col0, s * rhs_per_shift + g * MG);
+    const int c_hi = min(min(col0 + count, (s + 1) * rhs_per_shift), s * rhs_per_shift + g * MG + MG);
+    if (c_lo >= c_hi) return;
+    const int ng = c_hi - c_lo;
+    if (done) {
+        bool all = true;
+        for (int c = c_lo; c < c_hi; ++c) all = all && (done[c] <= tol);
+        if (all) return;
+    }
+    const int t = threadIdx.x, lane = t & 31, warp = t >> 5;
+    const double* Gt = Gt_all + (size_t)s * ldg * n;
+    const uint8_t* swp = swap_all + (size_t)s * n;
+    const double* rd = rdiag_all + (size_t)s * 2 * n;
+    // part p of right-hand side v (0 <= v < ng): column 2 (c_lo - col0 + v) + p of Y
+    auto ycol = [&](int v, int p) -> double* { return Y + (size_t)(2 * (c_lo - col0 + v) + p) * ldy; };
+
+    // ---- 1. forward recurrence, chunks of MFC steps: element k (1-based) of the chunk at row k0 + i
+    if (n >= 2) {
+        dc c = {0.0, 0.0};
+        if (t < ng) c = {ycol(t, 0)[0], ycol(t, 1)[0]};
+        for (int k0 = 1; k0 <= n - 1; k0 += MFC) {
+            const int cnt = min(MFC, n - k0);  // steps k0 .. k0 + cnt - 1
+            // stage y[k] (0-based index k, k = k0 .. k0+cnt-1), l_k and swap_k
+            for (int e = t; e < 2 * MG * MFC; e += MT) {
+                const int i = e % MFC, v = (e / MFC) % MG, p = e / (MFC * MG);
+                sm.F[p][i][v] = (i < cnt && v < ng) ? ycol(v, p)[k0 + i] : 0.0;
+            }
+            if (t < 2 * MFC) {
+                const int i = t % MFC, p = t / MFC;
+                const int k = k0 + i;
+                sm.FL[p][i] = i < cnt ? M1(Gt, ldg, p * po + k, k + 1) : 0.0;
+            }
+            if (t < MFC) sm.FS[t] = t < cnt ? swp[k0 + t - 1] : 0;
+            __syncthreads();
+            if (t < ng) {
+                for (int i = 0; i < cnt; ++i) {
+                    const dc b = {sm.F[0][i][t], sm.F[1][i][t]};
+                    const bool sw = sm.FS[i] != 0;
+                    const dc xk = sw ? b : c;
+                    sm.F[0][i][t] = xk.re;  // becomes y[k - 1]
+                    sm.F[1][i][t] = xk.im;
+                    const dc lk = {sm.FL[0][i], sm.FL[1][i]};
+                    c = csub(sw ? c : b, cmul(lk, xk));
+                }
+            }
+            __syncthreads();
+            for (int e = t; e < 2 * MG * MFC; e += MT) {  // y[k-1] for k = k0 .. k0+cnt-1
+                const int i = e % MFC, v = (e / MFC) % MG, p = e / (MFC * MG);
+                if (i < cnt && v < ng) ycol(v, p)[k0 + i - 1] = sm.F[p][i][v];
+            }
+            __syncthreads();
+        }
+        if (t < ng) {
+            ycol(t, 0)[n - 1] = c.re;
+            ycol(t, 1)[n - 1] = c.im;
+        }
+        __syncthreads();
+    }
+
+    // ---- 2. back substitution
+    const int q = t & 15;           // K slice: k = q + 16 u of each chunk
+    const int rg = (t >> 4) & 7;    // rows rg + 8 i of the block
+    const int gg = t >> 7;          // right-hand sides 4 gg + v
+    for (int r1 = n; r1 >= 1; r1 -= MRB) {
+        const int r0 = max(r1 - MRB + 1, 1);
+        const int bs = r1 - r0 + 1;
+        // diagonal block U[r0 + a, r0 + b] = Gt[r0 + b, r0 + a] (b >= a), both planes
+        for (int e = t; e < 2 * MRB * MRB; e += MT) {
+            const int bb = e % MRB, a = (e / MRB) % MRB, p = e / (MRB * MRB);
+            sm.T[p][a][bb] = (a < bs && bb < bs && bb >= a) ? M1(Gt, ldg, p * po + r0 + bb, r0 + a) : 0.0;
+        }
+        double ar[4][4], ai[4][4];
+#pragma unroll
+        for (int i = 0; i < 4; ++i)
+#pragma unroll
+            for (int v = 0; v < 4; ++v) ar[i][v] = ai[i][v] = 0.0;
+        const int K = n - r1;  // solved rows r1+1 .. n
+        const int nch = (K + MKC - 1) / MKC;
+        auto stage = [&](int ch, int st) {
+            const int j0 = r1 + 1 + ch * MKC;  // first row (1-based) of the chunk
+            for (int e = t; e < 2 * MRB * MKC; e += MT) {
+                const int kk = e % MKC, a = (e / MKC) % MRB, p = e / (MKC * MRB);
+                const int j = j0 + kk;
+                const bool ok = a < bs && j <= n;
+                cp_async8(&sm.U[st][p][a][kk], ok ? &M1(Gt, ldg, p * po + j, r0 + a) : Gt, ok, Gt);
+            }
+            for (int e = t; e < 2 * MKC * MG; e += MT) {
+                const int kk = e % MKC, v = (e / MKC) % MG, p = e / (MKC * MG);
+                const int j = j0 + kk;
+                const bool ok = v < ng && j <= n;
+                cp_async8(&sm.X[st][p][kk][v], ok ? &ycol(v, p)[j - 1] : Gt, ok, Gt);
+            }
+            cp_async_commit();
+        };
+        if (nch > 0) stage(0, 0);
+        for (int ch = 0; ch < nch; ++ch) {
+            const int st = ch & 1;
+            if (ch + 1 < nch) {
+                stage(ch + 1, st ^ 1);
+                cp_async_wait<1>();
+            } else {
+                cp_async_wait<0>();
+            }
+            __syncthreads();
+#pragma unroll
+            for (int u = 0; u < MKC / 16; ++u) {
+                const int kk = q + 16 * u;
+                double ur[4], ui[4], xr[4], xi[4];
+#pragma unroll
+                for (int i = 0; i < 4; ++i) {
+                    ur[i] = sm.U[st][0][rg + 8 * i][kk];
+                    ui[i] = sm.U[st][1][rg + 8 * i][kk];
+                }
+#pragma unroll
+                for (int v = 0; v < 4; ++v) {
+                    xr[v] = sm.X[st][0][kk][4 * gg + v];
+                    xi[v] = sm.X[st][1][kk][4 * gg + v];
+                }
+#pragma unroll
+                for (int i = 0; i < 4; ++i)
+#pragma unroll
+                    for (int v = 0; v < 4; ++v) {
+                        ar[i][v] = fma(ur[i], xr[v], ar[i][v]);
+                        ar[i][v] = fma(-ui[i], xi[v], ar[i][v]);
+                        ai[i][v] = fma(ur[i], xi[v], ai[i][v]);
+                        ai[i][v] = fma(ui[i], xr[v], ai[i][v]);
+                    }
+            }
+            __syncthreads();  // the stage this chunk used is refilled two chunks on
+        }
+        // sum the 16 K slices (lanes q of a half-warp)
+#pragma unroll
+        for (int i = 0; i < 4; ++i)
+#pragma unroll
+            for (int v = 0; v < 4; ++v) {
+#pragma unroll
+                for (int o = 8; o >= 1; o >>= 1) {
+                    ar[i][v] += __shfl_xor_sync(0xffffffffu, ar[i][v], o);
+                    ai[i][v] += __shfl_xor_sync(0xffffffffu, ai[i][v], o);
+                }
+            }
+        if (q == 0) {
+#pragma unroll
+            for (int i = 0; i < 4; ++i)
+#pragma unroll
+                for (int v = 0; v < 4; ++v) {
+                    sm.D[0][rg + 8 * i][4 * gg + v] = ar[i][v];
+                    sm.D[1][rg + 8 * i][4 * gg + v] = ai[i][v];
+                }
+        }
+        __syncthreads();
+        // triangle: warp v solves right-hand side v
+        if (warp < ng) {
+            const int v = warp;
+            const int i = r0 + lane;  // this lane's row
+            dc yv = {0.0, 0.0}, rdi = {0.0, 0.0};
+            if (i <= r1) {
+                yv = csub(dc{ycol(v, 0)[i - 1], ycol(v, 1)[i - 1]}, dc{sm.D[0][lane][v], sm.D[1][lane][v]});
+                rdi = dc{rd[2 * (i - 1)], rd[2 * (i - 1) + 1]};
+            }
+            for (int j = r1; j >= r0; --j) {
+                dc xj = {0.0, 0.0};
+                if (i == j) {
+                    yv = cmul(yv, rdi);
+                    xj = yv;
+                }
+                xj.re = __shfl_sync(0xffffffffu, xj.re, j - r0);
+                xj.im = __shfl_sync(0xffffffffu, xj.im, j - r0);
+                if (i < j) yv = csub(yv, cmul(dc{sm.T[0][lane][j - r0], sm.T[1][lane][j - r0]}, xj));
+            }
+            if (i <= r1) {
+                ycol(v, 0)[i - 1] = yv.re;
+                ycol(v, 1)[i - 1] = yv.im;
+            }
+        }
+        __syncthreads();  // x of this block is in Y before the next block's K chunks read it
+    }
+}
+
+cudaError_t launch_hess_cplx_mrhs(int n, const double* Gt, int ldg, int po, const uint8_t* swp, const double* rd,
+                                  double* Y, int ldy, int col0, int count, int rhs_per_shift, const double* done,
+                                  double tol, cudaStream_t st)
+{
+    if (count <= 0 || n <= 0) return cudaSuccess;
+    const int s_first = col0 / rhs_per_shift, s_last = (col0 + count - 1) / rhs_per_shift;
+    const int gps = (rhs_per_shift + MG - 1) / MG;
+    const long long grid = (long long)(s_last - s_first + 1) * gps;
+    if (grid > 0x7fffffffll) return cudaErrorInvalidValue;
+    const size_t smem = sizeof(MrhsSmem);
+    static bool attr = false;
+    if (!attr) {
+        cudaError_t e = cudaFuncSetAttribute(hess_cplx_mrhs_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                             (int)smem);
+        if (e != cudaSuccess) return e;
+        attr = true;
+    }
+    hess_cplx_mrhs_kernel<<<(unsigned)grid, MT, smem, st>>>(n, Gt, ldg, po, swp, rd, Y, ldy, col0, count,
+                                                             rhs_per_shift, s_first, gps, done, tol);
+    return cudaGetLastError();
+}
+
 // ---- complex residual r = b - (sigma_s x + tau_s J x), J real; b, x, r interleaved complex ----
 // Tiles of 16 rows x 8 complex right-hand sides (16 real columns), one complex column pair
 // per thread; k in chunks of 64 through shared memory.

@@ -172,6 +172,10 @@ cudaError_t launch_shift_lu_cplx(int n, const double* Ht, int ldh, const double*
 cudaError_t launch_hess_cplx(int n, const double* Gt, int ldg, int po, const uint8_t* swp, const double* rd,
                              double* Y, int ldy, int col0, int count, int rhs_per_shift, const double* done,
                              double tol, cudaStream_t st);
+// the same solve for groups of right-hand sides of one shift per CTA (rhs_per_shift >= 2)
+cudaError_t launch_hess_cplx_mrhs(int n, const double* Gt, int ldg, int po, const uint8_t* swp, const double* rd,
+                                  double* Y, int ldy, int col0, int count, int rhs_per_shift, const double* done,
+                                  double tol, cudaStream_t st);
 cudaError_t launch_residual_cplx(int n, const double* J, int ldj, const double* B, int ldb, const double* X, int ldx,
                                  double* R, int ldr, int nrhs, int rhs_per_shift, const double* sig, const double* tau,
                                  cudaStream_t st, const double* done = nullptr, double tol = 0.0);

@@ -843,7 +843,12 @@ cudaError_t launch_ldiv(const LdivArgs& a, int nrhs, cudaStream_t st)
             z.gather = 1;
             z.done = a.done ? a.done + c0 : nullptr;
             cudaError_t e = run_zinv(z, st);
-            if (e == cudaSuccess)
+            // several right-hand sides per shift: one CTA per group of them streams the shift's
+            // Gt once for the group; otherwise one CTA per right-hand side
+            if (e == cudaSuccess && a.rhs_per_shift >= 4)
+                e = launch_hess_cplx_mrhs(a.n, a.Gt, a.ldg, a.po, a.swp, a.rdiag, a.Y, a.n, c0, cnt,
+                                          a.rhs_per_shift, a.done, a.tol, st);
+            else if (e == cudaSuccess)
                 e = launch_hess_cplx(a.n, a.Gt, a.ldg, a.po, a.swp, a.rdiag, a.Y, a.n, c0, cnt, a.rhs_per_shift,
                                      a.done, a.tol, st);
             if (e != cudaSuccess) return e;

@@ -580,7 +580,7 @@ def _as_cols(x: torch.Tensor, n: int):
     if x.dim() == 1:
         if x.shape[0] != n:
             raise DimensionMismatch(f"x has length {x.shape[0]}, the workspace is {n}x{n}")
-        if x.stride(0) != 1:
+        if x.stride(0) != 1 and n > 1:  # one element: any stride
             raise ArgumentError("x must be contiguous")
         return x, 1, n
     if x.dim() == 2:

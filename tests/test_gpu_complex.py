@@ -112,6 +112,36 @@ def test_complex_batched_matches_single(n):
             assert bits_equal(x1, Xh[:, 2 * s + r])
 
 
+@pytest.mark.parametrize("n,rps,ncols", [(1, 4, 8), (2, 4, 5), (33, 11, 30), (100, 32, 96), (1000, 8, 24),
+                                          (2049, 5, 14)])
+def test_complex_multi_rhs_solve_matches_one_vector_solves(n, rps, ncols):
+    """Several right-hand sides per shift take the multi-vector Hessenberg solve (groups of up
+    to eight vectors of one shift per CTA; partial groups, a partial last shift and odd orders
+    included); each column agrees with the one-vector solve of the same shift slot to 1e-10
+    (the two sum in different orders; W's condition is up to ~1e3 here) and its backward error
+    is as small as that solve's."""
+    torch, G = _mods()
+    J = rng(50 + n).standard_normal((n, n)) / np.sqrt(max(n, 1))
+    ws = G.lhl(dev(J), shift_complex=True)
+    S = (ncols + rps - 1) // rps
+    g = rng(51)
+    sig = g.uniform(-2.0, 0.0, S) + 1j * g.uniform(0.0, 10.0, S)
+    tau = -np.ones(S, dtype=complex)
+    sh = G.LHLShift(n, S, complex=True)
+    G.lhl_shift_batched_(sh, ws, dev(sig), dev(tau))
+    B = rng(52).standard_normal((n, ncols)) + 1j * rng(53).standard_normal((n, ncols))
+    X = dev(B)
+    G.lhl_ldiv_(X, sh, ws, rhs_per_shift=rps)
+    Xh = host(X)
+    eps = np.finfo(float).eps
+    for c in range(ncols):
+        G.lhl_shift_(ws, sig[c // rps], tau[c // rps])
+        x1 = host(G.lhl_ldiv_(dev(np.ascontiguousarray(B[:, c])), ws))
+        assert np.linalg.norm(Xh[:, c] - x1) <= 1e-10 * np.linalg.norm(x1), (n, rps, c)
+        W = sig[c // rps] * np.eye(n) + tau[c // rps] * J
+        assert O.bwd(W, Xh[:, c], B[:, c]) <= 4 * O.bwd(W, x1, B[:, c]) + 50 * eps, (n, rps, c)
+
+
 @pytest.mark.parametrize("precision", ["fp64", "mixed"])
 def test_resolvent_sweep_reaches_1e10(precision):
     """Config 5's shape at n = 1024: J ~ N(0,1)/sqrt(n), complex shifts s = a + ib with a in
