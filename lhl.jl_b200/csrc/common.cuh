@@ -42,6 +42,27 @@ __device__ __forceinline__ int ld_acquire_i32(const int* p)
     return v;
 }
 
+// 8-byte asynchronous copy global -> shared (cp.async); a masked copy reads nothing (source
+// size 0, the destination is zero-filled) and is given `base`, a valid address, as its source
+__device__ __forceinline__ void cp_async8(double* dst, const double* src, bool valid, const double* base)
+{
+    const unsigned d = (unsigned)__cvta_generic_to_shared(dst);
+    const int sz = valid ? 8 : 0;
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;" ::"r"(d), "l"(valid ? src : base), "r"(sz)
+                 : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+template <int N> __device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory"); }
+
+// D = A B + D on the FP64 tensor pipe, one 8 x 8 x 4 tile per warp (mma.sync m8n8k4 .f64):
+// lane (g = lane / 4, t = lane % 4) holds A[g][t], B[t][g] and D[g][2t], D[g][2t+1]
+__device__ __forceinline__ void dmma_8x8x4(double (&c)[2], double a, double b)
+{
+    asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0, %1}, {%2}, {%3}, {%0, %1};"
+                 : "+d"(c[0]), "+d"(c[1])
+                 : "d"(a), "d"(b));
+}
+
 // Grid-wide barrier for a cooperative (co-resident) grid.  `counter` only grows: the
 // b-th barrier of a launch waits until it reaches b * gridDim.x.  The wait is bounded
 // by `limit_ns` of wall time; on expiry the CTA records LHL_ERR_TIMEOUT in *err and

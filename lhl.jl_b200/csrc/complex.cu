@@ -329,18 +329,6 @@ struct MrhsSmem {
     unsigned char FS[MFC];       // forward recurrence: swaps
 };
 
-// 8-byte asynchronous copy global -> shared; a masked copy reads nothing (source size 0, the
-// destination is zero-filled) and is given `base`, a valid address, as its source
-__device__ __forceinline__ void cp_async8(double* dst, const double* src, bool valid, const double* base)
-{
-    const unsigned d = (unsigned)__cvta_generic_to_shared(dst);
-    const int sz = valid ? 8 : 0;
-    asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;" ::"r"(d), "l"(valid ? src : base), "r"(sz)
-                 : "memory");
-}
-__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
-template <int N> __device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory"); }
-
 __global__ void __launch_bounds__(MT, 2) hess_cplx_mrhs_kernel(int n, const double* __restrict__ Gt_all, int ldg,
                                                                int po, const uint8_t* __restrict__ swap_all,
                                                                const double* __restrict__ rdiag_all, double* Y,
@@ -610,11 +598,126 @@ __global__ void __launch_bounds__(QT) residual_cplx_kernel(int n, const double* 
     }
 }
 
+// ---- the same residual for many right-hand sides: J X on the FP64 tensor pipe ----
+// J X is an n x n by n x 2m real product (the two planes of m complex vectors), so it runs as
+// a tiled GEMM with mma.sync m8n8k4 FP64 (D = A B + C, FP64 products and sums): a CTA owns 128
+// rows of J x 32 complex right-hand sides (64 real columns), eight warps of 32 x 32; K in chunks
+// of 32 staged by cp.async (double buffered) into padded tiles [k][row] and [k][column] whose
+// fragment loads hit 16 distinct 8-byte banks per half-warp.  The epilogue forms
+// r = b - (sigma_s x + tau_s (J x)) as the one-tile kernel above does.
+constexpr int RM = 128, RC = 32, RN = 2 * RC, RK = 32, RTT = 256;
+constexpr int RAP = RM + 4, RBP = RN + 4;
+struct ResSmem {
+    double A[2][RK][RAP];  // J tile [k][row]
+    double B[2][RK][RBP];  // X tile [k][2 c + part]
+};
+
+__global__ void __launch_bounds__(RTT, 2) residual_cplx_mma_kernel(int n, const double* __restrict__ J, int ldj,
+                                                                   const double* __restrict__ B, int ldb,
+                                                                   const double* __restrict__ X, int ldx,
+                                                                   double* __restrict__ R, int ldr, int nrhs,
+                                                                   int rhs_per_shift, const double* __restrict__ sig,
+                                                                   const double* __restrict__ tau,
+                                                                   const double* __restrict__ done, double tol)
+{
+    extern __shared__ __align__(16) unsigned char rsm_raw[];
+    ResSmem& sm = *reinterpret_cast<ResSmem*>(rsm_raw);
+    const int i0 = blockIdx.x * RM, c0 = blockIdx.y * RC;
+    if (done) {
+        bool all = true;
+        for (int c = c0; c < c0 + RC && c < nrhs; ++c) all = all && (done[c] <= tol);
+        if (all) return;
+    }
+    const int t = threadIdx.x, lane = t & 31, warp = t >> 5;
+    const int wm = warp & 3, wn = warp >> 2;  // warp tile: rows 32 wm .., real columns 32 wn ..
+    const int g = lane >> 2, t4 = lane & 3;
+    double acc[4][4][2];
+#pragma unroll
+    for (int a = 0; a < 4; ++a)
+#pragma unroll
+        for (int b = 0; b < 4; ++b) acc[a][b][0] = acc[a][b][1] = 0.0;
+    const int nch = (n + RK - 1) / RK;
+    auto stage = [&](int kc, int st) {
+        const int k0 = kc * RK;
+        for (int e = t; e < RK * RM; e += RTT) {
+            const int m = e % RM, kk = e / RM;
+            const int i = i0 + m, k = k0 + kk;
+            const bool ok = i < n && k < n;
+            cp_async8(&sm.A[st][kk][m], ok ? &J[(size_t)k * ldj + i] : J, ok, J);
+        }
+        for (int e = t; e < RK * RC; e += RTT) {
+            const int kk = e % RK, cc = e / RK;
+            const int k = k0 + kk, c = c0 + cc;
+            const bool ok = k < n && c < nrhs;
+            const double* src = ok ? &X[2 * ((size_t)c * ldx + k)] : X;
+            cp_async8(&sm.B[st][kk][2 * cc], src, ok, X);
+            cp_async8(&sm.B[st][kk][2 * cc + 1], ok ? src + 1 : X, ok, X);
+        }
+        cp_async_commit();
+    };
+    stage(0, 0);
+    for (int kc = 0; kc < nch; ++kc) {
+        const int st = kc & 1;
+        if (kc + 1 < nch) {
+            stage(kc + 1, st ^ 1);
+            cp_async_wait<1>();
+        } else {
+            cp_async_wait<0>();
+        }
+        __syncthreads();
+#pragma unroll
+        for (int kk = 0; kk < RK; kk += 4) {
+            double fa[4], fb[4];
+#pragma unroll
+            for (int a = 0; a < 4; ++a) fa[a] = sm.A[st][kk + t4][32 * wm + 8 * a + g];
+#pragma unroll
+            for (int b = 0; b < 4; ++b) fb[b] = sm.B[st][kk + t4][32 * wn + 8 * b + g];
+#pragma unroll
+            for (int a = 0; a < 4; ++a)
+#pragma unroll
+                for (int b = 0; b < 4; ++b) dmma_8x8x4(acc[a][b], fa[a], fb[b]);
+        }
+        __syncthreads();
+    }
+    // epilogue: thread holds (J x) at row 32 wm + 8 a + g, complex column (32 wn + 8 b) / 2 + t4
+#pragma unroll
+    for (int a = 0; a < 4; ++a) {
+        const int i = i0 + 32 * wm + 8 * a + g;
+#pragma unroll
+        for (int b = 0; b < 4; ++b) {
+            const int c = c0 + (32 * wn + 8 * b) / 2 + t4;
+            if (i < n && c < nrhs) {
+                const int s = c / rhs_per_shift;
+                const dc sg = {sig[2 * s], sig[2 * s + 1]}, tu = {tau[2 * s], tau[2 * s + 1]};
+                const dc xv = {X[2 * ((size_t)c * ldx + i)], X[2 * ((size_t)c * ldx + i) + 1]};
+                const dc bv = B ? dc{B[2 * ((size_t)c * ldb + i)], B[2 * ((size_t)c * ldb + i) + 1]} : dc{0.0, 0.0};
+                const dc w = cadd(cmul(sg, xv), cmul(tu, dc{acc[a][b][0], acc[a][b][1]}));
+                R[2 * ((size_t)c * ldr + i)] = bv.re - w.re;
+                R[2 * ((size_t)c * ldr + i) + 1] = bv.im - w.im;
+            }
+        }
+    }
+}
+
 cudaError_t launch_residual_cplx(int n, const double* J, int ldj, const double* B, int ldb, const double* X, int ldx,
                                  double* R, int ldr, int nrhs, int rhs_per_shift, const double* sig, const double* tau,
                                  cudaStream_t st, const double* done, double tol)
 {
     if (nrhs <= 0 || n <= 0) return cudaSuccess;
+    if (nrhs >= 16 && (nrhs + RC - 1) / RC <= 65535) {  // many right-hand sides: the tensor-pipe GEMM
+        const size_t smem = sizeof(ResSmem);
+        static bool attr = false;
+        if (!attr) {
+            cudaError_t e = cudaFuncSetAttribute(residual_cplx_mma_kernel,
+                                                 cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+            if (e != cudaSuccess) return e;
+            attr = true;
+        }
+        dim3 grid((n + RM - 1) / RM, (nrhs + RC - 1) / RC);
+        residual_cplx_mma_kernel<<<grid, RTT, smem, st>>>(n, J, ldj, B, ldb, X, ldx, R, ldr, nrhs, rhs_per_shift, sig,
+                                                           tau, done, tol);
+        return cudaGetLastError();
+    }
     dim3 grid((n + QM - 1) / QM, (nrhs + QC - 1) / QC);
     residual_cplx_kernel<<<grid, QT, 0, st>>>(n, J, ldj, B, ldb, X, ldx, R, ldr, nrhs, rhs_per_shift, sig, tau, done,
                                               tol);

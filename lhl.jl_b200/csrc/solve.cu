@@ -785,8 +785,13 @@ cudaError_t launch_solve_batch(const BatchDesc& d, const double* J, const double
     return cudaGetLastError();
 }
 
+// Columns from which the 64-wide tensor-pipe sweeps (zlw_kernel) replace zl_kernel's 4-wide tasks.
+constexpr int ZW_MIN_COLUMNS = 1024;
+static cudaError_t run_zinv_wide(ZArgs z, cudaStream_t st);
+
 static cudaError_t run_zinv(ZArgs z, cudaStream_t st)
 {
+    if (z.m >= ZW_MIN_COLUMNS) return run_zinv_wide(z, st);
     const int nblk = (z.n + ZR - 1) / ZR, ntile = (z.m + ZC - 1) / ZC;
     if ((size_t)nblk * ntile > (size_t)z.nflags) return cudaErrorInvalidValue;
     cudaError_t e = cudaMemsetAsync(z.flags, 0, (size_t)nblk * ntile * sizeof(int), st);
@@ -806,8 +811,259 @@ static cudaError_t run_zinv(ZArgs z, cudaStream_t st)
 
 // x <- D P L y: independent tasks (row block, 4 right-hand sides), no flags; the blocks of
 // the last rows (the most work) are handed out first.
+// ---- the same sweeps for many right-hand sides: tiles of 64 rows x 64 columns on the FP64
+// tensor pipe ----
+// zl_kernel re-reads each 64 x 64 tile of L once per four right-hand sides; with thousands of
+// them (config 5's 4096 complex vectors are 8192 real columns) that is hundreds of GB of L2
+// traffic per sweep.  Here a task owns 64 rows x 64 columns, so a tile of L serves 64
+// columns, and the products L_ij y_j run as mma.sync m8n8k4 FP64 (eight warps, each 32 rows x
+// 16 columns), with the L and y tiles staged by cp.async in K chunks of 32 (double buffered,
+// padded so that fragment loads hit 16 distinct 8-byte banks per half-warp).  The structure is
+// zl_kernel's: MUL = false is the blocked forward substitution over a cooperative grid with
+// ready flags per (row block, column tile), tasks block-major; the unit lower diagonal block is
+// then solved one column per lane group (plain form: substitution with shuffles) or multiplied
+// by its precomputed inverse (mixed form); MUL = true has no dependencies.
+constexpr int ZWR = 64;          // rows per block (the L blocks of zl_kernel)
+constexpr int ZWC = 64;          // columns per task
+constexpr int ZWK = 32;          // K chunk
+constexpr int ZWT = 256;
+constexpr int ZWAP = ZWR + 4, ZWBP = ZWC + 4;
+struct ZwSmem {
+    double A[2][ZWK][ZWAP];  // L tile [q][row]
+    double B[2][ZWK][ZWBP];  // y tile [q][column]
+    double D[ZWR][ZWC + 1];  // diagonal block: the block's values [row][column]
+    int ok;
+};
+
+template <bool MUL>
+__global__ void __launch_bounds__(ZWT, 2) zlw_kernel(ZArgs z)
+{
+    extern __shared__ __align__(16) unsigned char zw_raw[];
+    ZwSmem& sm = *reinterpret_cast<ZwSmem*>(zw_raw);
+    const int n = z.n, m = z.m;
+    const int t = threadIdx.x, lane = t & 31, warp = t >> 5;
+    const int wm = warp & 1, wn = warp >> 1;  // warp tile: rows 32 wm .., columns 16 wn ..
+    const int g = lane >> 2, t4 = lane & 3;
+    const int nblk = (n + ZWR - 1) / ZWR, ntile = (m + ZWC - 1) / ZWC;
+    const bool dinv = !MUL && z.linv != nullptr;
+    for (int task = blockIdx.x; task < nblk * ntile; task += gridDim.x) {
+        const int ib = task / ntile, c = task - ib * ntile;
+        const int i = MUL ? nblk - 1 - ib : ib;
+        if (tile_done(z.done, z.tol, c * ZWC, ZWC, m, z.cplx)) continue;
+        double acc[2][2][2];
+        // initial values: the gathered x (L^-1 sweep) or y itself (L sweep), at this thread's
+        // fragment positions (row 32 wm + 8 a + g, column 16 wn + 8 b + 2 t4 + e)
+#pragma unroll
+        for (int a = 0; a < 2; ++a)
+#pragma unroll
+            for (int b = 0; b < 2; ++b)
+#pragma unroll
+                for (int e = 0; e < 2; ++e) {
+                    const int row = i * ZWR + 32 * wm + 8 * a + g;
+                    const int col = c * ZWC + 16 * wn + 8 * b + 2 * t4 + e;
+                    double v = 0.0;
+                    if (row < n && col < m) {
+                        if (!MUL && z.gather && z.cplx) {
+                            const int64_t p = z.perm[row];
+                            v = z.src[2 * ((size_t)(col >> 1) * z.lds + (p - 1)) + (col & 1)] * z.iscale[p - 1];
+                        } else if (!MUL && z.gather) {
+                            const int64_t p = z.perm[row];
+                            v = z.src[(size_t)col * z.lds + (p - 1)] * z.iscale[p - 1];
+                        } else {
+                            v = z.src[(size_t)col * z.lds + row];
+                        }
+                    }
+                    acc[a][b][e] = v;
+                }
+        const double sgn = MUL ? 1.0 : -1.0;
+        const double* yb = MUL ? z.src : z.dst;  // L y reads the input; L^-1 y the solved blocks
+        const int ldy = MUL ? z.lds : z.ldd;
+        // products with the blocks j < i (L^-1 sweep) or j <= i (L sweep; L's diagonal is
+        // stored as zero and the unit part is the initial value above)
+        const int jend = MUL ? i : i - 1;
+        for (int j = 0; j <= jend; ++j) {
+            if (!MUL) {
+                if (t == 0) {
+                    int ok = 1;
+                    const int* f = z.flags + (size_t)j * ntile + c;
+                    const uint64_t t0 = globaltimer_ns();
+                    unsigned spins = 0;
+                    while (ld_acquire_i32(f) != 1) {
+                        if ((++spins & 63u) == 0) {
+                            if (ld_acquire_i32(z.err) != 0) { ok = 0; break; }
+                            if (globaltimer_ns() - t0 > z.limit_ns) {
+                                atomicCAS(z.err, 0, (int)LHL_ERR_TIMEOUT);
+                                ok = 0;
+                                break;
+                            }
+                        }
+                    }
+                    sm.ok = ok;
+                }
+                __syncthreads();
+                if (!sm.ok) return;
+            }
+            auto stage = [&](int h, int st) {  // K half h (columns 32 h .. of block j)
+                for (int e = t; e < ZWK * ZWR; e += ZWT) {
+                    const int rr = e % ZWR, qq = e / ZWR;
+                    const int gr = i * ZWR + rr, q = j * ZWR + h * ZWK + qq;
+                    // L[gr][q] = F[(q-1) ldf + gr] for 1 <= q <= n-2 and gr >= q+1, else 0
+                    const bool ok = gr < n && q >= 1 && q <= n - 2 && gr >= q + 1;
+                    cp_async8(&sm.A[st][qq][rr], ok ? &z.F[(size_t)(q - 1) * z.ldf + gr] : z.F, ok, z.F);
+                }
+                for (int e = t; e < ZWK * ZWC; e += ZWT) {
+                    const int qq = e % ZWK, cc = e / ZWK;
+                    const int q = j * ZWR + h * ZWK + qq, col = c * ZWC + cc;
+                    const bool ok = q < n && col < m;
+                    cp_async8(&sm.B[st][qq][cc], ok ? &yb[(size_t)col * ldy + q] : z.F, ok, z.F);
+                }
+                cp_async_commit();
+            };
+            stage(0, 0);
+            stage(1, 1);
+#pragma unroll
+            for (int h = 0; h < 2; ++h) {
+                if (h == 0) cp_async_wait<1>();
+                else cp_async_wait<0>();
+                __syncthreads();
+#pragma unroll
+                for (int kk = 0; kk < ZWK; kk += 4) {
+                    double fa[2], fb[2];
+#pragma unroll
+                    for (int a = 0; a < 2; ++a) fa[a] = sgn * sm.A[h][kk + t4][32 * wm + 8 * a + g];
+#pragma unroll
+                    for (int b = 0; b < 2; ++b) fb[b] = sm.B[h][kk + t4][16 * wn + 8 * b + g];
+#pragma unroll
+                    for (int a = 0; a < 2; ++a)
+#pragma unroll
+                        for (int b = 0; b < 2; ++b) dmma_8x8x4(acc[a][b], fa[a], fb[b]);
+                }
+            }
+            __syncthreads();  // both stages free for the next block
+        }
+        if constexpr (MUL) {  // x[perm[row]] = (L y)[row] * scale[perm[row]]
+#pragma unroll
+            for (int a = 0; a < 2; ++a)
+#pragma unroll
+                for (int b = 0; b < 2; ++b)
+#pragma unroll
+                    for (int e = 0; e < 2; ++e) {
+                        const int row = i * ZWR + 32 * wm + 8 * a + g;
+                        const int col = c * ZWC + 16 * wn + 8 * b + 2 * t4 + e;
+                        if (row < n && col < m) {
+                            const int64_t p = z.perm[row];
+                            if (z.cplx)
+                                z.dst[2 * ((size_t)(col >> 1) * z.ldd + (p - 1)) + (col & 1)] = acc[a][b][e] * z.scale[p - 1];
+                            else
+                                z.dst[(size_t)col * z.ldd + (p - 1)] = acc[a][b][e] * z.scale[p - 1];
+                        }
+                    }
+        } else {
+        // ---- the diagonal block: unit lower L_ii, values of this block in sm.D ----
+#pragma unroll
+        for (int a = 0; a < 2; ++a)
+#pragma unroll
+            for (int b = 0; b < 2; ++b)
+#pragma unroll
+                for (int e = 0; e < 2; ++e) sm.D[32 * wm + 8 * a + g][16 * wn + 8 * b + 2 * t4 + e] = acc[a][b][e];
+        // L_ii (strictly lower part, or its inverse) into sm.A as [row][q] pairs of halves
+        double* Lii = &sm.A[0][0][0];  // 64 x 65 doubles, row-major, fits in the two A stages
+        for (int e = t; e < ZWR * ZWR; e += ZWT) {
+            const int rr = e % ZWR, qq = e / ZWR;
+            const int gr = i * ZWR + rr, q = i * ZWR + qq;
+            double v;
+            if (dinv) v = z.linv[((size_t)i * ZWR + rr) * ZWR + qq];  // (L_ii)^-1, row-major
+            else v = (gr < n && q >= 1 && q <= n - 2 && gr >= q + 1) ? z.F[(size_t)(q - 1) * z.ldf + gr] : 0.0;
+            Lii[rr * (ZWR + 1) + qq] = v;
+        }
+        __syncthreads();
+        if (dinv) {
+            // y_i = (L_ii)^-1 D: one column per thread quarter, 64-term dot products
+            for (int e = t; e < ZWR * ZWC; e += ZWT) {
+                const int rr = e % ZWR, cc = e / ZWR;
+                double s0 = 0.0, s1 = 0.0;
+#pragma unroll 8
+                for (int q = 0; q < ZWR; q += 2) {
+                    s0 = dfma(Lii[rr * (ZWR + 1) + q], sm.D[q][cc], s0);
+                    s1 = dfma(Lii[rr * (ZWR + 1) + q + 1], sm.D[q + 1][cc], s1);
+                }
+                const int row = i * ZWR + rr, col = c * ZWC + cc;
+                if (row < n && col < m) z.dst[(size_t)col * z.ldd + row] = s0 + s1;
+            }
+        } else {
+            // forward substitution: warp w solves columns 8w .. 8w+7; lane holds rows lane, lane+32
+            double y0[8], y1[8];
+#pragma unroll
+            for (int v = 0; v < 8; ++v) {
+                y0[v] = sm.D[lane][8 * warp + v];
+                y1[v] = sm.D[lane + 32][8 * warp + v];
+            }
+            for (int q = 0; q < ZWR - 1; ++q) {
+                const double l0 = Lii[lane * (ZWR + 1) + q], l1 = Lii[(lane + 32) * (ZWR + 1) + q];
+#pragma unroll
+                for (int v = 0; v < 8; ++v) {
+                    const double xq = __shfl_sync(0xffffffffu, q < 32 ? y0[v] : y1[v], q & 31);
+                    if (lane > q) y0[v] = dfma(-l0, xq, y0[v]);
+                    if (lane + 32 > q) y1[v] = dfma(-l1, xq, y1[v]);
+                }
+            }
+#pragma unroll
+            for (int v = 0; v < 8; ++v) {
+                const int col = c * ZWC + 8 * warp + v;
+                if (col < m) {
+                    double* d = z.dst + (size_t)col * z.ldd;
+                    if (i * ZWR + lane < n) d[i * ZWR + lane] = y0[v];
+                    if (i * ZWR + lane + 32 < n) d[i * ZWR + lane + 32] = y1[v];
+                }
+            }
+        }
+        __syncthreads();
+        if (t == 0) {
+            __threadfence();
+            asm volatile("st.release.gpu.global.s32 [%0], %1;" ::"l"(z.flags + (size_t)i * ntile + c), "r"(1)
+                         : "memory");
+        }
+        }
+    }
+}
+
+static cudaError_t run_zinv_wide(ZArgs z, cudaStream_t st)
+{
+    const int nblk = (z.n + ZWR - 1) / ZWR, ntile = (z.m + ZWC - 1) / ZWC;
+    if ((size_t)nblk * ntile > (size_t)z.nflags) return cudaErrorInvalidValue;
+    cudaError_t e = cudaMemsetAsync(z.flags, 0, (size_t)nblk * ntile * sizeof(int), st);
+    if (e != cudaSuccess) return e;
+    const size_t smem = sizeof(ZwSmem);
+    static int maxgrid = 0;
+    if (maxgrid == 0) {
+        e = cudaFuncSetAttribute(zlw_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        if (e != cudaSuccess) return e;
+        int dev = 0, sms = 0, per = 0;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, zlw_kernel<false>, ZWT, smem);
+        maxgrid = sms * (per > 0 ? per : 1);
+    }
+    const int grid = min(nblk * ntile, maxgrid);
+    void* args[] = {&z};
+    return cudaLaunchCooperativeKernel((void*)zlw_kernel<false>, dim3(grid), dim3(ZWT), args, smem, st);
+}
+
 static cudaError_t run_zmul(const ZArgs& z, cudaStream_t st)
 {
+    if (z.m >= ZW_MIN_COLUMNS) {
+        const size_t smem = sizeof(ZwSmem);
+        static bool attr = false;
+        if (!attr) {
+            cudaError_t e = cudaFuncSetAttribute(zlw_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                                 (int)smem);
+            if (e != cudaSuccess) return e;
+            attr = true;
+        }
+        const int nblk = (z.n + ZWR - 1) / ZWR, ntile = (z.m + ZWC - 1) / ZWC;
+        zlw_kernel<true><<<nblk * ntile, ZWT, smem, st>>>(z);
+        return cudaGetLastError();
+    }
     const int nblk = (z.n + ZR - 1) / ZR, ntile = (z.m + ZC - 1) / ZC;
     zl_kernel<true><<<nblk * ntile, ZIT, 0, st>>>(z);
     return cudaGetLastError();

@@ -142,6 +142,59 @@ def test_complex_multi_rhs_solve_matches_one_vector_solves(n, rps, ncols):
         assert O.bwd(W, Xh[:, c], B[:, c]) <= 4 * O.bwd(W, x1, B[:, c]) + 50 * eps, (n, rps, c)
 
 
+@pytest.mark.parametrize("n,S,rps,precision", [(3, 20, 32, "fp64"), (65, 17, 32, "fp64"), (200, 9, 64, "mixed"),
+                                                (1030, 16, 32, "fp64"), (1030, 16, 32, "mixed")])
+def test_complex_wide_sweeps_match_one_vector_solves(n, S, rps, precision):
+    """From 1024 real columns (512 complex right-hand sides) on, the L sweeps of the solve run as
+    64-column tensor-pipe tiles (FP64 MMAs; the mixed form's diagonal blocks by their inverses).
+    Sampled columns agree with one-vector solves of the same shift to 1e-10, edges of the
+    64-row and 64-column tiles included."""
+    torch, G = _mods()
+    J = rng(70 + n).standard_normal((n, n)) / np.sqrt(n)
+    prec = G.LHL_PREC_MIXED if precision == "mixed" else G.LHL_PREC_FP64
+    ws = G.lhl(dev(J), precision=prec, shift_complex=True)
+    ws.check()
+    g = rng(71)
+    sig = g.uniform(-2.0, 0.0, S) + 1j * g.uniform(0.0, 10.0, S)
+    tau = -np.ones(S, dtype=complex)
+    sh = G.LHLShift(n, S, complex=True)
+    G.lhl_shift_batched_(sh, ws, dev(sig), dev(tau))
+    ncols = S * rps - 3  # a partial last shift and column tile
+    assert 2 * ncols >= 1024
+    B = rng(72).standard_normal((n, ncols)) + 1j * rng(73).standard_normal((n, ncols))
+    X = dev(B)
+    G.lhl_ldiv_(X, sh, ws, rhs_per_shift=rps)
+    Xh = host(X)
+    for c in sorted({0, 1, 31, 32, 63, ncols // 2, ncols - 1}):
+        G.lhl_shift_(ws, sig[c // rps], tau[c // rps])
+        x1 = host(G.lhl_ldiv_(dev(np.ascontiguousarray(B[:, c])), ws))
+        assert np.linalg.norm(Xh[:, c] - x1) <= 1e-10 * np.linalg.norm(x1), (n, c)
+
+
+@pytest.mark.parametrize("n,nrhs,rps", [(1, 16, 4), (37, 16, 1), (200, 45, 5), (1030, 64, 32)])
+def test_complex_residual_many_rhs(n, nrhs, rps):
+    """From 16 complex right-hand sides on, the residual r = b - (sigma x + tau J x) runs as a
+    tensor-pipe GEMM (FP64 MMAs); its norms agree with numpy's to 1e-12 relative, with edges of
+    the 128-row and 32-column tiles and a partial last shift."""
+    torch, G = _mods()
+    J = rng(60 + n).standard_normal((n, n))
+    ws = G.lhl(dev(J), shift_complex=True)
+    S = (nrhs + rps - 1) // rps
+    g = rng(61)
+    sig = g.uniform(-2.0, 0.0, S) + 1j * g.uniform(0.0, 10.0, S)
+    tau = g.uniform(-1.0, 1.0, S) + 1j * g.uniform(-1.0, 1.0, S)
+    sh = G.LHLShift(n, S, complex=True)
+    G.lhl_shift_batched_(sh, ws, dev(sig), dev(tau))
+    B = rng(62).standard_normal((n, nrhs)) + 1j * rng(63).standard_normal((n, nrhs))
+    X = rng(64).standard_normal((n, nrhs)) + 1j * rng(65).standard_normal((n, nrhs))
+    got = host(G.residual_norms(sh, dev(J), dev(B), dev(X), rhs_per_shift=rps))
+    for c in range(nrhs):
+        s = c // rps
+        r = B[:, c] - (sig[s] * X[:, c] + tau[s] * (J @ X[:, c]))
+        want = np.linalg.norm(r) / np.linalg.norm(B[:, c])
+        assert abs(got[c] - want) <= 1e-12 * want, (n, c, got[c], want)
+
+
 @pytest.mark.parametrize("precision", ["fp64", "mixed"])
 def test_resolvent_sweep_reaches_1e10(precision):
     """Config 5's shape at n = 1024: J ~ N(0,1)/sqrt(n), complex shifts s = a + ib with a in
