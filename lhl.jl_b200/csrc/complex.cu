@@ -306,24 +306,30 @@ cudaError_t launch_hess_cplx(int n, const double* Gt, int ldg, int po, const uin
 //   1. the forward select-swap recurrence (F:2827-2838), one thread per right-hand side, on
 //      chunks of 32 steps staged in shared memory by the whole CTA;
 //   2. the back substitution in blocks of 32 rows from the bottom, left-looking: for block b
-//      the products U[b, j] x[j] over the solved rows j below it are a small complex GEMM
-//      (32 rows x MG right-hand sides x K), K in chunks of 64 staged by cp.async (double
-//      buffered), each thread a 4 x 4 complex register tile over one of 16 interleaved K
-//      slices, the slices summed by half-warp shuffles; then one warp per right-hand side
-//      solves the 32 x 32 triangle with rdiag (shuffles, as the one-vector kernel does).
+//      the products U[b, j] x[j] over the solved rows j below it form a real GEMM
+//          [Re S  Im S] (32 x 2 MG) = [Re U  Im U] (32 x 2K) [[Re X, Im X]; [-Im X, Re X]]
+//      run as mma.sync m8n8k4 FP64 tiles: K in chunks of 64 staged by cp.async (double
+//      buffered, pitches chosen so that fragment loads hit 16 distinct 8-byte banks per
+//      half-warp), each warp a share of the chunk's k-steps over the whole 32 x 16 output,
+//      the eight warps' sums added in a fixed order; then one warp per right-hand side solves
+//      the 32 x 32 triangle with rdiag (shuffles, as the one-vector kernel does).
 // Results agree with the one-vector kernel to rounding (the summation order differs).
 constexpr int MG = 8;        // complex right-hand sides per CTA
 constexpr int MT = 256;      // threads
 constexpr int MRB = 32;      // rows per back-substitution block
 constexpr int MKC = 64;      // K chunk
-constexpr int MUP = MKC + 1; // padded row pitch of the staged U tile
-constexpr int MXP = MG + 1;  // padded pitch of the staged x tile
+constexpr int MUP = MKC + 4; // row pitch of the staged U tile (= 4 mod 16 doubles)
+constexpr int MXP = 12;      // pitch of the staged x tile (= 12 mod 16 doubles)
 constexpr int MFC = 32;      // forward-recurrence chunk (steps)
+constexpr int MW8 = MT / 32; // warps
 struct MrhsSmem {
-    double U[2][2][MRB][MUP];    // [stage][plane][row][k]
+    union {  // used in turn: the K chunks, then the warps' sums, then the diagonal block
+        double U[2][2][MRB][MUP];          // [stage][plane][row][k]
+        double red[MW8][MRB][2 * MG + 1];  // the warps' block sums [warp][row][part * MG + rhs]
+        double T[2][MRB][MRB + 1];         // diagonal block U_bb: [plane][row][col]
+    };
     double X[2][2][MKC][MXP];    // [stage][part][k][rhs]
-    double T[2][MRB][MRB + 1];   // diagonal block U_bb: [plane][row][col]
-    double D[2][MRB][MXP];       // block sums: [part][row][rhs]
+    double D[2][MRB][MG + 1];    // block sums: [part][row][rhs]
     double F[2][MFC + 1][MG];    // forward recurrence: y chunk [part][step][rhs]
     double FL[2][MFC];           // forward recurrence: multipliers l_k [part][step]
     unsigned char FS[MFC];       // forward recurrence: swaps
@@ -401,22 +407,17 @@ __global__ void __launch_bounds__(MT, 2) hess_cplx_mrhs_kernel(int n, const doub
     }
 
     // ---- 2. back substitution
-    const int q = t & 15;           // K slice: k = q + 16 u of each chunk
-    const int rg = (t >> 4) & 7;    // rows rg + 8 i of the block
-    const int gg = t >> 7;          // right-hand sides 4 gg + v
+    const int g8 = lane >> 2, t4 = lane & 3;  // mma fragment coordinates
     for (int r1 = n; r1 >= 1; r1 -= MRB) {
         const int r0 = max(r1 - MRB + 1, 1);
         const int bs = r1 - r0 + 1;
-        // diagonal block U[r0 + a, r0 + b] = Gt[r0 + b, r0 + a] (b >= a), both planes
-        for (int e = t; e < 2 * MRB * MRB; e += MT) {
-            const int bb = e % MRB, a = (e / MRB) % MRB, p = e / (MRB * MRB);
-            sm.T[p][a][bb] = (a < bs && bb < bs && bb >= a) ? M1(Gt, ldg, p * po + r0 + bb, r0 + a) : 0.0;
-        }
-        double ar[4][4], ai[4][4];
+        // acc[a][b]: rows 8 a + g8 of the block; b = 0: real parts, b = 1: imaginary parts of
+        // right-hand sides 2 t4, 2 t4 + 1
+        double acc[4][2][2];
 #pragma unroll
-        for (int i = 0; i < 4; ++i)
+        for (int a = 0; a < 4; ++a)
 #pragma unroll
-            for (int v = 0; v < 4; ++v) ar[i][v] = ai[i][v] = 0.0;
+            for (int b = 0; b < 2; ++b) acc[a][b][0] = acc[a][b][1] = 0.0;
         const int K = n - r1;  // solved rows r1+1 .. n
         const int nch = (K + MKC - 1) / MKC;
         auto stage = [&](int ch, int st) {
@@ -445,51 +446,47 @@ __global__ void __launch_bounds__(MT, 2) hess_cplx_mrhs_kernel(int n, const doub
                 cp_async_wait<0>();
             }
             __syncthreads();
+            // this warp's k-steps of the chunk: kk = 4 (warp + 8 u), u = 0, 1, in both planes
 #pragma unroll
-            for (int u = 0; u < MKC / 16; ++u) {
-                const int kk = q + 16 * u;
-                double ur[4], ui[4], xr[4], xi[4];
+            for (int u = 0; u < MKC / (4 * MW8); ++u) {
+                const int kk = 4 * (warp + MW8 * u) + t4;
+                const double xr = sm.X[st][0][kk][g8], xi = sm.X[st][1][kk][g8];
+                double far[4], fai[4];
 #pragma unroll
-                for (int i = 0; i < 4; ++i) {
-                    ur[i] = sm.U[st][0][rg + 8 * i][kk];
-                    ui[i] = sm.U[st][1][rg + 8 * i][kk];
+                for (int a = 0; a < 4; ++a) {
+                    far[a] = sm.U[st][0][8 * a + g8][kk];
+                    fai[a] = sm.U[st][1][8 * a + g8][kk];
                 }
 #pragma unroll
-                for (int v = 0; v < 4; ++v) {
-                    xr[v] = sm.X[st][0][kk][4 * gg + v];
-                    xi[v] = sm.X[st][1][kk][4 * gg + v];
+                for (int a = 0; a < 4; ++a) {
+                    dmma_8x8x4(acc[a][0], far[a], xr);   // Re U Re x
+                    dmma_8x8x4(acc[a][1], far[a], xi);   // Re U Im x
+                    dmma_8x8x4(acc[a][0], fai[a], -xi);  // - Im U Im x
+                    dmma_8x8x4(acc[a][1], fai[a], xr);   // Im U Re x
                 }
-#pragma unroll
-                for (int i = 0; i < 4; ++i)
-#pragma unroll
-                    for (int v = 0; v < 4; ++v) {
-                        ar[i][v] = fma(ur[i], xr[v], ar[i][v]);
-                        ar[i][v] = fma(-ui[i], xi[v], ar[i][v]);
-                        ai[i][v] = fma(ur[i], xi[v], ai[i][v]);
-                        ai[i][v] = fma(ui[i], xr[v], ai[i][v]);
-                    }
             }
             __syncthreads();  // the stage this chunk used is refilled two chunks on
         }
-        // sum the 16 K slices (lanes q of a half-warp)
+        // the eight warps' sums, added in a fixed order (the U stages are free now)
 #pragma unroll
-        for (int i = 0; i < 4; ++i)
+        for (int a = 0; a < 4; ++a)
 #pragma unroll
-            for (int v = 0; v < 4; ++v) {
+            for (int b = 0; b < 2; ++b)
 #pragma unroll
-                for (int o = 8; o >= 1; o >>= 1) {
-                    ar[i][v] += __shfl_xor_sync(0xffffffffu, ar[i][v], o);
-                    ai[i][v] += __shfl_xor_sync(0xffffffffu, ai[i][v], o);
-                }
-            }
-        if (q == 0) {
+                for (int e = 0; e < 2; ++e) sm.red[warp][8 * a + g8][b * MG + 2 * t4 + e] = acc[a][b][e];
+        __syncthreads();
+        for (int e = t; e < MRB * 2 * MG; e += MT) {
+            const int row = e % MRB, col = e / MRB;  // col = part * MG + rhs
+            double sum = 0.0;
 #pragma unroll
-            for (int i = 0; i < 4; ++i)
-#pragma unroll
-                for (int v = 0; v < 4; ++v) {
-                    sm.D[0][rg + 8 * i][4 * gg + v] = ar[i][v];
-                    sm.D[1][rg + 8 * i][4 * gg + v] = ai[i][v];
-                }
+            for (int w = 0; w < MW8; ++w) sum += sm.red[w][row][col];
+            sm.D[col / MG][row][col % MG] = sum;
+        }
+        __syncthreads();
+        // diagonal block U[r0 + a, r0 + b] = Gt[r0 + b, r0 + a] (b >= a), both planes
+        for (int e = t; e < 2 * MRB * MRB; e += MT) {
+            const int bb = e % MRB, a = (e / MRB) % MRB, p = e / (MRB * MRB);
+            sm.T[p][a][bb] = (a < bs && bb < bs && bb >= a) ? M1(Gt, ldg, p * po + r0 + bb, r0 + a) : 0.0;
         }
         __syncthreads();
         // triangle: warp v solves right-hand side v

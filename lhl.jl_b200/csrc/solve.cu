@@ -817,7 +817,7 @@ static cudaError_t run_zinv(ZArgs z, cudaStream_t st)
 // them (config 5's 4096 complex vectors are 8192 real columns) that is hundreds of GB of L2
 // traffic per sweep.  Here a task owns 64 rows x 64 columns, so a tile of L serves 64
 // columns, and the products L_ij y_j run as mma.sync m8n8k4 FP64 (eight warps, each 32 rows x
-// 16 columns), with the L and y tiles staged by cp.async in K chunks of 32 (double buffered,
+// 16 columns: 4 x 2 tiles of 8 x 8), with the L and y tiles staged by cp.async in K chunks of 32 (double buffered,
 // padded so that fragment loads hit 16 distinct 8-byte banks per half-warp).  The structure is
 // zl_kernel's: MUL = false is the blocked forward substitution over a cooperative grid with
 // ready flags per (row block, column tile), tasks block-major; the unit lower diagonal block is
@@ -850,11 +850,11 @@ __global__ void __launch_bounds__(ZWT, 2) zlw_kernel(ZArgs z)
         const int ib = task / ntile, c = task - ib * ntile;
         const int i = MUL ? nblk - 1 - ib : ib;
         if (tile_done(z.done, z.tol, c * ZWC, ZWC, m, z.cplx)) continue;
-        double acc[2][2][2];
+        double acc[4][2][2];
         // initial values: the gathered x (L^-1 sweep) or y itself (L sweep), at this thread's
         // fragment positions (row 32 wm + 8 a + g, column 16 wn + 8 b + 2 t4 + e)
 #pragma unroll
-        for (int a = 0; a < 2; ++a)
+        for (int a = 0; a < 4; ++a)
 #pragma unroll
             for (int b = 0; b < 2; ++b)
 #pragma unroll
@@ -928,13 +928,13 @@ __global__ void __launch_bounds__(ZWT, 2) zlw_kernel(ZArgs z)
                 __syncthreads();
 #pragma unroll
                 for (int kk = 0; kk < ZWK; kk += 4) {
-                    double fa[2], fb[2];
+                    double fa[4], fb[2];
 #pragma unroll
-                    for (int a = 0; a < 2; ++a) fa[a] = sgn * sm.A[h][kk + t4][32 * wm + 8 * a + g];
+                    for (int a = 0; a < 4; ++a) fa[a] = sgn * sm.A[h][kk + t4][32 * wm + 8 * a + g];
 #pragma unroll
                     for (int b = 0; b < 2; ++b) fb[b] = sm.B[h][kk + t4][16 * wn + 8 * b + g];
 #pragma unroll
-                    for (int a = 0; a < 2; ++a)
+                    for (int a = 0; a < 4; ++a)
 #pragma unroll
                         for (int b = 0; b < 2; ++b) dmma_8x8x4(acc[a][b], fa[a], fb[b]);
                 }
@@ -943,7 +943,7 @@ __global__ void __launch_bounds__(ZWT, 2) zlw_kernel(ZArgs z)
         }
         if constexpr (MUL) {  // x[perm[row]] = (L y)[row] * scale[perm[row]]
 #pragma unroll
-            for (int a = 0; a < 2; ++a)
+            for (int a = 0; a < 4; ++a)
 #pragma unroll
                 for (int b = 0; b < 2; ++b)
 #pragma unroll
@@ -961,7 +961,7 @@ __global__ void __launch_bounds__(ZWT, 2) zlw_kernel(ZArgs z)
         } else {
         // ---- the diagonal block: unit lower L_ii, values of this block in sm.D ----
 #pragma unroll
-        for (int a = 0; a < 2; ++a)
+        for (int a = 0; a < 4; ++a)
 #pragma unroll
             for (int b = 0; b < 2; ++b)
 #pragma unroll
