@@ -140,7 +140,7 @@ int lhl_ws_create(int64_t n, int precision, lhl_ws_t* out)
         const size_t ldr = (size_t)w->mplan.ldr, g = (size_t)w->mplan.grid;
         A_(mhdr, 2 * g);
         A_(mcval, 2 * (size_t)n);
-        A_(mcrow, 2 * g * ldr);
+        A_(mcrow, (size_t)(w->mplan.smem_rows ? 2 : lhl::MIX_LAZY_RING) * g * ldr);
         A_(mgrows, w->mplan.smem_rows ? 1 : (size_t)n * ldr);
         A_(linv, (size_t)((n + 63) / 64) * 64 * 64);
     }
@@ -391,9 +391,10 @@ static int reduce_loaded(lhl_ws_t ws, int balance, cudaStream_t st)
         if (e == cudaSuccess)
             e = cudaMemsetAsync(ws->mhdr, 0, 2 * (size_t)ws->mplan.grid * sizeof(unsigned long long), st);
         if (e == cudaSuccess) e = cudaMemsetAsync(ws->mcval, 0, 2 * (size_t)n * sizeof(unsigned long long), st);
+        const size_t ring = ws->mplan.smem_rows ? 2 : lhl::MIX_LAZY_RING;
         if (e == cudaSuccess)
             e = cudaMemsetAsync(ws->mcrow, 0,
-                                2 * (size_t)ws->mplan.grid * ws->mplan.ldr * sizeof(unsigned long long), st);
+                                ring * (size_t)ws->mplan.grid * ws->mplan.ldr * sizeof(unsigned long long), st);
         if (e == cudaSuccess) e = lhl::launch_reduce(a, balance ? 1 : 0, 0, st);
         if (e != cudaSuccess) return LHL_ERR_CUDA;
         lhl::MixArgs m;
@@ -410,7 +411,9 @@ static int reduce_loaded(lhl_ws_t ws, int balance, cudaStream_t st)
         m.err = ws->err;
         m.limit_ns = ws->limit_ns;
         m.ptimes = ws->probes ? ws->ptimes : nullptr;
-        e = lhl::launch_reduce_mixed(m, ws->mplan, st);  // writes perm / iperm too
+        // rows on chip: the eager kernel; rows in global memory: the panel-delayed one
+        e = ws->mplan.smem_rows ? lhl::launch_reduce_mixed(m, ws->mplan, st)
+                                : lhl::launch_reduce_mixed_lazy(m, ws->mplan, st);  // writes perm / iperm too
         if (e == cudaSuccess) e = lhl::launch_linv((int)n, ws->F, (int)n, ws->linv, st);
         if (e != cudaSuccess) return LHL_ERR_CUDA;
         return cuda_status(lhl::launch_ht_fill((int)n, ws->F, ws->Ht, st));

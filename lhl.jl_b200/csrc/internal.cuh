@@ -137,6 +137,10 @@ struct MixPlan {
 constexpr size_t MIX_SMEM_MAX = 227 * 1024 - 4096;  // dynamic part; the kernel's static shared arrays use 2.4 KB
 void mixed_plan(int n, int sms, MixPlan* pl);
 cudaError_t launch_reduce_mixed(MixArgs a, const MixPlan& pl, cudaStream_t st);
+// Rows in global memory (pl.smem_rows == 0): the panel-delayed form (reduce_lazy.cu), whose
+// candidate rows need MIX_LAZY_RING slots of grid x ldr exchange words instead of 2.
+constexpr int MIX_LAZY_RING = 18;
+cudaError_t launch_reduce_mixed_lazy(MixArgs a, const MixPlan& pl, cudaStream_t st);
 
 cudaError_t launch_reduce(RedArgs a, int balance, int mode, cudaStream_t st);
 cudaError_t launch_unblocked_assemble(int n, double* A, const double* B2, const int64_t* ipiv, cudaStream_t st);

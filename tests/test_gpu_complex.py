@@ -191,7 +191,7 @@ def test_complex_many_rhs_chain_is_deterministic():
         G.lhl_ldiv_(X, sh, ws, rhs_per_shift=rps)
         res = G.lhl_refine_tol_(X, Jd, Bd, sh, ws, tol=0.0, max_steps=2, rhs_per_shift=rps)
         out.append((host(X), host(res)))
-    assert np.array_equal(out[0][0].view(np.float64), out[1][0].view(np.float64))
+    assert np.array_equal(np.ascontiguousarray(out[0][0]).view(np.uint64), np.ascontiguousarray(out[1][0]).view(np.uint64))
     assert np.array_equal(out[0][1], out[1][1])
     assert (out[0][1] <= 1e-12).all()
 
