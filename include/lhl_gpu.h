@@ -88,6 +88,12 @@ int lhl_ws_probe_ns(lhl_ws_t ws, uint64_t* out16, void* stream);
  * lhl_ws_phase_ns and lhl_ws_probe_ns read (off by default: the timer reads and their
  * accumulation lengthen CTA 0's per-step path; with them off both read zeros). */
 int lhl_ws_set_probes(lhl_ws_t ws, int on);
+/* Test hook for the mixed form (LHL_PREC_MIXED): which FP32 reduction kernel later reductions
+ * use.  0 (default): by the order -- rows held on chip while they fit (the eager kernel, rank-1
+ * row updates every step), else the panel-delayed kernel (rows in global memory, rank-16 row
+ * updates once per panel); 1: the eager kernel at every order; 2: the panel-delayed kernel at
+ * every order.  Both give a similarity J = Z H Z^-1 to FP32 accuracy; their roundings differ. */
+int lhl_ws_set_mixed_kernel(lhl_ws_t ws, int which);
 /* Test hook: the wall-time limit of every grid-barrier wait of this workspace's kernels. */
 int lhl_ws_set_barrier_limit_ns(lhl_ws_t ws, uint64_t limit_ns);
 

@@ -34,6 +34,7 @@ struct lhl_ws_s {
     double* f32x;  // lhl_ldiv_f32: widened right-hand sides (grow-only)
     size_t f32x_cap;
     int cj;        // LHLWorkspace{ComplexF64}: F, Ht, buf2 interleaved complex (cplxj.cu)
+    int mix_kernel;  // mixed form: 0 by the plan (rows on chip: eager, else panel-delayed), 1 eager, 2 panel-delayed
 };
 
 struct lhl_shift_s {
@@ -140,8 +141,10 @@ int lhl_ws_create(int64_t n, int precision, lhl_ws_t* out)
         const size_t ldr = (size_t)w->mplan.ldr, g = (size_t)w->mplan.grid;
         A_(mhdr, 2 * g);
         A_(mcval, 2 * (size_t)n);
-        A_(mcrow, (size_t)(w->mplan.smem_rows ? 2 : lhl::MIX_LAZY_RING) * g * ldr);
-        A_(mgrows, w->mplan.smem_rows ? 1 : (size_t)n * ldr);
+        // the panel-delayed kernel's ring of candidate rows and global rows are allocated at every
+        // order (a test hook can select that kernel where rows would fit on chip)
+        A_(mcrow, (size_t)lhl::MIX_LAZY_RING * g * ldr);
+        A_(mgrows, (size_t)n * ldr);
         A_(linv, (size_t)((n + 63) / 64) * 64 * 64);
     }
 #undef A_
@@ -264,6 +267,14 @@ int lhl_ws_probe_ns(lhl_ws_t ws, uint64_t* out16, void* stream)
     cudaError_t e = cudaStreamSynchronize((cudaStream_t)stream);
     if (e == cudaSuccess) e = cudaMemcpy(out16, ws->ptimes + 8, 16 * sizeof(uint64_t), cudaMemcpyDeviceToHost);
     return cuda_status(e);
+}
+
+int lhl_ws_set_mixed_kernel(lhl_ws_t ws, int which)
+{
+    if (!ws) return LHL_ERR_ARG;
+    if (which < 0 || which > 2) return LHL_ERR_ARG;
+    ws->mix_kernel = which;
+    return LHL_OK;
 }
 
 int lhl_ws_set_probes(lhl_ws_t ws, int on)
@@ -391,7 +402,8 @@ static int reduce_loaded(lhl_ws_t ws, int balance, cudaStream_t st)
         if (e == cudaSuccess)
             e = cudaMemsetAsync(ws->mhdr, 0, 2 * (size_t)ws->mplan.grid * sizeof(unsigned long long), st);
         if (e == cudaSuccess) e = cudaMemsetAsync(ws->mcval, 0, 2 * (size_t)n * sizeof(unsigned long long), st);
-        const size_t ring = ws->mplan.smem_rows ? 2 : lhl::MIX_LAZY_RING;
+        const bool lazy = ws->mix_kernel == 2 || (ws->mix_kernel == 0 && !ws->mplan.smem_rows);
+        const size_t ring = lazy ? lhl::MIX_LAZY_RING : 2;
         if (e == cudaSuccess)
             e = cudaMemsetAsync(ws->mcrow, 0,
                                 ring * (size_t)ws->mplan.grid * ws->mplan.ldr * sizeof(unsigned long long), st);
@@ -412,8 +424,13 @@ static int reduce_loaded(lhl_ws_t ws, int balance, cudaStream_t st)
         m.limit_ns = ws->limit_ns;
         m.ptimes = ws->probes ? ws->ptimes : nullptr;
         // rows on chip: the eager kernel; rows in global memory: the panel-delayed one
-        e = ws->mplan.smem_rows ? lhl::launch_reduce_mixed(m, ws->mplan, st)
-                                : lhl::launch_reduce_mixed_lazy(m, ws->mplan, st);  // writes perm / iperm too
+        if (lazy) {
+            lhl::MixPlan pl = ws->mplan;
+            pl.smem_rows = 0;
+            e = lhl::launch_reduce_mixed_lazy(m, pl, st);  // writes perm / iperm too
+        } else {
+            e = lhl::launch_reduce_mixed(m, ws->mplan, st);  // rows on chip where they fit
+        }
         if (e == cudaSuccess) e = lhl::launch_linv((int)n, ws->F, (int)n, ws->linv, st);
         if (e != cudaSuccess) return LHL_ERR_CUDA;
         return cuda_status(lhl::launch_ht_fill((int)n, ws->F, ws->Ht, st));

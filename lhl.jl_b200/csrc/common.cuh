@@ -51,6 +51,15 @@ __device__ __forceinline__ void cp_async8(double* dst, const double* src, bool v
     asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;" ::"r"(d), "l"(valid ? src : base), "r"(sz)
                  : "memory");
 }
+// 16-byte asynchronous copy global -> shared, L2 only (.cg): both addresses 16-byte aligned;
+// `bytes` (0, 8 or 16) are read and the rest of the 16 zero-filled; a copy reading nothing is
+// given `base`, a valid address, as its source
+__device__ __forceinline__ void cp_async16(double* dst, const double* src, int bytes, const double* base)
+{
+    const unsigned d = (unsigned)__cvta_generic_to_shared(dst);
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;" ::"r"(d), "l"(bytes > 0 ? src : base), "r"(bytes)
+                 : "memory");
+}
 __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
 template <int N> __device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory"); }
 

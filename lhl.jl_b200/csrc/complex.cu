@@ -319,7 +319,7 @@ constexpr int MT = 256;      // threads
 constexpr int MRB = 32;      // rows per back-substitution block
 constexpr int MKC = 64;      // K chunk
 constexpr int MUP = MKC + 4; // row pitch of the staged U tile (= 4 mod 16 doubles)
-constexpr int MXP = 12;      // pitch of the staged x tile (= 12 mod 16 doubles)
+constexpr int MXP = MKC + 4; // pitch of the staged x tile (= 4 mod 16 doubles)
 constexpr int MFC = 32;      // forward-recurrence chunk (steps)
 constexpr int MW8 = MT / 32; // warps
 struct MrhsSmem {
@@ -328,7 +328,7 @@ struct MrhsSmem {
         double red[MW8][MRB][2 * MG + 1];  // the warps' block sums [warp][row][part * MG + rhs]
         double T[2][MRB][MRB + 1];         // diagonal block U_bb: [plane][row][col]
     };
-    double X[2][2][MKC][MXP];    // [stage][part][k][rhs]
+    double X[2][2][MG][MXP];     // [stage][part][rhs][k]
     double D[2][MRB][MG + 1];    // block sums: [part][row][rhs]
     double F[2][MFC + 1][MG];    // forward recurrence: y chunk [part][step][rhs]
     double FL[2][MFC];           // forward recurrence: multipliers l_k [part][step]
@@ -408,6 +408,8 @@ __global__ void __launch_bounds__(MT, 2) hess_cplx_mrhs_kernel(int n, const doub
 
     // ---- 2. back substitution
     const int g8 = lane >> 2, t4 = lane & 3;  // mma fragment coordinates
+    const bool vec16 = (n % 2) == 0 && ((ldg | po | ldy) % 2) == 0 &&
+                       (reinterpret_cast<uintptr_t>(Gt_all) % 16) == 0 && (reinterpret_cast<uintptr_t>(Y) % 16) == 0;
     for (int r1 = n; r1 >= 1; r1 -= MRB) {
         const int r0 = max(r1 - MRB + 1, 1);
         const int bs = r1 - r0 + 1;
@@ -420,19 +422,36 @@ __global__ void __launch_bounds__(MT, 2) hess_cplx_mrhs_kernel(int n, const doub
             for (int b = 0; b < 2; ++b) acc[a][b][0] = acc[a][b][1] = 0.0;
         const int K = n - r1;  // solved rows r1+1 .. n
         const int nch = (K + MKC - 1) / MKC;
+        // even n: every row of a chunk starts on an odd index (1-based), so the pairs (j, j+1)
+        // are 16-byte aligned in Gt (ldg and po even) and in Y (ldy = n): 16-byte copies
         auto stage = [&](int ch, int st) {
             const int j0 = r1 + 1 + ch * MKC;  // first row (1-based) of the chunk
-            for (int e = t; e < 2 * MRB * MKC; e += MT) {
-                const int kk = e % MKC, a = (e / MKC) % MRB, p = e / (MKC * MRB);
-                const int j = j0 + kk;
-                const bool ok = a < bs && j <= n;
-                cp_async8(&sm.U[st][p][a][kk], ok ? &M1(Gt, ldg, p * po + j, r0 + a) : Gt, ok, Gt);
-            }
-            for (int e = t; e < 2 * MKC * MG; e += MT) {
-                const int kk = e % MKC, v = (e / MKC) % MG, p = e / (MKC * MG);
-                const int j = j0 + kk;
-                const bool ok = v < ng && j <= n;
-                cp_async8(&sm.X[st][p][kk][v], ok ? &ycol(v, p)[j - 1] : Gt, ok, Gt);
+            if (vec16) {
+                for (int e = t; e < MRB * MKC; e += MT) {  // 2 planes x 32 rows x 32 pairs
+                    const int kk = 2 * (e % (MKC / 2)), a = (e / (MKC / 2)) % MRB, p = e / (MKC / 2 * MRB);
+                    const int j = j0 + kk;
+                    const int bytes = (a < bs && j <= n) ? (j + 1 <= n ? 16 : 8) : 0;
+                    cp_async16(&sm.U[st][p][a][kk], bytes ? &M1(Gt, ldg, p * po + j, r0 + a) : Gt, bytes, Gt);
+                }
+                for (int e = t; e < MKC * MG; e += MT) {  // 2 parts x 8 vectors x 32 pairs
+                    const int kk = 2 * (e % (MKC / 2)), v = (e / (MKC / 2)) % MG, p = e / (MKC / 2 * MG);
+                    const int j = j0 + kk;
+                    const int bytes = (v < ng && j <= n) ? (j + 1 <= n ? 16 : 8) : 0;
+                    cp_async16(&sm.X[st][p][v][kk], bytes ? &ycol(v, p)[j - 1] : Gt, bytes, Gt);
+                }
+            } else {
+                for (int e = t; e < 2 * MRB * MKC; e += MT) {
+                    const int kk = e % MKC, a = (e / MKC) % MRB, p = e / (MKC * MRB);
+                    const int j = j0 + kk;
+                    const bool ok = a < bs && j <= n;
+                    cp_async8(&sm.U[st][p][a][kk], ok ? &M1(Gt, ldg, p * po + j, r0 + a) : Gt, ok, Gt);
+                }
+                for (int e = t; e < 2 * MKC * MG; e += MT) {
+                    const int kk = e % MKC, v = (e / MKC) % MG, p = e / (MKC * MG);
+                    const int j = j0 + kk;
+                    const bool ok = v < ng && j <= n;
+                    cp_async8(&sm.X[st][p][v][kk], ok ? &ycol(v, p)[j - 1] : Gt, ok, Gt);
+                }
             }
             cp_async_commit();
         };
@@ -450,7 +469,7 @@ __global__ void __launch_bounds__(MT, 2) hess_cplx_mrhs_kernel(int n, const doub
 #pragma unroll
             for (int u = 0; u < MKC / (4 * MW8); ++u) {
                 const int kk = 4 * (warp + MW8 * u) + t4;
-                const double xr = sm.X[st][0][kk][g8], xi = sm.X[st][1][kk][g8];
+                const double xr = sm.X[st][0][g8][kk], xi = sm.X[st][1][g8][kk];
                 double far[4], fai[4];
 #pragma unroll
                 for (int a = 0; a < 4; ++a) {

@@ -100,6 +100,7 @@ __global__ void __launch_bounds__(MT, 1) reduce_mixed_lazy_kernel(MixArgs a)
     int* lg = (int*)(lv + ldr);  // physical row -> logical (1-based)
     int* ph = lg + ldr;          // logical (1-based) -> physical row, ph[0] unused
     float* Us = (float*)(ph + ldr + 4);  // panel update: the panel's U_s at LZ_CH columns (ph[n] may be ph[ldr])
+    unsigned* tbits = (unsigned*)(Us + LZ_NB * LZ_CH);  // bit P: position P is in the touched table
     float* rows = a.grows + (size_t)r0 * ldr;  // nr x ldr, FP32, global
     unsigned long long* hdr = a.hdr;
 
@@ -117,6 +118,7 @@ __global__ void __launch_bounds__(MT, 1) reduce_mixed_lazy_kernel(MixArgs a)
         }
     }
     for (int e = t; e < MIX_RPC_MAX * LZ_NB; e += MT) s_lm[e / LZ_NB][e % LZ_NB] = 0.f;
+    for (int q = t; q < (ldr + 31) / 32; q += MT) tbits[q] = 0u;
     if (t == 0) {
         z.ntouch = 0;
         z.K0 = 1;
@@ -269,8 +271,8 @@ __global__ void __launch_bounds__(MT, 1) reduce_mixed_lazy_kernel(MixArgs a)
                     if (z.tP[q] == Pa) qa = q;
                     if (z.tP[q] == Pb) qb = q;
                 }
-                if (qa < 0) { qa = z.ntouch++; z.tP[qa] = Pa; }
-                if (qb < 0) { qb = z.ntouch++; z.tP[qb] = Pb; }
+                if (qa < 0) { qa = z.ntouch++; z.tP[qa] = Pa; tbits[Pa >> 5] |= 1u << (Pa & 31); }
+                if (qb < 0) { qb = z.ntouch++; z.tP[qb] = Pb; tbits[Pb >> 5] |= 1u << (Pb & 31); }
                 z.tL[qa] = p;      // Pa held logical k+1, now p
                 z.tL[qb] = k + 1;  // Pb held logical p, now k+1
             }
@@ -470,9 +472,12 @@ __global__ void __launch_bounds__(MT, 1) reduce_mixed_lazy_kernel(MixArgs a)
                 const unsigned st = (unsigned)(k + 1);
                 const int nsd = js + 1;  // steps of the panel so far, this one included
                 bool ok = true;
+                // every word of the row is stored once (a reader may take any stored word whose tag
+                // is the step's): the touched positions only by the second loop below
                 for (int P = K0 + tw; P < ldr; P += TW) {
+                    if ((tbits[P >> 5] >> (P & 31)) & 1u) continue;
                     float x = rc[P];
-                    // identity positions: complete iff P + 1 <= k + 1; touched ones are fixed below
+                    // identity positions: complete iff P + 1 <= k + 1
                     if (P >= k + 1 && P < n) {
                         for (int s = 0; s < nsd; ++s) {
                             const float lm = s_lm[cl][s];
@@ -563,6 +568,7 @@ __global__ void __launch_bounds__(MT, 1) reduce_mixed_lazy_kernel(MixArgs a)
                 // the next panel starts in logical column order with no delayed rows
                 for (int e = tw; e < MIX_RPC_MAX * LZ_NB; e += TW) s_lm[e / LZ_NB][e % LZ_NB] = 0.f;
                 if (tw == 0) {
+                    for (int q = 0; q < ntouch; ++q) tbits[z.tP[q] >> 5] &= ~(1u << (z.tP[q] & 31));
                     z.ntouch = 0;
                     z.K0 = k + 1;
                 }
@@ -587,7 +593,8 @@ __global__ void __launch_bounds__(MT, 1) reduce_mixed_lazy_kernel(MixArgs a)
 
 size_t lazy_smem_bytes(int ldr)
 {
-    return (size_t)ldr * 4 * sizeof(float) + 4 * sizeof(int) + (size_t)LZ_NB * LZ_CH * sizeof(float);
+    return (size_t)ldr * 4 * sizeof(float) + 4 * sizeof(int) + (size_t)LZ_NB * LZ_CH * sizeof(float) +
+           (size_t)((ldr + 31) / 32) * sizeof(unsigned);
 }
 
 cudaError_t launch_reduce_mixed_lazy(MixArgs a, const MixPlan& pl, cudaStream_t st)

@@ -70,6 +70,7 @@ def _load():
         "lhl_ws_get_view": [vp, C.POINTER(_WsView)],
         "lhl_ws_check": [vp, vp],
         "lhl_ws_set_barrier_limit_ns": [vp, C.c_uint64],
+        "lhl_ws_set_mixed_kernel": [vp, i32],
         "lhl_reduce": [vp, vp, i64, i32, vp],
         "lhl_ws_phase_ns": [vp, C.POINTER(C.c_uint64), vp],
         "lhl_ws_probe_ns": [vp, C.POINTER(C.c_uint64), vp],
@@ -470,6 +471,11 @@ class LHLWorkspace:
         """Record the reduction's device timers (phase_ns, probe_ns); off by default."""
         _check(_lib.lhl_ws_set_probes(self._h, int(bool(on))), "set_probes")
         self._probes = bool(on)
+
+    def set_mixed_kernel(self, which: int):
+        """Test hook (mixed form): 0 by the order, 1 the eager FP32 kernel, 2 the panel-delayed one."""
+        _check(_lib.lhl_ws_set_mixed_kernel(self._h, int(which)), "set_mixed_kernel")
+        self._mixed_kernel = int(which)
 
     def set_barrier_limit_ns(self, ns: int):
         _check(_lib.lhl_ws_set_barrier_limit_ns(self._h, int(ns)))

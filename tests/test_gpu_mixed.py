@@ -162,6 +162,29 @@ def test_mixed_config2_all_shifts_reach_1e10():
         assert np.linalg.norm(b - W @ X[:, s]) <= 1.0001e-10 * np.linalg.norm(b)
 
 
+@pytest.mark.parametrize("n", [3, 4, 5, 17, 18, 40, 100, 131, 300, 600])
+@pytest.mark.parametrize("balance", [True, False])
+def test_panel_delayed_kernel_is_a_similarity(n, balance):
+    """The panel-delayed FP32 kernel (the one the mixed form uses when its rows no longer fit in
+    shared memory), forced at small orders through the test hook: a valid ELMHES similarity of J
+    to FP32 accuracy, with panels of 16 steps that end inside and at the end of the reduction;
+    and the eager FP32 kernel's pivots over the early steps (late steps pick among near-ties
+    that the two kernels' roundings may order differently)."""
+    torch, G = _mods()
+    J = rng(300 + n).standard_normal((n, n))
+    ws = G.LHLWorkspace(n, G.LHL_PREC_MIXED)
+    ws.set_mixed_kernel(2)
+    G.lhl_reduce_(ws, dev(J), balance)
+    ws.check()
+    check_similarity(ws, J)
+    we = G.LHLWorkspace(n, G.LHL_PREC_MIXED)
+    we.set_mixed_kernel(1)
+    G.lhl_reduce_(we, dev(J), balance)
+    we.check()
+    m = min(n - 2, 120)
+    assert np.array_equal(host(ws.ipiv)[:m], host(we.ipiv)[:m])
+
+
 def test_mixed_rows_in_global_memory():
     """n = 2600: the FP32 rows no longer fit in shared memory (global-memory rows)."""
     torch, G = _mods()
