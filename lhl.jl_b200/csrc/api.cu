@@ -143,7 +143,7 @@ int lhl_ws_create(int64_t n, int precision, lhl_ws_t* out)
         A_(mcval, 2 * (size_t)n);
         // the panel-delayed kernel's ring of candidate rows and global rows are allocated at every
         // order (a test hook can select that kernel where rows would fit on chip)
-        A_(mcrow, (size_t)lhl::MIX_LAZY_RING * g * ldr);
+        A_(mcrow, (size_t)lhl::MIX_LAZY_RING * g * (ldr + lhl::MIX_LAZY_LM));
         A_(mgrows, (size_t)n * ldr);
         A_(linv, (size_t)((n + 63) / 64) * 64 * 64);
     }
@@ -406,7 +406,8 @@ static int reduce_loaded(lhl_ws_t ws, int balance, cudaStream_t st)
         const size_t ring = lazy ? lhl::MIX_LAZY_RING : 2;
         if (e == cudaSuccess)
             e = cudaMemsetAsync(ws->mcrow, 0,
-                                ring * (size_t)ws->mplan.grid * ws->mplan.ldr * sizeof(unsigned long long), st);
+                                ring * (size_t)ws->mplan.grid * (ws->mplan.ldr + lhl::MIX_LAZY_LM) *
+                                    sizeof(unsigned long long), st);
         if (e == cudaSuccess) e = lhl::launch_reduce(a, balance ? 1 : 0, 0, st);
         if (e != cudaSuccess) return LHL_ERR_CUDA;
         lhl::MixArgs m;

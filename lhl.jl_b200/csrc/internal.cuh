@@ -140,6 +140,9 @@ cudaError_t launch_reduce_mixed(MixArgs a, const MixPlan& pl, cudaStream_t st);
 // Rows in global memory (pl.smem_rows == 0): the panel-delayed form (reduce_lazy.cu), whose
 // candidate rows need MIX_LAZY_RING slots of grid x ldr exchange words instead of 2.
 constexpr int MIX_LAZY_RING = 18;
+// each ring slot holds, per CTA, its candidate row (ldr words) and the row's multipliers of the
+// panel so far (MIX_LAZY_LM words)
+constexpr int MIX_LAZY_LM = 16;
 cudaError_t launch_reduce_mixed_lazy(MixArgs a, const MixPlan& pl, cudaStream_t st);
 
 cudaError_t launch_reduce(RedArgs a, int balance, int mode, cudaStream_t st);

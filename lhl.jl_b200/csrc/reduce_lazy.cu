@@ -9,55 +9,64 @@
 // labels); each step one exchange between CTAs (headers, column values, candidate rows: tagged
 // words, relaxed stores, polls bounded in wall time) and no grid barrier.
 //
-// What is delayed.  At step k the eager kernel subtracts l_i R from every own row below the
-// pivot (a read and a write of the whole trailing block per step).  Here the stored rows keep
-// their values from the start of the panel; row i's true entries are
-//     A[i, c] = S[i, c] - sum_{s in panel, s < k} l_i^(s) U_s[c]
-// for every column c not yet complete, where U_s is step s's pivot row and l_i^(s) row i's
-// multiplier at step s (zero unless the row was below that pivot).  Step k then needs:
-//   * the column update A[:, k+1] += A[:, k+2:n] l (the GEMV): with the stored rows,
-//         A[i, :] . l = S[i, :] . l - sum_s l_i^(s) (U_s . l),
-//     so every CTA also takes the panel's U_s rows against l (at most LZ_NB dot products);
-//   * the new column k+1 of row i, written into the stored row (the column is complete):
-//         c'_i = S[i, k+1] + S[i, :] . l - sum_{s <= k} l_i^(s) Gamma_s,
-//         Gamma_s = U_s[k+1] + U_s . l   (U_k = R, the pivot row, l_i^(k) = l_i);
-//   * the candidate row for step k+1 in its true form, computed from its stored values and the
-//     U_s when it is published (the winner's published row is U_{k+1}).
-// The candidate rows live in a ring of LZ_NS slots, so every CTA can read the panel's U_s from
-// the winners' slots until the panel ends.  Column interchanges are not applied to the stored
-// rows during a panel (that would put them out of step with the published U_s): logical column
-// L sits at physical position L - 1 except for the few positions the panel's interchanges
-// touched, kept in a small table; at the panel's end each CTA applies the rank-LZ_NB update
-//     S[i, c] -= sum_s l_i^(s) U_s[c]   for every column c after the panel,
-// then moves the touched positions to their logical places, so that each panel starts in
-// logical column order.  The dot products start at the panel's first column.
+// What is delayed.  The eager kernel subtracts l_i R from every own row below the pivot at
+// every step (a read and a write of the trailing block per step).  Here the stored rows S keep
+// their values from the start of the panel.  With U_s the true pivot row of panel step s and
+// l_i^(s) row i's multiplier at that step (zero unless the row was below that pivot), row i's
+// true entries in every column not yet complete are
+//     A[i, c] = S[i, c] - sum_{s < k} l_i^(s) U_s[c].
+// The winner of a step publishes its STORED row and its multipliers of the panel so far; the
+// true pivot rows then follow from the stored ones, V_s, through a unit lower triangular
+// transform: U_s = V_s - sum_{t < s} T[s][t] U_t with T[s][t] = l_{w_s}^(t), the multipliers of
+// step s's winning row (the form of a blocked Householder product, here for Gauss transforms).
+// Step k needs (l = the step's multipliers, P the physical column order):
+//   * g_s = V_s . l for the panel's earlier steps and g_k = V_k . l for this step's pivot row
+//     (every CTA takes them, from the ring of published rows), then by the transform
+//         gamma_s = g_s - sum_{t < s} T[s][t] gamma_t,   u_s = V_s[k+1] - sum_{t < s} T[s][t] u_t;
+//   * the new column k+1 of own row i (the column update A[:, k+1] += A[:, k+2:n] l after the
+//     row update), written into the stored row -- the column is complete from then on:
+//         c'_i = S[i, k+1] + S[i, :] . l - sum_{s <= k} l_i^(s) (u_s + gamma_s);
+//   * at the panel's end, S[i, c] -= sum_s l_i^(s) U_s[c] = sum_s w_i^(s) V_s[c] for every
+//     column c after the panel, with (I + T)^T w_i = l_i (a back substitution of 16 terms),
+//     then the candidate row of the next step is published in its updated form.
+// The published rows live in a ring of LZ_NS slots, so every CTA reads the panel's V_s from the
+// winners' slots until the panel ends.  Column interchanges are not applied to the stored rows
+// during a panel (the published V_s would go out of step): logical column L sits at physical
+// position L - 1 except at the few positions the panel's interchanges touched, kept in a small
+// table; at the panel's end each CTA moves those positions to their logical places, so each
+// panel starts in logical column order.  The dot products start at the panel's first column.
+// Every exchange word is stored once per step: a reader takes any word whose tag is the step's.
 //
-// Arithmetic: FP32 storage; dot products of FP32 products with FP64 accumulation; the new
-// column value and the Gamma corrections in FP64, rounded once to FP32 when stored; the
-// rank-LZ_NB update in FP32 fused multiply-adds.  The pivot search is the eager kernel's (the
-// reference's first maximum on the FP32 column values).  At the end every CTA writes its rows
-// in FP64 to their logical positions of `factors`, and CTA 0 writes perm / iperm: the same
-// outputs, in the same layout, as the eager kernel.
+// Arithmetic: FP32 storage; dot products of FP32 products with FP64 accumulation; the
+// transform and the new column value in FP64, rounded once when stored; the rank-LZ_NB update
+// in FP32 fused multiply-adds.  The pivot search is the eager kernel's (the reference's first
+// maximum on the FP32 column values).  At the end every CTA writes its rows in FP64 to their
+// logical positions of `factors`, and CTA 0 writes perm / iperm: the eager kernel's outputs.
 #include "mixed_common.cuh"
 
 namespace lhl {
 
-constexpr int LZ_NB = 16;               // steps per panel
-constexpr int LZ_NS = MIX_LAZY_RING;    // slots of the candidate-row ring
+constexpr int LZ_NB = MIX_LAZY_LM;      // steps per panel
+constexpr int LZ_NS = MIX_LAZY_RING;    // slots of the ring of published rows
 static_assert(LZ_NS >= LZ_NB + 2, "the ring holds a panel's pivot rows and the next step's candidates");
 constexpr int LZ_TMAX = 2 * LZ_NB + 2;  // column positions a panel's interchanges can touch
 constexpr int LZ_CH = 256;              // columns per staged chunk of the panel update
+constexpr int LZ_UC = 512;              // columns per warp item of the V_s . l products
+constexpr int LZ_UCMAX = 32;            // items per V_s row (n <= 16384)
+constexpr int LZ_UPL = LZ_UC / 32;      // words per lane in flight
 
 struct LazyShared {
-    int tP[LZ_TMAX];      // touched physical positions (0-based) ...
-    int tL[LZ_TMAX];      // ... and the logical column (1-based) each now holds
-    float tdl[LZ_TMAX];   // per step: l_{tL} - lv[tP] (the dot-product fix at touched positions)
+    int tP[LZ_TMAX];          // touched physical positions (0-based) ...
+    int tL[LZ_TMAX];          // ... and the logical column (1-based) each now holds
+    float tdl[LZ_TMAX];       // per step: l_{tL} - lv[tP] (the dot-product fix at touched positions)
     int ntouch;
-    int win[LZ_NB];       // winning CTA of each panel step
-    float ucol[LZ_NB];    // U_s[k+1] at the step's new column
-    double gam[LZ_NB];    // U_s . l
-    int K0;               // the panel's first step
-    int pk, pk1;          // physical positions of logical columns k and k+1
+    int win[LZ_NB];           // winning CTA of each panel step
+    float T[LZ_NB][LZ_NB];    // T[s][t] = l_{w_s}^(t), t < s
+    float vcol[LZ_NB];        // V_s at this step's new column
+    double gp[LZ_NB][LZ_UCMAX];  // V_s . l by column items
+    double Gam[LZ_NB + 1];    // u_s + gamma_s for s < k, [js]: this step's pivot row's
+    int K0;                   // the panel's first step
+    int pk, pk1;              // physical positions of logical columns k and k+1
 };
 
 // the physical position (0-based) of logical column L (1-based), through the panel's table of
@@ -75,10 +84,10 @@ __device__ __forceinline__ void named_bar_sync(int id, int count)
     asm volatile("bar.sync %0, %1;" ::"r"(id), "r"(count) : "memory");
 }
 
-// U_s[P] from the ring: winner w's row of step s, tagged with the step
+// winner w's published row of step s (ldr words, then LZ_NB multipliers), tagged with the step
 __device__ __forceinline__ const unsigned long long* lz_urow(const MixArgs& a, int s, int w, int G)
 {
-    return a.crow + ((size_t)(s % LZ_NS) * G + w) * a.ldr;
+    return a.crow + ((size_t)(s % LZ_NS) * G + w) * (size_t)(a.ldr + LZ_NB);
 }
 
 __global__ void __launch_bounds__(MT, 1) reduce_mixed_lazy_kernel(MixArgs a)
@@ -92,21 +101,21 @@ __global__ void __launch_bounds__(MT, 1) reduce_mixed_lazy_kernel(MixArgs a)
     __shared__ float s_piv;
 
     const int n = a.n, rpc = a.rpc, ldr = a.ldr, G = gridDim.x, b = blockIdx.x;
+    const int ldrr = ldr + LZ_NB;  // words per CTA in a ring slot
     const int t = threadIdx.x, lane = t & 31, warp = t >> 5;
     const int r0 = b * rpc;
     const int nr = min(rpc, n - r0);
-    float* R = slz;              // pivot row, physical column order; pads zero
+    float* R = slz;              // this step's pivot row as published (stored), physical order
     float* lv = R + ldr;         // multipliers by logical row (slot L-1)
     int* lg = (int*)(lv + ldr);  // physical row -> logical (1-based)
     int* ph = lg + ldr;          // logical (1-based) -> physical row, ph[0] unused
-    float* Us = (float*)(ph + ldr + 4);  // panel update: the panel's U_s at LZ_CH columns (ph[n] may be ph[ldr])
-    unsigned* tbits = (unsigned*)(Us + LZ_NB * LZ_CH);  // bit P: position P is in the touched table
+    float* Us = (float*)(ph + ldr + 4);  // panel update: the panel's V_s at LZ_CH columns (ph[n] may be ph[ldr])
     float* rows = a.grows + (size_t)r0 * ldr;  // nr x ldr, FP32, global
     unsigned long long* hdr = a.hdr;
 
     // ---- load own rows (FP64 -> FP32, zero pads), labels ----
     for (int e = t; e < nr * ldr; e += MT) {
-        const int c = e % ldr, i = e / ldr;  // along the row: coalesced stores, strided reads of A
+        const int c = e % ldr, i = e / ldr;
         rows[(size_t)i * ldr + c] = c < n ? (float)a.A[(size_t)c * n + r0 + i] : 0.f;
     }
     for (int q = t; q < ldr; q += MT) {
@@ -118,7 +127,6 @@ __global__ void __launch_bounds__(MT, 1) reduce_mixed_lazy_kernel(MixArgs a)
         }
     }
     for (int e = t; e < MIX_RPC_MAX * LZ_NB; e += MT) s_lm[e / LZ_NB][e % LZ_NB] = 0.f;
-    for (int q = t; q < (ldr + 31) / 32; q += MT) tbits[q] = 0u;
     if (t == 0) {
         z.ntouch = 0;
         z.K0 = 1;
@@ -149,9 +157,17 @@ __global__ void __launch_bounds__(MT, 1) reduce_mixed_lazy_kernel(MixArgs a)
         }
         if (!ok) atomicCAS(a.err, 0, (int)LHL_ERR_TIMEOUT);
     };
+    // the candidate row of step st (own row cl) as stored, from position p0, and its multipliers
+    // lm (null: zeros), into ring slot st; every word stored once (warps 1-15)
+    auto publish = [&](int st, int cl, int p0, const float* lm) {
+        const int tw = t - 32, TW = MT - 32;
+        const float* rc = rows + (size_t)cl * ldr;
+        unsigned long long* dst = a.crow + ((size_t)(st % LZ_NS) * G + b) * (size_t)ldrr;
+        for (int P = p0 + tw; P < ldr; P += TW) __stcg(&dst[P], mix_tag((unsigned)st, rc[P]));
+        if (tw < LZ_NB) __stcg(&dst[ldr + tw], mix_tag((unsigned)st, lm ? lm[tw] : 0.f));
+    };
 
-    // ---- publish step 1: column 1 values, candidate among logical rows >= 2 (its row as stored:
-    // nothing is delayed yet), into ring slot 1 ----
+    // ---- publish step 1: column 1 values, candidate among logical rows >= 2 ----
     if (warp != 0) prefetch_cval(1);
     if (warp == 0) {
         float bv = 0.f;
@@ -163,14 +179,12 @@ __global__ void __launch_bounds__(MT, 1) reduce_mixed_lazy_kernel(MixArgs a)
             if (L >= 2 && mix_better(v, L, bv, bi)) { bv = v; bi = L; bl = i; }
         }
         warp_best(bv, bi, bl);
-        if (bl >= 0) {
-            const float* src = rows + (size_t)bl * ldr;
-            unsigned long long* dst = a.crow + ((size_t)(1 % LZ_NS) * G + b) * ldr;
-            for (int c = lane; c < ldr; c += 32) __stcg(&dst[c], mix_tag(1u, src[c]));
-        }
+        if (lane == 0) s_cand = bl;
         __syncwarp();
         if (lane == 0) st_relaxed_u64(&hdr[(1 & 1) * G + b], mix_pack(1u, bi, bv));
     }
+    __syncthreads();
+    if (warp != 0 && s_cand >= 0) publish(1, s_cand, 0, nullptr);
 
     const uint64_t t_start = globaltimer_ns();
     for (int k = 1; k <= n - 2; ++k) {
@@ -271,8 +285,8 @@ __global__ void __launch_bounds__(MT, 1) reduce_mixed_lazy_kernel(MixArgs a)
                     if (z.tP[q] == Pa) qa = q;
                     if (z.tP[q] == Pb) qb = q;
                 }
-                if (qa < 0) { qa = z.ntouch++; z.tP[qa] = Pa; tbits[Pa >> 5] |= 1u << (Pa & 31); }
-                if (qb < 0) { qb = z.ntouch++; z.tP[qb] = Pb; tbits[Pb >> 5] |= 1u << (Pb & 31); }
+                if (qa < 0) { qa = z.ntouch++; z.tP[qa] = Pa; }
+                if (qb < 0) { qb = z.ntouch++; z.tP[qb] = Pb; }
                 z.tL[qa] = p;      // Pa held logical k+1, now p
                 z.tL[qb] = k + 1;  // Pb held logical p, now k+1
             }
@@ -282,14 +296,14 @@ __global__ void __launch_bounds__(MT, 1) reduce_mixed_lazy_kernel(MixArgs a)
         }
         __syncthreads();
         const int pk1 = z.pk1;
-        // ---- pivot row (physical order, from the winner's ring slot), multipliers by logical row
-        // (from the prefetched column values, slots by the labels before the interchange) ----
+        // ---- pivot row as published (stored values, physical order) and its multipliers (a row
+        // of T), from the winner's ring slot; multipliers by logical row from the prefetched column
+        // values (slots by the labels before the interchange) ----
         {
             const unsigned long long* src = win >= 0 ? lz_urow(a, k, win, G) : nullptr;
             const unsigned want = (unsigned)k & 0xffffu;
             bool ok = true;
-            const int P0 = K0;  // the panel's first column (0-based position of logical K0 + 1)
-            for (int base = P0; base < ldr; base += 4 * MT) {
+            for (int base = K0; base < ldr; base += 4 * MT) {
                 unsigned long long rv[4];
 #pragma unroll
                 for (int u = 0; u < 4; ++u) {
@@ -304,6 +318,7 @@ __global__ void __launch_bounds__(MT, 1) reduce_mixed_lazy_kernel(MixArgs a)
                     if (P < ldr) R[P] = P < n ? r : 0.f;
                 }
             }
+            if (t < js) z.T[js][t] = src ? ld_tagged(&src[ldr + t], k, a.limit_ns, ok) : 0.f;
             if (!ok) atomicCAS(a.err, 0, (int)LHL_ERR_TIMEOUT);
             for (int jj = k + 1 + t; jj < n; jj += MT) {  // slot of logical row jj + 1 >= k + 2
                 const float cq = lv[jj == p - 1 ? k : jj];
@@ -312,56 +327,68 @@ __global__ void __launch_bounds__(MT, 1) reduce_mixed_lazy_kernel(MixArgs a)
         }
         __syncthreads();
         // slots of logical rows K0+1 .. k+1 are no multipliers (zero for the dot products, which
-        // start at the panel's first column); U_s[k+1] of the panel's earlier steps
+        // start at the panel's first column); V_s at the new column for the panel's earlier steps
         for (int jj = K0 + t; jj <= k; jj += MT) lv[jj] = 0.f;
         if (t < js) {
             bool ok = true;
-            const unsigned long long* u = lz_urow(a, K0 + t, z.win[t], G);
-            z.ucol[t] = z.win[t] >= 0 ? ld_tagged(&u[pk1], K0 + t, a.limit_ns, ok) : 0.f;
+            z.vcol[t] = z.win[t] >= 0 ? ld_tagged(&lz_urow(a, K0 + t, z.win[t], G)[pk1], K0 + t, a.limit_ns, ok) : 0.f;
             if (!ok) atomicCAS(a.err, 0, (int)LHL_ERR_TIMEOUT);
         }
         __syncthreads();
-        // the dot-product fix at touched positions: l_{logical(P)} - lv[P]
-        if (t < z.ntouch) {
+        if (t < z.ntouch) {  // the dot-product fix at touched positions: l_{logical(P)} - lv[P]
             const int P = z.tP[t], L = z.tL[t];
             z.tdl[t] = (L >= k + 2 ? lv[L - 1] : 0.f) - lv[P];
         }
         __syncthreads();
 
         // ---- dot products (FP64 accumulation of FP32 products) from the panel's first column:
-        // own stored rows and R as in the eager kernel's items (4 rows x one of 4 column parts per
-        // warp, the touched-position fix in part 0), then the panel's U_s rows, one warp each ----
+        // own stored rows and the pivot row in the eager kernel's items (4 rows x one of 4 column
+        // parts per warp, the touched-position fix in part 0); then V_s . l for the panel's
+        // earlier steps, items of LZ_UC columns per warp with every lane's words in flight ----
         const int ntouch = z.ntouch;
+        const int c0 = K0;
+        const int nuc = (n - c0 + LZ_UC - 1) / LZ_UC;
         {
             const int nv = nr + 1;  // own rows, then R
-            const int c0 = K0, c4 = (c0 + 3) & ~3;
+            const int c4 = (c0 + 3) & ~3;
             const int g0 = c4 >> 2, g1 = ldr >> 2;
             const int per = (g1 - g0 + 3) >> 2;
             const float4* l4 = reinterpret_cast<const float4*>(lv);
             const int nitems = ((nv + 3) >> 2) * 4;
-            for (int item = warp; item < nitems + js; item += MW) {
-                if (item >= nitems) {  // U_s . l for the panel's step s = K0 + (item - nitems)
-                    const int si = item - nitems;
+            for (int item = warp; item < nitems + js * nuc; item += MW) {
+                if (item >= nitems) {
+                    const int si = (item - nitems) / nuc, ch = (item - nitems) % nuc;
                     double acc = 0.0;
                     const int w = z.win[si];
                     if (w >= 0) {
                         const unsigned long long* u = lz_urow(a, K0 + si, w, G);
+                        const unsigned want = (unsigned)(K0 + si) & 0xffffu;
                         bool ok = true;
-                        for (int P = c0 + lane; P < n; P += 32) {
-                            const unsigned long long v = ld_relaxed_u64(&u[P]);
-                            float x = __uint_as_float((unsigned)(v >> 32));
-                            if (((unsigned)(v >> 16) & 0xffffu) != ((unsigned)(K0 + si) & 0xffffu))
-                                x = ld_tagged(&u[P], K0 + si, a.limit_ns, ok);
-                            acc += (double)(x * lv[P]);
+                        const int pb = c0 + ch * LZ_UC + lane;
+                        unsigned long long v[LZ_UPL];
+#pragma unroll
+                        for (int j = 0; j < LZ_UPL; ++j) {
+                            const int P = pb + 32 * j;
+                            v[j] = P < n ? ld_relaxed_u64(&u[P]) : 0ull;
                         }
-                        for (int q = lane; q < ntouch; q += 32) {
-                            const float x = ld_tagged(&u[z.tP[q]], K0 + si, a.limit_ns, ok);
-                            acc += (double)(x * z.tdl[q]);
+#pragma unroll
+                        for (int j = 0; j < LZ_UPL; ++j) {
+                            const int P = pb + 32 * j;
+                            if (P < n) {
+                                float x = __uint_as_float((unsigned)(v[j] >> 32));
+                                if (((unsigned)(v[j] >> 16) & 0xffffu) != want) x = ld_tagged(&u[P], K0 + si, a.limit_ns, ok);
+                                acc += (double)(x * lv[P]);
+                            }
                         }
+                        if (ch == 0)
+                            for (int q = lane; q < ntouch; q += 32) {
+                                const float x = ld_tagged(&u[z.tP[q]], K0 + si, a.limit_ns, ok);
+                                acc += (double)(x * z.tdl[q]);
+                            }
                         if (!ok) atomicCAS(a.err, 0, (int)LHL_ERR_TIMEOUT);
                     }
                     acc = warp_sum(acc);
-                    if (lane == 0) z.gam[si] = acc;
+                    if (lane == 0) z.gp[si][ch] = acc;
                     continue;
                 }
                 const int rg = item >> 2, cp = item & 3;
@@ -424,16 +451,41 @@ __global__ void __launch_bounds__(MT, 1) reduce_mixed_lazy_kernel(MixArgs a)
             }
         }
         __syncthreads();
+        auto dot = [&](int v) {
+            return (s_part[4 * v] + s_part[4 * v + 1]) + (s_part[4 * v + 2] + s_part[4 * v + 3]);
+        };
+        // ---- the transform: true gamma_s and u_s of the panel's pivot rows, in step order
+        // (thread 0: gamma, thread 1: u), then Gamma = u + gamma ----
+        if (t < 2) {
+            double val[LZ_NB];
+            for (int s = 0; s <= js; ++s) {
+                double x;
+                if (t == 0) {
+                    if (s < js) {
+                        x = 0.0;
+                        for (int ch = 0; ch < nuc; ++ch) x += z.gp[s][ch];
+                    } else {
+                        x = dot(nr);
+                    }
+                } else {
+                    x = s < js ? (double)z.vcol[s] : (double)R[pk1];
+                }
+                for (int tt = 0; tt < s; ++tt) x -= (double)z.T[s][tt] * val[tt];
+                val[s] = x;
+            }
+            if (t == 0)
+                for (int s = 0; s <= js; ++s) z.Gam[s] = val[s];
+            __syncwarp(0x3u);
+            if (t == 1)
+                for (int s = 0; s <= js; ++s) z.Gam[s] += val[s];
+        }
+        __syncthreads();
         // ---- warp 0: new column k+1 of own rows (completed in the stored rows), multipliers into
         // column k, the next candidate and its header ----
         if (warp == 0) {
             float bv = 0.f;
             int bi = 0, bl = -1;
             const int np = (k + 1) & 1;
-            auto dot = [&](int v) {
-                return (s_part[4 * v] + s_part[4 * v + 1]) + (s_part[4 * v + 2] + s_part[4 * v + 3]);
-            };
-            const double gk = (double)R[pk1] + dot(nr);  // Gamma_k
             const int pk = z.pk;
             for (int i = lane; i < nr; i += 32) {
                 float* ri = rows + (size_t)i * ldr;
@@ -442,9 +494,9 @@ __global__ void __launch_bounds__(MT, 1) reduce_mixed_lazy_kernel(MixArgs a)
                 double cn = (double)ri[pk1] + dot(i);
                 for (int s = 0; s < js; ++s) {
                     const float lm = s_lm[i][s];
-                    if (lm != 0.f) cn -= (double)lm * ((double)z.ucol[s] + z.gam[s]);
+                    if (lm != 0.f) cn -= (double)lm * z.Gam[s];
                 }
-                cn -= (double)li * gk;
+                cn -= (double)li * z.Gam[js];
                 const float c32 = (float)cn;
                 ri[pk1] = c32;
                 if (L >= k + 2) ri[pk] = li;
@@ -463,71 +515,28 @@ __global__ void __launch_bounds__(MT, 1) reduce_mixed_lazy_kernel(MixArgs a)
         const int cl = s_cand;
         if (warp != 0) {
             const int tw = t - 32, TW = MT - 32;  // warps 1-15
-            // ---- publish step k+1's candidate row in its true form:
-            //   S[cl, P] - sum_{s <= k} l_cl^(s) U_s[P] at columns not yet complete (logical >= k+2),
-            // the stored value elsewhere; in the next panel's column order if this step ends the panel
-            if (k + 1 <= n - 2 && cl >= 0) {
-                const float* rc = rows + (size_t)cl * ldr;
-                unsigned long long* dst = a.crow + ((size_t)((k + 1) % LZ_NS) * G + b) * ldr;
-                const unsigned st = (unsigned)(k + 1);
-                const int nsd = js + 1;  // steps of the panel so far, this one included
-                bool ok = true;
-                // every word of the row is stored once (a reader may take any stored word whose tag
-                // is the step's): the touched positions only by the second loop below
-                for (int P = K0 + tw; P < ldr; P += TW) {
-                    if ((tbits[P >> 5] >> (P & 31)) & 1u) continue;
-                    float x = rc[P];
-                    // identity positions: complete iff P + 1 <= k + 1
-                    if (P >= k + 1 && P < n) {
-                        for (int s = 0; s < nsd; ++s) {
-                            const float lm = s_lm[cl][s];
-                            if (lm == 0.f) continue;
-                            const float u = s == js ? R[P] : ld_tagged(&lz_urow(a, K0 + s, z.win[s], G)[P], K0 + s,
-                                                                       a.limit_ns, ok);
-                            x = fmaf(-lm, u, x);
-                        }
-                    }
-                    __stcg(&dst[P], mix_tag(st, x));
-                }
-                if (!ok) atomicCAS(a.err, 0, (int)LHL_ERR_TIMEOUT);
-                named_bar_sync(1, TW);
-                // touched positions: their own completeness; and the move to logical order at a panel end
-                for (int q = tw; q < ntouch; q += TW) {
-                    const int P = z.tP[q], L = z.tL[q];
-                    float x = rc[P];
-                    if (L >= k + 2) {
-                        for (int s = 0; s < nsd; ++s) {
-                            const float lm = s_lm[cl][s];
-                            if (lm == 0.f) continue;
-                            const float u = s == js ? R[P] : ld_tagged(&lz_urow(a, K0 + s, z.win[s], G)[P], K0 + s,
-                                                                       a.limit_ns, ok);
-                            x = fmaf(-lm, u, x);
-                        }
-                    }
-                    z.tdl[q] = x;  // the value at P (tdl is free until the next step)
-                }
-                named_bar_sync(1, TW);
-                for (int q = tw; q < ntouch; q += TW) {
-                    const int P = z.tP[q], L = z.tL[q];
-                    __stcg(&dst[last ? L - 1 : P], mix_tag(st, z.tdl[q]));
-                }
-                if (!ok) atomicCAS(a.err, 0, (int)LHL_ERR_TIMEOUT);
-            }
-            if (last) {
-                // ---- panel end: S[i, P] -= sum_s l_i^(s) U_s[P] at the columns after the panel
-                // (logical >= k + 2), chunks of LZ_CH columns staged in lv, then the touched
-                // positions moved to their logical places ----
-                named_bar_sync(1, TW);
+            if (!last) {
+                // ---- publish step k+1's candidate: its stored row and its multipliers so far ----
+                if (k + 1 <= n - 2 && cl >= 0) publish(k + 1, cl, K0, s_lm[cl]);
+            } else {
+                // ---- panel end: S[i, P] -= sum_s w_i^(s) V_s[P] at the columns after the panel
+                // (logical >= k + 2), (I + T)^T w_i = l_i; chunks of LZ_CH columns staged in Us;
+                // then the touched positions moved to their logical places ----
                 const int nsd = js + 1;
-                for (int i = tw; i < nr; i += TW) {  // rows with a delayed update
+                for (int i = tw; i < nr; i += TW) {  // w_i over l_i, in place; rows with a delayed update
                     int any = 0;
-                    for (int s = 0; s < nsd; ++s) any |= s_lm[i][s] != 0.f;
+                    for (int s = nsd - 1; s >= 0; --s) {
+                        float x = s_lm[i][s];
+                        for (int s2 = s + 1; s2 < nsd; ++s2) x = fmaf(-z.T[s2][s], s_lm[i][s2], x);
+                        s_lm[i][s] = x;
+                        any |= x != 0.f;
+                    }
                     s_li[i] = any ? 1.f : 0.f;
                 }
                 bool ok = true;
-                for (int c0 = K0; c0 < n; c0 += LZ_CH) {
+                for (int cc0 = K0; cc0 < n; cc0 += LZ_CH) {
                     for (int e = tw; e < nsd * LZ_CH; e += TW) {
-                        const int s = e / LZ_CH, P = c0 + e % LZ_CH;
+                        const int s = e / LZ_CH, P = cc0 + e % LZ_CH;
                         float u = 0.f;
                         if (P < n && (s == js || z.win[s] >= 0)) {
                             int L = P + 1;
@@ -540,13 +549,13 @@ __global__ void __launch_bounds__(MT, 1) reduce_mixed_lazy_kernel(MixArgs a)
                     }
                     named_bar_sync(1, TW);
                     for (int e = tw; e < nr * LZ_CH; e += TW) {
-                        const int i = e / LZ_CH, cc = e % LZ_CH, P = c0 + cc;
+                        const int i = e / LZ_CH, cc = e % LZ_CH, P = cc0 + cc;
                         if (P >= n || s_li[i] == 0.f) continue;
                         float* ri = rows + (size_t)i * ldr;
                         float x = ri[P];
                         for (int s = 0; s < nsd; ++s) {
-                            const float lm = s_lm[i][s];
-                            if (lm != 0.f) x = fmaf(-lm, Us[s * LZ_CH + cc], x);
+                            const float w = s_lm[i][s];
+                            if (w != 0.f) x = fmaf(-w, Us[s * LZ_CH + cc], x);
                         }
                         ri[P] = x;
                     }
@@ -565,10 +574,11 @@ __global__ void __launch_bounds__(MT, 1) reduce_mixed_lazy_kernel(MixArgs a)
                     if (lane + 32 < ntouch) ri[z.tL[lane + 32] - 1] = v1;
                 }
                 named_bar_sync(1, TW);
-                // the next panel starts in logical column order with no delayed rows
+                // the candidate of step k+1 opens the next panel: its row is now complete and in
+                // logical order, with no delayed multipliers
+                if (k + 1 <= n - 2 && cl >= 0) publish(k + 1, cl, k + 1, nullptr);
                 for (int e = tw; e < MIX_RPC_MAX * LZ_NB; e += TW) s_lm[e / LZ_NB][e % LZ_NB] = 0.f;
                 if (tw == 0) {
-                    for (int q = 0; q < ntouch; ++q) tbits[z.tP[q] >> 5] &= ~(1u << (z.tP[q] & 31));
                     z.ntouch = 0;
                     z.K0 = k + 1;
                 }
@@ -593,8 +603,7 @@ __global__ void __launch_bounds__(MT, 1) reduce_mixed_lazy_kernel(MixArgs a)
 
 size_t lazy_smem_bytes(int ldr)
 {
-    return (size_t)ldr * 4 * sizeof(float) + 4 * sizeof(int) + (size_t)LZ_NB * LZ_CH * sizeof(float) +
-           (size_t)((ldr + 31) / 32) * sizeof(unsigned);
+    return (size_t)ldr * 4 * sizeof(float) + 4 * sizeof(int) + (size_t)LZ_NB * LZ_CH * sizeof(float);
 }
 
 cudaError_t launch_reduce_mixed_lazy(MixArgs a, const MixPlan& pl, cudaStream_t st)
@@ -602,6 +611,7 @@ cudaError_t launch_reduce_mixed_lazy(MixArgs a, const MixPlan& pl, cudaStream_t 
     if (!pl.ok) return cudaErrorInvalidValue;
     a.rpc = pl.rpc;
     a.ldr = pl.ldr;
+    if ((a.n - 1 + LZ_UC) / LZ_UC > LZ_UCMAX) return cudaErrorInvalidValue;
     const size_t smem = lazy_smem_bytes(pl.ldr);
     if (smem > MIX_SMEM_MAX) return cudaErrorInvalidValue;
     static size_t attr = 0;
