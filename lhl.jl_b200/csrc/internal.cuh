@@ -127,6 +127,7 @@ struct MixArgs {
     int* err;
     unsigned long long limit_ns;
     unsigned long long* ptimes;
+    int ring;               // panel-delayed form: rows in flight per thread in the panel update (set at launch)
 };
 
 struct MixPlan {
@@ -135,6 +136,7 @@ struct MixPlan {
 };
 
 constexpr size_t MIX_SMEM_MAX = 227 * 1024 - 4096;  // dynamic part; the kernel's static shared arrays use 2.4 KB
+constexpr size_t MIX_SMEM_TOTAL = 227 * 1024;       // dynamic + static shared memory per CTA
 void mixed_plan(int n, int sms, MixPlan* pl);
 cudaError_t launch_reduce_mixed(MixArgs a, const MixPlan& pl, cudaStream_t st);
 // Rows in global memory (pl.smem_rows == 0): the panel-delayed form (reduce_lazy.cu), whose

@@ -50,7 +50,7 @@ constexpr int LZ_NB = MIX_LAZY_LM;      // steps per panel
 constexpr int LZ_NS = MIX_LAZY_RING;    // slots of the ring of published rows
 static_assert(LZ_NS >= LZ_NB + 2, "the ring holds a panel's pivot rows and the next step's candidates");
 constexpr int LZ_TMAX = 2 * LZ_NB + 2;  // column positions a panel's interchanges can touch
-constexpr int LZ_CH = 256;              // columns per staged chunk of the panel update
+constexpr int LZ_RING_MAX = 16;         // rows in flight per thread in the panel update (cp.async ring)
 constexpr int LZ_UC = 512;              // columns per warp item of the V_s . l products
 constexpr int LZ_UCMAX = 32;            // items per V_s row (n <= 16384)
 constexpr int LZ_UPL = LZ_UC / 32;      // words per lane in flight
@@ -78,6 +78,14 @@ __device__ __forceinline__ int lz_cph(const LazyShared& z, int L)
     return L - 1;
 }
 
+// 8-byte asynchronous copy of 2 floats global -> shared (cp.async); both addresses 8-byte
+// aligned
+__device__ __forceinline__ void lz_cp8(float* dst, const float* src)
+{
+    const unsigned d = (unsigned)__cvta_generic_to_shared(dst);
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(d), "l"(src) : "memory");
+}
+
 // barrier of the `count` threads of warps 1-15 (id 1; warp 0 is polling meanwhile)
 __device__ __forceinline__ void named_bar_sync(int id, int count)
 {
@@ -90,6 +98,76 @@ __device__ __forceinline__ const unsigned long long* lz_urow(const MixArgs& a, i
     return a.crow + ((size_t)(s % LZ_NS) * G + w) * (size_t)(a.ldr + LZ_NB);
 }
 
+// The panel end's rank-LZ_NB update S[i, P] -= sum_s w_i^(s) V_s[P] for the rows in `ul`
+// (nu rows with a delayed update), every column P from the panel's first one whose logical
+// column is >= k + 2.  Thread tw of the TW threads of warps 1-15 takes pairs of columns: it
+// holds the 2 columns of every V_s in registers (V_js = R in shared memory, the others from
+// their winners' ring slots, every one of them read earlier in the panel) and streams the rows
+// through a ring of D 8-byte slots of its own, filled by cp.async D rows ahead, so that D rows
+// of its columns are in flight at once.  A slot is refilled only after its value has been used
+// (the refill follows the store that depends on it).  Columns that take no update keep their
+// values (V is zero there) and their exchange words are not read.
+template <int D>
+__device__ __forceinline__ void lz_panel_update(const MixArgs& a, float* rows, int ldr, int n, int k, int K0,
+                                                int js, int G, const float* R, const LazyShared& z,
+                                                const float (*w)[LZ_NB], const int* ul, int nu, float2* ring,
+                                                int tw, int TW, bool& ok)
+{
+    float2* mine = ring + (size_t)tw * D;
+    const int g0 = K0 >> 1, g1 = ldr >> 1;
+    const int ntouch = z.ntouch;
+    for (int g = g0 + tw; g < g1; g += TW) {
+        const int P0 = 2 * g;
+        // logical columns >= k + 2 take the update: positions >= k + 1 unless touched, and the
+        // touched positions by their table entry
+        bool m0 = P0 >= k + 1 && P0 < n, m1 = P0 + 1 >= k + 1 && P0 + 1 < n;
+        for (int q = 0; q < ntouch; ++q) {
+            const int P = z.tP[q];
+            if (P == P0) m0 = z.tL[q] >= k + 2;
+            if (P == P0 + 1) m1 = z.tL[q] >= k + 2;
+        }
+        if (!m0 && !m1) continue;
+        float v[LZ_NB][2];
+#pragma unroll
+        for (int s = 0; s < LZ_NB; ++s) {
+            v[s][0] = v[s][1] = 0.f;
+            if (s < js && z.win[s] >= 0) {
+                const unsigned long long* u = lz_urow(a, K0 + s, z.win[s], G) + P0;
+                const ulonglong2 p = __ldcg(reinterpret_cast<const ulonglong2*>(u));
+                const unsigned want = (unsigned)(K0 + s) & 0xffffu;
+                float x0 = __uint_as_float((unsigned)(p.x >> 32)), x1 = __uint_as_float((unsigned)(p.y >> 32));
+                if (m0 && ((unsigned)(p.x >> 16) & 0xffffu) != want) x0 = ld_tagged(u, K0 + s, a.limit_ns, ok);
+                if (m1 && ((unsigned)(p.y >> 16) & 0xffffu) != want) x1 = ld_tagged(u + 1, K0 + s, a.limit_ns, ok);
+                v[s][0] = m0 ? x0 : 0.f;
+                v[s][1] = m1 ? x1 : 0.f;
+            } else if (s == js) {
+                v[s][0] = m0 ? R[P0] : 0.f;
+                v[s][1] = m1 ? R[P0 + 1] : 0.f;
+            }
+        }
+#pragma unroll
+        for (int q = 0; q < D; ++q) {
+            if (q < nu) lz_cp8(reinterpret_cast<float*>(&mine[q]), rows + (size_t)ul[q] * ldr + P0);
+            cp_async_commit();
+        }
+        for (int q = 0; q < nu; ++q) {
+            cp_async_wait<D - 1>();
+            float2 x = mine[q % D];
+            const float* wi = w[ul[q]];
+#pragma unroll
+            for (int s = 0; s < LZ_NB; ++s) {
+                const float ws = wi[s];
+                x.x = fmaf(-ws, v[s][0], x.x);
+                x.y = fmaf(-ws, v[s][1], x.y);
+            }
+            *reinterpret_cast<float2*>(rows + (size_t)ul[q] * ldr + P0) = x;
+            if (q + D < nu) lz_cp8(reinterpret_cast<float*>(&mine[q % D]), rows + (size_t)ul[q + D] * ldr + P0);
+            cp_async_commit();
+        }
+        cp_async_wait<0>();
+    }
+}
+
 __global__ void __launch_bounds__(MT, 1) reduce_mixed_lazy_kernel(MixArgs a)
 {
     extern __shared__ __align__(16) float slz[];
@@ -99,6 +177,8 @@ __global__ void __launch_bounds__(MT, 1) reduce_mixed_lazy_kernel(MixArgs a)
     __shared__ LazyShared z;
     __shared__ int s_win, s_p, s_ok, s_cand;
     __shared__ float s_piv;
+    __shared__ int s_ul[MIX_RPC_MAX];  // panel end: own rows with a delayed update
+    __shared__ int s_nu;
 
     const int n = a.n, rpc = a.rpc, ldr = a.ldr, G = gridDim.x, b = blockIdx.x;
     const int ldrr = ldr + LZ_NB;  // words per CTA in a ring slot
@@ -109,7 +189,7 @@ __global__ void __launch_bounds__(MT, 1) reduce_mixed_lazy_kernel(MixArgs a)
     float* lv = R + ldr;         // multipliers by logical row (slot L-1)
     int* lg = (int*)(lv + ldr);  // physical row -> logical (1-based)
     int* ph = lg + ldr;          // logical (1-based) -> physical row, ph[0] unused
-    float* Us = (float*)(ph + ldr + 4);  // panel update: the panel's V_s at LZ_CH columns (ph[n] may be ph[ldr])
+    float2* ring = (float2*)(ph + ldr + 4);  // panel update: 8-byte slots (a.ring per thread of warps 1-15)
     float* rows = a.grows + (size_t)r0 * ldr;  // nr x ldr, FP32, global
     unsigned long long* hdr = a.hdr;
 
@@ -187,8 +267,23 @@ __global__ void __launch_bounds__(MT, 1) reduce_mixed_lazy_kernel(MixArgs a)
     if (warp != 0 && s_cand >= 0) publish(1, s_cand, 0, nullptr);
 
     const uint64_t t_start = globaltimer_ns();
+    // CTA 0's time per phase, summed over steps (lhl_ws_set_probes).  Thread 0: slot 0 the wait
+    // for step k (warp 0's poll, and warps 1-15's work of the step before), 1 interchange and
+    // pivot row, 2 dot products, 3 transform, 4 new column; slot 5 the poll alone.  Thread 32
+    // (warps 1-15): slot 8 publishing a candidate row, 9 the panel end, 10 the column-value
+    // prefetch.
+    unsigned long long* probe = (b == 0 && (t == 0 || t == 32) && a.ptimes) ? a.ptimes + 8 : nullptr;
+    uint64_t tp = t_start;
+    auto mark = [&](int slot) {
+        if (probe) {
+            const uint64_t now = globaltimer_ns();
+            probe[slot] += now - tp;
+            tp = now;
+        }
+    };
     for (int k = 1; k <= n - 2; ++k) {
         const int par = k & 1;
+        if (t == 0) tp = globaltimer_ns();
         // ---- wait for step k from every CTA; pick the pivot (the eager kernel's poll) ----
         if (warp == 0) {
             const unsigned long long* H = hdr + par * G;
@@ -240,6 +335,7 @@ __global__ void __launch_bounds__(MT, 1) reduce_mixed_lazy_kernel(MixArgs a)
                     if (__shfl_sync(0xffffffffu, bad, 0)) { ok = 0; break; }
                 }
             }
+            if (probe && t == 0) probe[5] += globaltimer_ns() - tp;
             float bv = 0.f;
             int bi = 0, bs = -1;
             if (ok) {
@@ -264,6 +360,7 @@ __global__ void __launch_bounds__(MT, 1) reduce_mixed_lazy_kernel(MixArgs a)
             }
         }
         __syncthreads();
+        if (t == 0) mark(0);
         if (!s_ok) return;
         const int p = s_p;
         const int win = s_win;
@@ -340,6 +437,7 @@ __global__ void __launch_bounds__(MT, 1) reduce_mixed_lazy_kernel(MixArgs a)
             z.tdl[t] = (L >= k + 2 ? lv[L - 1] : 0.f) - lv[P];
         }
         __syncthreads();
+        if (t == 0) mark(1);
 
         // ---- dot products (FP64 accumulation of FP32 products) from the panel's first column:
         // own stored rows and the pivot row in the eager kernel's items (4 rows x one of 4 column
@@ -416,7 +514,38 @@ __global__ void __launch_bounds__(MT, 1) reduce_mixed_lazy_kernel(MixArgs a)
                 for (int q = 0; q < 4; ++q) pp[q][0] = pp[q][1] = pp[q][2] = pp[q][3] = 0.f;
                 int it = 0;
                 const int ga = g0 + cp * per, gb = min(ga + per, g1);
-                for (int g = ga + lane; g < gb; g += 32) {
+                int g = ga + lane;
+                // two iterations' loads (8 float4 per lane) issued before their multiply-adds
+                for (; g + 32 < gb; g += 64) {
+                    float4 x0[4], x1[4];
+#pragma unroll
+                    for (int q = 0; q < 4; ++q) {
+                        // generic loads: the last item row may be R, in shared memory
+                        x0[q] = reinterpret_cast<const float4*>(xq[q])[g];
+                        x1[q] = reinterpret_cast<const float4*>(xq[q])[g + 32];
+                    }
+                    const float4 la = l4[g], lb = l4[g + 32];
+#pragma unroll
+                    for (int q = 0; q < 4; ++q) {
+                        pp[q][0] = fmaf(x0[q].x, la.x, pp[q][0]);
+                        pp[q][1] = fmaf(x0[q].y, la.y, pp[q][1]);
+                        pp[q][2] = fmaf(x0[q].z, la.z, pp[q][2]);
+                        pp[q][3] = fmaf(x0[q].w, la.w, pp[q][3]);
+                        pp[q][0] = fmaf(x1[q].x, lb.x, pp[q][0]);
+                        pp[q][1] = fmaf(x1[q].y, lb.y, pp[q][1]);
+                        pp[q][2] = fmaf(x1[q].z, lb.z, pp[q][2]);
+                        pp[q][3] = fmaf(x1[q].w, lb.w, pp[q][3]);
+                    }
+                    if ((it += 2) == MIX_FLUSH) {
+#pragma unroll
+                        for (int q = 0; q < 4; ++q) {
+                            acc[q] += ((double)pp[q][0] + (double)pp[q][1]) + ((double)pp[q][2] + (double)pp[q][3]);
+                            pp[q][0] = pp[q][1] = pp[q][2] = pp[q][3] = 0.f;
+                        }
+                        it = 0;
+                    }
+                }
+                for (; g < gb; g += 32) {
                     const float4 l = l4[g];
 #pragma unroll
                     for (int q = 0; q < 4; ++q) {
@@ -451,6 +580,7 @@ __global__ void __launch_bounds__(MT, 1) reduce_mixed_lazy_kernel(MixArgs a)
             }
         }
         __syncthreads();
+        if (t == 0) mark(2);
         auto dot = [&](int v) {
             return (s_part[4 * v] + s_part[4 * v + 1]) + (s_part[4 * v + 2] + s_part[4 * v + 3]);
         };
@@ -480,6 +610,7 @@ __global__ void __launch_bounds__(MT, 1) reduce_mixed_lazy_kernel(MixArgs a)
                 for (int s = 0; s <= js; ++s) z.Gam[s] += val[s];
         }
         __syncthreads();
+        if (t == 0) mark(3);
         // ---- warp 0: new column k+1 of own rows (completed in the stored rows), multipliers into
         // column k, the next candidate and its header ----
         if (warp == 0) {
@@ -512,16 +643,19 @@ __global__ void __launch_bounds__(MT, 1) reduce_mixed_lazy_kernel(MixArgs a)
             }
         }
         __syncthreads();
+        if (t == 0) mark(4);
         const int cl = s_cand;
         if (warp != 0) {
             const int tw = t - 32, TW = MT - 32;  // warps 1-15
+            if (t == 32) tp = globaltimer_ns();
             if (!last) {
                 // ---- publish step k+1's candidate: its stored row and its multipliers so far ----
                 if (k + 1 <= n - 2 && cl >= 0) publish(k + 1, cl, K0, s_lm[cl]);
+                if (t == 32) mark(8);
             } else {
                 // ---- panel end: S[i, P] -= sum_s w_i^(s) V_s[P] at the columns after the panel
-                // (logical >= k + 2), (I + T)^T w_i = l_i; chunks of LZ_CH columns staged in Us;
-                // then the touched positions moved to their logical places ----
+                // (logical >= k + 2), (I + T)^T w_i = l_i (lz_panel_update); then the touched
+                // positions moved to their logical places ----
                 const int nsd = js + 1;
                 for (int i = tw; i < nr; i += TW) {  // w_i over l_i, in place; rows with a delayed update
                     int any = 0;
@@ -533,34 +667,27 @@ __global__ void __launch_bounds__(MT, 1) reduce_mixed_lazy_kernel(MixArgs a)
                     }
                     s_li[i] = any ? 1.f : 0.f;
                 }
-                bool ok = true;
-                for (int cc0 = K0; cc0 < n; cc0 += LZ_CH) {
-                    for (int e = tw; e < nsd * LZ_CH; e += TW) {
-                        const int s = e / LZ_CH, P = cc0 + e % LZ_CH;
-                        float u = 0.f;
-                        if (P < n && (s == js || z.win[s] >= 0)) {
-                            int L = P + 1;
-                            for (int q = 0; q < ntouch; ++q)
-                                if (z.tP[q] == P) L = z.tL[q];
-                            if (L >= k + 2)
-                                u = s == js ? R[P] : ld_tagged(&lz_urow(a, K0 + s, z.win[s], G)[P], K0 + s, a.limit_ns, ok);
-                        }
-                        Us[e] = u;
+                named_bar_sync(1, TW);
+                if (warp == 1) {  // the list of rows with a delayed update, in row order
+                    int cnt = 0;
+                    for (int i0 = 0; i0 < nr; i0 += 32) {
+                        const int i = i0 + lane;
+                        const bool has = i < nr && s_li[i] != 0.f;
+                        const unsigned bal = __ballot_sync(0xffffffffu, has);
+                        if (has) s_ul[cnt + __popc(bal & ((1u << lane) - 1u))] = i;
+                        cnt += __popc(bal);
                     }
-                    named_bar_sync(1, TW);
-                    for (int e = tw; e < nr * LZ_CH; e += TW) {
-                        const int i = e / LZ_CH, cc = e % LZ_CH, P = cc0 + cc;
-                        if (P >= n || s_li[i] == 0.f) continue;
-                        float* ri = rows + (size_t)i * ldr;
-                        float x = ri[P];
-                        for (int s = 0; s < nsd; ++s) {
-                            const float w = s_lm[i][s];
-                            if (w != 0.f) x = fmaf(-w, Us[s * LZ_CH + cc], x);
-                        }
-                        ri[P] = x;
-                    }
-                    named_bar_sync(1, TW);
+                    if (lane == 0) s_nu = cnt;
                 }
+                named_bar_sync(1, TW);
+                bool ok = true;
+                if (a.ring >= 16)
+                    lz_panel_update<16>(a, rows, ldr, n, k, K0, js, G, R, z, s_lm, s_ul, s_nu, ring, tw, TW, ok);
+                else if (a.ring >= 8)
+                    lz_panel_update<8>(a, rows, ldr, n, k, K0, js, G, R, z, s_lm, s_ul, s_nu, ring, tw, TW, ok);
+                else
+                    lz_panel_update<4>(a, rows, ldr, n, k, K0, js, G, R, z, s_lm, s_ul, s_nu, ring, tw, TW, ok);
+                named_bar_sync(1, TW);
                 if (!ok) atomicCAS(a.err, 0, (int)LHL_ERR_TIMEOUT);
                 // move the touched positions: row i's value at P goes to L - 1 (at most 2 LZ_NB + 2
                 // of them: two per lane)
@@ -582,8 +709,10 @@ __global__ void __launch_bounds__(MT, 1) reduce_mixed_lazy_kernel(MixArgs a)
                     z.ntouch = 0;
                     z.K0 = k + 1;
                 }
+                if (t == 32) mark(9);
             }
             if (k + 1 <= n - 2) prefetch_cval(k + 1);
+            if (t == 32) mark(10);
         }
     }
     __syncthreads();
@@ -601,9 +730,21 @@ __global__ void __launch_bounds__(MT, 1) reduce_mixed_lazy_kernel(MixArgs a)
         }
 }
 
-size_t lazy_smem_bytes(int ldr)
+// dynamic shared memory with a panel-update ring of `ring` slots per thread of warps 1-15
+size_t lazy_smem_bytes(int ldr, int ring)
 {
-    return (size_t)ldr * 4 * sizeof(float) + 4 * sizeof(int) + (size_t)LZ_NB * LZ_CH * sizeof(float);
+    return (size_t)ldr * 4 * sizeof(float) + 4 * sizeof(int) + (size_t)(MT - 32) * ring * sizeof(float2);
+}
+
+// the deepest ring (16, 8 or 4 slots) whose shared memory fits beside the kernel's static arrays
+static int lazy_ring(int ldr)
+{
+    cudaFuncAttributes fa;
+    size_t stat = 16 * 1024;
+    if (cudaFuncGetAttributes(&fa, reduce_mixed_lazy_kernel) == cudaSuccess) stat = fa.sharedSizeBytes;
+    for (int r = LZ_RING_MAX; r >= 4; r /= 2)
+        if (lazy_smem_bytes(ldr, r) + stat <= MIX_SMEM_TOTAL) return r;
+    return 0;
 }
 
 cudaError_t launch_reduce_mixed_lazy(MixArgs a, const MixPlan& pl, cudaStream_t st)
@@ -612,8 +753,9 @@ cudaError_t launch_reduce_mixed_lazy(MixArgs a, const MixPlan& pl, cudaStream_t 
     a.rpc = pl.rpc;
     a.ldr = pl.ldr;
     if ((a.n - 1 + LZ_UC) / LZ_UC > LZ_UCMAX) return cudaErrorInvalidValue;
-    const size_t smem = lazy_smem_bytes(pl.ldr);
-    if (smem > MIX_SMEM_MAX) return cudaErrorInvalidValue;
+    a.ring = lazy_ring(pl.ldr);
+    if (a.ring == 0) return cudaErrorInvalidValue;
+    const size_t smem = lazy_smem_bytes(pl.ldr, a.ring);
     static size_t attr = 0;
     if (smem > attr) {
         cudaError_t e = cudaFuncSetAttribute(reduce_mixed_lazy_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
