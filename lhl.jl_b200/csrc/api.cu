@@ -434,6 +434,7 @@ static int reduce_loaded(lhl_ws_t ws, int balance, cudaStream_t st)
         }
         if (e == cudaSuccess) e = lhl::launch_linv((int)n, ws->F, (int)n, ws->linv, st);
         if (e != cudaSuccess) return LHL_ERR_CUDA;
+        if (lazy) return cuda_status(lhl::launch_lazy_finish((int)n, ws->F, ws->Ht, st));
         return cuda_status(lhl::launch_ht_fill((int)n, ws->F, ws->Ht, st));
     }
     const int mode = n <= 2 ? 0 : (n < 500 ? 1 : 2);

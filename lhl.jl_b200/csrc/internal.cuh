@@ -146,6 +146,8 @@ constexpr int MIX_LAZY_RING = 18;
 // panel so far (MIX_LAZY_LM words)
 constexpr int MIX_LAZY_LM = 16;
 cudaError_t launch_reduce_mixed_lazy(MixArgs a, const MixPlan& pl, cudaStream_t st);
+// after it: Ht, plus the deferred right updates of the rows above each panel (factors and Ht)
+cudaError_t launch_lazy_finish(int n, double* F, double* Ht, cudaStream_t st);
 
 cudaError_t launch_reduce(RedArgs a, int balance, int mode, cudaStream_t st);
 cudaError_t launch_unblocked_assemble(int n, double* A, const double* B2, const int64_t* ipiv, cudaStream_t st);

@@ -179,6 +179,8 @@ __global__ void __launch_bounds__(MT, 1) reduce_mixed_lazy_kernel(MixArgs a)
     __shared__ float s_piv;
     __shared__ int s_ul[MIX_RPC_MAX];  // panel end: own rows with a delayed update
     __shared__ int s_nu;
+    __shared__ int s_act[MIX_RPC_MAX];  // own rows below the panel's first step (logical label > K0)
+    __shared__ int s_nact;
 
     const int n = a.n, rpc = a.rpc, ldr = a.ldr, G = gridDim.x, b = blockIdx.x;
     const int ldrr = ldr + LZ_NB;  // words per CTA in a ring slot
@@ -210,10 +212,16 @@ __global__ void __launch_bounds__(MT, 1) reduce_mixed_lazy_kernel(MixArgs a)
     if (t == 0) {
         z.ntouch = 0;
         z.K0 = 1;
+        int c = 0;
+        for (int i = 0; i < nr; ++i)
+            if (r0 + i + 1 > 1) s_act[c++] = i;
+        s_nact = c;
     }
     __syncthreads();
 
-    auto prefetch_cval = [&](int st) {  // warps 1-15: column values of step st by logical row
+    // warps 1-15: column values of step st by logical row, of the rows with labels > kmin (the
+    // rows above the panel publish none)
+    auto prefetch_cval = [&](int st, int kmin) {
         constexpr int PF = 8;
         const unsigned long long* cv = a.cval + (size_t)(st & 1) * n;
         const unsigned want = (unsigned)st & 0xffffu;
@@ -223,12 +231,12 @@ __global__ void __launch_bounds__(MT, 1) reduce_mixed_lazy_kernel(MixArgs a)
 #pragma unroll
             for (int u = 0; u < PF; ++u) {
                 const int q = base + u * (MT - 32);
-                w[u] = q < n ? ld_relaxed_u64(&cv[q]) : 0ull;
+                w[u] = (q < n && lg[q] > kmin) ? ld_relaxed_u64(&cv[q]) : 0ull;
             }
 #pragma unroll
             for (int u = 0; u < PF; ++u) {
                 const int q = base + u * (MT - 32);
-                if (q < n) {
+                if (q < n && lg[q] > kmin) {
                     float v = __uint_as_float((unsigned)(w[u] >> 32));
                     if (((unsigned)(w[u] >> 16) & 0xffffu) != want) v = ok ? ld_tagged(&cv[q], (unsigned)st, a.limit_ns, ok) : 0.f;
                     lv[lg[q] - 1] = v;
@@ -248,7 +256,7 @@ __global__ void __launch_bounds__(MT, 1) reduce_mixed_lazy_kernel(MixArgs a)
     };
 
     // ---- publish step 1: column 1 values, candidate among logical rows >= 2 ----
-    if (warp != 0) prefetch_cval(1);
+    if (warp != 0) prefetch_cval(1, 1);
     if (warp == 0) {
         float bv = 0.f;
         int bi = 0, bl = -1;
@@ -366,6 +374,7 @@ __global__ void __launch_bounds__(MT, 1) reduce_mixed_lazy_kernel(MixArgs a)
         const int win = s_win;
         const float piv = s_piv;
         const int K0 = z.K0;
+        const int nact = s_nact;  // own rows below K0 (the rows above wait for the deferred product)
         const int js = k - K0;  // this step's index in the panel
         const bool last = (js == LZ_NB - 1) || (k == n - 2);  // the panel ends with this step
         // ---- interchange k+1 <-> p: row labels, and the column table (no data moves) ----
@@ -447,7 +456,7 @@ __global__ void __launch_bounds__(MT, 1) reduce_mixed_lazy_kernel(MixArgs a)
         const int c0 = K0;
         const int nuc = (n - c0 + LZ_UC - 1) / LZ_UC;
         {
-            const int nv = nr + 1;  // own rows, then R
+            const int nv = nact + 1;  // own rows below the panel's first step, then R
             const int c4 = (c0 + 3) & ~3;
             const int g0 = c4 >> 2, g1 = ldr >> 2;
             const int per = (g1 - g0 + 3) >> 2;
@@ -493,8 +502,8 @@ __global__ void __launch_bounds__(MT, 1) reduce_mixed_lazy_kernel(MixArgs a)
                 const float* xq[4];
 #pragma unroll
                 for (int q = 0; q < 4; ++q) {
-                    const int v = min(rg * 4 + q, nr);
-                    xq[q] = v < nr ? rows + (size_t)v * ldr : R;
+                    const int v = min(rg * 4 + q, nact);
+                    xq[q] = v < nact ? rows + (size_t)s_act[v] * ldr : R;
                 }
                 double acc[4] = {0.0, 0.0, 0.0, 0.0};
                 if (cp == 0) {
@@ -595,7 +604,7 @@ __global__ void __launch_bounds__(MT, 1) reduce_mixed_lazy_kernel(MixArgs a)
                         x = 0.0;
                         for (int ch = 0; ch < nuc; ++ch) x += z.gp[s][ch];
                     } else {
-                        x = dot(nr);
+                        x = dot(nact);
                     }
                 } else {
                     x = s < js ? (double)z.vcol[s] : (double)R[pk1];
@@ -618,11 +627,12 @@ __global__ void __launch_bounds__(MT, 1) reduce_mixed_lazy_kernel(MixArgs a)
             int bi = 0, bl = -1;
             const int np = (k + 1) & 1;
             const int pk = z.pk;
-            for (int i = lane; i < nr; i += 32) {
+            for (int q = lane; q < nact; q += 32) {  // rows above the panel take no step
+                const int i = s_act[q];
                 float* ri = rows + (size_t)i * ldr;
                 const int L = lg[r0 + i];
                 const float li = L >= k + 2 ? lv[L - 1] : 0.f;
-                double cn = (double)ri[pk1] + dot(i);
+                double cn = (double)ri[pk1] + dot(q);
                 for (int s = 0; s < js; ++s) {
                     const float lm = s_lm[i][s];
                     if (lm != 0.f) cn -= (double)lm * z.Gam[s];
@@ -678,6 +688,16 @@ __global__ void __launch_bounds__(MT, 1) reduce_mixed_lazy_kernel(MixArgs a)
                         cnt += __popc(bal);
                     }
                     if (lane == 0) s_nu = cnt;
+                    // the rows below the next panel's first step k + 1 (labels are final for step k)
+                    cnt = 0;
+                    for (int i0 = 0; i0 < nr; i0 += 32) {
+                        const int i = i0 + lane;
+                        const bool has = i < nr && lg[r0 + i] > k + 1;
+                        const unsigned bal = __ballot_sync(0xffffffffu, has);
+                        if (has) s_act[cnt + __popc(bal & ((1u << lane) - 1u))] = i;
+                        cnt += __popc(bal);
+                    }
+                    if (lane == 0) s_nact = cnt;
                 }
                 named_bar_sync(1, TW);
                 bool ok = true;
@@ -711,7 +731,7 @@ __global__ void __launch_bounds__(MT, 1) reduce_mixed_lazy_kernel(MixArgs a)
                 }
                 if (t == 32) mark(9);
             }
-            if (k + 1 <= n - 2) prefetch_cval(k + 1);
+            if (k + 1 <= n - 2) prefetch_cval(k + 1, last ? k + 1 : K0);
             if (t == 32) mark(10);
         }
     }
@@ -766,6 +786,141 @@ cudaError_t launch_reduce_mixed_lazy(MixArgs a, const MixPlan& pl, cudaStream_t 
     void* args[] = {&a};
     return cudaLaunchCooperativeKernel((const void*)reduce_mixed_lazy_kernel, dim3(pl.grid), dim3(MT), args, smem,
                                        st);
+}
+
+}  // namespace lhl
+
+namespace lhl {
+
+// ---- the deferred right updates of the rows above each panel ----------------------------
+// The panel-delayed kernel leaves out of every step the rows whose logical label is at most the
+// panel's first step K0 (the reference's rows 1:k0, whose right updates F:1588-1672 delays to the
+// panel end as its top GEMM).  Nothing in the elimination reads those rows' later columns: after
+// a row rises above a panel only the right updates A[:, c] += A[:, c+1:n] l_(c-1) still change
+// it, one column per step, from its stored values.  So the kernel writes them unchanged, and
+// row r (0-based) receives, for every column q >= qmin(r) = 1 + 16 ceil(r / 16),
+//     H[r, q] = F[r, q] + sum_{p > q} F[r, p] F[p, q - 1]
+// with F the written factors: the stored values in the upper part and the multipliers of
+// column q - 1 below its subdiagonal (final row order on both sides, as the similarity keeps).
+// One product of the upper part with the unit lower factor, here on the FP64 tensor pipe
+// (mma.sync m8n8k4: FP64 products and sums), added into Ht at the transposed positions; then
+// the same entries are copied back into the factors' upper part.
+constexpr int TPM = 64, TPN = 64, TPK = 32, TPT = 128;
+struct TopSmem {
+    double A[2][TPK][TPM + 4];  // F[r, p]: [k][row]
+    double B[2][TPK][TPN + 4];  // F[p, q - 1], zero unless p > q: [k][column]
+};
+
+__device__ __forceinline__ int top_qmin(int r) { return 1 + LZ_NB * ((r + LZ_NB - 1) / LZ_NB); }
+
+__global__ void __launch_bounds__(TPT) lz_top_kernel(int n, const double* __restrict__ F, double* __restrict__ Ht)
+{
+    extern __shared__ __align__(16) unsigned char top_raw[];
+    TopSmem& sm = *reinterpret_cast<TopSmem*>(top_raw);
+    const int r0 = blockIdx.y * TPM, q0 = blockIdx.x * TPN;
+    if (r0 >= n || q0 >= n || q0 + TPN - 1 < top_qmin(r0)) return;  // nothing deferred in this tile
+    const int t = threadIdx.x, lane = t & 31, warp = t >> 5;
+    const int wm = warp & 1, wn = warp >> 1;  // warp tile: rows 32 wm .., columns 32 wn ..
+    const int g = lane >> 2, t4 = lane & 3;
+    double acc[4][4][2];
+#pragma unroll
+    for (int x = 0; x < 4; ++x)
+#pragma unroll
+        for (int y = 0; y < 4; ++y) acc[x][y][0] = acc[x][y][1] = 0.0;
+    const int pbeg = q0 + 1;  // the smallest p any column of the tile takes
+    const int nch = (n - pbeg + TPK - 1) / TPK;
+    auto stage = [&](int kc, int st) {
+        const int pk = pbeg + kc * TPK;
+        for (int e = t; e < TPK * TPM; e += TPT) {
+            const int m = e % TPM, kk = e / TPM;
+            const int r = r0 + m, p = pk + kk;
+            const bool ok = r < n && p < n;
+            cp_async8(&sm.A[st][kk][m], ok ? &F[(size_t)p * n + r] : F, ok, F);
+        }
+        for (int e = t; e < TPK * TPN; e += TPT) {
+            const int kk = e % TPK, j = e / TPK;
+            const int p = pk + kk, q = q0 + j;
+            const bool ok = p < n && q < n && q >= 1 && p > q;  // the multipliers of column q - 1 below row q
+            cp_async8(&sm.B[st][kk][j], ok ? &F[(size_t)(q - 1) * n + p] : F, ok, F);
+        }
+        cp_async_commit();
+    };
+    if (nch > 0) stage(0, 0);
+    for (int kc = 0; kc < nch; ++kc) {
+        const int st = kc & 1;
+        if (kc + 1 < nch) {
+            stage(kc + 1, st ^ 1);
+            cp_async_wait<1>();
+        } else {
+            cp_async_wait<0>();
+        }
+        __syncthreads();
+#pragma unroll
+        for (int kk = 0; kk < TPK; kk += 4) {
+            double fa[4], fb[4];
+#pragma unroll
+            for (int x = 0; x < 4; ++x) fa[x] = sm.A[st][kk + t4][32 * wm + 8 * x + g];
+#pragma unroll
+            for (int y = 0; y < 4; ++y) fb[y] = sm.B[st][kk + t4][32 * wn + 8 * y + g];
+#pragma unroll
+            for (int x = 0; x < 4; ++x)
+#pragma unroll
+                for (int y = 0; y < 4; ++y) dmma_8x8x4(acc[x][y], fa[x], fb[y]);
+        }
+        __syncthreads();
+    }
+    // thread holds D at row 32 wm + 8 x + g, columns 32 wn + 8 y + 2 t4 + {0, 1}
+#pragma unroll
+    for (int x = 0; x < 4; ++x) {
+        const int r = r0 + 32 * wm + 8 * x + g;
+        if (r >= n) continue;
+        const int qm = top_qmin(r);
+#pragma unroll
+        for (int y = 0; y < 4; ++y)
+#pragma unroll
+            for (int h = 0; h < 2; ++h) {
+                const int q = q0 + 32 * wn + 8 * y + 2 * t4 + h;
+                if (q < n && q >= qm) Ht[(size_t)r * n + q] += acc[x][y][h];
+            }
+    }
+}
+
+// F[r, q] = Ht[q, r] at the deferred positions (q >= qmin(r)), 32 x 32 tiles through shared memory
+__global__ void lz_top_copy_kernel(int n, const double* __restrict__ Ht, double* __restrict__ F)
+{
+    __shared__ double tile[32][33];
+    const int rb = blockIdx.y * 32, qb = blockIdx.x * 32;
+    if (qb + 31 < top_qmin(rb)) return;
+    for (int y = threadIdx.y; y < 32; y += blockDim.y) {  // Ht column r = rb + y, rows q = qb + x
+        const int r = rb + y, q = qb + threadIdx.x;
+        tile[y][threadIdx.x] = (r < n && q < n) ? Ht[(size_t)r * n + q] : 0.0;
+    }
+    __syncthreads();
+    for (int y = threadIdx.y; y < 32; y += blockDim.y) {  // F column q = qb + y, rows r = rb + x
+        const int q = qb + y, r = rb + threadIdx.x;
+        if (r < n && q < n && q >= top_qmin(r)) F[(size_t)q * n + r] = tile[threadIdx.x][y];
+    }
+}
+
+// After the panel-delayed kernel: Ht from the factors, the deferred updates added into Ht, and
+// copied back into the factors' upper part.
+cudaError_t launch_lazy_finish(int n, double* F, double* Ht, cudaStream_t st)
+{
+    cudaError_t e = launch_ht_fill(n, F, Ht, st);
+    if (e != cudaSuccess || n < 3) return e;
+    static bool attr = false;
+    if (!attr) {
+        e = cudaFuncSetAttribute(lz_top_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(TopSmem));
+        if (e != cudaSuccess) return e;
+        attr = true;
+    }
+    dim3 grid((n + TPN - 1) / TPN, (n + TPM - 1) / TPM);
+    lz_top_kernel<<<grid, TPT, sizeof(TopSmem), st>>>(n, F, Ht);
+    e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+    dim3 g2((n + 31) / 32, (n + 31) / 32);
+    lz_top_copy_kernel<<<g2, dim3(32, 8), 0, st>>>(n, Ht, F);
+    return cudaGetLastError();
 }
 
 }  // namespace lhl
