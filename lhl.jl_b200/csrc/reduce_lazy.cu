@@ -409,15 +409,16 @@ __global__ void __launch_bounds__(MT, 1) reduce_mixed_lazy_kernel(MixArgs a)
             const unsigned long long* src = win >= 0 ? lz_urow(a, k, win, G) : nullptr;
             const unsigned want = (unsigned)k & 0xffffu;
             bool ok = true;
-            for (int base = K0; base < ldr; base += 4 * MT) {
-                unsigned long long rv[4];
+            constexpr int PU = 8;  // words per thread in flight
+            for (int base = K0; base < ldr; base += PU * MT) {
+                unsigned long long rv[PU];
 #pragma unroll
-                for (int u = 0; u < 4; ++u) {
+                for (int u = 0; u < PU; ++u) {
                     const int P = base + t + u * MT;
                     rv[u] = (src && P < n) ? ld_relaxed_u64(&src[P]) : mix_tag((unsigned)k, 0.f);
                 }
 #pragma unroll
-                for (int u = 0; u < 4; ++u) {
+                for (int u = 0; u < PU; ++u) {
                     const int P = base + t + u * MT;
                     float r = __uint_as_float((unsigned)(rv[u] >> 32));
                     if (src && P < n && ((unsigned)(rv[u] >> 16) & 0xffffu) != want) r = ld_tagged(&src[P], k, a.limit_ns, ok);
@@ -593,30 +594,29 @@ __global__ void __launch_bounds__(MT, 1) reduce_mixed_lazy_kernel(MixArgs a)
         auto dot = [&](int v) {
             return (s_part[4 * v] + s_part[4 * v + 1]) + (s_part[4 * v + 2] + s_part[4 * v + 3]);
         };
-        // ---- the transform: true gamma_s and u_s of the panel's pivot rows, in step order
-        // (thread 0: gamma, thread 1: u), then Gamma = u + gamma ----
-        if (t < 2) {
-            double val[LZ_NB];
-            for (int s = 0; s <= js; ++s) {
-                double x;
-                if (t == 0) {
-                    if (s < js) {
-                        x = 0.0;
-                        for (int ch = 0; ch < nuc; ++ch) x += z.gp[s][ch];
-                    } else {
-                        x = dot(nact);
-                    }
-                } else {
-                    x = s < js ? (double)z.vcol[s] : (double)R[pk1];
-                }
-                for (int tt = 0; tt < s; ++tt) x -= (double)z.T[s][tt] * val[tt];
-                val[s] = x;
+        // ---- the transform: true gamma_s and u_s of the panel's pivot rows, in step order, then
+        // Gamma = u + gamma.  Warp 0, lane s for step s: its V_s . l from the column items (or the
+        // pivot row's dot product), then a forward substitution by columns: once lane s is final
+        // it is broadcast and every later lane subtracts T[r][s] times it (the same terms in the
+        // same order as a row-by-row substitution) ----
+        if (warp == 0) {
+            double g = 0.0, u = 0.0;
+            if (lane < js) {
+                for (int ch = 0; ch < nuc; ++ch) g += z.gp[lane][ch];
+                u = (double)z.vcol[lane];
+            } else if (lane == js) {
+                g = dot(nact);
+                u = (double)R[pk1];
             }
-            if (t == 0)
-                for (int s = 0; s <= js; ++s) z.Gam[s] = val[s];
-            __syncwarp(0x3u);
-            if (t == 1)
-                for (int s = 0; s <= js; ++s) z.Gam[s] += val[s];
+            for (int s2 = 0; s2 < js; ++s2) {
+                const double gs = __shfl_sync(0xffffffffu, g, s2), us = __shfl_sync(0xffffffffu, u, s2);
+                if (lane > s2 && lane <= js) {
+                    const double tr = (double)z.T[lane][s2];
+                    g -= tr * gs;
+                    u -= tr * us;
+                }
+            }
+            if (lane <= js) z.Gam[lane] = g + u;
         }
         __syncthreads();
         if (t == 0) mark(3);
