@@ -194,7 +194,7 @@ class Form:
     """One form of the path on the device for workload w: workspace, the shift object (shared
     between forms when given), solution and residual scratch, and one step."""
 
-    def __init__(self, G, torch, w, form, dev, sh=None):
+    def __init__(self, G, torch, w, form, dev, sh=None, choice=None):
         self.G, self.torch, self.w, self.form = G, torch, w, form
         n, S, R = w["n"], w["S"], w["R"]
         dt = torch.complex128 if w["cplx"] else torch.float64
@@ -205,6 +205,18 @@ class Form:
         self.Rs = torch.empty((S * R, n), dtype=dt, device=dev)
         self.res = torch.empty(S * R, dtype=torch.float64, device=dev)
         self.refine = REFINE[(w["name"], form)]
+        self.choice = None
+        if choice:  # the tuner's choices for this workload (lhl_gpu/tune.py)
+            self.apply(choice)
+
+    def apply(self, choice):
+        sv = choice.get("shift_variant") or [0, 0]
+        self.ws.set_shift_variant(int(sv[0]), int(sv[1]))
+        if self.form == "mixed" and choice.get("mixed_kernel"):
+            self.ws.set_mixed_kernel(int(choice["mixed_kernel"]))
+        if choice.get("refine"):
+            self.refine = tuple(choice["refine"])
+        self.choice = {k: choice[k] for k in ("shift_variant", "mixed_kernel", "refine", "measured") if k in choice}
 
     def reduce(self, Jd):
         self.G.lhl_reduce_(self.ws, Jd, True)
@@ -238,6 +250,67 @@ class Form:
         r = self.refine
         return (f"GMRES-IR: GMRES({r[2]}) x {r[1]} cycles at most, host check per cycle" if r[0] == "gmres"
                 else f"fixed-point lhl_refine_tol, {r[1]} steps at most")
+
+
+def device_name(torch):
+    try:
+        return torch.cuda.get_device_name()
+    except Exception:  # pragma: no cover
+        return "unknown"
+
+
+def cached_choice(torch, w, form):
+    """The tuner's cached choice for workload w and form (lhl_gpu/tuning.json), or None."""
+    from lhl_gpu import tune as T
+    return T.lookup(device_name(torch), w["cplx"], w["n"], form, w["R"])
+
+
+def solves_accepted(w, f):
+    """Every solve at the tolerance (config 3: at the tolerance or at its FP64 floor)."""
+    if w["name"] == "c3":
+        return floor_counts(w, f)["neither"] == 0
+    return bool((f.res.cpu().numpy() <= TOL).all())
+
+
+def tune_config(G, torch, name, cfgs, dev):
+    """Timed trials of the open choices of configuration `name` for both forms (lhl_gpu/tune.py):
+    the mixed reduction kernel, the shift LU's launch shape, the refinement scheme.  Writes the
+    cache and returns the choices."""
+    from lhl_gpu import tune as T
+    w = workload(name, cfgs)
+    Jd = torch.as_tensor(w["J"]).to(dev)
+    Bd = torch.as_tensor(w["B"]).to(dev)
+    sig = torch.as_tensor(w["sigma"]).to(dev)
+    tau = torch.as_tensor(w["tau"]).to(dev)
+    sh = G.LHLShift(w["n"], w["S"], complex=w["cplx"])
+    cache = T.load_cache()
+    out = {}
+    for fm in ("mixed", "plain"):
+        f = Form(G, torch, w, fm, dev, sh)
+        choice = {}
+        if fm == "mixed":
+            choice["mixed_kernel"], choice["kernel_trials"] = T.tune_mixed_kernel(torch, f.ws, lambda: f.reduce(Jd))
+        f.reduce(Jd)
+        v, choice["shift_trials"] = T.tune_shift_variant(G, torch, f.ws, f.sh, sig, tau)
+        choice["shift_variant"] = [0, v] if w["cplx"] else [v, 0]
+        f.ws.set_shift_variant(*choice["shift_variant"])
+
+        def run_chain(ch, f=f):
+            f.refine = tuple(ch)
+            f.chain(Jd, Bd, sig, tau)
+
+        cands = [c for c in T.REFINE_CANDIDATES[fm] if not (w["cplx"] and c[0] == "gmres" and c[2] > 4)]
+        best, choice["refine_trials"] = T.tune_refine(torch, fm, run_chain, lambda f=f: solves_accepted(w, f),
+                                                      candidates=cands)
+        choice["refine"] = list(best) if best else list(REFINE[(name, fm)])
+        key = T.workload_key(device_name(torch), w["cplx"], w["n"], fm, w["R"])
+        T.record(cache, key, choice)
+        out[key] = cache[key]
+        del f
+    T.save_cache(cache)
+    del sh
+    torch.cuda.empty_cache()
+    return out
 
 
 def time_events(torch, stream, fn, reps, flush):
@@ -307,13 +380,14 @@ def config_extra(G, torch, name, cfgs, dev, stream, flush, steps):
     out = {"workload": DESCR[name], "steps": steps, "warmup": 1}
     X_plain = None
     for fm in ("mixed", "plain"):
-        f = Form(G, torch, w, fm, dev, sh)
+        f = Form(G, torch, w, fm, dev, sh, cached_choice(torch, w, fm))
         ms, _ = timed_steps(torch, f, (Jd, Bd, sig, tau), steps, 1, flush, stream)
         red = time_events(torch, stream, lambda: f.reduce(Jd), 2, flush)
         res = f.res.cpu().numpy()
         d = {"value": w["S"] * w["R"] / (ms * 1e-3), "unit": UNIT, "ms_per_step": ms, "reduce_ms": red,
              "chain_ms": ms - red, "max_rel_residual": float(res.max()), "n_at_1e-10": int((res <= TOL).sum()),
-             "solves": int(res.size), "refinement": f.describe_refine()}
+             "solves": int(res.size), "refinement": f.describe_refine(),
+             "tuning": f.choice or "defaults (no cached choice for this device)"}
         fe = forward_errors(w, f.X)
         if fe is not None:
             d["forward_error"] = fe
@@ -486,6 +560,8 @@ def main():
     ap.add_argument("--form", default="mixed", choices=["mixed", "plain"])
     ap.add_argument("--reps", type=int, default=2)
     ap.add_argument("--shifts", type=int, default=0, help="--case: use only the first SHIFTS shifts")
+    ap.add_argument("--tune", default="", help="comma-separated configurations (c1,c2,c3,c5) to tune by timed "
+                                               "trials (lhl_gpu/tune.py); writes lhl_gpu/tuning.json and exits")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3) if args.case is None else args.warmup
     world, rank, local = dist_setup(args.gpus)
@@ -507,6 +583,11 @@ def main():
     stream = torch.cuda.current_stream()
     flush = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.float32, device=dev)
 
+    if args.tune:
+        res = {nm: tune_config(G, torch, nm, cfgs, dev) for nm in args.tune.split(",") if nm}
+        print(json.dumps({"tuned": res}), flush=True)
+        return
+
     w = workload(args.config, cfgs)
     if args.case is not None and args.shifts:
         k = args.shifts
@@ -520,7 +601,7 @@ def main():
     dev_in = (Jd, Bd, sig, tau)
 
     if args.case is not None:  # one phase alone (profiling)
-        f = Form(G, torch, w, args.form, dev)
+        f = Form(G, torch, w, args.form, dev, None, cached_choice(torch, w, args.form))
         f.step(Jd, Bd, sig, tau)
         torch.cuda.synchronize()
         fn = {"reduce": lambda: f.reduce(Jd), "shift": lambda: f.shift(sig, tau), "ldiv": lambda: f.solve(Bd),
@@ -532,8 +613,8 @@ def main():
         return
 
     sh = G.LHLShift(n, S, complex=w["cplx"])
-    mixed = Form(G, torch, w, "mixed", dev, sh)
-    plain = Form(G, torch, w, "plain", dev, sh)
+    mixed = Form(G, torch, w, "mixed", dev, sh, cached_choice(torch, w, "mixed"))
+    plain = Form(G, torch, w, "plain", dev, sh, cached_choice(torch, w, "plain"))
     ms_mixed, clk_mixed = timed_steps(torch, mixed, dev_in, args.steps, args.warmup, flush, stream, pg, local)
     res_mixed = mixed.res.cpu().numpy()
     fe_mixed = forward_errors(w, mixed.X)
@@ -558,6 +639,9 @@ def main():
     ph_mixed = phases(mixed)
     ph_plain = phases(plain)
     launches = None if args.no_launch_count else count_launches(torch, lambda: mixed.step(Jd, Bd, sig, tau))
+    mixed_choice = mixed.choice or "defaults (no cached choice for this device)"
+    plain_choice = plain.choice or "defaults (no cached choice for this device)"
+    mixed_refine, plain_refine = mixed.describe_refine(), plain.describe_refine()
 
     # ---- roofline of the dominant kernel: the mixed form's reduction (its launches alone) ----
     # algorithmic bytes: the FP32 GEMV stream 4 n^3 / 3 (every step re-reads the trailing block)
@@ -663,13 +747,15 @@ def main():
                                    "refinement", "l2": "flushed between timed steps (256 MiB write)",
                            "replicas": world},
                 "max_rel_residual": float(res_mixed.max()), "forward_error": fe_mixed,
-                "refinement": mixed_refine_desc(args.config),
+                "refinement": mixed_refine,
                 "plain_fp64": {"value": plain_value, "unit": UNIT, "ms_per_step": ms_plain, "steps": steps_plain,
                                "warmup": 1, "max_rel_residual": float(res_plain.max()), "forward_error": fe_plain,
-                               "phases_ms": ph_plain, "refinement": plain_refine_desc(args.config),
+                               "phases_ms": ph_plain, "refinement": plain_refine,
                                "form": "plain: FP64 throughout, bit-identical reduction and shift LUs",
                                "clocks": clk_plain},
                 "mixed_vs_plain": value / plain_value,
+                "tuning": {"mixed": mixed_choice, "plain": plain_choice,
+                           "cache": "lhl.jl_b200/lhl_gpu/tuning.json (bench.py --tune)"},
                 "phases_ms": ph_mixed,
                 "excluding_reduction": {"mixed": S * R / ((ms_mixed - ph_mixed["reduce"]) * 1e-3),
                                         "plain": S * R / ((ms_plain - ph_plain["reduce"]) * 1e-3), "unit": UNIT,
@@ -692,17 +778,6 @@ def main():
         print(json.dumps(line), flush=True)
     if pg:
         pg.destroy_process_group()
-
-
-def mixed_refine_desc(name):
-    r = REFINE[(name, "mixed")]
-    return (f"GMRES-IR, GMRES({r[2]}) x {r[1]} cycles at most" if r[0] == "gmres"
-            else f"fixed-point lhl_refine_tol, {r[1]} steps at most")
-
-
-def plain_refine_desc(name):
-    r = REFINE[(name, "plain")]
-    return f"fixed-point lhl_refine_tol, {r[1]} steps at most"
 
 
 def batched_c4(G, torch, cfgs, dev, stream, flush, world, rank):

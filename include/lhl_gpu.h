@@ -94,6 +94,17 @@ int lhl_ws_set_probes(lhl_ws_t ws, int on);
  * updates once per panel); 1: the eager kernel at every order; 2: the panel-delayed kernel at
  * every order.  Both give a similarity J = Z H Z^-1 to FP32 accuracy; their roundings differ. */
 int lhl_ws_set_mixed_kernel(lhl_ws_t ws, int which);
+/* Launch shape of the shift LU for shifts on this workspace (no counterpart in the reference,
+ * which runs one code path per element type, F:2476-2492): 0 (default) picks it by the order;
+ * v >= 1 selects shape v of the real (real_variant) or complex (complex_variant) kernel, as
+ * lhl_shift_variant_shape describes it.  Every shape gives the same bits; only the time differs,
+ * which is what the host-side tuner (lhl_gpu/tune.py) measures.  A shape whose threads x
+ * elements per thread is below the order is LHL_ERR_ARG. */
+int lhl_ws_set_shift_variant(lhl_ws_t ws, int real_variant, int complex_variant);
+/* Shape `variant` (1-based) of the real (is_complex = 0) or complex shift LU kernel: threads per
+ * CTA and pending-row elements per thread (it serves orders n <= threads x per_thread).
+ * LHL_ERR_ARG past the last shape. */
+int lhl_shift_variant_shape(int is_complex, int variant, int* threads, int* per_thread);
 /* Test hook: the wall-time limit of every grid-barrier wait of this workspace's kernels. */
 int lhl_ws_set_barrier_limit_ns(lhl_ws_t ws, uint64_t limit_ns);
 

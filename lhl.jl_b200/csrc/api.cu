@@ -35,6 +35,7 @@ struct lhl_ws_s {
     size_t f32x_cap;
     int cj;        // LHLWorkspace{ComplexF64}: F, Ht, buf2 interleaved complex (cplxj.cu)
     int mix_kernel;  // mixed form: 0 by the plan (rows on chip: eager, else panel-delayed), 1 eager, 2 panel-delayed
+    int shift_variant[2];  // launch shape of the real / complex shift LU (0: by order; lhl_ws_set_shift_variant)
 };
 
 struct lhl_shift_s {
@@ -274,6 +275,31 @@ int lhl_ws_set_mixed_kernel(lhl_ws_t ws, int which)
     if (!ws) return LHL_ERR_ARG;
     if (which < 0 || which > 2) return LHL_ERR_ARG;
     ws->mix_kernel = which;
+    return LHL_OK;
+}
+
+int lhl_ws_set_shift_variant(lhl_ws_t ws, int real_variant, int complex_variant)
+{
+    if (!ws) return LHL_ERR_ARG;
+    int T, E, D;
+    if (real_variant < 0 || (real_variant > 0 && (!lhl::shift_shape(real_variant, &T, &E, &D) || T * E < ws->n)))
+        return LHL_ERR_ARG;
+    if (complex_variant < 0 ||
+        (complex_variant > 0 && (!lhl::shift_shape_cplx(complex_variant, &T, &E) || T * E < ws->n)))
+        return LHL_ERR_ARG;
+    ws->shift_variant[0] = real_variant;
+    ws->shift_variant[1] = complex_variant;
+    return LHL_OK;
+}
+
+int lhl_shift_variant_shape(int is_complex, int variant, int* threads, int* per_thread)
+{
+    if (!threads || !per_thread) return LHL_ERR_ARG;
+    int T, E, D;
+    const int ok = is_complex ? lhl::shift_shape_cplx(variant, &T, &E) : lhl::shift_shape(variant, &T, &E, &D);
+    if (!ok) return LHL_ERR_ARG;
+    *threads = T;
+    *per_thread = E;
     return LHL_OK;
 }
 
@@ -554,11 +580,11 @@ static int shift_run(lhl_shift_t sh, lhl_ws_t ws, int64_t s0, int64_t count, cud
     if (sh->cplx) {
         e = lhl::launch_shift_lu_cplx((int)ws->n, ws->Ht, (int)ws->n, sh->sigma + 2 * s0, sh->tau + 2 * s0, (int)s0,
                                       (int)count, sh->Gt, (int)sh->ldg, (int)sh->po, sh->swap, sh->rdiag, sh->info, st,
-                                      ws->cj);
+                                      ws->cj, ws->shift_variant[1]);
         return cuda_status(e);
     }
     e = lhl::launch_shift_lu((int)ws->n, ws->Ht, (int)ws->n, sh->sigma + s0, sh->tau + s0, (int)s0, (int)count,
-                             sh->Gt, (int)sh->ldg, sh->swap, sh->rdiag, sh->info, st, ws->f32);
+                             sh->Gt, (int)sh->ldg, sh->swap, sh->rdiag, sh->info, st, ws->f32, ws->shift_variant[0]);
     if (e == cudaSuccess && ws->precision == LHL_PREC_MIXED)
         e = lhl::launch_uinv((int)ws->n, sh->Gt, (int)sh->ldg, sh->rdiag, (int)s0, (int)count, sh->uinv, st);
     return cuda_status(e);

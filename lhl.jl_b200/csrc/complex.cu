@@ -153,9 +153,22 @@ __global__ void __launch_bounds__(T, 1) shift_lu_cplx_kernel(int n, const double
     }
 }
 
+// Launch shapes of the complex shift LU (threads T, elements per thread E), selectable per
+// workspace like the real ones (same bits for every shape); shape v serves n <= T E.
+static const int kCShiftShapes[][2] = {{256, 1}, {512, 2}, {512, 4}, {512, 8}, {1024, 8}, {1024, 2}, {1024, 4}, {256, 4}};
+constexpr int kNumCShiftShapes = sizeof(kCShiftShapes) / sizeof(kCShiftShapes[0]);
+
+int shift_shape_cplx(int variant, int* T, int* E)
+{
+    if (variant < 1 || variant > kNumCShiftShapes) return 0;
+    *T = kCShiftShapes[variant - 1][0];
+    *E = kCShiftShapes[variant - 1][1];
+    return 1;
+}
+
 cudaError_t launch_shift_lu_cplx(int n, const double* Ht, int ldh, const double* sig, const double* tau, int s0,
                                  int count, double* Gt, int ldg, int po, uint8_t* swp, double* rd, int32_t* info,
-                                 cudaStream_t st, int ht_complex)
+                                 cudaStream_t st, int ht_complex, int variant)
 {
     if (count <= 0 || n <= 0) return cudaSuccess;
 #define L_(T, E)                                                                                                  \
@@ -166,6 +179,22 @@ cudaError_t launch_shift_lu_cplx(int n, const double* Ht, int ldh, const double*
             shift_lu_cplx_kernel<T, E, double><<<count, T, 0, st>>>(n, Ht, ldh, sig, tau, s0, Gt, ldg, po, swp, rd,  \
                                                                     info);                                        \
     } while (0)
+    if (variant > 0) {
+        int T, E;
+        if (!shift_shape_cplx(variant, &T, &E) || T * E < n) return cudaErrorInvalidValue;
+        switch (variant) {
+            case 1: L_(256, 1); break;
+            case 2: L_(512, 2); break;
+            case 3: L_(512, 4); break;
+            case 4: L_(512, 8); break;
+            case 5: L_(1024, 8); break;
+            case 6: L_(1024, 2); break;
+            case 7: L_(1024, 4); break;
+            case 8: L_(256, 4); break;
+            default: return cudaErrorInvalidValue;
+        }
+        return cudaGetLastError();
+    }
     if (n <= 256) L_(256, 1);
     else if (n <= 1024) L_(512, 2);
     else if (n <= 2048) L_(512, 4);

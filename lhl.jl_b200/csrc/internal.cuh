@@ -163,9 +163,14 @@ bool make_tmap_2d(void* tmap, const double* base, int rows, int cols, int ld, in
 int reduce_grid_size();
 
 // f32 = 1: the elimination in float arithmetic (LHLWorkspace{Float32}); Ht holds float values
+// variant > 0: launch shape `variant` of the table in shift.cu (shift_shape), else by order
 cudaError_t launch_shift_lu(int n, const double* Ht, int ldh, const double* sig, const double* tau, int s0, int count,
                             double* Gt, int ldg, uint8_t* swp, double* rd, int32_t* info, cudaStream_t st,
-                            int f32 = 0);
+                            int f32 = 0, int variant = 0);
+// launch shape `variant` (1-based) of the real / complex shift LU: threads T, elements per thread
+// E (and rows in flight D for the real one); 0 when there is no such variant
+int shift_shape(int variant, int* T, int* E, int* D);
+int shift_shape_cplx(int variant, int* T, int* E);
 
 cudaError_t launch_ldiv(const LdivArgs& a, int nrhs, cudaStream_t st);
 cudaError_t launch_linv(int n, const double* F, int ldf, double* linv, cudaStream_t st);
@@ -179,7 +184,7 @@ cudaError_t launch_solve_batch(const BatchDesc& d, const double* J, const double
 // ht_complex = 1: Ht of a complex reduction (interleaved complex, ld ldh complex elements)
 cudaError_t launch_shift_lu_cplx(int n, const double* Ht, int ldh, const double* sig, const double* tau, int s0,
                                  int count, double* Gt, int ldg, int po, uint8_t* swp, double* rd, int32_t* info,
-                                 cudaStream_t st, int ht_complex = 0);
+                                 cudaStream_t st, int ht_complex = 0, int variant = 0);
 cudaError_t launch_hess_cplx(int n, const double* Gt, int ldg, int po, const uint8_t* swp, const double* rd,
                              double* Y, int ldy, int col0, int count, int rhs_per_shift, const double* done,
                              double tol, cudaStream_t st);

@@ -198,10 +198,40 @@ static cudaError_t launch_shift_T(int n, const double* Ht, int ldh, const double
     return cudaGetLastError();
 }
 
+// Launch shapes of the real shift LU (threads T, elements per thread E, rows of H in flight D),
+// selectable per workspace (lhl_ws_set_shift_variant) so that a tuner can time them; every shape
+// runs the same operations in the same order, so all give the same bits.  Shape v serves orders
+// n <= T E.  Variant 0 is the rule by order below.
+static const int kShiftShapes[][3] = {{256, 1, 4}, {512, 2, 4}, {512, 4, 4}, {512, 8, 2}, {1024, 8, 1},
+                                      {1024, 16, 1}, {1024, 2, 4}, {1024, 4, 2}, {256, 4, 4}, {256, 8, 2}};
+constexpr int kNumShiftShapes = sizeof(kShiftShapes) / sizeof(kShiftShapes[0]);
+
+int shift_shape(int variant, int* T, int* E, int* D)
+{
+    if (variant < 1 || variant > kNumShiftShapes) return 0;
+    *T = kShiftShapes[variant - 1][0];
+    *E = kShiftShapes[variant - 1][1];
+    *D = kShiftShapes[variant - 1][2];
+    return 1;
+}
+
 cudaError_t launch_shift_lu(int n, const double* Ht, int ldh, const double* sig, const double* tau, int s0, int count,
-                            double* Gt, int ldg, uint8_t* swp, double* rd, int32_t* info, cudaStream_t st, int f32)
+                            double* Gt, int ldg, uint8_t* swp, double* rd, int32_t* info, cudaStream_t st, int f32,
+                            int variant)
 {
     if (count <= 0 || n <= 0) return cudaSuccess;
+    if (variant > 0) {
+        int T, E, D;
+        if (!shift_shape(variant, &T, &E, &D) || T * E < n) return cudaErrorInvalidValue;
+#define V_(k, T_, E_, D_) \
+    case k: return launch_shift_T<T_, E_, D_>(n, Ht, ldh, sig, tau, s0, count, Gt, ldg, swp, rd, info, st, f32);
+        switch (variant) {
+            V_(1, 256, 1, 4) V_(2, 512, 2, 4) V_(3, 512, 4, 4) V_(4, 512, 8, 2) V_(5, 1024, 8, 1)
+            V_(6, 1024, 16, 1) V_(7, 1024, 2, 4) V_(8, 1024, 4, 2) V_(9, 256, 4, 4) V_(10, 256, 8, 2)
+            default: return cudaErrorInvalidValue;
+        }
+#undef V_
+    }
     if (n <= 256) return launch_shift_T<256, 1, 4>(n, Ht, ldh, sig, tau, s0, count, Gt, ldg, swp, rd, info, st, f32);
     if (n <= 1024) return launch_shift_T<512, 2, 4>(n, Ht, ldh, sig, tau, s0, count, Gt, ldg, swp, rd, info, st, f32);
     if (n <= 2048) return launch_shift_T<512, 4, 4>(n, Ht, ldh, sig, tau, s0, count, Gt, ldg, swp, rd, info, st, f32);

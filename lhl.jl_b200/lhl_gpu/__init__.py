@@ -71,6 +71,8 @@ def _load():
         "lhl_ws_check": [vp, vp],
         "lhl_ws_set_barrier_limit_ns": [vp, C.c_uint64],
         "lhl_ws_set_mixed_kernel": [vp, i32],
+        "lhl_ws_set_shift_variant": [vp, i32, i32],
+        "lhl_shift_variant_shape": [i32, i32, C.POINTER(C.c_int), C.POINTER(C.c_int)],
         "lhl_reduce": [vp, vp, i64, i32, vp],
         "lhl_ws_phase_ns": [vp, C.POINTER(C.c_uint64), vp],
         "lhl_ws_probe_ns": [vp, C.POINTER(C.c_uint64), vp],
@@ -351,6 +353,13 @@ class LHLWorkspace:
             _check(_lib.lhl_ws_set_probes(self._h, 1), "set_probes")
         if self.__dict__.get("_limit_ns") is not None:
             _check(_lib.lhl_ws_set_barrier_limit_ns(self._h, int(self._limit_ns)))
+        if self.__dict__.get("_mixed_kernel"):
+            _check(_lib.lhl_ws_set_mixed_kernel(self._h, int(self._mixed_kernel)), "set_mixed_kernel")
+        sv = self.__dict__.get("_shift_variant")
+        if sv:  # launch shapes chosen for the old order serve the new one only if they still cover it
+            rv = sv[0] if sv[0] in shift_variants(False, n) else 0
+            cv = sv[1] if sv[1] in shift_variants(True, n) else 0
+            self.set_shift_variant(rv, cv)
         return self
 
     def __getattr__(self, name):
@@ -480,6 +489,32 @@ class LHLWorkspace:
     def set_barrier_limit_ns(self, ns: int):
         _check(_lib.lhl_ws_set_barrier_limit_ns(self._h, int(ns)))
         self._limit_ns = int(ns)
+
+    def set_shift_variant(self, real_variant: int = 0, complex_variant: int = 0):
+        """Launch shape of the shift LU for shifts on this workspace (0: by the order; see
+        shift_variants).  Every shape gives the same bits."""
+        _check(_lib.lhl_ws_set_shift_variant(self._h, int(real_variant), int(complex_variant)), "set_shift_variant")
+        self._shift_variant = (int(real_variant), int(complex_variant))
+
+
+def shift_variant_shape(is_complex: bool, variant: int):
+    """(threads, elements per thread) of shift-LU launch shape `variant`, or None past the last."""
+    T, E = C.c_int(), C.c_int()
+    if _lib.lhl_shift_variant_shape(int(bool(is_complex)), int(variant), C.byref(T), C.byref(E)) != LHL_OK:
+        return None
+    return T.value, E.value
+
+
+def shift_variants(is_complex: bool, n: int):
+    """The shift-LU launch shapes (1-based) that serve order n (threads x elements >= n)."""
+    out, v = [], 1
+    while True:
+        sh = shift_variant_shape(is_complex, v)
+        if sh is None:
+            return out
+        if sh[0] * sh[1] >= n:
+            out.append(v)
+        v += 1
 
 
 # ---------------------------------------------------------------------------------------
