@@ -233,6 +233,11 @@ class Form:
         if self.refine[0] == "gmres":
             G.lhl_refine_gmres_(self.X, Jd, Bd, self.sh, self.ws, tol=TOL, max_cycles=self.refine[1],
                                 restart=self.refine[2], rhs_per_shift=R, host_check=True, R=self.Rs, res=self.res)
+        elif self.refine[0] == "hybrid":  # fixed-point steps for the bulk, then GMRES-IR for what is left
+            G.lhl_refine_tol_(self.X, Jd, Bd, self.sh, self.ws, tol=TOL, max_steps=self.refine[1],
+                              rhs_per_shift=R, R=self.Rs, res=self.res)
+            G.lhl_refine_gmres_(self.X, Jd, Bd, self.sh, self.ws, tol=TOL, max_cycles=self.refine[2],
+                                restart=self.refine[3], rhs_per_shift=R, host_check=True, R=self.Rs, res=self.res)
         else:
             G.lhl_refine_tol_(self.X, Jd, Bd, self.sh, self.ws, tol=TOL, max_steps=self.refine[1],
                               rhs_per_shift=R, R=self.Rs, res=self.res)
@@ -248,8 +253,12 @@ class Form:
 
     def describe_refine(self):
         r = self.refine
-        return (f"GMRES-IR: GMRES({r[2]}) x {r[1]} cycles at most, host check per cycle" if r[0] == "gmres"
-                else f"fixed-point lhl_refine_tol, {r[1]} steps at most")
+        if r[0] == "gmres":
+            return f"GMRES-IR: GMRES({r[2]}) x {r[1]} cycles at most, host check per cycle"
+        if r[0] == "hybrid":
+            return (f"{r[1]} fixed-point lhl_refine_tol steps, then GMRES-IR GMRES({r[3]}) x {r[2]} cycles at most "
+                    f"on the columns still above the tolerance")
+        return f"fixed-point lhl_refine_tol, {r[1]} steps at most"
 
 
 def device_name(torch):
@@ -558,6 +567,9 @@ def main():
     ap.add_argument("--case", choices=["reduce", "shift", "ldiv", "step"],
                     help="run one phase of --config's --form alone, --reps times (profiling cases)")
     ap.add_argument("--form", default="mixed", choices=["mixed", "plain"])
+    ap.add_argument("--mixed-kernel", type=int, default=0, choices=[0, 1, 2],
+                    help="--case, mixed form: 1 the eager FP32 reduction kernel, 2 the panel-delayed one "
+                         "(0: the cached choice)")
     ap.add_argument("--reps", type=int, default=2)
     ap.add_argument("--shifts", type=int, default=0, help="--case: use only the first SHIFTS shifts")
     ap.add_argument("--tune", default="", help="comma-separated configurations (c1,c2,c3,c5) to tune by timed "
@@ -602,6 +614,8 @@ def main():
 
     if args.case is not None:  # one phase alone (profiling)
         f = Form(G, torch, w, args.form, dev, None, cached_choice(torch, w, args.form))
+        if args.mixed_kernel and args.form == "mixed":
+            f.ws.set_mixed_kernel(args.mixed_kernel)
         f.step(Jd, Bd, sig, tau)
         torch.cuda.synchronize()
         fn = {"reduce": lambda: f.reduce(Jd), "shift": lambda: f.shift(sig, tau), "ldiv": lambda: f.solve(Bd),

@@ -141,7 +141,7 @@ int lhl_ws_create(int64_t n, int precision, lhl_ws_t* out)
         }
         const size_t ldr = (size_t)w->mplan.ldr, g = (size_t)w->mplan.grid;
         A_(mhdr, 2 * g);
-        A_(mcval, 2 * (size_t)n);
+        A_(mcval, 2 * (size_t)n + 4 * lhl::MIX_LAZY_LM);  // + the panel-delayed kernel's V_s . l exchange
         // the panel-delayed kernel's ring of candidate rows and global rows are allocated at every
         // order (a test hook can select that kernel where rows would fit on chip)
         A_(mcrow, (size_t)lhl::MIX_LAZY_RING * g * (ldr + lhl::MIX_LAZY_LM));
@@ -427,7 +427,8 @@ static int reduce_loaded(lhl_ws_t ws, int balance, cudaStream_t st)
         // exchange words are tagged with their step: clear the previous reduction's
         if (e == cudaSuccess)
             e = cudaMemsetAsync(ws->mhdr, 0, 2 * (size_t)ws->mplan.grid * sizeof(unsigned long long), st);
-        if (e == cudaSuccess) e = cudaMemsetAsync(ws->mcval, 0, 2 * (size_t)n * sizeof(unsigned long long), st);
+        if (e == cudaSuccess)
+            e = cudaMemsetAsync(ws->mcval, 0, (2 * (size_t)n + 4 * lhl::MIX_LAZY_LM) * sizeof(unsigned long long), st);
         const bool lazy = ws->mix_kernel == 2 || (ws->mix_kernel == 0 && !ws->mplan.smem_rows);
         const size_t ring = lazy ? lhl::MIX_LAZY_RING : 2;
         if (e == cudaSuccess)

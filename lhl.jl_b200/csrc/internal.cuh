@@ -121,7 +121,8 @@ struct MixArgs {
     int64_t* perm;          // out: perm and iperm (1-based), from the final row labels
     int64_t* iperm;
     unsigned long long* hdr;  // 2 x grid: per CTA and step parity, value << 32 | step << 16 | row
-    unsigned long long* cval;  // 2 x n column values by physical row (tagged words)
+    unsigned long long* cval;  // 2 x n column values by physical row (tagged words); the panel-delayed
+                               // kernel's V_s . l exchange follows (4 MIX_LAZY_LM words)
     unsigned long long* crow;  // 2 x grid x ldr candidate rows (tagged words)
     float* grows;           // n x ldr rows when they do not fit in shared memory
     int* err;

@@ -20,8 +20,9 @@
 // transform: U_s = V_s - sum_{t < s} T[s][t] U_t with T[s][t] = l_{w_s}^(t), the multipliers of
 // step s's winning row (the form of a blocked Householder product, here for Gauss transforms).
 // Step k needs (l = the step's multipliers, P the physical column order):
-//   * g_s = V_s . l for the panel's earlier steps and g_k = V_k . l for this step's pivot row
-//     (every CTA takes them, from the ring of published rows), then by the transform
+//   * g_s = V_s . l for the panel's earlier steps (from the owner of each of those rows, for
+//     whom it is one of its rows' dot products) and g_k = V_k . l for this step's pivot row
+//     (every CTA takes it, from the ring of published rows), then by the transform
 //         gamma_s = g_s - sum_{t < s} T[s][t] gamma_t,   u_s = V_s[k+1] - sum_{t < s} T[s][t] u_t;
 //   * the new column k+1 of own row i (the column update A[:, k+1] += A[:, k+2:n] l after the
 //     row update), written into the stored row -- the column is complete from then on:
@@ -51,9 +52,6 @@ constexpr int LZ_NS = MIX_LAZY_RING;    // slots of the ring of published rows
 static_assert(LZ_NS >= LZ_NB + 2, "the ring holds a panel's pivot rows and the next step's candidates");
 constexpr int LZ_TMAX = 2 * LZ_NB + 2;  // column positions a panel's interchanges can touch
 constexpr int LZ_RING_MAX = 16;         // rows in flight per thread in the panel update (cp.async ring)
-constexpr int LZ_UC = 512;              // columns per warp item of the V_s . l products
-constexpr int LZ_UCMAX = 32;            // items per V_s row (n <= 16384)
-constexpr int LZ_UPL = LZ_UC / 32;      // words per lane in flight
 
 struct LazyShared {
     int tP[LZ_TMAX];          // touched physical positions (0-based) ...
@@ -63,7 +61,7 @@ struct LazyShared {
     int win[LZ_NB];           // winning CTA of each panel step
     float T[LZ_NB][LZ_NB];    // T[s][t] = l_{w_s}^(t), t < s
     float vcol[LZ_NB];        // V_s at this step's new column
-    double gp[LZ_NB][LZ_UCMAX];  // V_s . l by column items
+    double gsum[LZ_NB];       // V_s . l of the panel's earlier pivot rows (from their owners)
     double Gam[LZ_NB + 1];    // u_s + gamma_s for s < k, [js]: this step's pivot row's
     int K0;                   // the panel's first step
     int pk, pk1;              // physical positions of logical columns k and k+1
@@ -181,6 +179,7 @@ __global__ void __launch_bounds__(MT, 1) reduce_mixed_lazy_kernel(MixArgs a)
     __shared__ int s_nu;
     __shared__ int s_act[MIX_RPC_MAX];  // own rows below the panel's first step (logical label > K0)
     __shared__ int s_nact;
+    __shared__ int s_pos[MIX_RPC_MAX];  // own row -> its place in s_act (-1: above the panel)
 
     const int n = a.n, rpc = a.rpc, ldr = a.ldr, G = gridDim.x, b = blockIdx.x;
     const int ldrr = ldr + LZ_NB;  // words per CTA in a ring slot
@@ -213,8 +212,13 @@ __global__ void __launch_bounds__(MT, 1) reduce_mixed_lazy_kernel(MixArgs a)
         z.ntouch = 0;
         z.K0 = 1;
         int c = 0;
-        for (int i = 0; i < nr; ++i)
-            if (r0 + i + 1 > 1) s_act[c++] = i;
+        for (int i = 0; i < nr; ++i) {
+            s_pos[i] = -1;
+            if (r0 + i + 1 > 1) {
+                s_pos[i] = c;
+                s_act[c++] = i;
+            }
+        }
         s_nact = c;
     }
     __syncthreads();
@@ -451,11 +455,9 @@ __global__ void __launch_bounds__(MT, 1) reduce_mixed_lazy_kernel(MixArgs a)
 
         // ---- dot products (FP64 accumulation of FP32 products) from the panel's first column:
         // own stored rows and the pivot row in the eager kernel's items (4 rows x one of 4 column
-        // parts per warp, the touched-position fix in part 0); then V_s . l for the panel's
-        // earlier steps, items of LZ_UC columns per warp with every lane's words in flight ----
+        // parts per warp, the touched-position fix in part 0) ----
         const int ntouch = z.ntouch;
         const int c0 = K0;
-        const int nuc = (n - c0 + LZ_UC - 1) / LZ_UC;
         {
             const int nv = nact + 1;  // own rows below the panel's first step, then R
             const int c4 = (c0 + 3) & ~3;
@@ -463,42 +465,7 @@ __global__ void __launch_bounds__(MT, 1) reduce_mixed_lazy_kernel(MixArgs a)
             const int per = (g1 - g0 + 3) >> 2;
             const float4* l4 = reinterpret_cast<const float4*>(lv);
             const int nitems = ((nv + 3) >> 2) * 4;
-            for (int item = warp; item < nitems + js * nuc; item += MW) {
-                if (item >= nitems) {
-                    const int si = (item - nitems) / nuc, ch = (item - nitems) % nuc;
-                    double acc = 0.0;
-                    const int w = z.win[si];
-                    if (w >= 0) {
-                        const unsigned long long* u = lz_urow(a, K0 + si, w, G);
-                        const unsigned want = (unsigned)(K0 + si) & 0xffffu;
-                        bool ok = true;
-                        const int pb = c0 + ch * LZ_UC + lane;
-                        unsigned long long v[LZ_UPL];
-#pragma unroll
-                        for (int j = 0; j < LZ_UPL; ++j) {
-                            const int P = pb + 32 * j;
-                            v[j] = P < n ? ld_relaxed_u64(&u[P]) : 0ull;
-                        }
-#pragma unroll
-                        for (int j = 0; j < LZ_UPL; ++j) {
-                            const int P = pb + 32 * j;
-                            if (P < n) {
-                                float x = __uint_as_float((unsigned)(v[j] >> 32));
-                                if (((unsigned)(v[j] >> 16) & 0xffffu) != want) x = ld_tagged(&u[P], K0 + si, a.limit_ns, ok);
-                                acc += (double)(x * lv[P]);
-                            }
-                        }
-                        if (ch == 0)
-                            for (int q = lane; q < ntouch; q += 32) {
-                                const float x = ld_tagged(&u[z.tP[q]], K0 + si, a.limit_ns, ok);
-                                acc += (double)(x * z.tdl[q]);
-                            }
-                        if (!ok) atomicCAS(a.err, 0, (int)LHL_ERR_TIMEOUT);
-                    }
-                    acc = warp_sum(acc);
-                    if (lane == 0) z.gp[si][ch] = acc;
-                    continue;
-                }
+            for (int item = warp; item < nitems; item += MW) {
                 const int rg = item >> 2, cp = item & 3;
                 const float* xq[4];
 #pragma unroll
@@ -590,19 +557,43 @@ __global__ void __launch_bounds__(MT, 1) reduce_mixed_lazy_kernel(MixArgs a)
             }
         }
         __syncthreads();
-        if (t == 0) mark(2);
         auto dot = [&](int v) {
             return (s_part[4 * v] + s_part[4 * v + 1]) + (s_part[4 * v + 2] + s_part[4 * v + 3]);
         };
+        // ---- V_s . l of the panel's earlier pivot rows: each is still one of its owner's rows
+        // below K0, and in every column where l is not zero its stored values are the ones it
+        // published, so the owner's dot product above is V_s . l.  Owners publish theirs (the
+        // FP64 value as two tagged 32-bit halves, slots by step parity); the others read them ----
+        if (t < js) {
+            unsigned long long* gx = a.cval + 2 * (size_t)n + (size_t)(k & 1) * 2 * LZ_NB;
+            const int w = z.win[t];
+            double g = 0.0;
+            if (w == b) {
+                g = dot(s_pos[ph[K0 + t + 1] - r0]);
+                const unsigned long long bits = (unsigned long long)__double_as_longlong(g);
+                const unsigned long long tag = (unsigned long long)((unsigned)k & 0xffffu) << 16;
+                __stcg(&gx[2 * t], ((bits >> 32) << 32) | tag);
+                __stcg(&gx[2 * t + 1], ((bits & 0xffffffffull) << 32) | tag);
+            } else if (w >= 0) {
+                bool ok = true;
+                const unsigned hi = __float_as_uint(ld_tagged(&gx[2 * t], (unsigned)k, a.limit_ns, ok));
+                const unsigned lo = __float_as_uint(ld_tagged(&gx[2 * t + 1], (unsigned)k, a.limit_ns, ok));
+                if (!ok) atomicCAS(a.err, 0, (int)LHL_ERR_TIMEOUT);
+                g = __longlong_as_double((long long)(((unsigned long long)hi << 32) | lo));
+            }
+            z.gsum[t] = g;
+        }
+        __syncthreads();
+        if (t == 0) mark(2);
         // ---- the transform: true gamma_s and u_s of the panel's pivot rows, in step order, then
-        // Gamma = u + gamma.  Warp 0, lane s for step s: its V_s . l from the column items (or the
-        // pivot row's dot product), then a forward substitution by columns: once lane s is final
+        // Gamma = u + gamma.  Warp 0, lane s for step s: its V_s . l (or the pivot row's dot
+        // product), then a forward substitution by columns: once lane s is final
         // it is broadcast and every later lane subtracts T[r][s] times it (the same terms in the
         // same order as a row-by-row substitution) ----
         if (warp == 0) {
             double g = 0.0, u = 0.0;
             if (lane < js) {
-                for (int ch = 0; ch < nuc; ++ch) g += z.gp[lane][ch];
+                g = z.gsum[lane];
                 u = (double)z.vcol[lane];
             } else if (lane == js) {
                 g = dot(nact);
@@ -698,6 +689,10 @@ __global__ void __launch_bounds__(MT, 1) reduce_mixed_lazy_kernel(MixArgs a)
                         cnt += __popc(bal);
                     }
                     if (lane == 0) s_nact = cnt;
+                    __syncwarp();
+                    for (int i = lane; i < nr; i += 32) s_pos[i] = -1;
+                    __syncwarp();
+                    for (int q = lane; q < cnt; q += 32) s_pos[s_act[q]] = q;
                 }
                 named_bar_sync(1, TW);
                 bool ok = true;
@@ -772,7 +767,6 @@ cudaError_t launch_reduce_mixed_lazy(MixArgs a, const MixPlan& pl, cudaStream_t 
     if (!pl.ok) return cudaErrorInvalidValue;
     a.rpc = pl.rpc;
     a.ldr = pl.ldr;
-    if ((a.n - 1 + LZ_UC) / LZ_UC > LZ_UCMAX) return cudaErrorInvalidValue;
     a.ring = lazy_ring(pl.ldr);
     if (a.ring == 0) return cudaErrorInvalidValue;
     const size_t smem = lazy_smem_bytes(pl.ldr, a.ring);

@@ -9,8 +9,9 @@ the GPU three choices per workload are left open, and this module picks them by 
   * the mixed form's FP32 reduction kernel: rows on chip with a rank-1 update every step
     (the eager kernel) or rows in global memory with rank-16 updates per panel (the
     panel-delayed one); both are similarities to FP32 accuracy, with different roundings;
-  * the refinement: fixed-point lhl_refine_tol with a step cap, or GMRES-IR with restart m and
-    a cycle cap.  A choice counts only if every solve reaches the tolerance (or, where the
+  * the refinement: fixed-point lhl_refine_tol with a step cap, GMRES-IR with restart m and a
+    cycle cap, or a few fixed-point steps followed by GMRES-IR on the columns still above the
+    tolerance.  A choice counts only if every solve reaches the tolerance (or, where the
     caller says so, the FP64 floor of its shift).
 
 A workload is keyed by device name, shift kind (real / complex), order bucket (the next power
@@ -26,9 +27,11 @@ import time
 HERE = os.path.dirname(os.path.abspath(__file__))
 CACHE = os.path.join(HERE, "tuning.json")
 
-# refinement candidates: ("fixed", max steps) or ("gmres", max cycles, restart)
+# refinement candidates: ("fixed", max steps), ("gmres", max cycles, restart), or ("hybrid",
+# fixed-point steps, then GMRES-IR max cycles, restart) for the columns still above the tolerance
 REFINE_CANDIDATES = {
-    "mixed": [("fixed", 16), ("gmres", 8, 2), ("gmres", 6, 3), ("gmres", 4, 4), ("gmres", 12, 8)],
+    "mixed": [("fixed", 16), ("gmres", 8, 2), ("gmres", 6, 3), ("gmres", 4, 4), ("gmres", 12, 8),
+              ("hybrid", 2, 6, 3), ("hybrid", 3, 6, 2)],
     "plain": [("fixed", 4), ("gmres", 4, 3)],
 }
 

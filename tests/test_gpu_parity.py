@@ -322,3 +322,27 @@ def test_barrier_timeout_reports_and_recovers():
     R = O.reduce(J)
     assert np.array_equal(host(ws.ipiv), R.ipiv)
     assert bits_equal(host(ws.factors), R.factors)
+
+
+@pytest.mark.parametrize("n", [300, 600])
+def test_nan_and_inf_inputs_end_with_valid_pivots(n):
+    """A J holding a NaN and an Inf: the reduction (unblocked at n = 300, blocked with TMA GEMV
+    tiles at n = 600) ends without a timeout and leaves only valid interchanges, and the shift
+    and solve that follow run (their values are not finite).  The wait limit is short, so a stall
+    would end as LHL_ERR_TIMEOUT rather than hold the GPU.  Balancing ends on the infinite norm
+    where the reference's _lhl_balance! (F:313-320) would not."""
+    torch, G = _mods()
+    rng = np.random.default_rng(n)
+    J = rng.standard_normal((n, n))
+    J[5, 7] = np.nan
+    J[n - 3, 2] = np.inf
+    ws = G.LHLWorkspace(n, G.LHL_PREC_FP64)
+    ws.set_barrier_limit_ns(500_000_000)
+    G.lhl_reduce_(ws, dev(J), True)
+    ws.check()
+    ip = host(ws.ipiv)[: n - 2]
+    assert ((ip >= np.arange(2, n)) & (ip <= n)).all()
+    G.lhl_shift_(ws, 1.0, -0.05)
+    x = G.lhl_ldiv_(torch.ones(n, dtype=torch.float64, device="cuda"), ws)
+    torch.cuda.synchronize()
+    assert x.shape == (n,)
