@@ -22,6 +22,7 @@ struct lhl_ws_s {
     int ycap;
     int* zflags;   // ldiv scratch: ready flags, ceil(n/64) x ceil(ycap/4)
     int nzflags;
+    int* tailw;    // ldiv scratch: the complex solve's few-groups plan and barrier counters (64 ints)
     // mixed form (LHL_PREC_MIXED) only
     lhl::MixPlan mplan;
     unsigned long long *mhdr, *mcval, *mcrow;
@@ -75,7 +76,7 @@ static void ws_free(lhl_ws_t w)
     if (!w) return;
     void* ptrs[] = {w->F, w->Ht, w->scale, w->iscale, w->B0, w->part, w->tab, w->cand_v, w->cand_s, w->buf2, w->tsnap,
                     w->bsum, w->bfac, w->ipiv, w->perm, w->iperm, w->cand_i, w->bflag, w->err, w->bar,
-                    w->ptimes, w->mhdr, w->mcval, w->mcrow, w->mgrows, w->ybuf, w->zflags, w->linv, w->gmV, w->gmS, w->gmA, w->f32x, w->gmP};
+                    w->ptimes, w->mhdr, w->mcval, w->mcrow, w->mgrows, w->ybuf, w->zflags, w->tailw, w->linv, w->gmV, w->gmS, w->gmA, w->f32x, w->gmP};
     for (void* p : ptrs)
         if (p) cudaFree(p);
     if (w->gmH) cudaFreeHost(w->gmH);
@@ -128,6 +129,7 @@ int lhl_ws_create(int64_t n, int precision, lhl_ws_t* out)
     A_(ybuf, (size_t)n * w->ycap);
     w->nzflags = (int)(((n + 63) / 64) * ((w->ycap + 3) / 4));
     A_(zflags, (size_t)w->nzflags);
+    A_(tailw, 64);
     if (precision == LHL_PREC_MIXED && n >= 3) {
         int dev = 0, sms = 0;
         if (e == cudaSuccess) e = cudaGetDevice(&dev);
@@ -141,7 +143,7 @@ int lhl_ws_create(int64_t n, int precision, lhl_ws_t* out)
         }
         const size_t ldr = (size_t)w->mplan.ldr, g = (size_t)w->mplan.grid;
         A_(mhdr, 2 * g);
-        A_(mcval, 2 * (size_t)n + 4 * lhl::MIX_LAZY_LM);  // + the panel-delayed kernel's V_s . l exchange
+        A_(mcval, 2 * (size_t)n + 8 * lhl::MIX_LAZY_LM);  // + the panel-delayed kernel's pivot-row exchange
         // the panel-delayed kernel's ring of candidate rows and global rows are allocated at every
         // order (a test hook can select that kernel where rows would fit on chip)
         A_(mcrow, (size_t)lhl::MIX_LAZY_RING * g * (ldr + lhl::MIX_LAZY_LM));
@@ -428,7 +430,7 @@ static int reduce_loaded(lhl_ws_t ws, int balance, cudaStream_t st)
         if (e == cudaSuccess)
             e = cudaMemsetAsync(ws->mhdr, 0, 2 * (size_t)ws->mplan.grid * sizeof(unsigned long long), st);
         if (e == cudaSuccess)
-            e = cudaMemsetAsync(ws->mcval, 0, (2 * (size_t)n + 4 * lhl::MIX_LAZY_LM) * sizeof(unsigned long long), st);
+            e = cudaMemsetAsync(ws->mcval, 0, (2 * (size_t)n + 8 * lhl::MIX_LAZY_LM) * sizeof(unsigned long long), st);
         const bool lazy = ws->mix_kernel == 2 || (ws->mix_kernel == 0 && !ws->mplan.smem_rows);
         const size_t ring = lazy ? lhl::MIX_LAZY_RING : 2;
         if (e == cudaSuccess)
@@ -732,6 +734,7 @@ static int ldiv_common(lhl_shift_t sh, lhl_ws_t ws, double* dX, int64_t ldx, int
     a.linv = ws->linv;  // null for the plain form
     a.zflags = ws->zflags;
     a.nzflags = ws->nzflags;
+    a.tail = ws->tailw;
     a.err = ws->err;
     a.limit_ns = ws->limit_ns;
     if (sh) {
@@ -886,6 +889,7 @@ static lhl::LdivArgs refine_ldiv_args(lhl_shift_t sh, lhl_ws_t ws, double* dR, i
     a.ycap = ws->ycap;
     a.zflags = ws->zflags;
     a.nzflags = ws->nzflags;
+    a.tail = ws->tailw;
     a.err = ws->err;
     a.limit_ns = ws->limit_ns;
     return a;

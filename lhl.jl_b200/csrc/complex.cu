@@ -364,13 +364,76 @@ struct MrhsSmem {
     unsigned char FS[MFC];       // forward recurrence: swaps
 };
 
+// the few-groups path of the solve (hess_cplx_tail_kernel, below)
+constexpr int HT_MAX = 16;  // active groups the grid takes on, each on its own share of the CTAs
+constexpr int HT_T = 256;   // threads per CTA
+constexpr int HT_BAR = 32;  // the plan's words for the groups' barrier counters (HT_MAX of them)
+constexpr int HT_WORDS = 64;
+
+// The forward select-swap recurrence (F:2827-2838) of ng <= MG complex right-hand sides of one
+// shift, in place in their scratch columns (part p of right-hand side v: Yg + (2 v + p) ldy):
+// chunks of MFC steps staged in shared memory by the CTA's NT threads, then one thread per
+// right-hand side through the chunk.  Every thread of the CTA calls it.
+template <int NT>
+__device__ __forceinline__ void hess_cplx_forward(int n, const double* __restrict__ Gt, int ldg, int po,
+                                                  const uint8_t* __restrict__ swp, double* Yg, int ldy, int ng,
+                                                  double (&F)[2][MFC + 1][MG], double (&FL)[2][MFC],
+                                                  unsigned char (&FS)[MFC])
+{
+    const int t = threadIdx.x;
+    auto col = [&](int v, int p) { return Yg + (size_t)(2 * v + p) * ldy; };
+    if (n >= 2) {
+        dc c = {0.0, 0.0};
+        if (t < ng) c = {col(t, 0)[0], col(t, 1)[0]};
+        for (int k0 = 1; k0 <= n - 1; k0 += MFC) {
+            const int cnt = min(MFC, n - k0);  // steps k0 .. k0 + cnt - 1
+            // stage y[k] (0-based index k, k = k0 .. k0+cnt-1), l_k and swap_k
+            for (int e = t; e < 2 * MG * MFC; e += NT) {
+                const int i = e % MFC, v = (e / MFC) % MG, p = e / (MFC * MG);
+                F[p][i][v] = (i < cnt && v < ng) ? col(v, p)[k0 + i] : 0.0;
+            }
+            if (t < 2 * MFC) {
+                const int i = t % MFC, p = t / MFC;
+                const int k = k0 + i;
+                FL[p][i] = i < cnt ? M1(Gt, ldg, p * po + k, k + 1) : 0.0;
+            }
+            if (t < MFC) FS[t] = t < cnt ? swp[k0 + t - 1] : 0;
+            __syncthreads();
+            if (t < ng) {
+                for (int i = 0; i < cnt; ++i) {
+                    const dc b = {F[0][i][t], F[1][i][t]};
+                    const bool sw = FS[i] != 0;
+                    const dc xk = sw ? b : c;
+                    F[0][i][t] = xk.re;  // becomes y[k - 1]
+                    F[1][i][t] = xk.im;
+                    const dc lk = {FL[0][i], FL[1][i]};
+                    c = csub(sw ? c : b, cmul(lk, xk));
+                }
+            }
+            __syncthreads();
+            for (int e = t; e < 2 * MG * MFC; e += NT) {  // y[k-1] for k = k0 .. k0+cnt-1
+                const int i = e % MFC, v = (e / MFC) % MG, p = e / (MFC * MG);
+                if (i < cnt && v < ng) col(v, p)[k0 + i - 1] = F[p][i][v];
+            }
+            __syncthreads();
+        }
+        if (t < ng) {
+            col(t, 0)[n - 1] = c.re;
+            col(t, 1)[n - 1] = c.im;
+        }
+        __syncthreads();
+    }
+}
+
 __global__ void __launch_bounds__(MT, 2) hess_cplx_mrhs_kernel(int n, const double* __restrict__ Gt_all, int ldg,
                                                                int po, const uint8_t* __restrict__ swap_all,
                                                                const double* __restrict__ rdiag_all, double* Y,
                                                                int ldy, int col0, int count, int rhs_per_shift,
                                                                int s_first, int groups_per_shift,
-                                                               const double* __restrict__ done, double tol)
+                                                               const double* __restrict__ done, double tol,
+                                                               const int* __restrict__ plan)
 {
+    if (plan && plan[0] <= HT_MAX) return;  // hess_cplx_tail_kernel has the work (or none is left)
     extern __shared__ __align__(16) unsigned char mrhs_raw[];
     MrhsSmem& sm = *reinterpret_cast<MrhsSmem*>(mrhs_raw);
     const int s = s_first + blockIdx.x / groups_per_shift;
@@ -393,47 +456,7 @@ __global__ void __launch_bounds__(MT, 2) hess_cplx_mrhs_kernel(int n, const doub
     auto ycol = [&](int v, int p) -> double* { return Y + (size_t)(2 * (c_lo - col0 + v) + p) * ldy; };
 
     // ---- 1. forward recurrence, chunks of MFC steps: element k (1-based) of the chunk at row k0 + i
-    if (n >= 2) {
-        dc c = {0.0, 0.0};
-        if (t < ng) c = {ycol(t, 0)[0], ycol(t, 1)[0]};
-        for (int k0 = 1; k0 <= n - 1; k0 += MFC) {
-            const int cnt = min(MFC, n - k0);  // steps k0 .. k0 + cnt - 1
-            // stage y[k] (0-based index k, k = k0 .. k0+cnt-1), l_k and swap_k
-            for (int e = t; e < 2 * MG * MFC; e += MT) {
-                const int i = e % MFC, v = (e / MFC) % MG, p = e / (MFC * MG);
-                sm.F[p][i][v] = (i < cnt && v < ng) ? ycol(v, p)[k0 + i] : 0.0;
-            }
-            if (t < 2 * MFC) {
-                const int i = t % MFC, p = t / MFC;
-                const int k = k0 + i;
-                sm.FL[p][i] = i < cnt ? M1(Gt, ldg, p * po + k, k + 1) : 0.0;
-            }
-            if (t < MFC) sm.FS[t] = t < cnt ? swp[k0 + t - 1] : 0;
-            __syncthreads();
-            if (t < ng) {
-                for (int i = 0; i < cnt; ++i) {
-                    const dc b = {sm.F[0][i][t], sm.F[1][i][t]};
-                    const bool sw = sm.FS[i] != 0;
-                    const dc xk = sw ? b : c;
-                    sm.F[0][i][t] = xk.re;  // becomes y[k - 1]
-                    sm.F[1][i][t] = xk.im;
-                    const dc lk = {sm.FL[0][i], sm.FL[1][i]};
-                    c = csub(sw ? c : b, cmul(lk, xk));
-                }
-            }
-            __syncthreads();
-            for (int e = t; e < 2 * MG * MFC; e += MT) {  // y[k-1] for k = k0 .. k0+cnt-1
-                const int i = e % MFC, v = (e / MFC) % MG, p = e / (MFC * MG);
-                if (i < cnt && v < ng) ycol(v, p)[k0 + i - 1] = sm.F[p][i][v];
-            }
-            __syncthreads();
-        }
-        if (t < ng) {
-            ycol(t, 0)[n - 1] = c.re;
-            ycol(t, 1)[n - 1] = c.im;
-        }
-        __syncthreads();
-    }
+    hess_cplx_forward<MT>(n, Gt, ldg, po, swp, ycol(0, 0), ldy, ng, sm.F, sm.FL, sm.FS);
 
     // ---- 2. back substitution
     const int g8 = lane >> 2, t4 = lane & 3;  // mma fragment coordinates
@@ -565,9 +588,200 @@ __global__ void __launch_bounds__(MT, 2) hess_cplx_mrhs_kernel(int n, const doub
     }
 }
 
+// ---- the planar Hessenberg solve when only a few groups of right-hand sides still refine ----
+// After the first refinement steps only the right-hand sides of shifts near the spectrum stay
+// above the tolerance, and one CTA per group (hess_cplx_mrhs_kernel) streams its shift's whole
+// planar Gt at one SM's rate: about 21 ms at n = 8192 however few vectors are left.  With at
+// most HT_MAX groups active, a cooperative grid of one CTA per SM takes them all at once, the
+// CTAs dealt out to the groups (CTA c to group c mod A, at least 9 CTAs per group), each group
+// with its own bounded barrier:
+//   * the forward recurrence of the group (its CTA 0, hess_cplx_forward), then a barrier;
+//   * the back substitution right-looking, in blocks of 32 rows from the bottom, block q owned
+//     by the group's CTA q mod G: the owner solves the block's triangle (rdiag, shuffles, as the
+//     multi-vector kernel does) and a barrier makes x_q visible; then every CTA of the group
+//     subtracts U[i, block q] x_q from the rows i of the blocks it owns above q (a row of U is a
+//     contiguous column of Gt: each lane streams its own row, both planes).  The owner of block
+//     q+1 has that block's rows complete after its own update and solves it: one barrier per
+//     block.
+// hess_tail_plan_kernel counts the active groups first; the multi-vector kernel returns at once
+// when this kernel takes the work, and this one when it does not.  Results agree with the
+// multi-vector kernel's to rounding (the sums run in another order).
+
+__global__ void hess_tail_plan_kernel(int col0, int count, int rhs_per_shift, int s_first, int gps, int ngroups,
+                                      const double* __restrict__ done, double tol, int* __restrict__ plan)
+{
+    __shared__ int s_cnt;
+    __shared__ int s_ids[HT_MAX];
+    if (threadIdx.x == 0) s_cnt = 0;
+    __syncthreads();
+    for (int gid = threadIdx.x; gid < ngroups; gid += blockDim.x) {
+        const int s = s_first + gid / gps, g = gid % gps;
+        const int c_lo = max(col0, s * rhs_per_shift + g * MG);
+        const int c_hi = min(min(col0 + count, (s + 1) * rhs_per_shift), s * rhs_per_shift + g * MG + MG);
+        bool act = false;  // the multi-vector kernel's test: some column not at the tolerance
+        for (int c = c_lo; c < c_hi; ++c) act = act || !(done[c] <= tol);
+        if (act) {
+            const int slot = atomicAdd(&s_cnt, 1);
+            if (slot < HT_MAX) s_ids[slot] = gid;
+        }
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        const int m = min(s_cnt, HT_MAX);
+        for (int i = 1; i < m; ++i)  // ascending, so the groups are taken in a fixed order
+            for (int j = i; j > 0 && s_ids[j - 1] > s_ids[j]; --j) {
+                const int x = s_ids[j];
+                s_ids[j] = s_ids[j - 1];
+                s_ids[j - 1] = x;
+            }
+        plan[0] = s_cnt;
+        for (int i = 0; i < HT_MAX; ++i) plan[1 + i] = i < m ? s_ids[i] : -1;
+        for (int i = 0; i < HT_MAX; ++i) plan[HT_BAR + i] = 0;
+    }
+}
+
+struct TailSmem {
+    double F[2][MFC + 1][MG];   // forward recurrence (CTA 0)
+    double FL[2][MFC];
+    unsigned char FS[MFC];
+    double X[2][MRB][MG];       // x of the block just solved: [part][row][rhs]
+    double T[2][MRB][MRB + 1];  // the diagonal block being solved: [plane][row][col]
+};
+
+__global__ void __launch_bounds__(HT_T, 1) hess_cplx_tail_kernel(int n, const double* __restrict__ Gt_all, int ldg,
+                                                                 int po, const uint8_t* __restrict__ swap_all,
+                                                                 const double* __restrict__ rdiag_all, double* Y,
+                                                                 int ldy, int col0, int count, int rhs_per_shift,
+                                                                 int s_first, int gps, int* plan, int* err,
+                                                                 unsigned long long limit_ns)
+{
+    __shared__ TailSmem sm;
+    __shared__ int s_ok;
+    const int A = plan[0];
+    if (A <= 0 || A > HT_MAX || (int)gridDim.x < A) return;  // the multi-vector kernel has the work
+    const int t = threadIdx.x, lane = t & 31, warp = t >> 5;
+    // CTA blockIdx.x takes group a = blockIdx.x mod A, as CTA b of that group's G CTAs
+    const int a = blockIdx.x % A, b = blockIdx.x / A, G = ((int)gridDim.x - a + A - 1) / A;
+    unsigned int* counter = reinterpret_cast<unsigned int*>(plan + HT_BAR + a);
+    unsigned int seq = 0;
+    // barrier of the group's G CTAs, bounded in wall time like GridBarrier
+    auto group_sync = [&]() -> bool {
+        ++seq;
+        __syncthreads();
+        if (t == 0) {
+            int ok = 1;
+            __threadfence();
+            atomicAdd(counter, 1u);
+            const unsigned int target = seq * (unsigned)G;
+            const uint64_t t0 = globaltimer_ns();
+            unsigned int spins = 0;
+            while (ld_acquire_u32(counter) < target) {
+                if (ld_acquire_i32(err) != 0) { ok = 0; break; }
+                if ((++spins & 63u) == 0 && globaltimer_ns() - t0 > limit_ns) {
+                    atomicCAS(err, 0, (int)LHL_ERR_TIMEOUT);
+                    ok = 0;
+                    break;
+                }
+            }
+            if (ok && ld_acquire_i32(err) != 0) ok = 0;
+            __threadfence();
+            s_ok = ok;
+        }
+        __syncthreads();
+        return s_ok != 0;
+    };
+    const int nq = (n + MRB - 1) / MRB;
+    {
+        const int gid = plan[1 + a];
+        const int s = s_first + gid / gps, g = gid % gps;
+        const int c_lo = max(col0, s * rhs_per_shift + g * MG);
+        const int c_hi = min(min(col0 + count, (s + 1) * rhs_per_shift), s * rhs_per_shift + g * MG + MG);
+        const int ng = c_hi - c_lo;
+        const double* Gt = Gt_all + (size_t)s * ldg * n;
+        const uint8_t* swp = swap_all + (size_t)s * n;
+        const double* rd = rdiag_all + (size_t)s * 2 * n;
+        double* Yg = Y + (size_t)2 * (c_lo - col0) * ldy;
+        auto col = [&](int v, int p) { return Yg + (size_t)(2 * v + p) * ldy; };
+
+        if (b == 0) hess_cplx_forward<HT_T>(n, Gt, ldg, po, swp, Yg, ldy, ng, sm.F, sm.FL, sm.FS);
+        if (!group_sync()) return;
+
+        // the triangle of block q (rows r0 .. r1, 1-based), by its owner: every thread calls it
+        auto solve_block = [&](int q) {
+            const int r1 = n - MRB * q, r0 = max(r1 - MRB + 1, 1), bs = r1 - r0 + 1;
+            for (int e = t; e < 2 * MRB * MRB; e += HT_T) {
+                const int bb = e % MRB, aa = (e / MRB) % MRB, p = e / (MRB * MRB);
+                sm.T[p][aa][bb] = (aa < bs && bb < bs && bb >= aa) ? M1(Gt, ldg, p * po + r0 + bb, r0 + aa) : 0.0;
+            }
+            __syncthreads();
+            if (warp < ng) {  // warp v solves right-hand side v
+                const int v = warp;
+                const int i = r0 + lane;
+                dc yv = {0.0, 0.0}, rdi = {0.0, 0.0};
+                if (i <= r1) {
+                    yv = {col(v, 0)[i - 1], col(v, 1)[i - 1]};
+                    rdi = {rd[2 * (i - 1)], rd[2 * (i - 1) + 1]};
+                }
+                for (int j = r1; j >= r0; --j) {
+                    dc xj = {0.0, 0.0};
+                    if (i == j) {
+                        yv = cmul(yv, rdi);
+                        xj = yv;
+                    }
+                    xj.re = __shfl_sync(0xffffffffu, xj.re, j - r0);
+                    xj.im = __shfl_sync(0xffffffffu, xj.im, j - r0);
+                    if (i < j) yv = csub(yv, cmul(dc{sm.T[0][lane][j - r0], sm.T[1][lane][j - r0]}, xj));
+                }
+                if (i <= r1) {
+                    col(v, 0)[i - 1] = yv.re;
+                    col(v, 1)[i - 1] = yv.im;
+                }
+            }
+            __syncthreads();
+        };
+        if (b == 0) solve_block(0);  // the bottom block has nothing below it
+        if (!group_sync()) return;
+        for (int q = 0; q + 1 < nq; ++q) {
+            const int r1 = n - MRB * q, r0 = max(r1 - MRB + 1, 1), bs = r1 - r0 + 1;
+            for (int e = t; e < 2 * MRB * MG; e += HT_T) {  // x_q, solved by another CTA
+                const int jj = e % MRB, v = (e / MRB) % MG, p = e / (MRB * MG);
+                sm.X[p][jj][v] = (jj < bs && v < ng) ? __ldcg(&col(v, p)[r0 + jj - 1]) : 0.0;
+            }
+            __syncthreads();
+            // this CTA's blocks above q (q' > q, q' = b mod G): warp w takes every (HT_T/32)-th
+            const int first = q + 1 + ((b - (q + 1)) % G + G) % G;
+            for (int qq = first + warp * G; qq < nq; qq += (HT_T / 32) * G) {
+                const int s1 = n - MRB * qq, s0 = max(s1 - MRB + 1, 1);
+                const int i = s0 + lane;  // this lane's row
+                if (i <= s1) {
+                    dc acc[MG];
+#pragma unroll
+                    for (int v = 0; v < MG; ++v) acc[v] = {0.0, 0.0};
+                    const double* ur = &M1(Gt, ldg, r0, i);       // U[i, r0 ..] = Gt[r0 .., i], real plane
+                    const double* ui = &M1(Gt, ldg, po + r0, i);  // and imaginary plane
+                    for (int jj = 0; jj < bs; ++jj) {
+                        const dc u = {ur[jj], ui[jj]};
+#pragma unroll
+                        for (int v = 0; v < MG; ++v) acc[v] = cadd(acc[v], cmul(u, dc{sm.X[0][jj][v], sm.X[1][jj][v]}));
+                    }
+#pragma unroll
+                    for (int v = 0; v < MG; ++v)
+                        if (v < ng) {
+                            col(v, 0)[i - 1] -= acc[v].re;
+                            col(v, 1)[i - 1] -= acc[v].im;
+                        }
+                }
+            }
+            __syncthreads();
+            if (b == (q + 1) % G) solve_block(q + 1);
+            if (!group_sync()) return;
+        }
+    }
+}
+
 cudaError_t launch_hess_cplx_mrhs(int n, const double* Gt, int ldg, int po, const uint8_t* swp, const double* rd,
                                   double* Y, int ldy, int col0, int count, int rhs_per_shift, const double* done,
-                                  double tol, cudaStream_t st)
+                                  double tol, cudaStream_t st, int* tail, int* err, unsigned long long limit_ns)
 {
     if (count <= 0 || n <= 0) return cudaSuccess;
     const int s_first = col0 / rhs_per_shift, s_last = (col0 + count - 1) / rhs_per_shift;
@@ -582,9 +796,30 @@ cudaError_t launch_hess_cplx_mrhs(int n, const double* Gt, int ldg, int po, cons
         if (e != cudaSuccess) return e;
         attr = true;
     }
+    // refinement steps (done given): the few-groups path takes over when at most HT_MAX groups
+    // are left; its plan is counted on the device, so neither launch waits for the host
+    const bool tail_path = done && tail && err;
+    if (tail_path) {
+        hess_tail_plan_kernel<<<1, 256, 0, st>>>(col0, count, rhs_per_shift, s_first, gps, (int)grid, done, tol, tail);
+        cudaError_t e = cudaGetLastError();
+        if (e != cudaSuccess) return e;
+    }
     hess_cplx_mrhs_kernel<<<(unsigned)grid, MT, smem, st>>>(n, Gt, ldg, po, swp, rd, Y, ldy, col0, count,
-                                                             rhs_per_shift, s_first, gps, done, tol);
-    return cudaGetLastError();
+                                                             rhs_per_shift, s_first, gps, done, tol,
+                                                             tail_path ? tail : nullptr);
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess || !tail_path) return e;
+    static int sms = 0;
+    if (!sms) {
+        int dev = 0;
+        e = cudaGetDevice(&dev);
+        if (e == cudaSuccess) e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+        if (e != cudaSuccess) return e;
+    }
+    int sf = s_first, gp = gps;
+    void* args[] = {&n, &Gt, &ldg, &po, &swp, &rd, &Y, &ldy, &col0, &count, &rhs_per_shift, &sf, &gp,
+                    &tail, &err, &limit_ns};
+    return cudaLaunchCooperativeKernel((const void*)hess_cplx_tail_kernel, dim3(sms), dim3(HT_T), args, 0, st);
 }
 
 // ---- complex residual r = b - (sigma_s x + tau_s J x), J real; b, x, r interleaved complex ----

@@ -61,6 +61,7 @@ struct LdivArgs {
     int po;
     int* zflags;          // ldiv scratch: ready flags of the blocked forward substitution
     int nzflags;
+    int* tail;            // ldiv scratch: the complex solve's few-groups plan and barrier counters (64 ints)
     int* err;             // bounded-wait status (the workspace's error word)
     unsigned long long limit_ns;
     int cj;               // complex reduction (LHLWorkspace{ComplexF64}): F interleaved complex (cplxj.cu)
@@ -122,7 +123,7 @@ struct MixArgs {
     int64_t* iperm;
     unsigned long long* hdr;  // 2 x grid: per CTA and step parity, value << 32 | step << 16 | row
     unsigned long long* cval;  // 2 x n column values by physical row (tagged words); the panel-delayed
-                               // kernel's V_s . l exchange follows (4 MIX_LAZY_LM words)
+                               // kernel's pivot-row exchange follows (8 MIX_LAZY_LM words)
     unsigned long long* crow;  // 2 x grid x ldr candidate rows (tagged words)
     float* grows;           // n x ldr rows when they do not fit in shared memory
     int* err;
@@ -190,9 +191,12 @@ cudaError_t launch_hess_cplx(int n, const double* Gt, int ldg, int po, const uin
                              double* Y, int ldy, int col0, int count, int rhs_per_shift, const double* done,
                              double tol, cudaStream_t st);
 // the same solve for groups of right-hand sides of one shift per CTA (rhs_per_shift >= 2)
+// tail (64 ints of scratch), err and limit_ns: the few-groups path of refinement steps (done
+// given); null tail: the multi-vector kernel alone
 cudaError_t launch_hess_cplx_mrhs(int n, const double* Gt, int ldg, int po, const uint8_t* swp, const double* rd,
                                   double* Y, int ldy, int col0, int count, int rhs_per_shift, const double* done,
-                                  double tol, cudaStream_t st);
+                                  double tol, cudaStream_t st, int* tail = nullptr, int* err = nullptr,
+                                  unsigned long long limit_ns = 0);
 cudaError_t launch_residual_cplx(int n, const double* J, int ldj, const double* B, int ldb, const double* X, int ldx,
                                  double* R, int ldr, int nrhs, int rhs_per_shift, const double* sig, const double* tau,
                                  cudaStream_t st, const double* done = nullptr, double tol = 0.0);

@@ -20,9 +20,10 @@
 // transform: U_s = V_s - sum_{t < s} T[s][t] U_t with T[s][t] = l_{w_s}^(t), the multipliers of
 // step s's winning row (the form of a blocked Householder product, here for Gauss transforms).
 // Step k needs (l = the step's multipliers, P the physical column order):
-//   * g_s = V_s . l for the panel's earlier steps (from the owner of each of those rows, for
-//     whom it is one of its rows' dot products) and g_k = V_k . l for this step's pivot row
-//     (every CTA takes it, from the ring of published rows), then by the transform
+//   * g_s = V_s . l and V_s[k+1] for the panel's steps s <= k: each V_s is still one of its
+//     owner's rows, so its owner has both (its own dot product and stored value) and publishes
+//     them, with the row T[k] of this step's winner; nobody else reads the pivot rows during
+//     the panel.  Then by the transform
 //         gamma_s = g_s - sum_{t < s} T[s][t] gamma_t,   u_s = V_s[k+1] - sum_{t < s} T[s][t] u_t;
 //   * the new column k+1 of own row i (the column update A[:, k+1] += A[:, k+2:n] l after the
 //     row update), written into the stored row -- the column is complete from then on:
@@ -51,6 +52,7 @@ constexpr int LZ_NB = MIX_LAZY_LM;      // steps per panel
 constexpr int LZ_NS = MIX_LAZY_RING;    // slots of the ring of published rows
 static_assert(LZ_NS >= LZ_NB + 2, "the ring holds a panel's pivot rows and the next step's candidates");
 constexpr int LZ_TMAX = 2 * LZ_NB + 2;  // column positions a panel's interchanges can touch
+constexpr int LZ_XW = 4 * LZ_NB;        // words per step parity of the pivot rows' exchange
 constexpr int LZ_RING_MAX = 16;         // rows in flight per thread in the panel update (cp.async ring)
 
 struct LazyShared {
@@ -60,8 +62,8 @@ struct LazyShared {
     int ntouch;
     int win[LZ_NB];           // winning CTA of each panel step
     float T[LZ_NB][LZ_NB];    // T[s][t] = l_{w_s}^(t), t < s
-    float vcol[LZ_NB];        // V_s at this step's new column
-    double gsum[LZ_NB];       // V_s . l of the panel's earlier pivot rows (from their owners)
+    float vcol[LZ_NB];        // V_s[pk1] of the panel's pivot rows s <= js (from their owners)
+    double gsum[LZ_NB];       // V_s . l of the panel's pivot rows s <= js (from their owners)
     double Gam[LZ_NB + 1];    // u_s + gamma_s for s < k, [js]: this step's pivot row's
     int K0;                   // the panel's first step
     int pk, pk1;              // physical positions of logical columns k and k+1
@@ -99,15 +101,15 @@ __device__ __forceinline__ const unsigned long long* lz_urow(const MixArgs& a, i
 // The panel end's rank-LZ_NB update S[i, P] -= sum_s w_i^(s) V_s[P] for the rows in `ul`
 // (nu rows with a delayed update), every column P from the panel's first one whose logical
 // column is >= k + 2.  Thread tw of the TW threads of warps 1-15 takes pairs of columns: it
-// holds the 2 columns of every V_s in registers (V_js = R in shared memory, the others from
-// their winners' ring slots, every one of them read earlier in the panel) and streams the rows
+// holds the 2 columns of every V_s in registers (from the winners' ring slots, every one of
+// them published before this step ended) and streams the rows
 // through a ring of D 8-byte slots of its own, filled by cp.async D rows ahead, so that D rows
 // of its columns are in flight at once.  A slot is refilled only after its value has been used
 // (the refill follows the store that depends on it).  Columns that take no update keep their
 // values (V is zero there) and their exchange words are not read.
 template <int D>
 __device__ __forceinline__ void lz_panel_update(const MixArgs& a, float* rows, int ldr, int n, int k, int K0,
-                                                int js, int G, const float* R, const LazyShared& z,
+                                                int js, int G, const LazyShared& z,
                                                 const float (*w)[LZ_NB], const int* ul, int nu, float2* ring,
                                                 int tw, int TW, bool& ok)
 {
@@ -129,7 +131,7 @@ __device__ __forceinline__ void lz_panel_update(const MixArgs& a, float* rows, i
 #pragma unroll
         for (int s = 0; s < LZ_NB; ++s) {
             v[s][0] = v[s][1] = 0.f;
-            if (s < js && z.win[s] >= 0) {
+            if (s <= js && z.win[s] >= 0) {
                 const unsigned long long* u = lz_urow(a, K0 + s, z.win[s], G) + P0;
                 const ulonglong2 p = __ldcg(reinterpret_cast<const ulonglong2*>(u));
                 const unsigned want = (unsigned)(K0 + s) & 0xffffu;
@@ -138,9 +140,6 @@ __device__ __forceinline__ void lz_panel_update(const MixArgs& a, float* rows, i
                 if (m1 && ((unsigned)(p.y >> 16) & 0xffffu) != want) x1 = ld_tagged(u + 1, K0 + s, a.limit_ns, ok);
                 v[s][0] = m0 ? x0 : 0.f;
                 v[s][1] = m1 ? x1 : 0.f;
-            } else if (s == js) {
-                v[s][0] = m0 ? R[P0] : 0.f;
-                v[s][1] = m1 ? R[P0 + 1] : 0.f;
             }
         }
 #pragma unroll
@@ -186,8 +185,7 @@ __global__ void __launch_bounds__(MT, 1) reduce_mixed_lazy_kernel(MixArgs a)
     const int t = threadIdx.x, lane = t & 31, warp = t >> 5;
     const int r0 = b * rpc;
     const int nr = min(rpc, n - r0);
-    float* R = slz;              // this step's pivot row as published (stored), physical order
-    float* lv = R + ldr;         // multipliers by logical row (slot L-1)
+    float* lv = slz;             // multipliers by logical row (slot L-1)
     int* lg = (int*)(lv + ldr);  // physical row -> logical (1-based)
     int* ph = lg + ldr;          // logical (1-based) -> physical row, ph[0] unused
     float2* ring = (float2*)(ph + ldr + 4);  // panel update: 8-byte slots (a.ring per thread of warps 1-15)
@@ -200,7 +198,6 @@ __global__ void __launch_bounds__(MT, 1) reduce_mixed_lazy_kernel(MixArgs a)
         rows[(size_t)i * ldr + c] = c < n ? (float)a.A[(size_t)c * n + r0 + i] : 0.f;
     }
     for (int q = t; q < ldr; q += MT) {
-        R[q] = 0.f;
         lv[q] = 0.f;
         if (q < n) {
             lg[q] = q + 1;
@@ -406,31 +403,11 @@ __global__ void __launch_bounds__(MT, 1) reduce_mixed_lazy_kernel(MixArgs a)
         }
         __syncthreads();
         const int pk1 = z.pk1;
-        // ---- pivot row as published (stored values, physical order) and its multipliers (a row
-        // of T), from the winner's ring slot; multipliers by logical row from the prefetched column
-        // values (slots by the labels before the interchange) ----
+        // ---- multipliers by logical row from the prefetched column values (slots by the labels
+        // before the interchange).  The pivot row itself is not loaded: what the step needs of it
+        // (its product with l, its value at the new column, its panel multipliers) comes from its
+        // owner after the dot products ----
         {
-            const unsigned long long* src = win >= 0 ? lz_urow(a, k, win, G) : nullptr;
-            const unsigned want = (unsigned)k & 0xffffu;
-            bool ok = true;
-            constexpr int PU = 8;  // words per thread in flight
-            for (int base = K0; base < ldr; base += PU * MT) {
-                unsigned long long rv[PU];
-#pragma unroll
-                for (int u = 0; u < PU; ++u) {
-                    const int P = base + t + u * MT;
-                    rv[u] = (src && P < n) ? ld_relaxed_u64(&src[P]) : mix_tag((unsigned)k, 0.f);
-                }
-#pragma unroll
-                for (int u = 0; u < PU; ++u) {
-                    const int P = base + t + u * MT;
-                    float r = __uint_as_float((unsigned)(rv[u] >> 32));
-                    if (src && P < n && ((unsigned)(rv[u] >> 16) & 0xffffu) != want) r = ld_tagged(&src[P], k, a.limit_ns, ok);
-                    if (P < ldr) R[P] = P < n ? r : 0.f;
-                }
-            }
-            if (t < js) z.T[js][t] = src ? ld_tagged(&src[ldr + t], k, a.limit_ns, ok) : 0.f;
-            if (!ok) atomicCAS(a.err, 0, (int)LHL_ERR_TIMEOUT);
             for (int jj = k + 1 + t; jj < n; jj += MT) {  // slot of logical row jj + 1 >= k + 2
                 const float cq = lv[jj == p - 1 ? k : jj];
                 lv[jj] = piv != 0.f ? cq / piv : 0.f;
@@ -438,13 +415,8 @@ __global__ void __launch_bounds__(MT, 1) reduce_mixed_lazy_kernel(MixArgs a)
         }
         __syncthreads();
         // slots of logical rows K0+1 .. k+1 are no multipliers (zero for the dot products, which
-        // start at the panel's first column); V_s at the new column for the panel's earlier steps
+        // start at the panel's first column)
         for (int jj = K0 + t; jj <= k; jj += MT) lv[jj] = 0.f;
-        if (t < js) {
-            bool ok = true;
-            z.vcol[t] = z.win[t] >= 0 ? ld_tagged(&lz_urow(a, K0 + t, z.win[t], G)[pk1], K0 + t, a.limit_ns, ok) : 0.f;
-            if (!ok) atomicCAS(a.err, 0, (int)LHL_ERR_TIMEOUT);
-        }
         __syncthreads();
         if (t < z.ntouch) {  // the dot-product fix at touched positions: l_{logical(P)} - lv[P]
             const int P = z.tP[t], L = z.tL[t];
@@ -454,12 +426,12 @@ __global__ void __launch_bounds__(MT, 1) reduce_mixed_lazy_kernel(MixArgs a)
         if (t == 0) mark(1);
 
         // ---- dot products (FP64 accumulation of FP32 products) from the panel's first column:
-        // own stored rows and the pivot row in the eager kernel's items (4 rows x one of 4 column
-        // parts per warp, the touched-position fix in part 0) ----
+        // own stored rows in the eager kernel's items (4 rows x one of 4 column parts per warp,
+        // the touched-position fix in part 0) ----
         const int ntouch = z.ntouch;
         const int c0 = K0;
         {
-            const int nv = nact + 1;  // own rows below the panel's first step, then R
+            const int nv = nact;  // own rows below the panel's first step
             const int c4 = (c0 + 3) & ~3;
             const int g0 = c4 >> 2, g1 = ldr >> 2;
             const int per = (g1 - g0 + 3) >> 2;
@@ -471,7 +443,7 @@ __global__ void __launch_bounds__(MT, 1) reduce_mixed_lazy_kernel(MixArgs a)
 #pragma unroll
                 for (int q = 0; q < 4; ++q) {
                     const int v = min(rg * 4 + q, nact);
-                    xq[q] = v < nact ? rows + (size_t)s_act[v] * ldr : R;
+                    xq[q] = v < nact ? rows + (size_t)s_act[v] * ldr : rows;  // rows: a pad, never stored
                 }
                 double acc[4] = {0.0, 0.0, 0.0, 0.0};
                 if (cp == 0) {
@@ -497,7 +469,6 @@ __global__ void __launch_bounds__(MT, 1) reduce_mixed_lazy_kernel(MixArgs a)
                     float4 x0[4], x1[4];
 #pragma unroll
                     for (int q = 0; q < 4; ++q) {
-                        // generic loads: the last item row may be R, in shared memory
                         x0[q] = reinterpret_cast<const float4*>(xq[q])[g];
                         x1[q] = reinterpret_cast<const float4*>(xq[q])[g + 32];
                     }
@@ -560,44 +531,63 @@ __global__ void __launch_bounds__(MT, 1) reduce_mixed_lazy_kernel(MixArgs a)
         auto dot = [&](int v) {
             return (s_part[4 * v] + s_part[4 * v + 1]) + (s_part[4 * v + 2] + s_part[4 * v + 3]);
         };
-        // ---- V_s . l of the panel's earlier pivot rows: each is still one of its owner's rows
-        // below K0, and in every column where l is not zero its stored values are the ones it
-        // published, so the owner's dot product above is V_s . l.  Owners publish theirs (the
-        // FP64 value as two tagged 32-bit halves, slots by step parity); the others read them ----
-        if (t < js) {
-            unsigned long long* gx = a.cval + 2 * (size_t)n + (size_t)(k & 1) * 2 * LZ_NB;
-            const int w = z.win[t];
-            double g = 0.0;
-            if (w == b) {
-                g = dot(s_pos[ph[K0 + t + 1] - r0]);
-                const unsigned long long bits = (unsigned long long)__double_as_longlong(g);
-                const unsigned long long tag = (unsigned long long)((unsigned)k & 0xffffu) << 16;
-                __stcg(&gx[2 * t], ((bits >> 32) << 32) | tag);
-                __stcg(&gx[2 * t + 1], ((bits & 0xffffffffull) << 32) | tag);
-            } else if (w >= 0) {
-                bool ok = true;
-                const unsigned hi = __float_as_uint(ld_tagged(&gx[2 * t], (unsigned)k, a.limit_ns, ok));
-                const unsigned lo = __float_as_uint(ld_tagged(&gx[2 * t + 1], (unsigned)k, a.limit_ns, ok));
-                if (!ok) atomicCAS(a.err, 0, (int)LHL_ERR_TIMEOUT);
-                g = __longlong_as_double((long long)(((unsigned long long)hi << 32) | lo));
+        // ---- the panel's pivot rows V_s, s = 0 .. js (js: this step's): each is still one of its
+        // owner's rows below K0, and in every column where l is not zero its stored values are
+        // the ones it published, so the owner's dot product above is V_s . l, and its stored value
+        // at the new column is V_s[pk1].  Owners publish both (the FP64 product as two tagged
+        // 32-bit halves), and this step's winner its panel multipliers, the row T[js]; the others
+        // read them.  Words by step parity: [3 s, 3 s + 1] V_s . l, [3 s + 2] V_s[pk1], then
+        // [3 LZ_NB + t] T[js][t] ----
+        {
+            unsigned long long* gx = a.cval + 2 * (size_t)n + (size_t)(k & 1) * LZ_XW;
+            const unsigned long long tag = (unsigned long long)((unsigned)k & 0xffffu) << 16;
+            if (t <= js) {
+                const int w = z.win[t];
+                double g = 0.0;
+                float u = 0.f;
+                if (w == b) {
+                    const int i = ph[K0 + t + 1] - r0;  // the pivot row of panel step t
+                    g = dot(s_pos[i]);
+                    u = rows[(size_t)i * ldr + pk1];
+                    const unsigned long long bits = (unsigned long long)__double_as_longlong(g);
+                    __stcg(&gx[3 * t], ((bits >> 32) << 32) | tag);
+                    __stcg(&gx[3 * t + 1], ((bits & 0xffffffffull) << 32) | tag);
+                    __stcg(&gx[3 * t + 2], mix_tag((unsigned)k, u));
+                } else if (w >= 0) {
+                    bool ok = true;
+                    const unsigned hi = __float_as_uint(ld_tagged(&gx[3 * t], (unsigned)k, a.limit_ns, ok));
+                    const unsigned lo = __float_as_uint(ld_tagged(&gx[3 * t + 1], (unsigned)k, a.limit_ns, ok));
+                    u = ld_tagged(&gx[3 * t + 2], (unsigned)k, a.limit_ns, ok);
+                    if (!ok) atomicCAS(a.err, 0, (int)LHL_ERR_TIMEOUT);
+                    g = __longlong_as_double((long long)(((unsigned long long)hi << 32) | lo));
+                }
+                z.gsum[t] = g;
+                z.vcol[t] = u;
             }
-            z.gsum[t] = g;
+            if (t < js) {  // T[js][t]: this step's pivot row's multiplier of panel step t
+                float x = 0.f;
+                if (win == b) {
+                    x = s_lm[ph[k + 1] - r0][t];  // s_lm is by own row, s_part by place in s_act
+                    __stcg(&gx[3 * LZ_NB + t], mix_tag((unsigned)k, x));
+                } else if (win >= 0) {
+                    bool ok = true;
+                    x = ld_tagged(&gx[3 * LZ_NB + t], (unsigned)k, a.limit_ns, ok);
+                    if (!ok) atomicCAS(a.err, 0, (int)LHL_ERR_TIMEOUT);
+                }
+                z.T[js][t] = x;
+            }
         }
         __syncthreads();
         if (t == 0) mark(2);
         // ---- the transform: true gamma_s and u_s of the panel's pivot rows, in step order, then
-        // Gamma = u + gamma.  Warp 0, lane s for step s: its V_s . l (or the pivot row's dot
-        // product), then a forward substitution by columns: once lane s is final
+        // Gamma = u + gamma.  Warp 0, lane s for step s: V_s . l and V_s[pk1] from the exchange, then a forward substitution by columns: once lane s is final
         // it is broadcast and every later lane subtracts T[r][s] times it (the same terms in the
         // same order as a row-by-row substitution) ----
         if (warp == 0) {
             double g = 0.0, u = 0.0;
-            if (lane < js) {
+            if (lane <= js) {
                 g = z.gsum[lane];
                 u = (double)z.vcol[lane];
-            } else if (lane == js) {
-                g = dot(nact);
-                u = (double)R[pk1];
             }
             for (int s2 = 0; s2 < js; ++s2) {
                 const double gs = __shfl_sync(0xffffffffu, g, s2), us = __shfl_sync(0xffffffffu, u, s2);
@@ -697,11 +687,11 @@ __global__ void __launch_bounds__(MT, 1) reduce_mixed_lazy_kernel(MixArgs a)
                 named_bar_sync(1, TW);
                 bool ok = true;
                 if (a.ring >= 16)
-                    lz_panel_update<16>(a, rows, ldr, n, k, K0, js, G, R, z, s_lm, s_ul, s_nu, ring, tw, TW, ok);
+                    lz_panel_update<16>(a, rows, ldr, n, k, K0, js, G, z, s_lm, s_ul, s_nu, ring, tw, TW, ok);
                 else if (a.ring >= 8)
-                    lz_panel_update<8>(a, rows, ldr, n, k, K0, js, G, R, z, s_lm, s_ul, s_nu, ring, tw, TW, ok);
+                    lz_panel_update<8>(a, rows, ldr, n, k, K0, js, G, z, s_lm, s_ul, s_nu, ring, tw, TW, ok);
                 else
-                    lz_panel_update<4>(a, rows, ldr, n, k, K0, js, G, R, z, s_lm, s_ul, s_nu, ring, tw, TW, ok);
+                    lz_panel_update<4>(a, rows, ldr, n, k, K0, js, G, z, s_lm, s_ul, s_nu, ring, tw, TW, ok);
                 named_bar_sync(1, TW);
                 if (!ok) atomicCAS(a.err, 0, (int)LHL_ERR_TIMEOUT);
                 // move the touched positions: row i's value at P goes to L - 1 (at most 2 LZ_NB + 2
@@ -748,7 +738,7 @@ __global__ void __launch_bounds__(MT, 1) reduce_mixed_lazy_kernel(MixArgs a)
 // dynamic shared memory with a panel-update ring of `ring` slots per thread of warps 1-15
 size_t lazy_smem_bytes(int ldr, int ring)
 {
-    return (size_t)ldr * 4 * sizeof(float) + 4 * sizeof(int) + (size_t)(MT - 32) * ring * sizeof(float2);
+    return (size_t)ldr * 3 * sizeof(float) + 4 * sizeof(int) + (size_t)(MT - 32) * ring * sizeof(float2);
 }
 
 // the deepest ring (16, 8 or 4 slots) whose shared memory fits beside the kernel's static arrays

@@ -1103,7 +1103,7 @@ cudaError_t launch_ldiv(const LdivArgs& a, int nrhs, cudaStream_t st)
             // Gt once for the group; otherwise one CTA per right-hand side
             if (e == cudaSuccess && a.rhs_per_shift >= 4)
                 e = launch_hess_cplx_mrhs(a.n, a.Gt, a.ldg, a.po, a.swp, a.rdiag, a.Y, a.n, c0, cnt,
-                                          a.rhs_per_shift, a.done, a.tol, st);
+                                          a.rhs_per_shift, a.done, a.tol, st, a.tail, a.err, a.limit_ns);
             else if (e == cudaSuccess)
                 e = launch_hess_cplx(a.n, a.Gt, a.ldg, a.po, a.swp, a.rdiag, a.Y, a.n, c0, cnt, a.rhs_per_shift,
                                      a.done, a.tol, st);

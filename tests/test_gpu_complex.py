@@ -302,3 +302,43 @@ def test_complex_shift_bitexact_large(n, complex_ht):
         assert bits_equal(Gt[off + np.arange(n - 1), np.arange(1, n)], So.Gt[off + np.arange(n - 1), np.arange(1, n)])
     assert np.array_equal(host(sh.swap())[:n], So.swap[:n])
     assert bits_equal(host(sh.rdiag()), So.rdiag[:n])
+
+
+@pytest.mark.parametrize("n,rps,groups", [(33, 11, [(1, 0), (1, 1), (4, 0)]), (1000, 8, [(2, 0)]),
+                                          (2049, 11, [(0, 1), (3, 0), (5, 0), (5, 1)]),
+                                          (1000, 32, [(s, g) for s in range(4) for g in range(4)]),
+                                          (1000, 32, [(s, g) for s in range(6) for g in range(4)])])
+def test_few_groups_refine_through_the_grid_wide_solve(n, rps, groups):
+    """Refinement steps where only a few groups of right-hand sides (<= 16) are above the
+    tolerance take the grid-wide planar Hessenberg solve (hess_cplx_tail_kernel: the CTAs shared
+    out among the groups) instead of one CTA per group; with 24 groups left the multi-vector
+    kernel keeps them.  Columns zeroed and refined by one step equal W~^-1 b again, to 1e-10 of
+    the multi-vector kernel's solution, and the columns already at the tolerance are left bit for
+    bit."""
+    torch, G = _mods()
+    S = 6
+    ncols = S * rps
+    J = rng(60 + n).standard_normal((n, n)) / np.sqrt(n)
+    Jd = dev(J)
+    ws = G.lhl(Jd, shift_complex=True)
+    g = rng(61)
+    sig = g.uniform(-2.0, 0.0, S) + 1j * g.uniform(0.0, 10.0, S)
+    tau = -np.ones(S, dtype=complex)
+    sh = G.LHLShift(n, S, complex=True)
+    G.lhl_shift_batched_(sh, ws, dev(sig), dev(tau))
+    B = rng(62).standard_normal((n, ncols)) + 1j * rng(63).standard_normal((n, ncols))
+    Bd = dev(B)
+    X = Bd.clone()
+    G.lhl_ldiv_(X, sh, ws, rhs_per_shift=rps)
+    Xh = host(X)
+    active = sorted({s * rps + gg * 8 + v for s, gg in groups for v in range(8)
+                     if gg * 8 + v < rps})
+    X2 = X.clone()
+    X2[:, active] = 0
+    G.lhl_refine_tol_(X2, Jd, Bd, sh, ws, tol=1e-8, max_steps=1, rhs_per_shift=rps)
+    X2h = host(X2)
+    for c in range(ncols):
+        if c in active:
+            assert np.linalg.norm(X2h[:, c] - Xh[:, c]) <= 1e-10 * np.linalg.norm(Xh[:, c]), (n, c)
+        else:
+            assert bits_equal(X2h[:, c], Xh[:, c]), (n, c)
