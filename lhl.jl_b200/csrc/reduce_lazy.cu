@@ -53,7 +53,7 @@ constexpr int LZ_NS = MIX_LAZY_RING;    // slots of the ring of published rows
 static_assert(LZ_NS >= LZ_NB + 2, "the ring holds a panel's pivot rows and the next step's candidates");
 constexpr int LZ_TMAX = 2 * LZ_NB + 2;  // column positions a panel's interchanges can touch
 constexpr int LZ_XW = 4 * LZ_NB;        // words per step parity of the pivot rows' exchange
-constexpr int LZ_RING_MAX = 16;         // rows in flight per thread in the panel update (cp.async ring)
+constexpr int LZ_RING_MAX = 24;         // rows in flight per thread in the panel update (cp.async ring)
 
 struct LazyShared {
     int tP[LZ_TMAX];          // touched physical positions (0-based) ...
@@ -69,14 +69,6 @@ struct LazyShared {
     int pk, pk1;              // physical positions of logical columns k and k+1
 };
 
-// the physical position (0-based) of logical column L (1-based), through the panel's table of
-// touched positions
-__device__ __forceinline__ int lz_cph(const LazyShared& z, int L)
-{
-    for (int q = 0; q < z.ntouch; ++q)
-        if (z.tL[q] == L) return z.tP[q];
-    return L - 1;
-}
 
 // 8-byte asynchronous copy of 2 floats global -> shared (cp.async); both addresses 8-byte
 // aligned
@@ -379,27 +371,48 @@ __global__ void __launch_bounds__(MT, 1) reduce_mixed_lazy_kernel(MixArgs a)
         const int js = k - K0;  // this step's index in the panel
         const bool last = (js == LZ_NB - 1) || (k == n - 2);  // the panel ends with this step
         // ---- interchange k+1 <-> p: row labels, and the column table (no data moves) ----
-        if (t == 0) {
+        // (warp 0: the table's at most 2 LZ_NB + 2 entries two per lane, looked up by ballots)
+        if (warp == 0) {
+            const int nt = z.ntouch;
+            const int P0v = lane < nt ? z.tP[lane] : -1, L0v = lane < nt ? z.tL[lane] : -1;
+            const int P1v = lane + 32 < nt ? z.tP[lane + 32] : -1, L1v = lane + 32 < nt ? z.tL[lane + 32] : -1;
+            auto cph = [&](int L) {  // physical position (0-based) of logical column L (1-based)
+                const unsigned m0 = __ballot_sync(0xffffffffu, L0v == L), m1 = __ballot_sync(0xffffffffu, L1v == L);
+                if (m0) return __shfl_sync(0xffffffffu, P0v, __ffs(m0) - 1);
+                if (m1) return __shfl_sync(0xffffffffu, P1v, __ffs(m1) - 1);
+                return L - 1;
+            };
+            auto entry = [&](int P) {  // the table entry of position P, or -1
+                const unsigned m0 = __ballot_sync(0xffffffffu, P0v == P), m1 = __ballot_sync(0xffffffffu, P1v == P);
+                return m0 ? __ffs(m0) - 1 : (m1 ? 32 + __ffs(m1) - 1 : -1);
+            };
+            const int pkv = cph(k);  // logical k is not part of this step's interchange
+            int pk1v;
             if (p != k + 1) {
-                const int x = ph[k + 1], w = ph[p];
-                ph[k + 1] = w;
-                ph[p] = x;
-                lg[w] = k + 1;
-                lg[x] = p;
-                const int Pa = lz_cph(z, k + 1), Pb = lz_cph(z, p);
-                int qa = -1, qb = -1;
-                for (int q = 0; q < z.ntouch; ++q) {
-                    if (z.tP[q] == Pa) qa = q;
-                    if (z.tP[q] == Pb) qb = q;
+                const int Pa = cph(k + 1), Pb = cph(p);
+                int qa = entry(Pa), qb = entry(Pb);
+                if (lane == 0) {
+                    const int x = ph[k + 1], w = ph[p];
+                    ph[k + 1] = w;
+                    ph[p] = x;
+                    lg[w] = k + 1;
+                    lg[x] = p;
+                    int nt2 = nt;
+                    if (qa < 0) { qa = nt2++; z.tP[qa] = Pa; }
+                    if (qb < 0) { qb = nt2++; z.tP[qb] = Pb; }
+                    z.tL[qa] = p;      // Pa held logical k+1, now p
+                    z.tL[qb] = k + 1;  // Pb held logical p, now k+1
+                    z.ntouch = nt2;
                 }
-                if (qa < 0) { qa = z.ntouch++; z.tP[qa] = Pa; }
-                if (qb < 0) { qb = z.ntouch++; z.tP[qb] = Pb; }
-                z.tL[qa] = p;      // Pa held logical k+1, now p
-                z.tL[qb] = k + 1;  // Pb held logical p, now k+1
+                pk1v = Pb;
+            } else {
+                pk1v = cph(k + 1);
             }
-            z.win[js] = win;
-            z.pk = lz_cph(z, k);
-            z.pk1 = lz_cph(z, k + 1);
+            if (lane == 0) {
+                z.win[js] = win;
+                z.pk = pkv;
+                z.pk1 = pk1v;
+            }
         }
         __syncthreads();
         const int pk1 = z.pk1;
@@ -408,9 +421,10 @@ __global__ void __launch_bounds__(MT, 1) reduce_mixed_lazy_kernel(MixArgs a)
         // (its product with l, its value at the new column, its panel multipliers) comes from its
         // owner after the dot products ----
         {
+            const float rp = piv != 0.f ? 1.f / piv : 0.f;  // FP32 form: one division per step
             for (int jj = k + 1 + t; jj < n; jj += MT) {  // slot of logical row jj + 1 >= k + 2
                 const float cq = lv[jj == p - 1 ? k : jj];
-                lv[jj] = piv != 0.f ? cq / piv : 0.f;
+                lv[jj] = cq * rp;
             }
         }
         __syncthreads();
@@ -686,7 +700,9 @@ __global__ void __launch_bounds__(MT, 1) reduce_mixed_lazy_kernel(MixArgs a)
                 }
                 named_bar_sync(1, TW);
                 bool ok = true;
-                if (a.ring >= 16)
+                if (a.ring >= 24)
+                    lz_panel_update<24>(a, rows, ldr, n, k, K0, js, G, z, s_lm, s_ul, s_nu, ring, tw, TW, ok);
+                else if (a.ring >= 16)
                     lz_panel_update<16>(a, rows, ldr, n, k, K0, js, G, z, s_lm, s_ul, s_nu, ring, tw, TW, ok);
                 else if (a.ring >= 8)
                     lz_panel_update<8>(a, rows, ldr, n, k, K0, js, G, z, s_lm, s_ul, s_nu, ring, tw, TW, ok);
@@ -741,13 +757,13 @@ size_t lazy_smem_bytes(int ldr, int ring)
     return (size_t)ldr * 3 * sizeof(float) + 4 * sizeof(int) + (size_t)(MT - 32) * ring * sizeof(float2);
 }
 
-// the deepest ring (16, 8 or 4 slots) whose shared memory fits beside the kernel's static arrays
+// the deepest ring (24, 16, 8 or 4 slots) whose shared memory fits beside the kernel's static arrays
 static int lazy_ring(int ldr)
 {
     cudaFuncAttributes fa;
     size_t stat = 16 * 1024;
     if (cudaFuncGetAttributes(&fa, reduce_mixed_lazy_kernel) == cudaSuccess) stat = fa.sharedSizeBytes;
-    for (int r = LZ_RING_MAX; r >= 4; r /= 2)
+    for (int r : {LZ_RING_MAX, 16, 8, 4})
         if (lazy_smem_bytes(ldr, r) + stat <= MIX_SMEM_TOTAL) return r;
     return 0;
 }
