@@ -70,7 +70,8 @@ typedef struct {
 /* ---- workspace ------------------------------------------------------------------ */
 /* LHLWorkspace{Float64}(n) (F:164-178).  precision: LHL_PREC_*.  With LHL_PREC_MIXED,
  * lhl_reduce computes the factors in FP32 (stored widened to FP64 in the same layout), for
- * use with lhl_refine_tol; every other entry point is unchanged. */
+ * use with lhl_refine_tol; every other entry point is unchanged.  Orders: n <= 16384 in
+ * both forms, else LHL_ERR_DIM. */
 int lhl_ws_create(int64_t n, int precision, lhl_ws_t* ws);
 int lhl_ws_destroy(lhl_ws_t ws);
 int lhl_ws_get_view(lhl_ws_t ws, lhl_ws_view* view);

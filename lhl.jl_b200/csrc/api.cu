@@ -136,6 +136,8 @@ int lhl_ws_create(int64_t n, int precision, lhl_ws_t* out)
         if (e == cudaSuccess) e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
         if (e == cudaSuccess) {
             lhl::mixed_plan((int)n, sms, &w->mplan);
+            // rows that do not fit on chip need the panel-delayed kernel's shared memory
+            if (w->mplan.ok && !w->mplan.smem_rows && !lhl::lazy_fits(w->mplan.ldr)) w->mplan.ok = 0;
             if (!w->mplan.ok) {
                 ws_free(w);
                 return LHL_ERR_DIM;

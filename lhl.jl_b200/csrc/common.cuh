@@ -20,6 +20,11 @@ __device__ __forceinline__ double dmul(double a, double b) { return __dmul_rn(a,
 __device__ __forceinline__ double dadd(double a, double b) { return __dadd_rn(a, b); }
 __device__ __forceinline__ double dsub(double a, double b) { return __dsub_rn(a, b); }
 __device__ __forceinline__ double dfma(double a, double b, double c) { return __fma_rn(a, b, c); }
+// the same four in single precision (the Float32 workspace's reduction)
+__device__ __forceinline__ float dmul(float a, float b) { return __fmul_rn(a, b); }
+__device__ __forceinline__ float dadd(float a, float b) { return __fadd_rn(a, b); }
+__device__ __forceinline__ float dsub(float a, float b) { return __fsub_rn(a, b); }
+__device__ __forceinline__ float dfma(float a, float b, float c) { return __fmaf_rn(a, b, c); }
 
 __device__ __forceinline__ uint64_t globaltimer_ns()
 {

@@ -148,6 +148,8 @@ constexpr int MIX_LAZY_RING = 18;
 // panel so far (MIX_LAZY_LM words)
 constexpr int MIX_LAZY_LM = 16;
 cudaError_t launch_reduce_mixed_lazy(MixArgs a, const MixPlan& pl, cudaStream_t st);
+// whether the panel-delayed kernel's shared memory fits for row pitch ldr (n up to about 10400)
+bool lazy_fits(int ldr);
 // after it: Ht, plus the deferred right updates of the rows above each panel (factors and Ht)
 cudaError_t launch_lazy_finish(int n, double* F, double* Ht, cudaStream_t st);
 

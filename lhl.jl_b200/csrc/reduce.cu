@@ -228,11 +228,12 @@ __device__ bool balance_phase(const RedArgs& a, GridBarrier& gb)
 // j's final values land in buffer j&1 at step j; later interchanges reach them in the
 // final assembly.
 // ---------------------------------------------------------------------------------
-__device__ bool unblocked_phase(const RedArgs& a, GridBarrier& gb)
+template <typename T>
+__device__ bool unblocked_phase(const RedArgs& a, GridBarrier& gb, T* A0, T* A1)
 {
     const int n = a.n;
-    double* buf[2] = {a.A, a.buf2};
-    __shared__ double s_l[512];
+    T* buf[2] = {A0, A1};
+    __shared__ T s_l[4096 / sizeof(T)];  // n < 512 (FP64) or n < 1024 (float)
     __shared__ double s_red[RW];
     __shared__ int s_redi[RW];
     __shared__ int s_p;
@@ -246,57 +247,57 @@ __device__ bool unblocked_phase(const RedArgs& a, GridBarrier& gb)
     {
         double v = 0.0;
         int vi = 0;
-        if (i >= 2 && i <= n) { v = fabs(M1(a.A, n, i, 1)); vi = i; }
+        if (i >= 2 && i <= n) { v = fabs((double)M1(A0, n, i, 1)); vi = i; }
         publish_candidate(a, v, vi, s_red, s_redi);
     }
     if (!gb.sync()) return false;
     for (int k = 1; k <= n - 2; ++k) {
-        const double* R = buf[(k - 1) & 1];
-        double* W = buf[k & 1];
+        const T* R = buf[(k - 1) & 1];
+        T* W = buf[k & 1];
         combine_candidates(a, &s_p, s_red, s_redi);
         const int p = (s_p >= k + 1 && s_p <= n) ? s_p : k + 1;
         if (gt == 0) a.ipiv[k - 1] = p;
         auto sw = [&](int r) { return r == k + 1 ? p : (r == p ? k + 1 : r); };
-        const double piv = M1(R, n, p, k);
+        const T piv = M1(R, n, p, k);
         // multipliers l_j = A'[j,k] / piv, j = k+2..n, into shared memory
         for (int j = k + 2 + threadIdx.x; j <= n; j += RT)
-            s_l[j - 1] = (piv != 0.0) ? M1(R, n, sw(j), k) / piv : M1(R, n, sw(j), k);
+            s_l[j - 1] = (piv != (T)0) ? M1(R, n, sw(j), k) / piv : M1(R, n, sw(j), k);
         __syncthreads();
         double cand = 0.0;
         int candi = 0;
         if (i <= n) {
             const int si = sw(i);
             // column k
-            double ck = M1(R, n, si, k);
-            if (piv != 0.0 && i >= k + 2) ck = s_l[i - 1];
+            T ck = M1(R, n, si, k);
+            if (piv != (T)0 && i >= k + 2) ck = s_l[i - 1];
             M1(W, n, i, k) = ck;
             // column k+1 (swapped with p), left update by pk = A'[k+1,k+1]
-            double ck1 = M1(R, n, si, p);
-            if (piv == 0.0) {
+            T ck1 = M1(R, n, si, p);
+            if (piv == (T)0) {
                 // step skipped (F:488): rows/columns still carry the interchange
                 for (int j = k + 2; j <= n; ++j) M1(W, n, i, j) = M1(R, n, si, sw(j));
                 M1(W, n, i, k + 1) = ck1;
             } else {
-                const double pk = M1(R, n, p, p);
-                const double li = (i >= k + 2) ? s_l[i - 1] : 0.0;
-                if (pk != 0.0 && i >= k + 2) ck1 = dsub(ck1, dmul(li, pk));
+                const T pk = M1(R, n, p, p);
+                const T li = (i >= k + 2) ? s_l[i - 1] : (T)0;
+                if (pk != (T)0 && i >= k + 2) ck1 = dsub(ck1, dmul(li, pk));
                 if (!generic) {
-                    double s = 0.0;
+                    T s = 0;
                     const bool low = i >= k + 2;
                     int j = k + 2;
                     // sixteen columns at a time: every load of the block is issued before its
                     // stores (a store to W could otherwise hold back the next load from R)
                     for (; j + 15 <= n; j += 16) {
-                        double v[16], pr[16];
+                        T v[16], pr[16];
 #pragma unroll
                         for (int u = 0; u < 16; ++u) {
                             const int sj = sw(j + u);
                             v[u] = M1(R, n, si, sj);
-                            pr[u] = low ? M1(R, n, p, sj) : 0.0;
+                            pr[u] = low ? M1(R, n, p, sj) : (T)0;
                         }
 #pragma unroll
                         for (int u = 0; u < 16; ++u) {
-                            double x = v[u];
+                            T x = v[u];
                             if (low) x = dfma(li, -pr[u], x);
                             M1(W, n, i, j + u) = x;
                             s = dfma(s_l[j + u - 1], x, s);
@@ -304,7 +305,7 @@ __device__ bool unblocked_phase(const RedArgs& a, GridBarrier& gb)
                     }
                     for (; j <= n; ++j) {
                         const int sj = sw(j);
-                        double v = M1(R, n, si, sj);
+                        T v = M1(R, n, si, sj);
                         if (low) v = dfma(li, -M1(R, n, p, sj), v);
                         M1(W, n, i, j) = v;
                         s = dfma(s_l[j - 1], v, s);
@@ -313,7 +314,7 @@ __device__ bool unblocked_phase(const RedArgs& a, GridBarrier& gb)
                 } else {
                     int j = k + 2;
                     while (j + 1 <= n) {
-                        double v0 = M1(R, n, si, sw(j)), v1 = M1(R, n, si, sw(j + 1));
+                        T v0 = M1(R, n, si, sw(j)), v1 = M1(R, n, si, sw(j + 1));
                         if (i >= k + 2) {
                             v0 = dsub(v0, dmul(li, M1(R, n, p, sw(j))));
                             v1 = dsub(v1, dmul(li, M1(R, n, p, sw(j + 1))));
@@ -324,7 +325,7 @@ __device__ bool unblocked_phase(const RedArgs& a, GridBarrier& gb)
                         j += 2;
                     }
                     if (j <= n) {
-                        double v0 = M1(R, n, si, sw(j));
+                        T v0 = M1(R, n, si, sw(j));
                         if (i >= k + 2) v0 = dsub(v0, dmul(li, M1(R, n, p, sw(j))));
                         M1(W, n, i, j) = v0;
                         ck1 = dadd(ck1, dmul(s_l[j - 1], v0));
@@ -332,7 +333,7 @@ __device__ bool unblocked_phase(const RedArgs& a, GridBarrier& gb)
                 }
                 M1(W, n, i, k + 1) = ck1;
             }
-            if (i >= k + 2) { cand = fabs(ck1); candi = i; }
+            if (i >= k + 2) { cand = fabs((double)ck1); candi = i; }
         }
         publish_candidate(a, cand, candi, s_red, s_redi);
         if (!gb.sync()) return false;
@@ -343,12 +344,13 @@ __device__ bool unblocked_phase(const RedArgs& a, GridBarrier& gb)
 // Final assembly of the unblocked result into a.A: column j from buffer j&1 (columns
 // n-1, n from the last step's buffer), with the interchanges of steps j+1..n-2 applied
 // (the reference applies them as they happen, F:480-485).  One CTA per column.
-__global__ void __launch_bounds__(RT) unblocked_assemble_kernel(int n, double* A, const double* B2,
+template <typename T>
+__global__ void __launch_bounds__(RT) unblocked_assemble_kernel(int n, double* out, const T* A, const T* B2,
                                                                 const int64_t* ipiv)
 {
     const int j = blockIdx.x + 1;
     if (j > n) return;
-    const double* src;
+    const T* src;
     int from;
     if (j <= n - 2) {
         src = (j & 1) ? B2 : A;
@@ -358,21 +360,21 @@ __global__ void __launch_bounds__(RT) unblocked_assemble_kernel(int n, double* A
         src = (kl >= 1 && (kl & 1)) ? B2 : A;
         from = n - 1;
     }
-    __shared__ double col[512];
+    __shared__ T col[4096 / sizeof(T)];
     for (int i = threadIdx.x; i < n; i += RT) col[i] = src[(size_t)(j - 1) * n + i];
     __syncthreads();
     if (threadIdx.x == 0) {
         for (int k = from; k <= n - 2; ++k) {
             const int p = (int)ipiv[k - 1];
             if (p > k + 1 && p <= n) {
-                const double t = col[k];
+                const T t = col[k];
                 col[k] = col[p - 1];
                 col[p - 1] = t;
             }
         }
     }
     __syncthreads();
-    for (int i = threadIdx.x; i < n; i += RT) A[(size_t)(j - 1) * n + i] = col[i];
+    for (int i = threadIdx.x; i < n; i += RT) out[(size_t)(j - 1) * n + i] = (double)col[i];
 }
 
 // ---------------------------------------------------------------------------------
@@ -1340,7 +1342,7 @@ __global__ void __launch_bounds__(RT, 1) reduce_kernel(RedArgs a, int balance, i
     }
     tmark(a, 0, last);
     if (mode == 1) {
-        unblocked_phase(a, gb);
+        unblocked_phase<double>(a, gb, a.A, a.buf2);
         tmark(a, 1, last);
     } else if (mode == 2) {
         blocked_phase<NBMAX>(a, gb, S, last, &tmA, &tmP, bars, tiles);

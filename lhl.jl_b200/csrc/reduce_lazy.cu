@@ -768,6 +768,8 @@ static int lazy_ring(int ldr)
     return 0;
 }
 
+bool lazy_fits(int ldr) { return lazy_ring(ldr) > 0; }
+
 cudaError_t launch_reduce_mixed_lazy(MixArgs a, const MixPlan& pl, cudaStream_t st)
 {
     if (!pl.ok) return cudaErrorInvalidValue;

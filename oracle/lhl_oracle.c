@@ -726,6 +726,146 @@ int lhlo_shift(int n, const double* Ht, int ldh, double sigma, double tau, doubl
     return info;
 }
 
+/* ------------------------------------------------------------------------------------ */
+/* lhl_reduce! for LHLWorkspace{Float32} below _lhl_block_min(Float32) = 1024 (F:703-705): */
+/* balancing (F:299-340 with Tr = Float32: sums, halvings and Tr(0.95) in float, scale in  */
+/* float) and the unblocked ELMHES (F:466-501) with the Float32 trailing update: the row-  */
+/* block kernel for n >= max(W, 8) = 8 (F:547-552, W = 32 / 4 = 8 on x86-64, F:1713), whose */
+/* per-row order does not depend on W (each lane is one row), and the paired sweep below.  */
+/* J is rounded to float first (copyto! into the Float32 fstore).  The outputs are float   */
+/* values in double storage.  The reference's blocked Float32 form (n >= 1024) is not       */
+/* restated: returns -2 there.                                                             */
+/* ------------------------------------------------------------------------------------ */
+#define M1F(A, ld, i, j) ((A)[(size_t)((j) - 1) * (size_t)(ld) + (size_t)((i) - 1)])
+
+static void balance_f32(int n, float* A, int ld, float* d, float* isc)
+{
+    for (int i = 1; i <= n; ++i) { d[i - 1] = 1.0f; isc[i - 1] = 1.0f; }
+    for (int sweep = 0; sweep < 20; ++sweep) {
+        int converged = 1;
+        for (int i = 1; i <= n; ++i) {
+            float c = 0.0f, r = 0.0f;
+            for (int j = 1; j <= n; ++j) {
+                if (j == i) continue;
+                c += fabsf(M1F(A, ld, j, i));
+                r += fabsf(M1F(A, ld, i, j));
+            }
+            if (c == 0.0f || r == 0.0f) continue;
+            float f = 1.0f;
+            float s = c + r;
+            int guard = 0;  /* the device's bounds, as in lhlo_balance */
+            while (c < r / 2.0f && guard < 4200) { c *= 2.0f; r /= 2.0f; f *= 2.0f; ++guard; }
+            while (c >= 2.0f * r && guard < 8400) { c /= 2.0f; r *= 2.0f; f /= 2.0f; ++guard; }
+            if (c + r < 0.95f * s) {
+                converged = 0;
+                d[i - 1] *= f;
+                isc[i - 1] /= f;
+                for (int j = 1; j <= n; ++j) {
+                    M1F(A, ld, i, j) /= f;
+                    M1F(A, ld, j, i) *= f;
+                }
+            }
+        }
+        if (converged) break;
+    }
+}
+
+static void reduce_unblocked_f32(int n, float* A, int ld, int64_t* ipiv)
+{
+    for (int k = 1; k <= n - 2; ++k) {
+        int p = k + 1;
+        float amax = fabsf(M1F(A, ld, k + 1, k));
+        for (int i = k + 2; i <= n; ++i) {
+            float a = fabsf(M1F(A, ld, i, k));
+            if (a > amax) { amax = a; p = i; }
+        }
+        ipiv[k - 1] = p;
+        if (p != k + 1) {
+            for (int j = 1; j <= n; ++j) {
+                float t = M1F(A, ld, k + 1, j); M1F(A, ld, k + 1, j) = M1F(A, ld, p, j); M1F(A, ld, p, j) = t;
+            }
+            for (int i = 1; i <= n; ++i) {
+                float t = M1F(A, ld, i, k + 1); M1F(A, ld, i, k + 1) = M1F(A, ld, i, p); M1F(A, ld, i, p) = t;
+            }
+        }
+        float piv = M1F(A, ld, k + 1, k);
+        if (piv == 0.0f) continue;
+        for (int i = k + 2; i <= n; ++i) M1F(A, ld, i, k) /= piv;
+        float pk = M1F(A, ld, k + 1, k + 1);
+        if (pk != 0.0f)
+            for (int i = k + 2; i <= n; ++i) M1F(A, ld, i, k + 1) -= M1F(A, ld, i, k) * pk;
+        if (n < 8) {  /* F:508-538 */
+            int j = k + 2;
+            while (j + 1 <= n) {
+                float pj = M1F(A, ld, k + 1, j), pj1 = M1F(A, ld, k + 1, j + 1);
+                for (int i = k + 2; i <= n; ++i) {
+                    float l = M1F(A, ld, i, k);
+                    M1F(A, ld, i, j) -= l * pj;
+                    M1F(A, ld, i, j + 1) -= l * pj1;
+                }
+                float vj = M1F(A, ld, j, k), vj1 = M1F(A, ld, j + 1, k);
+                for (int i = 1; i <= n; ++i)
+                    M1F(A, ld, i, k + 1) += vj * M1F(A, ld, i, j) + vj1 * M1F(A, ld, i, j + 1);
+                j += 2;
+            }
+            if (j <= n) {
+                float pj = M1F(A, ld, k + 1, j);
+                for (int i = k + 2; i <= n; ++i) M1F(A, ld, i, j) -= M1F(A, ld, i, k) * pj;
+                float vj = M1F(A, ld, j, k);
+                for (int i = 1; i <= n; ++i) M1F(A, ld, i, k + 1) += vj * M1F(A, ld, i, j);
+            }
+        } else {  /* F:547-678, per row */
+#pragma omp parallel for schedule(static) if (n >= 256)
+            for (int i = 1; i <= n; ++i) {
+                float s = 0.0f;
+                if (i >= k + 2) {
+                    float li = M1F(A, ld, i, k);
+                    for (int j = k + 2; j <= n; ++j) {
+                        float a = fmaf(li, -M1F(A, ld, k + 1, j), M1F(A, ld, i, j));
+                        M1F(A, ld, i, j) = a;
+                        s = fmaf(M1F(A, ld, j, k), a, s);
+                    }
+                } else {
+                    for (int j = k + 2; j <= n; ++j) s = fmaf(M1F(A, ld, j, k), M1F(A, ld, i, j), s);
+                }
+                M1F(A, ld, i, k + 1) = M1F(A, ld, i, k + 1) + s;
+            }
+        }
+    }
+}
+
+int lhlo_reduce_f32(int n, const double* J, int ldj, int balance, double* F, int ldf, int64_t* ipiv, double* scale,
+                    double* iscale, int64_t* perm, int64_t* iperm, double* Ht)
+{
+    if (n < 0 || ldj < n || ldf < n) return -1;
+    if (n >= 1024) return -2;
+    float* A = (float*)malloc(sizeof(float) * ((size_t)n * (size_t)n + 2 * (size_t)n + 1));
+    if (!A) return -3;
+    float* d = A + (size_t)n * (size_t)n;
+    float* isc = d + n;
+    for (int j = 1; j <= n; ++j)
+        for (int i = 1; i <= n; ++i) M1F(A, n, i, j) = (float)M1(J, ldj, i, j);
+    if (balance) balance_f32(n, A, n, d, isc);
+    else for (int i = 0; i < n; ++i) { d[i] = 1.0f; isc[i] = 1.0f; }
+    reduce_unblocked_f32(n, A, n, ipiv);
+    for (int j = 1; j <= n; ++j)
+        for (int i = 1; i <= n; ++i) M1(F, ldf, i, j) = M1F(A, n, i, j);
+    for (int i = 0; i < n; ++i) { scale[i] = d[i]; iscale[i] = isc[i]; }
+    free(A);
+    if (Ht) {
+        memset(Ht, 0, sizeof(double) * (size_t)n * (size_t)n);
+        for (int i = 1; i <= n; ++i)
+            for (int j = (i - 1 > 1 ? i - 1 : 1); j <= n; ++j) M1(Ht, n, j, i) = M1(F, ldf, i, j);
+    }
+    for (int i = 1; i <= n; ++i) perm[i - 1] = i;
+    for (int k = 1; k <= n - 2; ++k) {
+        int64_t p = ipiv[k - 1];
+        int64_t t = perm[k]; perm[k] = perm[p - 1]; perm[p - 1] = t;
+    }
+    for (int i = 1; i <= n; ++i) iperm[perm[i - 1] - 1] = i;
+    return 0;
+}
+
 /* lhl_shift! for LHLWorkspace{Float32} (F:2529-2594 with T = Float32): the same steps in
  * float arithmetic, sigma and tau rounded to float first (T(sigma), T(tau)).  Ht holds float
  * values in double storage; Gt and rdiag receive float values in double storage. */

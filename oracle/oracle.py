@@ -46,6 +46,8 @@ def lib():
         L.lhlo_reduce_blocked_ptr.argtypes = [i, _dp, i, _iv, i]
         L.lhlo_reduce.argtypes = [i, _dp, i, i, i, i, _dp, i, _iv, _dv, _dv, _iv, _iv, _dp]
         L.lhlo_reduce.restype = i
+        L.lhlo_reduce_f32.argtypes = [i, _dp, i, i, _dp, i, _iv, _dv, _dv, _iv, _iv, _dp]
+        L.lhlo_reduce_f32.restype = i
         L.lhlo_shift.argtypes = [i, _dp, i, d, d, _dp, i, _u8, _dv, _dv]
         L.lhlo_shift.restype = i
         L.lhlo_shift_f32.argtypes = [i, _dp, i, d, d, _dp, i, _u8, _dv, _dv]
@@ -141,6 +143,33 @@ def reduce(J, balance=True, path=0, nb=16) -> Reduction:
     ipm = np.zeros(max(n, 1), dtype=np.int64)
     Jp = J if n > 0 else np.zeros((1, 1), order="F")
     rc = lib().lhlo_reduce(n, Jp, max(n, 1), int(balance), path, nb, F, max(n, 1), ip, sc, isc, pm, ipm, Ht)
+    assert rc == 0
+    R.factors = F[:n, :n].copy(order="F")
+    R.ipiv = ip[: max(n - 2, 0)].copy()
+    R.scale, R.iscale = sc[:n].copy(), isc[:n].copy()
+    R.perm, R.iperm = pm[:n].copy(), ipm[:n].copy()
+    R.Ht = Ht[:n, :n].copy(order="F")
+    return R
+
+
+def reduce_f32(J, balance=True) -> Reduction:
+    """``lhl(J)`` on ``LHLWorkspace{Float32}`` below its blocked threshold (n < 1024): J rounded
+    to float, balancing and the unblocked reduction in float arithmetic (lhlo_reduce_f32).  The
+    arrays hold float values in float64."""
+    J = np.asfortranarray(J, dtype=np.float64)
+    n = J.shape[0]
+    if n >= 1024:
+        raise ValueError("the oracle restates the Float32 reduction below n = 1024 only")
+    R = Reduction(n)
+    ip = _ipiv_buf(n)
+    F = np.zeros((max(n, 1), max(n, 1)), order="F")
+    Ht = np.zeros((max(n, 1), max(n, 1)), order="F")
+    sc = np.ones(max(n, 1))
+    isc = np.ones(max(n, 1))
+    pm = np.zeros(max(n, 1), dtype=np.int64)
+    ipm = np.zeros(max(n, 1), dtype=np.int64)
+    Jp = J if n > 0 else np.zeros((1, 1), order="F")
+    rc = lib().lhlo_reduce_f32(n, Jp, max(n, 1), int(balance), F, max(n, 1), ip, sc, isc, pm, ipm, Ht)
     assert rc == 0
     R.factors = F[:n, :n].copy(order="F")
     R.ipiv = ip[: max(n - 2, 0)].copy()
