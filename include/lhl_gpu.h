@@ -128,19 +128,24 @@ int lhl_ws_import(lhl_ws_t ws, const double* dfactors, const double* dHt, const 
  * storage holding float values, so every view, shift object and solve entry point of this
  * header applies unchanged:
  *   - J is rounded to float on the way in (lhl_reduce) or taken as float (lhl_reduce_f32);
- *   - the reduction runs in FP64 (plain) or as the mixed form, and its factors and Ht are
- *     then rounded to float;
+ *   - below n = 1024 (_lhl_block_min(Float32), F:703-705) the plain form reduces in float
+ *     arithmetic as the reference does (balancing F:299-340 and the unblocked ELMHES F:466-678
+ *     with T = Float32); from n = 1024, and in the mixed form, the FP64 or mixed reduction
+ *     runs and its factors and Ht are rounded to float;
  *   - the shift LU (lhl_shift, lhl_shift_batched) runs in float arithmetic with sigma and tau
  *     rounded to float, as LHLShift{Float32} does (F:2529-2594 with T = Float32);
+ *   - complex shifts (LHLShift{ComplexF32}, a shift object from lhl_shift_create_complex):
+ *     sigma and tau rounded to ComplexF32, the LU in FP64 arithmetic on the float Ht;
  *   - solves take FP64 vectors (lhl_ldiv) or float ones (lhl_ldiv_f32, widened, solved in
- *     FP64 with the float factors, rounded back).
- * Complex shifts on a Float32 workspace are LHL_ERR_ARG. */
+ *     FP64 with the float factors, rounded back; ComplexF32 vectors, interleaved, for a
+ *     complex shift object). */
 int lhl_ws_create_f32(int64_t n, int precision, lhl_ws_t* ws);
 /* lhl_reduce!(ws, J, balance) with J Float32 (dJ n x n, ld ldj, float).  On a Float64
  * workspace the float values are taken exactly, as the reference converts them. */
 int lhl_reduce_f32(lhl_ws_t ws, const float* dJ, int64_t ldj, int balance, void* stream);
-/* lhl_ldiv!(x, sh, ws) for float right-hand sides (dX n x nrhs, ld ldx, float), in place.
- * The widened copy lives in a workspace buffer, allocated by the first call that needs it. */
+/* lhl_ldiv!(x, sh, ws) for float right-hand sides (dX n x nrhs, ld ldx, float; for a complex
+ * shift object interleaved ComplexF32, ld ldx complex elements), in place.  The widened copy
+ * lives in a workspace buffer, allocated by the first call that needs it. */
 int lhl_ldiv_f32(lhl_shift_t sh, lhl_ws_t ws, float* dX, int64_t ldx, int64_t nrhs, int64_t rhs_per_shift,
                  void* stream);
 

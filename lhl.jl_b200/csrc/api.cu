@@ -114,7 +114,7 @@ int lhl_ws_create(int64_t n, int precision, lhl_ws_t* out)
     A_(cand_v, w->grid > 0 ? w->grid : 1);
     A_(cand_s, w->grid > 0 ? w->grid : 1);
     A_(cand_i, w->grid > 0 ? w->grid : 1);
-    A_(buf2, n < 500 ? nn : 1);
+    A_(buf2, n < 1024 ? nn : 1);  // unblocked path: second buffer (FP64 n < 500; float n < 1024: two)
     A_(tsnap, (size_t)n * 17);
     A_(bsum, 2 * (size_t)n);
     A_(bfac, n);
@@ -317,10 +317,12 @@ int lhl_ws_set_probes(lhl_ws_t ws, int on)
 // The reduction of the matrix already copied into ws->F (the entry points below load it).
 static int reduce_loaded(lhl_ws_t ws, int balance, cudaStream_t st);
 
-// Float32 workspace: the reduction's factors and Ht rounded to float values, in place
+// Float32 workspace: the reduction's factors and Ht rounded to float values, in place (the
+// FP64 and mixed reductions; below n = 1024 the plain form already reduces in float)
 static int round_reduction_f32(lhl_ws_t ws, cudaStream_t st)
 {
     const int n = (int)ws->n;
+    if (n < 1024 && ws->precision != LHL_PREC_MIXED) return LHL_OK;
     cudaError_t e = lhl::launch_round_f32(ws->F, n, ws->F, n, n, n, st);
     if (e == cudaSuccess) e = lhl::launch_round_f32(ws->Ht, n, ws->Ht, n, n, n, st);
     return cuda_status(e);
@@ -468,6 +470,16 @@ static int reduce_loaded(lhl_ws_t ws, int balance, cudaStream_t st)
         if (lazy) return cuda_status(lhl::launch_lazy_finish((int)n, ws->F, ws->Ht, st));
         return cuda_status(lhl::launch_ht_fill((int)n, ws->F, ws->Ht, st));
     }
+    if (ws->f32 && n < 1024) {
+        // LHLWorkspace{Float32} below its blocked threshold: the reference's Float32 arithmetic
+        if (!balance) e = lhl::launch_fill_ones(ws->scale, ws->iscale, (int)n, st);
+        float* A32 = (float*)ws->buf2;
+        if (e == cudaSuccess) e = lhl::launch_reduce_f32(a, balance ? 1 : 0, A32, A32 + (size_t)n * n, st);
+        if (e == cudaSuccess)
+            e = lhl::launch_unblocked_assemble_f32((int)n, ws->F, A32, A32 + (size_t)n * n, ws->ipiv, st);
+        if (e == cudaSuccess) e = lhl::launch_ht_perm((int)n, ws->F, ws->Ht, ws->ipiv, ws->perm, ws->iperm, st);
+        return cuda_status(e);
+    }
     const int mode = n <= 2 ? 0 : (n < 500 ? 1 : 2);
     if (!balance) {
         // scale = iscale = 1
@@ -580,9 +592,18 @@ int lhl_shift_get_view(lhl_shift_t s, lhl_shift_view* v)
 static int shift_run(lhl_shift_t sh, lhl_ws_t ws, int64_t s0, int64_t count, cudaStream_t st)
 {
     cudaError_t e;
-    if (sh->cplx && ws->f32) return LHL_ERR_ARG;  // complex shifts need a Float64 workspace
     sh->cj = ws->cj;
     if (sh->cplx) {
+        // LHLShift{ComplexF32} on a Float32 workspace: sigma and tau rounded to ComplexF32 as the
+        // reference stores them; the LU itself runs in FP64 on the float Ht
+        if (ws->f32) {
+            e = lhl::launch_round_f32(sh->sigma + 2 * s0, (int)(2 * count), sh->sigma + 2 * s0, (int)(2 * count),
+                                      (int)(2 * count), 1, st);
+            if (e == cudaSuccess)
+                e = lhl::launch_round_f32(sh->tau + 2 * s0, (int)(2 * count), sh->tau + 2 * s0, (int)(2 * count),
+                                          (int)(2 * count), 1, st);
+            if (e != cudaSuccess) return LHL_ERR_CUDA;
+        }
         e = lhl::launch_shift_lu_cplx((int)ws->n, ws->Ht, (int)ws->n, sh->sigma + 2 * s0, sh->tau + 2 * s0, (int)s0,
                                       (int)count, sh->Gt, (int)sh->ldg, (int)sh->po, sh->swap, sh->rdiag, sh->info, st,
                                       ws->cj, ws->shift_variant[1]);
@@ -766,7 +787,6 @@ int lhl_ldiv_f32(lhl_shift_t sh, lhl_ws_t ws, float* dX, int64_t ldx, int64_t nr
                  void* stream)
 {
     if (!sh || !ws) return LHL_ERR_ARG;
-    if (sh->cplx) return LHL_ERR_ARG;
     if (sh->n != ws->n) return LHL_ERR_DIM;
     if (rhs_per_shift < 1) return LHL_ERR_ARG;
     if (nrhs < 0) return LHL_ERR_DIM;
@@ -776,7 +796,9 @@ int lhl_ldiv_f32(lhl_shift_t sh, lhl_ws_t ws, float* dX, int64_t ldx, int64_t nr
     if (!dX) return LHL_ERR_ARG;
     if (ldx < n) return LHL_ERR_DIM;
     cudaStream_t st = (cudaStream_t)stream;
-    const size_t need = (size_t)n * (size_t)nrhs;
+    // a complex shift takes ComplexF32 vectors: interleaved, 2n floats per column, ld 2 ldx
+    const int P = sh->cplx ? 2 : 1;
+    const size_t need = (size_t)P * (size_t)n * (size_t)nrhs;
     if (ws->f32x_cap < need || !ws->f32x) {
         if (ws->f32x) cudaFree(ws->f32x);
         ws->f32x = nullptr;
@@ -784,11 +806,13 @@ int lhl_ldiv_f32(lhl_shift_t sh, lhl_ws_t ws, float* dX, int64_t ldx, int64_t nr
         if (cudaMalloc((void**)&ws->f32x, need * sizeof(double)) != cudaSuccess) return LHL_ERR_ALLOC;
         ws->f32x_cap = need;
     }
-    if (lhl::launch_f32_to_f64(dX, (int)ldx, ws->f32x, (int)n, (int)n, (int)nrhs, st) != cudaSuccess)
+    if (lhl::launch_f32_to_f64(dX, (int)(P * ldx), ws->f32x, (int)(P * n), (int)(P * n), (int)nrhs, st) !=
+        cudaSuccess)
         return LHL_ERR_CUDA;
     const int rc = ldiv_common(sh, ws, ws->f32x, n, nrhs, rhs_per_shift, 0, st);
     if (rc != LHL_OK) return rc;
-    return cuda_status(lhl::launch_f64_to_f32(ws->f32x, (int)n, dX, (int)ldx, (int)n, (int)nrhs, st));
+    return cuda_status(
+        lhl::launch_f64_to_f32(ws->f32x, (int)(P * n), dX, (int)(P * ldx), (int)(P * n), (int)nrhs, st));
 }
 
 int lhl_applyZ(lhl_ws_t ws, double* dX, int64_t ldx, int64_t nrhs, void* stream)

@@ -155,6 +155,11 @@ cudaError_t launch_lazy_finish(int n, double* F, double* Ht, cudaStream_t st);
 
 cudaError_t launch_reduce(RedArgs a, int balance, int mode, cudaStream_t st);
 cudaError_t launch_unblocked_assemble(int n, double* A, const double* B2, const int64_t* ipiv, cudaStream_t st);
+// LHLWorkspace{Float32}, n < 1024: balancing and the unblocked reduction in float over the
+// buffers A32 / B32 (n x n floats each), then the factors widened into F
+cudaError_t launch_reduce_f32(RedArgs a, int balance, float* A32, float* B32, cudaStream_t st);
+cudaError_t launch_unblocked_assemble_f32(int n, double* F, const float* A32, const float* B32, const int64_t* ipiv,
+                                          cudaStream_t st);
 cudaError_t launch_ht_perm(int n, const double* A, double* Ht, const int64_t* ipiv, int64_t* perm, int64_t* iperm,
                            cudaStream_t st);
 cudaError_t launch_ht_fill(int n, const double* A, double* Ht, cudaStream_t st);

@@ -378,6 +378,159 @@ __global__ void __launch_bounds__(RT) unblocked_assemble_kernel(int n, double* o
 }
 
 // ---------------------------------------------------------------------------------
+// LHLWorkspace{Float32} below _lhl_block_min(Float32) = 1024 (F:703-705): J rounded to
+// float, balancing in float (F:299-340 with Tr = Float32) and the unblocked ELMHES in float
+// with the row-block kernel's per-row fma order (F:547-678; the paired sweep F:508-538 below
+// n = 8), so pivots, factors, Ht and scale are the reference's Float32 results.
+// ---------------------------------------------------------------------------------
+__device__ __forceinline__ bool balance_decide_f32(float c, float r, float& f)
+{
+    if (c == 0.0f || r == 0.0f) return false;
+    f = 1.0f;
+    const float s = __fadd_rn(c, r);
+    int guard = 0;  // never reached by finite norms; ends the loops on an infinite one
+    while (c < __fdiv_rn(r, 2.0f) && guard < 4200) {
+        c = __fmul_rn(c, 2.0f);
+        r = __fdiv_rn(r, 2.0f);
+        f = __fmul_rn(f, 2.0f);
+        ++guard;
+    }
+    while (c >= __fmul_rn(2.0f, r) && guard < 8400) {
+        c = __fdiv_rn(c, 2.0f);
+        r = __fmul_rn(r, 2.0f);
+        f = __fdiv_rn(f, 2.0f);
+        ++guard;
+    }
+    return __fadd_rn(c, r) < __fmul_rn(0.95f, s);
+}
+
+// Column and row 1-norms of index i without the diagonal, summed in j order, of the matrix
+// as the reference holds it when its sweep reaches i: the sweep's starting matrix with the
+// factors of the indices scaled so far in the sweep (row j divided by fac[j], column j
+// multiplied, the same single operations the reference applies); fac == nullptr: none yet.
+__device__ __forceinline__ void bal_sums_f32(const float* A, int n, int i, const float* fac, float& c, float& r)
+{
+    c = 0.0f;
+    r = 0.0f;
+    int j = 1;
+    for (; j + 7 <= n; j += 8) {
+        float vc[8], vr[8];
+#pragma unroll
+        for (int u = 0; u < 8; ++u) {
+            vc[u] = M1(A, n, j + u, i);
+            vr[u] = M1(A, n, i, j + u);
+        }
+#pragma unroll
+        for (int u = 0; u < 8; ++u) {
+            if (j + u == i) continue;
+            const float fc = fac ? __fdiv_rn(vc[u], fac[j + u - 1]) : vc[u];
+            const float fr = fac ? __fmul_rn(vr[u], fac[j + u - 1]) : vr[u];
+            c = __fadd_rn(c, fabsf(fc));
+            r = __fadd_rn(r, fabsf(fr));
+        }
+    }
+    for (; j <= n; ++j) {
+        if (j == i) continue;
+        const float vc = M1(A, n, j, i), vr = M1(A, n, i, j);
+        c = __fadd_rn(c, fabsf(fac ? __fdiv_rn(vc, fac[j - 1]) : vc));
+        r = __fadd_rn(r, fabsf(fac ? __fmul_rn(vr, fac[j - 1]) : vr));
+    }
+}
+
+// Balancing in float.  Per sweep: (1) every index's sums from the sweep's starting matrix,
+// one thread per index; (2) CTA 0 walks i = 1..n in order, RT indices at a time, and takes
+// the first index of the chunk that scales; once an index has scaled in the sweep, every
+// later chunk sums afresh with the sweep's factors so far (bal_sums_f32), so each decision
+// reads exactly the reference's sums; (3) all CTAs apply the sweep's factors to A in the
+// reference's order per element (row i divided when i is reached, column j multiplied when
+// j is: (a / f_i) f_j for i <= j, (a f_j) / f_i otherwise).
+__device__ bool balance_phase_f32(const RedArgs& a, float* A, GridBarrier& gb)
+{
+    const int n = a.n;
+    const int gt = blockIdx.x * RT + threadIdx.x;
+    const int gsz = gridDim.x * RT;
+    for (int i = gt; i < n; i += gsz) {
+        a.scale[i] = 1.0;
+        a.iscale[i] = 1.0;
+    }
+    __shared__ int s_first;
+    __shared__ float s_fac[1024];
+    for (int sweep = 0; sweep < 20; ++sweep) {
+        for (int i = 1 + gt; i <= n; i += gsz) {
+            float c, r;
+            bal_sums_f32(A, n, i, nullptr, c, r);
+            a.bsum[i - 1] = c;
+            a.bsum[n + i - 1] = r;
+            a.bfac[i - 1] = 1.0;
+        }
+        if (gt == 0) a.bflag[0] = 0;
+        if (!gb.sync()) return false;
+        if (blockIdx.x == 0) {
+            for (int i = threadIdx.x; i < n; i += RT) s_fac[i] = 1.0f;
+            bool fresh = false;  // an index has scaled in this sweep: sum afresh
+            int base = 1;
+            __syncthreads();
+            while (base <= n) {
+                if (threadIdx.x == 0) s_first = 0x7fffffff;
+                __syncthreads();
+                const int i = base + threadIdx.x;
+                float f = 1.0f;
+                if (i <= n) {
+                    float c, r;
+                    if (fresh) {
+                        bal_sums_f32(A, n, i, s_fac, c, r);
+                    } else {
+                        c = (float)a.bsum[i - 1];
+                        r = (float)a.bsum[n + i - 1];
+                    }
+                    if (balance_decide_f32(c, r, f)) atomicMin(&s_first, i);
+                }
+                __syncthreads();
+                const int si = s_first;
+                if (si == 0x7fffffff) {
+                    base += RT;
+                    continue;
+                }
+                if (i == si) {
+                    s_fac[si - 1] = f;
+                    a.bfac[si - 1] = f;
+                    a.bflag[0] = 1;
+                    a.scale[si - 1] = __fmul_rn((float)a.scale[si - 1], f);
+                    a.iscale[si - 1] = __fdiv_rn((float)a.iscale[si - 1], f);
+                }
+                __syncthreads();
+                fresh = true;
+                base = si + 1;
+            }
+        }
+        if (!gb.sync()) return false;
+        const int scaled = ((volatile int*)a.bflag)[0];
+        if (!scaled) break;
+        for (size_t e = gt; e < (size_t)n * n; e += gsz) {
+            const int i = (int)(e % n), j = (int)(e / n);
+            const float fi = (float)a.bfac[i], fj = (float)a.bfac[j];
+            if (fi != 1.0f || fj != 1.0f)
+                A[e] = i <= j ? __fmul_rn(__fdiv_rn(A[e], fi), fj) : __fdiv_rn(__fmul_rn(A[e], fj), fi);
+        }
+        if (!gb.sync()) return false;
+    }
+    return true;
+}
+
+// One cooperative launch: J (float values in a.A) into A32, balancing, the unblocked
+// reduction over the float buffers A32 / B32 (assembled into a.A by unblocked_assemble_kernel).
+__global__ void __launch_bounds__(RT, 1) reduce_f32_kernel(RedArgs a, int balance, float* A32, float* B32)
+{
+    GridBarrier gb{a.bar, a.err, a.limit_ns, 0, nullptr};
+    const int n = a.n;
+    const int gt = blockIdx.x * RT + threadIdx.x;
+    for (size_t e = gt; e < (size_t)n * n; e += (size_t)gridDim.x * RT) A32[e] = (float)a.A[e];
+    if (!gb.sync()) return;
+    if (balance && !balance_phase_f32(a, A32, gb)) return;
+    unblocked_phase<float>(a, gb, A32, B32);
+}
+
+// ---------------------------------------------------------------------------------
 // Blocked reduction (the reference's Float64 pointer path), nb = 16.
 // ---------------------------------------------------------------------------------
 struct PanelSh {
@@ -1467,7 +1620,31 @@ cudaError_t launch_reduce(RedArgs a, int balance, int mode, cudaStream_t st)
 cudaError_t launch_unblocked_assemble(int n, double* A, const double* B2, const int64_t* ipiv, cudaStream_t st)
 {
     if (n <= 0 || n > 512) return cudaErrorInvalidValue;
-    unblocked_assemble_kernel<<<n, RT, 0, st>>>(n, A, B2, ipiv);
+    unblocked_assemble_kernel<double><<<n, RT, 0, st>>>(n, A, A, B2, ipiv);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_reduce_f32(RedArgs a, int balance, float* A32, float* B32, cudaStream_t st)
+{
+    if (a.n < 1 || a.n >= 1024) return cudaErrorInvalidValue;
+    int dev = 0, sms = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e == cudaSuccess) e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    if (e != cudaSuccess) return e;
+    // one thread per row in warps of 32 rows; the candidate arrays hold one entry per CTA
+    const int rows = (a.n + 31) / 32, grid = rows < sms ? rows : sms;
+    reduce_init_kernel<<<64, 256, 0, st>>>(a.n, a.ipiv, a.cand_v, a.cand_i, grid);
+    e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+    void* args[] = {&a, &balance, &A32, &B32};
+    return cudaLaunchCooperativeKernel((void*)reduce_f32_kernel, dim3(grid), dim3(RT), args, 0, st);
+}
+
+cudaError_t launch_unblocked_assemble_f32(int n, double* F, const float* A32, const float* B32, const int64_t* ipiv,
+                                          cudaStream_t st)
+{
+    if (n <= 0 || n >= 1024) return cudaErrorInvalidValue;
+    unblocked_assemble_kernel<float><<<n, RT, 0, st>>>(n, F, A32, B32, ipiv);
     return cudaGetLastError();
 }
 

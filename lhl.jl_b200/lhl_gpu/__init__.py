@@ -300,9 +300,7 @@ class LHLWorkspace:
     def __init__(self, n: int, precision: int = LHL_PREC_FP64, shift_complex: bool = False,
                  dtype: torch.dtype = torch.float64):
         self._h = C.c_void_p()
-        if dtype == torch.float32:  # LHLWorkspace{Float32}
-            if shift_complex:
-                raise ArgumentError("complex shifts need a Float64 workspace")
+        if dtype == torch.float32:  # LHLWorkspace{Float32}; shift_complex: LHLShift{ComplexF32}
             _check(_lib.lhl_ws_create_f32(int(n), int(precision), C.byref(self._h)), "LHLWorkspace")
         elif dtype == torch.float64:
             _check(_lib.lhl_ws_create(int(n), int(precision), C.byref(self._h)), "LHLWorkspace")
@@ -645,6 +643,10 @@ def lhl_ldiv_(x: torch.Tensor, *args, rhs_per_shift: int = 1, stream=None) -> to
         raise ArgumentError("a complex right-hand side needs an LHLShift built for complex shifts")
     if x.dtype == torch.float32 and not sh.is_complex:  # float vectors: widened, solved, rounded back
         _require_cuda_real(x, "x")
+        fn = _lib.lhl_ldiv_f32
+    elif x.dtype == torch.complex64 and sh.is_complex:  # ComplexF32 vectors, the same way
+        if not x.is_cuda:
+            raise ArgumentError("x must be a CUDA tensor")
         fn = _lib.lhl_ldiv_f32
     else:
         _require_cuda_f64(x, "x", sh.is_complex)

@@ -3,9 +3,10 @@
 The shift LU bit for bit against the oracle's float restatement on the device's Ht
 (test/core_tests.jl:192-212 with T = Float32); solves against a dense LU with the reference's
 Float32 bounds (test/core_tests.jl:38-58: rtol 1e-3 and a backward error below 50 eps32 up to
-n = 500); the reduction is a valid similarity with float factors and the FP64 pivots; float
-right-hand sides in and out; a Float64 workspace takes float J exactly; complex shifts on a
-Float32 workspace are refused."""
+n = 500); the reduction bit for bit against the oracle's float restatement below n = 1024 and,
+from there, a valid similarity with float factors and the FP64 pivots; float
+right-hand sides in and out; a Float64 workspace takes float J exactly; ComplexF32 shifts and
+vectors on a Float32 workspace (test/core_tests.jl:324-329)."""
 import numpy as np
 import pytest
 
@@ -100,9 +101,66 @@ def test_f32_solves(n, precision):
     assert np.linalg.norm(x64 - xr) <= 1e-3 * np.linalg.norm(xr)
 
 
-@pytest.mark.parametrize("n", [5, 80, 300, 600])
-def test_f32_reduction_is_a_float_similarity(n):
-    """Plain form: the FP64 reduction of the widened J, rounded: FP64 pivots, float factors,
+F32_SIZES = list(range(1, 34)) + [64, 130, 255, 256, 257, 499, 500, 511, 512, 520, 777, 1000, 1023]
+
+
+def _f32_matrix(n, kind):
+    g = rng(4000 + n)
+    if kind == "tie":
+        return g.integers(-2, 3, (n, n)).astype(np.float32)
+    J = g.standard_normal((n, n))
+    if kind == "graded":
+        D = 2.0 ** g.integers(-10, 11, n)
+        J = (J * D[None, :]) / D[:, None]
+    return J.astype(np.float32)
+
+
+@pytest.mark.parametrize("n", F32_SIZES)
+@pytest.mark.parametrize("kind", ["gauss", "tie", "graded"])
+def test_f32_reduction_bitexact(n, kind):
+    """Below _lhl_block_min(Float32) = 1024 the Float32 workspace reduces in float, as the
+    reference does: balancing (F:299-340, Tr = Float32) and the unblocked ELMHES (F:466-678).
+    ipiv, factors, Ht, scale, iscale, perm and iperm bit for bit against the oracle's float
+    restatement, with and without balancing, through both entry points (J as float and as
+    float64 rounded on the way in)."""
+    torch, G = _mods()
+    J = _f32_matrix(n, kind)
+    for balance in (True, False):
+        R = O.reduce_f32(J.astype(np.float64), balance=balance)
+        for Jd in (dev(J), dev(J.astype(np.float64))):
+            ws = G.LHLWorkspace(n, dtype=torch.float32)
+            G.lhl_reduce_(ws, Jd, balance)
+            ws.check()
+            assert bits_equal(host(ws.factors), R.factors), (n, kind, balance)
+            assert np.array_equal(host(ws.ipiv)[: max(n - 2, 0)], R.ipiv)
+            assert bits_equal(host(ws.Ht), R.Ht)
+            assert bits_equal(host(ws.scale), R.scale) and bits_equal(host(ws.iscale), R.iscale)
+            assert np.array_equal(host(ws.perm), R.perm) and np.array_equal(host(ws.iperm), R.iperm)
+
+
+def test_f32_reduction_timeout_reports_and_recovers():
+    """The float reduction's grid barriers are bounded like the FP64 ones: a 1 ns limit ends it
+    with LHL_ERR_TIMEOUT, and the same workspace then reduces bit-exactly.  A graded matrix, so
+    that the other CTAs wait at a barrier while CTA 0 takes the balancing decisions."""
+    torch, G = _mods()
+    n = 1000
+    J = _f32_matrix(n, "graded")
+    ws = G.LHLWorkspace(n, dtype=torch.float32)
+    ws.set_barrier_limit_ns(1)
+    G.lhl_reduce_(ws, dev(J), True)
+    with pytest.raises(G.LHLDeviceError):
+        ws.check()
+    ws.set_barrier_limit_ns(2_000_000_000)
+    G.lhl_reduce_(ws, dev(J), True)
+    ws.check()
+    R = O.reduce_f32(J.astype(np.float64))
+    assert bits_equal(host(ws.factors), R.factors)
+
+
+@pytest.mark.parametrize("n", [1024, 1100])
+def test_f32_blocked_orders_are_a_float_similarity(n):
+    """From n = 1024 the reference runs its blocked Float32 form, which this build does not
+    restate: the FP64 reduction of the widened J, rounded.  FP64 pivots, float factors,
     Z H Z^-1 = J to float accuracy, |l| <= 1."""
     torch, G = _mods()
     J = rng(70 + n).standard_normal((n, n)).astype(np.float32)
@@ -123,8 +181,7 @@ def test_f32_reduction_is_a_float_similarity(n):
     Jd = J.astype(np.float64)
     rel = np.linalg.norm(R.Z() @ R.H @ R.Zinv() - Jd) / np.linalg.norm(Jd)
     assert rel <= 2 * EPS32 * n ** 1.5, rel  # the mixed form's bound: rounding the factors to float
-    if n > 2:
-        assert np.abs(np.tril(F, -2)).max() <= 1.0
+    assert np.abs(np.tril(F, -2)).max() <= 1.0
 
 
 def test_f64_workspace_takes_float_J_exactly():
@@ -137,12 +194,34 @@ def test_f64_workspace_takes_float_J_exactly():
     assert bits_equal(host(ws.factors), host(w2.factors))
 
 
-def test_f32_refuses_complex_shifts():
+def test_f32_complex_shifts_like_the_reference():
+    """test/core_tests.jl:324-329: lhl(J32; shift = ComplexF32), lhl_shift!(w32, 0.4 + 0.7im, -1),
+    lhl_ldiv! of a ComplexF32 vector against the dense solve, rtol 1e-3.  The shift is stored
+    rounded to ComplexF32; a block of ComplexF32 right-hand sides and a batch of shifts too."""
     torch, G = _mods()
-    J = rng(3).standard_normal((6, 6)).astype(np.float32)
-    with pytest.raises(G.ArgumentError):
-        G.lhl(dev(J), shift_complex=True)
-    ws = G.lhl(dev(J))
-    sh = G.LHLShift(6, 1, complex=True)
-    with pytest.raises(G.ArgumentError):
-        G.lhl_shift_batched_(sh, ws, dev(np.array([1.0 + 1j])), dev(np.array([-0.5 + 0j])))
+    n = 70
+    J = rng(95).standard_normal((n, n)).astype(np.float32)
+    b = (rng(96).standard_normal(n) + 1j * rng(97).standard_normal(n)).astype(np.complex64)
+    ws = G.lhl(dev(J), shift_complex=True)
+    assert ws.dtype == torch.float32 and ws.shift.is_complex
+    s = np.complex64(0.4 + 0.7j)
+    G.lhl_shift_(ws, complex(s), -1.0)
+    x = G.lhl_ldiv_(dev(b), ws)
+    assert x.dtype == torch.complex64
+    W = s * np.eye(n) - J.astype(np.complex128)
+    xr = np.linalg.solve(W, b.astype(np.complex128))
+    assert np.linalg.norm(host(x) - xr) <= 1e-3 * np.linalg.norm(xr)
+    assert ws.shift.σ == complex(s)  # stored rounded to ComplexF32 (0.4 and 0.7 are not floats)
+    # a batch of complex shifts, several ComplexF32 right-hand sides each
+    S, R = 3, 2
+    sh = G.LHLShift(n, S, complex=True)
+    sigs = np.array([0.4 + 0.7j, 1.5 - 0.2j, 3j], dtype=np.complex128)
+    taus = np.array([-1.0 + 0j, -0.5 + 0.1j, 1.0 + 0j], dtype=np.complex128)
+    G.lhl_shift_batched_(sh, ws, dev(sigs), dev(taus))
+    B = (rng(98).standard_normal((n, S * R)) + 1j * rng(99).standard_normal((n, S * R))).astype(np.complex64)
+    X = host(G.lhl_ldiv_(dev(B), sh, ws, rhs_per_shift=R))
+    for c in range(S * R):
+        sg, tg = sigs[c // R].astype(np.complex64), taus[c // R].astype(np.complex64)
+        Wc = sg * np.eye(n) + tg * J.astype(np.complex128)
+        xc = np.linalg.solve(Wc, B[:, c].astype(np.complex128))
+        assert np.linalg.norm(X[:, c] - xc) <= 1e-3 * np.linalg.norm(xc), c
