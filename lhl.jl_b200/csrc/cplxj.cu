@@ -1,11 +1,9 @@
 // cplxj.cu -- LHLWorkspace{ComplexF64}: the reduction of a complex J and the solves on it.
 //
 //   * balancing (F:299-340) with the complex modulus |z| = hypot(re, im) (cplx.cuh);
-//   * the unblocked ELMHES reduction (F:466-501) with the generic paired sweep (F:508-538),
-//     the path the reference takes for ComplexF64 below _lhl_block_min = 768 (F:703-705);
-//     at and above 768 the reference switches to its blocked form, whose pivots are the
-//     unblocked ones and whose factors agree with them to rounding (test/threading.jl:58-79);
-//     this build keeps the unblocked order at every n;
+//   * below _lhl_block_min = 768 (F:703-705) the unblocked ELMHES reduction (F:466-501) with
+//     the generic paired sweep (F:508-538); from 768 the generic blocked form (F:765-850 and
+//     its helpers), as the reference chooses (F:398-399);
 //   * Ht = H transposed (F:2005-2061) and perm / iperm (F:376-387);
 //   * lhl_ldiv! on the complex reduction (F:3111-3121): applyZinv! (gather with the real
 //     iscale, the generic L^-1 sweep F:2151-2195), the planar Hessenberg solve (complex.cu),
@@ -16,11 +14,12 @@
 // as a CuArray{ComplexF64}; scale and iscale are real.  The complex shift LU on the complex
 // Ht is complex.cu's kernel with a complex Ht.
 //
-// The reduction is one cooperative launch, one thread per row (rows by warps, spread over up to
-// one CTA per SM), double-buffered like the real unblocked kernel (reduce.cu): step k reads the
-// matrix of step k-1 with rows and columns k+1 <-> p swapped on the fly and writes the other
-// buffer, so a step needs one grid barrier (the pivot search).  Every element sees the
-// reference's complex operations in its order.
+// Either reduction is one cooperative launch, one thread per row (rows by warps, spread over up
+// to one CTA per SM).  The unblocked one is double-buffered like the real unblocked kernel
+// (reduce.cu): step k reads the matrix of step k-1 with rows and columns k+1 <-> p swapped on
+// the fly and writes the other buffer, so a step needs one grid barrier (the pivot search).
+// The blocked one works in place (cj_blocked).  Every element sees the reference's complex
+// operations in its order.
 #include "cplx.cuh"
 #include "internal.cuh"
 
@@ -269,6 +268,294 @@ __device__ bool cj_unblocked(const CjArgs& a, GridBarrier& gb, dc* s_l)
     return true;
 }
 
+// ---- the blocked form (n >= 768) ---------------------------------------------------
+// The generic delayed-update reduction the reference runs for T = ComplexF64 from
+// _lhl_block_min = 768 (F:398-399, F:705), nb = 16 (F:706).  Per panel k0..kb: the pre-panel
+// copy B0 of the panel columns; per step the pivot search, the step's interchanges
+// (F:857-890, CTA 0 alone: the row exchange over the panel columns, then the column exchange
+// within the panel or the pulled column with its missed interchanges and left transforms),
+// the multipliers and left transforms of the panel columns, the right transforms inside the
+// panel, the GEMV against the pre-panel trailing block (F:1418-1440, groups of four columns),
+// its interchanges and corrections, and the add into column k+1 (F:787-850).  Panel end: per
+// trailing column the row interchanges (F:1336-1342), the TRSM (F:1917-1927) and the rank-nb
+// GEMM with b = -one(T) * B element (F:1676-1689); the rows above the panel take their
+// in-panel right updates, then the top GEMM (F:1588-1607).  After the last panel the deferred
+// interchanges of the panel columns (F:1383-1393).  Every element sees the reference's complex
+// operations in its order.  One thread per row for the per-step work (rows by warps spread
+// over the CTAs), one CTA per trailing column for the panel-end update.
+constexpr int CJ_NB = 16;          // panel width (F:706)
+constexpr int CJ_BLOCK_MIN = 768;  // _lhl_block_min(ComplexF64), F:705
+
+// the rows the step interchanges of w touch and where each one's value comes from:
+// w[kk+1] <-> w[q] for kk = k0..k in order (F:826-829)
+struct CjPerm {
+    int row[2 * CJ_NB + 2];
+    int src[2 * CJ_NB + 2];
+    int cnt;
+};
+
+__device__ __forceinline__ int cj_perm_slot(CjPerm& P, int r)
+{
+    for (int s = 0; s < P.cnt; ++s)
+        if (P.row[s] == r) return s;
+    P.row[P.cnt] = r;
+    P.src[P.cnt] = r;
+    return P.cnt++;
+}
+
+__device__ __forceinline__ int cj_perm_src(const CjPerm& P, int r)
+{
+    for (int s = 0; s < P.cnt; ++s)
+        if (P.row[s] == r) return P.src[s];
+    return r;
+}
+
+// The interchange of step k with pivot row p != k+1 (F:806-808, F:857-890), CTA 0 alone.
+__device__ void cj_step_swaps(const CjArgs& a, double* B0, int k0, int kb, int k, int p)
+{
+    const int n = a.n, t = threadIdx.x;
+    double* A = a.A;
+    if (t == 0)
+        for (int j = k0; j <= kb + 1; ++j) {  // column k first in the reference; distinct elements
+            const dc x = ldc(A, n, k + 1, j);
+            stc(A, n, k + 1, j, ldc(A, n, p, j));
+            stc(A, n, p, j, x);
+        }
+    __syncthreads();
+    if (p <= kb + 1) {
+        for (int i = 1 + t; i <= n; i += CJT) {
+            const dc x = ldc(A, n, i, k + 1);
+            stc(A, n, i, k + 1, ldc(A, n, i, p));
+            stc(A, n, i, p, x);
+            const dc y = ldc(B0, n, i, k + 1 - k0);
+            stc(B0, n, i, k + 1 - k0, ldc(B0, n, i, p - k0));
+            stc(B0, n, i, p - k0, y);
+        }
+        __syncthreads();
+        return;
+    }
+    for (int i = 1 + t; i <= n; i += CJT) {
+        const dc x = ldc(A, n, i, p);
+        stc(A, n, i, p, ldc(B0, n, i, k + 1 - k0));
+        stc(B0, n, i, k + 1 - k0, x);
+        stc(A, n, i, k + 1, x);
+    }
+    __syncthreads();
+    if (t == 0)
+        for (int kk = k0; kk <= k; ++kk) {
+            const int q = (int)a.ipiv[kk - 1];
+            if (q != kk + 1) {
+                const dc x = ldc(A, n, kk + 1, k + 1);
+                stc(A, n, kk + 1, k + 1, ldc(A, n, q, k + 1));
+                stc(A, n, q, k + 1, x);
+            }
+        }
+    __syncthreads();
+    for (int kk = k0; kk <= k - 1; ++kk) {
+        const dc x = ldc(A, n, kk + 1, k + 1);
+        if (!ciszero(x))
+            for (int i = kk + 2 + t; i <= n; i += CJT) stc(A, n, i, k + 1, csub(ldc(A, n, i, k + 1), cmul(ldc(A, n, i, kk), x)));
+        __syncthreads();
+    }
+}
+
+// w for row r: sum over columns c0..c1 of A[j,k] A[r,j], from zero, four columns per pass
+__device__ __forceinline__ dc cj_gemv_row(const double* A, int n, int k, int r, int c0, int c1)
+{
+    dc acc = {0.0, 0.0};
+    int j = c0;
+#pragma unroll 2
+    for (; j + 3 <= c1; j += 4) {
+        const dc l1 = ldc(A, n, j, k), l2 = ldc(A, n, j + 1, k), l3 = ldc(A, n, j + 2, k), l4 = ldc(A, n, j + 3, k);
+        const dc a1 = ldc(A, n, r, j), a2 = ldc(A, n, r, j + 1), a3 = ldc(A, n, r, j + 2), a4 = ldc(A, n, r, j + 3);
+        acc = cadd(acc, cadd(cadd(cmul(l1, a1), cmul(l2, a2)), cadd(cmul(l3, a3), cmul(l4, a4))));
+    }
+    for (; j <= c1; ++j) {
+        const dc lj = ldc(A, n, j, k);
+        if (!ciszero(lj)) acc = cadd(acc, cmul(lj, ldc(A, n, r, j)));
+    }
+    return acc;
+}
+
+__device__ bool cj_blocked(const CjArgs& a, GridBarrier& gb)
+{
+    const int n = a.n;
+    double* A = a.A;
+    double* B0 = a.B;                                 // n x (nb + 1) complex
+    double* w = a.B + 2 * (size_t)n * (CJ_NB + 1);    // the chain rows' GEMV values (n complex)
+    __shared__ double s_red[CJW];
+    __shared__ int s_redi[CJW];
+    __shared__ int s_p;
+    __shared__ CjPerm s_perm;
+    __shared__ dc s_w[CJ_NB + 2], s_x[CJ_NB + 1], s_b[CJ_NB + 1];
+    const int t = threadIdx.x;
+    const int gt = blockIdx.x * CJT + t, gsz = gridDim.x * CJT;
+    const int r = 32 * ((t >> 5) * (int)gridDim.x + (int)blockIdx.x) + (t & 31) + 1;  // this thread's row
+    const dc minus_one = {-1.0, -0.0}, one = {1.0, 0.0};
+    {
+        double v = 0.0;
+        int vi = 0;
+        if (r >= 2 && r <= n) { v = cabs_h(ldc(A, n, r, 1)); vi = r; }
+        cj_publish(a, v, vi, s_red, s_redi);
+    }
+    if (!gb.sync()) return false;
+    for (int k0 = 1; k0 <= n - 2; k0 += CJ_NB) {
+        const int kb = k0 + CJ_NB - 1 < n - 2 ? k0 + CJ_NB - 1 : n - 2;
+        const int np = kb + 1 - k0;  // panel columns k0+1..kb+1
+        for (size_t e = gt; e < (size_t)n * np; e += gsz) {
+            const int i = (int)(e % n) + 1, jj = (int)(e / n) + 1;
+            stc(B0, n, i, jj, ldc(A, n, i, k0 + jj));
+        }
+        if (!gb.sync()) return false;
+        for (int k = k0; k <= kb; ++k) {
+            cj_combine(a, &s_p, s_red, s_redi);
+            const int p = (s_p >= k + 1 && s_p <= n) ? s_p : k + 1;
+            if (gt == 0) a.ipiv[k - 1] = p;
+            if (p != k + 1) {
+                if (blockIdx.x == 0) {
+                    __syncthreads();  // ipiv[k-1] from thread 0
+                    cj_step_swaps(a, B0, k0, kb, k, p);
+                }
+                if (!gb.sync()) return false;
+            }
+            const dc piv = ldc(A, n, k + 1, k);
+            if (!ciszero(piv)) {
+                // multipliers and the left transforms of the panel columns (F:813-821)
+                if (r >= k + 2 && r <= n) {
+                    const dc l = cdiv(ldc(A, n, r, k), piv);
+                    stc(A, n, r, k, l);
+                    for (int j = k + 1; j <= kb + 1; ++j) {
+                        const dc pj = ldc(A, n, k + 1, j);
+                        if (!ciszero(pj)) stc(A, n, r, j, csub(ldc(A, n, r, j), cmul(l, pj)));
+                    }
+                }
+                if (t == 0) {  // the step interchanges of w, as a map of the touched rows
+                    s_perm.cnt = 0;
+                    for (int kk = k0; kk <= k; ++kk) {
+                        const int q = kk == k ? p : (int)a.ipiv[kk - 1];  // step k's entry may not be visible yet
+                        if (q == kk + 1) continue;
+                        const int s1 = cj_perm_slot(s_perm, kk + 1), s2 = cj_perm_slot(s_perm, q);
+                        const int x = s_perm.src[s1];
+                        s_perm.src[s1] = s_perm.src[s2];
+                        s_perm.src[s2] = x;
+                    }
+                }
+                if (!gb.sync()) return false;
+                // right transforms inside the panel (F:822-827), then the GEMV of the row whose
+                // value the interchanges bring to this row (F:829-833)
+                dc acc = {0.0, 0.0}, wv = {0.0, 0.0};
+                const bool mine = r >= k0 + 1 && r <= n;
+                if (mine) {
+                    acc = ldc(A, n, r, k + 1);
+                    for (int j = k + 2; j <= kb + 1; ++j) {
+                        const dc vj = ldc(A, n, j, k);
+                        if (!ciszero(vj)) acc = cadd(acc, cmul(vj, ldc(A, n, r, j)));
+                    }
+                    wv = cj_gemv_row(A, n, k, cj_perm_src(s_perm, r), kb + 2, n);
+                    if (r <= k + 1) stc(w, n, r, 1, wv);
+                }
+                if (!gb.sync()) return false;
+                // the corrections' chain on the rows k0+1..k+1, in every CTA (F:834-839)
+                if (t == 0) {
+                    for (int i = k0 + 1; i <= k + 1; ++i) s_w[i - k0] = ldc(w, n, i, 1);
+                    for (int kk = k0; kk <= k; ++kk) {
+                        const dc x = s_w[kk + 1 - k0];
+                        s_x[kk - k0] = x;
+                        if (ciszero(x)) continue;
+                        for (int i = kk + 2; i <= k + 1; ++i) s_w[i - k0] = csub(s_w[i - k0], cmul(ldc(A, n, i, kk), x));
+                    }
+                }
+                __syncthreads();
+                if (mine) {
+                    if (r <= k + 1) {
+                        wv = s_w[r - k0];
+                    } else {
+                        for (int kk = k0; kk <= k; ++kk) {
+                            const dc x = s_x[kk - k0];
+                            if (!ciszero(x)) wv = csub(wv, cmul(ldc(A, n, r, kk), x));
+                        }
+                    }
+                    stc(A, n, r, k + 1, cadd(acc, wv));  // F:840-842
+                }
+            }
+            // the next step's pivot candidates: column k+1, rows k+2..n
+            double v = 0.0;
+            int vi = 0;
+            if (r >= k + 2 && r <= n) { v = cabs_h(ldc(A, n, r, k + 1)); vi = r; }
+            cj_publish(a, v, vi, s_red, s_redi);
+            if (!gb.sync()) return false;
+        }
+        // panel end, trailing columns: interchanges, TRSM, GEMM (one CTA per column)
+        for (int c = kb + 2 + (int)blockIdx.x; c <= n; c += gridDim.x) {
+            if (t == 0) {
+                for (int k = k0; k <= kb; ++k) {
+                    const int q = (int)a.ipiv[k - 1];
+                    if (q != k + 1) {
+                        const dc x = ldc(A, n, k + 1, c);
+                        stc(A, n, k + 1, c, ldc(A, n, q, c));
+                        stc(A, n, q, c, x);
+                    }
+                }
+                for (int k = k0; k <= kb; ++k) {
+                    const dc x = ldc(A, n, k + 1, c);
+                    if (ciszero(x)) continue;
+                    for (int i = k + 2; i <= kb + 1; ++i) stc(A, n, i, c, csub(ldc(A, n, i, c), cmul(ldc(A, n, i, k), x)));
+                }
+                for (int j = k0; j <= kb; ++j) s_b[j - k0] = cmul(minus_one, ldc(A, n, j + 1, c));
+            }
+            __syncthreads();
+            for (int i = kb + 2 + t; i <= n; i += CJT) {
+                dc x = ldc(A, n, i, c);
+                for (int j = k0; j <= kb; ++j) {
+                    const dc b = s_b[j - k0];
+                    if (!ciszero(b)) x = cadd(x, cmul(ldc(A, n, i, j), b));
+                }
+                stc(A, n, i, c, x);
+            }
+            __syncthreads();
+        }
+        // rows above the panel: the in-panel right updates (F:1597-1606) ...
+        for (int i = 1 + gt; i <= k0; i += gsz)
+            for (int k = k0; k <= kb; ++k)
+                for (int j = k + 2; j <= kb + 1; ++j) {
+                    const dc vj = ldc(A, n, j, k);
+                    if (!ciszero(vj)) stc(A, n, i, k + 1, cadd(ldc(A, n, i, k + 1), cmul(vj, ldc(A, n, i, j))));
+                }
+        if (!gb.sync()) return false;
+        // ... then the top GEMM A[1:k0, k0+1:kb+1] += A[1:k0, kb+2:n] * (one * A[kb+2:n, k0:kb])
+        for (size_t e = gt; e < (size_t)k0 * np; e += gsz) {
+            const int i = (int)(e % k0) + 1, c = k0 + 1 + (int)(e / k0);
+            dc x = ldc(A, n, i, c);
+            for (int j = kb + 2; j <= n; ++j) {
+                const dc b = cmul(one, ldc(A, n, j, c - 1));
+                if (!ciszero(b)) x = cadd(x, cmul(ldc(A, n, i, j), b));
+            }
+            stc(A, n, i, c, x);
+        }
+        if (!gb.sync()) return false;
+    }
+    // the interchanges deferred on the multipliers (F:1383-1393)
+    for (int c = 1 + gt; c <= n - 2; c += gsz) {
+        const int kbc = ((c - 1) / CJ_NB + 1) * CJ_NB < n - 2 ? ((c - 1) / CJ_NB + 1) * CJ_NB : n - 2;
+        for (int k = kbc + 1; k <= n - 2; ++k) {
+            const int q = (int)a.ipiv[k - 1];
+            if (q != k + 1) {
+                const dc x = ldc(A, n, k + 1, c);
+                stc(A, n, k + 1, c, ldc(A, n, q, c));
+                stc(A, n, q, c, x);
+            }
+        }
+    }
+    return true;
+}
+
+__global__ void __launch_bounds__(CJT, 1) cj_blocked_kernel(CjArgs a, int balance)
+{
+    GridBarrier gb{a.bar, a.err, a.limit_ns, 0, nullptr};
+    if (balance && !cj_balance(a, gb)) return;
+    if (a.n >= 3) cj_blocked(a, gb);
+}
+
 __global__ void __launch_bounds__(CJT, 1) cj_reduce_kernel(CjArgs a, int balance)
 {
     extern __shared__ double2 cj_dyn[];
@@ -382,9 +669,11 @@ cudaError_t launch_reduce_cj(CjArgs a, int balance, cudaStream_t st)
     if (e != cudaSuccess) return e;
     int bal = balance;
     void* args[] = {&a, &bal};
-    e = cudaLaunchCooperativeKernel((void*)cj_reduce_kernel, dim3(grid), dim3(CJT), args, smem, st);
+    const bool blocked = n >= CJ_BLOCK_MIN;  // the reference's choice (F:398-399, F:705)
+    e = blocked ? cudaLaunchCooperativeKernel((void*)cj_blocked_kernel, dim3(grid), dim3(CJT), args, 0, st)
+                : cudaLaunchCooperativeKernel((void*)cj_reduce_kernel, dim3(grid), dim3(CJT), args, smem, st);
     if (e != cudaSuccess) return e;
-    if (n >= 3) {
+    if (n >= 3 && !blocked) {
         cj_assemble_kernel<<<n, CJT, smem, st>>>(n, a.A, a.B, a.ipiv);
         e = cudaGetLastError();
         if (e != cudaSuccess) return e;

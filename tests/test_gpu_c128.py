@@ -54,13 +54,15 @@ def matrix(n, kind, seed):
     return crandn(g, n, n)
 
 
-@pytest.mark.parametrize("n", list(range(1, 18)) + [31, 64, 65, 129, 256, 300, 600])
+@pytest.mark.parametrize("n", list(range(1, 18)) + [31, 64, 65, 129, 256, 300, 600, 767, 768, 769, 800, 1030])
 @pytest.mark.parametrize("kind", ["randn", "tie", "graded"])
 @pytest.mark.parametrize("balance", [True, False])
 def test_complex_reduction_bitexact(n, kind, balance):
+    """The reference's own order at every n: unblocked below _lhl_block_min(ComplexF64) = 768,
+    the generic blocked form (nb = 16) from there (F:398-399, F:703-706)."""
     torch, G = _mods()
     J = matrix(n, kind, 100 + n)
-    R = O.reduce_c128(J, balance)
+    R = O.reduce_c128(J, balance, path=2)
     ws = G.lhl(dev(J), balance=balance)
     assert ws.dtype == torch.complex128 and ws.shift.is_complex
     torch.cuda.synchronize()
@@ -242,8 +244,9 @@ def test_complex_refinement_to_tolerance_and_gmres():
 
 
 def test_complex_above_block_threshold():
-    """n = 1000 (>= 768, where the reference would switch to its blocked form): the unblocked
-    order still reconstructs J and solves to 1e-9."""
+    """n = 1000 (>= 768: the reference's blocked form): the factors reconstruct J and are the
+    oracle's blocked factors bit for bit, the pivots are the unblocked order's
+    (test/threading.jl:58-79), and a shifted solve agrees with a dense solve to 1e-9."""
     torch, G = _mods()
     g = np.random.default_rng(1000)
     n = 1000
@@ -257,6 +260,9 @@ def test_complex_above_block_threshold():
     Zh, Zih = host(Z), host(Zi)
     assert np.linalg.norm(Zh @ H @ Zih - J) <= 1e-9 * np.linalg.norm(J)
     assert np.abs(np.tril(host(ws.factors), -2)).max() <= 1.0
+    Ru = O.reduce_c128(J, True, path=0)
+    assert np.array_equal(host(ws.ipiv), Ru.ipiv)
+    assert bits_equal(host(ws.factors), O.reduce_c128(J, True, path=2).factors)
     b = crandn(g, n)
     G.lhl_shift_(ws, 1, -0.01 + 0.02j)
     x = host(G.lhl_ldiv_(dev(b), ws))
