@@ -528,11 +528,17 @@ __global__ void __launch_bounds__(MT, 2) hess_cplx_mrhs_kernel(int n, const doub
                     far[a] = sm.U[st][0][8 * a + g8][kk];
                     fai[a] = sm.U[st][1][8 * a + g8][kk];
                 }
+                // two passes over the eight accumulators, so that the two products into one
+                // accumulator are eight instructions apart (each waits for the previous result)
+                const double nxi = -xi;
 #pragma unroll
                 for (int a = 0; a < 4; ++a) {
                     dmma_8x8x4(acc[a][0], far[a], xr);   // Re U Re x
                     dmma_8x8x4(acc[a][1], far[a], xi);   // Re U Im x
-                    dmma_8x8x4(acc[a][0], fai[a], -xi);  // - Im U Im x
+                }
+#pragma unroll
+                for (int a = 0; a < 4; ++a) {
+                    dmma_8x8x4(acc[a][0], fai[a], nxi);  // - Im U Im x
                     dmma_8x8x4(acc[a][1], fai[a], xr);   // Im U Re x
                 }
             }

@@ -191,11 +191,27 @@ __device__ bool balance_phase(const RedArgs& a, GridBarrier& gb)
                 const double fs = s_f;
                 // patch the sums of m > si: row si's entry in column m is divided by fs,
                 // column si's entry in row m multiplied (indices > si are unscaled so far)
-                for (int m = si + 1 + threadIdx.x; m <= n; m += RT) {
-                    const double vr = fabs(M1(A, n, si, m));
-                    const double vc = fabs(M1(A, n, m, si));
-                    a.bsum[m - 1] = (a.bsum[m - 1] - vr) + vr / fs;
-                    a.bsum[n + m - 1] = (a.bsum[n + m - 1] - vc) + vc * fs;
+                // (four indices per thread at a time, every load issued before the stores)
+                for (int m0 = si + 1 + threadIdx.x; m0 <= n; m0 += 4 * RT) {
+                    double vr[4], vc[4], br[4], bc[4];
+#pragma unroll
+                    for (int u = 0; u < 4; ++u) {
+                        const int m = m0 + u * RT;
+                        if (m <= n) {
+                            vr[u] = fabs(M1(A, n, si, m));
+                            vc[u] = fabs(M1(A, n, m, si));
+                            br[u] = a.bsum[m - 1];
+                            bc[u] = a.bsum[n + m - 1];
+                        }
+                    }
+#pragma unroll
+                    for (int u = 0; u < 4; ++u) {
+                        const int m = m0 + u * RT;
+                        if (m <= n) {
+                            a.bsum[m - 1] = (br[u] - vr[u]) + vr[u] / fs;
+                            a.bsum[n + m - 1] = (bc[u] - vc[u]) + vc[u] * fs;
+                        }
+                    }
                 }
                 if (threadIdx.x == 0) {
                     a.bfac[si - 1] = fs;

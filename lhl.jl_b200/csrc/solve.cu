@@ -881,65 +881,82 @@ __global__ void __launch_bounds__(ZWT, 2) zlw_kernel(ZArgs z)
         // products with the blocks j < i (L^-1 sweep) or j <= i (L sweep; L's diagonal is
         // stored as zero and the unit part is the initial value above)
         const int jend = MUL ? i : i - 1;
-        for (int j = 0; j <= jend; ++j) {
-            if (!MUL) {
-                if (t == 0) {
-                    int ok = 1;
-                    const int* f = z.flags + (size_t)j * ntile + c;
-                    const uint64_t t0 = globaltimer_ns();
-                    unsigned spins = 0;
-                    while (ld_acquire_i32(f) != 1) {
-                        if ((++spins & 63u) == 0) {
-                            if (ld_acquire_i32(z.err) != 0) { ok = 0; break; }
-                            if (globaltimer_ns() - t0 > z.limit_ns) {
-                                atomicCAS(z.err, 0, (int)LHL_ERR_TIMEOUT);
-                                ok = 0;
-                                break;
-                            }
+        // block j's readiness (its flag, set when that block of this column tile is solved); the
+        // wait is bounded and ends the kernel with LHL_ERR_TIMEOUT
+        auto ready = [&](int j) -> bool {
+            if (MUL) return true;
+            if (t == 0) {
+                int ok = 1;
+                const int* f = z.flags + (size_t)j * ntile + c;
+                const uint64_t t0 = globaltimer_ns();
+                unsigned spins = 0;
+                while (ld_acquire_i32(f) != 1) {
+                    if ((++spins & 63u) == 0) {
+                        if (ld_acquire_i32(z.err) != 0) { ok = 0; break; }
+                        if (globaltimer_ns() - t0 > z.limit_ns) {
+                            atomicCAS(z.err, 0, (int)LHL_ERR_TIMEOUT);
+                            ok = 0;
+                            break;
                         }
                     }
-                    sm.ok = ok;
                 }
-                __syncthreads();
-                if (!sm.ok) return;
+                sm.ok = ok;
             }
-            auto stage = [&](int h, int st) {  // K half h (columns 32 h .. of block j)
-                for (int e = t; e < ZWK * ZWR; e += ZWT) {
-                    const int rr = e % ZWR, qq = e / ZWR;
-                    const int gr = i * ZWR + rr, q = j * ZWR + h * ZWK + qq;
-                    // L[gr][q] = F[(q-1) ldf + gr] for 1 <= q <= n-2 and gr >= q+1, else 0
-                    const bool ok = gr < n && q >= 1 && q <= n - 2 && gr >= q + 1;
-                    cp_async8(&sm.A[st][qq][rr], ok ? &z.F[(size_t)(q - 1) * z.ldf + gr] : z.F, ok, z.F);
-                }
-                for (int e = t; e < ZWK * ZWC; e += ZWT) {
-                    const int qq = e % ZWK, cc = e / ZWK;
-                    const int q = j * ZWR + h * ZWK + qq, col = c * ZWC + cc;
-                    const bool ok = q < n && col < m;
-                    cp_async8(&sm.B[st][qq][cc], ok ? &yb[(size_t)col * ldy + q] : z.F, ok, z.F);
-                }
-                cp_async_commit();
-            };
+            __syncthreads();
+            return sm.ok != 0;
+        };
+        auto stage = [&](int q, int st) {  // K chunk q: half q & 1 (columns 32 (q & 1) ..) of block q >> 1
+            const int j = q >> 1, h = q & 1;
+            for (int e = t; e < ZWK * ZWR; e += ZWT) {
+                const int rr = e % ZWR, qq = e / ZWR;
+                const int gr = i * ZWR + rr, k = j * ZWR + h * ZWK + qq;
+                // L[gr][k] = F[(k-1) ldf + gr] for 1 <= k <= n-2 and gr >= k+1, else 0
+                const bool ok = gr < n && k >= 1 && k <= n - 2 && gr >= k + 1;
+                cp_async8(&sm.A[st][qq][rr], ok ? &z.F[(size_t)(k - 1) * z.ldf + gr] : z.F, ok, z.F);
+            }
+            for (int e = t; e < ZWK * ZWC; e += ZWT) {
+                const int qq = e % ZWK, cc = e / ZWK;
+                const int k = j * ZWR + h * ZWK + qq, col = c * ZWC + cc;
+                const bool ok = k < n && col < m;
+                cp_async8(&sm.B[st][qq][cc], ok ? &yb[(size_t)col * ldy + k] : z.F, ok, z.F);
+            }
+            cp_async_commit();
+        };
+        // products with the blocks j < i (L^-1 sweep) or j <= i (L sweep; L's diagonal is
+        // stored as zero and the unit part is the initial value above), as one stream of K
+        // chunks over the two stages: chunk q + 1 (the next block's first half included) is in
+        // flight while chunk q is multiplied
+        const int nq = 2 * (jend + 1);
+        if (nq > 0) {
+            if (!ready(0)) return;
             stage(0, 0);
-            stage(1, 1);
-#pragma unroll
-            for (int h = 0; h < 2; ++h) {
-                if (h == 0) cp_async_wait<1>();
-                else cp_async_wait<0>();
-                __syncthreads();
-#pragma unroll
-                for (int kk = 0; kk < ZWK; kk += 4) {
-                    double fa[4], fb[2];
-#pragma unroll
-                    for (int a = 0; a < 4; ++a) fa[a] = sgn * sm.A[h][kk + t4][32 * wm + 8 * a + g];
-#pragma unroll
-                    for (int b = 0; b < 2; ++b) fb[b] = sm.B[h][kk + t4][16 * wn + 8 * b + g];
-#pragma unroll
-                    for (int a = 0; a < 4; ++a)
-#pragma unroll
-                        for (int b = 0; b < 2; ++b) dmma_8x8x4(acc[a][b], fa[a], fb[b]);
+        }
+        for (int q = 0; q < nq; ++q) {
+            const int st = q & 1;
+            if (q + 1 < nq) {
+                if (((q + 1) & 1) == 0 && !ready((q + 1) >> 1)) {
+                    cp_async_wait<0>();  // nothing of this CTA's stays in flight into shared memory
+                    return;
                 }
+                stage(q + 1, st ^ 1);
+                cp_async_wait<1>();
+            } else {
+                cp_async_wait<0>();
             }
-            __syncthreads();  // both stages free for the next block
+            __syncthreads();
+#pragma unroll
+            for (int kk = 0; kk < ZWK; kk += 4) {
+                double fa[4], fb[2];
+#pragma unroll
+                for (int a = 0; a < 4; ++a) fa[a] = sgn * sm.A[st][kk + t4][32 * wm + 8 * a + g];
+#pragma unroll
+                for (int b = 0; b < 2; ++b) fb[b] = sm.B[st][kk + t4][16 * wn + 8 * b + g];
+#pragma unroll
+                for (int a = 0; a < 4; ++a)
+#pragma unroll
+                    for (int b = 0; b < 2; ++b) dmma_8x8x4(acc[a][b], fa[a], fb[b]);
+            }
+            __syncthreads();  // stage st is refilled by the next iteration's copy
         }
         if constexpr (MUL) {  // x[perm[row]] = (L y)[row] * scale[perm[row]]
 #pragma unroll
