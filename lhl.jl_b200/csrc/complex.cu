@@ -52,8 +52,10 @@ __global__ void __launch_bounds__(T, 1) shift_lu_cplx_kernel(int n, const double
     __shared__ int s_info;
 
     dc r[E];
-    HV h[E];     // Ht[j, k+1] for the current step
-    HV hsub[E];  // Ht[j, j+1]: the subdiagonal of the step this thread decides
+    HV h[E];  // Ht[j, k+1] for the current step, reloaded in place for the next one
+    // Ht[j, j+1] for the one element j whose pivot decision this thread takes next (step j,
+    // taken during step j - 1): loaded a step ahead by the owner of element k + 2
+    HV hs = hzero<HV>();
 #pragma unroll
     for (int e = 0; e < E; ++e) {
         const int j = 1 + t + e * T;
@@ -63,8 +65,7 @@ __global__ void __launch_bounds__(T, 1) shift_lu_cplx_kernel(int n, const double
         if (j == 1) r[e] = cadd(r[e], sigma);
         h[e] = hzero<HV>();
         if (j <= n && n >= 2) ht_load(Ht, ldh, j, 2, h[e]);
-        hsub[e] = hzero<HV>();
-        if (j + 1 <= n) ht_load(Ht, ldh, j, j + 1, hsub[e]);
+        if (j == 2 && j + 1 <= n) ht_load(Ht, ldh, j, j + 1, hs);  // decides step 2, during step 1
     }
     auto decide = [&](int k, dc a, HV hs) {
         const dc b = tmul(tau, hs);
@@ -81,7 +82,11 @@ __global__ void __launch_bounds__(T, 1) shift_lu_cplx_kernel(int n, const double
     if (t == 0) {
         s_next[1] = r[0];
         s_info = 0;
-        if (n >= 2) decide(1, r[0], hsub[0]);
+        if (n >= 2) {
+            HV h12 = hzero<HV>();
+            ht_load(Ht, ldh, 1, 2, h12);
+            decide(1, r[0], h12);
+        }
     }
     __syncthreads();
     for (int k = 1; k <= n - 1; ++k) {
@@ -97,13 +102,9 @@ __global__ void __launch_bounds__(T, 1) shift_lu_cplx_kernel(int n, const double
             M1(Gt, ldg, po + k, k + 1) = l.im;
             if (!sw && a.re == 0.0 && a.im == 0.0 && s_info == 0) s_info = k;
         }
-        HV hn[E];
-#pragma unroll
-        for (int e = 0; e < E; ++e) {
-            const int j = 1 + t + e * T;
-            hn[e] = hzero<HV>();
-            if (j >= k + 1 && j <= n && k + 2 <= n) ht_load(Ht, ldh, j, k + 2, hn[e]);
-        }
+        // the subdiagonal entry of the decision this thread takes next step (element k + 2)
+        HV hs_next = hs;
+        if (k + 3 <= n && (k + 1) % T == t) ht_load(Ht, ldh, k + 2, k + 3, hs_next);
 #pragma unroll
         for (int e = 0; e < E; ++e) {
             const int j = 1 + t + e * T;
@@ -129,11 +130,13 @@ __global__ void __launch_bounds__(T, 1) shift_lu_cplx_kernel(int n, const double
                 M1(Gt, ldg, po + j, k) = gk.im;
                 if (j == k + 1) {  // owner of element k+1: publish it and decide step k+1
                     s_next[(k + 1) & 1] = r[e];
-                    if (k + 1 <= n - 1) decide(k + 1, r[e], hsub[e]);
+                    if (k + 1 <= n - 1) decide(k + 1, r[e], hs);
                 }
             }
-            h[e] = hn[e];
+            // Ht[j, k+2] for the next step, into the same register
+            if (j >= k + 1 && j <= n && k + 2 <= n) ht_load(Ht, ldh, j, k + 2, h[e]);
         }
+        hs = hs_next;
         __syncthreads();
     }
     if (t == 0) {  // finish (F:2579-2594)
@@ -155,7 +158,8 @@ __global__ void __launch_bounds__(T, 1) shift_lu_cplx_kernel(int n, const double
 
 // Launch shapes of the complex shift LU (threads T, elements per thread E), selectable per
 // workspace like the real ones (same bits for every shape); shape v serves n <= T E.
-static const int kCShiftShapes[][2] = {{256, 1}, {512, 2}, {512, 4}, {512, 8}, {1024, 8}, {1024, 2}, {1024, 4}, {256, 4}};
+static const int kCShiftShapes[][2] = {{256, 1}, {512, 2}, {512, 4}, {512, 8}, {1024, 8}, {1024, 2}, {1024, 4}, {256, 4},
+                                        {512, 16}, {256, 32}};
 constexpr int kNumCShiftShapes = sizeof(kCShiftShapes) / sizeof(kCShiftShapes[0]);
 
 int shift_shape_cplx(int variant, int* T, int* E)
@@ -191,6 +195,8 @@ cudaError_t launch_shift_lu_cplx(int n, const double* Ht, int ldh, const double*
             case 6: L_(1024, 2); break;
             case 7: L_(1024, 4); break;
             case 8: L_(256, 4); break;
+            case 9: L_(512, 16); break;
+            case 10: L_(256, 32); break;
             default: return cudaErrorInvalidValue;
         }
         return cudaGetLastError();
@@ -199,7 +205,7 @@ cudaError_t launch_shift_lu_cplx(int n, const double* Ht, int ldh, const double*
     else if (n <= 1024) L_(512, 2);
     else if (n <= 2048) L_(512, 4);
     else if (n <= 4096) L_(512, 8);
-    else if (n <= 8192) L_(1024, 8);
+    else if (n <= 8192) L_(512, 16);
     else return cudaErrorInvalidValue;
 #undef L_
     return cudaGetLastError();

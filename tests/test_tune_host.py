@@ -107,4 +107,4 @@ def test_python_lists_the_shapes_that_cover_an_order():
     v = G.shift_variants(False, 2048)
     assert v and all(G.shift_variant_shape(False, k)[0] * G.shift_variant_shape(False, k)[1] >= 2048 for k in v)
     assert 1 not in v  # 256 x 1 does not cover 2048
-    assert G.shift_variants(True, 8192) == [5]
+    assert G.shift_variants(True, 8192) == [5, 9, 10]  # 1024 x 8, 512 x 16, 256 x 32
