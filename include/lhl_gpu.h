@@ -128,10 +128,10 @@ int lhl_ws_import(lhl_ws_t ws, const double* dfactors, const double* dHt, const 
  * storage holding float values, so every view, shift object and solve entry point of this
  * header applies unchanged:
  *   - J is rounded to float on the way in (lhl_reduce) or taken as float (lhl_reduce_f32);
- *   - below n = 1024 (_lhl_block_min(Float32), F:703-705) the plain form reduces in float
- *     arithmetic as the reference does (balancing F:299-340 and the unblocked ELMHES F:466-678
- *     with T = Float32); from n = 1024, and in the mixed form, the FP64 or mixed reduction
- *     runs and its factors and Ht are rounded to float;
+ *   - the plain form reduces in float arithmetic as the reference does: balancing
+ *     (F:299-340) and, below n = 1024 (_lhl_block_min(Float32), F:703-705), the unblocked
+ *     ELMHES (F:466-678), from there the blocked form (F:765-1006), with T = Float32; the
+ *     mixed form runs the mixed reduction and rounds its factors and Ht to float;
  *   - the shift LU (lhl_shift, lhl_shift_batched) runs in float arithmetic with sigma and tau
  *     rounded to float, as LHLShift{Float32} does (F:2529-2594 with T = Float32);
  *   - complex shifts (LHLShift{ComplexF32}, a shift object from lhl_shift_create_complex):

@@ -33,6 +33,7 @@ struct lhl_ws_s {
     int probes;  // device timers in the reduction kernels (lhl_ws_set_probes)
     int f32;     // LHLWorkspace{Float32}: float values in the FP64 arrays, float shift arithmetic
     double* f32x;  // lhl_ldiv_f32: widened right-hand sides (grow-only)
+    float* f32a;   // LHLWorkspace{Float32}, n >= 1024: the blocked float reduction's matrix and scratch
     size_t f32x_cap;
     int cj;        // LHLWorkspace{ComplexF64}: F, Ht, buf2 interleaved complex (cplxj.cu)
     int mix_kernel;  // mixed form: 0 by the plan (rows on chip: eager, else panel-delayed), 1 eager, 2 panel-delayed
@@ -76,7 +77,7 @@ static void ws_free(lhl_ws_t w)
     if (!w) return;
     void* ptrs[] = {w->F, w->Ht, w->scale, w->iscale, w->B0, w->part, w->tab, w->cand_v, w->cand_s, w->buf2, w->tsnap,
                     w->bsum, w->bfac, w->ipiv, w->perm, w->iperm, w->cand_i, w->bflag, w->err, w->bar,
-                    w->ptimes, w->mhdr, w->mcval, w->mcrow, w->mgrows, w->ybuf, w->zflags, w->tailw, w->linv, w->gmV, w->gmS, w->gmA, w->f32x, w->gmP};
+                    w->ptimes, w->mhdr, w->mcval, w->mcrow, w->mgrows, w->ybuf, w->zflags, w->tailw, w->linv, w->gmV, w->gmS, w->gmA, w->f32x, w->gmP, w->f32a};
     for (void* p : ptrs)
         if (p) cudaFree(p);
     if (w->gmH) cudaFreeHost(w->gmH);
@@ -166,9 +167,19 @@ int lhl_ws_create(int64_t n, int precision, lhl_ws_t* out)
 
 int lhl_ws_create_f32(int64_t n, int precision, lhl_ws_t* out)
 {
-    const int rc = lhl_ws_create(n, precision, out);
-    if (rc == LHL_OK) (*out)->f32 = 1;
-    return rc;
+    int rc = lhl_ws_create(n, precision, out);
+    if (rc != LHL_OK) return rc;
+    (*out)->f32 = 1;
+    if (n >= 1024 && precision == LHL_PREC_FP64) {
+        const size_t cnt = (size_t)n * (size_t)n + 40 * (size_t)n;
+        if (cudaMalloc((void**)&(*out)->f32a, cnt * sizeof(float)) != cudaSuccess) {
+            (*out)->f32a = nullptr;
+            lhl_ws_destroy(*out);
+            *out = nullptr;
+            return LHL_ERR_ALLOC;
+        }
+    }
+    return LHL_OK;
 }
 
 int lhl_ws_create_c128(int64_t n, lhl_ws_t* out)
@@ -322,7 +333,7 @@ static int reduce_loaded(lhl_ws_t ws, int balance, cudaStream_t st);
 static int round_reduction_f32(lhl_ws_t ws, cudaStream_t st)
 {
     const int n = (int)ws->n;
-    if (n < 1024 && ws->precision != LHL_PREC_MIXED) return LHL_OK;
+    if (ws->precision != LHL_PREC_MIXED && (n < 1024 || ws->f32a)) return LHL_OK;
     cudaError_t e = lhl::launch_round_f32(ws->F, n, ws->F, n, n, n, st);
     if (e == cudaSuccess) e = lhl::launch_round_f32(ws->Ht, n, ws->Ht, n, n, n, st);
     return cuda_status(e);
@@ -469,6 +480,16 @@ static int reduce_loaded(lhl_ws_t ws, int balance, cudaStream_t st)
         if (e != cudaSuccess) return LHL_ERR_CUDA;
         if (lazy) return cuda_status(lhl::launch_lazy_finish((int)n, ws->F, ws->Ht, st));
         return cuda_status(lhl::launch_ht_fill((int)n, ws->F, ws->Ht, st));
+    }
+    if (ws->f32 && n >= 1024 && ws->f32a) {
+        // LHLWorkspace{Float32} from its blocked threshold: the reference's blocked Float32 form
+        if (!balance) e = lhl::launch_fill_ones(ws->scale, ws->iscale, (int)n, st);
+        float* A32 = ws->f32a;
+        float* B0 = A32 + (size_t)n * n;
+        if (e == cudaSuccess)
+            e = lhl::launch_reduce_f32_blocked(a, balance ? 1 : 0, A32, B0, B0 + 17 * (size_t)n, B0 + 18 * (size_t)n, st);
+        if (e == cudaSuccess) e = lhl::launch_ht_perm((int)n, ws->F, ws->Ht, ws->ipiv, ws->perm, ws->iperm, st);
+        return cuda_status(e);
     }
     if (ws->f32 && n < 1024) {
         // LHLWorkspace{Float32} below its blocked threshold: the reference's Float32 arithmetic

@@ -160,6 +160,10 @@ cudaError_t launch_unblocked_assemble(int n, double* A, const double* B2, const 
 cudaError_t launch_reduce_f32(RedArgs a, int balance, float* A32, float* B32, cudaStream_t st);
 cudaError_t launch_unblocked_assemble_f32(int n, double* F, const float* A32, const float* B32, const int64_t* ipiv,
                                           cudaStream_t st);
+// from n = 1024 the blocked float form: A32 n x n floats, B0 and pre n x 17 floats, w n floats;
+// the factors are widened into a.A
+cudaError_t launch_reduce_f32_blocked(RedArgs a, int balance, float* A32, float* B0, float* w, float* pre,
+                                     cudaStream_t st);
 cudaError_t launch_ht_perm(int n, const double* A, double* Ht, const int64_t* ipiv, int64_t* perm, int64_t* iperm,
                            cudaStream_t st);
 cudaError_t launch_ht_fill(int n, const double* A, double* Ht, cudaStream_t st);

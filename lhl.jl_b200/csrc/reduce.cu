@@ -424,7 +424,7 @@ __device__ __forceinline__ bool balance_decide_f32(float c, float r, float& f)
 // as the reference holds it when its sweep reaches i: the sweep's starting matrix with the
 // factors of the indices scaled so far in the sweep (row j divided by fac[j], column j
 // multiplied, the same single operations the reference applies); fac == nullptr: none yet.
-__device__ __forceinline__ void bal_sums_f32(const float* A, int n, int i, const float* fac, float& c, float& r)
+__device__ __forceinline__ void bal_sums_f32(const float* A, int n, int i, const double* fac, float& c, float& r)
 {
     c = 0.0f;
     r = 0.0f;
@@ -439,8 +439,8 @@ __device__ __forceinline__ void bal_sums_f32(const float* A, int n, int i, const
 #pragma unroll
         for (int u = 0; u < 8; ++u) {
             if (j + u == i) continue;
-            const float fc = fac ? __fdiv_rn(vc[u], fac[j + u - 1]) : vc[u];
-            const float fr = fac ? __fmul_rn(vr[u], fac[j + u - 1]) : vr[u];
+            const float fc = fac ? __fdiv_rn(vc[u], (float)fac[j + u - 1]) : vc[u];
+            const float fr = fac ? __fmul_rn(vr[u], (float)fac[j + u - 1]) : vr[u];
             c = __fadd_rn(c, fabsf(fc));
             r = __fadd_rn(r, fabsf(fr));
         }
@@ -448,8 +448,8 @@ __device__ __forceinline__ void bal_sums_f32(const float* A, int n, int i, const
     for (; j <= n; ++j) {
         if (j == i) continue;
         const float vc = M1(A, n, j, i), vr = M1(A, n, i, j);
-        c = __fadd_rn(c, fabsf(fac ? __fdiv_rn(vc, fac[j - 1]) : vc));
-        r = __fadd_rn(r, fabsf(fac ? __fmul_rn(vr, fac[j - 1]) : vr));
+        c = __fadd_rn(c, fabsf(fac ? __fdiv_rn(vc, (float)fac[j - 1]) : vc));
+        r = __fadd_rn(r, fabsf(fac ? __fmul_rn(vr, (float)fac[j - 1]) : vr));
     }
 }
 
@@ -470,7 +470,6 @@ __device__ bool balance_phase_f32(const RedArgs& a, float* A, GridBarrier& gb)
         a.iscale[i] = 1.0;
     }
     __shared__ int s_first;
-    __shared__ float s_fac[1024];
     for (int sweep = 0; sweep < 20; ++sweep) {
         for (int i = 1 + gt; i <= n; i += gsz) {
             float c, r;
@@ -482,7 +481,6 @@ __device__ bool balance_phase_f32(const RedArgs& a, float* A, GridBarrier& gb)
         if (gt == 0) a.bflag[0] = 0;
         if (!gb.sync()) return false;
         if (blockIdx.x == 0) {
-            for (int i = threadIdx.x; i < n; i += RT) s_fac[i] = 1.0f;
             bool fresh = false;  // an index has scaled in this sweep: sum afresh
             int base = 1;
             __syncthreads();
@@ -494,7 +492,7 @@ __device__ bool balance_phase_f32(const RedArgs& a, float* A, GridBarrier& gb)
                 if (i <= n) {
                     float c, r;
                     if (fresh) {
-                        bal_sums_f32(A, n, i, s_fac, c, r);
+                        bal_sums_f32(A, n, i, a.bfac, c, r);
                     } else {
                         c = (float)a.bsum[i - 1];
                         r = (float)a.bsum[n + i - 1];
@@ -508,7 +506,6 @@ __device__ bool balance_phase_f32(const RedArgs& a, float* A, GridBarrier& gb)
                     continue;
                 }
                 if (i == si) {
-                    s_fac[si - 1] = f;
                     a.bfac[si - 1] = f;
                     a.bflag[0] = 1;
                     a.scale[si - 1] = __fmul_rn((float)a.scale[si - 1], f);
@@ -531,6 +528,427 @@ __device__ bool balance_phase_f32(const RedArgs& a, float* A, GridBarrier& gb)
         if (!gb.sync()) return false;
     }
     return true;
+}
+
+// ---------------------------------------------------------------------------------
+// The blocked Float32 form (n >= 1024): the reference's pointer path (F:765-1006 and its
+// helpers) with T = Float32.  Its vector width only spreads rows over lanes, so every element
+// sees the operations of the Float64 path in the same order: per step the pivot, the step
+// table (the rows k+1 and p of the panel columns, the pulled column's values and corrections,
+// F:1088-1132), the multipliers, the GEMV over the trailing columns in 64-column groups of
+// four-column passes with the group sums added in order (F:1451-1553), the row kernel (row and
+// column interchange, the pulled column, left and right transforms inside the panel,
+// F:1166-1296) and the correction of w by the panel's interchanges and left transforms; at the
+// panel end the row interchanges, the TRSM through the explicit (M^-1 - I) (F:1944-1955), the
+// rank-16 GEMM as fused multiply-add chains, the top rows' panel part and their fma chain
+// over the trailing columns (F:1588-1672); after the last panel the deferred interchanges.
+// Not tuned: one thread per row walks its row of the trailing block in each step's GEMV.
+// ---------------------------------------------------------------------------------
+constexpr int FB = 16;  // panel width (F:706)
+struct F32Tab {
+    int p, skip, pulled, nov;
+    float piv;
+    float R1[FB + 2], RP[FB + 2], PJ[FB + 2], OV[2 * FB + 4], CX[FB + 1];
+    int OR[2 * FB + 4];
+};
+struct F32Chain {
+    float LW[FB + 2], LQ[FB + 2], XS[FB + 1];
+    int LR[FB + 2];
+    int nq;
+};
+
+// One 64-column group's part of row i's GEMV (F:1496-1553): multipliers l_j = A[j,k] (already
+// divided by the pivot); column psub is read from `sub`.
+__device__ __forceinline__ float f32_gemv_group(const float* A, int n, int k, int i, int c0, int c1, int psub,
+                                                const float* sub)
+{
+    auto col = [&](int j) -> float { return j == psub ? sub[i - 1] : M1(A, n, i, j); };
+    float out;
+    int j = c0;
+    if (j + 3 <= c1) {
+        const float l1 = M1(A, n, j, k), l2 = M1(A, n, j + 1, k), l3 = M1(A, n, j + 2, k), l4 = M1(A, n, j + 3, k);
+        out = dadd(dadd(dmul(l1, col(j)), dmul(l2, col(j + 1))), dadd(dmul(l3, col(j + 2)), dmul(l4, col(j + 3))));
+        j += 4;
+    } else {
+        out = dmul(M1(A, n, j, k), col(j));
+        j += 1;
+    }
+    for (; j + 3 <= c1; j += 4) {
+        const float l1 = M1(A, n, j, k), l2 = M1(A, n, j + 1, k), l3 = M1(A, n, j + 2, k), l4 = M1(A, n, j + 3, k);
+        out = dadd(out, dadd(dadd(dmul(l1, col(j)), dmul(l2, col(j + 1))), dadd(dmul(l3, col(j + 2)), dmul(l4, col(j + 3)))));
+    }
+    for (; j <= c1; ++j) {
+        const float lj = M1(A, n, j, k);
+        if (lj != 0.0f) out = dadd(out, dmul(lj, col(j)));
+    }
+    return out;
+}
+
+// The interchange of a step whose pivot is zero (the generic step swaps, F:857-890), CTA 0 alone.
+__device__ void f32_step_swaps(float* A, int n, float* B0, const int64_t* ipiv, int k0, int kb, int k, int p)
+{
+    const int t = threadIdx.x;
+    if (t == 0)
+        for (int j = k0; j <= kb + 1; ++j) {
+            if (j == k) continue;
+            const float x = M1(A, n, k + 1, j);
+            M1(A, n, k + 1, j) = M1(A, n, p, j);
+            M1(A, n, p, j) = x;
+        }
+    __syncthreads();
+    if (p <= kb + 1) {
+        for (int i = 1 + t; i <= n; i += RT) {
+            float x = M1(A, n, i, k + 1);
+            M1(A, n, i, k + 1) = M1(A, n, i, p);
+            M1(A, n, i, p) = x;
+            x = M1(B0, n, i, k + 1 - k0);
+            M1(B0, n, i, k + 1 - k0) = M1(B0, n, i, p - k0);
+            M1(B0, n, i, p - k0) = x;
+        }
+        __syncthreads();
+        return;
+    }
+    for (int i = 1 + t; i <= n; i += RT) {
+        const float x = M1(A, n, i, p);
+        M1(A, n, i, p) = M1(B0, n, i, k + 1 - k0);
+        M1(B0, n, i, k + 1 - k0) = x;
+        M1(A, n, i, k + 1) = x;
+    }
+    __syncthreads();
+    if (t == 0)
+        for (int kk = k0; kk <= k; ++kk) {
+            const int q = (int)ipiv[kk - 1];
+            if (q != kk + 1) {
+                const float x = M1(A, n, kk + 1, k + 1);
+                M1(A, n, kk + 1, k + 1) = M1(A, n, q, k + 1);
+                M1(A, n, q, k + 1) = x;
+            }
+        }
+    __syncthreads();
+    for (int kk = k0; kk <= k - 1; ++kk) {
+        const float x = M1(A, n, kk + 1, k + 1);
+        if (x != 0.0f)
+            for (int i = kk + 2 + t; i <= n; i += RT) M1(A, n, i, k + 1) = dsub(M1(A, n, i, k + 1), dmul(M1(A, n, i, kk), x));
+        __syncthreads();
+    }
+}
+
+// The step table (thread 0 of every CTA, from the matrix as the previous step left it; no
+// writes): F:1060-1132 of the pointer path.  Column k's rows k+1 and p are exchanged later by
+// their owners, so every CTA reads the same values here.
+__device__ void f32_step_table(const RedArgs& a, const float* A, int n, F32Tab& T, int k0, int kb, int k, int p)
+{
+    T.p = p;
+    for (int j = k0; j <= kb + 1; ++j) {
+        T.R1[j - k0] = M1(A, n, k + 1, j);
+        T.RP[j - k0] = M1(A, n, p, j);
+    }
+    const float piv = T.RP[k - k0];  // A[k+1, k] after the exchange
+    T.piv = piv;
+    T.pulled = p > kb + 1;
+    T.skip = piv == 0.0f;
+    T.nov = 0;
+    if (T.skip) return;
+    if (T.pulled) {  // pulled_tables (F:1088-1132)
+        const int m = k - k0 + 1;
+        for (int kk = k0; kk <= k; ++kk) {
+            T.OV[kk - k0] = M1(A, n, kk + 1, p);
+            T.OR[kk - k0] = kk + 1;
+        }
+        int nov = m;
+        for (int kk = k0; kk <= k; ++kk) {
+            const int q = kk == k ? p : (int)a.ipiv[kk - 1];  // step k's entry may not be visible yet
+            if (q == kk + 1) continue;
+            int sl = -1;
+            for (int r = 0; r < nov; ++r)
+                if (T.OR[r] == q) { sl = r; break; }
+            if (sl < 0) {
+                sl = nov++;
+                T.OV[sl] = M1(A, n, q, p);
+                T.OR[sl] = q;
+            }
+            const float x = T.OV[kk - k0];
+            T.OV[kk - k0] = T.OV[sl];
+            T.OV[sl] = x;
+        }
+        for (int kk = k0; kk <= k - 1; ++kk) {
+            const float x = T.OV[kk - k0];
+            T.CX[kk - k0] = x;
+            if (x == 0.0f) continue;
+            for (int i = kk + 2; i <= k + 1; ++i) {
+                const float aik = (i == k + 1) ? T.RP[kk - k0] : M1(A, n, i, kk);
+                T.OV[i - k0 - 1] = dsub(T.OV[i - k0 - 1], dmul(aik, x));
+            }
+        }
+        T.nov = nov;
+    }
+    for (int j = k + 1; j <= kb + 1; ++j) T.PJ[j - k - 1] = T.RP[j - k0];
+    if (T.pulled) {
+        T.PJ[0] = T.OV[k - k0];
+    } else if (p != k + 1) {
+        T.PJ[0] = T.RP[p - k0];
+        T.PJ[p - k - 1] = T.RP[k + 1 - k0];
+    }
+}
+
+// blocked float reduction over A (n x n floats, ld n), after balancing; scratch: B0 (n x 17),
+// w (n), pre (n x 17), the step table in global memory
+__device__ bool f32_blocked(const RedArgs& a, GridBarrier& gb, float* A, float* B0, float* w, float* pre)
+{
+    const int n = a.n;
+    __shared__ double s_red[RW];
+    __shared__ int s_redi[RW];
+    __shared__ F32Tab T;
+    __shared__ F32Chain C;
+    __shared__ float Pm[FB][FB];
+    __shared__ float Bs[FB];
+    __shared__ int s_p;
+    const int t = threadIdx.x;
+    const int gt = blockIdx.x * RT + t, gsz = gridDim.x * RT;
+    const int i = 32 * ((t >> 5) * (int)gridDim.x + (int)blockIdx.x) + (t & 31) + 1;  // this thread's row
+    {
+        double v = 0.0;
+        int vi = 0;
+        if (i >= 2 && i <= n) { v = fabs((double)M1(A, n, i, 1)); vi = i; }
+        publish_candidate(a, v, vi, s_red, s_redi);
+    }
+    if (!gb.sync()) return false;
+    for (int k0 = 1; k0 <= n - 2; k0 += FB) {
+        const int kb = k0 + FB - 1 < n - 2 ? k0 + FB - 1 : n - 2;
+        const int np = kb + 1 - k0;
+        for (size_t e = gt; e < (size_t)n * np; e += gsz) {
+            const int r = (int)(e % n) + 1, jj = (int)(e / n) + 1;
+            M1(B0, n, r, jj) = M1(A, n, r, k0 + jj);
+        }
+        if (!gb.sync()) return false;
+        for (int k = k0; k <= kb; ++k) {
+            // the pivot: first maximum of |A[k+1:n, k]| (F:1038-1051), then the step table
+            combine_candidates(a, &s_p, s_red, s_redi);
+            const int p = (s_p >= k + 1 && s_p <= n) ? s_p : k + 1;
+            if (gt == 0) a.ipiv[k - 1] = p;
+            if (t == 0) f32_step_table(a, A, n, T, k0, kb, k, p);
+            __syncthreads();
+            if (T.skip) {
+                // a zero pivot: the interchange alone (F:1054-1057, generic step swaps), CTA 0
+                if (!gb.sync()) return false;
+                if (blockIdx.x == 0 && p != k + 1) {
+                    if (t == 0) {
+                        const float x = M1(A, n, k + 1, k);
+                        M1(A, n, k + 1, k) = M1(A, n, p, k);
+                        M1(A, n, p, k) = x;
+                    }
+                    __syncthreads();
+                    f32_step_swaps(A, n, B0, a.ipiv, k0, kb, k, p);
+                }
+                if (!gb.sync()) return false;
+            }
+            if (!T.skip) {
+                const float piv = T.piv;
+                // column k's exchange of rows k+1 and p, and the multipliers (F:1058,
+                // F:1506-1509) of every row below k+1; every CTA has read its table first
+                if (!gb.sync()) return false;
+                if (i == k + 1) M1(A, n, k + 1, k) = piv;
+                if (i >= k + 2 && i <= n) M1(A, n, i, k) = __fdiv_rn(i == p ? T.R1[k - k0] : M1(A, n, i, k), piv);
+                if (!gb.sync()) return false;
+                const bool trailing = kb + 2 <= n;
+                float wi = 0.0f;
+                if (i >= 1 && i <= n) {
+                    // GEMV of this row over the trailing columns, groups of 64 added in order
+                    if (trailing && i >= k0 + 1) {
+                        const float* sub = T.pulled ? B0 + (size_t)(k - k0) * n : nullptr;
+                        const int psub = T.pulled ? p : 0;
+                        for (int ga = kb + 2; ga <= n; ga += 64) {
+                            const int gb2 = ga + 63 < n ? ga + 63 : n;
+                            const float part = f32_gemv_group(A, n, k, i, ga, gb2, psub, sub);
+                            wi = ga == kb + 2 ? part : dadd(wi, part);
+                        }
+                        w[i - 1] = wi;
+                    }
+                    // the row kernel (F:1166-1296): interchange (every row), pulled column,
+                    // left transforms (rows below k+1), right transforms (rows below k0)
+                    if (p != k + 1) {
+                        if (i == k + 1)
+                            for (int j = k0; j <= kb + 1; ++j) if (j != k) M1(A, n, k + 1, j) = T.RP[j - k0];
+                        if (i == p)
+                            for (int j = k0; j <= kb + 1; ++j) if (j != k) M1(A, n, p, j) = T.R1[j - k0];
+                        if (p <= kb + 1) {
+                            float x = M1(A, n, i, k + 1);
+                            M1(A, n, i, k + 1) = M1(A, n, i, p);
+                            M1(A, n, i, p) = x;
+                            x = M1(B0, n, i, k + 1 - k0);
+                            M1(B0, n, i, k + 1 - k0) = M1(B0, n, i, p - k0);
+                            M1(B0, n, i, p - k0) = x;
+                        } else {
+                            const float x = M1(A, n, i, p);
+                            M1(A, n, i, p) = M1(B0, n, i, k + 1 - k0);
+                            M1(B0, n, i, k + 1 - k0) = x;
+                            M1(A, n, i, k + 1) = x;
+                        }
+                    }
+                    if (T.pulled) {
+                        for (int r = 0; r < T.nov; ++r)
+                            if (T.OR[r] == i) M1(A, n, i, k + 1) = T.OV[r];
+                        if (i >= k + 2)
+                            for (int kk = k0; kk <= k - 1; ++kk) {
+                                const float x = T.CX[kk - k0];
+                                if (x != 0.0f) M1(A, n, i, k + 1) = dsub(M1(A, n, i, k + 1), dmul(M1(A, n, i, kk), x));
+                            }
+                    }
+                    if (i >= k + 2)
+                        for (int j = k + 1; j <= kb + 1; ++j) {
+                            const float pj = T.PJ[j - k - 1];
+                            if (pj != 0.0f) M1(A, n, i, j) = dsub(M1(A, n, i, j), dmul(M1(A, n, i, k), pj));
+                        }
+                    if (i >= k0 + 1)
+                        for (int j = k + 2; j <= kb + 1; ++j) {
+                            const float vj = M1(A, n, j, k);
+                            if (vj != 0.0f) M1(A, n, i, k + 1) = dadd(M1(A, n, i, k + 1), dmul(vj, M1(A, n, i, j)));
+                        }
+                }
+                if (!gb.sync()) return false;
+                if (trailing) {
+                    // the correction of w by the panel's interchanges and left transforms, on
+                    // rows k0+1..k+1 and the swap partners beyond (every CTA, thread 0)
+                    if (t == 0) {
+                        for (int r = k0 + 1; r <= k + 1; ++r) C.LW[r - k0 - 1] = w[r - 1];
+                        int nq = 0;
+                        for (int kk = k0; kk <= k; ++kk) {
+                            const int q = kk == k ? p : (int)a.ipiv[kk - 1];
+                            if (q == kk + 1) continue;
+                            if (q <= k + 1) {
+                                const float x = C.LW[kk - k0];
+                                C.LW[kk - k0] = C.LW[q - k0 - 1];
+                                C.LW[q - k0 - 1] = x;
+                            } else {
+                                int sl = -1;
+                                for (int r = 0; r < nq; ++r)
+                                    if (C.LR[r] == q) { sl = r; break; }
+                                if (sl < 0) { sl = nq++; C.LQ[sl] = w[q - 1]; C.LR[sl] = q; }
+                                const float x = C.LW[kk - k0];
+                                C.LW[kk - k0] = C.LQ[sl];
+                                C.LQ[sl] = x;
+                            }
+                        }
+                        C.nq = nq;
+                        for (int kk = k0; kk <= k; ++kk) {
+                            const float x = C.LW[kk - k0];
+                            C.XS[kk - k0] = x;
+                            if (x == 0.0f) continue;
+                            for (int r = kk + 2; r <= k; ++r) C.LW[r - k0 - 1] = dsub(C.LW[r - k0 - 1], dmul(M1(A, n, r, kk), x));
+                            if (kk + 2 <= k + 1) C.LW[k - k0] = dsub(C.LW[k - k0], dmul(T.RP[kk - k0], x));
+                        }
+                    }
+                    __syncthreads();
+                    if (i >= k0 + 1 && i <= n) {
+                        if (i <= k + 1) {
+                            M1(A, n, i, k + 1) = dadd(M1(A, n, i, k + 1), C.LW[i - k0 - 1]);
+                        } else {
+                            for (int r = 0; r < C.nq; ++r)
+                                if (C.LR[r] == i) wi = C.LQ[r];
+                            for (int kk = k0; kk <= k; ++kk) {
+                                const float x = C.XS[kk - k0];
+                                if (x != 0.0f) wi = dsub(wi, dmul(M1(A, n, i, kk), x));
+                            }
+                            M1(A, n, i, k + 1) = dadd(M1(A, n, i, k + 1), wi);
+                        }
+                    }
+                    __syncthreads();  // C is rewritten next step
+                }
+            }
+            // the next step's candidates: column k+1, rows k+2..n
+            double v = 0.0;
+            int vi = 0;
+            if (i >= k + 2 && i <= n) { v = fabs((double)M1(A, n, i, k + 1)); vi = i; }
+            publish_candidate(a, v, vi, s_red, s_redi);
+            if (!gb.sync()) return false;
+        }
+        const int nbp = kb - k0 + 1;
+        if (kb + 2 <= n) {
+            // P = M^-1 - I, M[r,s] = A[k0+r, k0+s-1] for r > s (F:1944-1955), in every CTA
+            if (t == 0)
+                for (int q = 1; q <= nbp; ++q) {
+                    for (int r = 1; r <= q; ++r) Pm[r - 1][q - 1] = 0.0f;
+                    for (int r = q + 1; r <= nbp; ++r) {
+                        float acc = -M1(A, n, k0 + r, k0 + q - 1);
+                        for (int s2 = q + 1; s2 <= r - 1; ++s2) acc = dsub(acc, dmul(M1(A, n, k0 + r, k0 + s2 - 1), Pm[s2 - 1][q - 1]));
+                        Pm[r - 1][q - 1] = acc;
+                    }
+                }
+            __syncthreads();
+            for (int c = kb + 2 + (int)blockIdx.x; c <= n; c += gridDim.x) {
+                if (t == 0) {
+                    for (int k = k0; k <= kb; ++k) {
+                        const int q = (int)a.ipiv[k - 1];
+                        if (q != k + 1) {
+                            const float x = M1(A, n, k + 1, c);
+                            M1(A, n, k + 1, c) = M1(A, n, q, c);
+                            M1(A, n, q, c) = x;
+                        }
+                    }
+                    if (nbp >= 2) {
+                        for (int s2 = 1; s2 <= nbp; ++s2) Bs[s2 - 1] = M1(A, n, k0 + s2, c);
+                        for (int r = 1; r <= nbp; ++r) {
+                            float v = M1(A, n, k0 + r, c);
+                            for (int s2 = 1; s2 <= nbp; ++s2) v = dfma(Pm[r - 1][s2 - 1], Bs[s2 - 1], v);
+                            M1(A, n, k0 + r, c) = v;
+                        }
+                    }
+                }
+                __syncthreads();
+                for (int r = kb + 2 + t; r <= n; r += RT) {
+                    float v = M1(A, n, r, c);
+                    for (int kk = 1; kk <= nbp; ++kk) v = dfma(-M1(A, n, r, k0 + kk - 1), M1(A, n, k0 + kk, c), v);
+                    M1(A, n, r, c) = v;
+                }
+                __syncthreads();
+            }
+        }
+        // the top rows' snapshot of the panel columns (rows 1..k0)
+        for (size_t e = gt; e < (size_t)k0 * nbp; e += gsz) {
+            const int r = (int)(e % k0) + 1, c = k0 + 1 + (int)(e / k0);
+            pre[(size_t)(c - k0 - 1) * k0 + r - 1] = M1(A, n, r, c);
+        }
+        if (!gb.sync()) return false;
+        // top rows: panel part, then one fma chain over the trailing columns (F:1635-1672)
+        for (size_t e = gt; e < (size_t)k0 * nbp; e += gsz) {
+            const int r = (int)(e % k0) + 1, c = k0 + 1 + (int)(e / k0);
+            float v = M1(A, n, r, c);
+            for (int j = c + 1; j <= kb + 1; ++j) {
+                const float vj = M1(A, n, j, c - 1);
+                if (vj != 0.0f) v = dadd(v, dmul(vj, pre[(size_t)(j - k0 - 1) * k0 + r - 1]));
+            }
+            for (int j = kb + 2; j <= n; ++j) v = dfma(M1(A, n, r, j), M1(A, n, j, c - 1), v);
+            M1(A, n, r, c) = v;
+        }
+        if (!gb.sync()) return false;
+    }
+    // the interchanges deferred on the multipliers (F:1383-1393)
+    for (int c = 1 + gt; c <= n - 2; c += gsz) {
+        const int kbc = ((c - 1) / FB + 1) * FB < n - 2 ? ((c - 1) / FB + 1) * FB : n - 2;
+        for (int k = kbc + 1; k <= n - 2; ++k) {
+            const int q = (int)a.ipiv[k - 1];
+            if (q != k + 1) {
+                const float x = M1(A, n, k + 1, c);
+                M1(A, n, k + 1, c) = M1(A, n, q, c);
+                M1(A, n, q, c) = x;
+            }
+        }
+    }
+    return true;
+}
+
+__global__ void __launch_bounds__(RT, 1) reduce_f32_blocked_kernel(RedArgs a, int balance, float* A32, float* B0,
+                                                                    float* w, float* pre)
+{
+    GridBarrier gb{a.bar, a.err, a.limit_ns, 0, nullptr};
+    const int n = a.n;
+    const int gt = blockIdx.x * RT + threadIdx.x;
+    for (size_t e = gt; e < (size_t)n * n; e += (size_t)gridDim.x * RT) A32[e] = (float)a.A[e];
+    if (!gb.sync()) return;
+    if (balance && !balance_phase_f32(a, A32, gb)) return;
+    if (!f32_blocked(a, gb, A32, B0, w, pre)) return;
+    if (!gb.sync()) return;
+    for (size_t e = gt; e < (size_t)n * n; e += (size_t)gridDim.x * RT) a.A[e] = (double)A32[e];  // widened
 }
 
 // One cooperative launch: J (float values in a.A) into A32, balancing, the unblocked
@@ -1654,6 +2072,22 @@ cudaError_t launch_reduce_f32(RedArgs a, int balance, float* A32, float* B32, cu
     if (e != cudaSuccess) return e;
     void* args[] = {&a, &balance, &A32, &B32};
     return cudaLaunchCooperativeKernel((void*)reduce_f32_kernel, dim3(grid), dim3(RT), args, 0, st);
+}
+
+cudaError_t launch_reduce_f32_blocked(RedArgs a, int balance, float* A32, float* B0, float* w, float* pre,
+                                     cudaStream_t st)
+{
+    if (a.n < 3) return cudaErrorInvalidValue;
+    int dev = 0, sms = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e == cudaSuccess) e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    if (e != cudaSuccess) return e;
+    const int rows = (a.n + 31) / 32, grid = rows < sms ? rows : sms;
+    reduce_init_kernel<<<64, 256, 0, st>>>(a.n, a.ipiv, a.cand_v, a.cand_i, grid);
+    e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+    void* args[] = {&a, &balance, &A32, &B0, &w, &pre};
+    return cudaLaunchCooperativeKernel((void*)reduce_f32_blocked_kernel, dim3(grid), dim3(RT), args, 0, st);
 }
 
 cudaError_t launch_unblocked_assemble_f32(int n, double* F, const float* A32, const float* B32, const int64_t* ipiv,

@@ -733,8 +733,8 @@ int lhlo_shift(int n, const double* Ht, int ldh, double sigma, double tau, doubl
 /* block kernel for n >= max(W, 8) = 8 (F:547-552, W = 32 / 4 = 8 on x86-64, F:1713), whose */
 /* per-row order does not depend on W (each lane is one row), and the paired sweep below.  */
 /* J is rounded to float first (copyto! into the Float32 fstore).  The outputs are float   */
-/* values in double storage.  The reference's blocked Float32 form (n >= 1024) is not       */
-/* restated: returns -2 there.                                                             */
+/* values in double storage.  From n = 1024 the blocked Float32 form (lhlo_reduce_blocked_  */
+/* ptr_f32, below).                                                                        */
 /* ------------------------------------------------------------------------------------ */
 #define M1F(A, ld, i, j) ((A)[(size_t)((j) - 1) * (size_t)(ld) + (size_t)((i) - 1)])
 
@@ -834,11 +834,369 @@ static void reduce_unblocked_f32(int n, float* A, int ld, int64_t* ipiv)
     }
 }
 
+/* The reference's blocked Float32 form (n >= _lhl_block_min(Float32) = 1024): the pointer
+ * path of F:765-1006 and its helpers with T = Float32.  Its vector width W = 8 only spreads
+ * rows over lanes; every element sees the Float64 path's operations in the same order (the
+ * GEMV's 64-column groups and four-column passes, the group sums in order, the fused
+ * multiply-add chains of the TRSM, the trailing GEMM and the top GEMM), so this is
+ * lhlo_reduce_blocked_ptr above with float arithmetic (fmaf where that one calls fma). */
+static inline void fswap(float* a, float* b) { float t = *a; *a = *b; *b = t; }
+
+static void step_swaps_f32(int n, float* A, int ld, float* B0, int ldb, const int64_t* ipiv,
+                       int k0, int kb, int k, int p)
+{
+    for (int j = k0; j <= kb + 1; ++j) {
+        if (j == k) continue;
+        fswap(&M1(A, ld, k + 1, j), &M1(A, ld, p, j));
+    }
+    if (p <= kb + 1) {
+        for (int i = 1; i <= n; ++i) {
+            fswap(&M1(A, ld, i, k + 1), &M1(A, ld, i, p));
+            fswap(&M1(B0, ldb, i, k + 1 - k0), &M1(B0, ldb, i, p - k0));
+        }
+    } else {
+        for (int i = 1; i <= n; ++i) {
+            float t = M1(A, ld, i, p);
+            M1(A, ld, i, p) = M1(B0, ldb, i, k + 1 - k0);
+            M1(B0, ldb, i, k + 1 - k0) = t;
+            M1(A, ld, i, k + 1) = t;
+        }
+        for (int kk = k0; kk <= k; ++kk) {
+            int q = (int)ipiv[kk - 1];
+            if (q != kk + 1) fswap(&M1(A, ld, kk + 1, k + 1), &M1(A, ld, q, k + 1));
+        }
+        for (int kk = k0; kk <= k - 1; ++kk) {
+            float x = M1(A, ld, kk + 1, k + 1);
+            if (x == 0.0f) continue;
+            for (int i = kk + 2; i <= n; ++i) M1(A, ld, i, k + 1) -= M1(A, ld, i, kk) * x;
+        }
+    }
+}
+
+/* F:1088-1132: the pulled column p's values at rows k0+1..k+1 and at the swap partners of */
+/* steps k0..k, after those interchanges and the left transforms k0..k-1 (rows <= k+1).   */
+static int pulled_tables_f32(const float* A, int ld, const float* RP, float* OV, int* OR, float* CX,
+                         const int64_t* ipiv, int k0, int k, int p)
+{
+    int m = k - k0 + 1;
+    for (int kk = k0; kk <= k; ++kk) {
+        OV[kk - k0] = M1(A, ld, kk + 1, p);
+        OR[kk - k0] = kk + 1;
+    }
+    int nov = m;
+    for (int kk = k0; kk <= k; ++kk) {
+        int q = (int)ipiv[kk - 1];
+        if (q == kk + 1) continue;
+        int s = -1;
+        for (int r = 0; r < nov; ++r)
+            if (OR[r] == q) { s = r; break; }
+        if (s < 0) {
+            s = nov++;
+            OV[s] = M1(A, ld, q, p);
+            OR[s] = q;
+        }
+        float a = OV[kk - k0];
+        OV[kk - k0] = OV[s];
+        OV[s] = a;
+    }
+    for (int kk = k0; kk <= k - 1; ++kk) {
+        float x = OV[kk - k0];
+        CX[kk - k0] = x;
+        if (x == 0.0f) continue;
+        for (int i = kk + 2; i <= k + 1; ++i) {
+            float aik = (i == k + 1) ? RP[kk - k0] : M1(A, ld, i, kk);
+            OV[i - k0 - 1] = OV[i - k0 - 1] - aik * x;
+        }
+    }
+    return nov;
+}
+
+/* One 64-column group's partial for rows r0..r1 (F:1496-1553).  The multipliers A[c0:c1,k] */
+/* are already divided by the pivot; column psub is read from `sub`.                       */
+static void gemv_group_f32(float* out, const float* A, int ld, int k, int r0, int r1, int c0, int c1,
+                       int psub, const float* sub)
+{
+#define COLP(j) ((j) == psub ? sub : A + (size_t)((j) - 1) * ld)
+    /* per row: the same operation order as the reference's vector loop; rows run innermost */
+    int j = c0;
+    if (j + 3 <= c1) {
+        const float *p1 = COLP(j), *p2 = COLP(j + 1), *p3 = COLP(j + 2), *p4 = COLP(j + 3);
+        float l1 = M1(A, ld, j, k), l2 = M1(A, ld, j + 1, k), l3 = M1(A, ld, j + 2, k), l4 = M1(A, ld, j + 3, k);
+        for (int i = r0; i <= r1; ++i)
+            out[i - 1] = (l1 * p1[i - 1] + l2 * p2[i - 1]) + (l3 * p3[i - 1] + l4 * p4[i - 1]);
+        j += 4;
+    } else {
+        const float* p1 = COLP(j);
+        float lj = M1(A, ld, j, k);
+        for (int i = r0; i <= r1; ++i) out[i - 1] = lj * p1[i - 1];
+        j += 1;
+    }
+    while (j + 3 <= c1) {
+        const float *p1 = COLP(j), *p2 = COLP(j + 1), *p3 = COLP(j + 2), *p4 = COLP(j + 3);
+        float l1 = M1(A, ld, j, k), l2 = M1(A, ld, j + 1, k), l3 = M1(A, ld, j + 2, k), l4 = M1(A, ld, j + 3, k);
+        for (int i = r0; i <= r1; ++i)
+            out[i - 1] = out[i - 1] + ((l1 * p1[i - 1] + l2 * p2[i - 1]) + (l3 * p3[i - 1] + l4 * p4[i - 1]));
+        j += 4;
+    }
+    while (j <= c1) {
+        float lj = M1(A, ld, j, k);
+        if (lj != 0.0f) {
+            const float* p1 = COLP(j);
+            for (int i = r0; i <= r1; ++i) out[i - 1] = out[i - 1] + lj * p1[i - 1];
+        }
+        j += 1;
+    }
+#undef COLP
+}
+
+static void panel_steps_ptr_f32(int n, float* A, int ld, int64_t* ipiv, float* B0, int ldb, float* w,
+                            float* part, int k0, int kb, int nb)
+{
+    float R1[64], RP[64], PJ[64], OV[160], CX[64], LW[64], LQ[64], XS[64];
+    int OR[160], LR[64];
+    for (int j = k0 + 1; j <= kb + 1; ++j)
+        for (int i = 1; i <= n; ++i) M1(B0, ldb, i, j - k0) = M1(A, ld, i, j);
+    for (int k = k0; k <= kb; ++k) {
+        int p = k + 1;
+        float amax = fabsf(M1(A, ld, k + 1, k));
+        for (int i = k + 2; i <= n; ++i) {
+            float a = fabsf(M1(A, ld, i, k));
+            if (a > amax) { amax = a; p = i; }
+        }
+        ipiv[k - 1] = p;
+        for (int j = k0; j <= kb + 1; ++j) {
+            R1[j - k0] = M1(A, ld, k + 1, j);
+            RP[j - k0] = M1(A, ld, p, j);
+        }
+        if (p != k + 1) fswap(&M1(A, ld, k + 1, k), &M1(A, ld, p, k));
+        float piv = M1(A, ld, k + 1, k);
+        int pulled = p > kb + 1;
+        if (piv == 0.0f) {
+            if (p != k + 1) step_swaps_f32(n, A, ld, B0, ldb, ipiv, k0, kb, k, p);
+            continue;
+        }
+        for (int i = k + 2; i <= kb + 1; ++i) M1(A, ld, i, k) /= piv;
+        int nov = pulled ? pulled_tables_f32(A, ld, RP, OV, OR, CX, ipiv, k0, k, p) : 0;
+        for (int j = k + 1; j <= kb + 1; ++j) PJ[j - k - 1] = RP[j - k0];
+        if (pulled) PJ[0] = OV[k - k0];
+        else if (p != k + 1) {
+            PJ[0] = RP[p - k0];
+            PJ[p - k - 1] = RP[k + 1 - k0];
+        }
+        int trailing = kb + 2 <= n;
+        if (trailing) {
+            /* groups: scale their rows of the multiplier column, then their partials */
+            int c0 = kb + 2, P = (n - c0 + 1 + LHL_GEMV_GROUP - 1) / LHL_GEMV_GROUP;
+            const float* sub = pulled ? B0 + (size_t)(k - k0) * ldb : NULL;
+            int psub = pulled ? p : 0;
+#pragma omp parallel for schedule(static) if (n - k0 >= 256)
+            for (int g = 1; g <= P; ++g) {
+                int ga = c0 + (g - 1) * LHL_GEMV_GROUP;
+                int gb = ga + LHL_GEMV_GROUP - 1 < n ? ga + LHL_GEMV_GROUP - 1 : n;
+                for (int j = ga; j <= gb; ++j) M1(A, ld, j, k) = M1(A, ld, j, k) / piv;
+            }
+#pragma omp parallel for schedule(static) if (n - k0 >= 256)
+            for (int g = 1; g <= P; ++g) {
+                int ga = c0 + (g - 1) * LHL_GEMV_GROUP;
+                int gb = ga + LHL_GEMV_GROUP - 1 < n ? ga + LHL_GEMV_GROUP - 1 : n;
+                gemv_group_f32(part + (size_t)(g - 1) * n, A, ld, k, k0 + 1, n, ga, gb, psub, sub);
+            }
+#pragma omp parallel for schedule(static) if (n - k0 >= 256)
+            for (int i = k0 + 1; i <= n; ++i) {
+                float s = part[i - 1];
+                for (int g = 2; g <= P; ++g) s += part[(size_t)(g - 1) * n + i - 1];
+                w[i - 1] = s;
+            }
+        }
+        /* the row kernel (F:1166-1296) over rows k0+1..n */
+        if (p != k + 1) {
+            for (int j = k0; j <= kb + 1; ++j) {
+                if (j == k) continue;
+                M1(A, ld, k + 1, j) = RP[j - k0];
+                M1(A, ld, p, j) = R1[j - k0];
+            }
+            for (int i = 1; i <= n; ++i) { /* column part of the interchange, all rows (F:1135-1161) */
+                if (p <= kb + 1) {
+                    fswap(&M1(A, ld, i, k + 1), &M1(A, ld, i, p));
+                    fswap(&M1(B0, ldb, i, k + 1 - k0), &M1(B0, ldb, i, p - k0));
+                } else {
+                    float t = M1(A, ld, i, p);
+                    M1(A, ld, i, p) = M1(B0, ldb, i, k + 1 - k0);
+                    M1(B0, ldb, i, k + 1 - k0) = t;
+                    M1(A, ld, i, k + 1) = t;
+                }
+            }
+        }
+        if (pulled) {
+            for (int r = 0; r < nov; ++r) M1(A, ld, OR[r], k + 1) = OV[r];
+            for (int kk = k0; kk <= k - 1; ++kk) {
+                float x = CX[kk - k0];
+                if (x == 0.0f) continue;
+                for (int i = k + 2; i <= n; ++i)
+                    M1(A, ld, i, k + 1) = M1(A, ld, i, k + 1) - M1(A, ld, i, kk) * x;
+            }
+        }
+        for (int j = k + 1; j <= kb + 1; ++j) {
+            float pj = PJ[j - k - 1];
+            if (pj == 0.0f) continue;
+            for (int i = k + 2; i <= n; ++i) M1(A, ld, i, j) = M1(A, ld, i, j) - M1(A, ld, i, k) * pj;
+        }
+        for (int j = k + 2; j <= kb + 1; ++j) {
+            float vj = M1(A, ld, j, k);
+            if (vj == 0.0f) continue;
+            for (int i = k0 + 1; i <= n; ++i) M1(A, ld, i, k + 1) = M1(A, ld, i, k + 1) + vj * M1(A, ld, i, j);
+        }
+        if (trailing) {
+            int m = k - k0 + 1;
+            for (int i = k0 + 1; i <= k + 1; ++i) LW[i - k0 - 1] = w[i - 1];
+            int nq = 0;
+            for (int kk = k0; kk <= k; ++kk) {
+                int q = (int)ipiv[kk - 1];
+                if (q == kk + 1) continue;
+                if (q <= k + 1) {
+                    float a = LW[kk - k0];
+                    LW[kk - k0] = LW[q - k0 - 1];
+                    LW[q - k0 - 1] = a;
+                } else {
+                    int s = -1;
+                    for (int r = 0; r < nq; ++r)
+                        if (LR[r] == q) { s = r; break; }
+                    if (s < 0) { s = nq++; LQ[s] = w[q - 1]; LR[s] = q; }
+                    float a = LW[kk - k0];
+                    LW[kk - k0] = LQ[s];
+                    LQ[s] = a;
+                }
+            }
+            (void)m;
+            for (int kk = k0; kk <= k; ++kk) {
+                float x = LW[kk - k0];
+                XS[kk - k0] = x;
+                if (x == 0.0f) continue;
+                for (int i = kk + 2; i <= k; ++i) LW[i - k0 - 1] = LW[i - k0 - 1] - M1(A, ld, i, kk) * x;
+                if (kk + 2 <= k + 1) LW[k - k0] = LW[k - k0] - RP[kk - k0] * x;
+            }
+            for (int i = k0 + 1; i <= k + 1; ++i) {
+                float v = LW[i - k0 - 1];
+                w[i - 1] = v;
+                M1(A, ld, i, k + 1) = M1(A, ld, i, k + 1) + v;
+            }
+            for (int r = 0; r < nq; ++r) w[LR[r] - 1] = LQ[r];
+            for (int kk = k0; kk <= k; ++kk) {
+                float x = XS[kk - k0];
+                if (x == 0.0f) continue;
+                for (int i = k + 2; i <= n; ++i) w[i - 1] = w[i - 1] - M1(A, ld, i, kk) * x;
+            }
+            for (int i = k + 2; i <= n; ++i) M1(A, ld, i, k + 1) = M1(A, ld, i, k + 1) + w[i - 1];
+        }
+    }
+    (void)nb;
+}
+
+void lhlo_reduce_blocked_ptr_f32(int n, float* A, int ld, int64_t* ipiv, int nb)
+{
+    if (n < 3) return;
+    int ldb = n;
+    float* B0 = (float*)malloc(sizeof(float) * (size_t)n * (size_t)(nb + 1));
+    float* w = (float*)malloc(sizeof(float) * (size_t)n);
+    int Pmax = (n + LHL_GEMV_GROUP - 1) / LHL_GEMV_GROUP;
+    float* part = (float*)malloc(sizeof(float) * (size_t)n * (size_t)Pmax);
+    float* Pm = (float*)malloc(sizeof(float) * (size_t)nb * (size_t)nb);
+    float* Tsnap = (float*)malloc(sizeof(float) * (size_t)n * (size_t)(nb + 1));
+    for (int k0 = 1; k0 <= n - 2; k0 += nb) {
+        int kb = k0 + nb - 1 < n - 2 ? k0 + nb - 1 : n - 2;
+        panel_steps_ptr_f32(n, A, ld, ipiv, B0, ldb, w, part, k0, kb, nb);
+        if (kb + 2 <= n) {
+            int nbp = kb - k0 + 1;
+            /* P = M^-1 - I, M[r,s] = A[k0+r, k0+s-1] for r > s (F:1944-1955) */
+            for (int q = 1; q <= nbp; ++q) {
+                for (int r = 1; r <= q; ++r) Pm[(r - 1) + (size_t)(q - 1) * nbp] = 0.0f;
+                for (int r = q + 1; r <= nbp; ++r) {
+                    float acc = -M1(A, ld, k0 + r, k0 + q - 1);
+                    for (int s = q + 1; s <= r - 1; ++s)
+                        acc = acc - M1(A, ld, k0 + r, k0 + s - 1) * Pm[(s - 1) + (size_t)(q - 1) * nbp];
+                    Pm[(r - 1) + (size_t)(q - 1) * nbp] = acc;
+                }
+            }
+#pragma omp parallel for schedule(static) if (n >= 512)
+            for (int c = kb + 2; c <= n; ++c) {
+                float Bs[64];
+                for (int k = k0; k <= kb; ++k) {
+                    int p = (int)ipiv[k - 1];
+                    if (p != k + 1) fswap(&M1(A, ld, k + 1, c), &M1(A, ld, p, c));
+                }
+                if (nbp >= 2) {
+                    for (int s = 1; s <= nbp; ++s) Bs[s - 1] = M1(A, ld, k0 + s, c);
+                    for (int r = 1; r <= nbp; ++r) {
+                        float v = M1(A, ld, k0 + r, c);
+                        for (int s = 1; s <= nbp; ++s) v = fmaf(Pm[(r - 1) + (size_t)(s - 1) * nbp], Bs[s - 1], v);
+                        M1(A, ld, k0 + r, c) = v;
+                    }
+                }
+                for (int i = kb + 2; i <= n; ++i) {
+                    float v = M1(A, ld, i, c);
+                    for (int kk = 1; kk <= nbp; ++kk)
+                        v = fmaf(-M1(A, ld, i, k0 + kk - 1), M1(A, ld, k0 + kk, c), v);
+                    M1(A, ld, i, c) = v;
+                }
+            }
+        }
+        /* top rows 1..k0 of the panel columns: panel part (plain), then one fma chain over
+         * j = kb+2..n per element (F:1635-1672); rows run innermost, same per-element order */
+        {
+            int ncp = kb - k0 + 1;
+            float* pre = Tsnap; /* k0 x ncp snapshot of the panel columns' top rows */
+            for (int c = k0 + 1; c <= kb + 1; ++c)
+                for (int i = 1; i <= k0; ++i) pre[(size_t)(c - k0 - 1) * k0 + i - 1] = M1(A, ld, i, c);
+#pragma omp parallel for schedule(dynamic, 1) if (k0 >= 128)
+            for (int c = k0 + 1; c <= kb + 1; ++c) {
+                float* v = A + (size_t)(c - 1) * ld;
+                for (int j = c + 1; j <= kb + 1; ++j) {
+                    float vj = M1(A, ld, j, c - 1);
+                    if (vj == 0.0f) continue;
+                    const float* pj = pre + (size_t)(j - k0 - 1) * k0;
+                    for (int i = 1; i <= k0; ++i) v[i - 1] = v[i - 1] + vj * pj[i - 1];
+                }
+                for (int j = kb + 2; j <= n; ++j) {
+                    float b = M1(A, ld, j, c - 1);
+                    const float* aj = A + (size_t)(j - 1) * ld;
+                    for (int i = 1; i <= k0; ++i) v[i - 1] = fmaf(aj[i - 1], b, v[i - 1]);
+                }
+            }
+            (void)ncp;
+        }
+    }
+    for (int k0 = 1; k0 <= n - 2; k0 += nb) {
+        int kb = k0 + nb - 1 < n - 2 ? k0 + nb - 1 : n - 2;
+        for (int c = k0; c <= kb; ++c)
+            for (int k = kb + 1; k <= n - 2; ++k) {
+                int p = (int)ipiv[k - 1];
+                if (p != k + 1) fswap(&M1(A, ld, k + 1, c), &M1(A, ld, p, c));
+            }
+    }
+    free(B0); free(w); free(part); free(Pm); free(Tsnap);
+}
+
+
+/* The blocked Float32 form on its own (no balancing), at any n: A (float values in double
+ * storage) is reduced in place; for the relation tests of test/threading.jl:58-79. */
+int lhlo_reduce_blocked_ptr_f32_raw(int n, double* A, int ld, int64_t* ipiv)
+{
+    if (n < 0 || ld < n) return -1;
+    float* Af = (float*)malloc(sizeof(float) * ((size_t)n * (size_t)n + 1));
+    if (!Af) return -3;
+    for (int j = 1; j <= n; ++j)
+        for (int i = 1; i <= n; ++i) M1F(Af, n, i, j) = (float)M1(A, ld, i, j);
+    lhlo_reduce_blocked_ptr_f32(n, Af, n, ipiv, 16);
+    for (int j = 1; j <= n; ++j)
+        for (int i = 1; i <= n; ++i) M1(A, ld, i, j) = M1F(Af, n, i, j);
+    free(Af);
+    return 0;
+}
+
 int lhlo_reduce_f32(int n, const double* J, int ldj, int balance, double* F, int ldf, int64_t* ipiv, double* scale,
                     double* iscale, int64_t* perm, int64_t* iperm, double* Ht)
 {
     if (n < 0 || ldj < n || ldf < n) return -1;
-    if (n >= 1024) return -2;
     float* A = (float*)malloc(sizeof(float) * ((size_t)n * (size_t)n + 2 * (size_t)n + 1));
     if (!A) return -3;
     float* d = A + (size_t)n * (size_t)n;
@@ -847,7 +1205,8 @@ int lhlo_reduce_f32(int n, const double* J, int ldj, int balance, double* F, int
         for (int i = 1; i <= n; ++i) M1F(A, n, i, j) = (float)M1(J, ldj, i, j);
     if (balance) balance_f32(n, A, n, d, isc);
     else for (int i = 0; i < n; ++i) { d[i] = 1.0f; isc[i] = 1.0f; }
-    reduce_unblocked_f32(n, A, n, ipiv);
+    if (n >= 1024) lhlo_reduce_blocked_ptr_f32(n, A, n, ipiv, 16);
+    else reduce_unblocked_f32(n, A, n, ipiv);
     for (int j = 1; j <= n; ++j)
         for (int i = 1; i <= n; ++i) M1(F, ldf, i, j) = M1F(A, n, i, j);
     for (int i = 0; i < n; ++i) { scale[i] = d[i]; iscale[i] = isc[i]; }

@@ -48,6 +48,8 @@ def lib():
         L.lhlo_reduce.restype = i
         L.lhlo_reduce_f32.argtypes = [i, _dp, i, i, _dp, i, _iv, _dv, _dv, _iv, _iv, _dp]
         L.lhlo_reduce_f32.restype = i
+        L.lhlo_reduce_blocked_ptr_f32_raw.argtypes = [i, _dp, i, _iv]
+        L.lhlo_reduce_blocked_ptr_f32_raw.restype = i
         L.lhlo_shift.argtypes = [i, _dp, i, d, d, _dp, i, _u8, _dv, _dv]
         L.lhlo_shift.restype = i
         L.lhlo_shift_f32.argtypes = [i, _dp, i, d, d, _dp, i, _u8, _dv, _dv]
@@ -153,13 +155,11 @@ def reduce(J, balance=True, path=0, nb=16) -> Reduction:
 
 
 def reduce_f32(J, balance=True) -> Reduction:
-    """``lhl(J)`` on ``LHLWorkspace{Float32}`` below its blocked threshold (n < 1024): J rounded
-    to float, balancing and the unblocked reduction in float arithmetic (lhlo_reduce_f32).  The
-    arrays hold float values in float64."""
+    """``lhl(J)`` on ``LHLWorkspace{Float32}``: J rounded to float, balancing and the reduction in
+    float arithmetic (lhlo_reduce_f32): unblocked below n = 1024, the blocked pointer path from
+    there, as the reference chooses.  The arrays hold float values in float64."""
     J = np.asfortranarray(J, dtype=np.float64)
     n = J.shape[0]
-    if n >= 1024:
-        raise ValueError("the oracle restates the Float32 reduction below n = 1024 only")
     R = Reduction(n)
     ip = _ipiv_buf(n)
     F = np.zeros((max(n, 1), max(n, 1)), order="F")
@@ -177,6 +177,16 @@ def reduce_f32(J, balance=True) -> Reduction:
     R.perm, R.iperm = pm[:n].copy(), ipm[:n].copy()
     R.Ht = Ht[:n, :n].copy(order="F")
     return R
+
+
+def reduce_blocked_f32_raw(A):
+    """The reference's blocked Float32 form alone (nb = 16, no balancing) at any n, on A rounded
+    to float: (factors in float64 storage, ipiv)."""
+    A = np.asfortranarray(np.asarray(A, dtype=np.float32).astype(np.float64))
+    n = A.shape[0]
+    ip = _ipiv_buf(n)
+    assert lib().lhlo_reduce_blocked_ptr_f32_raw(n, A if n > 0 else np.zeros((1, 1), order="F"), max(n, 1), ip) == 0
+    return A, ip[: max(n - 2, 0)].copy()
 
 
 def reduce_unblocked_raw(A):

@@ -101,7 +101,8 @@ def test_f32_solves(n, precision):
     assert np.linalg.norm(x64 - xr) <= 1e-3 * np.linalg.norm(xr)
 
 
-F32_SIZES = list(range(1, 34)) + [64, 130, 255, 256, 257, 499, 500, 511, 512, 520, 777, 1000, 1023]
+F32_SIZES = list(range(1, 34)) + [64, 130, 255, 256, 257, 499, 500, 511, 512, 520, 777, 1000, 1023, 1024, 1025, 1100,
+                                    1500, 2048]
 
 
 def _f32_matrix(n, kind):
@@ -118,11 +119,11 @@ def _f32_matrix(n, kind):
 @pytest.mark.parametrize("n", F32_SIZES)
 @pytest.mark.parametrize("kind", ["gauss", "tie", "graded"])
 def test_f32_reduction_bitexact(n, kind):
-    """Below _lhl_block_min(Float32) = 1024 the Float32 workspace reduces in float, as the
-    reference does: balancing (F:299-340, Tr = Float32) and the unblocked ELMHES (F:466-678).
-    ipiv, factors, Ht, scale, iscale, perm and iperm bit for bit against the oracle's float
-    restatement, with and without balancing, through both entry points (J as float and as
-    float64 rounded on the way in)."""
+    """The Float32 workspace reduces in float, as the reference does: balancing (F:299-340,
+    Tr = Float32), then below _lhl_block_min(Float32) = 1024 the unblocked ELMHES (F:466-678)
+    and from there the blocked pointer path (F:765-1006).  ipiv, factors, Ht, scale, iscale,
+    perm and iperm bit for bit against the oracle's float restatement, with and without
+    balancing, through both entry points (J as float and as float64 rounded on the way in)."""
     torch, G = _mods()
     J = _f32_matrix(n, kind)
     for balance in (True, False):
@@ -159,17 +160,15 @@ def test_f32_reduction_timeout_reports_and_recovers():
 
 @pytest.mark.parametrize("n", [1024, 1100])
 def test_f32_blocked_orders_are_a_float_similarity(n):
-    """From n = 1024 the reference runs its blocked Float32 form, which this build does not
-    restate: the FP64 reduction of the widened J, rounded.  FP64 pivots, float factors,
-    Z H Z^-1 = J to float accuracy, |l| <= 1."""
+    """From n = 1024 (the blocked float form): float factors, Z H Z^-1 = J to float accuracy,
+    |l| <= 1.  (The pivots are the oracle's float ones, bit for bit above; near the end of an
+    order this large they can differ from the Float64 reduction's on near-ties.)"""
     torch, G = _mods()
     J = rng(70 + n).standard_normal((n, n)).astype(np.float32)
     ws = G.lhl(dev(J))
-    R64 = O.reduce(J.astype(np.float64))
-    assert np.array_equal(host(ws.ipiv)[: max(n - 2, 0)], R64.ipiv)
     F = host(ws.factors)
     assert is_float_valued(F) and is_float_valued(host(ws.Ht))
-    assert np.array_equal(host(ws.scale), R64.scale)
+    assert np.array_equal(host(ws.scale), O.reduce_f32(J.astype(np.float64)).scale)
     R = O.Reduction(n)
     R.factors = np.asfortranarray(F)
     R.ipiv = host(ws.ipiv)[: max(n - 2, 0)].copy()

@@ -162,6 +162,37 @@ def test_float_reconstruction(n, balance):
         assert np.array_equal(np.asarray(a, dtype=f32).astype(np.float64), a)
 
 
-def test_blocked_float_form_is_not_restated():
-    with pytest.raises(ValueError):
-        O.reduce_f32(np.eye(1024))
+@pytest.mark.parametrize("n", [20, 33, 160, 300])
+def test_blocked_float_form_like_the_reference(n):
+    """test/threading.jl:58-79 with T = Float32: the blocked form takes the unblocked Float64
+    reduction's pivots, and its factors are within 100 n eps(Float32) of them."""
+    J = np.random.default_rng(n).standard_normal((n, n)).astype(np.float32)
+    Ab, ipb = O.reduce_blocked_f32_raw(J)
+    Ru = O.reduce(J.astype(np.float64), balance=False, path=1)
+    assert np.array_equal(ipb, Ru.ipiv)
+    assert np.linalg.norm(Ab - Ru.factors) <= 100 * n * np.finfo(np.float32).eps * np.linalg.norm(Ru.factors)
+    assert np.array_equal(Ab.astype(np.float32).astype(np.float64), Ab)
+
+
+def test_blocked_float_form_on_ties():
+    """Gaussian-integer ties (many equal moduli, zero pivots): the blocked and unblocked float
+    forms take the same pivots (test/threading.jl:62, the rand(-1:1) matrix)."""
+    J = np.random.default_rng(9).integers(-1, 2, (200, 200)).astype(np.float32)
+    Ab, ipb = O.reduce_blocked_f32_raw(J)
+    Au = O.reduce_f32(J, balance=False)
+    assert np.array_equal(ipb, Au.ipiv)
+
+
+@pytest.mark.parametrize("n", [1024, 1100])
+def test_reference_choice_from_1024(n):
+    """From n = 1024 reduce_f32 runs the blocked form (the reference's choice, F:398, F:704):
+    bit-identical to the raw blocked form after the same balancing, Z H Z^-1 = J to float
+    accuracy, |l| <= 1."""
+    J = np.random.default_rng(n).standard_normal((n, n)).astype(np.float32).astype(np.float64)
+    R = O.reduce_f32(J, balance=False)
+    Ab, ipb = O.reduce_blocked_f32_raw(J)
+    assert np.array_equal(R.ipiv, ipb) and np.array_equal(R.factors, Ab)
+    Rb = O.reduce_f32(J, balance=True)
+    Z, Zi = Rb.Z(), Rb.Zinv()
+    assert relerr(Z @ Rb.H @ Zi, J) < 50 * n * np.finfo(f32).eps
+    assert np.abs(np.tril(Rb.factors, -2)).max() <= 1.0
