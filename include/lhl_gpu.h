@@ -167,6 +167,17 @@ int lhl_ws_create_c128(int64_t n, lhl_ws_t* ws);
  * elements); a workspace not made by lhl_ws_create_c128 is LHL_ERR_ARG. */
 int lhl_reduce_c128(lhl_ws_t ws, const double* dJ, int64_t ldj, int balance, void* stream);
 
+/* ---- element type ComplexF32 (LHLWorkspace{ComplexF32}) ------------------------------
+ * lhl_ws_create_c64 makes a complex-J workspace whose element type is ComplexF32: the arrays
+ * of lhl_ws_create_c128, holding ComplexF32 values.  J is rounded to ComplexF32 on the way in
+ * (lhl_reduce_c128) or taken as ComplexF32 (lhl_reduce_c64, interleaved complex64, ld ldj
+ * complex elements); the reduction runs as for ComplexF64 (FP64 arithmetic on the float
+ * values) and its factors and Ht are rounded to ComplexF32; shifts are rounded to ComplexF32;
+ * solves take ComplexF64 vectors (lhl_ldiv) or ComplexF32 ones (lhl_ldiv_f32).  Not the
+ * reference's single-precision rounding, which is not restated. */
+int lhl_ws_create_c64(int64_t n, lhl_ws_t* ws);
+int lhl_reduce_c64(lhl_ws_t ws, const float* dJ, int64_t ldj, int balance, void* stream);
+
 /* ---- shifts --------------------------------------------------------------------- */
 /* A batch of nshifts LHLShift{Float64}(n) objects (F:107-116). */
 int lhl_shift_create(int64_t n, int64_t nshifts, lhl_shift_t* sh);

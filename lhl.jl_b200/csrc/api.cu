@@ -370,6 +370,8 @@ int lhl_reduce_f32(lhl_ws_t ws, const float* dJ, int64_t ldj, int balance, void*
     return rc;
 }
 
+static int reduce_cj_loaded(lhl_ws_t ws, int balance, cudaStream_t st);
+
 int lhl_reduce_c128(lhl_ws_t ws, const double* dJ, int64_t ldj, int balance, void* stream)
 {
     if (!ws || (!dJ && ws->n > 0)) return LHL_ERR_ARG;
@@ -378,8 +380,40 @@ int lhl_reduce_c128(lhl_ws_t ws, const double* dJ, int64_t ldj, int balance, voi
     if (ldj < n || ldj < 1) return LHL_ERR_DIM;
     if (n == 0) return LHL_OK;
     cudaStream_t st = (cudaStream_t)stream;
-    cudaError_t e = cudaMemcpy2DAsync(ws->F, n * 2 * sizeof(double), dJ, ldj * 2 * sizeof(double),
-                                      n * 2 * sizeof(double), n, cudaMemcpyDeviceToDevice, st);
+    // LHLWorkspace{ComplexF32}: J rounded to ComplexF32 on the way in
+    cudaError_t e = ws->f32 ? lhl::launch_round_f32(dJ, (int)(2 * ldj), ws->F, (int)(2 * n), (int)(2 * n), (int)n, st)
+                            : cudaMemcpy2DAsync(ws->F, n * 2 * sizeof(double), dJ, ldj * 2 * sizeof(double),
+                                                n * 2 * sizeof(double), n, cudaMemcpyDeviceToDevice, st);
+    if (e != cudaSuccess) return LHL_ERR_CUDA;
+    return reduce_cj_loaded(ws, balance, st);
+}
+
+int lhl_ws_create_c64(int64_t n, lhl_ws_t* out)
+{
+    const int rc = lhl_ws_create_c128(n, out);
+    if (rc == LHL_OK) (*out)->f32 = 1;
+    return rc;
+}
+
+int lhl_reduce_c64(lhl_ws_t ws, const float* dJ, int64_t ldj, int balance, void* stream)
+{
+    if (!ws || (!dJ && ws->n > 0)) return LHL_ERR_ARG;
+    if (!ws->cj) return LHL_ERR_ARG;
+    const int64_t n = ws->n;
+    if (ldj < n || ldj < 1) return LHL_ERR_DIM;
+    if (n == 0) return LHL_OK;
+    cudaStream_t st = (cudaStream_t)stream;
+    if (lhl::launch_f32_to_f64(dJ, (int)(2 * ldj), ws->F, (int)(2 * n), (int)(2 * n), (int)n, st) != cudaSuccess)
+        return LHL_ERR_CUDA;
+    return reduce_cj_loaded(ws, balance, st);
+}
+
+// The reduction of the complex J already in ws->F; on a ComplexF32 workspace the factors and Ht
+// are rounded to ComplexF32 values afterwards.
+static int reduce_cj_loaded(lhl_ws_t ws, int balance, cudaStream_t st)
+{
+    const int64_t n = ws->n;
+    cudaError_t e = cudaSuccess;
     if (e == cudaSuccess) e = cudaMemsetAsync(ws->bar, 0, sizeof(unsigned int), st);
     if (e == cudaSuccess) e = cudaMemsetAsync(ws->err, 0, sizeof(int), st);
     if (e == cudaSuccess && !balance) e = lhl::launch_fill_ones(ws->scale, ws->iscale, (int)n, st);
@@ -403,7 +437,12 @@ int lhl_reduce_c128(lhl_ws_t ws, const double* dJ, int64_t ldj, int balance, voi
     a.bar = ws->bar;
     a.err = ws->err;
     a.limit_ns = ws->limit_ns;
-    return cuda_status(lhl::launch_reduce_cj(a, balance ? 1 : 0, st));
+    e = lhl::launch_reduce_cj(a, balance ? 1 : 0, st);
+    if (e == cudaSuccess && ws->f32) {
+        e = lhl::launch_round_f32(ws->F, (int)(2 * n), ws->F, (int)(2 * n), (int)(2 * n), (int)n, st);
+        if (e == cudaSuccess) e = lhl::launch_round_f32(ws->Ht, (int)(2 * n), ws->Ht, (int)(2 * n), (int)(2 * n), (int)n, st);
+    }
+    return cuda_status(e);
 }
 
 static int reduce_loaded(lhl_ws_t ws, int balance, cudaStream_t st)

@@ -82,9 +82,11 @@ def _load():
         "lhl_reduce_f32": [vp, vp, i64, i32, vp],
         "lhl_ldiv_f32": [vp, vp, vp, i64, i64, i64, vp],
         "lhl_ws_create_c128": [i64, C.POINTER(vp)],
+        "lhl_ws_create_c64": [i64, C.POINTER(vp)],
         "lhl_refine_system": [vp, vp, i64, vp, i64, vp, i64, vp, i64, vp, vp, i64, d, i32, vp],
         "lhl_refine_system_gmres": [vp, vp, i64, vp, i64, vp, i64, vp, i64, vp, vp, i64, d, i32, i32, i32, vp],
         "lhl_reduce_c128": [vp, vp, i64, i32, vp],
+        "lhl_reduce_c64": [vp, vp, i64, i32, vp],
         "lhl_shift_create": [i64, i64, C.POINTER(vp)],
         "lhl_shift_destroy": [vp],
         "lhl_shift_get_view": [vp, C.POINTER(_ShView)],
@@ -304,14 +306,16 @@ class LHLWorkspace:
             _check(_lib.lhl_ws_create_f32(int(n), int(precision), C.byref(self._h)), "LHLWorkspace")
         elif dtype == torch.float64:
             _check(_lib.lhl_ws_create(int(n), int(precision), C.byref(self._h)), "LHLWorkspace")
-        elif dtype == torch.complex128:  # LHLWorkspace{ComplexF64}: shift type ComplexF64 (F:164-169)
+        elif dtype in (torch.complex128, torch.complex64):  # LHLWorkspace{ComplexF64 / ComplexF32} (F:164-169)
             if precision != LHL_PREC_FP64:
-                raise ArgumentError("a ComplexF64 workspace has the FP64 form only")
-            _check(_lib.lhl_ws_create_c128(int(n), C.byref(self._h)), "LHLWorkspace")
+                raise ArgumentError("a complex workspace has the FP64 form only")
+            create = _lib.lhl_ws_create_c128 if dtype == torch.complex128 else _lib.lhl_ws_create_c64
+            _check(create(int(n), C.byref(self._h)), "LHLWorkspace")
             shift_complex = True
         else:
-            raise ArgumentError(f"element type {dtype} is not supported (float64, float32 or complex128)")
+            raise ArgumentError(f"element type {dtype} is not supported (float64, float32, complex128 or complex64)")
         self.dtype = dtype
+        self.cj = dtype in (torch.complex128, torch.complex64)  # a complex J (its factors are complex128 views)
         self.device = torch.device("cuda", torch.cuda.current_device())  # where its arrays live
         self.n = int(n)
         self.precision = precision
@@ -371,14 +375,14 @@ class LHLWorkspace:
     @property
     def factors(self) -> torch.Tensor:
         n = self.n
-        if self.dtype == torch.complex128:
+        if self.cj:
             return _view(self._v.factors, (n, n), "<c16", strides=(16, 16 * n))
         return _view(self._v.factors, (n, n), strides=(8, 8 * n))
 
     @property
     def Ht(self) -> torch.Tensor:
         n = self.n
-        if self.dtype == torch.complex128:
+        if self.cj:
             return _view(self._v.Ht, (n, n), "<c16", strides=(16, 16 * n))
         return _view(self._v.Ht, (n, n), strides=(8, 8 * n))
 
@@ -427,6 +431,7 @@ class LHLWorkspace:
         torch.cuda.current_stream().synchronize() if stream is None else stream.synchronize()
         np.savez(path, n=self.n, precision=self.precision, shift_complex=self.shift_complex,
                  f32=self.dtype == torch.float32, c128=self.dtype == torch.complex128,
+                 c64=self.dtype == torch.complex64,
                  factors=self.factors.cpu().numpy(), Ht=self.Ht.cpu().numpy(), ipiv=self.ipiv.cpu().numpy(),
                  perm=self.perm.cpu().numpy(), iperm=self.iperm.cpu().numpy(), scale=self.scale.cpu().numpy(),
                  iscale=self.iscale.cpu().numpy())
@@ -440,6 +445,8 @@ class LHLWorkspace:
             dt = torch.float32
         elif "c128" in d and bool(d["c128"]):
             dt = torch.complex128
+        elif "c64" in d and bool(d["c64"]):
+            dt = torch.complex64
         ws = cls(int(d["n"]), int(d["precision"]), bool(d["shift_complex"]), dtype=dt)
         ws.import_arrays({k: torch.as_tensor(np.asarray(d[k])).cuda() for k in REDUCTION_ARRAYS}, stream)
         (stream or torch.cuda.current_stream()).synchronize()
@@ -452,7 +459,7 @@ class LHLWorkspace:
         int64, scale and iscale (n) float64.  Copies are taken on the stream; the arrays may be
         released once it has passed them."""
         n = self.n
-        mat = torch.complex128 if self.dtype == torch.complex128 else torch.float64
+        mat = torch.complex128 if self.cj else torch.float64
         want = {"factors": (mat, (n, n)), "Ht": (mat, (n, n)), "ipiv": (torch.int64, (max(n - 2, 0),)),
                 "perm": (torch.int64, (n,)), "iperm": (torch.int64, (n,)), "scale": (torch.float64, (n,)),
                 "iscale": (torch.float64, (n,))}
@@ -519,7 +526,10 @@ def shift_variants(is_complex: bool, n: int):
 def lhl_reduce_(ws: LHLWorkspace, J: torch.Tensor, balance: bool, thread=True, stream=None) -> LHLWorkspace:
     """``lhl_reduce!(ws, J, balance)`` (F:355).  J is not modified.  A workspace of another
     order is resized to J's first, as the reference does (F:357)."""
-    if ws.dtype == torch.complex128:
+    if ws.cj and isinstance(J, torch.Tensor) and J.dtype == torch.complex64:
+        if not J.is_cuda:
+            raise ArgumentError("J must be a CUDA tensor")
+    elif ws.cj:
         _require_cuda_f64(J, "J", True)
     elif isinstance(J, torch.Tensor) and J.dtype == torch.float32:
         _require_cuda_real(J, "J")
@@ -533,6 +543,8 @@ def lhl_reduce_(ws: LHLWorkspace, J: torch.Tensor, balance: bool, thread=True, s
     fn = _lib.lhl_reduce_f32 if Jc.dtype == torch.float32 else _lib.lhl_reduce
     if Jc.dtype == torch.complex128:
         fn = _lib.lhl_reduce_c128
+    elif Jc.dtype == torch.complex64:
+        fn = _lib.lhl_reduce_c64
     _check(fn(ws._h, C.c_void_p(Jc.data_ptr()), ld, int(bool(balance)), _stream(stream)), "lhl_reduce")
     ws.reduced = True
     ws._J_keepalive = Jc
@@ -543,9 +555,12 @@ def lhl(J: torch.Tensor, balance: bool = True, thread=True, precision: int = LHL
         shift_complex: bool = False, stream=None) -> LHLWorkspace:
     """``lhl(J; balance=true, shift=...)`` (F:3179): allocate a workspace and reduce J into it;
     ``shift_complex=True`` is ``shift = ComplexF64`` (complex shifts on the real reduction); a
-    complex128 J makes an ``LHLWorkspace{ComplexF64}``."""
+    complex128 J makes an ``LHLWorkspace{ComplexF64}``, a complex64 one an ``LHLWorkspace{ComplexF32}``."""
     if isinstance(J, torch.Tensor) and J.dtype == torch.complex128:
         _require_cuda_f64(J, "J", True)
+    elif isinstance(J, torch.Tensor) and J.dtype == torch.complex64:
+        if not J.is_cuda:
+            raise ArgumentError("J must be a CUDA tensor")
     else:
         _require_cuda_real(J, "J")
     if J.dim() != 2 or J.shape[0] != J.shape[1]:
@@ -572,7 +587,7 @@ def _shift_args(a):
 def lhl_shift_(*args, slot: int = 0, stream=None):
     """``lhl_shift!(ws, sigma, tau)`` / ``lhl_shift!(sh, ws, sigma, tau)`` (F:2456-2489)."""
     sh, ws, sigma, tau, ret = _shift_args(args)
-    if ws.dtype == torch.complex128 and not sh.is_complex:
+    if ws.cj and not sh.is_complex:
         raise ArgumentError("an LHLShift{Float64} cannot serve a workspace of element type ComplexF64")
     if not sh.is_complex:
         for v in (sigma, tau):
@@ -674,7 +689,7 @@ def lhl_refine_(x: torch.Tensor, J: torch.Tensor, b: torch.Tensor, *args, steps:
         raise TypeError("lhl_refine_(x, J, b, ws, steps) or (x, J, b, sh, ws, steps)")
     if steps <= 0:
         return x
-    _require_cuda_f64(J, "J", ws.dtype == torch.complex128)
+    _require_cuda_f64(J, "J", ws.cj)
     for t, nm in ((x, "x"), (b, "b")):
         _require_cuda_f64(t, nm, sh.is_complex)
     n = ws.n
@@ -701,7 +716,7 @@ def lhl_refine_tol_(x: torch.Tensor, J: torch.Tensor, b: torch.Tensor, sh: LHLSh
     ``lhl_refine!`` (F:3144-3157); columns already at relative residual <= tol are skipped on
     the device.  Returns the per-column final relative residuals (device tensor); x is updated
     in place.  `R` (n x k scratch) and `res` (k) may be passed to avoid allocation."""
-    _require_cuda_f64(J, "J", ws.dtype == torch.complex128)
+    _require_cuda_f64(J, "J", ws.cj)
     for t, nm in ((x, "x"), (b, "b")):
         _require_cuda_f64(t, nm, sh.is_complex)
     n = ws.n
@@ -734,7 +749,7 @@ def lhl_refine_gmres_(x: torch.Tensor, J: torch.Tensor, b: torch.Tensor, sh: LHL
     factorisation, for every column above relative residual `tol`.  Returns the per-column
     final relative residuals (device tensor); x is updated in place.  For complex shifts x and b
     are complex128 and GMRES runs on the realified system."""
-    _require_cuda_f64(J, "J", ws.dtype == torch.complex128)
+    _require_cuda_f64(J, "J", ws.cj)
     for t, nm in ((x, "x"), (b, "b")):
         _require_cuda_f64(t, nm, sh.is_complex)
     n = ws.n
@@ -828,7 +843,7 @@ def residual_norms(sh: LHLShift, J: torch.Tensor, b: torch.Tensor, x: torch.Tens
 
 def applyZ_(x: torch.Tensor, ws: LHLWorkspace, stream=None) -> torch.Tensor:
     """``applyZ!(x, ws)``: x <- Z x (F:2069)."""
-    _require_cuda_f64(x, "x", ws.dtype == torch.complex128)
+    _require_cuda_f64(x, "x", ws.cj)
     xx, k, ld = _as_cols(x, ws.n)
     _check(_lib.lhl_applyZ(ws._h, C.c_void_p(xx.data_ptr()), ld, k, _stream(stream)), "applyZ")
     return x
@@ -836,7 +851,7 @@ def applyZ_(x: torch.Tensor, ws: LHLWorkspace, stream=None) -> torch.Tensor:
 
 def applyZinv_(x: torch.Tensor, ws: LHLWorkspace, stream=None) -> torch.Tensor:
     """``applyZinv!(x, ws)``: x <- Z^-1 x (F:2104)."""
-    _require_cuda_f64(x, "x", ws.dtype == torch.complex128)
+    _require_cuda_f64(x, "x", ws.cj)
     xx, k, ld = _as_cols(x, ws.n)
     _check(_lib.lhl_applyZinv(ws._h, C.c_void_p(xx.data_ptr()), ld, k, _stream(stream)), "applyZinv")
     return x

@@ -327,3 +327,42 @@ def test_complex_solves_at_2048(complex_j):
     x = host(G.lhl_ldiv_(dev(b), ws))
     xr = np.linalg.solve(s * np.eye(n) + t * J, b)
     assert np.linalg.norm(x - xr) <= 1e-9 * np.linalg.norm(xr)
+
+
+@pytest.mark.parametrize("n", [30, 200, 800])
+def test_complexf32_workspace(n):
+    """LHLWorkspace{ComplexF32} (a complex64 J): test/core_tests.jl:241-249's solve with
+    T = ComplexF32 and the Float32 tolerance (rtol 1e-3), ComplexF32 right-hand sides in and out;
+    the factors and Ht hold ComplexF32 values and are the ComplexF64 reduction of the rounded J,
+    rounded (bit for bit against the oracle's reduction, the reference's order from n = 768);
+    a complex128 J on the same workspace is rounded on the way in; save / load."""
+    torch, G = _mods()
+    g = np.random.default_rng(13 + n)
+    J = crandn(g, n, n).astype(np.complex64)
+    b = crandn(g, n).astype(np.complex64)
+    gam = np.complex64(0.2 + 0.3j)
+    ws = G.lhl(dev(J))
+    assert ws.dtype == torch.complex64 and ws.shift.is_complex
+    ws.check()
+    R = O.reduce_c128(J.astype(np.complex128), True, path=2)
+    F = host(ws.factors)
+    assert np.array_equal(F, R.factors.astype(np.complex64).astype(np.complex128))
+    assert np.array_equal(host(ws.Ht), R.Ht.astype(np.complex64).astype(np.complex128))
+    assert np.array_equal(host(ws.ipiv), R.ipiv)
+    G.lhl_shift_(ws, 1, complex(-gam))
+    x = G.lhl_ldiv_(dev(b), ws)
+    assert x.dtype == torch.complex64
+    W = np.eye(n) - gam.astype(np.complex128) * J.astype(np.complex128)
+    xr = np.linalg.solve(W, b.astype(np.complex128))
+    assert np.linalg.norm(host(x) - xr) <= 1e-3 * np.linalg.norm(xr)
+    # a complex128 J is rounded to ComplexF32 on the way in: the same reduction
+    w2 = G.LHLWorkspace(n, dtype=torch.complex64)
+    G.lhl_reduce_(w2, dev(J.astype(np.complex128)), True)
+    assert np.array_equal(host(w2.factors), F)
+    if n == 30:
+        import tempfile, os
+        with tempfile.TemporaryDirectory() as d:
+            pth = os.path.join(d, "ws.npz")
+            ws.save(pth)
+            w3 = G.LHLWorkspace.load(pth)
+            assert w3.dtype == torch.complex64 and np.array_equal(host(w3.factors), F)
