@@ -5,8 +5,8 @@ computed by the oracle in the test, since its J depends on the host's BLAS round
 
 Plain FP64 form, through the C ABI via the host mirror:
   * the reduction bit for bit: ipiv equal, factors, Ht, scale, iscale, perm and iperm with the
-    oracle's SHA-256 (the north star's "identical pivot sequence P, H and L"; the reference's
-    own blocked-vs-unblocked pins are test/core_tests.jl:61-92, test/threading.jl:58-79);
+    oracle's SHA-256 (identical pivot sequence P, H and L; the reference's own
+    blocked-vs-unblocked pins are test/core_tests.jl:61-92, test/threading.jl:58-79);
   * the shift LU of sampled shifts bit for bit (test/core_tests.jl:192-233's state, hashed);
   * the sampled right-hand sides solved and refined to relative residual <= 1e-12 (config 3:
     to its FP64 floor eps ||W|| ||x|| / ||b|| where that is higher), with the forward error
