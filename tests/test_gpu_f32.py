@@ -224,3 +224,38 @@ def test_f32_complex_shifts_like_the_reference():
         Wc = sg * np.eye(n) + tg * J.astype(np.complex128)
         xc = np.linalg.solve(Wc, B[:, c].astype(np.complex128))
         assert np.linalg.norm(X[:, c] - xc) <= 1e-3 * np.linalg.norm(xc), c
+
+
+def test_f32_mixed_form_above_the_blocked_threshold():
+    """A mixed Float32 workspace from n = 1024 takes the mixed reduction rounded to float (no
+    blocked float scratch): float factors, a float-accurate similarity, solves within the Float32
+    tolerance."""
+    torch, G = _mods()
+    n = 1100
+    J = rng(1100).standard_normal((n, n)).astype(np.float32)
+    ws = G.lhl(dev(J), precision=G.LHL_PREC_MIXED)
+    ws.check()
+    F = host(ws.factors)
+    assert is_float_valued(F) and is_float_valued(host(ws.Ht))
+    assert np.abs(np.tril(F, -2)).max() <= 1.0
+    b = rng(1101).standard_normal(n).astype(np.float32)
+    G.lhl_shift_(ws, 1, -0.05)
+    x = host(G.lhl_ldiv_(dev(b), ws))
+    W = np.eye(n) - 0.05 * J.astype(np.float64)
+    xr = np.linalg.solve(W, b.astype(np.float64))
+    assert np.linalg.norm(x - xr) <= 1e-3 * np.linalg.norm(xr)
+
+
+def test_element_type_entry_points_refuse_the_wrong_workspace():
+    """lhl_reduce_c64 / lhl_reduce_c128 need a complex-J workspace, lhl_reduce and lhl_reduce_f32
+    a real one (LHL_ERR_ARG, the reference's ArgumentError)."""
+    import ctypes
+    torch, G = _mods()
+    L = G._lib
+    real = G.LHLWorkspace(8, dtype=torch.float32)
+    cplx = G.LHLWorkspace(8, dtype=torch.complex64)
+    Jc = torch.zeros((8, 8), dtype=torch.complex64, device="cuda")
+    Jr = torch.zeros((8, 8), dtype=torch.float32, device="cuda")
+    assert L.lhl_reduce_c64(real._h, ctypes.c_void_p(Jc.data_ptr()), 8, 1, None) == G.LHL_ERR_ARG
+    assert L.lhl_reduce_f32(cplx._h, ctypes.c_void_p(Jr.data_ptr()), 8, 1, None) == G.LHL_ERR_ARG
+    assert L.lhl_reduce_c64(cplx._h, ctypes.c_void_p(Jc.data_ptr()), 4, 1, None) == G.LHL_ERR_DIM
