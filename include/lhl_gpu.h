@@ -123,6 +123,13 @@ int lhl_reduce(lhl_ws_t ws, const double* dJ, int64_t ldj, int balance, void* st
 int lhl_ws_import(lhl_ws_t ws, const double* dfactors, const double* dHt, const int64_t* dipiv, const int64_t* dperm,
                   const int64_t* diperm, const double* dscale, const double* discale, void* stream);
 
+/* lhl_ldiv!(x, sh, ws) with a complex x on a real shift object (F:3052-3074: eltype(x) differs
+ * from the shift's, the generic path): x n x nrhs interleaved complex (ld ldx complex elements),
+ * in place.  A real shift is real-linear, so the real and imaginary parts are solved as two real
+ * right-hand sides of the same shift slot.  A complex shift object takes the plain lhl_ldiv. */
+int lhl_ldiv_complex_rhs(lhl_shift_t sh, lhl_ws_t ws, double* dX, int64_t ldx, int64_t nrhs, int64_t rhs_per_shift,
+                         void* stream);
+
 /* ---- element type Float32 (LHLWorkspace{Float32}, F:703-705) ------------------------
  * lhl_ws_create_f32 makes a workspace whose element type is Float32.  Its arrays keep FP64
  * storage holding float values, so every view, shift object and solve entry point of this

@@ -843,6 +843,36 @@ int lhl_ldiv(lhl_shift_t sh, lhl_ws_t ws, double* dX, int64_t ldx, int64_t nrhs,
     return ldiv_common(sh, ws, dX, ldx, nrhs, rhs_per_shift, 0, (cudaStream_t)stream);
 }
 
+int lhl_ldiv_complex_rhs(lhl_shift_t sh, lhl_ws_t ws, double* dX, int64_t ldx, int64_t nrhs, int64_t rhs_per_shift,
+                         void* stream)
+{
+    if (!sh || !ws) return LHL_ERR_ARG;
+    if (sh->cplx) return lhl_ldiv(sh, ws, dX, ldx, nrhs, rhs_per_shift, stream);  // a complex shift: as always
+    if (sh->n != ws->n) return LHL_ERR_DIM;
+    if (ws->cj) return LHL_ERR_ARG;  // a complex J takes complex shift objects only
+    if (rhs_per_shift < 1) return LHL_ERR_ARG;
+    if (nrhs < 0) return LHL_ERR_DIM;
+    if (nrhs > 0 && (nrhs + rhs_per_shift - 1) / rhs_per_shift > sh->nshifts) return LHL_ERR_DIM;
+    const int64_t n = ws->n;
+    if (nrhs == 0 || n == 0) return LHL_OK;
+    if (!dX) return LHL_ERR_ARG;
+    if (ldx < n) return LHL_ERR_DIM;
+    cudaStream_t st = (cudaStream_t)stream;
+    // a real shift is real-linear: the real and imaginary parts solve as two real columns
+    const size_t need = 2 * (size_t)n * (size_t)nrhs;
+    if (ws->f32x_cap < need || !ws->f32x) {
+        if (ws->f32x) cudaFree(ws->f32x);
+        ws->f32x = nullptr;
+        ws->f32x_cap = 0;
+        if (cudaMalloc((void**)&ws->f32x, need * sizeof(double)) != cudaSuccess) return LHL_ERR_ALLOC;
+        ws->f32x_cap = need;
+    }
+    if (lhl::launch_split_complex(dX, (int)ldx, ws->f32x, (int)n, (int)nrhs, st) != cudaSuccess) return LHL_ERR_CUDA;
+    const int rc = ldiv_common(sh, ws, ws->f32x, n, 2 * nrhs, 2 * rhs_per_shift, 0, st);
+    if (rc != LHL_OK) return rc;
+    return cuda_status(lhl::launch_join_complex(ws->f32x, (int)n, dX, (int)ldx, (int)nrhs, st));
+}
+
 int lhl_ldiv_f32(lhl_shift_t sh, lhl_ws_t ws, float* dX, int64_t ldx, int64_t nrhs, int64_t rhs_per_shift,
                  void* stream)
 {

@@ -39,6 +39,26 @@ __global__ void f64_to_f32_kernel(const double* __restrict__ src, int lds, float
     }
 }
 
+// complex columns <-> pairs of real columns: column c of the interleaved complex block X (ld
+// ldx complex elements) is real column 2c (real parts) and 2c + 1 (imaginary parts) of R (ld n)
+__global__ void split_complex_kernel(const double* __restrict__ X, int ldx, double* __restrict__ R, int n, int cols)
+{
+    const size_t total = (size_t)n * cols * 2;
+    for (size_t e = (size_t)blockIdx.x * blockDim.x + threadIdx.x; e < total; e += (size_t)gridDim.x * blockDim.x) {
+        const int rc = (int)(e / n), r = (int)(e - (size_t)rc * n);  // real column rc = 2c + p
+        R[(size_t)rc * n + r] = X[2 * ((size_t)(rc >> 1) * ldx + r) + (rc & 1)];
+    }
+}
+
+__global__ void join_complex_kernel(const double* __restrict__ R, int n, double* __restrict__ X, int ldx, int cols)
+{
+    const size_t total = (size_t)n * cols * 2;
+    for (size_t e = (size_t)blockIdx.x * blockDim.x + threadIdx.x; e < total; e += (size_t)gridDim.x * blockDim.x) {
+        const int rc = (int)(e / n), r = (int)(e - (size_t)rc * n);
+        X[2 * ((size_t)(rc >> 1) * ldx + r) + (rc & 1)] = R[(size_t)rc * n + r];
+    }
+}
+
 static unsigned conv_grid(size_t total)
 {
     const size_t b = (total + 255) / 256;
@@ -63,6 +83,20 @@ cudaError_t launch_f64_to_f32(const double* src, int lds, float* dst, int ldd, i
 {
     if (rows <= 0 || cols <= 0) return cudaSuccess;
     f64_to_f32_kernel<<<conv_grid((size_t)rows * cols), 256, 0, st>>>(src, lds, dst, ldd, rows, cols);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_split_complex(const double* X, int ldx, double* R, int n, int cols, cudaStream_t st)
+{
+    if (n <= 0 || cols <= 0) return cudaSuccess;
+    split_complex_kernel<<<conv_grid((size_t)n * cols * 2), 256, 0, st>>>(X, ldx, R, n, cols);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_join_complex(const double* R, int n, double* X, int ldx, int cols, cudaStream_t st)
+{
+    if (n <= 0 || cols <= 0) return cudaSuccess;
+    join_complex_kernel<<<conv_grid((size_t)n * cols * 2), 256, 0, st>>>(R, n, X, ldx, cols);
     return cudaGetLastError();
 }
 

@@ -257,6 +257,9 @@ cudaError_t launch_residual_cj(int n, const double* J, int ldj, const double* B,
 cudaError_t launch_f32_to_f64(const float* src, int lds, double* dst, int ldd, int rows, int cols, cudaStream_t st);
 cudaError_t launch_round_f32(const double* src, int lds, double* dst, int ldd, int rows, int cols, cudaStream_t st);
 cudaError_t launch_f64_to_f32(const double* src, int lds, float* dst, int ldd, int rows, int cols, cudaStream_t st);
+// interleaved complex columns (ld ldx complex elements) <-> real column pairs (re, im; ld n)
+cudaError_t launch_split_complex(const double* X, int ldx, double* R, int n, int cols, cudaStream_t st);
+cudaError_t launch_join_complex(const double* R, int n, double* X, int ldx, int cols, cudaStream_t st);
 
 // GMRES-IR (gmres.cu)
 size_t gm_state_doubles(int m);

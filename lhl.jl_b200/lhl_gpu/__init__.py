@@ -87,6 +87,7 @@ def _load():
         "lhl_refine_system_gmres": [vp, vp, i64, vp, i64, vp, i64, vp, i64, vp, vp, i64, d, i32, i32, i32, vp],
         "lhl_reduce_c128": [vp, vp, i64, i32, vp],
         "lhl_reduce_c64": [vp, vp, i64, i32, vp],
+        "lhl_ldiv_complex_rhs": [vp, vp, vp, i64, i64, i64, vp],
         "lhl_shift_create": [i64, i64, C.POINTER(vp)],
         "lhl_shift_destroy": [vp],
         "lhl_shift_get_view": [vp, C.POINTER(_ShView)],
@@ -646,6 +647,22 @@ def _as_cols(x: torch.Tensor, n: int):
     raise DimensionMismatch("x must be a vector or an (n, k) block")
 
 
+def _split_complex(v: torch.Tensor, n: int) -> torch.Tensor:
+    """A complex (n,) or (n, k) tensor as real column pairs: (n, 2k) float64, column-major,
+    column 2c holding the real parts of column c and 2c + 1 its imaginary parts."""
+    k = 1 if v.dim() == 1 else v.shape[1]
+    r = torch.empty((2 * k, n), dtype=torch.float64, device=v.device).t()
+    r.unflatten(1, (k, 2)).copy_(torch.view_as_real(v.reshape(n, k)))
+    return r
+
+
+def _join_complex(r: torch.Tensor, v: torch.Tensor) -> None:
+    """The inverse of _split_complex, into v."""
+    n = r.shape[0]
+    k = 1 if v.dim() == 1 else v.shape[1]
+    torch.view_as_real(v.view(n, k) if v.dim() == 1 else v).copy_(r.unflatten(1, (k, 2)))
+
+
 def lhl_ldiv_(x: torch.Tensor, *args, rhs_per_shift: int = 1, stream=None) -> torch.Tensor:
     """``lhl_ldiv!(x, ws)`` / ``lhl_ldiv!(x, sh, ws)`` (F:3052-3068).  Column j of an (n, k)
     block uses shift slot j // rhs_per_shift."""
@@ -655,7 +672,18 @@ def lhl_ldiv_(x: torch.Tensor, *args, rhs_per_shift: int = 1, stream=None) -> to
     else:
         sh, ws = args
     if x.is_complex() and not sh.is_complex:
-        raise ArgumentError("a complex right-hand side needs an LHLShift built for complex shifts")
+        # the generic path (F:3052-3074): a real shift solves the real and imaginary parts
+        if sh.n != ws.n:
+            raise DimensionMismatch(f"the LHLShift is {sh.n}x{sh.n}, the workspace {ws.n}x{ws.n}")
+        if not x.is_cuda:
+            raise ArgumentError("x must be a CUDA tensor")
+        xd = x if x.dtype == torch.complex128 else x.to(torch.complex128)
+        xx, k, ld = _as_cols(xd, ws.n)
+        _check(_lib.lhl_ldiv_complex_rhs(sh._h, ws._h, C.c_void_p(xx.data_ptr()), ld, k, int(rhs_per_shift),
+                                         _stream(stream)), "lhl_ldiv")
+        if xd is not x:
+            x.copy_(xd)
+        return x
     if x.dtype == torch.float32 and not sh.is_complex:  # float vectors: widened, solved, rounded back
         _require_cuda_real(x, "x")
         fn = _lib.lhl_ldiv_f32
@@ -690,6 +718,14 @@ def lhl_refine_(x: torch.Tensor, J: torch.Tensor, b: torch.Tensor, *args, steps:
     if steps <= 0:
         return x
     _require_cuda_f64(J, "J", ws.cj)
+    if not sh.is_complex and isinstance(x, torch.Tensor) and x.dtype == torch.complex128:
+        # complex vectors on a real shift (the reference's generic path, F:3144-3157 with F:3052-3074):
+        # A = sigma I + tau J is real, so the real and imaginary parts refine as two real columns
+        _require_cuda_f64(b, "b", True)
+        xr, br = _split_complex(x, ws.n), _split_complex(b, ws.n)
+        lhl_refine_(xr, J, br, sh, ws, steps, rhs_per_shift=2 * rhs_per_shift, stream=stream)
+        _join_complex(xr, x)
+        return x
     for t, nm in ((x, "x"), (b, "b")):
         _require_cuda_f64(t, nm, sh.is_complex)
     n = ws.n

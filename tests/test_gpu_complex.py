@@ -257,8 +257,13 @@ def test_complex_errors_mirror_the_reference():
     with pytest.raises(G.ArgumentError):  # complex shift on a real LHLShift (F:2466-2472)
         G.lhl_shift_(ws, 1.0, -0.3j)
     G.lhl_shift_(ws, 1.0, -0.3)
-    with pytest.raises(G.ArgumentError):  # complex x with a real shift
-        G.lhl_ldiv_(dev(np.ones(n) + 0j), ws)
+    # complex x with a real shift: the reference's generic path (F:3052-3074), the two parts
+    # solved as real vectors
+    z = dev(np.arange(1.0, n + 1) + 1j * np.ones(n))
+    assert G.lhl_ldiv_(z, ws) is z
+    xr = host(G.lhl_ldiv_(dev(np.arange(1.0, n + 1)), ws))
+    xi = host(G.lhl_ldiv_(dev(np.ones(n)), ws))
+    assert np.allclose(host(z), xr + 1j * xi, rtol=1e-13, atol=0)
     wc = G.lhl(dev(J), shift_complex=True)
     G.lhl_shift_(wc, 1.0 + 1j, -0.3)
     with pytest.raises(G.ArgumentError):  # a real x cannot hold a complex shift's solution (F:3084-3085)
@@ -342,3 +347,36 @@ def test_few_groups_refine_through_the_grid_wide_solve(n, rps, groups):
             assert np.linalg.norm(X2h[:, c] - Xh[:, c]) <= 1e-10 * np.linalg.norm(Xh[:, c]), (n, c)
         else:
             assert bits_equal(X2h[:, c], Xh[:, c]), (n, c)
+
+
+@pytest.mark.parametrize("T", ["float64", "float32"])
+@pytest.mark.parametrize("n", [3, 7, 33, 130, 331, 500])
+def test_complex_vectors_on_a_real_shift_like_the_reference(n, T):
+    """test/core_tests.jl:38-58's third solve: z = lhl_ldiv!(complex.(b), ws) on a real shift
+    (another element type: the generic path) agrees with W \\ b at the element type's tolerance;
+    the imaginary part stays zero; and lhl_refine! with complex vectors refines both parts as the
+    real refinement does."""
+    torch, G = _mods()
+    dt = np.float64 if T == "float64" else np.float32
+    J = rng(n).standard_normal((n, n)).astype(dt)
+    b = rng(n + 7).standard_normal(n).astype(dt)
+    ws = G.lhl(dev(J))
+    G.lhl_shift_(ws, 1, -0.05)
+    W = np.eye(n) - dt(0.05) * J.astype(np.float64)
+    z = dev(b.astype(np.complex128 if T == "float64" else np.complex64))
+    G.lhl_ldiv_(z, ws)
+    zh = host(z).astype(np.complex128)
+    xr = np.linalg.solve(W, b.astype(np.float64))
+    assert np.linalg.norm(zh.real - xr) <= (1e-9 if T == "float64" else 1e-3) * np.linalg.norm(xr)
+    assert np.all(zh.imag == 0)
+    if T == "float64":
+        Jd = dev(J)
+        B = b + 1j * rng(n + 8).standard_normal(n)
+        x = G.lhl_ldiv_(dev(B), ws)
+        G.lhl_refine_(x, Jd, dev(B), ws, 1)
+        xre = G.lhl_ldiv_(dev(B.real.copy()), ws)
+        G.lhl_refine_(xre, Jd, dev(B.real.copy()), ws, 1)
+        xim = G.lhl_ldiv_(dev(B.imag.copy()), ws)
+        G.lhl_refine_(xim, Jd, dev(B.imag.copy()), ws, 1)
+        assert np.allclose(host(x), host(xre) + 1j * host(xim), rtol=1e-12, atol=0)
+        assert O.bwd(W, host(x), B) < 50 * np.finfo(float).eps
