@@ -206,6 +206,12 @@ int lhl_shift(lhl_shift_t sh, lhl_ws_t ws, int64_t slot, double sigma, double ta
  * dR (CuArray{ComplexF64} memory; leading dimensions counted in complex elements), and the
  * solve is the reference's complex-on-real one (F:3080-3110). */
 int lhl_shift_create_complex(int64_t n, int64_t nshifts, lhl_shift_t* sh);
+/* LHLShift{Float32} / LHLShift{ComplexF32}: shift objects for the single-precision workspaces
+ * (lhl_ws_create_f32, lhl_ws_create_c64).  An LHLShift{TG} serves an LHLWorkspace{T} only for
+ * TG = T or Complex{real(T)} (F:2461-2465): a single-precision shift object on a double-precision
+ * workspace, or the other way round, makes the shift calls return LHL_ERR_ARG. */
+int lhl_shift_create_f32(int64_t n, int64_t nshifts, lhl_shift_t* sh);
+int lhl_shift_create_complex64(int64_t n, int64_t nshifts, lhl_shift_t* sh);
 /* lhl_shift!(sh, ws, sigma, tau) with complex sigma, tau (F:2456-2594 with TG = ComplexF64).
  * A shift object made by lhl_shift_create takes only real shifts: LHL_ERR_ARG otherwise
  * (F:2466-2472).  A real shift on a complex object is converted. */

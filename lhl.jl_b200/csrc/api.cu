@@ -49,6 +49,7 @@ struct lhl_shift_s {
     uint8_t* swap;
     int32_t* info;
     int cj;        // the slots were last loaded from a complex reduction: residuals take a complex J
+    int single;    // element type Float32 / ComplexF32: serves Float32 and ComplexF32 workspaces only
 };
 
 struct lhl_batch_s {
@@ -622,6 +623,21 @@ int lhl_shift_create_complex(int64_t n, int64_t nshifts, lhl_shift_t* out)
     return shift_create(n, nshifts, 1, out);
 }
 
+// LHLShift{Float32} and LHLShift{ComplexF32}: the shift objects of single-precision workspaces
+int lhl_shift_create_f32(int64_t n, int64_t nshifts, lhl_shift_t* out)
+{
+    const int rc = shift_create(n, nshifts, 0, out);
+    if (rc == LHL_OK) (*out)->single = 1;
+    return rc;
+}
+
+int lhl_shift_create_complex64(int64_t n, int64_t nshifts, lhl_shift_t* out)
+{
+    const int rc = shift_create(n, nshifts, 1, out);
+    if (rc == LHL_OK) (*out)->single = 1;
+    return rc;
+}
+
 int lhl_shift_destroy(lhl_shift_t s)
 {
     if (!s) return LHL_ERR_ARG;
@@ -680,6 +696,8 @@ static int shift_args(lhl_shift_t sh, lhl_ws_t ws, int64_t s0, int64_t count)
 {
     if (!sh || !ws) return LHL_ERR_ARG;
     if (ws->cj && !sh->cplx) return LHL_ERR_ARG;  // an LHLShift{Float64} cannot serve a ComplexF64 workspace (F:2463-2465)
+    // an LHLShift{TG} serves an LHLWorkspace{T} for TG = T or Complex{real(T)} only (F:2461-2465)
+    if (sh->single != (ws->f32 ? 1 : 0)) return LHL_ERR_ARG;
     if (sh->n != ws->n) return LHL_ERR_DIM;
     if (s0 < 0 || count < 0 || s0 + count > sh->nshifts) return LHL_ERR_DIM;
     return LHL_OK;

@@ -87,6 +87,8 @@ def _load():
         "lhl_refine_system_gmres": [vp, vp, i64, vp, i64, vp, i64, vp, i64, vp, vp, i64, d, i32, i32, i32, vp],
         "lhl_reduce_c128": [vp, vp, i64, i32, vp],
         "lhl_reduce_c64": [vp, vp, i64, i32, vp],
+        "lhl_shift_create_f32": [i64, i64, C.POINTER(vp)],
+        "lhl_shift_create_complex64": [i64, i64, C.POINTER(vp)],
         "lhl_ldiv_complex_rhs": [vp, vp, vp, i64, i64, i64, vp],
         "lhl_shift_create": [i64, i64, C.POINTER(vp)],
         "lhl_shift_destroy": [vp],
@@ -196,18 +198,29 @@ def _require_cuda_real(x: torch.Tensor, name: str):
         raise ArgumentError(f"{name} must be float64 or float32")
 
 
+def _shift_creator(complex_: bool, single: bool):
+    if single:
+        return _lib.lhl_shift_create_complex64 if complex_ else _lib.lhl_shift_create_f32
+    return _lib.lhl_shift_create_complex if complex_ else _lib.lhl_shift_create
+
+
 class LHLShift:
     """``LHLShift{Float64}(n)`` or, with ``complex=True``, ``LHLShift{ComplexF64}(n)`` on a real
     reduction: a batch of ``nshifts`` shift slots (src/LHLFactorization.jl:84-116).  A complex
     shift object's Gt is planar: (2 po) x n per slot, real parts in rows 0..n-1, imaginary
-    parts in rows po..po+n-1."""
+    parts in rows po..po+n-1.  ``single=True`` makes ``LHLShift{Float32}`` /
+    ``LHLShift{ComplexF32}``, the shift objects of single-precision workspaces; given a workspace
+    instead of an order (``LHLShift{TG}(ws)``), the precision is the workspace's.  An
+    ``LHLShift{TG}`` serves an ``LHLWorkspace{T}`` only for TG = T or Complex{real(T)}."""
 
-    def __init__(self, n, nshifts: int = 1, complex: bool = False):
+    def __init__(self, n, nshifts: int = 1, complex: bool = False, single: bool = None):
         if isinstance(n, LHLWorkspace):
+            if single is None:
+                single = n.single
             n = n.n
+        self.single = bool(single)
         self._h = C.c_void_p()
-        create = _lib.lhl_shift_create_complex if complex else _lib.lhl_shift_create
-        _check(create(int(n), int(nshifts), C.byref(self._h)), "LHLShift")
+        _check(_shift_creator(complex, self.single)(int(n), int(nshifts), C.byref(self._h)), "LHLShift")
         self.n = int(n)
         self.nshifts = int(nshifts)
         v = _ShView()
@@ -229,8 +242,7 @@ class LHLShift:
         if n == self.n:
             return self
         h = C.c_void_p()
-        create = _lib.lhl_shift_create_complex if self.is_complex else _lib.lhl_shift_create
-        _check(create(n, self.nshifts, C.byref(h)), "LHLShift")
+        _check(_shift_creator(self.is_complex, self.single)(n, self.nshifts, C.byref(h)), "LHLShift")
         old, self._h = self._h, h
         if old is not None and old.value:
             _lib.lhl_shift_destroy(old)
@@ -317,6 +329,7 @@ class LHLWorkspace:
             raise ArgumentError(f"element type {dtype} is not supported (float64, float32, complex128 or complex64)")
         self.dtype = dtype
         self.cj = dtype in (torch.complex128, torch.complex64)  # a complex J (its factors are complex128 views)
+        self.single = dtype in (torch.float32, torch.complex64)  # Float32 / ComplexF32 element type
         self.device = torch.device("cuda", torch.cuda.current_device())  # where its arrays live
         self.n = int(n)
         self.precision = precision
@@ -325,7 +338,7 @@ class LHLWorkspace:
         _check(_lib.lhl_ws_get_view(self._h, C.byref(v)))
         self._v = v
         # ws.shift: LHLShift{Float64}, or LHLShift{ComplexF64} for shift = Complex{T} (F:164-178)
-        self.shift = LHLShift(self.n, 1, complex=self.shift_complex)
+        self.shift = LHLShift(self.n, 1, complex=self.shift_complex, single=self.single)
         self.reduced = False
 
     def __del__(self):

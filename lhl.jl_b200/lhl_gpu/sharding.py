@@ -166,8 +166,8 @@ def sharded_chain(G, ws, J: torch.Tensor, B: torch.Tensor, sigmas: torch.Tensor,
         X_local = torch.empty((n, 0), dtype=B.dtype, device=B.device)
         res = torch.empty(0, dtype=torch.float64, device=B.device)
     else:
-        cplx = sigmas.is_complex() or taus.is_complex() or getattr(ws, "dtype", None) == torch.complex128
-        sh = G.LHLShift(n, cnt, complex=cplx)
+        cplx = sigmas.is_complex() or taus.is_complex() or getattr(ws, "cj", False)
+        sh = G.LHLShift(ws, cnt, complex=cplx)  # the workspace's precision
         G.lhl_shift_batched_(sh, ws, sigmas[s0:s0 + cnt].contiguous(), taus[s0:s0 + cnt].contiguous())
         Bl = B[:, s0 * R:(s0 + cnt) * R]
         X_local = torch.empty((cnt * R, n), dtype=B.dtype, device=B.device).t()

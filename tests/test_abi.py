@@ -122,7 +122,7 @@ def test_creators_check_sizes_and_pointers_on_host():
     L = C.CDLL(LIB)
     vp, i64, i32 = C.c_void_p, C.c_int64, C.c_int
     h = vp()
-    for name in ("lhl_shift_create", "lhl_shift_create_complex"):
+    for name in ("lhl_shift_create", "lhl_shift_create_complex", "lhl_shift_create_f32", "lhl_shift_create_complex64"):
         f = getattr(L, name)
         f.argtypes = [i64, i64, C.POINTER(vp)]
         assert f(-1, 1, C.byref(h)) == 2 and f(4, -1, C.byref(h)) == 2 and f(4, 1, None) == 1, name

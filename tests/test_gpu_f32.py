@@ -213,7 +213,7 @@ def test_f32_complex_shifts_like_the_reference():
     assert ws.shift.σ == complex(s)  # stored rounded to ComplexF32 (0.4 and 0.7 are not floats)
     # a batch of complex shifts, several ComplexF32 right-hand sides each
     S, R = 3, 2
-    sh = G.LHLShift(n, S, complex=True)
+    sh = G.LHLShift(ws, S, complex=True)  # LHLShift{ComplexF32}(ws)
     sigs = np.array([0.4 + 0.7j, 1.5 - 0.2j, 3j], dtype=np.complex128)
     taus = np.array([-1.0 + 0j, -0.5 + 0.1j, 1.0 + 0j], dtype=np.complex128)
     G.lhl_shift_batched_(sh, ws, dev(sigs), dev(taus))
@@ -259,3 +259,24 @@ def test_element_type_entry_points_refuse_the_wrong_workspace():
     assert L.lhl_reduce_c64(real._h, ctypes.c_void_p(Jc.data_ptr()), 8, 1, None) == G.LHL_ERR_ARG
     assert L.lhl_reduce_f32(cplx._h, ctypes.c_void_p(Jr.data_ptr()), 8, 1, None) == G.LHL_ERR_ARG
     assert L.lhl_reduce_c64(cplx._h, ctypes.c_void_p(Jc.data_ptr()), 4, 1, None) == G.LHL_ERR_DIM
+
+
+def test_shift_types_follow_the_reference_rule():
+    """An LHLShift{TG} serves an LHLWorkspace{T} only for TG = T or Complex{real(T)}
+    (F:2461-2465; test/core_tests.jl:315: LHLShift{ComplexF64} on a Float32 workspace is an
+    ArgumentError), and the other way round."""
+    torch, G = _mods()
+    J32 = rng(3).standard_normal((3, 3)).astype(np.float32)
+    w32 = G.lhl(dev(J32))
+    with pytest.raises(G.ArgumentError):
+        G.lhl_shift_(G.LHLShift(3, complex=True), w32, 1, 1)      # LHLShift{ComplexF64}
+    with pytest.raises(G.ArgumentError):
+        G.lhl_shift_(G.LHLShift(3), w32, 1, 1)                    # LHLShift{Float64}
+    G.lhl_shift_(G.LHLShift(3, complex=True, single=True), w32, 1, 1)   # LHLShift{ComplexF32}
+    G.lhl_shift_(G.LHLShift(w32), w32, 1, 1)                      # LHLShift{Float32}(ws)
+    w64 = G.lhl(dev(J32.astype(np.float64)))
+    with pytest.raises(G.ArgumentError):
+        G.lhl_shift_(G.LHLShift(3, single=True), w64, 1, 1)       # LHLShift{Float32} on Float64
+    with pytest.raises(G.ArgumentError):
+        G.lhl_shift_(G.LHLShift(3, complex=True, single=True), w64, 1, 1)
+    G.lhl_shift_(G.LHLShift(3, complex=True), w64, 1, 1)
