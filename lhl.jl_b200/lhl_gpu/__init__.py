@@ -842,6 +842,20 @@ def lhl_refine_system_(x: torch.Tensor, A: torch.Tensor, b: torch.Tensor, *args,
     else:
         raise TypeError("lhl_refine_system_(x, A, b, ws, steps) or (x, A, b, sh, ws, steps)")
     cplx = sh.is_complex
+    if (not cplx and isinstance(x, torch.Tensor) and x.dtype == torch.complex128 and isinstance(A, torch.Tensor)
+            and not A.is_complex()):
+        # complex vectors, a real A and a real shift (the reference's generic path): the real and
+        # imaginary parts refine as real columns of the same slot
+        _require_cuda_f64(b, "b", True)
+        xr, br = _split_complex(x, ws.n), _split_complex(b, ws.n)
+        r2 = None if res is None else torch.empty(xr.shape[1], dtype=torch.float64, device=xr.device)
+        lhl_refine_system_(xr, A, br, sh, ws, steps, slot=slot, tol=tol, gmres=gmres, restart=restart,
+                           host_check=host_check, res=r2, stream=stream)
+        _join_complex(xr, x)
+        if res is not None:  # a complex column's residual from its two parts' (2-norms combine)
+            part = torch.nan_to_num(r2 * br.norm(dim=0)).view(-1, 2)  # ||r_re||, ||r_im|| per column
+            res.copy_(part.norm(dim=1) / torch.linalg.vector_norm(b.reshape(ws.n, -1), dim=0))
+        return x
     _require_cuda_f64(A, "A", cplx)
     for t, nm in ((x, "x"), (b, "b")):
         _require_cuda_f64(t, nm, cplx)

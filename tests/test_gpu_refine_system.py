@@ -130,3 +130,28 @@ def test_system_refusals():
         G.lhl_refine_system_(x, dev(np.eye(n)), dev(np.ones(n)), ws, 1, slot=1)
     with pytest.raises(G.ArgumentError):  # a real shift object takes a real A
         G.lhl_refine_system_(x, dev(np.eye(n, dtype=np.complex128)), dev(np.ones(n)), ws, 1)
+
+
+def test_complex_vectors_with_a_real_A_on_a_real_shift():
+    """lhl_refine!(x, A, b, ws, steps) with complex x and b, a real A and a real shift (the
+    reference's generic path): the same as refining the real and imaginary parts on their own,
+    and the returned residuals are at the FP64 floor, as the complex columns' ||b - A x|| / ||b||."""
+    torch, G = _mods()
+    n = 60
+    g = np.random.default_rng(61)
+    J = g.standard_normal((n, n))
+    A = np.eye(n) - 0.1 * J
+    b = g.standard_normal((n, 2)) + 1j * g.standard_normal((n, 2))
+    ws = G.lhl(dev(J))
+    G.lhl_shift_(ws, 1, -0.1)
+    x = G.lhl_ldiv_(dev(b), ws, rhs_per_shift=2)
+    res = torch.empty(2, dtype=torch.float64, device="cuda")
+    G.lhl_refine_system_(x, dev(A), dev(b), ws, 2, res=res)
+    xr = G.lhl_ldiv_(dev(np.ascontiguousarray(b.real)), ws, rhs_per_shift=2)
+    G.lhl_refine_system_(xr, dev(A), dev(np.ascontiguousarray(b.real)), ws, 2)
+    xi = G.lhl_ldiv_(dev(np.ascontiguousarray(b.imag)), ws, rhs_per_shift=2)
+    G.lhl_refine_system_(xi, dev(A), dev(np.ascontiguousarray(b.imag)), ws, 2)
+    assert np.allclose(host(x), host(xr) + 1j * host(xi), rtol=1e-12, atol=0)
+    xh = host(x)
+    want = np.linalg.norm(b - A @ xh, axis=0) / np.linalg.norm(b, axis=0)
+    assert np.all(want <= 1e-13) and np.all(host(res) <= 1e-13)  # both at the FP64 floor
