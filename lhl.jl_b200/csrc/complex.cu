@@ -323,12 +323,9 @@ cudaError_t launch_hess_cplx(int n, const double* Gt, int ldg, int po, const uin
     if (count <= 0 || n <= 0) return cudaSuccess;
     const size_t smem = (size_t)2 * n * sizeof(double);
     if (smem > 150 * 1024) return cudaErrorInvalidValue;
-    static size_t attr = 0;
-    if (smem > attr) {  // opt in for any size: the static tiles (17 KB) come on top of it
-        cudaError_t e = cudaFuncSetAttribute(hess_cplx_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-        if (e != cudaSuccess) return e;
-        attr = smem;
-    }
+    static size_t attr[MAX_DEVICES] = {};  // opt in for any size: the static tiles (17 KB) come on top of it
+    cudaError_t e = opt_in_smem((const void*)hess_cplx_kernel, smem, attr);
+    if (e != cudaSuccess) return e;
     hess_cplx_kernel<<<count, CT, smem, st>>>(n, Gt, ldg, po, swp, rd, Y, ldy, col0, rhs_per_shift, done, tol);
     return cudaGetLastError();
 }
@@ -801,12 +798,10 @@ cudaError_t launch_hess_cplx_mrhs(int n, const double* Gt, int ldg, int po, cons
     const long long grid = (long long)(s_last - s_first + 1) * gps;
     if (grid > 0x7fffffffll) return cudaErrorInvalidValue;
     const size_t smem = sizeof(MrhsSmem);
-    static bool attr = false;
-    if (!attr) {
-        cudaError_t e = cudaFuncSetAttribute(hess_cplx_mrhs_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                             (int)smem);
+    static size_t attr[MAX_DEVICES] = {};
+    {
+        cudaError_t e = opt_in_smem((const void*)hess_cplx_mrhs_kernel, smem, attr);
         if (e != cudaSuccess) return e;
-        attr = true;
     }
     // refinement steps (done given): the few-groups path takes over when at most HT_MAX groups
     // are left; its plan is counted on the device, so neither launch waits for the host
@@ -821,13 +816,15 @@ cudaError_t launch_hess_cplx_mrhs(int n, const double* Gt, int ldg, int po, cons
                                                              tail_path ? tail : nullptr);
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess || !tail_path) return e;
-    static int sms = 0;
-    if (!sms) {
-        int dev = 0;
-        e = cudaGetDevice(&dev);
-        if (e == cudaSuccess) e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    static int sms_of[MAX_DEVICES] = {};
+    int dev = 0;
+    e = current_device(&dev);
+    if (e != cudaSuccess) return e;
+    if (!sms_of[dev]) {
+        e = cudaDeviceGetAttribute(&sms_of[dev], cudaDevAttrMultiProcessorCount, dev);
         if (e != cudaSuccess) return e;
     }
+    const int sms = sms_of[dev];
     int sf = s_first, gp = gps;
     void* args[] = {&n, &Gt, &ldg, &po, &swp, &rd, &Y, &ldy, &col0, &count, &rhs_per_shift, &sf, &gp,
                     &tail, &err, &limit_ns};
@@ -998,13 +995,9 @@ cudaError_t launch_residual_cplx(int n, const double* J, int ldj, const double* 
     if (nrhs <= 0 || n <= 0) return cudaSuccess;
     if (nrhs >= 16 && (nrhs + RC - 1) / RC <= 65535) {  // many right-hand sides: the tensor-pipe GEMM
         const size_t smem = sizeof(ResSmem);
-        static bool attr = false;
-        if (!attr) {
-            cudaError_t e = cudaFuncSetAttribute(residual_cplx_mma_kernel,
-                                                 cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-            if (e != cudaSuccess) return e;
-            attr = true;
-        }
+        static size_t attr[MAX_DEVICES] = {};
+        cudaError_t e = opt_in_smem((const void*)residual_cplx_mma_kernel, smem, attr);
+        if (e != cudaSuccess) return e;
         dim3 grid((n + RM - 1) / RM, (nrhs + RC - 1) / RC);
         residual_cplx_mma_kernel<<<grid, RTT, smem, st>>>(n, J, ldj, B, ldb, X, ldx, R, ldr, nrhs, rhs_per_shift, sig,
                                                            tau, done, tol);

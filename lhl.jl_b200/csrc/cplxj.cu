@@ -629,13 +629,14 @@ __global__ void cj_ht_kernel(int n, const double* __restrict__ A, double* __rest
 // one CTA per SM at most, at least one warp of rows per CTA; together they hold >= n rows
 int cj_grid_size(int n)
 {
-    static int sms = 0;
-    if (sms == 0) {
-        int dev = 0;
-        if (cudaGetDevice(&dev) != cudaSuccess ||
-            cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || sms <= 0)
-            sms = 1;
+    static int sms_of[MAX_DEVICES] = {};
+    int dev = 0;
+    if (current_device(&dev) != cudaSuccess) dev = 0;
+    if (sms_of[dev] == 0) {
+        int c = 0;
+        sms_of[dev] = (cudaDeviceGetAttribute(&c, cudaDevAttrMultiProcessorCount, dev) == cudaSuccess && c > 0) ? c : 1;
     }
+    const int sms = sms_of[dev];
     const int warps = (n + 31) / 32;
     int g = warps < sms ? warps : sms;
     if (g < 1) g = 1;
@@ -652,18 +653,11 @@ cudaError_t launch_reduce_cj(CjArgs a, int balance, cudaStream_t st)
     if (n > CJ_NMAX) return cudaErrorInvalidValue;
     const int grid = cj_grid_size(n);
     const size_t smem = cj_smem(n);
-    static size_t attr_r = 0, attr_a = 0;
-    cudaError_t e = cudaSuccess;
-    if (smem > attr_r) {
-        e = cudaFuncSetAttribute(cj_reduce_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-        if (e != cudaSuccess) return e;
-        attr_r = smem;
-    }
-    if (smem > attr_a) {
-        e = cudaFuncSetAttribute(cj_assemble_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-        if (e != cudaSuccess) return e;
-        attr_a = smem;
-    }
+    static size_t attr_r[MAX_DEVICES] = {}, attr_a[MAX_DEVICES] = {};
+    cudaError_t e = opt_in_smem((const void*)cj_reduce_kernel, smem, attr_r);
+    if (e != cudaSuccess) return e;
+    e = opt_in_smem((const void*)cj_assemble_kernel, smem, attr_a);
+    if (e != cudaSuccess) return e;
     cj_init_kernel<<<16, 256, 0, st>>>(n, a.ipiv, a.cand_v, a.cand_i, grid);
     e = cudaGetLastError();
     if (e != cudaSuccess) return e;
@@ -825,18 +819,11 @@ cudaError_t launch_ldiv_cj(const LdivArgs& a, int nrhs, cudaStream_t st)
     if (nrhs <= 0 || n <= 0) return cudaSuccess;
     if (n > CJ_NMAX || !a.Y || a.ycap < 2) return cudaErrorInvalidValue;
     const size_t smem = cj_smem(n);
-    static size_t attr_zi = 0, attr_z = 0;
-    cudaError_t e = cudaSuccess;
-    if (smem > attr_zi) {
-        e = cudaFuncSetAttribute(cj_zinv_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-        if (e != cudaSuccess) return e;
-        attr_zi = smem;
-    }
-    if (smem > attr_z) {
-        e = cudaFuncSetAttribute(cj_z_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-        if (e != cudaSuccess) return e;
-        attr_z = smem;
-    }
+    static size_t attr_zi[MAX_DEVICES] = {}, attr_z[MAX_DEVICES] = {};
+    cudaError_t e = opt_in_smem((const void*)cj_zinv_kernel, smem, attr_zi);
+    if (e != cudaSuccess) return e;
+    e = opt_in_smem((const void*)cj_z_kernel, smem, attr_z);
+    if (e != cudaSuccess) return e;
     if (a.mode == 1) {  // applyZinv!
         cj_zinv_kernel<<<nrhs, CJT, smem, st>>>(n, a.F, a.perm, a.iscale, a.X, a.ldx, 0, nullptr, 0, 0, a.done, a.tol);
         return cudaGetLastError();

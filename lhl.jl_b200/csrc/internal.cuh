@@ -7,6 +7,32 @@
 
 namespace lhl {
 
+// Launch settings that belong to a device.  A kernel's dynamic shared-memory opt-in is an
+// attribute of the function in one device's context, and SM counts and occupancy are per
+// device, so a process that drives several GPUs (a Julia session switching devices, one
+// host thread per GPU) needs them on every device it launches on.  The launchers keep one
+// entry per device ordinal, filled the first time that device is current.
+constexpr int MAX_DEVICES = 64;
+
+inline cudaError_t current_device(int* dev)
+{
+    cudaError_t e = cudaGetDevice(dev);
+    if (e == cudaSuccess && (*dev < 0 || *dev >= MAX_DEVICES)) e = cudaErrorInvalidDevice;
+    return e;
+}
+
+// Opts fn in to `bytes` of dynamic shared memory on the current device, unless it already
+// holds at least that much there (set[dev] keeps the largest size set on device dev).
+inline cudaError_t opt_in_smem(const void* fn, size_t bytes, size_t (&set)[MAX_DEVICES])
+{
+    int dev = 0;
+    cudaError_t e = current_device(&dev);
+    if (e != cudaSuccess || bytes <= set[dev]) return e;
+    e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+    if (e == cudaSuccess) set[dev] = bytes;
+    return e;
+}
+
 // Device buffers of one reduction (see reduce.cu).
 struct RedArgs {
     int n;

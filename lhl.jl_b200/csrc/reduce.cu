@@ -1993,18 +1993,19 @@ constexpr size_t REDUCE_DSMEM = (size_t)T64_SLOTS * TILE64_BYTES > (size_t)PBOX_
 
 int reduce_grid_size()
 {
-    static int g = 0;
-    if (g == 0) {
-        int dev = 0, sms = 0, per = 0;
-        cudaGetDevice(&dev);
+    static int g_of[MAX_DEVICES] = {};
+    int dev = 0;
+    if (current_device(&dev) != cudaSuccess) return 0;
+    if (g_of[dev] == 0) {
+        int sms = 0, per = 0;
         cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
         if (cudaFuncSetAttribute(reduce_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)REDUCE_DSMEM) !=
             cudaSuccess)
             return 0;
         cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, reduce_kernel, RT, REDUCE_DSMEM);
-        g = sms * (per > 0 ? 1 : 0);
+        g_of[dev] = sms * (per > 0 ? 1 : 0);
     }
-    return g;
+    return g_of[dev];
 }
 
 // 2-D tensor map of a column-major FP64 array (rows x cols, leading dimension ld) in

@@ -778,13 +778,9 @@ cudaError_t launch_reduce_mixed_lazy(MixArgs a, const MixPlan& pl, cudaStream_t 
     a.ring = lazy_ring(pl.ldr);
     if (a.ring == 0) return cudaErrorInvalidValue;
     const size_t smem = lazy_smem_bytes(pl.ldr, a.ring);
-    static size_t attr = 0;
-    if (smem > attr) {
-        cudaError_t e = cudaFuncSetAttribute(reduce_mixed_lazy_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                             (int)smem);
-        if (e != cudaSuccess) return e;
-        attr = smem;
-    }
+    static size_t attr[MAX_DEVICES] = {};
+    cudaError_t e = opt_in_smem((const void*)reduce_mixed_lazy_kernel, smem, attr);
+    if (e != cudaSuccess) return e;
     void* args[] = {&a};
     return cudaLaunchCooperativeKernel((const void*)reduce_mixed_lazy_kernel, dim3(pl.grid), dim3(MT), args, smem,
                                        st);
@@ -910,12 +906,9 @@ cudaError_t launch_lazy_finish(int n, double* F, double* Ht, cudaStream_t st)
 {
     cudaError_t e = launch_ht_fill(n, F, Ht, st);
     if (e != cudaSuccess || n < 3) return e;
-    static bool attr = false;
-    if (!attr) {
-        e = cudaFuncSetAttribute(lz_top_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(TopSmem));
-        if (e != cudaSuccess) return e;
-        attr = true;
-    }
+    static size_t attr[MAX_DEVICES] = {};
+    e = opt_in_smem((const void*)lz_top_kernel, sizeof(TopSmem), attr);
+    if (e != cudaSuccess) return e;
     dim3 grid((n + TPN - 1) / TPN, (n + TPM - 1) / TPM);
     lz_top_kernel<<<grid, TPT, sizeof(TopSmem), st>>>(n, F, Ht);
     e = cudaGetLastError();

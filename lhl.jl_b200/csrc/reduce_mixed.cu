@@ -483,13 +483,10 @@ cudaError_t launch_reduce_mixed(MixArgs a, const MixPlan& pl, cudaStream_t st)
     if (!pl.ok) return cudaErrorInvalidValue;
     a.rpc = pl.rpc;
     a.ldr = pl.ldr;
-    static size_t attr[2] = {0, 0};
+    static size_t attr[2][MAX_DEVICES] = {};
     const void* fn = pl.smem_rows ? (const void*)reduce_mixed_kernel<true> : (const void*)reduce_mixed_kernel<false>;
-    if (pl.smem > attr[pl.smem_rows]) {
-        cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)pl.smem);
-        if (e != cudaSuccess) return e;
-        attr[pl.smem_rows] = pl.smem;
-    }
+    cudaError_t e = opt_in_smem(fn, pl.smem, attr[pl.smem_rows ? 1 : 0]);
+    if (e != cudaSuccess) return e;
     void* args[] = {&a};
     return cudaLaunchCooperativeKernel(fn, dim3(pl.grid), dim3(MT), args, pl.smem, st);
 }

@@ -315,12 +315,9 @@ cudaError_t launch_linv(int n, const double* F, int ldf, double* linv, cudaStrea
 {
     if (n <= 0) return cudaSuccess;
     const size_t smem = 2 * (size_t)ZR * (ZR + 1) * sizeof(double);
-    static bool attr = false;
-    if (!attr) {
-        cudaError_t e = cudaFuncSetAttribute(linv_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-        if (e != cudaSuccess) return e;
-        attr = true;
-    }
+    static size_t attr[MAX_DEVICES] = {};
+    cudaError_t e = opt_in_smem((const void*)linv_kernel, smem, attr);
+    if (e != cudaSuccess) return e;
     linv_kernel<<<(n + ZR - 1) / ZR, ZR, smem, st>>>(n, F, ldf, linv);
     return cudaGetLastError();
 }
@@ -796,15 +793,17 @@ static cudaError_t run_zinv(ZArgs z, cudaStream_t st)
     if ((size_t)nblk * ntile > (size_t)z.nflags) return cudaErrorInvalidValue;
     cudaError_t e = cudaMemsetAsync(z.flags, 0, (size_t)nblk * ntile * sizeof(int), st);
     if (e != cudaSuccess) return e;
-    static int maxgrid = 0;
-    if (maxgrid == 0) {
-        int dev = 0, sms = 0, per = 0;
-        cudaGetDevice(&dev);
+    static int maxgrid_of[MAX_DEVICES] = {};
+    int dev = 0;
+    e = current_device(&dev);
+    if (e != cudaSuccess) return e;
+    if (maxgrid_of[dev] == 0) {
+        int sms = 0, per = 0;
         cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
         cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, zl_kernel<false>, ZIT, 0);
-        maxgrid = sms * (per > 0 ? per : 1);
+        maxgrid_of[dev] = sms * (per > 0 ? per : 1);
     }
-    const int grid = min(nblk * ntile, maxgrid);
+    const int grid = min(nblk * ntile, maxgrid_of[dev]);
     void* args[] = {&z};
     return cudaLaunchCooperativeKernel((void*)zl_kernel<false>, dim3(grid), dim3(ZIT), args, 0, st);
 }
@@ -1051,17 +1050,19 @@ static cudaError_t run_zinv_wide(ZArgs z, cudaStream_t st)
     cudaError_t e = cudaMemsetAsync(z.flags, 0, (size_t)nblk * ntile * sizeof(int), st);
     if (e != cudaSuccess) return e;
     const size_t smem = sizeof(ZwSmem);
-    static int maxgrid = 0;
-    if (maxgrid == 0) {
+    static int maxgrid_of[MAX_DEVICES] = {};
+    int dev = 0;
+    e = current_device(&dev);
+    if (e != cudaSuccess) return e;
+    if (maxgrid_of[dev] == 0) {
         e = cudaFuncSetAttribute(zlw_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
         if (e != cudaSuccess) return e;
-        int dev = 0, sms = 0, per = 0;
-        cudaGetDevice(&dev);
+        int sms = 0, per = 0;
         cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
         cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, zlw_kernel<false>, ZWT, smem);
-        maxgrid = sms * (per > 0 ? per : 1);
+        maxgrid_of[dev] = sms * (per > 0 ? per : 1);
     }
-    const int grid = min(nblk * ntile, maxgrid);
+    const int grid = min(nblk * ntile, maxgrid_of[dev]);
     void* args[] = {&z};
     return cudaLaunchCooperativeKernel((void*)zlw_kernel<false>, dim3(grid), dim3(ZWT), args, smem, st);
 }
@@ -1070,13 +1071,9 @@ static cudaError_t run_zmul(const ZArgs& z, cudaStream_t st)
 {
     if (z.m >= ZW_MIN_COLUMNS) {
         const size_t smem = sizeof(ZwSmem);
-        static bool attr = false;
-        if (!attr) {
-            cudaError_t e = cudaFuncSetAttribute(zlw_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                                 (int)smem);
-            if (e != cudaSuccess) return e;
-            attr = true;
-        }
+        static size_t attr[MAX_DEVICES] = {};
+        cudaError_t e = opt_in_smem((const void*)zlw_kernel<true>, smem, attr);
+        if (e != cudaSuccess) return e;
         const int nblk = (z.n + ZWR - 1) / ZWR, ntile = (z.m + ZWC - 1) / ZWC;
         zlw_kernel<true><<<nblk * ntile, ZWT, smem, st>>>(z);
         return cudaGetLastError();
@@ -1160,11 +1157,10 @@ cudaError_t launch_ldiv(const LdivArgs& a, int nrhs, cudaStream_t st)
     const size_t hsm = (size_t)a.n * 2 * sizeof(double) + (size_t)a.n + 16;
     // dynamic + static shared memory must stay within the 227 KB a CTA may use
     if (hsm > 200 * 1024) return cudaErrorInvalidValue;
-    static size_t attr = 0;
-    if (hsm > 32 * 1024 && hsm > attr) {  // the kernel's static shared arrays add about 8.5 KB
-        cudaError_t e = cudaFuncSetAttribute(hess_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)hsm);
+    static size_t attr[MAX_DEVICES] = {};
+    if (hsm > 32 * 1024) {  // the kernel's static shared arrays add about 8.5 KB
+        cudaError_t e = opt_in_smem((const void*)hess_kernel, hsm, attr);
         if (e != cudaSuccess) return e;
-        attr = hsm;
     }
     // Gt through TMA: even n (16-byte row pitch and box origins) and room for >= 2 slots
     const size_t vec = (size_t)a.n * 2 * sizeof(double) + (size_t)a.n + 16;
@@ -1174,14 +1170,8 @@ cudaError_t launch_ldiv(const LdivArgs& a, int nrhs, cudaStream_t st)
     bool use_tma = (a.n % 2 == 0) && a.n >= 2 && ns >= 2 && a.nshifts > 0 &&
                    make_tmap_2d(&tmG, a.Gt, a.ldg, a.nshifts * a.n, a.ldg, HB_ROWS, HB_COLS);
     if (use_tma) {
-        static size_t tattr = 0;
-        if (tsm > tattr) {
-            if (cudaFuncSetAttribute(hess_tma_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)tsm) !=
-                cudaSuccess)
-                use_tma = false;
-            else
-                tattr = tsm;
-        }
+        static size_t tattr[MAX_DEVICES] = {};
+        if (opt_in_smem((const void*)hess_tma_kernel, tsm, tattr) != cudaSuccess) use_tma = false;
     }
     for (int c0 = 0; c0 < nrhs; c0 += a.ycap) {
         const int cnt = min(a.ycap, nrhs - c0);
