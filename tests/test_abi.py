@@ -153,3 +153,24 @@ def test_configs_are_seeded_and_shaped():
     c2a, c2b = configs.config2(8), configs.config2(8)
     assert (c2a["J"] == c2b["J"]).all() and (c2a["tau"] == c2b["tau"]).all()
     assert (-c2a["tau"] >= 1e-4).all() and (-c2a["tau"] <= 1e-1).all()
+
+
+def test_launch_settings_are_cached_per_device():
+    """A kernel's dynamic shared-memory opt-in belongs to one device's context, and SM counts and
+    cooperative grid sizes are per device: a launcher that cached them in one process-wide
+    variable would launch with the wrong settings once a process switches devices.  Every such
+    cache in the CUDA sources is an array indexed by the device ordinal."""
+    csrc = os.path.join(REPO, "lhl.jl_b200", "csrc")
+    scalar_cache = re.compile(r"^\s*static\s+(?:bool|int|size_t|unsigned)\s+\w+\s*(?:=\s*[^;{]+)?;", re.M)
+    bad = []
+    for name in sorted(os.listdir(csrc)):
+        if not name.endswith((".cu", ".cuh")):
+            continue
+        src = open(os.path.join(csrc, name)).read()
+        bad += [f"{name}: {m.group(0).strip()}" for m in scalar_cache.finditer(src)]
+        # a dynamic shared-memory opt-in outside the per-device helper sits in a per-device branch
+        for m in re.finditer(r"cudaFuncSetAttribute\(", src):
+            head = src[max(0, m.start() - 600):m.start()]
+            if name != "internal.cuh" and "_of[dev]" not in head and "MAX_DEVICES" not in head:
+                bad.append(f"{name}: cudaFuncSetAttribute outside a per-device cache")
+    assert not bad, bad
